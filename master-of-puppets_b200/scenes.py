@@ -1,0 +1,384 @@
+"""Seeded synthetic scenes for the CPU software-rasterizer frame path.
+
+Every workload the tests and the benchmark render is built here, once, from a
+seed, so that the reference CPU backend, the plain-C oracle and the CUDA
+backend all consume byte-identical vertex/index arrays, matrices, materials,
+textures and lights.
+
+Vertex layout is the reference's fixed ``MopVertex`` (include/mop/types.h:58):
+position f32x3, normal f32x3, colour RGBA f32x4, uv f32x2 = 12 floats, 48 B.
+Matrices are column-major ``d[col*4+row]`` (include/mop/types.h:39).
+
+The scene descriptions follow the workloads the project is measured on:
+
+* ``config1``  800x600, ssaa 1, UV sphere 64x32 at (0,0.5,0) + 20x20 ground
+  plane, one directional light, untextured GGX materials.
+* ``config2``  1920x1080, ssaa 2, 256 mesh instances (icospheres subdiv 4-6 and
+  64x128 tori) with random TRS, 1 directional + 4 point + 2 spot lights,
+  1024^2 value-noise base-colour textures, procedural-sky IBL, ACES.
+* ``config3``  1920x1080, ssaa 1: clipping/depth stress (near-plane
+  stragglers, out-of-frustum triangles, coplanar pairs with distinct IDs).
+* ``small_*``  reduced-size variants for fast parity tests.
+"""
+from __future__ import annotations
+
+import dataclasses
+import math
+from typing import List, Optional, Tuple
+
+import numpy as np
+
+LIGHT_DIRECTIONAL, LIGHT_POINT, LIGHT_SPOT = 0, 1, 2
+POST_GAMMA, POST_TONEMAP, POST_VIGNETTE, POST_FOG, POST_FXAA = 1, 2, 4, 8, 16
+DEFAULT_POST = POST_GAMMA | POST_FXAA  # reference viewport.c:646
+
+
+@dataclasses.dataclass
+class Mesh:
+    vertices: np.ndarray          # float32 [V, 12]
+    indices: np.ndarray           # uint32 [I]
+    object_id: int
+    transform: np.ndarray         # float32 [16], column-major
+    metallic: float = 0.0
+    roughness: float = 0.5
+    has_material: bool = True
+    texture: int = -1
+    opacity: float = 1.0
+
+    @property
+    def triangle_count(self) -> int:
+        return int(self.indices.size // 3)
+
+
+@dataclasses.dataclass
+class Light:
+    type: int
+    position: Tuple[float, float, float] = (0.0, 0.0, 0.0)
+    direction: Tuple[float, float, float] = (0.0, -1.0, 0.0)
+    color: Tuple[float, float, float, float] = (1.0, 1.0, 1.0, 1.0)
+    intensity: float = 1.0
+    range: float = 0.0
+    spot_inner_cos: float = 0.95
+    spot_outer_cos: float = 0.85
+    active: bool = True
+
+
+@dataclasses.dataclass
+class Scene:
+    name: str
+    width: int
+    height: int
+    ssaa: int
+    eye: Tuple[float, float, float]
+    target: Tuple[float, float, float]
+    up: Tuple[float, float, float] = (0.0, 1.0, 0.0)
+    fov_deg: float = 45.0
+    near: float = 0.1
+    far: float = 100.0
+    clear: Tuple[float, float, float, float] = (0.12, 0.13, 0.16, 1.0)
+    ambient: float = 0.25
+    exposure: float = 1.0
+    post_effects: int = DEFAULT_POST
+    meshes: List[Mesh] = dataclasses.field(default_factory=list)
+    textures: List[np.ndarray] = dataclasses.field(default_factory=list)  # uint8 [h, w, 4]
+    lights: List[Light] = dataclasses.field(default_factory=list)
+    env: int = 0                  # 0 none, 1 procedural sky IBL
+    sun_dir: Tuple[float, float, float] = (0.5, 0.7, 0.3)
+    turbidity: float = 3.0
+    ground_albedo: float = 0.3
+    env_rotation: float = 0.0
+    env_intensity: float = 1.0
+    smooth: bool = True           # MOP_SHADING_SMOOTH (viewport default)
+
+    @property
+    def samples(self) -> int:
+        return self.width * self.ssaa * self.height * self.ssaa
+
+    @property
+    def pixels(self) -> int:
+        return self.width * self.height
+
+    @property
+    def triangle_count(self) -> int:
+        return sum(m.triangle_count for m in self.meshes)
+
+
+# --------------------------------------------------------------------------
+# matrices (column-major float32)
+# --------------------------------------------------------------------------
+
+def mat_identity() -> np.ndarray:
+    m = np.zeros(16, np.float32)
+    m[0] = m[5] = m[10] = m[15] = 1.0
+    return m
+
+
+def mat_trs(translation, rot3x3, scale) -> np.ndarray:
+    """World = T * R * S, computed in float64 then rounded once to float32.
+
+    The result is just input data: both renderers receive the same float32
+    matrix, so how it was produced does not affect parity.
+    """
+    m = np.zeros((4, 4), np.float64)
+    m[:3, :3] = np.asarray(rot3x3, np.float64) * np.asarray(scale, np.float64)[None, :]
+    m[:3, 3] = translation
+    m[3, 3] = 1.0
+    return m.T.reshape(16).astype(np.float32)  # column-major flatten
+
+
+def random_rotation(rng: np.random.Generator) -> np.ndarray:
+    q = rng.normal(size=4)
+    q /= np.linalg.norm(q)
+    w, x, y, z = q
+    return np.array([
+        [1 - 2 * (y * y + z * z), 2 * (x * y - z * w), 2 * (x * z + y * w)],
+        [2 * (x * y + z * w), 1 - 2 * (x * x + z * z), 2 * (y * z - x * w)],
+        [2 * (x * z - y * w), 2 * (y * z + x * w), 1 - 2 * (x * x + y * y)],
+    ])
+
+
+# --------------------------------------------------------------------------
+# geometry
+# --------------------------------------------------------------------------
+
+def _pack(pos, nrm, col, uv) -> np.ndarray:
+    v = np.zeros((pos.shape[0], 12), np.float32)
+    v[:, 0:3] = pos
+    v[:, 3:6] = nrm
+    v[:, 6:10] = col
+    v[:, 10:12] = uv
+    return v
+
+
+def uv_sphere(segments: int, rings: int, radius: float, color) -> Tuple[np.ndarray, np.ndarray]:
+    """UV sphere with (rings+1)*(segments+1) vertices; the degenerate pole
+    triangles are dropped, giving segments*(2*rings-2) triangles (3,968 for
+    64x32)."""
+    th = np.linspace(0.0, math.pi, rings + 1)
+    ph = np.linspace(0.0, 2.0 * math.pi, segments + 1)
+    T, P = np.meshgrid(th, ph, indexing="ij")
+    n = np.stack([np.sin(T) * np.cos(P), np.cos(T), np.sin(T) * np.sin(P)], -1).reshape(-1, 3)
+    uv = np.stack([P / (2 * math.pi), T / math.pi], -1).reshape(-1, 2)
+    col = np.tile(np.asarray(color, np.float32), (n.shape[0], 1))
+    verts = _pack(n * radius, n, col, uv)
+    idx = []
+    for r in range(rings):
+        for s in range(segments):
+            a = r * (segments + 1) + s
+            b = a + segments + 1
+            if r != 0:
+                idx += [a, a + 1, b]
+            if r != rings - 1:
+                idx += [a + 1, b + 1, b]
+    return verts, np.asarray(idx, np.uint32)
+
+
+def ground_plane(size: float, color) -> Tuple[np.ndarray, np.ndarray]:
+    h = size * 0.5
+    pos = np.array([[-h, 0, -h], [h, 0, -h], [h, 0, h], [-h, 0, h]], np.float32)
+    nrm = np.tile(np.array([0, 1, 0], np.float32), (4, 1))
+    col = np.tile(np.asarray(color, np.float32), (4, 1))
+    uv = np.array([[0, 0], [1, 0], [1, 1], [0, 1]], np.float32)
+    return _pack(pos, nrm, col, uv), np.array([0, 2, 1, 0, 3, 2], np.uint32)
+
+
+def icosphere(subdiv: int, radius: float, color) -> Tuple[np.ndarray, np.ndarray]:
+    """Icosahedron subdivided ``subdiv`` times: 20*4^subdiv triangles."""
+    t = (1.0 + math.sqrt(5.0)) / 2.0
+    verts = [(-1, t, 0), (1, t, 0), (-1, -t, 0), (1, -t, 0), (0, -1, t), (0, 1, t),
+             (0, -1, -t), (0, 1, -t), (t, 0, -1), (t, 0, 1), (-t, 0, -1), (-t, 0, 1)]
+    verts = [np.array(v, np.float64) / np.linalg.norm(v) for v in verts]
+    faces = [(0, 11, 5), (0, 5, 1), (0, 1, 7), (0, 7, 10), (0, 10, 11), (1, 5, 9), (5, 11, 4),
+             (11, 10, 2), (10, 7, 6), (7, 1, 8), (3, 9, 4), (3, 4, 2), (3, 2, 6), (3, 6, 8),
+             (3, 8, 9), (4, 9, 5), (2, 4, 11), (6, 2, 10), (8, 6, 7), (9, 8, 1)]
+    for _ in range(subdiv):
+        cache = {}
+        nf = []
+
+        def mid(a, b):
+            key = (a, b) if a < b else (b, a)
+            if key not in cache:
+                m = verts[a] + verts[b]
+                verts.append(m / np.linalg.norm(m))
+                cache[key] = len(verts) - 1
+            return cache[key]
+
+        for a, b, c in faces:
+            ab, bc, ca = mid(a, b), mid(b, c), mid(c, a)
+            nf += [(a, ab, ca), (b, bc, ab), (c, ca, bc), (ab, bc, ca)]
+        faces = nf
+    n = np.asarray(verts, np.float64)
+    uv = np.stack([np.arctan2(n[:, 2], n[:, 0]) / (2 * math.pi) + 0.5,
+                   np.arcsin(np.clip(n[:, 1], -1, 1)) / math.pi + 0.5], -1)
+    col = np.tile(np.asarray(color, np.float32), (n.shape[0], 1))
+    # Counter-clockwise seen from outside: the reference's front faces.
+    idx = np.asarray(faces, np.uint32).reshape(-1)
+    return _pack(n * radius, n, col, uv), idx
+
+
+def torus(major_seg: int, minor_seg: int, R: float, r: float, color) -> Tuple[np.ndarray, np.ndarray]:
+    """Torus with major_seg x minor_seg quads = 2*major*minor triangles."""
+    u = np.linspace(0, 2 * math.pi, major_seg + 1)
+    v = np.linspace(0, 2 * math.pi, minor_seg + 1)
+    U, V = np.meshgrid(u, v, indexing="ij")
+    cx, cz = np.cos(U), np.sin(U)
+    pos = np.stack([(R + r * np.cos(V)) * cx, r * np.sin(V), (R + r * np.cos(V)) * cz], -1).reshape(-1, 3)
+    nrm = np.stack([np.cos(V) * cx, np.sin(V), np.cos(V) * cz], -1).reshape(-1, 3)
+    uv = np.stack([U / (2 * math.pi), V / (2 * math.pi)], -1).reshape(-1, 2)
+    col = np.tile(np.asarray(color, np.float32), (pos.shape[0], 1))
+    idx = []
+    for i in range(major_seg):
+        for j in range(minor_seg):
+            a = i * (minor_seg + 1) + j
+            b = a + minor_seg + 1
+            idx += [a, a + 1, b, a + 1, b + 1, b]
+    return _pack(pos, nrm, col, uv), np.asarray(idx, np.uint32)
+
+
+def value_noise_texture(rng: np.random.Generator, size: int, cells: int = 16) -> np.ndarray:
+    """Seeded value noise, RGBA8 [size, size, 4]."""
+    grid = rng.random((cells + 1, cells + 1, 3))
+    x = np.linspace(0, cells, size, endpoint=False)
+    xi = x.astype(np.int64)
+    xf = x - xi
+    xf = xf * xf * (3 - 2 * xf)
+    a = grid[xi][:, xi]
+    b = grid[xi][:, xi + 1]
+    c = grid[xi + 1][:, xi]
+    d = grid[xi + 1][:, xi + 1]
+    fx = xf[None, :, None]
+    fy = xf[:, None, None]
+    top = a * (1 - fx) + b * fx
+    bot = c * (1 - fx) + d * fx
+    rgb = top * (1 - fy) + bot * fy
+    tex = np.empty((size, size, 4), np.uint8)
+    tex[..., :3] = np.clip(rgb * 255.0 + 0.5, 0, 255).astype(np.uint8)
+    tex[..., 3] = 255
+    return tex
+
+
+def _mat_rand(rng):
+    return (float(rng.uniform(0.0, 1.0)), float(rng.uniform(0.05, 1.0)))
+
+
+def _color(rng):
+    return (*[float(c) for c in rng.uniform(0.0, 1.0, 3)], 1.0)
+
+
+# --------------------------------------------------------------------------
+# configurations
+# --------------------------------------------------------------------------
+
+def config1(seed: int = 1, width: int = 800, height: int = 600, ssaa: int = 1) -> Scene:
+    rng = np.random.default_rng(seed)
+    sc = Scene("config1", width, height, ssaa, eye=(0.0, 3.0, 8.0), target=(0.0, 0.0, 0.0),
+               fov_deg=45.0, near=0.1, far=100.0)
+    sc.lights.append(Light(LIGHT_DIRECTIONAL, direction=(-0.4, -0.9, -0.3), intensity=3.0))
+    c = _color(rng)
+    metallic, rough = _mat_rand(rng)
+    v, i = uv_sphere(64, 32, 1.0, c)
+    t = mat_identity()
+    t[13] = 0.5
+    sc.meshes.append(Mesh(v, i, 1, t, metallic, rough))
+    c = _color(rng)
+    metallic, rough = _mat_rand(rng)
+    v, i = ground_plane(20.0, c)
+    sc.meshes.append(Mesh(v, i, 2, mat_identity(), metallic, rough))
+    return sc
+
+
+def config2(seed: int = 2, width: int = 1920, height: int = 1080, ssaa: int = 2,
+            instances: int = 256, tex_size: int = 1024, n_textures: int = 4) -> Scene:
+    """Large static scene.  256 instances: one subdiv-6 and one subdiv-5
+    icosphere, 6 tori 64x128 and 248 subdiv-4 icospheres (1,470,464 tris)."""
+    rng = np.random.default_rng(seed)
+    sc = Scene("config2", width, height, ssaa, eye=(28.0, 18.0, 36.0), target=(0.0, 0.0, 0.0),
+               fov_deg=50.0, near=0.5, far=200.0, env=1, sun_dir=(0.4, 0.8, 0.35),
+               turbidity=3.0, ground_albedo=0.3)
+    sc.lights.append(Light(LIGHT_DIRECTIONAL, direction=(-0.3, -0.8, -0.5), intensity=2.5,
+                           color=(1.0, 0.96, 0.9, 1.0)))
+    for _ in range(4):
+        p = tuple(float(x) for x in rng.uniform(-18, 18, 3))
+        sc.lights.append(Light(LIGHT_POINT, position=p, intensity=float(rng.uniform(20, 80)),
+                               color=(*[float(x) for x in rng.uniform(0.5, 1.0, 3)], 1.0)))
+    for _ in range(2):
+        p = rng.uniform(-15, 15, 3)
+        p[1] = abs(p[1]) + 10.0
+        d = -p / np.linalg.norm(p)
+        sc.lights.append(Light(LIGHT_SPOT, position=tuple(float(x) for x in p),
+                               direction=tuple(float(x) for x in d),
+                               intensity=float(rng.uniform(100, 300)), range=0.0,
+                               spot_inner_cos=0.95, spot_outer_cos=0.85,
+                               color=(*[float(x) for x in rng.uniform(0.5, 1.0, 3)], 1.0)))
+    for _ in range(n_textures):
+        sc.textures.append(value_noise_texture(rng, tex_size))
+    kinds = ["s6", "s5"] + ["torus"] * 6 + ["s4"] * (instances - 8)
+    kinds = kinds[:instances]
+    rng.shuffle(kinds)
+    proto = {}
+    for k in set(kinds):
+        if k == "torus":
+            proto[k] = torus(64, 128, 1.0, 0.35, (1, 1, 1, 1))
+        else:
+            proto[k] = icosphere(int(k[1]), 1.0, (1, 1, 1, 1))
+    for n, k in enumerate(kinds):
+        v, i = proto[k]
+        v = v.copy()
+        v[:, 6:10] = _color(rng)
+        metallic, rough = _mat_rand(rng)
+        t = rng.uniform(-20, 20, 3)
+        s = float(math.exp(rng.uniform(math.log(0.2), math.log(3.0))))
+        m = mat_trs(t, random_rotation(rng), (s, s, s))
+        sc.meshes.append(Mesh(v, i, n + 1, m, metallic, rough, texture=int(rng.integers(0, n_textures))))
+    return sc
+
+
+def small_scene(seed: int = 7, width: int = 160, height: int = 120, ssaa: int = 1,
+                n_meshes: int = 6, lights: str = "mixed", textured: bool = True,
+                env: int = 0) -> Scene:
+    """A few spheres/tori with mixed lights; seconds on the oracle."""
+    rng = np.random.default_rng(seed)
+    sc = Scene(f"small{seed}", width, height, ssaa, eye=(4.0, 3.0, 7.0), target=(0.0, 0.3, 0.0),
+               fov_deg=50.0, near=0.1, far=50.0, env=env, sun_dir=(0.3, 0.8, 0.4))
+    if lights != "none":
+        sc.lights.append(Light(LIGHT_DIRECTIONAL, direction=(-0.4, -0.9, -0.3), intensity=2.0))
+    if lights == "mixed":
+        sc.lights.append(Light(LIGHT_POINT, position=(2.0, 2.0, 2.0), intensity=6.0,
+                               color=(1.0, 0.8, 0.6, 1.0)))
+        sc.lights.append(Light(LIGHT_POINT, position=(-2.0, 1.0, 1.0), intensity=4.0, range=6.0,
+                               color=(0.6, 0.8, 1.0, 1.0)))
+        sc.lights.append(Light(LIGHT_SPOT, position=(0.0, 4.0, 2.0), direction=(0.0, -1.0, -0.4),
+                               intensity=20.0, spot_inner_cos=0.95, spot_outer_cos=0.8))
+        sc.lights.append(Light(LIGHT_SPOT, position=(3.0, 3.0, -1.0), direction=(-0.6, -0.7, 0.2),
+                               intensity=10.0, range=8.0, spot_inner_cos=0.9, spot_outer_cos=0.7,
+                               active=True))
+        sc.lights.append(Light(LIGHT_POINT, position=(0.0, 1.0, 0.0), intensity=50.0, active=False))
+    if textured:
+        sc.textures.append(value_noise_texture(rng, 64, 8))
+    v, i = ground_plane(12.0, _color(rng))
+    m, r = _mat_rand(rng)
+    sc.meshes.append(Mesh(v, i, 1, mat_identity(), m, r))
+    for n in range(n_meshes):
+        c = _color(rng)
+        if n % 3 == 2:
+            v, i = torus(24, 12, 0.7, 0.25, c)
+        elif n % 3 == 1:
+            v, i = icosphere(2, 0.6, c)
+        else:
+            v, i = uv_sphere(16, 8, 0.6, c)
+        t = rng.uniform(-2.5, 2.5, 3)
+        t[1] = abs(t[1]) * 0.5 + 0.6
+        s = float(rng.uniform(0.6, 1.4))
+        mtx = mat_trs(t, random_rotation(rng), (s, s, s))
+        m, r = _mat_rand(rng)
+        tex = 0 if (textured and n % 2 == 0) else -1
+        sc.meshes.append(Mesh(v, i, n + 2, mtx, m, r, texture=tex))
+    return sc
+
+
+def pick_points(scene: Scene, n: int = 1000, seed: int = 11) -> np.ndarray:
+    rng = np.random.default_rng(seed)
+    xy = np.empty((n, 2), np.int32)
+    xy[:, 0] = rng.integers(0, scene.width, n)
+    xy[:, 1] = rng.integers(0, scene.height, n)
+    return xy

@@ -1,0 +1,201 @@
+"""ctypes driver for the plain-C oracle (oracle/liboracle.so).
+
+Test infrastructure only: builds the per-draw records a viewport would emit
+for a scene (EMIT_DRAW, reference src/core/viewport.c:2015-2088) and runs the
+serial restatement of the CPU frame path on them.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+ORACLE_SO = HERE / "liboracle.so"
+
+DEFAULT_LIGHT_DIR = (0.3, 1.0, 0.5)  # viewport default, reference viewport.c:641
+
+
+class OrLight(C.Structure):
+    _fields_ = [("type", C.c_int32), ("position", C.c_float * 3),
+                ("direction", C.c_float * 3), ("color", C.c_float * 4),
+                ("intensity", C.c_float), ("range", C.c_float),
+                ("spot_inner_cos", C.c_float), ("spot_outer_cos", C.c_float),
+                ("active", C.c_int32)]
+
+
+class OrDraw(C.Structure):
+    _fields_ = [("vertices", C.c_void_p), ("vertex_count", C.c_uint32),
+                ("indices", C.c_void_p), ("index_count", C.c_uint32),
+                ("object_id", C.c_uint32), ("model", C.c_float * 16),
+                ("mvp", C.c_float * 16), ("light_dir", C.c_float * 3),
+                ("ambient", C.c_float), ("opacity", C.c_float),
+                ("metallic", C.c_float), ("roughness", C.c_float),
+                ("depth_bias", C.c_float), ("cam_eye", C.c_float * 3),
+                ("smooth", C.c_int32), ("depth_test", C.c_int32),
+                ("backface_cull", C.c_int32), ("blend_mode", C.c_int32),
+                ("lights", C.POINTER(OrLight)), ("light_count", C.c_uint32),
+                ("texture", C.c_void_p), ("tex_w", C.c_int32), ("tex_h", C.c_int32)]
+
+
+class OrIBL(C.Structure):
+    _fields_ = [("irr", C.c_void_p), ("irr_w", C.c_int32), ("irr_h", C.c_int32),
+                ("pf", C.c_void_p), ("pf_w", C.c_int32), ("pf_h", C.c_int32),
+                ("pf_levels", C.c_int32), ("brdf", C.c_void_p), ("brdf_size", C.c_int32),
+                ("rotation", C.c_float), ("intensity", C.c_float)]
+
+
+class OrFrame(C.Structure):
+    _fields_ = [("width", C.c_int32), ("height", C.c_int32), ("ssaa", C.c_int32),
+                ("clear", C.c_float * 4), ("exposure", C.c_float),
+                ("post_effects", C.c_uint32), ("ibl", C.POINTER(OrIBL)),
+                ("color_full", C.c_void_p), ("depth", C.c_void_p),
+                ("object_id", C.c_void_p), ("color_presented", C.c_void_p),
+                ("hdr", C.c_void_p)]
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not ORACLE_SO.exists():
+            raise FileNotFoundError(f"oracle not built: {ORACLE_SO} (run make -C oracle oracle)")
+        _lib = C.CDLL(str(ORACLE_SO))
+        _lib.oracle_render.argtypes = [C.POINTER(OrFrame), C.POINTER(OrDraw), C.c_uint32]
+        _lib.oracle_camera.argtypes = [C.c_void_p] * 3 + [C.c_float] * 3 + [C.c_int] * 2 + [C.c_void_p] * 3
+        _lib.oracle_mat4_multiply.argtypes = [C.c_void_p] * 3
+        _lib.oracle_pick.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int,
+                                     C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+        _lib.oracle_gamma_lut.argtypes = [C.c_void_p]
+    return _lib
+
+
+def _f32(a):
+    return np.ascontiguousarray(a, np.float32)
+
+
+def camera(scene):
+    """(view, proj, eye) of the frame, as mop_viewport_render derives them."""
+    view = np.zeros(16, np.float32)
+    proj = np.zeros(16, np.float32)
+    eye = np.zeros(3, np.float32)
+    e, t, u = _f32(scene.eye), _f32(scene.target), _f32(scene.up)
+    lib().oracle_camera(e.ctypes.data, t.ctypes.data, u.ctypes.data, scene.fov_deg, scene.near,
+                        scene.far, scene.width, scene.height, view.ctypes.data, proj.ctypes.data,
+                        eye.ctypes.data)
+    return view, proj, eye
+
+
+def mat4_multiply(a, b):
+    a, b = _f32(a), _f32(b)
+    c = np.zeros(16, np.float32)
+    lib().oracle_mat4_multiply(a.ctypes.data, b.ctypes.data, c.ctypes.data)
+    return c
+
+
+def gamma_lut():
+    lut = np.zeros(256, np.uint8)
+    lib().oracle_gamma_lut(lut.ctypes.data)
+    return lut
+
+
+def _light(l):
+    s = OrLight()
+    s.type = l.type
+    s.position[:] = l.position
+    s.direction[:] = l.direction
+    s.color[:] = l.color
+    s.intensity = l.intensity
+    s.range = l.range
+    s.spot_inner_cos = l.spot_inner_cos
+    s.spot_outer_cos = l.spot_outer_cos
+    s.active = 1 if l.active else 0
+    return s
+
+
+def render(scene, ibl=None, want_hdr=False):
+    """Render `scene` with the oracle.  `ibl` is the dict returned by
+    refdrive.Reference.env_maps() (or None for no IBL)."""
+    L = lib()
+    view, proj, eye = camera(scene)
+    keep = []
+    lights = (OrLight * max(1, len(scene.lights)))()
+    for k, l in enumerate(scene.lights):
+        lights[k] = _light(l)
+    texs = [np.ascontiguousarray(t, np.uint8) for t in scene.textures]
+    draws = (OrDraw * max(1, len(scene.meshes)))()
+    amb = min(max(scene.ambient, 0.0), 1.0)
+    for k, m in enumerate(scene.meshes):
+        v = _f32(m.vertices)
+        i = np.ascontiguousarray(m.indices, np.uint32)
+        keep += [v, i]
+        d = draws[k]
+        d.vertices, d.vertex_count = v.ctypes.data, v.shape[0]
+        d.indices, d.index_count = i.ctypes.data, i.size
+        d.object_id = m.object_id
+        d.model[:] = [float(x) for x in m.transform]
+        d.mvp[:] = [float(x) for x in mat4_multiply(proj, mat4_multiply(view, m.transform))]
+        d.light_dir[:] = DEFAULT_LIGHT_DIR
+        d.ambient = amb
+        d.opacity = m.opacity
+        d.metallic = m.metallic if m.has_material else 0.0
+        d.roughness = m.roughness if m.has_material else 0.5
+        d.depth_bias = 0.0
+        d.cam_eye[:] = [float(x) for x in eye]
+        d.smooth = 1 if getattr(scene, "smooth", True) else 0
+        d.depth_test, d.backface_cull, d.blend_mode = 1, 1, 0
+        d.lights = lights
+        d.light_count = len(scene.lights)
+        if m.texture >= 0:
+            t = texs[m.texture]
+            d.texture, d.tex_h, d.tex_w = t.ctypes.data, t.shape[0], t.shape[1]
+    sw, sh = scene.width * scene.ssaa, scene.height * scene.ssaa
+    out = {
+        "color": np.zeros((scene.height, scene.width, 4), np.uint8),
+        "color_full": np.zeros((sh, sw, 4), np.uint8),
+        "depth": np.zeros((sh, sw), np.float32),
+        "object_id": np.zeros((sh, sw), np.uint32),
+        "view": view, "proj": proj, "eye": eye,
+    }
+    f = OrFrame()
+    f.width, f.height, f.ssaa = sw, sh, scene.ssaa
+    f.clear[:] = scene.clear
+    f.exposure = scene.exposure
+    f.post_effects = scene.post_effects
+    if ibl is not None:
+        arrs = [_f32(ibl["irr"]), _f32(ibl["pf"]), _f32(ibl["brdf"])]
+        keep += arrs
+        ib = OrIBL()
+        ib.irr, ib.irr_w, ib.irr_h = arrs[0].ctypes.data, ibl["irr_w"], ibl["irr_h"]
+        ib.pf, ib.pf_w, ib.pf_h, ib.pf_levels = arrs[1].ctypes.data, ibl["pf_w"], ibl["pf_h"], ibl["pf_levels"]
+        ib.brdf, ib.brdf_size = arrs[2].ctypes.data, ibl["brdf_size"]
+        ib.rotation, ib.intensity = ibl["rotation"], ibl["intensity"]
+        keep.append(ib)
+        f.ibl = C.pointer(ib)
+    f.color_full = out["color_full"].ctypes.data
+    f.depth = out["depth"].ctypes.data
+    f.object_id = out["object_id"].ctypes.data
+    f.color_presented = out["color"].ctypes.data
+    if want_hdr:
+        out["hdr"] = np.zeros((sh, sw, 4), np.float32)
+        f.hdr = out["hdr"].ctypes.data
+    rc = L.oracle_render(C.byref(f), draws, len(scene.meshes))
+    if rc != 0:
+        raise RuntimeError(f"oracle_render failed: {rc}")
+    return out
+
+
+def pick(scene, frame, xy):
+    xy = np.ascontiguousarray(xy, np.int32)
+    n = xy.shape[0]
+    ids = np.zeros(n, np.uint32)
+    dep = np.zeros(n, np.float32)
+    hits = np.zeros(n, np.int32)
+    oid = np.ascontiguousarray(frame["object_id"], np.uint32)
+    d = np.ascontiguousarray(frame["depth"], np.float32)
+    lib().oracle_pick(oid.ctypes.data, d.ctypes.data, scene.width, scene.height, scene.ssaa, n,
+                      xy.ctypes.data, ids.ctypes.data, dep.ctypes.data, hits.ctypes.data)
+    return ids, dep, hits

@@ -1,0 +1,120 @@
+/*
+ * mop_oracle.h — plain-C restatement of the reference CPU frame path.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This is the checker the CUDA backend is compared
+ * against; nothing in the product links it.  It restates, serially and in the
+ * reference's float evaluation order, the path
+ *   cpu_draw (reference src/backend/cpu/cpu_backend.c:528-629)
+ *   -> mop_sw_rasterize_triangle_full / mop_sw_rasterize_triangle
+ *      (src/rasterizer/rasterizer.c:2458-2612, 1093-1242)
+ *   -> smooth multi-light / flat / legacy smooth rasterisers
+ *   -> mop_sw_hdr_resolve (rasterizer.c:2776-2803)
+ *   -> mop_postprocess_apply (src/render/postprocess.c:24-116)
+ *   -> mop_viewport_read_color SSAA box (src/core/viewport.c:3364-3418)
+ *   -> mop_viewport_pick (viewport.c:3687-3749)
+ * and the camera chain that produces the view/projection matrices
+ * (viewport.c:1058-1130, src/interact/camera.c:35-63, src/math/math.c).
+ *
+ * Parity is pinned against the reference library itself (oracle/_ref, built
+ * from the reference sources by oracle/Makefile) on seeded scenes, and against
+ * golden fixtures committed under tests/golden/.
+ */
+#ifndef MOP_ORACLE_H
+#define MOP_ORACLE_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct OrLight {
+  int32_t type; /* 0 directional, 1 point, 2 spot */
+  float position[3];
+  float direction[3];
+  float color[4];
+  float intensity;
+  float range;
+  float spot_inner_cos;
+  float spot_outer_cos;
+  int32_t active;
+} OrLight;
+
+typedef struct OrDraw {
+  const float *vertices; /* vertex_count * 12 floats (MopVertex) */
+  uint32_t vertex_count;
+  const uint32_t *indices;
+  uint32_t index_count;
+  uint32_t object_id;
+  float model[16];
+  float mvp[16];
+  float light_dir[3];
+  float ambient;
+  float opacity;
+  float metallic;
+  float roughness;
+  float depth_bias;
+  float cam_eye[3];
+  int32_t smooth;        /* MOP_SHADING_SMOOTH */
+  int32_t depth_test;
+  int32_t backface_cull;
+  int32_t blend_mode;    /* MopBlendMode */
+  const OrLight *lights; /* NULL / 0 = legacy single-light path */
+  uint32_t light_count;
+  const uint8_t *texture; /* RGBA8 or NULL */
+  int32_t tex_w, tex_h;
+} OrDraw;
+
+typedef struct OrIBL {
+  const float *irr;
+  int32_t irr_w, irr_h;
+  const float *pf;
+  int32_t pf_w, pf_h, pf_levels;
+  const float *brdf;
+  int32_t brdf_size;
+  float rotation;
+  float intensity;
+} OrIBL;
+
+typedef struct OrFrame {
+  int32_t width, height; /* sample resolution (presented * ssaa) */
+  int32_t ssaa;
+  float clear[4];
+  float exposure;
+  uint32_t post_effects;
+  const OrIBL *ibl; /* NULL = no IBL maps bound */
+  /* outputs (caller-allocated; NULL to skip) */
+  uint8_t *color_full;      /* width*height*4, after resolve + post */
+  float *depth;             /* width*height */
+  uint32_t *object_id;      /* width*height */
+  uint8_t *color_presented; /* (width/ssaa)*(height/ssaa)*4 */
+  float *hdr;               /* width*height*4, before resolve */
+} OrFrame;
+
+/* Render one frame of draws in submission order.  Returns 0 on success. */
+int oracle_render(OrFrame *frame, const OrDraw *draws, uint32_t draw_count);
+
+/* Camera chain: mop_viewport_set_camera followed by the orbit re-derivation
+ * mop_viewport_render performs every frame.  width/height are the
+ * presentation size (the projection aspect). */
+void oracle_camera(const float eye[3], const float target[3], const float up[3],
+                   float fov_deg, float near_plane, float far_plane, int width,
+                   int height, float view[16], float proj[16],
+                   float eye_out[3]);
+
+/* c = a * b, column-major (mop_mat4_multiply, math.c:182-194). */
+void oracle_mat4_multiply(const float a[16], const float b[16], float c[16]);
+
+/* Pick at presentation pixels: ID/depth of the top-left sample of each
+ * SSAA block (viewport.c:3687-3749, cpu_backend.c:673-687). */
+void oracle_pick(const uint32_t *object_id, const float *depth, int width,
+                 int height, int ssaa, int n, const int32_t *xy,
+                 uint32_t *ids, float *depths, int32_t *hits);
+
+/* sRGB gamma byte map used by the post-process (postprocess.c:75-82). */
+void oracle_gamma_lut(uint8_t lut[256]);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

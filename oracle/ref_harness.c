@@ -1,0 +1,268 @@
+/*
+ * ref_harness.c — drives the unmodified reference library on its CPU backend.
+ *
+ * Test infrastructure only (see ref_harness.h).  Scene construction follows
+ * the parity rules for the CPU frame path:
+ *   - chrome off (mop_viewport_set_chrome, reference viewport.c:3934-3942) so
+ *     no gradient quad / grid draws are issued;
+ *   - the always-on outline overlay disabled (viewport.c:745);
+ *   - lights cleared, then the scene's lights added with cast_shadows=false
+ *     (the default sun would otherwise drive the shadow pass,
+ *     viewport.c:683-692, 2288-2442);
+ *   - base colour baked into vertex colours by the caller (CPU shading reads
+ *     vertex colour only); metallic/roughness through mop_mesh_set_material.
+ * Serial mode nulls the CPU device's tile pool so cpu_draw takes its
+ * single-threaded loop (reference cpu_backend.c:29-31, 589-620).
+ */
+#include "ref_harness.h"
+
+#include "core/viewport_internal.h"
+#include "rasterizer/rasterizer_mt.h"
+
+#include <mop/mop.h>
+#include <stdlib.h>
+#include <string.h>
+#include <time.h>
+#include <unistd.h>
+
+typedef struct RefH {
+  MopViewport *vp;
+  MopTexture **textures;
+  uint32_t texture_count;
+  int w, h, ssaa;
+  int threads;
+} RefH;
+
+static double now_ms(void) {
+  struct timespec ts;
+  clock_gettime(CLOCK_MONOTONIC, &ts);
+  return (double)ts.tv_sec * 1e3 + (double)ts.tv_nsec * 1e-6;
+}
+
+void *refh_create(const RefScene *sc) {
+  if (!sc || sc->width <= 0 || sc->height <= 0)
+    return NULL;
+  RefH *h = calloc(1, sizeof(RefH));
+  if (!h)
+    return NULL;
+  MopViewportDesc desc = {.width = sc->width,
+                          .height = sc->height,
+                          .backend = MOP_BACKEND_CPU,
+                          .reverse_z = false,
+                          .ssaa_factor = sc->ssaa};
+  h->vp = mop_viewport_create(&desc);
+  if (!h->vp) {
+    free(h);
+    return NULL;
+  }
+  MopViewport *vp = h->vp;
+  h->w = sc->width;
+  h->h = sc->height;
+  h->ssaa = vp->ssaa_factor;
+
+  long n = sysconf(_SC_NPROCESSORS_ONLN);
+  h->threads = n > 1 ? (int)n : 1;
+  if (sc->serial) {
+    /* The CPU device's only member is its tile pool pointer. */
+    MopSwThreadPool **pool = (MopSwThreadPool **)vp->device;
+    if (*pool) {
+      mop_sw_threadpool_destroy(*pool);
+      *pool = NULL;
+    }
+    h->threads = 1;
+  }
+
+  mop_viewport_set_chrome(vp, false);
+  mop_viewport_set_overlay_enabled(vp, MOP_OVERLAY_OUTLINE, false);
+  mop_viewport_set_clear_color(
+      vp, (MopColor){sc->clear_color[0], sc->clear_color[1],
+                     sc->clear_color[2], sc->clear_color[3]});
+  mop_viewport_set_ambient(vp, sc->ambient);
+  mop_viewport_set_exposure(vp, sc->exposure);
+  mop_viewport_set_post_effects(vp, sc->post_effects);
+  if (sc->flat)
+    mop_viewport_set_shading(vp, MOP_SHADING_FLAT);
+  mop_viewport_set_camera(
+      vp, (MopVec3){sc->eye[0], sc->eye[1], sc->eye[2]},
+      (MopVec3){sc->target[0], sc->target[1], sc->target[2]},
+      (MopVec3){sc->up[0], sc->up[1], sc->up[2]}, sc->fov_deg, sc->near_plane,
+      sc->far_plane);
+
+  mop_viewport_clear_lights(vp);
+  for (uint32_t i = 0; i < sc->light_count; i++) {
+    const RefLight *L = &sc->lights[i];
+    MopLight d = {
+        .type = (MopLightType)L->type,
+        .position = {L->position[0], L->position[1], L->position[2]},
+        .direction = {L->direction[0], L->direction[1], L->direction[2]},
+        .color = {L->color[0], L->color[1], L->color[2], L->color[3]},
+        .intensity = L->intensity,
+        .range = L->range,
+        .spot_inner_cos = L->spot_inner_cos,
+        .spot_outer_cos = L->spot_outer_cos,
+        .active = L->active != 0,
+        .cast_shadows = false,
+    };
+    MopLight *slot = mop_viewport_add_light(vp, &d);
+    /* add_light always activates its slot (reference light.c:26-71). */
+    if (slot && !L->active)
+      mop_viewport_remove_light(vp, slot);
+  }
+
+  if (sc->texture_count) {
+    h->textures = calloc(sc->texture_count, sizeof(MopTexture *));
+    h->texture_count = sc->texture_count;
+    for (uint32_t t = 0; t < sc->texture_count; t++)
+      h->textures[t] = mop_viewport_create_texture(vp, sc->tex_w[t],
+                                                   sc->tex_h[t], sc->tex_data[t]);
+  }
+
+  for (uint32_t m = 0; m < sc->mesh_count; m++) {
+    const RefMesh *rm = &sc->meshes[m];
+    MopMeshDesc md = {.vertices = (const MopVertex *)rm->vertices,
+                      .vertex_count = rm->vertex_count,
+                      .indices = rm->indices,
+                      .index_count = rm->index_count,
+                      .object_id = rm->object_id};
+    MopMesh *mesh = mop_viewport_add_mesh(vp, &md);
+    if (!mesh)
+      continue;
+    MopMat4 t;
+    memcpy(t.d, rm->transform, sizeof(t.d));
+    mop_mesh_set_transform(mesh, &t);
+    if (rm->has_material) {
+      MopMaterial mat = mop_material_default();
+      mat.metallic = rm->metallic;
+      mat.roughness = rm->roughness;
+      mop_mesh_set_material(mesh, &mat);
+    }
+    if (rm->texture >= 0 && (uint32_t)rm->texture < h->texture_count)
+      mop_mesh_set_texture(mesh, h->textures[rm->texture]);
+    if (rm->opacity != 1.0f)
+      mop_mesh_set_opacity(mesh, rm->opacity);
+  }
+
+  if (sc->env == 1) {
+    MopProceduralSkyDesc sky = {
+        .sun_direction = {sc->sun_dir[0], sc->sun_dir[1], sc->sun_dir[2]},
+        .turbidity = sc->turbidity,
+        .ground_albedo = sc->ground_albedo};
+    mop_viewport_set_procedural_sky(vp, &sky);
+    MopEnvironmentDesc env = {.type = MOP_ENV_PROCEDURAL_SKY,
+                              .rotation = sc->env_rotation,
+                              .intensity = sc->env_intensity};
+    mop_viewport_set_environment(vp, &env);
+  }
+  return h;
+}
+
+int refh_render(void *hp, RefFrame *out) {
+  RefH *h = hp;
+  if (!h)
+    return -1;
+  MopViewport *vp = h->vp;
+  if (mop_viewport_render(vp) != MOP_RENDER_OK)
+    return -2;
+  int w = 0, hh = 0;
+  const uint8_t *c = mop_viewport_read_color(vp, &w, &hh);
+  if (!c)
+    return -3;
+  if (out->color)
+    memcpy(out->color, c, (size_t)w * hh * 4);
+  int fw = 0, fh = 0;
+  const uint8_t *cf =
+      vp->rhi->framebuffer_read_color(vp->device, vp->framebuffer, &fw, &fh);
+  if (out->color_full && cf)
+    memcpy(out->color_full, cf, (size_t)fw * fh * 4);
+  const float *d =
+      vp->rhi->framebuffer_read_depth(vp->device, vp->framebuffer, &fw, &fh);
+  if (out->depth && d)
+    memcpy(out->depth, d, (size_t)fw * fh * sizeof(float));
+  const uint32_t *id = vp->rhi->framebuffer_read_object_id(
+      vp->device, vp->framebuffer, &fw, &fh);
+  if (out->object_id && id)
+    memcpy(out->object_id, id, (size_t)fw * fh * sizeof(uint32_t));
+  memcpy(out->view, vp->view_matrix.d, sizeof(out->view));
+  memcpy(out->proj, vp->projection_matrix.d, sizeof(out->proj));
+  out->eye[0] = vp->cam_eye.x;
+  out->eye[1] = vp->cam_eye.y;
+  out->eye[2] = vp->cam_eye.z;
+  MopFrameStats st = mop_viewport_get_stats(vp);
+  out->triangle_count = st.triangle_count;
+  out->frame_ms = st.frame_time_ms;
+  return 0;
+}
+
+int refh_pick(void *hp, int n, const int32_t *xy, uint32_t *ids, float *depths,
+              int32_t *hits) {
+  RefH *h = hp;
+  if (!h)
+    return -1;
+  for (int i = 0; i < n; i++) {
+    MopPickResult r = mop_viewport_pick(h->vp, xy[2 * i], xy[2 * i + 1]);
+    ids[i] = r.object_id;
+    depths[i] = r.depth;
+    hits[i] = r.hit ? 1 : 0;
+  }
+  return 0;
+}
+
+int refh_env_maps(void *hp, const float **irr, int32_t *iw, int32_t *ih,
+                  const float **pf, int32_t *pw, int32_t *ph, int32_t *levels,
+                  const float **brdf, int32_t *brdf_size) {
+  RefH *h = hp;
+  if (!h || !h->vp->env_irradiance_data)
+    return -1;
+  MopViewport *vp = h->vp;
+  *irr = vp->env_irradiance_data;
+  *iw = vp->env_irradiance_w;
+  *ih = vp->env_irradiance_h;
+  *pf = vp->env_prefiltered_data;
+  *pw = vp->env_prefiltered_w;
+  *ph = vp->env_prefiltered_h;
+  *levels = vp->env_prefiltered_levels;
+  *brdf = vp->env_brdf_lut_data;
+  *brdf_size = 256; /* BRDF_LUT_SIZE, reference viewport.c:2702 */
+  return 0;
+}
+
+static int cmp_double(const void *a, const void *b) {
+  double x = *(const double *)a, y = *(const double *)b;
+  return (x > y) - (x < y);
+}
+
+double refh_time_frames(void *hp, int warm, int frames) {
+  RefH *h = hp;
+  if (!h || frames <= 0)
+    return -1.0;
+  for (int i = 0; i < warm; i++) {
+    mop_viewport_render(h->vp);
+    mop_viewport_read_color(h->vp, NULL, NULL);
+  }
+  double *t = malloc(sizeof(double) * (size_t)frames);
+  for (int i = 0; i < frames; i++) {
+    double t0 = now_ms();
+    mop_viewport_render(h->vp);
+    mop_viewport_read_color(h->vp, NULL, NULL);
+    t[i] = now_ms() - t0;
+  }
+  qsort(t, (size_t)frames, sizeof(double), cmp_double);
+  double med = t[frames / 2];
+  free(t);
+  return med;
+}
+
+int refh_num_threads(void *hp) {
+  RefH *h = hp;
+  return h ? h->threads : 0;
+}
+
+void refh_destroy(void *hp) {
+  RefH *h = hp;
+  if (!h)
+    return;
+  /* Textures belong to the viewport and are released with it. */
+  free(h->textures);
+  mop_viewport_destroy(h->vp);
+  free(h);
+}

@@ -1,0 +1,99 @@
+/*
+ * ref_harness.h — test-only driver for the reference library's CPU backend.
+ *
+ * This is oracle infrastructure: it builds a viewport through the reference's
+ * public scene API (include/mop/core/viewport.h, scene.h, light.h,
+ * environment.h), renders with MOP_BACKEND_CPU, and copies out the buffers a
+ * parity test compares.  It is compiled together with the unmodified
+ * reference sources into oracle/_ref/libmopref.so by oracle/Makefile.
+ *
+ * All structs are plain C so that ctypes (tests/, bench.py cpu leg) can bind
+ * them without headers.
+ */
+#ifndef MOP_REF_HARNESS_H
+#define MOP_REF_HARNESS_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct RefMesh {
+  const float *vertices;    /* vertex_count * 12 floats, MopVertex layout   */
+  uint32_t vertex_count;
+  const uint32_t *indices;
+  uint32_t index_count;
+  uint32_t object_id;
+  float transform[16];      /* column-major world matrix                   */
+  float metallic;
+  float roughness;
+  int32_t has_material;     /* 0: reference defaults (metallic 0, rough .5) */
+  int32_t texture;          /* index into RefScene textures, -1 = none      */
+  float opacity;
+} RefMesh;
+
+typedef struct RefLight {
+  int32_t type;             /* 0 directional, 1 point, 2 spot              */
+  float position[3];
+  float direction[3];
+  float color[4];
+  float intensity;
+  float range;
+  float spot_inner_cos;
+  float spot_outer_cos;
+  int32_t active;
+} RefLight;
+
+typedef struct RefScene {
+  int32_t width, height, ssaa;
+  float clear_color[4];
+  float eye[3], target[3], up[3];
+  float fov_deg, near_plane, far_plane;
+  float ambient;
+  float exposure;
+  uint32_t post_effects;
+  uint32_t mesh_count;
+  const RefMesh *meshes;
+  uint32_t texture_count;
+  const int32_t *tex_w;
+  const int32_t *tex_h;
+  const uint8_t *const *tex_data;
+  uint32_t light_count;
+  const RefLight *lights;
+  int32_t env;              /* 0: gradient (no IBL), 1: procedural sky IBL */
+  float sun_dir[3];
+  float turbidity, ground_albedo;
+  float env_rotation, env_intensity;
+  int32_t serial;           /* 1: null the tile thread pool (serial path)  */
+  int32_t flat;             /* 1: MOP_SHADING_FLAT for the viewport        */
+} RefScene;
+
+typedef struct RefFrame {
+  uint8_t *color;           /* presented RGBA8, W*H*4 (after SSAA box)     */
+  uint8_t *color_full;      /* optional sample-res RGBA8 (may be NULL)     */
+  float *depth;             /* sample-res float                             */
+  uint32_t *object_id;      /* sample-res uint32                            */
+  float view[16];
+  float proj[16];
+  float eye[3];
+  uint32_t triangle_count;  /* MopFrameStats.triangle_count                 */
+  double frame_ms;          /* MopFrameStats.frame_time_ms                  */
+} RefFrame;
+
+void *refh_create(const RefScene *scene);
+int refh_render(void *h, RefFrame *out);
+int refh_pick(void *h, int n, const int32_t *xy, uint32_t *ids, float *depths,
+              int32_t *hits);
+int refh_env_maps(void *h, const float **irr, int32_t *iw, int32_t *ih,
+                  const float **pf, int32_t *pw, int32_t *ph, int32_t *levels,
+                  const float **brdf, int32_t *brdf_size);
+/* Median wall time (ms) of render + read_color over `frames` after `warm`. */
+double refh_time_frames(void *h, int warm, int frames);
+int refh_num_threads(void *h);
+void refh_destroy(void *h);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,235 @@
+"""ctypes driver for the reference library built into oracle/_ref/libmopref.so.
+
+Test infrastructure only: tests/ use it to pin the C oracle against the
+reference itself, and bench.py's CPU-baseline leg uses it to time the
+reference CPU backend.  Structures mirror oracle/ref_harness.h.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+REF_SO = HERE / "_ref" / "libmopref.so"
+
+
+class RefMesh(C.Structure):
+    _fields_ = [("vertices", C.c_void_p), ("vertex_count", C.c_uint32),
+                ("indices", C.c_void_p), ("index_count", C.c_uint32),
+                ("object_id", C.c_uint32), ("transform", C.c_float * 16),
+                ("metallic", C.c_float), ("roughness", C.c_float),
+                ("has_material", C.c_int32), ("texture", C.c_int32),
+                ("opacity", C.c_float)]
+
+
+class RefLight(C.Structure):
+    _fields_ = [("type", C.c_int32), ("position", C.c_float * 3),
+                ("direction", C.c_float * 3), ("color", C.c_float * 4),
+                ("intensity", C.c_float), ("range", C.c_float),
+                ("spot_inner_cos", C.c_float), ("spot_outer_cos", C.c_float),
+                ("active", C.c_int32)]
+
+
+class RefScene(C.Structure):
+    _fields_ = [("width", C.c_int32), ("height", C.c_int32), ("ssaa", C.c_int32),
+                ("clear_color", C.c_float * 4), ("eye", C.c_float * 3),
+                ("target", C.c_float * 3), ("up", C.c_float * 3),
+                ("fov_deg", C.c_float), ("near_plane", C.c_float), ("far_plane", C.c_float),
+                ("ambient", C.c_float), ("exposure", C.c_float),
+                ("post_effects", C.c_uint32), ("mesh_count", C.c_uint32),
+                ("meshes", C.POINTER(RefMesh)), ("texture_count", C.c_uint32),
+                ("tex_w", C.POINTER(C.c_int32)), ("tex_h", C.POINTER(C.c_int32)),
+                ("tex_data", C.POINTER(C.c_void_p)), ("light_count", C.c_uint32),
+                ("lights", C.POINTER(RefLight)), ("env", C.c_int32),
+                ("sun_dir", C.c_float * 3), ("turbidity", C.c_float),
+                ("ground_albedo", C.c_float), ("env_rotation", C.c_float),
+                ("env_intensity", C.c_float), ("serial", C.c_int32),
+                ("flat", C.c_int32)]
+
+
+class RefFrame(C.Structure):
+    _fields_ = [("color", C.c_void_p), ("color_full", C.c_void_p),
+                ("depth", C.c_void_p), ("object_id", C.c_void_p),
+                ("view", C.c_float * 16), ("proj", C.c_float * 16),
+                ("eye", C.c_float * 3), ("triangle_count", C.c_uint32),
+                ("frame_ms", C.c_double)]
+
+
+def light_struct(L, cls=RefLight):
+    s = cls()
+    s.type = L.type
+    s.position[:] = L.position
+    s.direction[:] = L.direction
+    s.color[:] = L.color
+    s.intensity = L.intensity
+    s.range = L.range
+    s.spot_inner_cos = L.spot_inner_cos
+    s.spot_outer_cos = L.spot_outer_cos
+    s.active = 1 if L.active else 0
+    return s
+
+
+_lib = None
+
+
+def available() -> bool:
+    return REF_SO.exists()
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not REF_SO.exists():
+            raise FileNotFoundError(f"reference library not built: {REF_SO}")
+        _lib = C.CDLL(str(REF_SO))
+        _lib.refh_create.restype = C.c_void_p
+        _lib.refh_create.argtypes = [C.POINTER(RefScene)]
+        _lib.refh_render.argtypes = [C.c_void_p, C.POINTER(RefFrame)]
+        _lib.refh_pick.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+        _lib.refh_env_maps.argtypes = [C.c_void_p] + [C.c_void_p] * 9
+        _lib.refh_time_frames.restype = C.c_double
+        _lib.refh_time_frames.argtypes = [C.c_void_p, C.c_int, C.c_int]
+        _lib.refh_num_threads.argtypes = [C.c_void_p]
+        _lib.refh_destroy.argtypes = [C.c_void_p]
+    return _lib
+
+
+class Reference:
+    """A reference CPU-backend viewport holding one scene."""
+
+    def __init__(self, scene, serial: bool = True):
+        L = lib()
+        self.scene = scene
+        self._keep = []
+        meshes = (RefMesh * max(1, len(scene.meshes)))()
+        for k, m in enumerate(scene.meshes):
+            v = np.ascontiguousarray(m.vertices, np.float32)
+            i = np.ascontiguousarray(m.indices, np.uint32)
+            self._keep += [v, i]
+            rm = meshes[k]
+            rm.vertices = v.ctypes.data
+            rm.vertex_count = v.shape[0]
+            rm.indices = i.ctypes.data
+            rm.index_count = i.size
+            rm.object_id = m.object_id
+            rm.transform[:] = [float(x) for x in m.transform]
+            rm.metallic = m.metallic
+            rm.roughness = m.roughness
+            rm.has_material = 1 if m.has_material else 0
+            rm.texture = m.texture
+            rm.opacity = m.opacity
+        lights = (RefLight * max(1, len(scene.lights)))()
+        for k, l in enumerate(scene.lights):
+            lights[k] = light_struct(l)
+        nt = len(scene.textures)
+        tw = (C.c_int32 * max(1, nt))()
+        th = (C.c_int32 * max(1, nt))()
+        td = (C.c_void_p * max(1, nt))()
+        for k, t in enumerate(scene.textures):
+            t = np.ascontiguousarray(t, np.uint8)
+            self._keep.append(t)
+            th[k], tw[k] = t.shape[0], t.shape[1]
+            td[k] = t.ctypes.data
+        sc = RefScene()
+        sc.width, sc.height, sc.ssaa = scene.width, scene.height, scene.ssaa
+        sc.clear_color[:] = scene.clear
+        sc.eye[:] = scene.eye
+        sc.target[:] = scene.target
+        sc.up[:] = scene.up
+        sc.fov_deg, sc.near_plane, sc.far_plane = scene.fov_deg, scene.near, scene.far
+        sc.ambient, sc.exposure = scene.ambient, scene.exposure
+        sc.post_effects = scene.post_effects
+        sc.mesh_count = len(scene.meshes)
+        sc.meshes = meshes
+        sc.texture_count = nt
+        sc.tex_w, sc.tex_h, sc.tex_data = tw, th, td
+        sc.light_count = len(scene.lights)
+        sc.lights = lights
+        sc.env = scene.env
+        sc.sun_dir[:] = scene.sun_dir
+        sc.turbidity, sc.ground_albedo = scene.turbidity, scene.ground_albedo
+        sc.env_rotation, sc.env_intensity = scene.env_rotation, scene.env_intensity
+        sc.serial = 1 if serial else 0
+        sc.flat = 0 if getattr(scene, "smooth", True) else 1
+        self._keep += [meshes, lights, tw, th, td, sc]
+        self.h = L.refh_create(C.byref(sc))
+        if not self.h:
+            raise RuntimeError("refh_create failed")
+
+    def render(self):
+        s = self.scene
+        S = s.samples
+        out = {
+            "color": np.zeros((s.height, s.width, 4), np.uint8),
+            "color_full": np.zeros((s.height * s.ssaa, s.width * s.ssaa, 4), np.uint8),
+            "depth": np.zeros((s.height * s.ssaa, s.width * s.ssaa), np.float32),
+            "object_id": np.zeros((s.height * s.ssaa, s.width * s.ssaa), np.uint32),
+        }
+        f = RefFrame()
+        f.color = out["color"].ctypes.data
+        f.color_full = out["color_full"].ctypes.data
+        f.depth = out["depth"].ctypes.data
+        f.object_id = out["object_id"].ctypes.data
+        rc = lib().refh_render(self.h, C.byref(f))
+        if rc != 0:
+            raise RuntimeError(f"refh_render failed: {rc}")
+        out["view"] = np.array(f.view[:], np.float32)
+        out["proj"] = np.array(f.proj[:], np.float32)
+        out["eye"] = np.array(f.eye[:], np.float32)
+        out["triangle_count"] = f.triangle_count
+        assert S == out["depth"].size
+        return out
+
+    def pick(self, xy: np.ndarray):
+        xy = np.ascontiguousarray(xy, np.int32)
+        n = xy.shape[0]
+        ids = np.zeros(n, np.uint32)
+        dep = np.zeros(n, np.float32)
+        hits = np.zeros(n, np.int32)
+        lib().refh_pick(self.h, n, xy.ctypes.data, ids.ctypes.data, dep.ctypes.data, hits.ctypes.data)
+        return ids, dep, hits
+
+    def env_maps(self):
+        ptrs = [C.c_void_p() for _ in range(3)]
+        ints = [C.c_int32() for _ in range(7)]
+        irr, pf, brdf = ptrs
+        iw, ih, pw, ph, lv, bs = ints[:6]
+        rc = lib().refh_env_maps(self.h, C.byref(irr), C.byref(iw), C.byref(ih), C.byref(pf),
+                                 C.byref(pw), C.byref(ph), C.byref(lv), C.byref(brdf), C.byref(bs))
+        if rc != 0:
+            return None
+
+        def arr(p, n):
+            return np.ctypeslib.as_array(C.cast(p, C.POINTER(C.c_float)), shape=(n,)).copy()
+
+        pf_total = 0
+        for l in range(lv.value):
+            pf_total += max(1, pw.value >> l) * max(1, ph.value >> l)
+        return {
+            "irr": arr(irr, iw.value * ih.value * 4), "irr_w": iw.value, "irr_h": ih.value,
+            "pf": arr(pf, pf_total * 4), "pf_w": pw.value, "pf_h": ph.value, "pf_levels": lv.value,
+            "brdf": arr(brdf, bs.value * bs.value * 4), "brdf_size": bs.value,
+            "rotation": self.scene.env_rotation,
+            "intensity": self.scene.env_intensity if self.scene.env_intensity > 0 else 1.0,
+        }
+
+    def time_frames(self, warm: int, frames: int) -> float:
+        return lib().refh_time_frames(self.h, warm, frames)
+
+    @property
+    def threads(self) -> int:
+        return lib().refh_num_threads(self.h)
+
+    def close(self):
+        if self.h:
+            lib().refh_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
