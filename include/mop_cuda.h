@@ -1,0 +1,216 @@
+/*
+ * mop_cuda.h — C ABI of the B200 (sm_100a) backend for the Master of Puppets
+ * software-rasterizer frame path.
+ *
+ * Every entry point takes plain pointers, sizes and POD structs; nothing in
+ * this header depends on CUDA, C++ or the reference's headers, so it can be
+ * bound from C, ctypes or any FFI.  The entry points replace, one for one,
+ * the reference's RHI function table entries (src/rhi/rhi.h:132-339) as
+ * implemented by its CPU backend (src/backend/cpu/cpu_backend.c); the
+ * reference-typed table itself is produced by mop_rhi_backend_cuda() in
+ * master-of-puppets_b200/host/mop_rhi_cuda.c on top of these calls.
+ *
+ * Execution model.  Draws are recorded on the host between frame_begin and
+ * frame_end; frame_end (or the first readback that needs the frame) runs the
+ * whole frame on the device as a fixed sequence of kernels: vertex
+ * transform, triangle setup + clipping, screen-tile binning, per-tile
+ * visibility (64-bit atomicMin on depth|submission order) fused with deferred
+ * shading and the ACES resolve, then FXAA + gamma + SSAA box.  Results are
+ * order-independent and deterministic; object IDs and depth are bit-exact to
+ * the reference CPU backend.
+ *
+ * Errors: create calls return NULL; int-returning calls return MOPCUDA_OK
+ * (0) or a negative MOPCUDA_E* code; mopcuda_last_error() gives text.
+ */
+#ifndef MOP_CUDA_H
+#define MOP_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MOPCUDA_OK 0
+#define MOPCUDA_EINVAL (-1)       /* bad argument                              */
+#define MOPCUDA_ENOMEM (-2)       /* device or pinned-host allocation failed   */
+#define MOPCUDA_ECUDA (-3)        /* CUDA runtime error                        */
+#define MOPCUDA_ETIMEOUT (-4)     /* bounded wait expired (device lost)        */
+#define MOPCUDA_EUNSUPPORTED (-5) /* draw state outside the supported path     */
+
+/* post-effect bits (reference include/mop/render/postprocess.h:20-33) */
+#define MOPCUDA_POST_GAMMA (1u << 0)
+#define MOPCUDA_POST_TONEMAP (1u << 1)
+#define MOPCUDA_POST_VIGNETTE (1u << 2)
+#define MOPCUDA_POST_FXAA (1u << 4)
+
+typedef struct MopCudaDevice MopCudaDevice;
+typedef struct MopCudaBuffer MopCudaBuffer;
+typedef struct MopCudaTexture MopCudaTexture;
+typedef struct MopCudaFramebuffer MopCudaFramebuffer;
+
+/* Light record; same fields and meaning as MopLight
+ * (reference include/mop/core/light.h:37-60). */
+typedef struct MopCudaLight {
+  int32_t type; /* 0 directional, 1 point, 2 spot */
+  float position[3];
+  float direction[3];
+  float color[4];
+  float intensity;
+  float range;
+  float spot_inner_cos;
+  float spot_outer_cos;
+  int32_t active;
+} MopCudaLight;
+
+/* Flexible vertex layout (reference include/mop/core/vertex_format.h:70):
+ * byte offsets of each attribute inside a vertex of `stride` bytes, or -1
+ * when absent (normal defaults to (0,1,0), colour to white, uv to 0). */
+typedef struct MopCudaVertexLayout {
+  uint32_t stride;
+  int32_t position_offset;
+  int32_t position_components; /* 1..4 */
+  int32_t normal_offset;
+  int32_t normal_components;
+  int32_t color_offset;
+  int32_t color_components;
+  int32_t uv_offset;
+  int32_t uv_components;
+} MopCudaVertexLayout;
+
+/* One draw; the fields of MopRhiDrawCall (reference src/rhi/rhi.h:51-110)
+ * that the frame path reads.  Matrices are column-major d[col*4+row]. */
+typedef struct MopCudaDraw {
+  MopCudaBuffer *vertex_buffer;
+  MopCudaBuffer *index_buffer;
+  uint32_t vertex_count;
+  uint32_t index_count;
+  uint32_t object_id;
+  float model[16];
+  float mvp[16];
+  float light_dir[3];
+  float ambient;
+  float opacity;
+  float metallic;
+  float roughness;
+  float depth_bias;
+  float cam_eye[3];
+  int32_t smooth;        /* MOP_SHADING_SMOOTH                              */
+  int32_t wireframe;
+  int32_t depth_test;
+  int32_t depth_write;
+  int32_t backface_cull;
+  int32_t blend_mode;    /* MopBlendMode                                    */
+  MopCudaTexture *texture;
+  const MopCudaLight *lights; /* copied at draw time; NULL = no light list  */
+  uint32_t light_count;
+  const MopCudaVertexLayout *layout; /* NULL = 48-byte MopVertex           */
+} MopCudaDraw;
+
+/* ---- device lifecycle: MopRhiBackend.device_create/destroy (rhi.h:136-137),
+ *      cpu_device_create cpu_backend.c:55-75 ---------------------------- */
+MopCudaDevice *mopcuda_device_create(int cuda_ordinal);
+void mopcuda_device_destroy(MopCudaDevice *dev);
+const char *mopcuda_last_error(void);
+/* Number of kernel launches issued by this device since creation. */
+uint64_t mopcuda_launch_count(const MopCudaDevice *dev);
+
+/* ---- buffers: buffer_create/destroy/update/read (rhi.h:140-143, 230-237),
+ *      cpu_backend.c:87-115, 663-667, 1077-1080 ------------------------- */
+MopCudaBuffer *mopcuda_buffer_create(MopCudaDevice *dev, const void *data, size_t size);
+void mopcuda_buffer_destroy(MopCudaDevice *dev, MopCudaBuffer *buf);
+int mopcuda_buffer_update(MopCudaDevice *dev, MopCudaBuffer *buf, const void *data,
+                          size_t offset, size_t size);
+/* Host shadow of the buffer contents (the core reads vertex data back). */
+const void *mopcuda_buffer_read(const MopCudaBuffer *buf);
+size_t mopcuda_buffer_size(const MopCudaBuffer *buf);
+
+/* ---- textures: texture_create/_hdr/destroy (rhi.h:197-211),
+ *      cpu_backend.c:811-853, 1064-1072 --------------------------------- */
+MopCudaTexture *mopcuda_texture_create(MopCudaDevice *dev, int width, int height,
+                                       const uint8_t *rgba);
+MopCudaTexture *mopcuda_texture_create_hdr(MopCudaDevice *dev, int width, int height,
+                                           const float *rgba);
+void mopcuda_texture_destroy(MopCudaDevice *dev, MopCudaTexture *tex);
+int mopcuda_texture_read_rgba8(MopCudaDevice *dev, MopCudaTexture *tex, uint8_t *out,
+                               size_t out_size);
+
+/* ---- framebuffers: framebuffer_create/destroy/resize (rhi.h:146-151),
+ *      cpu_backend.c:121-188 ------------------------------------------- */
+MopCudaFramebuffer *mopcuda_framebuffer_create(MopCudaDevice *dev, int width, int height);
+void mopcuda_framebuffer_destroy(MopCudaDevice *dev, MopCudaFramebuffer *fb);
+int mopcuda_framebuffer_resize(MopCudaDevice *dev, MopCudaFramebuffer *fb, int width,
+                               int height);
+/* Presentation (SSAA) factor of the framebuffer, as the viewport allocates
+ * (width*ssaa) x (height*ssaa) samples (reference viewport.c:552-577).  When
+ * set, frame_end fuses the box resolve of mop_viewport_read_color
+ * (viewport.c:3385-3411) into its post pass. */
+int mopcuda_framebuffer_set_ssaa(MopCudaFramebuffer *fb, int ssaa);
+
+/* ---- frame state ------------------------------------------------------ */
+/* set_exposure (rhi.h:244): exposure for the ACES resolve
+ * (reference mop_sw_hdr_resolve, rasterizer.c:2776). */
+void mopcuda_set_exposure(MopCudaDevice *dev, float exposure);
+/* Post-effect bits applied after the resolve (mop_postprocess_apply,
+ * postprocess.c:24); default GAMMA|FXAA as the viewport sets it. */
+void mopcuda_set_post_effects(MopCudaDevice *dev, uint32_t effects);
+/* IBL maps, as mop_sw_ibl_set (rasterizer.h:212-215): irradiance RGBA32F
+ * iw x ih, prefiltered RGBA32F mip chain concatenated (levels), BRDF LUT
+ * RGBA32F size x size.  Copied to the device.  NULL irradiance clears. */
+int mopcuda_set_ibl(MopCudaDevice *dev, const float *irradiance, int iw, int ih,
+                    const float *prefiltered, int pw, int ph, int levels,
+                    const float *brdf_lut, int brdf_size, float rotation, float intensity);
+
+/* ---- frame commands: frame_begin/end/submit, draw, draw_instanced
+ *      (rhi.h:160-175, 214-218), cpu_backend.c:197-211, 528-657 -------- */
+int mopcuda_frame_begin(MopCudaDevice *dev, MopCudaFramebuffer *fb, const float clear_rgba[4]);
+int mopcuda_draw(MopCudaDevice *dev, MopCudaFramebuffer *fb, const MopCudaDraw *draw);
+/* view/projection multiply per instance as cpu_draw_instanced does
+ * (mvp = P * (V * instance), cpu_backend.c:638-657). */
+int mopcuda_draw_instanced(MopCudaDevice *dev, MopCudaFramebuffer *fb, const MopCudaDraw *draw,
+                           const float *view, const float *projection,
+                           const float *instance_models, uint32_t instance_count);
+/* Launch the recorded frame (asynchronous; returns after enqueueing). */
+int mopcuda_frame_end(MopCudaDevice *dev, MopCudaFramebuffer *fb);
+/* Bounded wait for the last launched frame; MOPCUDA_ETIMEOUT after
+ * timeout_ms (the frame's result is then undefined). */
+int mopcuda_frame_wait(MopCudaDevice *dev, int timeout_ms);
+/* Device time of the last completed frame (frame_gpu_time_ms, rhi.h:240). */
+float mopcuda_frame_gpu_time_ms(MopCudaDevice *dev);
+
+/* ---- readbacks (rhi.h:177-195), cpu_backend.c:673-735.  Returned pointers
+ *      are pinned host mirrors owned by the framebuffer, valid until the next
+ *      frame, resize or destroy; the caller may write through them. ----- */
+const uint8_t *mopcuda_read_color(MopCudaDevice *dev, MopCudaFramebuffer *fb, int *w, int *h);
+const uint32_t *mopcuda_read_object_id(MopCudaDevice *dev, MopCudaFramebuffer *fb, int *w,
+                                       int *h);
+const float *mopcuda_read_depth(MopCudaDevice *dev, MopCudaFramebuffer *fb, int *w, int *h);
+/* SSAA box resolve on the device (mop_viewport_read_color,
+ * viewport.c:3385-3411) into a caller buffer of (w/ssaa)*(h/ssaa)*4 bytes. */
+int mopcuda_read_color_resolved(MopCudaDevice *dev, MopCudaFramebuffer *fb, int ssaa,
+                                uint8_t *out, size_t out_size);
+uint32_t mopcuda_pick_read_id(MopCudaDevice *dev, MopCudaFramebuffer *fb, int x, int y);
+float mopcuda_pick_read_depth(MopCudaDevice *dev, MopCudaFramebuffer *fb, int x, int y);
+/* Batched pick at presentation pixels (mop_viewport_pick, viewport.c:3687):
+ * xy[2n]; outputs ids/depths/hits per query; out-of-range -> (0, 1.0, 0). */
+int mopcuda_pick_batch(MopCudaDevice *dev, MopCudaFramebuffer *fb, int ssaa, const int32_t *xy,
+                       uint32_t n, uint32_t *ids, float *depths, int32_t *hits);
+
+/* ---- host-side matrices (the device receives finished matrices) ------- */
+/* out = a * b, column-major (mop_mat4_multiply, reference math.c:182-194). */
+void mopcuda_mat4_multiply(const float a[16], const float b[16], float out[16]);
+/* T * Rz * Ry * Rx * S (mop_mat4_compose_trs, math.c:205-215). */
+void mopcuda_mat4_compose_trs(const float position[3], const float rotation[3],
+                              const float scale[3], float out[16]);
+/* View/projection/eye of a frame after mop_viewport_set_camera: the orbit
+ * camera re-derives eye and up each render (viewport.c:1058-1128,
+ * camera.c:35-63).  width/height are the presentation size. */
+void mopcuda_camera_matrices(const float eye[3], const float target[3], const float up[3],
+                             float fov_deg, float near_plane, float far_plane, int width,
+                             int height, float view[16], float proj[16], float eye_out[3]);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,147 @@
+/*
+ * host_math.c — the host-side matrix work of the frame path (C11).
+ *
+ * The device receives finished matrices; these helpers produce them with
+ * the reference's exact float operation order so that mvp, world and
+ * camera matrices match the CPU backend bit for bit:
+ *   column-major multiply        reference src/math/math.c:182-194
+ *   TRS compose T*Rz*Ry*Rx*S     math.c:205-215 (rotations :132-162)
+ *   look_at / perspective        math.c:69-79, 111-130
+ *   camera chain                 mop_viewport_set_camera viewport.c:1058-1093,
+ *                                orbit re-application each frame
+ *                                camera.c:35-63 -> viewport.c:1095-1128
+ * sinf/cosf/tanf/atan2f/asinf are the host C library's, as in the reference.
+ * Compiled with -ffp-contract=off (no FMA contraction).
+ */
+#include "../../include/mop_cuda.h"
+
+#include <math.h>
+#include <string.h>
+
+#define E(m, r, c) ((m)[(c)*4 + (r)])
+
+void mopcuda_mat4_multiply(const float a[16], const float b[16], float out[16]) {
+  float r[16];
+  for (int c = 0; c < 4; c++)
+    for (int row = 0; row < 4; row++) {
+      float s = 0.0f;
+      for (int k = 0; k < 4; k++)
+        s += E(a, row, k) * E(b, k, c);
+      E(r, row, c) = s;
+    }
+  memcpy(out, r, sizeof r);
+}
+
+static void ident(float m[16]) {
+  memset(m, 0, 16 * sizeof(float));
+  m[0] = m[5] = m[10] = m[15] = 1.0f;
+}
+
+void mopcuda_mat4_compose_trs(const float pos[3], const float rot[3], const float scl[3],
+                              float out[16]) {
+  float s[16], rx[16], ry[16], rz[16], t[16], m1[16], m2[16], m3[16];
+  memset(s, 0, sizeof s);
+  E(s, 0, 0) = scl[0];
+  E(s, 1, 1) = scl[1];
+  E(s, 2, 2) = scl[2];
+  E(s, 3, 3) = 1.0f;
+  float c = cosf(rot[0]), n = sinf(rot[0]);
+  ident(rx);
+  E(rx, 1, 1) = c;
+  E(rx, 1, 2) = -n;
+  E(rx, 2, 1) = n;
+  E(rx, 2, 2) = c;
+  c = cosf(rot[1]);
+  n = sinf(rot[1]);
+  ident(ry);
+  E(ry, 0, 0) = c;
+  E(ry, 0, 2) = n;
+  E(ry, 2, 0) = -n;
+  E(ry, 2, 2) = c;
+  c = cosf(rot[2]);
+  n = sinf(rot[2]);
+  ident(rz);
+  E(rz, 0, 0) = c;
+  E(rz, 0, 1) = -n;
+  E(rz, 1, 0) = n;
+  E(rz, 1, 1) = c;
+  ident(t);
+  E(t, 0, 3) = pos[0];
+  E(t, 1, 3) = pos[1];
+  E(t, 2, 3) = pos[2];
+  mopcuda_mat4_multiply(rx, s, m1);
+  mopcuda_mat4_multiply(ry, m1, m2);
+  mopcuda_mat4_multiply(rz, m2, m3);
+  mopcuda_mat4_multiply(t, m3, out);
+}
+
+typedef struct {
+  float x, y, z;
+} v3;
+
+static float dot(v3 a, v3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+
+static v3 unit(v3 a) {
+  float l = sqrtf(a.x * a.x + a.y * a.y + a.z * a.z);
+  if (l < 1e-8f) {
+    v3 z = {0.0f, 0.0f, 0.0f};
+    return z;
+  }
+  float inv = 1.0f / l;
+  v3 r = {a.x * inv, a.y * inv, a.z * inv};
+  return r;
+}
+
+static v3 cross(v3 a, v3 b) {
+  v3 r = {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
+  return r;
+}
+
+void mopcuda_camera_matrices(const float eye[3], const float target[3], const float up[3],
+                             float fov_deg, float near_plane, float far_plane, int width,
+                             int height, float view[16], float proj[16], float eye_out[3]) {
+  v3 e = {eye[0], eye[1], eye[2]}, t = {target[0], target[1], target[2]};
+  v3 u = {up[0], up[1], up[2]};
+  v3 off = {e.x - t.x, e.y - t.y, e.z - t.z};
+  float dist = sqrtf(off.x * off.x + off.y * off.y + off.z * off.z);
+  if (dist > 1e-6f) {
+    /* orbit parameters recovered by set_camera, re-applied by render */
+    float yaw = atan2f(off.x, off.z);
+    float pitch = asinf(off.y / dist);
+    float sp = sinf(pitch), cp = cosf(pitch), sy = sinf(yaw), cy = cosf(yaw);
+    v3 ou = {-sp * sy, cp, -sp * cy};
+    u = ou;
+    float cp2 = cosf(pitch);
+    v3 oe = {t.x + dist * cp2 * sinf(yaw), t.y + dist * sinf(pitch),
+             t.z + dist * cp2 * cosf(yaw)};
+    e = oe;
+  }
+  v3 f = unit((v3){t.x - e.x, t.y - e.y, t.z - e.z});
+  v3 s = unit(cross(f, u));
+  v3 uu = cross(s, f);
+  ident(view);
+  E(view, 0, 0) = s.x;
+  E(view, 0, 1) = s.y;
+  E(view, 0, 2) = s.z;
+  E(view, 1, 0) = uu.x;
+  E(view, 1, 1) = uu.y;
+  E(view, 1, 2) = uu.z;
+  E(view, 2, 0) = -f.x;
+  E(view, 2, 1) = -f.y;
+  E(view, 2, 2) = -f.z;
+  E(view, 0, 3) = -dot(s, e);
+  E(view, 1, 3) = -dot(uu, e);
+  E(view, 2, 3) = dot(f, e);
+  float fov = fov_deg * (3.14159265358979323846f / 180.0f);
+  float aspect = (float)width / (float)height;
+  float th = tanf(fov * 0.5f);
+  memset(proj, 0, 16 * sizeof(float));
+  E(proj, 0, 0) = 1.0f / (aspect * th);
+  E(proj, 1, 1) = 1.0f / th;
+  E(proj, 2, 2) = -(far_plane + near_plane) / (far_plane - near_plane);
+  E(proj, 3, 2) = -1.0f;
+  E(proj, 2, 3) = -(2.0f * far_plane * near_plane) / (far_plane - near_plane);
+  eye_out[0] = e.x;
+  eye_out[1] = e.y;
+  eye_out[2] = e.z;
+}

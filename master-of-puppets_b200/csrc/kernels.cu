@@ -1,0 +1,1325 @@
+/*
+ * kernels.cu — sm_100a kernels of the CUDA frame path.
+ *
+ * Stage map (reference file:line of the CPU code each stage reproduces):
+ *   k_vertex     per-vertex transform     cpu_prepare_triangle[_ex]
+ *                                         cpu_backend.c:224-324, 412-526
+ *   k_setup      cull / trivial accept /  mop_sw_rasterize_triangle_full
+ *                screen map / edge setup  rasterizer.c:2458-2612, 1825-1924
+ *   k_clip       Sutherland-Hodgman fan   rasterizer.c:514-626
+ *   k_bin_*      screen-tile binning      (replaces rasterizer_mt.c binning)
+ *   k_tile       visibility (64-bit key   rasterizer.c:1926-1960 coverage +
+ *                atomicMin) + deferred    depth; 1961-2108 shading;
+ *                shading + ACES resolve   2776-2803 resolve
+ *   k_post       FXAA + post + SSAA box   rasterizer.c:2625-2761,
+ *                                         postprocess.c:24-116,
+ *                                         viewport.c:3385-3411
+ *   k_pick       batched pick             viewport.c:3687-3749
+ *
+ * Every float expression keeps the reference's operand order; the file is
+ * compiled with -fmad=false so nothing is contracted into FMA.
+ */
+#include "mopcuda_internal.cuh"
+
+#define PI_F 3.14159274f /* (float)M_PI */
+
+/* ------------------------------------------------------------------------
+ * small vector math (reference math.c:17-50, 196-203)
+ * ------------------------------------------------------------------------ */
+struct V3 {
+  float x, y, z;
+};
+
+__device__ __forceinline__ V3 mk3(float x, float y, float z) {
+  V3 r;
+  r.x = x;
+  r.y = y;
+  r.z = z;
+  return r;
+}
+__device__ __forceinline__ V3 add3(V3 a, V3 b) { return mk3(a.x + b.x, a.y + b.y, a.z + b.z); }
+__device__ __forceinline__ V3 sub3(V3 a, V3 b) { return mk3(a.x - b.x, a.y - b.y, a.z - b.z); }
+__device__ __forceinline__ V3 scale3(V3 a, float s) { return mk3(a.x * s, a.y * s, a.z * s); }
+__device__ __forceinline__ float dot3(V3 a, V3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+__device__ __forceinline__ float len3(V3 a) { return sqrtf(a.x * a.x + a.y * a.y + a.z * a.z); }
+__device__ __forceinline__ V3 norm3(V3 a) {
+  float l = len3(a);
+  if (l < 1e-8f)
+    return mk3(0.0f, 0.0f, 0.0f);
+  float inv = 1.0f / l;
+  return mk3(a.x * inv, a.y * inv, a.z * inv);
+}
+__device__ __forceinline__ float clamp01(float x) { return x < 0.0f ? 0.0f : (x > 1.0f ? 1.0f : x); }
+
+/* rows of a column-major matrix times (x, y, z, w), summed left to right */
+__device__ __forceinline__ float4 xform(const float *m, float x, float y, float z, float w) {
+  float4 r;
+  r.x = m[0] * x + m[4] * y + m[8] * z + m[12] * w;
+  r.y = m[1] * x + m[5] * y + m[9] * z + m[13] * w;
+  r.z = m[2] * x + m[6] * y + m[10] * z + m[14] * w;
+  r.w = m[3] * x + m[7] * y + m[11] * z + m[15] * w;
+  return r;
+}
+
+__device__ __forceinline__ int find_draw_by(const DrawRec *draws, uint32_t n, uint32_t g,
+                                            bool by_vertex) {
+  uint32_t lo = 0, hi = n; /* last draw with base <= g */
+  while (hi - lo > 1) {
+    uint32_t mid = (lo + hi) >> 1;
+    uint32_t b = by_vertex ? draws[mid].vbase : draws[mid].tbase;
+    if (b <= g)
+      lo = mid;
+    else
+      hi = mid;
+  }
+  return (int)lo;
+}
+
+/* ------------------------------------------------------------------------
+ * k_vertex — one thread per (draw, vertex)
+ * ------------------------------------------------------------------------ */
+__device__ __forceinline__ void read_attr(const uint8_t *v, int off, int n, float dflt_last,
+                                          int want, float *out) {
+  /* read_attrib_float{2,3,4}, cpu_backend.c:332-410: missing components are
+   * zero, except a 4-component read's last one which defaults to 1. */
+  for (int k = 0; k < want; k++)
+    out[k] = 0.0f;
+  if (want == 4)
+    out[3] = dflt_last;
+  if (off < 0 || n <= 0)
+    return;
+  const float *f = (const float *)(v + off);
+  int m = n < want ? n : want;
+  for (int k = 0; k < m; k++)
+    out[k] = __ldg(f + k);
+}
+
+__global__ void k_vertex(FrameArgs a) {
+  uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= a.total_vertices)
+    return;
+  const DrawRec &d = a.draws[find_draw_by(a.draws, a.draw_count, g, true)];
+  uint32_t i = g - d.vbase;
+  float pos[3], nrm[3], col[4], uv[2];
+  if (!(d.flags & DF_FLEX)) {
+    const float *v = (const float *)(d.vbuf + (size_t)i * 48u);
+    float4 q0 = __ldg((const float4 *)v);
+    float4 q1 = __ldg((const float4 *)v + 1);
+    float4 q2 = __ldg((const float4 *)v + 2);
+    pos[0] = q0.x; pos[1] = q0.y; pos[2] = q0.z;
+    nrm[0] = q0.w; nrm[1] = q1.x; nrm[2] = q1.y;
+    col[0] = q1.z; col[1] = q1.w; col[2] = q2.x; col[3] = q2.y;
+    uv[0] = q2.z; uv[1] = q2.w;
+  } else {
+    const uint8_t *v = d.vbuf + (size_t)i * d.stride;
+    read_attr(v, d.off_pos, d.n_pos, 1.0f, 3, pos);
+    if (d.off_nrm >= 0) {
+      read_attr(v, d.off_nrm, d.n_nrm, 1.0f, 3, nrm);
+    } else {
+      nrm[0] = 0.0f; nrm[1] = 1.0f; nrm[2] = 0.0f;
+    }
+    if (d.off_col >= 0) {
+      read_attr(v, d.off_col, d.n_col, 1.0f, 4, col);
+    } else {
+      col[0] = col[1] = col[2] = col[3] = 1.0f;
+    }
+    read_attr(v, d.off_uv, d.n_uv, 1.0f, 2, uv);
+  }
+  float4 c = xform(d.mvp, pos[0], pos[1], pos[2], 1.0f);
+  if (d.depth_bias != 0.0f)
+    c.z += d.depth_bias * c.w; /* cpu_backend.c:238-242 */
+  float4 w = xform(d.model, pos[0], pos[1], pos[2], 1.0f);
+  float4 n = xform(d.model, nrm[0], nrm[1], nrm[2], 0.0f);
+  if (d.flags & DF_TEXTURED) { /* nearest texel at the vertex, :276-303 */
+    float tu = uv[0] - floorf(uv[0]);
+    float tv = uv[1] - floorf(uv[1]);
+    int tx = x86_f2i(tu * (float)(d.tex_w - 1) + 0.5f);
+    int ty = x86_f2i(tv * (float)(d.tex_h - 1) + 0.5f);
+    tx = tx < 0 ? 0 : (tx >= d.tex_w ? d.tex_w - 1 : tx);
+    ty = ty < 0 ? 0 : (ty >= d.tex_h ? d.tex_h - 1 : ty);
+    uchar4 t = __ldg((const uchar4 *)d.tex + ((size_t)ty * (size_t)d.tex_w + (size_t)tx));
+    col[0] *= (float)t.x / 255.0f;
+    col[1] *= (float)t.y / 255.0f;
+    col[2] *= (float)t.z / 255.0f;
+    col[3] *= (float)t.w / 255.0f;
+  }
+  a.clip[g] = c;
+  a.world[g] = make_float4(w.x, w.y, w.z, 0.0f);
+  a.normal[g] = make_float4(n.x, n.y, n.z, 0.0f);
+  a.color[g] = make_float4(col[0], col[1], col[2], col[3]);
+}
+
+/* ------------------------------------------------------------------------
+ * lighting (rasterizer.c:1497-1814) and IBL (161-301)
+ * ------------------------------------------------------------------------ */
+__device__ __forceinline__ float falloff_inv_sq(const LightRec &L, float dist) {
+  if (L.range > 0.0f) {
+    float r = dist / L.range;
+    float at = 1.0f - r;
+    if (at < 0.0f)
+      at = 0.0f;
+    return at * at;
+  }
+  float d2 = dist * dist;
+  if (d2 < 0.01f)
+    d2 = 0.01f;
+  return 1.0f / d2;
+}
+
+__device__ __forceinline__ float spot_cone(const LightRec &L, V3 dir) {
+  V3 sd = norm3(mk3(L.direction[0], L.direction[1], L.direction[2]));
+  float ca = -dot3(dir, sd);
+  if (ca < L.spot_outer_cos)
+    return 0.0f;
+  if (ca < L.spot_inner_cos) {
+    float rs = L.spot_inner_cos - L.spot_outer_cos;
+    if (rs > 1e-6f) {
+      float t = (ca - L.spot_outer_cos) / rs;
+      return t * t * (3.0f - 2.0f * t);
+    }
+  }
+  return 1.0f;
+}
+
+/* compute_multi_light_rgb, rasterizer.c:1596-1688 */
+__device__ void diffuse_rgb(V3 n, V3 wp, const LightRec *Ls, uint32_t cnt, float amb,
+                            float out[3]) {
+  out[0] = out[1] = out[2] = amb;
+  for (uint32_t i = 0; i < cnt; i++) {
+    const LightRec &L = Ls[i];
+    if (!L.active)
+      continue;
+    float ndotl = 0.0f, att = 1.0f, spot = 1.0f;
+    if (L.type == 0) {
+      V3 dir = norm3(mk3(L.direction[0], L.direction[1], L.direction[2]));
+      ndotl = -dot3(n, dir);
+    } else if (L.type == 1 || L.type == 2) {
+      V3 tl = sub3(mk3(L.position[0], L.position[1], L.position[2]), wp);
+      float dist = len3(tl);
+      if (dist < 1e-6f)
+        dist = 1e-6f;
+      V3 dir = scale3(tl, 1.0f / dist);
+      ndotl = dot3(n, dir);
+      if (L.type == 2)
+        spot = spot_cone(L, dir);
+      att = falloff_inv_sq(L, dist);
+    }
+    if (ndotl < 0.0f)
+      ndotl = 0.0f;
+    float contrib = ndotl * L.intensity * att * spot * 1.0f;
+    out[0] += contrib * L.color[0];
+    out[1] += contrib * L.color[1];
+    out[2] += contrib * L.color[2];
+  }
+}
+
+/* compute_multi_light (flat path), rasterizer.c:1497-1588 */
+__device__ float diffuse_flat(V3 n, V3 wp, const LightRec *Ls, uint32_t cnt, float amb) {
+  float total = amb;
+  for (uint32_t i = 0; i < cnt; i++) {
+    const LightRec &L = Ls[i];
+    if (!L.active)
+      continue;
+    float ndotl = 0.0f, att = 1.0f, spot = 1.0f;
+    if (L.type == 0) {
+      V3 dir = norm3(mk3(L.direction[0], L.direction[1], L.direction[2]));
+      ndotl = -dot3(n, dir);
+    } else if (L.type == 1 || L.type == 2) {
+      V3 tl = sub3(mk3(L.position[0], L.position[1], L.position[2]), wp);
+      float dist = len3(tl);
+      if (dist < 1e-6f)
+        dist = 1e-6f;
+      V3 dir = scale3(tl, 1.0f / dist);
+      ndotl = dot3(n, dir);
+      if (L.type == 1) {
+        att = falloff_inv_sq(L, dist);
+      } else {
+        spot = spot_cone(L, dir);
+        if (L.range > 0.0f) {
+          float r = dist / L.range;
+          att = 1.0f - r;
+          if (att < 0.0f)
+            att = 0.0f;
+          att *= att;
+        } else {
+          att = 1.0f / (1.0f + dist * dist);
+        }
+      }
+    }
+    if (ndotl < 0.0f)
+      ndotl = 0.0f;
+    total += ndotl * L.intensity * att * spot * 1.0f;
+  }
+  return clamp01(total);
+}
+
+/* compute_multi_specular_ggx, rasterizer.c:1701-1814 */
+__device__ void specular_ggx(V3 n, V3 wp, V3 vdir, const LightRec *Ls, uint32_t cnt, float rough,
+                             float metal, const float base[3], float out[3]) {
+  out[0] = out[1] = out[2] = 0.0f;
+  float alpha = rough * rough;
+  float alpha2 = alpha * alpha;
+  if (alpha2 < 1e-7f)
+    alpha2 = 1e-7f;
+  float ndotv = dot3(n, vdir);
+  if (ndotv < 1e-4f)
+    ndotv = 1e-4f;
+  float f0[3];
+  for (int c = 0; c < 3; c++)
+    f0[c] = 0.04f * (1.0f - metal) + base[c] * metal;
+  float k = alpha * 0.5f;
+  float g1v = ndotv / (ndotv * (1.0f - k) + k);
+  for (uint32_t i = 0; i < cnt; i++) {
+    const LightRec &L = Ls[i];
+    if (!L.active)
+      continue;
+    V3 ldir = mk3(0.0f, 0.0f, 0.0f);
+    float att = 1.0f;
+    if (L.type == 0) {
+      V3 dd = norm3(mk3(L.direction[0], L.direction[1], L.direction[2]));
+      ldir = mk3(-dd.x, -dd.y, -dd.z);
+    } else if (L.type == 1 || L.type == 2) {
+      V3 tl = sub3(mk3(L.position[0], L.position[1], L.position[2]), wp);
+      float dist = len3(tl);
+      if (dist < 1e-6f)
+        dist = 1e-6f;
+      ldir = scale3(tl, 1.0f / dist);
+      att = falloff_inv_sq(L, dist);
+    }
+    float ndotl = dot3(n, ldir);
+    if (ndotl <= 0.0f)
+      continue;
+    V3 h = norm3(add3(ldir, vdir));
+    float ndoth = dot3(n, h);
+    if (ndoth < 0.0f)
+      ndoth = 0.0f;
+    float vdoth = dot3(vdir, h);
+    if (vdoth < 0.0f)
+      vdoth = 0.0f;
+    float ndoth2 = ndoth * ndoth;
+    float dd = ndoth2 * (alpha2 - 1.0f) + 1.0f;
+    float D = alpha2 / (PI_F * dd * dd);
+    float g1l = ndotl / (ndotl * (1.0f - k) + k);
+    float G = g1v * g1l;
+    float omv = 1.0f - vdoth;
+    float omv2 = omv * omv;
+    float omv5 = omv2 * omv2 * omv;
+    float den = 4.0f * ndotl * ndotv;
+    if (den < 1e-6f)
+      den = 1e-6f;
+    float st = D * G / den;
+    float wgt = st * L.intensity * att * ndotl * 1.0f * PI_F;
+    for (int c = 0; c < 3; c++) {
+      float fr = f0[c] + (1.0f - f0[c]) * omv5;
+      out[c] += wgt * fr * L.color[c];
+    }
+  }
+}
+
+__device__ __forceinline__ void ibl_bilinear(const float *d, int w, int h, float u, float v,
+                                             float out[3]) {
+  u = u - floorf(u);
+  v = v - floorf(v);
+  float fx = u * (float)(w - 1);
+  float fy = v * (float)(h - 1);
+  int x0 = (int)fx, y0 = (int)fy;
+  x0 = x0 < 0 ? 0 : (x0 > w - 1 ? w - 1 : x0);
+  y0 = y0 < 0 ? 0 : (y0 > h - 1 ? h - 1 : y0);
+  int x1 = (x0 + 1) % w;
+  int y1 = y0 + 1 < h ? y0 + 1 : h - 1;
+  float sx = fx - (float)x0, sy = fy - (float)y0;
+  const float4 p00 = __ldg((const float4 *)d + ((size_t)y0 * w + x0));
+  const float4 p10 = __ldg((const float4 *)d + ((size_t)y0 * w + x1));
+  const float4 p01 = __ldg((const float4 *)d + ((size_t)y1 * w + x0));
+  const float4 p11 = __ldg((const float4 *)d + ((size_t)y1 * w + x1));
+  float a00[3] = {p00.x, p00.y, p00.z}, a10[3] = {p10.x, p10.y, p10.z};
+  float a01[3] = {p01.x, p01.y, p01.z}, a11[3] = {p11.x, p11.y, p11.z};
+  for (int c = 0; c < 3; c++) {
+    float top = a00[c] * (1.0f - sx) + a10[c] * sx;
+    float bot = a01[c] * (1.0f - sx) + a11[c] * sx;
+    out[c] = top * (1.0f - sy) + bot * sy;
+  }
+}
+
+/* dir_to_uv, rasterizer.c:216-222.  atan2f/asinf are CUDA's; glibc's differ
+ * in the last ulp for some inputs, which perturbs IBL colour by at most a
+ * rounding step. */
+__device__ __forceinline__ void dir_uv(float dx, float dy, float dz, float rot, float *u,
+                                       float *v) {
+  float phi = atan2f(dz, dx) + rot;
+  float cdy = dy < -1.0f ? -1.0f : (dy > 1.0f ? 1.0f : dy);
+  *u = phi / (2.0f * 3.14159265f) + 0.5f;
+  *v = asinf(cdy) / 3.14159265f + 0.5f;
+}
+
+__device__ void ibl_irr(const FrameArgs &a, V3 n, float out[3]) {
+  out[0] = out[1] = out[2] = 0.0f;
+  float len = sqrtf(n.x * n.x + n.y * n.y + n.z * n.z);
+  if (len < 1e-6f)
+    return;
+  float u, v;
+  dir_uv(n.x / len, n.y / len, n.z / len, a.ibl_rotation, &u, &v);
+  ibl_bilinear(a.irr, a.irr_w, a.irr_h, u, v, out);
+  for (int c = 0; c < 3; c++)
+    out[c] *= a.ibl_intensity;
+}
+
+__device__ void ibl_pf(const FrameArgs &a, V3 r, float rough, float out[3]) {
+  out[0] = out[1] = out[2] = 0.0f;
+  float len = sqrtf(r.x * r.x + r.y * r.y + r.z * r.z);
+  if (len < 1e-6f)
+    return;
+  int level = x86_f2i(rough * (float)(a.pf_levels - 1));
+  if (level >= a.pf_levels)
+    level = a.pf_levels - 1;
+  if (level < 0)
+    level = 0; /* only reachable for roughness < 0, undefined in the reference */
+  size_t off = 0;
+  for (int l = 0; l < level; l++) {
+    int lw = a.pf_w >> l, lh = a.pf_h >> l;
+    off += (size_t)(lw < 1 ? 1 : lw) * (size_t)(lh < 1 ? 1 : lh);
+  }
+  int lw = a.pf_w >> level, lh = a.pf_h >> level;
+  if (lw < 1)
+    lw = 1;
+  if (lh < 1)
+    lh = 1;
+  float u, v;
+  dir_uv(r.x / len, r.y / len, r.z / len, a.ibl_rotation, &u, &v);
+  ibl_bilinear(a.pf + off * 4, lw, lh, u, v, out);
+  for (int c = 0; c < 3; c++)
+    out[c] *= a.ibl_intensity;
+}
+
+__device__ __forceinline__ void ibl_lut(const FrameArgs &a, float ndv, float rough, float *sc,
+                                        float *bi) {
+  ndv = ndv < 0.0f ? 0.0f : (ndv > 1.0f ? 1.0f : ndv);
+  rough = rough < 0.0f ? 0.0f : (rough > 1.0f ? 1.0f : rough);
+  int n = a.brdf_size;
+  int x = (int)(ndv * (float)(n - 1) + 0.5f);
+  int y = (int)(rough * (float)(n - 1) + 0.5f);
+  if (x >= n)
+    x = n - 1;
+  if (y >= n)
+    y = n - 1;
+  float4 t = __ldg((const float4 *)a.brdf + ((size_t)y * n + x));
+  *sc = t.x;
+  *bi = t.y;
+}
+
+/* Per-sample shading of the smooth multi-light path (rasterizer.c:1963-2099)
+ * from the normalised perspective-correct weights pc[]. */
+__device__ void shade_smooth(const FrameArgs &a, const DrawRec &d, const uint32_t v[3],
+                             const float pc[3], float out[3]) {
+  float4 N[3], C[3], W[3];
+  for (int k = 0; k < 3; k++) {
+    N[k] = a.normal[v[k]];
+    C[k] = a.color[v[k]];
+    W[k] = a.world[v[k]];
+  }
+  V3 n = mk3(pc[0] * N[0].x + pc[1] * N[1].x + pc[2] * N[2].x,
+             pc[0] * N[0].y + pc[1] * N[1].y + pc[2] * N[2].y,
+             pc[0] * N[0].z + pc[1] * N[1].z + pc[2] * N[2].z);
+  n = norm3(n);
+  float base[3];
+  base[0] = pc[0] * C[0].x + pc[1] * C[1].x + pc[2] * C[2].x;
+  base[1] = pc[0] * C[0].y + pc[1] * C[1].y + pc[2] * C[2].y;
+  base[2] = pc[0] * C[0].z + pc[1] * C[1].z + pc[2] * C[2].z;
+  V3 wp = mk3(pc[0] * W[0].x + pc[1] * W[1].x + pc[2] * W[2].x,
+              pc[0] * W[0].y + pc[1] * W[1].y + pc[2] * W[2].y,
+              pc[0] * W[0].z + pc[1] * W[1].z + pc[2] * W[2].z);
+  V3 vdir = norm3(sub3(mk3(d.cam_eye[0], d.cam_eye[1], d.cam_eye[2]), wp));
+  const LightRec *Ls = a.lights + d.light_off;
+  float lit[3], spec[3];
+  diffuse_rgb(n, wp, Ls, d.light_count, d.ambient, lit);
+  specular_ggx(n, wp, vdir, Ls, d.light_count, d.roughness, d.metallic, base, spec);
+  float ds = 1.0f - d.metallic;
+  float env[3] = {0.0f, 0.0f, 0.0f}, irr[3] = {0.0f, 0.0f, 0.0f};
+  bool has_irr = a.irr != nullptr;
+  if (has_irr)
+    ibl_irr(a, n, irr);
+  {
+    float vdn = dot3(vdir, n);
+    V3 refl = mk3(2.0f * vdn * n.x - vdir.x, 2.0f * vdn * n.y - vdir.y, 2.0f * vdn * n.z - vdir.z);
+    float ndv = dot3(n, vdir);
+    if (ndv < 0.0f)
+      ndv = 0.0f;
+    float f0[3];
+    for (int c = 0; c < 3; c++)
+      f0[c] = 0.04f * (1.0f - d.metallic) + base[c] * d.metallic;
+    if (a.pf != nullptr && a.brdf != nullptr) {
+      float pf[3], bs, bb;
+      ibl_pf(a, refl, d.roughness, pf);
+      ibl_lut(a, ndv, d.roughness, &bs, &bb);
+      for (int c = 0; c < 3; c++)
+        env[c] = pf[c] * (f0[c] * bs + bb);
+    } else if (d.metallic > 0.01f) { /* hemisphere fallback, :2042-2072 */
+      float sky_t = refl.y * 0.5f + 0.5f;
+      if (sky_t < 0.0f)
+        sky_t = 0.0f;
+      if (sky_t > 1.0f)
+        sky_t = 1.0f;
+      const float sky[3] = {0.35f, 0.38f, 0.45f}, gnd[3] = {0.08f, 0.07f, 0.06f};
+      float he[3];
+      for (int c = 0; c < 3; c++)
+        he[c] = gnd[c] + sky_t * (sky[c] - gnd[c]);
+      float mix = d.roughness * d.roughness;
+      float avg = (he[0] + he[1] + he[2]) * (1.0f / 3.0f);
+      for (int c = 0; c < 3; c++)
+        he[c] += mix * (avg - he[c]);
+      float om = 1.0f - ndv;
+      float om2 = om * om;
+      float om5 = om2 * om2 * om;
+      for (int c = 0; c < 3; c++) {
+        float fe = f0[c] + (1.0f - f0[c]) * om5;
+        env[c] = he[c] * fe * d.ambient * 3.0f;
+      }
+    }
+  }
+  for (int c = 0; c < 3; c++) {
+    float p;
+    if (has_irr)
+      p = base[c] * (lit[c] + irr[c]) * ds + env[c] + spec[c];
+    else
+      p = base[c] * lit[c] * ds + env[c] + spec[c];
+    out[c] = p < 0.0f ? 0.0f : p;
+  }
+}
+
+/* ------------------------------------------------------------------------
+ * triangle setup
+ * ------------------------------------------------------------------------ */
+
+/* Clip-space vertex with the attributes the flat colour needs. */
+struct CV {
+  float4 p;
+  V3 n, wp;
+  float c[4];
+};
+
+__device__ __forceinline__ CV load_cv(const FrameArgs &a, uint32_t g) {
+  CV r;
+  r.p = a.clip[g];
+  float4 n = a.normal[g], w = a.world[g], c = a.color[g];
+  r.n = mk3(n.x, n.y, n.z);
+  r.wp = mk3(w.x, w.y, w.z);
+  r.c[0] = c.x;
+  r.c[1] = c.y;
+  r.c[2] = c.z;
+  r.c[3] = c.w;
+  return r;
+}
+
+/* Edge setup shared by the rasterisers (e.g. rasterizer.c:1842-1924).
+ * Returns false when the reference returns before its pixel loop. */
+__device__ bool edge_setup(const float sx[3], const float sy[3], int W, int H, RasterRec &r) {
+  float fmin_x = sx[0], fmin_y = sy[0], fmax_x = sx[0], fmax_y = sy[0];
+  for (int k = 1; k < 3; k++) {
+    if (sx[k] < fmin_x)
+      fmin_x = sx[k];
+    if (sy[k] < fmin_y)
+      fmin_y = sy[k];
+    if (sx[k] > fmax_x)
+      fmax_x = sx[k];
+    if (sy[k] > fmax_y)
+      fmax_y = sy[k];
+  }
+  int x0 = x86_f2i(floorf(fmin_x)), y0 = x86_f2i(floorf(fmin_y));
+  int x1 = x86_f2i(ceilf(fmax_x)), y1 = x86_f2i(ceilf(fmax_y));
+  if (x0 < 0)
+    x0 = 0;
+  if (y0 < 0)
+    y0 = 0;
+  if (x1 >= W)
+    x1 = W - 1;
+  if (y1 >= H)
+    y1 = H - 1;
+  if (x0 > x1 || y0 > y1)
+    return false;
+  float area = (sx[1] - sx[0]) * (sy[2] - sy[0]) - (sx[2] - sx[0]) * (sy[1] - sy[0]);
+  if (fabsf(area) < 1e-6f)
+    return false;
+  bool flip = area < 0.0f;
+  r.inv_area = 1.0f / fabsf(area);
+  for (int k = 0; k < 3; k++) {
+    int p = (k + 1) % 3, q = (k + 2) % 3;
+    float ex = sy[p] - sy[q], ey = sx[q] - sx[p];
+    r.dx[k] = flip ? -ex : ex;
+    r.dy[k] = flip ? -ey : ey;
+  }
+  float px = (float)x0 + 0.5f, py = (float)y0 + 0.5f;
+  for (int k = 0; k < 3; k++) {
+    int p = (k + 1) % 3, q = (k + 2) % 3;
+    float w = (sx[q] - sx[p]) * (py - sy[p]) - (sy[q] - sy[p]) * (px - sx[p]);
+    r.w0[k] = flip ? -w : w;
+  }
+  r.x0 = (uint16_t)x0;
+  r.y0 = (uint16_t)y0;
+  r.x1 = (uint16_t)x1;
+  r.y1 = (uint16_t)y1;
+  return true;
+}
+
+__device__ __forceinline__ void mark_dead(RasterRec &r) {
+  r.x0 = 1;
+  r.x1 = 0;
+  r.y0 = 1;
+  r.y1 = 0;
+}
+
+/* Screen mapping, cull and edge setup of one fan triangle (the body of the
+ * fan loop, rasterizer.c:2532-2609).  Fills `rr`/`sr`; returns false if the
+ * reference would draw nothing for it. */
+__device__ bool fan_setup(const FrameArgs &a, const DrawRec &d, const CV v[3], const uint32_t slot[3],
+                          uint32_t order, RasterRec &rr, ShadeRec &sr) {
+  if (fabsf(v[0].p.w) < 1e-7f || fabsf(v[1].p.w) < 1e-7f || fabsf(v[2].p.w) < 1e-7f)
+    return false;
+  float hw = (float)a.width * 0.5f, hh = (float)a.height * 0.5f;
+  float sx[3], sy[3], sz[3];
+  for (int k = 0; k < 3; k++) {
+    float iw = 1.0f / v[k].p.w;
+    sx[k] = (v[k].p.x * iw + 1.0f) * hw;
+    sy[k] = (1.0f - v[k].p.y * iw) * hh;
+    sz[k] = (v[k].p.z * iw + 1.0f) * 0.5f;
+  }
+  float sarea = (sx[1] - sx[0]) * (sy[2] - sy[0]) - (sx[2] - sx[0]) * (sy[1] - sy[0]);
+  if ((d.flags & DF_CULL) && sarea >= 0.0f)
+    return false;
+  if (!edge_setup(sx, sy, a.width, a.height, rr))
+    return false;
+  rr.order = order;
+  sr.draw = (uint32_t)(&d - a.draws);
+  if (d.flags & DF_SMOOTH) {
+    rr.zc[0] = sz[0];
+    rr.zc[1] = sz[1];
+    rr.zc[2] = sz[2];
+    sr.v[0] = slot[0];
+    sr.v[1] = slot[1];
+    sr.v[2] = slot[2];
+    return true;
+  }
+  /* flat: constant colour and incremental depth (rasterizer.c:2549-2609,
+   * 1164-1232, 971-974) */
+  rr.y1 |= REC_FLAT_BIT;
+  rr.zc[0] = (rr.w0[0] * sz[0] + rr.w0[1] * sz[1] + rr.w0[2] * sz[2]) * rr.inv_area;
+  rr.zc[1] = (rr.dx[0] * sz[0] + rr.dx[1] * sz[1] + rr.dx[2] * sz[2]) * rr.inv_area;
+  rr.zc[2] = (rr.dy[0] * sz[0] + rr.dy[1] * sz[1] + rr.dy[2] * sz[2]) * rr.inv_area;
+  V3 fn = norm3(mk3(v[0].n.x + v[1].n.x + v[2].n.x, v[0].n.y + v[1].n.y + v[2].n.y,
+                    v[0].n.z + v[1].n.z + v[2].n.z));
+  float avg[3];
+  for (int k = 0; k < 3; k++)
+    avg[k] = (v[0].c[k] + v[1].c[k] + v[2].c[k]) * (1.0f / 3.0f);
+  float col[3];
+  if (d.flags & DF_LIT) {
+    V3 wp = mk3((v[0].wp.x + v[1].wp.x + v[2].wp.x) / 3.0f, (v[0].wp.y + v[1].wp.y + v[2].wp.y) / 3.0f,
+                (v[0].wp.z + v[1].wp.z + v[2].wp.z) / 3.0f);
+    float lighting = diffuse_flat(fn, wp, a.lights + d.light_off, d.light_count, d.ambient);
+    float ds = 1.0f - d.metallic;
+    float env_flat = d.ambient * d.metallic * 0.3f;
+    for (int k = 0; k < 3; k++)
+      col[k] = avg[k] * (lighting * ds + env_flat);
+  } else {
+    V3 nl = norm3(mk3(d.light_dir[0], d.light_dir[1], d.light_dir[2]));
+    float ndotl = dot3(fn, nl);
+    if (ndotl < 0.0f)
+      ndotl = 0.0f;
+    float lighting = clamp01(d.ambient + (1.0f - d.ambient) * ndotl);
+    for (int k = 0; k < 3; k++)
+      col[k] = avg[k] * lighting;
+  }
+  for (int k = 0; k < 3; k++)
+    sr.col[k] = col[k] < 0.0f ? 0.0f : col[k];
+  return true;
+}
+
+__device__ __forceinline__ bool outside_same_plane(float4 a, float4 b, float4 c) {
+  return (a.x < -a.w && b.x < -b.w && c.x < -c.w) || (a.x > a.w && b.x > b.w && c.x > c.w) ||
+         (a.y < -a.w && b.y < -b.w && c.y < -c.w) || (a.y > a.w && b.y > b.w && c.y > c.w) ||
+         (a.z < -a.w && b.z < -b.w && c.z < -c.w) || (a.z > a.w && b.z > b.w && c.z > c.w);
+}
+
+__device__ __forceinline__ bool inside_all(float4 p) {
+  return p.x >= -p.w && p.x <= p.w && p.y >= -p.w && p.y <= p.w && p.z >= -p.w && p.z <= p.w;
+}
+
+/* Warp-aggregated allocation of one slot from *counter: the converged lanes
+ * share a single atomicAdd and take consecutive slots in lane order. */
+__device__ __forceinline__ uint32_t warp_alloc1(uint32_t *counter) {
+  const uint32_t mask = __activemask();
+  const uint32_t lane = threadIdx.x & 31u;
+  const int leader = __ffs(mask) - 1;
+  uint32_t base = 0;
+  if ((int)lane == leader)
+    base = atomicAdd(counter, (uint32_t)__popc(mask));
+  base = __shfl_sync(mask, base, leader);
+  return base + (uint32_t)__popc(mask & ((1u << lane) - 1u));
+}
+
+/* k_setup — one thread per triangle (mop_sw_rasterize_triangle_full
+ * rasterizer.c:2458-2530 up to the fan loop). */
+__global__ void k_setup(FrameArgs a) {
+  uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= a.total_tris)
+    return;
+  const DrawRec &d = a.draws[find_draw_by(a.draws, a.draw_count, t, false)];
+  uint32_t lt = t - d.tbase;
+  uint32_t i0 = __ldg(d.ibuf + 3u * lt), i1 = __ldg(d.ibuf + 3u * lt + 1u),
+           i2 = __ldg(d.ibuf + 3u * lt + 2u);
+  bool alive = !(i0 >= d.vertex_count || i1 >= d.vertex_count || i2 >= d.vertex_count);
+  int status = 0; /* 0 dead, 1 single fan triangle, 2 needs clipping */
+  uint32_t g[3] = {d.vbase + i0, d.vbase + i1, d.vbase + i2};
+  CV v[3];
+  if (alive) {
+    float4 A = a.clip[g[0]], B = a.clip[g[1]], C = a.clip[g[2]];
+    if (!outside_same_plane(A, B, C)) {
+      bool culled = false;
+      if ((d.flags & DF_CULL) && A.w > 0.0f && B.w > 0.0f && C.w > 0.0f) {
+        float ex = B.x * A.w - A.x * B.w;
+        float ey = B.y * A.w - A.y * B.w;
+        float fx = C.x * A.w - A.x * C.w;
+        float fy = C.y * A.w - A.y * C.w;
+        culled = (ex * fy - ey * fx <= 0.0f);
+      }
+      if (!culled) {
+        if (A.w > 0.0f && B.w > 0.0f && C.w > 0.0f && inside_all(A) && inside_all(B) &&
+            inside_all(C))
+          status = 1;
+        else
+          status = 2;
+      }
+    }
+  }
+  RasterRec rr;
+  ShadeRec sr;
+  if (status == 1) {
+    for (int k = 0; k < 3; k++)
+      v[k] = load_cv(a, g[k]);
+    if (!fan_setup(a, d, v, g, t << ORDER_FAN_BITS, rr, sr))
+      status = 0;
+  }
+  if (status == 2) {
+    uint32_t q = warp_alloc1(&a.ctr->clip_count);
+    if (q < a.clip_cap) {
+      a.clipq[q] = t;
+    } else {
+      atomicOr(&a.ctr->overflow, 4u);
+    }
+    a.rec_base[t] = REC_DEAD; /* k_clip overwrites it */
+    return;
+  }
+  if (status == 1) {
+    uint32_t r = warp_alloc1(&a.ctr->rec_count);
+    if (r < a.rec_cap) {
+      a.rrec[r] = rr;
+      a.srec[r] = sr;
+      a.rec_base[t] = r;
+    } else {
+      atomicOr(&a.ctr->overflow, 1u);
+      a.rec_base[t] = REC_DEAD;
+    }
+    return;
+  }
+  a.rec_base[t] = REC_DEAD;
+}
+
+/* Sutherland-Hodgman (rasterizer.c:514-626) on the triangles queued by
+ * k_setup; one thread per queued triangle. */
+#define MAX_CLIP 24
+
+__device__ __forceinline__ float lerpf(float x, float y, float t) { return x + t * (y - x); }
+
+__device__ __forceinline__ CV cv_lerp(const CV &p, const CV &q, float t) {
+  CV r;
+  r.p.x = lerpf(p.p.x, q.p.x, t);
+  r.p.y = lerpf(p.p.y, q.p.y, t);
+  r.p.z = lerpf(p.p.z, q.p.z, t);
+  r.p.w = lerpf(p.p.w, q.p.w, t);
+  r.n = mk3(lerpf(p.n.x, q.n.x, t), lerpf(p.n.y, q.n.y, t), lerpf(p.n.z, q.n.z, t));
+  r.wp = mk3(lerpf(p.wp.x, q.wp.x, t), lerpf(p.wp.y, q.wp.y, t), lerpf(p.wp.z, q.wp.z, t));
+  for (int k = 0; k < 4; k++)
+    r.c[k] = lerpf(p.c[k], q.c[k], t);
+  return r;
+}
+
+__device__ __forceinline__ float plane_dist(int pl, float4 p) {
+  /* the reference multiplies by every plane coefficient, zeros included */
+  const float nx[6] = {1.0f, -1.0f, 0.0f, 0.0f, 0.0f, 0.0f};
+  const float ny[6] = {0.0f, 0.0f, 1.0f, -1.0f, 0.0f, 0.0f};
+  const float nz[6] = {0.0f, 0.0f, 0.0f, 0.0f, 1.0f, -1.0f};
+  return nx[pl] * p.x + ny[pl] * p.y + nz[pl] * p.z + 1.0f * p.w;
+}
+
+__global__ void k_clip(FrameArgs a) {
+  uint32_t n_q = a.ctr->clip_count;
+  if (n_q > a.clip_cap)
+    n_q = a.clip_cap;
+  for (uint32_t qi = blockIdx.x * blockDim.x + threadIdx.x; qi < n_q;
+       qi += gridDim.x * blockDim.x) {
+    uint32_t t = a.clipq[qi];
+    const DrawRec &d = a.draws[find_draw_by(a.draws, a.draw_count, t, false)];
+    uint32_t lt = t - d.tbase;
+    CV buf0[MAX_CLIP], buf1[MAX_CLIP];
+    for (int k = 0; k < 3; k++)
+      buf0[k] = load_cv(a, d.vbase + __ldg(d.ibuf + 3u * lt + k));
+    CV *src = buf0, *dst = buf1;
+    int cnt = 3;
+    for (int pl = 0; pl < 6 && cnt > 0; pl++) {
+      int m = 0;
+      CV prev = src[cnt - 1];
+      float dp = plane_dist(pl, prev.p);
+      for (int i = 0; i < cnt; i++) {
+        CV cur = src[i];
+        float dc = plane_dist(pl, cur.p);
+        if (dc >= 0.0f) {
+          if (dp < 0.0f) {
+            float tt = dp / (dp - dc);
+            if (m < MAX_CLIP)
+              dst[m++] = cv_lerp(prev, cur, tt);
+          }
+          if (m < MAX_CLIP)
+            dst[m++] = cur;
+        } else if (dp >= 0.0f) {
+          float tt = dp / (dp - dc);
+          if (m < MAX_CLIP)
+            dst[m++] = cv_lerp(prev, cur, tt);
+        }
+        prev = cur;
+        dp = dc;
+      }
+      cnt = m;
+      CV *tmp = src;
+      src = dst;
+      dst = tmp;
+    }
+    if (cnt < 3) {
+      a.rec_base[t] = REC_DEAD;
+      continue;
+    }
+    /* store the polygon's vertices, then one record per fan triangle */
+    uint32_t e = atomicAdd(&a.ctr->extra_vertices, (uint32_t)cnt);
+    uint32_t nf = (uint32_t)cnt - 2u;
+    uint32_t r = atomicAdd(&a.ctr->rec_count, nf);
+    if (a.total_vertices + e + (uint32_t)cnt > a.vertex_cap || r + nf > a.rec_cap) {
+      atomicOr(&a.ctr->overflow, (a.total_vertices + e + (uint32_t)cnt > a.vertex_cap) ? 2u : 1u);
+      a.rec_base[t] = REC_DEAD;
+      continue;
+    }
+    uint32_t vs = a.total_vertices + e;
+    for (int k = 0; k < cnt; k++) {
+      const CV &c = src[k];
+      a.clip[vs + k] = c.p;
+      a.normal[vs + k] = make_float4(c.n.x, c.n.y, c.n.z, 0.0f);
+      a.world[vs + k] = make_float4(c.wp.x, c.wp.y, c.wp.z, 0.0f);
+      a.color[vs + k] = make_float4(c.c[0], c.c[1], c.c[2], c.c[3]);
+    }
+    for (int i = 1; i < cnt - 1; i++) {
+      CV fv[3] = {src[0], src[i], src[i + 1]};
+      uint32_t slot[3] = {vs, vs + (uint32_t)i, vs + (uint32_t)i + 1u};
+      RasterRec rr;
+      ShadeRec sr;
+      if (!fan_setup(a, d, fv, slot, (t << ORDER_FAN_BITS) | (uint32_t)(i - 1), rr, sr)) {
+        mark_dead(rr);
+        rr.order = (t << ORDER_FAN_BITS) | (uint32_t)(i - 1);
+        sr.draw = (uint32_t)(&d - a.draws);
+      }
+      a.rrec[r + i - 1] = rr;
+      a.srec[r + i - 1] = sr;
+    }
+    a.rec_base[t] = r;
+  }
+}
+
+/* ------------------------------------------------------------------------
+ * screen-tile binning
+ * ------------------------------------------------------------------------ */
+__device__ __forceinline__ bool rec_tiles(const FrameArgs &a, const RasterRec &r, int &tx0, int &ty0,
+                                          int &tx1, int &ty1) {
+  int y1 = (int)(r.y1 & 0x7fffu);
+  if ((int)r.x0 > (int)r.x1 || (int)r.y0 > y1)
+    return false;
+  /* live records always lie inside the framebuffer; anything else is an
+   * unwritten slot of an overflowed frame (which the host re-runs) */
+  if ((int)r.x1 >= a.width || y1 >= a.height)
+    return false;
+  tx0 = (int)r.x0 >> a.tile_shift;
+  tx1 = (int)r.x1 >> a.tile_shift;
+  ty0 = (int)r.y0 >> a.tile_shift;
+  ty1 = y1 >> a.tile_shift;
+  return true;
+}
+
+__global__ void k_bin_count(FrameArgs a) {
+  uint32_t n = a.ctr->rec_count;
+  if (n > a.rec_cap)
+    n = a.rec_cap;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    RasterRec r = a.rrec[i];
+    int tx0, ty0, tx1, ty1;
+    if (!rec_tiles(a, r, tx0, ty0, tx1, ty1))
+      continue;
+    for (int ty = ty0; ty <= ty1; ty++)
+      for (int tx = tx0; tx <= tx1; tx++)
+        atomicAdd(&a.tile_count[ty * a.tiles_x + tx], 1u);
+  }
+}
+
+/* Exclusive scan of the per-tile counts; one block of 1024 threads. */
+__global__ void k_bin_scan(FrameArgs a) {
+  __shared__ uint32_t part[1024];
+  int n = a.tiles_x * a.tiles_y;
+  int per = (n + 1023) / 1024;
+  int b = threadIdx.x * per, e = min(b + per, n);
+  uint32_t s = 0;
+  for (int i = b; i < e; i++)
+    s += a.tile_count[i];
+  part[threadIdx.x] = s;
+  __syncthreads();
+  for (int o = 1; o < 1024; o <<= 1) {
+    uint32_t v = threadIdx.x >= (unsigned)o ? part[threadIdx.x - o] : 0u;
+    __syncthreads();
+    part[threadIdx.x] += v;
+    __syncthreads();
+  }
+  uint32_t run = threadIdx.x ? part[threadIdx.x - 1] : 0u;
+  for (int i = b; i < e; i++) {
+    a.tile_off[i] = run;
+    run += a.tile_count[i];
+  }
+  if (threadIdx.x == 1023) {
+    a.ctr->bin_total = part[1023];
+    if (part[1023] > a.bin_cap)
+      atomicOr(&a.ctr->overflow, 8u);
+  }
+}
+
+__global__ void k_bin_fill(FrameArgs a) {
+  uint32_t n = a.ctr->rec_count;
+  if (n > a.rec_cap)
+    n = a.rec_cap;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    RasterRec r = a.rrec[i];
+    int tx0, ty0, tx1, ty1;
+    if (!rec_tiles(a, r, tx0, ty0, tx1, ty1))
+      continue;
+    for (int ty = ty0; ty <= ty1; ty++)
+      for (int tx = tx0; tx <= tx1; tx++) {
+        int tile = ty * a.tiles_x + tx;
+        uint32_t pos = a.tile_off[tile] + atomicAdd(&a.tile_fill[tile], 1u);
+        if (pos < a.bin_cap)
+          a.bins[pos] = i;
+      }
+  }
+}
+
+/* ------------------------------------------------------------------------
+ * k_tile — per screen tile: visibility into shared memory, then deferred
+ * shading + ACES resolve of every sample of the tile.
+ * ------------------------------------------------------------------------ */
+__device__ __forceinline__ float aces(float x) { /* rasterizer.c:2770-2774 */
+  float a = 2.51f, b = 0.03f, c = 2.43f, d = 0.59f, e = 0.14f;
+  float m = (x * (a * x + b)) / (x * (c * x + d) + e);
+  return m < 0.0f ? 0.0f : (m > 1.0f ? 1.0f : m);
+}
+
+template <int TS>
+__global__ void __launch_bounds__(TS *TS) k_tile(FrameArgs a) {
+  constexpr int NT = TS * TS;
+  __shared__ unsigned long long key[NT];
+  __shared__ uint32_t s_rec[NT];
+  __shared__ uint32_t s_scan[NT + 1];
+  __shared__ uint32_t s_warp[NT / 32];
+  __shared__ int s_tile;
+  const int tid = threadIdx.x;
+  const int ntiles = a.tiles_x * a.tiles_y;
+  for (;;) {
+    if (tid == 0)
+      s_tile = (int)atomicAdd(&a.ctr->tile_cursor, 1u);
+    key[tid] = KEY_EMPTY;
+    __syncthreads();
+    const int tile = s_tile;
+    if (tile >= ntiles)
+      break;
+    const int tx0 = (tile % a.tiles_x) * TS, ty0 = (tile / a.tiles_x) * TS;
+    uint32_t beg = a.tile_off[tile], cnt = a.tile_count[tile];
+    if (beg >= a.bin_cap)
+      cnt = 0;
+    else if (cnt > a.bin_cap - beg)
+      cnt = a.bin_cap - beg;
+    /* ---- visibility ---- */
+    for (uint32_t base = 0; base < cnt; base += NT) {
+      uint32_t i = base + (uint32_t)tid;
+      uint32_t rows = 0, rid = 0;
+      if (i < cnt) {
+        rid = a.bins[beg + i];
+        if (rid >= a.rec_cap)
+          rid = 0; /* defensive: only reachable in an overflowed frame */
+        const RasterRec &r = a.rrec[rid];
+        int ry0 = max((int)r.y0, ty0), ry1 = min((int)(r.y1 & 0x7fffu), ty0 + TS - 1);
+        int rx0 = max((int)r.x0, tx0), rx1 = min((int)r.x1, tx0 + TS - 1);
+        if (ry0 <= ry1 && rx0 <= rx1)
+          rows = (uint32_t)(ry1 - ry0 + 1);
+      }
+      s_rec[tid] = rid;
+      /* block exclusive scan of rows */
+      uint32_t incl = rows;
+      for (int o = 1; o < 32; o <<= 1) {
+        uint32_t v = __shfl_up_sync(0xffffffffu, incl, o);
+        if ((tid & 31) >= o)
+          incl += v;
+      }
+      if ((tid & 31) == 31)
+        s_warp[tid >> 5] = incl;
+      __syncthreads();
+      if (tid < 32) {
+        uint32_t wv = tid < NT / 32 ? s_warp[tid] : 0u;
+        for (int o = 1; o < 32; o <<= 1) {
+          uint32_t v = __shfl_up_sync(0xffffffffu, wv, o);
+          if (tid >= o)
+            wv += v;
+        }
+        if (tid < NT / 32)
+          s_warp[tid] = wv;
+      }
+      __syncthreads();
+      uint32_t excl = incl - rows + ((tid >> 5) ? s_warp[(tid >> 5) - 1] : 0u);
+      s_scan[tid] = excl;
+      if (tid == NT - 1)
+        s_scan[NT] = excl + rows;
+      __syncthreads();
+      const uint32_t total = s_scan[NT];
+      for (uint32_t it = (uint32_t)tid; it < total; it += NT) {
+        /* item -> (record, row): last j with s_scan[j] <= it */
+        int lo = 0, hi = NT;
+        while (hi - lo > 1) {
+          int mid = (lo + hi) >> 1;
+          if (s_scan[mid] <= it)
+            lo = mid;
+          else
+            hi = mid;
+        }
+        const RasterRec r = a.rrec[s_rec[lo]];
+        const bool flat = (r.y1 & REC_FLAT_BIT) != 0;
+        const int ry0 = max((int)r.y0, ty0);
+        const int y = ry0 + (int)(it - s_scan[lo]);
+        const int xs = max((int)r.x0, tx0), xe = min((int)r.x1, tx0 + TS - 1);
+        const int jr = y - (int)r.y0, kc = xs - (int)r.x0;
+        float w0 = fold_add(fold_add(r.w0[0], r.dy[0], jr), r.dx[0], kc);
+        float w1 = fold_add(fold_add(r.w0[1], r.dy[1], jr), r.dx[1], kc);
+        float w2 = fold_add(fold_add(r.w0[2], r.dy[2], jr), r.dx[2], kc);
+        float z = 0.0f;
+        if (flat)
+          z = fold_add(fold_add(r.zc[0], r.zc[2], jr), r.zc[1], kc);
+        bool seen = false;
+        for (int x = xs; x <= xe; x++) {
+          if (w0 >= 0.0f && w1 >= 0.0f && w2 >= 0.0f) {
+            seen = true;
+            float zz = z;
+            if (!flat) {
+              float b0 = w0 * r.inv_area, b1 = w1 * r.inv_area, b2 = w2 * r.inv_area;
+              zz = b0 * r.zc[0] + b1 * r.zc[1] + b2 * r.zc[2];
+            }
+            if (zz < 1.0f) {
+              unsigned long long k =
+                  ((unsigned long long)depth_key(zz) << 32) | (unsigned long long)r.order;
+              atomicMin(&key[(y - ty0) * TS + (x - tx0)], k);
+            }
+          } else if (seen) {
+            break; /* edge values are monotone along a row: coverage ended */
+          }
+          w0 = __fadd_rn(w0, r.dx[0]);
+          w1 = __fadd_rn(w1, r.dx[1]);
+          w2 = __fadd_rn(w2, r.dx[2]);
+          if (flat)
+            z = __fadd_rn(z, r.zc[1]);
+        }
+      }
+      __syncthreads();
+    }
+    /* ---- shading + resolve of sample `tid` ---- */
+    const int x = tx0 + (tid % TS), y = ty0 + (tid / TS);
+    if (x < a.width && y < a.height) {
+      const size_t px = (size_t)y * (size_t)a.width + (size_t)x;
+      const unsigned long long k = key[tid];
+      uchar4 out;
+      float depth = 1.0f;
+      uint32_t oid = 0;
+      uint32_t rid = 0xffffffffu;
+      if (k != KEY_EMPTY) {
+        const uint32_t t = (uint32_t)k >> ORDER_FAN_BITS;
+        if (t < a.total_tris) {
+          const uint32_t rb = a.rec_base[t];
+          if (rb != REC_DEAD)
+            rid = rb + ((uint32_t)k & ((1u << ORDER_FAN_BITS) - 1u));
+        }
+        if (rid >= a.rec_cap)
+          rid = 0xffffffffu; /* overflowed frame: the host discards it */
+      }
+      if (rid == 0xffffffffu) {
+        /* background: clear colour, id 0 (rasterizer.c:2785-2792) */
+        out.x = x86_f2u8(fminf(a.clear[0], 1.0f) * 255.0f + 0.5f);
+        out.y = x86_f2u8(fminf(a.clear[1], 1.0f) * 255.0f + 0.5f);
+        out.z = x86_f2u8(fminf(a.clear[2], 1.0f) * 255.0f + 0.5f);
+        out.w = 255;
+      } else {
+        const RasterRec r = a.rrec[rid];
+        const ShadeRec s = a.srec[rid];
+        const DrawRec &d = a.draws[s.draw < a.draw_count ? s.draw : 0];
+        const int jr = y - (int)r.y0, kc = x - (int)r.x0;
+        float hdr[3];
+        if (r.y1 & REC_FLAT_BIT) {
+          depth = fold_add(fold_add(r.zc[0], r.zc[2], jr), r.zc[1], kc);
+          hdr[0] = s.col[0];
+          hdr[1] = s.col[1];
+          hdr[2] = s.col[2];
+        } else if (s.v[0] >= a.vertex_cap || s.v[1] >= a.vertex_cap || s.v[2] >= a.vertex_cap) {
+          hdr[0] = hdr[1] = hdr[2] = 0.0f; /* unreachable for live records */
+        } else {
+          float w[3];
+          for (int e = 0; e < 3; e++)
+            w[e] = fold_add(fold_add(r.w0[e], r.dy[e], jr), r.dx[e], kc);
+          float b0 = w[0] * r.inv_area, b1 = w[1] * r.inv_area, b2 = w[2] * r.inv_area;
+          depth = b0 * r.zc[0] + b1 * r.zc[1] + b2 * r.zc[2];
+          float iw0 = 1.0f / a.clip[s.v[0]].w, iw1 = 1.0f / a.clip[s.v[1]].w,
+                iw2 = 1.0f / a.clip[s.v[2]].w;
+          float pc[3] = {b0 * iw0, b1 * iw1, b2 * iw2};
+          float ip = 1.0f / (pc[0] + pc[1] + pc[2]);
+          pc[0] *= ip;
+          pc[1] *= ip;
+          pc[2] *= ip;
+          shade_smooth(a, d, s.v, pc, hdr);
+        }
+        oid = d.object_id;
+        out.x = x86_f2u8(aces(hdr[0] * a.exposure) * 255.0f + 0.5f);
+        out.y = x86_f2u8(aces(hdr[1] * a.exposure) * 255.0f + 0.5f);
+        out.z = x86_f2u8(aces(hdr[2] * a.exposure) * 255.0f + 0.5f);
+        out.w = x86_f2u8(1.0f * 255.0f + 0.5f);
+      }
+      a.pre[px] = out;
+      a.depth[px] = depth;
+      a.ids[px] = oid;
+    }
+    __syncthreads();
+  }
+}
+
+template __global__ void k_tile<16>(FrameArgs);
+template __global__ void k_tile<8>(FrameArgs);
+
+/* ------------------------------------------------------------------------
+ * k_post — FXAA (rasterizer.c:2625-2761), tonemap/gamma/vignette
+ * (postprocess.c:24-116) and the SSAA box (viewport.c:3385-3411); one
+ * thread per presented pixel covering its ssaa x ssaa samples.
+ * ------------------------------------------------------------------------ */
+__device__ __forceinline__ float luma(uchar4 p) {
+  return 0.299f * (float)p.x + 0.587f * (float)p.y + 0.114f * (float)p.z;
+}
+
+__device__ uchar4 post_sample(const PostArgs &a, const float *lut, int x, int y) {
+  const int w = a.width, h = a.height;
+  uchar4 c = a.pre[(size_t)y * w + x];
+  if ((a.effects & 16u) && w >= 3 && h >= 3 && x >= 1 && y >= 1 && x < w - 1 && y < h - 1) {
+#define PX(xx, yy) a.pre[(size_t)(yy)*w + (xx)]
+    float lM = luma(c), lN = luma(PX(x, y - 1)), lS = luma(PX(x, y + 1)), lW = luma(PX(x - 1, y)),
+          lE = luma(PX(x + 1, y));
+    float mn = lM, mx = lM;
+    if (lN < mn) mn = lN;
+    if (lS < mn) mn = lS;
+    if (lW < mn) mn = lW;
+    if (lE < mn) mn = lE;
+    if (lN > mx) mx = lN;
+    if (lS > mx) mx = lS;
+    if (lW > mx) mx = lW;
+    if (lE > mx) mx = lE;
+    float range = mx - mn;
+    if (!(range < 0.0625f * mx + 0.004f)) {
+      float lNW = luma(PX(x - 1, y - 1)), lNE = luma(PX(x + 1, y - 1)), lSW = luma(PX(x - 1, y + 1)),
+            lSE = luma(PX(x + 1, y + 1));
+      float avg = (lN + lS + lW + lE) * (2.0f / 12.0f) + (lNW + lNE + lSW + lSE) * (1.0f / 12.0f);
+      float sub = fabsf(avg - lM);
+      sub = sub / range;
+      if (sub > 1.0f)
+        sub = 1.0f;
+      sub = sub * sub * (3.0f - 2.0f * sub);
+      sub *= 0.75f;
+      float eh = fabsf(-2.0f * lW + lNW + lSW) + fabsf(-2.0f * lM + lN + lS) * 2.0f +
+                 fabsf(-2.0f * lE + lNE + lSE);
+      float ev = fabsf(-2.0f * lN + lNW + lNE) + fabsf(-2.0f * lM + lW + lE) * 2.0f +
+                 fabsf(-2.0f * lS + lSW + lSE);
+      bool horiz = eh >= ev;
+      int stx = horiz ? 0 : 1, sty = horiz ? 1 : 0;
+      float lp = horiz ? lS : lE, ln = horiz ? lN : lW;
+      float gp = fabsf(lp - lM), gn = fabsf(ln - lM);
+      int nx = x + (gp >= gn ? stx : -stx), ny = y + (gp >= gn ? sty : -sty);
+      uchar4 nb = PX(nx, ny);
+      float ib = 1.0f - sub;
+      uchar4 o = c;
+      o.x = x86_f2u8((float)c.x * ib + (float)nb.x * sub);
+      o.y = x86_f2u8((float)c.y * ib + (float)nb.y * sub);
+      o.z = x86_f2u8((float)c.z * ib + (float)nb.z * sub);
+      c = o;
+    }
+#undef PX
+  }
+  if (a.effects != 0u) {
+    float v[3] = {lut[c.x], lut[c.y], lut[c.z]};
+    if (a.effects & 4u) {
+      float cx = (float)w * 0.5f, cy = (float)h * 0.5f;
+      float maxd = sqrtf(cx * cx + cy * cy);
+      float dx = (float)x - cx, dy = (float)y - cy;
+      float dist = sqrtf(dx * dx + dy * dy) / maxd;
+      float vg = 1.0f - dist * dist * 0.5f;
+      if (vg < 0.0f)
+        vg = 0.0f;
+      for (int k = 0; k < 3; k++)
+        v[k] *= vg;
+    }
+    for (int k = 0; k < 3; k++) {
+      if (v[k] > 1.0f)
+        v[k] = 1.0f;
+      if (v[k] < 0.0f)
+        v[k] = 0.0f;
+    }
+    c.x = x86_f2u8(v[0] * 255.0f + 0.5f);
+    c.y = x86_f2u8(v[1] * 255.0f + 0.5f);
+    c.z = x86_f2u8(v[2] * 255.0f + 0.5f);
+  }
+  return c;
+}
+
+__global__ void k_post(PostArgs a) {
+  __shared__ float s_lut[256];
+  for (int i = threadIdx.y * blockDim.x + threadIdx.x; i < 256; i += blockDim.x * blockDim.y)
+    s_lut[i] = a.lut[i];
+  __syncthreads();
+  const int sf = a.ssaa;
+  const int pw = a.width / sf, ph = a.height / sf;
+  int px = blockIdx.x * blockDim.x + threadIdx.x;
+  int py = blockIdx.y * blockDim.y + threadIdx.y;
+  if (px >= pw || py >= ph)
+    return;
+  uint32_t acc[4] = {0, 0, 0, 0};
+  for (int dy = 0; dy < sf; dy++)
+    for (int dx = 0; dx < sf; dx++) {
+      int x = px * sf + dx, y = py * sf + dy;
+      uchar4 c = post_sample(a, s_lut, x, y);
+      a.out[(size_t)y * a.width + x] = c;
+      acc[0] += c.x;
+      acc[1] += c.y;
+      acc[2] += c.z;
+      acc[3] += c.w;
+    }
+  if (a.presented) {
+    uint32_t n = (uint32_t)(sf * sf);
+    a.presented[(size_t)py * pw + px] =
+        make_uchar4((uint8_t)(acc[0] / n), (uint8_t)(acc[1] / n), (uint8_t)(acc[2] / n),
+                    (uint8_t)(acc[3] / n));
+  }
+}
+
+/* SSAA box of an already post-processed buffer (read_color path). */
+__global__ void k_box(const uchar4 *src, int width, int height, int sf, uchar4 *dst) {
+  const int pw = width / sf, ph = height / sf;
+  int px = blockIdx.x * blockDim.x + threadIdx.x;
+  int py = blockIdx.y * blockDim.y + threadIdx.y;
+  if (px >= pw || py >= ph)
+    return;
+  uint32_t acc[4] = {0, 0, 0, 0};
+  for (int dy = 0; dy < sf; dy++)
+    for (int dx = 0; dx < sf; dx++) {
+      uchar4 c = src[(size_t)(py * sf + dy) * width + px * sf + dx];
+      acc[0] += c.x;
+      acc[1] += c.y;
+      acc[2] += c.z;
+      acc[3] += c.w;
+    }
+  uint32_t n = (uint32_t)(sf * sf);
+  dst[(size_t)py * pw + px] = make_uchar4((uint8_t)(acc[0] / n), (uint8_t)(acc[1] / n),
+                                          (uint8_t)(acc[2] / n), (uint8_t)(acc[3] / n));
+}
+
+/* ------------------------------------------------------------------------
+ * k_pick — mop_viewport_pick at presentation pixels (viewport.c:3687-3749):
+ * ID and depth of the top-left sample of the SSAA block.
+ * ------------------------------------------------------------------------ */
+__global__ void k_pick(const uint32_t *ids, const float *depth, int width, int height, int sf,
+                       const int2 *xy, uint32_t n, uint32_t *out_id, float *out_depth,
+                       int32_t *out_hit) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n)
+    return;
+  int2 q = xy[i];
+  uint32_t id = 0;
+  float dp = 1.0f;
+  int pw = width / sf, ph = height / sf;
+  if (q.x >= 0 && q.x < pw && q.y >= 0 && q.y < ph) {
+    size_t s = (size_t)(q.y * sf) * (size_t)width + (size_t)(q.x * sf);
+    id = ids[s];
+    if (id != 0)
+      dp = depth[s];
+  }
+  out_id[i] = id;
+  out_depth[i] = dp;
+  out_hit[i] = id != 0 ? 1 : 0;
+}
+
+/* ------------------------------------------------------------------------
+ * launchers (called from mopcuda_api.cu)
+ * ------------------------------------------------------------------------ */
+static inline unsigned blocks_for(uint32_t n, unsigned bs) { return (n + bs - 1u) / bs; }
+
+int mopcuda_launch_frame(const FrameArgs &a, const PostArgs &p, int tile_size, int grid_tiles,
+                         cudaStream_t s) {
+  int launches = 0;
+  if (a.total_vertices) {
+    k_vertex<<<blocks_for(a.total_vertices, 256), 256, 0, s>>>(a);
+    launches++;
+  }
+  if (a.total_tris) {
+    k_setup<<<blocks_for(a.total_tris, 256), 256, 0, s>>>(a);
+    k_clip<<<blocks_for(a.clip_cap < 65536u ? a.clip_cap : 65536u, 128), 128, 0, s>>>(a);
+    launches += 2;
+  }
+  const uint32_t rec_grid = blocks_for(a.rec_cap < (1u << 22) ? a.rec_cap : (1u << 22), 256);
+  k_bin_count<<<rec_grid, 256, 0, s>>>(a);
+  k_bin_scan<<<1, 1024, 0, s>>>(a);
+  k_bin_fill<<<rec_grid, 256, 0, s>>>(a);
+  launches += 3;
+  if (tile_size == 8)
+    k_tile<8><<<grid_tiles, 64, 0, s>>>(a);
+  else
+    k_tile<16><<<grid_tiles, 256, 0, s>>>(a);
+  launches++;
+  const int sf = p.ssaa;
+  dim3 pb(16, 16);
+  dim3 pg(blocks_for((uint32_t)(p.width / sf), 16), blocks_for((uint32_t)(p.height / sf), 16));
+  k_post<<<pg, pb, 0, s>>>(p);
+  launches++;
+  return launches;
+}
+
+int mopcuda_launch_box(const uchar4 *src, int width, int height, int sf, uchar4 *dst,
+                       cudaStream_t s) {
+  dim3 b(16, 16);
+  dim3 g(blocks_for((uint32_t)(width / sf), 16), blocks_for((uint32_t)(height / sf), 16));
+  k_box<<<g, b, 0, s>>>(src, width, height, sf, dst);
+  return 1;
+}
+
+int mopcuda_launch_pick(const uint32_t *ids, const float *depth, int width, int height, int sf,
+                        const int2 *xy, uint32_t n, uint32_t *out_id, float *out_depth,
+                        int32_t *out_hit, cudaStream_t s) {
+  if (n == 0)
+    return 0;
+  k_pick<<<blocks_for(n, 128), 128, 0, s>>>(ids, depth, width, height, sf, xy, n, out_id,
+                                             out_depth, out_hit);
+  return 1;
+}
+
+int mopcuda_tile_occupancy(int tile_size) {
+  int nb = 0;
+  if (tile_size == 8)
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_tile<8>, 64, 0);
+  else
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_tile<16>, 256, 0);
+  return nb > 0 ? nb : 1;
+}

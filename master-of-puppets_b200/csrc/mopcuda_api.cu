@@ -1,0 +1,1075 @@
+/*
+ * mopcuda_api.cu — host side of the C ABI declared in include/mop_cuda.h.
+ *
+ * Owns device memory (grow-only arenas per device, pinned host mirrors per
+ * framebuffer), records draws on the host, and launches the frame as one
+ * stream-ordered kernel sequence (kernels.cu).  Every host wait is bounded.
+ *
+ * Reference correspondence: this file plays the role of the CPU backend's
+ * RHI implementation (src/backend/cpu/cpu_backend.c), with the per-draw
+ * software rasterisation replaced by a deferred whole-frame device launch.
+ */
+#include "../../include/mop_cuda.h"
+#include "mopcuda_internal.cuh"
+
+#include <math.h>
+#include <stdarg.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+#include <time.h>
+
+#include <mutex>
+#include <vector>
+
+/* ------------------------------------------------------------------------
+ * errors
+ * ------------------------------------------------------------------------ */
+static thread_local char g_err[512] = "";
+
+static int fail(int code, const char *fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(g_err, sizeof g_err, fmt, ap);
+  va_end(ap);
+  return code;
+}
+
+#define CU_TRY(expr)                                                                      \
+  do {                                                                                    \
+    cudaError_t e_ = (expr);                                                              \
+    if (e_ != cudaSuccess)                                                                \
+      return fail(MOPCUDA_ECUDA, "%s: %s (%s:%d)", #expr, cudaGetErrorString(e_), __FILE__, \
+                  __LINE__);                                                              \
+  } while (0)
+
+extern "C" const char *mopcuda_last_error(void) { return g_err; }
+
+#define FRAME_TIMEOUT_MS 20000
+
+/* ------------------------------------------------------------------------
+ * objects
+ * ------------------------------------------------------------------------ */
+struct DevArena {
+  void *p = nullptr;
+  size_t cap = 0;
+  int ensure(size_t bytes) {
+    if (bytes <= cap)
+      return 0;
+    size_t n = bytes + bytes / 2 + 4096;
+    if (p)
+      cudaFree(p);
+    p = nullptr;
+    cap = 0;
+    if (cudaMalloc(&p, n) != cudaSuccess) {
+      cudaGetLastError();
+      return fail(MOPCUDA_ENOMEM, "cudaMalloc(%zu) failed", n);
+    }
+    cap = n;
+    return 0;
+  }
+  void release() {
+    if (p)
+      cudaFree(p);
+    p = nullptr;
+    cap = 0;
+  }
+  template <class T> T *as() const { return (T *)p; }
+};
+
+struct HostArena {
+  void *p = nullptr;
+  size_t cap = 0;
+  int ensure(size_t bytes) {
+    if (bytes <= cap)
+      return 0;
+    size_t n = bytes + bytes / 2 + 4096;
+    if (p)
+      cudaFreeHost(p);
+    p = nullptr;
+    cap = 0;
+    if (cudaMallocHost(&p, n) != cudaSuccess) {
+      cudaGetLastError();
+      return fail(MOPCUDA_ENOMEM, "cudaMallocHost(%zu) failed", n);
+    }
+    cap = n;
+    return 0;
+  }
+  void release() {
+    if (p)
+      cudaFreeHost(p);
+    p = nullptr;
+    cap = 0;
+  }
+  template <class T> T *as() const { return (T *)p; }
+};
+
+struct MopCudaBuffer {
+  void *d = nullptr;
+  void *h = nullptr; /* host shadow for buffer_read */
+  size_t size = 0;
+};
+
+struct MopCudaTexture {
+  int w = 0, h = 0;
+  bool hdr = false;
+  void *d = nullptr;
+  void *hcopy = nullptr;
+};
+
+struct MopCudaFramebuffer {
+  int w = 0, h = 0;
+  int ssaa = 1; /* presentation factor when known (fused SSAA output) */
+  DevArena pre, out, depth, ids, presented;
+  HostArena h_color, h_depth, h_ids;
+  bool host_color = false, host_depth = false, host_ids = false;
+  bool presented_valid = false;
+  uint64_t frame_serial = 0;
+};
+
+struct MopCudaDevice {
+  int ordinal = 0;
+  int num_sms = 148;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  std::mutex mu;
+  /* recorded frame */
+  MopCudaFramebuffer *fb = nullptr;
+  float clear[4] = {0, 0, 0, 1};
+  std::vector<DrawRec> draws;
+  std::vector<LightRec> lights;
+  uint32_t unsupported_draws = 0;
+  uint32_t skipped_draws = 0;
+  bool frame_open = false;
+  bool pending = false;
+  int frame_status = 0;
+  /* state */
+  float exposure = 1.0f;
+  uint32_t post = MOPCUDA_POST_GAMMA | MOPCUDA_POST_FXAA;
+  float lut[256];
+  int tile_size = 16;
+  /* IBL */
+  DevArena irr, pf, brdf;
+  int irr_w = 0, irr_h = 0, pf_w = 0, pf_h = 0, pf_levels = 0, brdf_size = 0;
+  float ibl_rot = 0.0f, ibl_int = 1.0f;
+  bool ibl_on = false;
+  /* frame arenas */
+  DevArena d_draws, d_lights, clip, world, normal, color, rec_base, rrec, srec, clipq, tile_count,
+      tile_off, tile_fill, bins, counters, pick_xy, pick_out;
+  HostArena h_draws, h_lights, h_counters, h_pick;
+  uint32_t vertex_cap = 0, rec_cap = 0, clip_cap = 0, bin_cap = 0;
+  uint32_t extra_hint = 0, rec_hint = 0, clip_hint = 0, bin_hint = 0;
+  uint64_t launches = 0;
+  float last_ms = 0.0f;
+};
+
+static int finish_frame(MopCudaDevice *d, int timeout_ms);
+
+/* float x86-compatible evaluation of the post-process byte map
+ * (postprocess.c:43-86 for one channel value) */
+static void build_lut(float lut[256], uint32_t fx) {
+  for (int i = 0; i < 256; i++) {
+    volatile float c = (float)i / 255.0f;
+    if (fx & MOPCUDA_POST_TONEMAP)
+      c = c / (c + 1.0f);
+    if (fx & MOPCUDA_POST_GAMMA) {
+      float x = c > 0.0f ? c : 0.0f;
+      c = x <= 0.0031308f ? x * 12.92f : 1.055f * powf(x, 1.0f / 2.4f) - 0.055f;
+    }
+    lut[i] = c;
+  }
+}
+
+/* ------------------------------------------------------------------------
+ * device
+ * ------------------------------------------------------------------------ */
+extern "C" MopCudaDevice *mopcuda_device_create(int ordinal) {
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || n <= 0) {
+    cudaGetLastError();
+    fail(MOPCUDA_ECUDA, "no CUDA device available");
+    return nullptr;
+  }
+  if (ordinal < 0 || ordinal >= n) {
+    fail(MOPCUDA_EINVAL, "CUDA ordinal %d out of range (%d devices)", ordinal, n);
+    return nullptr;
+  }
+  if (cudaSetDevice(ordinal) != cudaSuccess) {
+    cudaGetLastError();
+    fail(MOPCUDA_ECUDA, "cudaSetDevice(%d) failed", ordinal);
+    return nullptr;
+  }
+  MopCudaDevice *d = new MopCudaDevice();
+  d->ordinal = ordinal;
+  cudaDeviceGetAttribute(&d->num_sms, cudaDevAttrMultiProcessorCount, ordinal);
+  if (cudaStreamCreateWithFlags(&d->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreate(&d->ev0) != cudaSuccess || cudaEventCreate(&d->ev1) != cudaSuccess) {
+    cudaGetLastError();
+    fail(MOPCUDA_ECUDA, "stream/event creation failed");
+    delete d;
+    return nullptr;
+  }
+  build_lut(d->lut, d->post);
+  return d;
+}
+
+static int bounded_sync(MopCudaDevice *d, cudaEvent_t ev, int timeout_ms) {
+  struct timespec t0, t1;
+  clock_gettime(CLOCK_MONOTONIC, &t0);
+  for (;;) {
+    cudaError_t e = cudaEventQuery(ev);
+    if (e == cudaSuccess)
+      return MOPCUDA_OK;
+    if (e != cudaErrorNotReady)
+      return fail(MOPCUDA_ECUDA, "device error: %s", cudaGetErrorString(e));
+    clock_gettime(CLOCK_MONOTONIC, &t1);
+    double ms = (t1.tv_sec - t0.tv_sec) * 1e3 + (t1.tv_nsec - t0.tv_nsec) * 1e-6;
+    if (timeout_ms >= 0 && ms > (double)timeout_ms)
+      return fail(MOPCUDA_ETIMEOUT, "frame did not complete within %d ms", timeout_ms);
+    struct timespec nap = {0, 20000};
+    nanosleep(&nap, nullptr);
+  }
+}
+
+static int stream_sync(MopCudaDevice *d, int timeout_ms) {
+  cudaEvent_t e;
+  CU_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  cudaEventRecord(e, d->stream);
+  int rc = bounded_sync(d, e, timeout_ms);
+  cudaEventDestroy(e);
+  return rc;
+}
+
+extern "C" void mopcuda_device_destroy(MopCudaDevice *d) {
+  if (!d)
+    return;
+  cudaSetDevice(d->ordinal);
+  stream_sync(d, 10000);
+  DevArena *arenas[] = {&d->irr,       &d->pf,        &d->brdf,       &d->d_draws,  &d->d_lights,
+                        &d->clip,      &d->world,     &d->normal,     &d->color,    &d->rec_base,
+                        &d->rrec,      &d->srec,      &d->clipq,      &d->tile_count,
+                        &d->tile_off,  &d->tile_fill, &d->bins,       &d->counters, &d->pick_xy,
+                        &d->pick_out};
+  for (DevArena *a : arenas)
+    a->release();
+  d->h_draws.release();
+  d->h_lights.release();
+  d->h_counters.release();
+  d->h_pick.release();
+  cudaEventDestroy(d->ev0);
+  cudaEventDestroy(d->ev1);
+  cudaStreamDestroy(d->stream);
+  delete d;
+}
+
+extern "C" uint64_t mopcuda_launch_count(const MopCudaDevice *d) { return d ? d->launches : 0; }
+
+/* ------------------------------------------------------------------------
+ * buffers
+ * ------------------------------------------------------------------------ */
+extern "C" MopCudaBuffer *mopcuda_buffer_create(MopCudaDevice *d, const void *data, size_t size) {
+  if (!d || (!data && size)) {
+    fail(MOPCUDA_EINVAL, "buffer_create: bad arguments");
+    return nullptr;
+  }
+  std::lock_guard<std::mutex> lk(d->mu);
+  cudaSetDevice(d->ordinal);
+  MopCudaBuffer *b = new MopCudaBuffer();
+  b->size = size;
+  size_t alloc = size ? size : 16;
+  b->h = malloc(alloc);
+  if (!b->h || cudaMalloc(&b->d, alloc) != cudaSuccess) {
+    cudaGetLastError();
+    free(b->h);
+    delete b;
+    fail(MOPCUDA_ENOMEM, "buffer_create(%zu) failed", size);
+    return nullptr;
+  }
+  if (size) {
+    memcpy(b->h, data, size);
+    if (cudaMemcpy(b->d, data, size, cudaMemcpyHostToDevice) != cudaSuccess) {
+      cudaGetLastError();
+      cudaFree(b->d);
+      free(b->h);
+      delete b;
+      fail(MOPCUDA_ECUDA, "buffer_create: upload failed");
+      return nullptr;
+    }
+  }
+  return b;
+}
+
+extern "C" void mopcuda_buffer_destroy(MopCudaDevice *d, MopCudaBuffer *b) {
+  if (!d || !b)
+    return;
+  std::lock_guard<std::mutex> lk(d->mu);
+  cudaSetDevice(d->ordinal);
+  stream_sync(d, 10000); /* a launched frame may still read it */
+  cudaFree(b->d);
+  free(b->h);
+  delete b;
+}
+
+extern "C" int mopcuda_buffer_update(MopCudaDevice *d, MopCudaBuffer *b, const void *data,
+                                     size_t offset, size_t size) {
+  if (!d || !b || (!data && size) || offset > b->size || size > b->size - offset)
+    return fail(MOPCUDA_EINVAL, "buffer_update: range outside buffer");
+  std::lock_guard<std::mutex> lk(d->mu);
+  cudaSetDevice(d->ordinal);
+  int rc = stream_sync(d, 10000);
+  if (rc)
+    return rc;
+  memcpy((uint8_t *)b->h + offset, data, size);
+  CU_TRY(cudaMemcpy((uint8_t *)b->d + offset, data, size, cudaMemcpyHostToDevice));
+  return MOPCUDA_OK;
+}
+
+extern "C" const void *mopcuda_buffer_read(const MopCudaBuffer *b) { return b ? b->h : nullptr; }
+extern "C" size_t mopcuda_buffer_size(const MopCudaBuffer *b) { return b ? b->size : 0; }
+
+/* ------------------------------------------------------------------------
+ * textures
+ * ------------------------------------------------------------------------ */
+static MopCudaTexture *tex_create(MopCudaDevice *d, int w, int h, const void *data, size_t bpp,
+                                  bool hdr) {
+  if (!d || w <= 0 || h <= 0 || !data) {
+    fail(MOPCUDA_EINVAL, "texture_create: bad arguments");
+    return nullptr;
+  }
+  std::lock_guard<std::mutex> lk(d->mu);
+  cudaSetDevice(d->ordinal);
+  size_t bytes = (size_t)w * (size_t)h * bpp;
+  MopCudaTexture *t = new MopCudaTexture();
+  t->w = w;
+  t->h = h;
+  t->hdr = hdr;
+  t->hcopy = malloc(bytes);
+  if (!t->hcopy || cudaMalloc(&t->d, bytes) != cudaSuccess) {
+    cudaGetLastError();
+    free(t->hcopy);
+    delete t;
+    fail(MOPCUDA_ENOMEM, "texture_create: allocation failed");
+    return nullptr;
+  }
+  memcpy(t->hcopy, data, bytes);
+  if (cudaMemcpy(t->d, data, bytes, cudaMemcpyHostToDevice) != cudaSuccess) {
+    cudaGetLastError();
+    cudaFree(t->d);
+    free(t->hcopy);
+    delete t;
+    fail(MOPCUDA_ECUDA, "texture_create: upload failed");
+    return nullptr;
+  }
+  return t;
+}
+
+extern "C" MopCudaTexture *mopcuda_texture_create(MopCudaDevice *d, int w, int h,
+                                                  const uint8_t *rgba) {
+  return tex_create(d, w, h, rgba, 4, false);
+}
+
+extern "C" MopCudaTexture *mopcuda_texture_create_hdr(MopCudaDevice *d, int w, int h,
+                                                      const float *rgba) {
+  return tex_create(d, w, h, rgba, 16, true);
+}
+
+extern "C" void mopcuda_texture_destroy(MopCudaDevice *d, MopCudaTexture *t) {
+  if (!d || !t)
+    return;
+  std::lock_guard<std::mutex> lk(d->mu);
+  cudaSetDevice(d->ordinal);
+  stream_sync(d, 10000);
+  cudaFree(t->d);
+  free(t->hcopy);
+  delete t;
+}
+
+extern "C" int mopcuda_texture_read_rgba8(MopCudaDevice *d, MopCudaTexture *t, uint8_t *out,
+                                          size_t out_size) {
+  if (!t || t->hdr || !out)
+    return fail(MOPCUDA_EINVAL, "texture_read_rgba8: bad arguments");
+  size_t need = (size_t)t->w * (size_t)t->h * 4;
+  if (out_size < need)
+    return fail(MOPCUDA_EINVAL, "texture_read_rgba8: buffer too small");
+  memcpy(out, t->hcopy, need);
+  return MOPCUDA_OK;
+}
+
+/* ------------------------------------------------------------------------
+ * framebuffers
+ * ------------------------------------------------------------------------ */
+static int fb_alloc(MopCudaFramebuffer *fb, int w, int h) {
+  size_t s = (size_t)w * (size_t)h;
+  int rc = 0;
+  rc |= fb->pre.ensure(s * 4);
+  rc |= fb->out.ensure(s * 4);
+  rc |= fb->depth.ensure(s * 4);
+  rc |= fb->ids.ensure(s * 4);
+  rc |= fb->presented.ensure(s * 4);
+  rc |= fb->h_color.ensure(s * 4);
+  rc |= fb->h_depth.ensure(s * 4);
+  rc |= fb->h_ids.ensure(s * 4);
+  if (rc)
+    return MOPCUDA_ENOMEM;
+  fb->w = w;
+  fb->h = h;
+  fb->host_color = fb->host_depth = fb->host_ids = false;
+  fb->presented_valid = false;
+  return MOPCUDA_OK;
+}
+
+extern "C" MopCudaFramebuffer *mopcuda_framebuffer_create(MopCudaDevice *d, int w, int h) {
+  /* reference limit: mop_sw_framebuffer_alloc, rasterizer.c:31-35 */
+  if (!d || w <= 0 || h <= 0 || w > 16384 || h > 16384) {
+    fail(MOPCUDA_EINVAL, "framebuffer dimensions out of range: %dx%d", w, h);
+    return nullptr;
+  }
+  std::lock_guard<std::mutex> lk(d->mu);
+  cudaSetDevice(d->ordinal);
+  MopCudaFramebuffer *fb = new MopCudaFramebuffer();
+  if (fb_alloc(fb, w, h)) {
+    delete fb;
+    return nullptr;
+  }
+  return fb;
+}
+
+static void fb_release(MopCudaFramebuffer *fb) {
+  fb->pre.release();
+  fb->out.release();
+  fb->depth.release();
+  fb->ids.release();
+  fb->presented.release();
+  fb->h_color.release();
+  fb->h_depth.release();
+  fb->h_ids.release();
+}
+
+extern "C" void mopcuda_framebuffer_destroy(MopCudaDevice *d, MopCudaFramebuffer *fb) {
+  if (!d || !fb)
+    return;
+  std::lock_guard<std::mutex> lk(d->mu);
+  cudaSetDevice(d->ordinal);
+  stream_sync(d, 10000);
+  if (d->fb == fb)
+    d->fb = nullptr;
+  fb_release(fb);
+  delete fb;
+}
+
+extern "C" int mopcuda_framebuffer_resize(MopCudaDevice *d, MopCudaFramebuffer *fb, int w, int h) {
+  if (!d || !fb || w <= 0 || h <= 0 || w > 16384 || h > 16384)
+    return fail(MOPCUDA_EINVAL, "framebuffer_resize: %dx%d out of range", w, h);
+  std::lock_guard<std::mutex> lk(d->mu);
+  cudaSetDevice(d->ordinal);
+  int rc = stream_sync(d, 10000);
+  if (rc)
+    return rc;
+  fb_release(fb);
+  return fb_alloc(fb, w, h);
+}
+
+/* ------------------------------------------------------------------------
+ * frame state
+ * ------------------------------------------------------------------------ */
+extern "C" void mopcuda_set_exposure(MopCudaDevice *d, float e) {
+  if (d)
+    d->exposure = e;
+}
+
+extern "C" void mopcuda_set_post_effects(MopCudaDevice *d, uint32_t fx) {
+  if (!d)
+    return;
+  d->post = fx;
+  build_lut(d->lut, fx);
+}
+
+extern "C" int mopcuda_set_ibl(MopCudaDevice *d, const float *irr, int iw, int ih, const float *pf,
+                               int pw, int ph, int levels, const float *brdf, int bs, float rot,
+                               float intensity) {
+  if (!d)
+    return fail(MOPCUDA_EINVAL, "set_ibl: no device");
+  std::lock_guard<std::mutex> lk(d->mu);
+  cudaSetDevice(d->ordinal);
+  int rc = stream_sync(d, 10000);
+  if (rc)
+    return rc;
+  if (!irr) {
+    d->ibl_on = false;
+    return MOPCUDA_OK;
+  }
+  if (iw <= 0 || ih <= 0 || !pf || pw <= 0 || ph <= 0 || levels <= 0 || !brdf || bs <= 0)
+    return fail(MOPCUDA_EINVAL, "set_ibl: bad map dimensions");
+  size_t pf_px = 0;
+  for (int l = 0; l < levels; l++) {
+    int lw = pw >> l, lh = ph >> l;
+    pf_px += (size_t)(lw < 1 ? 1 : lw) * (size_t)(lh < 1 ? 1 : lh);
+  }
+  size_t ib = (size_t)iw * ih * 16, pb = pf_px * 16, bb = (size_t)bs * bs * 16;
+  if (d->irr.ensure(ib) || d->pf.ensure(pb) || d->brdf.ensure(bb))
+    return MOPCUDA_ENOMEM;
+  CU_TRY(cudaMemcpy(d->irr.p, irr, ib, cudaMemcpyHostToDevice));
+  CU_TRY(cudaMemcpy(d->pf.p, pf, pb, cudaMemcpyHostToDevice));
+  CU_TRY(cudaMemcpy(d->brdf.p, brdf, bb, cudaMemcpyHostToDevice));
+  d->irr_w = iw;
+  d->irr_h = ih;
+  d->pf_w = pw;
+  d->pf_h = ph;
+  d->pf_levels = levels;
+  d->brdf_size = bs;
+  d->ibl_rot = rot;
+  d->ibl_int = intensity;
+  d->ibl_on = true;
+  return MOPCUDA_OK;
+}
+
+/* ------------------------------------------------------------------------
+ * frame commands
+ * ------------------------------------------------------------------------ */
+extern "C" int mopcuda_frame_begin(MopCudaDevice *d, MopCudaFramebuffer *fb, const float clear[4]) {
+  if (!d || !fb)
+    return fail(MOPCUDA_EINVAL, "frame_begin: bad arguments");
+  std::lock_guard<std::mutex> lk(d->mu);
+  cudaSetDevice(d->ordinal);
+  /* The previous frame must be complete (or re-run after an overflow) before
+   * its recorded draws and pinned staging are reused. */
+  if (d->pending) {
+    int rc = finish_frame(d, FRAME_TIMEOUT_MS);
+    if (rc)
+      return rc;
+  }
+  d->fb = fb;
+  for (int k = 0; k < 4; k++)
+    d->clear[k] = clear ? clear[k] : 0.0f;
+  d->draws.clear();
+  d->lights.clear();
+  d->unsupported_draws = 0;
+  d->skipped_draws = 0;
+  d->frame_open = true;
+  return MOPCUDA_OK;
+}
+
+static float clamp01f(float x) { return x < 0.0f ? 0.0f : (x > 1.0f ? 1.0f : x); }
+
+/* Records one draw.  Order-independent opaque state is rendered exactly;
+ * zero-opacity draws are colour no-ops in the reference and are dropped;
+ * blended, wireframe, depth-test-off and unlit smooth (edge-AA) draws depend
+ * on submission order and are reported as unsupported. */
+static int record_draw(MopCudaDevice *d, const MopCudaDraw *c, const float *model,
+                       const float *mvp) {
+  if (!c->vertex_buffer || !c->index_buffer)
+    return fail(MOPCUDA_EINVAL, "draw: missing buffers");
+  float op = clamp01f(c->opacity);
+  if (op == 0.0f && c->blend_mode != 3) {
+    d->skipped_draws++;
+    return MOPCUDA_OK;
+  }
+  bool lit = c->lights && c->light_count > 0;
+  if (c->wireframe || !c->depth_test || !c->depth_write || c->blend_mode != 0 || op < 1.0f ||
+      (c->smooth && !lit)) {
+    d->unsupported_draws++;
+    return fail(MOPCUDA_EUNSUPPORTED,
+                "draw: blended / wireframe / depth-test-off / unlit-smooth state is not on "
+                "the order-independent path");
+  }
+  uint32_t stride = 48;
+  DrawRec r;
+  memset(&r, 0, sizeof r);
+  if (c->layout) {
+    const MopCudaVertexLayout *L = c->layout;
+    stride = L->stride;
+    if (stride == 0 || stride % 4 || L->position_offset < 0 || (L->position_offset % 4) ||
+        (L->normal_offset >= 0 && L->normal_offset % 4) ||
+        (L->color_offset >= 0 && L->color_offset % 4) || (L->uv_offset >= 0 && L->uv_offset % 4))
+      return fail(MOPCUDA_EINVAL, "draw: vertex layout must be 4-byte aligned with a position");
+    auto fits = [&](int off, int n) { return off < 0 || (uint32_t)off + 4u * (uint32_t)n <= stride; };
+    if (!fits(L->position_offset, L->position_components) ||
+        !fits(L->normal_offset, L->normal_components) || !fits(L->color_offset, L->color_components) ||
+        !fits(L->uv_offset, L->uv_components))
+      return fail(MOPCUDA_EINVAL, "draw: attribute outside the vertex stride");
+    r.flags |= DF_FLEX;
+    r.stride = stride;
+    r.off_pos = (int16_t)L->position_offset;
+    r.off_nrm = (int16_t)L->normal_offset;
+    r.off_col = (int16_t)L->color_offset;
+    r.off_uv = (int16_t)L->uv_offset;
+    r.n_pos = (int8_t)L->position_components;
+    r.n_nrm = (int8_t)L->normal_components;
+    r.n_col = (int8_t)L->color_components;
+    r.n_uv = (int8_t)L->uv_components;
+  }
+  if ((size_t)c->vertex_count * stride > c->vertex_buffer->size)
+    return fail(MOPCUDA_EINVAL, "draw: vertex_count exceeds the vertex buffer");
+  uint32_t tris = c->index_count / 3u;
+  if ((size_t)tris * 12u > c->index_buffer->size)
+    return fail(MOPCUDA_EINVAL, "draw: index_count exceeds the index buffer");
+  memcpy(r.mvp, mvp, sizeof r.mvp);
+  memcpy(r.model, model, sizeof r.model);
+  memcpy(r.light_dir, c->light_dir, sizeof r.light_dir);
+  r.ambient = c->ambient;
+  r.opacity = c->opacity;
+  r.metallic = c->metallic;
+  r.roughness = c->roughness;
+  r.depth_bias = c->depth_bias;
+  memcpy(r.cam_eye, c->cam_eye, sizeof r.cam_eye);
+  r.object_id = c->object_id;
+  r.vbuf = (const uint8_t *)c->vertex_buffer->d;
+  r.ibuf = (const uint32_t *)c->index_buffer->d;
+  if (c->texture && !c->texture->hdr && c->texture->w >= 1 && c->texture->h >= 1) {
+    r.tex = (const uint8_t *)c->texture->d;
+    r.tex_w = c->texture->w;
+    r.tex_h = c->texture->h;
+    r.flags |= DF_TEXTURED;
+  }
+  r.vertex_count = c->vertex_count;
+  r.index_count = tris * 3u;
+  if (c->smooth)
+    r.flags |= DF_SMOOTH;
+  if (c->backface_cull)
+    r.flags |= DF_CULL;
+  if (lit) {
+    r.flags |= DF_LIT;
+    r.light_off = (uint32_t)d->lights.size();
+    r.light_count = c->light_count;
+    for (uint32_t i = 0; i < c->light_count; i++) {
+      const MopCudaLight &s = c->lights[i];
+      LightRec L;
+      L.type = s.type;
+      memcpy(L.position, s.position, sizeof L.position);
+      memcpy(L.direction, s.direction, sizeof L.direction);
+      memcpy(L.color, s.color, sizeof L.color);
+      L.intensity = s.intensity;
+      L.range = s.range;
+      L.spot_inner_cos = s.spot_inner_cos;
+      L.spot_outer_cos = s.spot_outer_cos;
+      L.active = s.active;
+      d->lights.push_back(L);
+    }
+  }
+  d->draws.push_back(r);
+  return MOPCUDA_OK;
+}
+
+extern "C" int mopcuda_draw(MopCudaDevice *d, MopCudaFramebuffer *fb, const MopCudaDraw *c) {
+  if (!d || !fb || !c)
+    return fail(MOPCUDA_EINVAL, "draw: bad arguments");
+  std::lock_guard<std::mutex> lk(d->mu);
+  if (!d->frame_open || d->fb != fb)
+    return fail(MOPCUDA_EINVAL, "draw outside frame_begin/frame_end");
+  return record_draw(d, c, c->model, c->mvp);
+}
+
+/* mop_mat4_multiply order (math.c:182-194): running sum from 0.0f. */
+static void mat4_mul(const float *a, const float *b, float *c) {
+  float r[16];
+  for (int col = 0; col < 4; col++)
+    for (int row = 0; row < 4; row++) {
+      volatile float s = 0.0f;
+      for (int k = 0; k < 4; k++) {
+        volatile float p = a[k * 4 + row] * b[col * 4 + k];
+        s = s + p;
+      }
+      r[col * 4 + row] = s;
+    }
+  memcpy(c, r, sizeof r);
+}
+
+extern "C" int mopcuda_draw_instanced(MopCudaDevice *d, MopCudaFramebuffer *fb,
+                                      const MopCudaDraw *c, const float *view, const float *proj,
+                                      const float *inst, uint32_t n) {
+  if (!d || !fb || !c || !view || !proj || (!inst && n))
+    return fail(MOPCUDA_EINVAL, "draw_instanced: bad arguments");
+  std::lock_guard<std::mutex> lk(d->mu);
+  if (!d->frame_open || d->fb != fb)
+    return fail(MOPCUDA_EINVAL, "draw outside frame_begin/frame_end");
+  for (uint32_t i = 0; i < n; i++) {
+    float vm[16], mvp[16];
+    mat4_mul(view, inst + 16 * (size_t)i, vm);
+    mat4_mul(proj, vm, mvp);
+    int rc = record_draw(d, c, inst + 16 * (size_t)i, mvp);
+    if (rc)
+      return rc;
+  }
+  return MOPCUDA_OK;
+}
+
+static int launch_frame(MopCudaDevice *d) {
+  MopCudaFramebuffer *fb = d->fb;
+  const uint32_t nd = (uint32_t)d->draws.size();
+  uint64_t V = 0, T = 0;
+  for (uint32_t i = 0; i < nd; i++) {
+    d->draws[i].vbase = (uint32_t)V;
+    d->draws[i].tbase = (uint32_t)T;
+    V += d->draws[i].vertex_count;
+    T += d->draws[i].index_count / 3u;
+  }
+  if (T >= (1ull << (32 - ORDER_FAN_BITS)) || V >= (1ull << 31))
+    return fail(MOPCUDA_EINVAL, "frame too large: %llu triangles", (unsigned long long)T);
+  const int ts = d->tile_size, shift = ts == 8 ? 3 : 4;
+  const int tiles_x = (fb->w + ts - 1) / ts, tiles_y = (fb->h + ts - 1) / ts;
+  const uint32_t ntiles = (uint32_t)tiles_x * (uint32_t)tiles_y;
+  /* capacities: grow from the last frame's observed counts */
+  uint32_t extra = (uint32_t)(T / 8 + 1024);
+  if (extra < d->extra_hint)
+    extra = d->extra_hint;
+  uint32_t vcap = (uint32_t)V + extra;
+  uint32_t rcap = (uint32_t)(T + T / 4 + 1024);
+  if (rcap < d->rec_hint)
+    rcap = d->rec_hint;
+  uint32_t ccap = (uint32_t)(T / 8 + 1024);
+  if (ccap < d->clip_hint)
+    ccap = d->clip_hint;
+  uint32_t bcap = rcap * 2u + ntiles;
+  if (bcap < d->bin_hint)
+    bcap = d->bin_hint;
+  int rc = 0;
+  rc |= d->d_draws.ensure(sizeof(DrawRec) * (nd ? nd : 1));
+  rc |= d->d_lights.ensure(sizeof(LightRec) * (d->lights.size() + 1));
+  rc |= d->clip.ensure(16ull * vcap);
+  rc |= d->world.ensure(16ull * vcap);
+  rc |= d->normal.ensure(16ull * vcap);
+  rc |= d->color.ensure(16ull * vcap);
+  rc |= d->rec_base.ensure(4ull * (T ? T : 1));
+  rc |= d->rrec.ensure(sizeof(RasterRec) * (size_t)rcap);
+  rc |= d->srec.ensure(sizeof(ShadeRec) * (size_t)rcap);
+  rc |= d->clipq.ensure(4ull * ccap);
+  rc |= d->tile_count.ensure(4ull * ntiles);
+  rc |= d->tile_off.ensure(4ull * ntiles);
+  rc |= d->tile_fill.ensure(4ull * ntiles);
+  rc |= d->bins.ensure(4ull * bcap);
+  rc |= d->counters.ensure(sizeof(Counters));
+  rc |= d->h_draws.ensure(sizeof(DrawRec) * (nd ? nd : 1));
+  rc |= d->h_lights.ensure(sizeof(LightRec) * (d->lights.size() + 1));
+  rc |= d->h_counters.ensure(sizeof(Counters));
+  if (rc)
+    return MOPCUDA_ENOMEM;
+  d->vertex_cap = vcap;
+  d->rec_cap = rcap;
+  d->clip_cap = ccap;
+  d->bin_cap = bcap;
+  if (nd)
+    memcpy(d->h_draws.p, d->draws.data(), sizeof(DrawRec) * nd);
+  if (!d->lights.empty())
+    memcpy(d->h_lights.p, d->lights.data(), sizeof(LightRec) * d->lights.size());
+
+  FrameArgs a;
+  memset(&a, 0, sizeof a);
+  a.draws = d->d_draws.as<DrawRec>();
+  a.draw_count = nd;
+  a.lights = d->d_lights.as<LightRec>();
+  a.total_vertices = (uint32_t)V;
+  a.total_tris = (uint32_t)T;
+  a.clip = d->clip.as<float4>();
+  a.world = d->world.as<float4>();
+  a.normal = d->normal.as<float4>();
+  a.color = d->color.as<float4>();
+  a.vertex_cap = vcap;
+  a.rec_base = d->rec_base.as<uint32_t>();
+  a.rrec = d->rrec.as<RasterRec>();
+  a.srec = d->srec.as<ShadeRec>();
+  a.rec_cap = rcap;
+  a.clipq = d->clipq.as<uint32_t>();
+  a.clip_cap = ccap;
+  a.width = fb->w;
+  a.height = fb->h;
+  a.tile_shift = shift;
+  a.tiles_x = tiles_x;
+  a.tiles_y = tiles_y;
+  a.tile_count = d->tile_count.as<uint32_t>();
+  a.tile_off = d->tile_off.as<uint32_t>();
+  a.tile_fill = d->tile_fill.as<uint32_t>();
+  a.bins = d->bins.as<uint32_t>();
+  a.bin_cap = bcap;
+  a.ctr = d->counters.as<Counters>();
+  memcpy(a.clear, d->clear, sizeof a.clear);
+  a.exposure = d->exposure;
+  if (d->ibl_on) {
+    a.irr = d->irr.as<float>();
+    a.irr_w = d->irr_w;
+    a.irr_h = d->irr_h;
+    a.pf = d->pf.as<float>();
+    a.pf_w = d->pf_w;
+    a.pf_h = d->pf_h;
+    a.pf_levels = d->pf_levels;
+    a.brdf = d->brdf.as<float>();
+    a.brdf_size = d->brdf_size;
+    a.ibl_rotation = d->ibl_rot;
+    a.ibl_intensity = d->ibl_int;
+  }
+  a.pre = fb->pre.as<uchar4>();
+  a.depth = fb->depth.as<float>();
+  a.ids = fb->ids.as<uint32_t>();
+
+  PostArgs p;
+  memset(&p, 0, sizeof p);
+  p.pre = fb->pre.as<uchar4>();
+  p.out = fb->out.as<uchar4>();
+  int sf = fb->ssaa > 0 && fb->w % fb->ssaa == 0 && fb->h % fb->ssaa == 0 ? fb->ssaa : 1;
+  p.presented = sf > 1 ? fb->presented.as<uchar4>() : nullptr;
+  p.width = fb->w;
+  p.height = fb->h;
+  p.ssaa = sf;
+  p.effects = d->post & (MOPCUDA_POST_GAMMA | MOPCUDA_POST_TONEMAP | MOPCUDA_POST_VIGNETTE |
+                         MOPCUDA_POST_FXAA);
+  memcpy(p.lut, d->lut, sizeof p.lut);
+
+  cudaStream_t s = d->stream;
+  CU_TRY(cudaEventRecord(d->ev0, s));
+  if (nd)
+    CU_TRY(cudaMemcpyAsync(d->d_draws.p, d->h_draws.p, sizeof(DrawRec) * nd,
+                           cudaMemcpyHostToDevice, s));
+  if (!d->lights.empty())
+    CU_TRY(cudaMemcpyAsync(d->d_lights.p, d->h_lights.p, sizeof(LightRec) * d->lights.size(),
+                           cudaMemcpyHostToDevice, s));
+  CU_TRY(cudaMemsetAsync(d->counters.p, 0, sizeof(Counters), s));
+  CU_TRY(cudaMemsetAsync(d->tile_count.p, 0, 4ull * ntiles, s));
+  CU_TRY(cudaMemsetAsync(d->tile_fill.p, 0, 4ull * ntiles, s));
+  int occ = mopcuda_tile_occupancy(ts);
+  int grid_tiles = d->num_sms * occ;
+  if ((uint32_t)grid_tiles > ntiles)
+    grid_tiles = (int)ntiles;
+  d->launches += (uint64_t)mopcuda_launch_frame(a, p, ts, grid_tiles, s);
+  CU_TRY(cudaGetLastError());
+  CU_TRY(cudaMemcpyAsync(d->h_counters.p, d->counters.p, sizeof(Counters), cudaMemcpyDeviceToHost,
+                         s));
+  CU_TRY(cudaEventRecord(d->ev1, s));
+  fb->host_color = fb->host_depth = fb->host_ids = false;
+  fb->presented_valid = sf > 1;
+  fb->frame_serial++;
+  d->pending = true;
+  return MOPCUDA_OK;
+}
+
+
+/* Waits for the launched frame; re-runs it with larger arenas if any
+ * capacity overflowed (the counters say by how much). */
+static int finish_frame(MopCudaDevice *d, int timeout_ms) {
+  for (int attempt = 0; d->pending; attempt++) {
+    int rc = bounded_sync(d, d->ev1, timeout_ms);
+    if (rc) {
+      d->pending = false;
+      return rc;
+    }
+    d->pending = false;
+    cudaEventElapsedTime(&d->last_ms, d->ev0, d->ev1);
+    const Counters *c = d->h_counters.as<Counters>();
+    if (!c->overflow)
+      break;
+    if (attempt >= 4)
+      return fail(MOPCUDA_ENOMEM, "frame arenas overflowed repeatedly (flags %u)", c->overflow);
+    d->rec_hint = c->rec_count + c->rec_count / 4 + 1024;
+    d->clip_hint = c->clip_count + c->clip_count / 4 + 1024;
+    d->extra_hint = c->extra_vertices + c->extra_vertices / 4 + 1024;
+    d->bin_hint = c->bin_total + c->bin_total / 4 + 1024;
+    if (c->overflow & 1u)
+      d->rec_hint *= 2;
+    if (c->overflow & 2u)
+      d->extra_hint *= 2;
+    if (c->overflow & 4u)
+      d->clip_hint *= 2;
+    if (c->overflow & 8u)
+      d->bin_hint *= 2;
+    rc = launch_frame(d);
+    if (rc)
+      return rc;
+  }
+  return MOPCUDA_OK;
+}
+
+extern "C" int mopcuda_frame_end(MopCudaDevice *d, MopCudaFramebuffer *fb) {
+  if (!d || !fb)
+    return fail(MOPCUDA_EINVAL, "frame_end: bad arguments");
+  std::lock_guard<std::mutex> lk(d->mu);
+  if (!d->frame_open || d->fb != fb)
+    return fail(MOPCUDA_EINVAL, "frame_end without frame_begin");
+  d->frame_open = false;
+  cudaSetDevice(d->ordinal);
+  int rc = launch_frame(d);
+  if (rc)
+    return rc;
+  if (d->unsupported_draws)
+    return fail(MOPCUDA_EUNSUPPORTED, "%u draw(s) outside the order-independent path were skipped",
+                d->unsupported_draws);
+  return MOPCUDA_OK;
+}
+
+extern "C" int mopcuda_frame_wait(MopCudaDevice *d, int timeout_ms) {
+  if (!d)
+    return fail(MOPCUDA_EINVAL, "frame_wait: no device");
+  std::lock_guard<std::mutex> lk(d->mu);
+  cudaSetDevice(d->ordinal);
+  return finish_frame(d, timeout_ms);
+}
+
+extern "C" float mopcuda_frame_gpu_time_ms(MopCudaDevice *d) { return d ? d->last_ms : 0.0f; }
+
+/* ------------------------------------------------------------------------
+ * readbacks
+ * ------------------------------------------------------------------------ */
+static int ready(MopCudaDevice *d, MopCudaFramebuffer *fb) {
+  if (!d || !fb)
+    return fail(MOPCUDA_EINVAL, "readback: bad arguments");
+  cudaSetDevice(d->ordinal);
+  if (d->fb == fb && d->pending)
+    return finish_frame(d, FRAME_TIMEOUT_MS);
+  return MOPCUDA_OK;
+}
+
+static int fetch(MopCudaDevice *d, DevArena &src, HostArena &dst, size_t bytes, bool &valid) {
+  if (valid)
+    return MOPCUDA_OK;
+  CU_TRY(cudaMemcpyAsync(dst.p, src.p, bytes, cudaMemcpyDeviceToHost, d->stream));
+  int rc = stream_sync(d, FRAME_TIMEOUT_MS);
+  if (rc)
+    return rc;
+  valid = true;
+  return MOPCUDA_OK;
+}
+
+extern "C" const uint8_t *mopcuda_read_color(MopCudaDevice *d, MopCudaFramebuffer *fb, int *w,
+                                             int *h) {
+  if (!d || !fb)
+    return nullptr;
+  std::lock_guard<std::mutex> lk(d->mu);
+  if (ready(d, fb) || fetch(d, fb->out, fb->h_color, (size_t)fb->w * fb->h * 4, fb->host_color))
+    return nullptr;
+  if (w)
+    *w = fb->w;
+  if (h)
+    *h = fb->h;
+  return fb->h_color.as<uint8_t>();
+}
+
+extern "C" const uint32_t *mopcuda_read_object_id(MopCudaDevice *d, MopCudaFramebuffer *fb, int *w,
+                                                  int *h) {
+  if (!d || !fb)
+    return nullptr;
+  std::lock_guard<std::mutex> lk(d->mu);
+  if (ready(d, fb) || fetch(d, fb->ids, fb->h_ids, (size_t)fb->w * fb->h * 4, fb->host_ids))
+    return nullptr;
+  if (w)
+    *w = fb->w;
+  if (h)
+    *h = fb->h;
+  return fb->h_ids.as<uint32_t>();
+}
+
+extern "C" const float *mopcuda_read_depth(MopCudaDevice *d, MopCudaFramebuffer *fb, int *w,
+                                           int *h) {
+  if (!d || !fb)
+    return nullptr;
+  std::lock_guard<std::mutex> lk(d->mu);
+  if (ready(d, fb) || fetch(d, fb->depth, fb->h_depth, (size_t)fb->w * fb->h * 4, fb->host_depth))
+    return nullptr;
+  if (w)
+    *w = fb->w;
+  if (h)
+    *h = fb->h;
+  return fb->h_depth.as<float>();
+}
+
+extern "C" int mopcuda_read_color_resolved(MopCudaDevice *d, MopCudaFramebuffer *fb, int sf,
+                                           uint8_t *out, size_t out_size) {
+  if (!d || !fb || !out || sf <= 0 || fb->w % sf || fb->h % sf)
+    return fail(MOPCUDA_EINVAL, "read_color_resolved: bad arguments");
+  std::lock_guard<std::mutex> lk(d->mu);
+  int rc = ready(d, fb);
+  if (rc)
+    return rc;
+  size_t need = (size_t)(fb->w / sf) * (size_t)(fb->h / sf) * 4;
+  if (out_size < need)
+    return fail(MOPCUDA_EINVAL, "read_color_resolved: buffer too small");
+  const void *src = fb->out.p;
+  if (sf > 1) {
+    if (!(fb->presented_valid && fb->ssaa == sf)) {
+      d->launches += (uint64_t)mopcuda_launch_box(fb->out.as<uchar4>(), fb->w, fb->h, sf,
+                                                  fb->presented.as<uchar4>(), d->stream);
+      CU_TRY(cudaGetLastError());
+    }
+    src = fb->presented.p;
+  }
+  CU_TRY(cudaMemcpyAsync(out, src, need, cudaMemcpyDeviceToHost, d->stream));
+  return stream_sync(d, FRAME_TIMEOUT_MS);
+}
+
+/* Presentation factor of a framebuffer: lets frame_end fuse the SSAA box
+ * into the post pass (the viewport allocates W*ssaa x H*ssaa samples). */
+extern "C" int mopcuda_framebuffer_set_ssaa(MopCudaFramebuffer *fb, int sf) {
+  if (!fb || sf <= 0)
+    return fail(MOPCUDA_EINVAL, "framebuffer_set_ssaa: bad arguments");
+  fb->ssaa = sf;
+  return MOPCUDA_OK;
+}
+
+static int pick_one(MopCudaDevice *d, MopCudaFramebuffer *fb, int x, int y, uint32_t *id,
+                    float *dep) {
+  *id = 0;
+  *dep = 1.0f;
+  if (x < 0 || x >= fb->w || y < 0 || y >= fb->h)
+    return MOPCUDA_OK;
+  int rc = ready(d, fb);
+  if (rc)
+    return rc;
+  size_t i = (size_t)y * (size_t)fb->w + (size_t)x;
+  if (fb->host_ids)
+    *id = fb->h_ids.as<uint32_t>()[i];
+  else
+    CU_TRY(cudaMemcpy(id, fb->ids.as<uint32_t>() + i, 4, cudaMemcpyDeviceToHost));
+  if (fb->host_depth)
+    *dep = fb->h_depth.as<float>()[i];
+  else
+    CU_TRY(cudaMemcpy(dep, fb->depth.as<float>() + i, 4, cudaMemcpyDeviceToHost));
+  return MOPCUDA_OK;
+}
+
+extern "C" uint32_t mopcuda_pick_read_id(MopCudaDevice *d, MopCudaFramebuffer *fb, int x, int y) {
+  if (!d || !fb)
+    return 0;
+  std::lock_guard<std::mutex> lk(d->mu);
+  uint32_t id;
+  float dp;
+  return pick_one(d, fb, x, y, &id, &dp) ? 0u : id;
+}
+
+extern "C" float mopcuda_pick_read_depth(MopCudaDevice *d, MopCudaFramebuffer *fb, int x, int y) {
+  if (!d || !fb)
+    return 1.0f;
+  std::lock_guard<std::mutex> lk(d->mu);
+  uint32_t id;
+  float dp;
+  return pick_one(d, fb, x, y, &id, &dp) ? 1.0f : dp;
+}
+
+extern "C" int mopcuda_pick_batch(MopCudaDevice *d, MopCudaFramebuffer *fb, int sf,
+                                  const int32_t *xy, uint32_t n, uint32_t *ids, float *depths,
+                                  int32_t *hits) {
+  if (!d || !fb || sf <= 0 || (n && (!xy || !ids || !depths || !hits)))
+    return fail(MOPCUDA_EINVAL, "pick_batch: bad arguments");
+  if (n == 0)
+    return MOPCUDA_OK;
+  std::lock_guard<std::mutex> lk(d->mu);
+  int rc = ready(d, fb);
+  if (rc)
+    return rc;
+  size_t in_b = 8ull * n, out_b = 12ull * n;
+  if (d->pick_xy.ensure(in_b) || d->pick_out.ensure(out_b) || d->h_pick.ensure(in_b + out_b))
+    return MOPCUDA_ENOMEM;
+  memcpy(d->h_pick.p, xy, in_b);
+  cudaStream_t s = d->stream;
+  CU_TRY(cudaMemcpyAsync(d->pick_xy.p, d->h_pick.p, in_b, cudaMemcpyHostToDevice, s));
+  uint32_t *oid = d->pick_out.as<uint32_t>();
+  float *odp = (float *)(oid + n);
+  int32_t *oht = (int32_t *)(odp + n);
+  d->launches += (uint64_t)mopcuda_launch_pick(fb->ids.as<uint32_t>(), fb->depth.as<float>(), fb->w,
+                                               fb->h, sf, d->pick_xy.as<int2>(), n, oid, odp, oht, s);
+  CU_TRY(cudaGetLastError());
+  uint8_t *hb = d->h_pick.as<uint8_t>() + in_b;
+  CU_TRY(cudaMemcpyAsync(hb, d->pick_out.p, out_b, cudaMemcpyDeviceToHost, s));
+  rc = stream_sync(d, FRAME_TIMEOUT_MS);
+  if (rc)
+    return rc;
+  memcpy(ids, hb, 4ull * n);
+  memcpy(depths, hb + 4ull * n, 4ull * n);
+  memcpy(hits, hb + 8ull * n, 4ull * n);
+  return MOPCUDA_OK;
+}

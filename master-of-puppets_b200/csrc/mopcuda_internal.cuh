@@ -1,0 +1,198 @@
+/*
+ * mopcuda_internal.cuh — device records and exact-arithmetic helpers.
+ *
+ * All kernels are compiled with -fmad=false -prec-div=true -prec-sqrt=true
+ * -ftz=false: every float expression below is evaluated as the sequence of
+ * IEEE single-precision round-to-nearest operations written, in the same
+ * order as the reference CPU rasteriser (ISO C11, scalar SSE2, no
+ * contraction).  That is what makes depth, coverage and object IDs
+ * bit-exact and colour bit-exact except where a transcendental (atan2f,
+ * asinf in the IBL lookups) differs between CUDA and glibc.
+ */
+#ifndef MOPCUDA_INTERNAL_CUH
+#define MOPCUDA_INTERNAL_CUH
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "fold.h"
+
+/* ------------------------------------------------------------------------
+ * frame records
+ * ------------------------------------------------------------------------ */
+
+enum DrawFlags : uint32_t {
+  DF_SMOOTH = 1u << 0,
+  DF_CULL = 1u << 1,
+  DF_LIT = 1u << 2,     /* light list present: _full entry (rasterizer.c:2458) */
+  DF_TEXTURED = 1u << 3,
+  DF_FLEX = 1u << 4,    /* flexible vertex layout                              */
+};
+
+/* One recorded draw, uploaded per frame (the MopRhiDrawCall fields the path
+ * reads, plus where its vertices/triangles land in the frame arrays). */
+struct DrawRec {
+  float mvp[16];
+  float model[16];
+  float light_dir[3];
+  float ambient;
+  float opacity;
+  float metallic;
+  float roughness;
+  float depth_bias;
+  float cam_eye[3];
+  uint32_t object_id;
+  const uint8_t *vbuf;     /* device vertex bytes                        */
+  const uint32_t *ibuf;    /* device indices                             */
+  const uint8_t *tex;      /* device RGBA8 or null                       */
+  int32_t tex_w, tex_h;
+  uint32_t vertex_count, index_count;
+  uint32_t vbase;          /* first slot in the frame vertex arrays      */
+  uint32_t tbase;          /* first global triangle index                */
+  uint32_t light_off, light_count;
+  uint32_t flags;
+  uint32_t stride;
+  int16_t off_pos, off_nrm, off_col, off_uv; /* -1 = absent             */
+  int8_t n_pos, n_nrm, n_col, n_uv;          /* component counts         */
+};
+
+struct LightRec {
+  int32_t type;
+  float position[3];
+  float direction[3];
+  float color[4];
+  float intensity;
+  float range;
+  float spot_inner_cos;
+  float spot_outer_cos;
+  int32_t active;
+};
+
+/* Per fan-triangle raster record, 64 bytes. */
+struct __align__(16) RasterRec {
+  float w0[3];      /* edge values at the clamped bbox corner (x0+.5, y0+.5) */
+  float dx[3];      /* per-pixel increments                                  */
+  float dy[3];      /* per-row increments                                    */
+  float zc[3];      /* smooth: sz0..2 ; flat: z_row0, z_dx, z_dy             */
+  float inv_area;
+  uint32_t order;   /* (triangle << ORDER_FAN_BITS) | fan: submission order  */
+  uint16_t x0, y0, x1, y1; /* inclusive clamped bbox; y1 bit 15 = flat       */
+};
+
+#define ORDER_FAN_BITS 5
+#define REC_FLAT_BIT 0x8000u
+#define REC_DEAD 0xffffffffu
+
+/* Per fan-triangle shading record, 16 bytes. */
+struct __align__(16) ShadeRec {
+  union {
+    uint32_t v[3];  /* smooth: frame vertex slots of the fan vertices        */
+    float col[3];   /* flat: constant colour                                 */
+  };
+  uint32_t draw;
+};
+
+/* Frame counters and error flags, zeroed at frame start. */
+struct Counters {
+  uint32_t rec_count;
+  uint32_t extra_vertices;
+  uint32_t clip_count;
+  uint32_t bin_total;
+  uint32_t tile_cursor;
+  uint32_t overflow;     /* bit0 records, bit1 extra vertices, bit2 clip queue, bit3 bins */
+  uint32_t bin_fill_total;
+  uint32_t pad;
+};
+
+struct FrameArgs {
+  const DrawRec *draws;
+  uint32_t draw_count;
+  const LightRec *lights;
+  uint32_t total_vertices;
+  uint32_t total_tris;
+  /* vertex streams (total_vertices + extra capacity) */
+  float4 *clip;
+  float4 *world;
+  float4 *normal;
+  float4 *color;
+  uint32_t vertex_cap;
+  /* triangle -> first record */
+  uint32_t *rec_base;
+  RasterRec *rrec;
+  ShadeRec *srec;
+  uint32_t rec_cap;
+  uint32_t *clipq;
+  uint32_t clip_cap;
+  /* binning */
+  int width, height;      /* sample resolution */
+  int tile_shift;         /* log2 tile size */
+  int tiles_x, tiles_y;
+  uint32_t *tile_count;
+  uint32_t *tile_off;
+  uint32_t *tile_fill;
+  uint32_t *bins;
+  uint32_t bin_cap;
+  Counters *ctr;
+  /* resolve */
+  float clear[4];
+  float exposure;
+  /* IBL */
+  const float *irr;
+  int irr_w, irr_h;
+  const float *pf;
+  int pf_w, pf_h, pf_levels;
+  const float *brdf;
+  int brdf_size;
+  float ibl_rotation, ibl_intensity;
+  /* outputs */
+  uchar4 *pre;     /* resolved RGBA8 before post effects */
+  float *depth;
+  uint32_t *ids;
+};
+
+struct PostArgs {
+  const uchar4 *pre;
+  uchar4 *out;        /* sample-res after post */
+  uchar4 *presented;  /* (w/ssaa) x (h/ssaa) or null */
+  int width, height, ssaa;
+  uint32_t effects;
+  float lut[256];     /* per-byte value after tonemap/gamma */
+};
+
+/* ------------------------------------------------------------------------
+ * exact helpers
+ * ------------------------------------------------------------------------ */
+
+/* float -> int as the x86-64 reference build converts (cvttss2si):
+ * truncation, and INT_MIN for NaN or out-of-range values. */
+__device__ __forceinline__ int x86_f2i(float f) {
+  if (!(f >= -2147483648.0f && f < 2147483648.0f))
+    return (int)0x80000000;
+  return (int)f;
+}
+
+/* float -> uint8_t through int32 truncation, keeping the low byte. */
+__device__ __forceinline__ uint8_t x86_f2u8(float f) { return (uint8_t)(uint32_t)x86_f2i(f); }
+
+/* Order-preserving map of a depth value to 32 bits; -0 and +0 share a key
+ * (they compare equal under the reference's strict `<` test). */
+__device__ __forceinline__ uint32_t depth_key(float z) {
+  uint32_t b = __float_as_uint(z);
+  if ((b & 0x7fffffffu) == 0u)
+    b = 0u;
+  return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
+}
+
+#define KEY_EMPTY 0xffffffffffffffffull
+
+/* launchers (kernels.cu); each returns the number of kernels it launched */
+int mopcuda_launch_frame(const FrameArgs &a, const PostArgs &p, int tile_size, int grid_tiles,
+                         cudaStream_t s);
+int mopcuda_launch_box(const uchar4 *src, int width, int height, int sf, uchar4 *dst,
+                       cudaStream_t s);
+int mopcuda_launch_pick(const uint32_t *ids, const float *depth, int width, int height, int sf,
+                        const int2 *xy, uint32_t n, uint32_t *out_id, float *out_depth,
+                        int32_t *out_hit, cudaStream_t s);
+int mopcuda_tile_occupancy(int tile_size);
+
+#endif

@@ -1,0 +1,338 @@
+"""ctypes binding of the CUDA backend's C ABI (include/mop_cuda.h).
+
+This is the host-side mirror of the reference's viewport/RHI usage for the
+frame path: a ``SceneRenderer`` uploads a scene once (mop_viewport_add_mesh ->
+buffer_create, mop_viewport_create_texture -> texture_create), then each frame
+issues frame_begin / one draw per mesh (EMIT_DRAW, reference
+src/core/viewport.c:2015-2088) / frame_end, and reads back colour, depth,
+object IDs and picks.  All arithmetic runs in libmopcuda.so; there is no
+Python or CPU fallback — if the native library or a GPU is missing, this
+module raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB_PATH = HERE / "libmopcuda.so"
+
+OK, EINVAL, ENOMEM, ECUDA, ETIMEOUT, EUNSUPPORTED = 0, -1, -2, -3, -4, -5
+POST_GAMMA, POST_TONEMAP, POST_VIGNETTE, POST_FXAA = 1, 2, 4, 16
+DEFAULT_LIGHT_DIR = (0.3, 1.0, 0.5)  # viewport default light_dir (viewport.c:641)
+
+
+class MopCudaLight(C.Structure):
+    _fields_ = [("type", C.c_int32), ("position", C.c_float * 3), ("direction", C.c_float * 3),
+                ("color", C.c_float * 4), ("intensity", C.c_float), ("range", C.c_float),
+                ("spot_inner_cos", C.c_float), ("spot_outer_cos", C.c_float),
+                ("active", C.c_int32)]
+
+
+class MopCudaVertexLayout(C.Structure):
+    _fields_ = [("stride", C.c_uint32), ("position_offset", C.c_int32),
+                ("position_components", C.c_int32), ("normal_offset", C.c_int32),
+                ("normal_components", C.c_int32), ("color_offset", C.c_int32),
+                ("color_components", C.c_int32), ("uv_offset", C.c_int32),
+                ("uv_components", C.c_int32)]
+
+
+class MopCudaDraw(C.Structure):
+    _fields_ = [("vertex_buffer", C.c_void_p), ("index_buffer", C.c_void_p),
+                ("vertex_count", C.c_uint32), ("index_count", C.c_uint32),
+                ("object_id", C.c_uint32), ("model", C.c_float * 16), ("mvp", C.c_float * 16),
+                ("light_dir", C.c_float * 3), ("ambient", C.c_float), ("opacity", C.c_float),
+                ("metallic", C.c_float), ("roughness", C.c_float), ("depth_bias", C.c_float),
+                ("cam_eye", C.c_float * 3), ("smooth", C.c_int32), ("wireframe", C.c_int32),
+                ("depth_test", C.c_int32), ("depth_write", C.c_int32),
+                ("backface_cull", C.c_int32), ("blend_mode", C.c_int32),
+                ("texture", C.c_void_p), ("lights", C.POINTER(MopCudaLight)),
+                ("light_count", C.c_uint32), ("layout", C.POINTER(MopCudaVertexLayout))]
+
+
+# (name, restype, argtypes) for every entry point of include/mop_cuda.h
+_P = C.c_void_p
+SIGNATURES = [
+    ("mopcuda_device_create", _P, [C.c_int]),
+    ("mopcuda_device_destroy", None, [_P]),
+    ("mopcuda_last_error", C.c_char_p, []),
+    ("mopcuda_launch_count", C.c_uint64, [_P]),
+    ("mopcuda_buffer_create", _P, [_P, _P, C.c_size_t]),
+    ("mopcuda_buffer_destroy", None, [_P, _P]),
+    ("mopcuda_buffer_update", C.c_int, [_P, _P, _P, C.c_size_t, C.c_size_t]),
+    ("mopcuda_buffer_read", _P, [_P]),
+    ("mopcuda_buffer_size", C.c_size_t, [_P]),
+    ("mopcuda_texture_create", _P, [_P, C.c_int, C.c_int, _P]),
+    ("mopcuda_texture_create_hdr", _P, [_P, C.c_int, C.c_int, _P]),
+    ("mopcuda_texture_destroy", None, [_P, _P]),
+    ("mopcuda_texture_read_rgba8", C.c_int, [_P, _P, _P, C.c_size_t]),
+    ("mopcuda_framebuffer_create", _P, [_P, C.c_int, C.c_int]),
+    ("mopcuda_framebuffer_destroy", None, [_P, _P]),
+    ("mopcuda_framebuffer_resize", C.c_int, [_P, _P, C.c_int, C.c_int]),
+    ("mopcuda_framebuffer_set_ssaa", C.c_int, [_P, C.c_int]),
+    ("mopcuda_set_exposure", None, [_P, C.c_float]),
+    ("mopcuda_set_post_effects", None, [_P, C.c_uint32]),
+    ("mopcuda_set_ibl", C.c_int, [_P, _P, C.c_int, C.c_int, _P, C.c_int, C.c_int, C.c_int, _P,
+                                  C.c_int, C.c_float, C.c_float]),
+    ("mopcuda_frame_begin", C.c_int, [_P, _P, _P]),
+    ("mopcuda_draw", C.c_int, [_P, _P, C.POINTER(MopCudaDraw)]),
+    ("mopcuda_draw_instanced", C.c_int, [_P, _P, C.POINTER(MopCudaDraw), _P, _P, _P, C.c_uint32]),
+    ("mopcuda_frame_end", C.c_int, [_P, _P]),
+    ("mopcuda_frame_wait", C.c_int, [_P, C.c_int]),
+    ("mopcuda_frame_gpu_time_ms", C.c_float, [_P]),
+    ("mopcuda_read_color", _P, [_P, _P, _P, _P]),
+    ("mopcuda_read_object_id", _P, [_P, _P, _P, _P]),
+    ("mopcuda_read_depth", _P, [_P, _P, _P, _P]),
+    ("mopcuda_read_color_resolved", C.c_int, [_P, _P, C.c_int, _P, C.c_size_t]),
+    ("mopcuda_pick_read_id", C.c_uint32, [_P, _P, C.c_int, C.c_int]),
+    ("mopcuda_pick_read_depth", C.c_float, [_P, _P, C.c_int, C.c_int]),
+    ("mopcuda_pick_batch", C.c_int, [_P, _P, C.c_int, _P, C.c_uint32, _P, _P, _P]),
+    ("mopcuda_mat4_multiply", None, [_P, _P, _P]),
+    ("mopcuda_mat4_compose_trs", None, [_P, _P, _P, _P]),
+    ("mopcuda_camera_matrices", None, [_P, _P, _P, C.c_float, C.c_float, C.c_float, C.c_int,
+                                       C.c_int, _P, _P, _P]),
+]
+
+_lib = None
+
+
+def lib():
+    """Load libmopcuda.so (built in-tree by __graft_entry__.build / make)."""
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise RuntimeError(f"CUDA backend library missing: {LIB_PATH} (run the build)")
+        L = C.CDLL(str(LIB_PATH))
+        for name, res, args in SIGNATURES:
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def last_error() -> str:
+    return lib().mopcuda_last_error().decode(errors="replace")
+
+
+class MopCudaError(RuntimeError):
+    def __init__(self, code, what):
+        super().__init__(f"{what} failed ({code}): {last_error()}")
+        self.code = code
+
+
+def _check(rc, what):
+    if rc != OK:
+        raise MopCudaError(rc, what)
+    return rc
+
+
+def _f32(a):
+    return np.ascontiguousarray(a, np.float32)
+
+
+# --------------------------------------------------------------------------
+# host matrices (run in libmopcuda.so host code)
+# --------------------------------------------------------------------------
+
+def mat4_multiply(a, b):
+    a, b = _f32(a), _f32(b)
+    out = np.zeros(16, np.float32)
+    lib().mopcuda_mat4_multiply(a.ctypes.data, b.ctypes.data, out.ctypes.data)
+    return out
+
+
+def camera_matrices(scene):
+    view = np.zeros(16, np.float32)
+    proj = np.zeros(16, np.float32)
+    eye = np.zeros(3, np.float32)
+    e, t, u = _f32(scene.eye), _f32(scene.target), _f32(scene.up)
+    lib().mopcuda_camera_matrices(e.ctypes.data, t.ctypes.data, u.ctypes.data, scene.fov_deg,
+                                  scene.near, scene.far, scene.width, scene.height,
+                                  view.ctypes.data, proj.ctypes.data, eye.ctypes.data)
+    return view, proj, eye
+
+
+def light_struct(l) -> MopCudaLight:
+    s = MopCudaLight()
+    s.type = l.type
+    s.position[:] = l.position
+    s.direction[:] = l.direction
+    s.color[:] = l.color
+    s.intensity = l.intensity
+    s.range = l.range
+    s.spot_inner_cos = l.spot_inner_cos
+    s.spot_outer_cos = l.spot_outer_cos
+    s.active = 1 if l.active else 0
+    return s
+
+
+class Device:
+    def __init__(self, ordinal: int = 0):
+        self.L = lib()
+        self.h = self.L.mopcuda_device_create(ordinal)
+        if not self.h:
+            raise RuntimeError(f"mopcuda_device_create({ordinal}) failed: {last_error()}")
+
+    @property
+    def launches(self) -> int:
+        return int(self.L.mopcuda_launch_count(self.h))
+
+    def close(self):
+        if self.h:
+            self.L.mopcuda_device_destroy(self.h)
+            self.h = None
+
+
+class SceneRenderer:
+    """Scene resident on one device; renders frames through the C ABI."""
+
+    def __init__(self, device: Device, scene, ibl=None):
+        self.dev = device
+        self.scene = scene
+        L = device.L
+        d = device.h
+        self.L = L
+        self._buffers = []
+        self.meshes = []
+        for m in scene.meshes:
+            v = _f32(m.vertices)
+            i = np.ascontiguousarray(m.indices, np.uint32)
+            vb = L.mopcuda_buffer_create(d, v.ctypes.data, v.nbytes)
+            ib = L.mopcuda_buffer_create(d, i.ctypes.data, i.nbytes)
+            if not vb or not ib:
+                raise RuntimeError(f"buffer_create failed: {last_error()}")
+            self._buffers += [vb, ib]
+            self.meshes.append((m, vb, ib, v.shape[0], i.size))
+        self.textures = []
+        for t in scene.textures:
+            t = np.ascontiguousarray(t, np.uint8)
+            th = L.mopcuda_texture_create(d, t.shape[1], t.shape[0], t.ctypes.data)
+            if not th:
+                raise RuntimeError(f"texture_create failed: {last_error()}")
+            self.textures.append(th)
+        self.sw, self.sh = scene.width * scene.ssaa, scene.height * scene.ssaa
+        self.fb = L.mopcuda_framebuffer_create(d, self.sw, self.sh)
+        if not self.fb:
+            raise RuntimeError(f"framebuffer_create failed: {last_error()}")
+        _check(L.mopcuda_framebuffer_set_ssaa(self.fb, scene.ssaa), "framebuffer_set_ssaa")
+        L.mopcuda_set_exposure(d, scene.exposure)
+        L.mopcuda_set_post_effects(d, scene.post_effects)
+        if ibl is not None:
+            self.set_ibl(ibl)
+        else:
+            _check(L.mopcuda_set_ibl(d, None, 0, 0, None, 0, 0, 0, None, 0, 0.0, 1.0), "set_ibl")
+        self.lights = (MopCudaLight * max(1, len(scene.lights)))()
+        for k, l in enumerate(scene.lights):
+            self.lights[k] = light_struct(l)
+        self.update_camera()
+        self.clear = (C.c_float * 4)(*scene.clear)
+
+    def set_ibl(self, ibl):
+        self._ibl = [_f32(ibl["irr"]), _f32(ibl["pf"]), _f32(ibl["brdf"])]
+        irr, pf, brdf = self._ibl
+        _check(self.L.mopcuda_set_ibl(self.dev.h, irr.ctypes.data, ibl["irr_w"], ibl["irr_h"],
+                                      pf.ctypes.data, ibl["pf_w"], ibl["pf_h"], ibl["pf_levels"],
+                                      brdf.ctypes.data, ibl["brdf_size"], ibl["rotation"],
+                                      ibl["intensity"]), "set_ibl")
+
+    def update_camera(self):
+        sc = self.scene
+        self.view, self.proj, self.eye = camera_matrices(sc)
+        amb = min(max(sc.ambient, 0.0), 1.0)
+        self.draws = []
+        for (m, vb, ib, vc, ic) in self.meshes:
+            dr = MopCudaDraw()
+            dr.vertex_buffer, dr.index_buffer = vb, ib
+            dr.vertex_count, dr.index_count = vc, ic
+            dr.object_id = m.object_id
+            dr.model[:] = [float(x) for x in m.transform]
+            dr.mvp[:] = [float(x) for x in mat4_multiply(self.proj, mat4_multiply(self.view, m.transform))]
+            dr.light_dir[:] = DEFAULT_LIGHT_DIR
+            dr.ambient = amb
+            dr.opacity = m.opacity
+            dr.metallic = m.metallic if m.has_material else 0.0
+            dr.roughness = m.roughness if m.has_material else 0.5
+            dr.depth_bias = 0.0
+            dr.cam_eye[:] = [float(x) for x in self.eye]
+            dr.smooth = 1 if getattr(sc, "smooth", True) else 0
+            dr.wireframe = 0
+            dr.depth_test = dr.depth_write = dr.backface_cull = 1
+            dr.blend_mode = 0
+            dr.texture = self.textures[m.texture] if m.texture >= 0 else None
+            dr.lights = self.lights
+            dr.light_count = len(sc.lights)
+            dr.layout = None
+            self.draws.append(dr)
+
+    def submit(self):
+        """Record and launch one frame (asynchronous)."""
+        L, d, fb = self.L, self.dev.h, self.fb
+        _check(L.mopcuda_frame_begin(d, fb, self.clear), "frame_begin")
+        for dr in self.draws:
+            _check(L.mopcuda_draw(d, fb, C.byref(dr)), "draw")
+        _check(L.mopcuda_frame_end(d, fb), "frame_end")
+
+    def wait(self, timeout_ms: int = 20000):
+        _check(self.L.mopcuda_frame_wait(self.dev.h, timeout_ms), "frame_wait")
+
+    def render(self):
+        self.submit()
+        self.wait()
+        return self
+
+    @property
+    def gpu_ms(self) -> float:
+        return float(self.L.mopcuda_frame_gpu_time_ms(self.dev.h))
+
+    def _view(self, p, dtype, shape):
+        if not p:
+            raise RuntimeError(f"readback failed: {last_error()}")
+        n = int(np.prod(shape))
+        return np.ctypeslib.as_array(C.cast(p, C.POINTER(dtype)), shape=(n,)).reshape(shape).copy()
+
+    def color_full(self):
+        return self._view(self.L.mopcuda_read_color(self.dev.h, self.fb, None, None), C.c_uint8,
+                          (self.sh, self.sw, 4))
+
+    def depth(self):
+        return self._view(self.L.mopcuda_read_depth(self.dev.h, self.fb, None, None), C.c_float,
+                          (self.sh, self.sw))
+
+    def object_id(self):
+        return self._view(self.L.mopcuda_read_object_id(self.dev.h, self.fb, None, None),
+                          C.c_uint32, (self.sh, self.sw))
+
+    def color(self, out=None):
+        sc = self.scene
+        if out is None:
+            out = np.zeros((sc.height, sc.width, 4), np.uint8)
+        _check(self.L.mopcuda_read_color_resolved(self.dev.h, self.fb, sc.ssaa, out.ctypes.data,
+                                                  out.nbytes), "read_color_resolved")
+        return out
+
+    def pick(self, xy):
+        xy = np.ascontiguousarray(xy, np.int32)
+        n = xy.shape[0]
+        ids = np.zeros(n, np.uint32)
+        dep = np.zeros(n, np.float32)
+        hits = np.zeros(n, np.int32)
+        _check(self.L.mopcuda_pick_batch(self.dev.h, self.fb, self.scene.ssaa, xy.ctypes.data, n,
+                                         ids.ctypes.data, dep.ctypes.data, hits.ctypes.data),
+               "pick_batch")
+        return ids, dep, hits
+
+    def close(self):
+        L, d = self.L, self.dev.h
+        if not d:
+            return
+        for b in self._buffers:
+            L.mopcuda_buffer_destroy(d, b)
+        for t in self.textures:
+            L.mopcuda_texture_destroy(d, t)
+        if self.fb:
+            L.mopcuda_framebuffer_destroy(d, self.fb)
+        self._buffers, self.textures, self.fb = [], [], None

@@ -376,6 +376,37 @@ def small_scene(seed: int = 7, width: int = 160, height: int = 120, ssaa: int = 
     return sc
 
 
+def _quad(x0, y0, x1, y1, z, color, tilt=0.0):
+    pos = np.array([[x0, y0, z + tilt * x0], [x1, y0, z + tilt * x1], [x1, y1, z + tilt * x1],
+                    [x0, y1, z + tilt * x0]], np.float32)
+    n = np.array([-tilt, 0.0, 1.0])
+    n = n / np.linalg.norm(n)
+    nrm = np.tile(n.astype(np.float32), (4, 1))
+    col = np.tile(np.asarray(color, np.float32), (4, 1))
+    uv = np.array([[0, 0], [1, 0], [1, 1], [0, 1]], np.float32)
+    return _pack(pos, nrm, col, uv), np.array([0, 1, 2, 0, 2, 3], np.uint32)
+
+
+def coplanar_scene(seed: int = 3, width: int = 192, height: int = 144) -> Scene:
+    """Overlapping quads on shared planes with distinct object IDs: exact
+    depth ties must resolve to the earliest draw (strict `<` test,
+    reference rasterizer.c:1960), rounding differences to the nearer."""
+    rng = np.random.default_rng(seed)
+    sc = Scene("coplanar", width, height, 1, eye=(0.0, 0.0, 5.0), target=(0.0, 0.0, 0.0),
+               fov_deg=50.0, near=0.1, far=50.0)
+    sc.lights.append(Light(LIGHT_DIRECTIONAL, direction=(-0.2, -0.3, -1.0), intensity=2.0))
+    oid = 1
+    for plane_z, tilt in ((0.0, 0.0), (-0.5, 0.35)):
+        for _ in range(5):
+            x0, y0 = rng.uniform(-2.2, 0.2, 2)
+            x1, y1 = x0 + rng.uniform(1.0, 2.5), y0 + rng.uniform(1.0, 2.5)
+            v, i = _quad(float(x0), float(y0), float(x1), float(y1), plane_z, _color(rng), tilt)
+            m, r = _mat_rand(rng)
+            sc.meshes.append(Mesh(v, i, oid, mat_identity(), m, r))
+            oid += 1
+    return sc
+
+
 def pick_points(scene: Scene, n: int = 1000, seed: int = 11) -> np.ndarray:
     rng = np.random.default_rng(seed)
     xy = np.empty((n, 2), np.int32)
