@@ -197,6 +197,21 @@ float mopcuda_pick_read_depth(MopCudaDevice *dev, MopCudaFramebuffer *fb, int x,
 int mopcuda_pick_batch(MopCudaDevice *dev, MopCudaFramebuffer *fb, int ssaa, const int32_t *xy,
                        uint32_t n, uint32_t *ids, float *depths, int32_t *hits);
 
+/* ---- measurement (no reference counterpart: the reference reports only
+ *      wall-clock MopFrameStats, include/mop/util/profile.h:51-81) ------- */
+/* Record CUDA events between the frame's stages on the device stream. */
+void mopcuda_set_stage_timing(MopCudaDevice *dev, int on);
+/* Stage durations of the last completed frame, ms: [0] vertex transform,
+ * [1] triangle setup + clipping, [2] binning, [3] tile visibility + shading
+ * + resolve, [4] post (FXAA, gamma, SSAA).  `ms` holds >= 5 floats. */
+int mopcuda_stage_times(MopCudaDevice *dev, float *ms, int n);
+/* Measured FP32 add/multiply issue rate without FMA, Gop/s: the roofline
+ * denominator of the shading stage. */
+int mopcuda_measure_fp32_peak(MopCudaDevice *dev, double *gops);
+/* Host->device and device->host bytes of the last frame launch itself (draw
+ * table + light records up; frame counters down), excluding readbacks. */
+int mopcuda_frame_io_bytes(MopCudaDevice *dev, uint64_t *h2d, uint64_t *d2h);
+
 /* ---- host-side matrices (the device receives finished matrices) ------- */
 /* out = a * b, column-major (mop_mat4_multiply, reference math.c:182-194). */
 void mopcuda_mat4_multiply(const float a[16], const float b[16], float out[16]);

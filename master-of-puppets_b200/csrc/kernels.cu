@@ -1268,33 +1268,71 @@ __global__ void k_pick(const uint32_t *ids, const float *depth, int width, int h
 static inline unsigned blocks_for(uint32_t n, unsigned bs) { return (n + bs - 1u) / bs; }
 
 int mopcuda_launch_frame(const FrameArgs &a, const PostArgs &p, int tile_size, int grid_tiles,
-                         cudaStream_t s) {
+                         cudaStream_t s, cudaEvent_t *ev) {
   int launches = 0;
+  if (ev)
+    cudaEventRecord(ev[0], s);
   if (a.total_vertices) {
     k_vertex<<<blocks_for(a.total_vertices, 256), 256, 0, s>>>(a);
     launches++;
   }
+  if (ev)
+    cudaEventRecord(ev[1], s);
   if (a.total_tris) {
     k_setup<<<blocks_for(a.total_tris, 256), 256, 0, s>>>(a);
     k_clip<<<blocks_for(a.clip_cap < 65536u ? a.clip_cap : 65536u, 128), 128, 0, s>>>(a);
     launches += 2;
   }
+  if (ev)
+    cudaEventRecord(ev[2], s);
   const uint32_t rec_grid = blocks_for(a.rec_cap < (1u << 22) ? a.rec_cap : (1u << 22), 256);
   k_bin_count<<<rec_grid, 256, 0, s>>>(a);
   k_bin_scan<<<1, 1024, 0, s>>>(a);
   k_bin_fill<<<rec_grid, 256, 0, s>>>(a);
   launches += 3;
+  if (ev)
+    cudaEventRecord(ev[3], s);
   if (tile_size == 8)
     k_tile<8><<<grid_tiles, 64, 0, s>>>(a);
   else
     k_tile<16><<<grid_tiles, 256, 0, s>>>(a);
   launches++;
+  if (ev)
+    cudaEventRecord(ev[4], s);
   const int sf = p.ssaa;
   dim3 pb(16, 16);
   dim3 pg(blocks_for((uint32_t)(p.width / sf), 16), blocks_for((uint32_t)(p.height / sf), 16));
   k_post<<<pg, pb, 0, s>>>(p);
   launches++;
+  if (ev)
+    cudaEventRecord(ev[5], s);
   return launches;
+}
+
+/* FP32 add/multiply issue peak without FMA: the denominator of the shading
+ * roofline (the frame path is compiled with -fmad=false).  Each thread runs
+ * 8 independent chains of alternating FMUL and FADD. */
+__global__ void k_fp32_peak(float *out, int iters, float a, float b) {
+  float x[8];
+  for (int k = 0; k < 8; k++)
+    x[k] = (float)(threadIdx.x + k) * 1e-3f;
+  for (int i = 0; i < iters; i++) {
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+      x[k] = __fmul_rn(x[k], a);
+      x[k] = __fadd_rn(x[k], b);
+    }
+  }
+  float s = 0.0f;
+  for (int k = 0; k < 8; k++)
+    s += x[k];
+  if (s == 123.456f)
+    out[blockIdx.x] = s;
+}
+
+int mopcuda_launch_fp32_peak(float *out, int blocks, int iters, cudaStream_t s) {
+  k_fp32_peak<<<blocks, 256, 0, s>>>(out, iters, 0.999999f, 1e-7f);
+  return 1;
 }
 
 int mopcuda_launch_box(const uchar4 *src, int width, int height, int sf, uchar4 *dst,

@@ -132,6 +132,9 @@ struct MopCudaDevice {
   int num_sms = 148;
   cudaStream_t stream = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  cudaEvent_t stage_ev[MOPCUDA_STAGES + 1] = {};
+  bool stage_timing = false;
+  float stage_ms[MOPCUDA_STAGES] = {};
   std::mutex mu;
   /* recorded frame */
   MopCudaFramebuffer *fb = nullptr;
@@ -161,6 +164,7 @@ struct MopCudaDevice {
   uint32_t extra_hint = 0, rec_hint = 0, clip_hint = 0, bin_hint = 0;
   uint64_t launches = 0;
   float last_ms = 0.0f;
+  uint64_t io_h2d = 0, io_d2h = 0; /* bytes moved by the last frame launch */
 };
 
 static int finish_frame(MopCudaDevice *d, int timeout_ms);
@@ -209,6 +213,8 @@ extern "C" MopCudaDevice *mopcuda_device_create(int ordinal) {
     delete d;
     return nullptr;
   }
+  for (int i = 0; i <= MOPCUDA_STAGES; i++)
+    cudaEventCreate(&d->stage_ev[i]);
   build_lut(d->lut, d->post);
   return d;
 }
@@ -258,6 +264,9 @@ extern "C" void mopcuda_device_destroy(MopCudaDevice *d) {
   d->h_pick.release();
   cudaEventDestroy(d->ev0);
   cudaEventDestroy(d->ev1);
+  for (int i = 0; i <= MOPCUDA_STAGES; i++)
+    if (d->stage_ev[i])
+      cudaEventDestroy(d->stage_ev[i]);
   cudaStreamDestroy(d->stream);
   delete d;
 }
@@ -828,7 +837,8 @@ static int launch_frame(MopCudaDevice *d) {
   int grid_tiles = d->num_sms * occ;
   if ((uint32_t)grid_tiles > ntiles)
     grid_tiles = (int)ntiles;
-  d->launches += (uint64_t)mopcuda_launch_frame(a, p, ts, grid_tiles, s);
+  d->launches += (uint64_t)mopcuda_launch_frame(a, p, ts, grid_tiles, s,
+                                                d->stage_timing ? d->stage_ev : nullptr);
   CU_TRY(cudaGetLastError());
   CU_TRY(cudaMemcpyAsync(d->h_counters.p, d->counters.p, sizeof(Counters), cudaMemcpyDeviceToHost,
                          s));
@@ -837,6 +847,16 @@ static int launch_frame(MopCudaDevice *d) {
   fb->presented_valid = sf > 1;
   fb->frame_serial++;
   d->pending = true;
+  d->io_h2d = sizeof(DrawRec) * (uint64_t)nd + sizeof(LightRec) * (uint64_t)d->lights.size();
+  d->io_d2h = sizeof(Counters);
+  return MOPCUDA_OK;
+}
+
+extern "C" int mopcuda_frame_io_bytes(MopCudaDevice *d, uint64_t *h2d, uint64_t *d2h) {
+  if (!d || !h2d || !d2h)
+    return fail(MOPCUDA_EINVAL, "frame_io_bytes: bad arguments");
+  *h2d = d->io_h2d;
+  *d2h = d->io_d2h;
   return MOPCUDA_OK;
 }
 
@@ -852,6 +872,9 @@ static int finish_frame(MopCudaDevice *d, int timeout_ms) {
     }
     d->pending = false;
     cudaEventElapsedTime(&d->last_ms, d->ev0, d->ev1);
+    if (d->stage_timing)
+      for (int i = 0; i < MOPCUDA_STAGES; i++)
+        cudaEventElapsedTime(&d->stage_ms[i], d->stage_ev[i], d->stage_ev[i + 1]);
     const Counters *c = d->h_counters.as<Counters>();
     if (!c->overflow)
       break;
@@ -1071,5 +1094,55 @@ extern "C" int mopcuda_pick_batch(MopCudaDevice *d, MopCudaFramebuffer *fb, int 
   memcpy(ids, hb, 4ull * n);
   memcpy(depths, hb + 4ull * n, 4ull * n);
   memcpy(hits, hb + 8ull * n, 4ull * n);
+  return MOPCUDA_OK;
+}
+
+/* ------------------------------------------------------------------------
+ * measurement helpers
+ * ------------------------------------------------------------------------ */
+extern "C" void mopcuda_set_stage_timing(MopCudaDevice *d, int on) {
+  if (d)
+    d->stage_timing = on != 0;
+}
+
+extern "C" int mopcuda_stage_times(MopCudaDevice *d, float *ms, int n) {
+  if (!d || !ms || n < MOPCUDA_STAGES)
+    return fail(MOPCUDA_EINVAL, "stage_times: need %d floats", MOPCUDA_STAGES);
+  for (int i = 0; i < MOPCUDA_STAGES; i++)
+    ms[i] = d->stage_ms[i];
+  return MOPCUDA_OK;
+}
+
+extern "C" int mopcuda_measure_fp32_peak(MopCudaDevice *d, double *gops) {
+  if (!d || !gops)
+    return fail(MOPCUDA_EINVAL, "measure_fp32_peak: bad arguments");
+  std::lock_guard<std::mutex> lk(d->mu);
+  cudaSetDevice(d->ordinal);
+  float *tmp = nullptr;
+  const int blocks = d->num_sms * 8, iters = 4096;
+  CU_TRY(cudaMalloc(&tmp, sizeof(float) * (size_t)blocks));
+  cudaEvent_t a, b;
+  cudaEventCreate(&a);
+  cudaEventCreate(&b);
+  double best = 0.0;
+  for (int rep = 0; rep < 6; rep++) {
+    cudaEventRecord(a, d->stream);
+    d->launches += (uint64_t)mopcuda_launch_fp32_peak(tmp, blocks, iters, d->stream);
+    cudaEventRecord(b, d->stream);
+    int rc = bounded_sync(d, b, FRAME_TIMEOUT_MS);
+    if (rc) {
+      cudaFree(tmp);
+      return rc;
+    }
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, a, b);
+    double ops = (double)blocks * 256.0 * (double)iters * 16.0;
+    if (rep > 0 && ms > 0.0f && ops / (ms * 1e6) > best)
+      best = ops / (ms * 1e6);
+  }
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  cudaFree(tmp);
+  *gops = best;
   return MOPCUDA_OK;
 }

@@ -186,8 +186,11 @@ __device__ __forceinline__ uint32_t depth_key(float z) {
 #define KEY_EMPTY 0xffffffffffffffffull
 
 /* launchers (kernels.cu); each returns the number of kernels it launched */
+/* ev (optional, 6 events): stage boundaries vertex|setup+clip|bin|tile|post */
 int mopcuda_launch_frame(const FrameArgs &a, const PostArgs &p, int tile_size, int grid_tiles,
-                         cudaStream_t s);
+                         cudaStream_t s, cudaEvent_t *ev);
+int mopcuda_launch_fp32_peak(float *out, int blocks, int iters, cudaStream_t s);
+#define MOPCUDA_STAGES 5
 int mopcuda_launch_box(const uchar4 *src, int width, int height, int sf, uchar4 *dst,
                        cudaStream_t s);
 int mopcuda_launch_pick(const uint32_t *ids, const float *depth, int width, int height, int sf,

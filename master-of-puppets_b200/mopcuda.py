@@ -90,6 +90,10 @@ SIGNATURES = [
     ("mopcuda_pick_read_id", C.c_uint32, [_P, _P, C.c_int, C.c_int]),
     ("mopcuda_pick_read_depth", C.c_float, [_P, _P, C.c_int, C.c_int]),
     ("mopcuda_pick_batch", C.c_int, [_P, _P, C.c_int, _P, C.c_uint32, _P, _P, _P]),
+    ("mopcuda_set_stage_timing", None, [_P, C.c_int]),
+    ("mopcuda_stage_times", C.c_int, [_P, _P, C.c_int]),
+    ("mopcuda_measure_fp32_peak", C.c_int, [_P, C.POINTER(C.c_double)]),
+    ("mopcuda_frame_io_bytes", C.c_int, [_P, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
     ("mopcuda_mat4_multiply", None, [_P, _P, _P]),
     ("mopcuda_mat4_compose_trs", None, [_P, _P, _P, _P]),
     ("mopcuda_camera_matrices", None, [_P, _P, _P, C.c_float, C.c_float, C.c_float, C.c_int,
@@ -180,6 +184,26 @@ class Device:
     @property
     def launches(self) -> int:
         return int(self.L.mopcuda_launch_count(self.h))
+
+    STAGES = ("vertex", "setup_clip", "bin", "tile_visibility_shade", "post")
+
+    def set_stage_timing(self, on: bool = True):
+        self.L.mopcuda_set_stage_timing(self.h, 1 if on else 0)
+
+    def stage_times(self):
+        ms = np.zeros(len(self.STAGES), np.float32)
+        _check(self.L.mopcuda_stage_times(self.h, ms.ctypes.data, ms.size), "stage_times")
+        return dict(zip(self.STAGES, [float(x) for x in ms]))
+
+    def frame_io_bytes(self):
+        h, d = C.c_uint64(), C.c_uint64()
+        _check(self.L.mopcuda_frame_io_bytes(self.h, C.byref(h), C.byref(d)), "frame_io_bytes")
+        return int(h.value), int(d.value)
+
+    def fp32_peak_gops(self) -> float:
+        g = C.c_double()
+        _check(self.L.mopcuda_measure_fp32_peak(self.h, C.byref(g)), "measure_fp32_peak")
+        return float(g.value)
 
     def close(self):
         if self.h:

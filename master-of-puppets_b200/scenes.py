@@ -407,6 +407,60 @@ def coplanar_scene(seed: int = 3, width: int = 192, height: int = 144) -> Scene:
     return sc
 
 
+def procedural_ibl(sun_dir=(0.4, 0.8, 0.35), irr_size=(64, 32), pf_size=(128, 64), levels=5,
+                   brdf_size=256, rotation=0.0, intensity=1.0) -> dict:
+    """Seedless procedural sky and derived IBL maps with the reference's map
+    sizes (irradiance 64x32, prefiltered 128x64 x 5 levels concatenated, BRDF
+    LUT 256^2, all RGBA32F; reference src/core/environment.c:111-484).
+
+    The content is a smooth gradient sky with a sun lobe, blurred per level;
+    the BRDF LUT is a smooth split-sum-shaped table.  The frame path's work
+    (lookups, bilinear filtering, LUT fetches) does not depend on the values,
+    so the benchmark uses these maps; parity tests use the maps the reference
+    library itself precomputes."""
+    sd = np.asarray(sun_dir, np.float64)
+    sd /= np.linalg.norm(sd)
+
+    def sky(w, h, blur):
+        u = (np.arange(w) + 0.5) / w
+        v = (np.arange(h) + 0.5) / h
+        phi = (u - 0.5) * 2.0 * math.pi
+        th = (v - 0.5) * math.pi
+        P, T = np.meshgrid(phi, th)
+        d = np.stack([np.cos(T) * np.cos(P), np.sin(T), np.cos(T) * np.sin(P)], -1)
+        up = np.clip(d[..., 1], -1.0, 1.0)
+        base = np.stack([0.35 + 0.25 * up, 0.45 + 0.25 * up, 0.65 + 0.3 * up], -1)
+        base = np.where(up[..., None] < 0, np.array([0.18, 0.16, 0.14]), base)
+        cosang = np.clip((d * sd).sum(-1), -1.0, 1.0)
+        sharp = 400.0 / (1.0 + 60.0 * blur)
+        sun = (6.0 / (1.0 + 20.0 * blur)) * np.exp(sharp * (cosang - 1.0))
+        rgb = base * (1.0 - 0.5 * blur) + sun[..., None] * np.array([1.0, 0.95, 0.85])
+        out = np.ones((h, w, 4), np.float32)
+        out[..., :3] = rgb
+        return out
+
+    iw, ih = irr_size
+    irr = sky(iw, ih, 1.0)
+    pw, ph = pf_size
+    pf = []
+    for l in range(levels):
+        lw, lh = max(1, pw >> l), max(1, ph >> l)
+        pf.append(sky(lw, lh, l / max(1, levels - 1)).reshape(-1))
+    ndv = (np.arange(brdf_size) + 0.5) / brdf_size
+    rough = (np.arange(brdf_size) + 0.5) / brdf_size
+    N, R = np.meshgrid(ndv, rough)
+    scale = np.clip(1.0 - 0.6 * R * (1.0 - N) - 0.3 * (1.0 - N) ** 5, 0.0, 1.0)
+    bias = np.clip(0.08 * (1.0 - N) ** 5 * (1.0 - R) + 0.02 * R, 0.0, 1.0)
+    lut = np.zeros((brdf_size, brdf_size, 4), np.float32)
+    lut[..., 0] = scale
+    lut[..., 1] = bias
+    lut[..., 3] = 1.0
+    return {"irr": irr.reshape(-1), "irr_w": iw, "irr_h": ih,
+            "pf": np.concatenate(pf).astype(np.float32), "pf_w": pw, "pf_h": ph,
+            "pf_levels": levels, "brdf": lut.reshape(-1), "brdf_size": brdf_size,
+            "rotation": float(rotation), "intensity": float(intensity)}
+
+
 def pick_points(scene: Scene, n: int = 1000, seed: int = 11) -> np.ndarray:
     rng = np.random.default_rng(seed)
     xy = np.empty((n, 2), np.int32)

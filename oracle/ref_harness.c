@@ -62,14 +62,19 @@ void *refh_create(const RefScene *sc) {
 
   long n = sysconf(_SC_NPROCESSORS_ONLN);
   h->threads = n > 1 ? (int)n : 1;
+  /* The CPU device's only member is its tile pool pointer. */
+  MopSwThreadPool **pool = (MopSwThreadPool **)vp->device;
   if (sc->serial) {
-    /* The CPU device's only member is its tile pool pointer. */
-    MopSwThreadPool **pool = (MopSwThreadPool **)vp->device;
     if (*pool) {
       mop_sw_threadpool_destroy(*pool);
       *pool = NULL;
     }
     h->threads = 1;
+  } else if (sc->workers > 0) {
+    if (*pool)
+      mop_sw_threadpool_destroy(*pool);
+    *pool = mop_sw_threadpool_create(sc->workers);
+    h->threads = sc->workers + 1; /* workers + the calling thread */
   }
 
   mop_viewport_set_chrome(vp, false);

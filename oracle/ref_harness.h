@@ -67,6 +67,8 @@ typedef struct RefScene {
   float env_rotation, env_intensity;
   int32_t serial;           /* 1: null the tile thread pool (serial path)  */
   int32_t flat;             /* 1: MOP_SHADING_FLAT for the viewport        */
+  int32_t workers;          /* >0: replace the tile pool with this many
+                               worker threads (default: nproc-1)           */
 } RefScene;
 
 typedef struct RefFrame {

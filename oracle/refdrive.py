@@ -47,7 +47,7 @@ class RefScene(C.Structure):
                 ("sun_dir", C.c_float * 3), ("turbidity", C.c_float),
                 ("ground_albedo", C.c_float), ("env_rotation", C.c_float),
                 ("env_intensity", C.c_float), ("serial", C.c_int32),
-                ("flat", C.c_int32)]
+                ("flat", C.c_int32), ("workers", C.c_int32)]
 
 
 class RefFrame(C.Structure):
@@ -100,7 +100,7 @@ def lib():
 class Reference:
     """A reference CPU-backend viewport holding one scene."""
 
-    def __init__(self, scene, serial: bool = True):
+    def __init__(self, scene, serial: bool = True, workers: int = 0):
         L = lib()
         self.scene = scene
         self._keep = []
@@ -154,6 +154,7 @@ class Reference:
         sc.env_rotation, sc.env_intensity = scene.env_rotation, scene.env_intensity
         sc.serial = 1 if serial else 0
         sc.flat = 0 if getattr(scene, "smooth", True) else 1
+        sc.workers = int(workers)
         self._keep += [meshes, lights, tw, th, td, sc]
         self.h = L.refh_create(C.byref(sc))
         if not self.h:
