@@ -172,6 +172,25 @@ def emit(line):
     print(json.dumps(line), flush=True)
 
 
+def max_over_ranks(x, dist=None, device="cpu"):
+    """Max of a per-rank float over the process group (identity when alone)."""
+    if dist is None:
+        return float(x)
+    import torch
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def aggregate(local_ms, steps, world, pixels, triangles, dist=None, device="cpu"):
+    """Replica aggregation: every rank rendered `steps` frames of `pixels`
+    presented pixels; the job's time is the slowest rank's.  Returns
+    (max_ms, Mpix/s, Mtri/s) for the whole job."""
+    total = max_over_ranks(local_ms, dist, device)
+    return (total, world * steps * pixels / (total * 1e3),
+            world * steps * triangles / (total * 1e3))
+
+
 def run_reference(args):
     rank, world, local = dist_setup(args)
     if rank != 0:
@@ -213,13 +232,6 @@ def run_cuda(args):
             dist.barrier()
         torch.cuda.synchronize()
 
-    def max_over_ranks(x):
-        if dist is None:
-            return float(x)
-        t = torch.tensor([float(x)], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
-
     import mopcuda
     import scenes
     sc, desc = workload(args.config)
@@ -251,9 +263,8 @@ def run_cuda(args):
     launches = dev.launches - l0
     barrier()
     clocks = sampler.stop()
-    total_ms = max_over_ranks(sum(frame_ms))
-    value = world * steps * sc.pixels / (total_ms * 1e3)
-    mtri = world * steps * sc.triangle_count / (total_ms * 1e3)
+    total_ms, value, mtri = aggregate(sum(frame_ms), steps, world, sc.pixels,
+                                      sc.triangle_count, dist, "cuda")
 
     # ---- end to end through the C ABI with host buffers ----
     dev.set_stage_timing(False)
@@ -269,7 +280,7 @@ def run_cuda(args):
         r.color(out_np)
     t1 = time.perf_counter()
     barrier()
-    e2e_ms = max_over_ranks((t1 - t0) * 1e3)
+    e2e_ms = max_over_ranks((t1 - t0) * 1e3, dist, "cuda")
     e2e = world * steps * sc.pixels / (e2e_ms * 1e3)
     h2d, d2h = dev.frame_io_bytes()
     d2h += out_np.nbytes

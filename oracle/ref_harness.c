@@ -45,9 +45,10 @@ void *refh_create(const RefScene *sc) {
   RefH *h = calloc(1, sizeof(RefH));
   if (!h)
     return NULL;
+  bool cpu = sc->backend == 0;
   MopViewportDesc desc = {.width = sc->width,
                           .height = sc->height,
-                          .backend = MOP_BACKEND_CPU,
+                          .backend = cpu ? MOP_BACKEND_CPU : (MopBackendType)sc->backend,
                           .reverse_z = false,
                           .ssaa_factor = sc->ssaa};
   h->vp = mop_viewport_create(&desc);
@@ -64,7 +65,9 @@ void *refh_create(const RefScene *sc) {
   h->threads = n > 1 ? (int)n : 1;
   /* The CPU device's only member is its tile pool pointer. */
   MopSwThreadPool **pool = (MopSwThreadPool **)vp->device;
-  if (sc->serial) {
+  if (!cpu) {
+    h->threads = 0;
+  } else if (sc->serial) {
     if (*pool) {
       mop_sw_threadpool_destroy(*pool);
       *pool = NULL;

@@ -69,6 +69,8 @@ typedef struct RefScene {
   int32_t flat;             /* 1: MOP_SHADING_FLAT for the viewport        */
   int32_t workers;          /* >0: replace the tile pool with this many
                                worker threads (default: nproc-1)           */
+  int32_t backend;          /* 0: MOP_BACKEND_CPU; 4: the CUDA backend
+                               (only in the drop-in harness library)       */
 } RefScene;
 
 typedef struct RefFrame {

@@ -47,7 +47,8 @@ class RefScene(C.Structure):
                 ("sun_dir", C.c_float * 3), ("turbidity", C.c_float),
                 ("ground_albedo", C.c_float), ("env_rotation", C.c_float),
                 ("env_intensity", C.c_float), ("serial", C.c_int32),
-                ("flat", C.c_int32), ("workers", C.c_int32)]
+                ("flat", C.c_int32), ("workers", C.c_int32),
+                ("backend", C.c_int32)]
 
 
 class RefFrame(C.Structure):
@@ -72,19 +73,21 @@ def light_struct(L, cls=RefLight):
     return s
 
 
-_lib = None
+_libs = {}
+REF_CUDA_SO = HERE / "_ref" / "libmopref_cuda.so"
+BACKEND_CUDA = 4  # MOP_BACKEND_CUDA in the integration patch
 
 
 def available() -> bool:
     return REF_SO.exists()
 
 
-def lib():
-    global _lib
-    if _lib is None:
-        if not REF_SO.exists():
-            raise FileNotFoundError(f"reference library not built: {REF_SO}")
-        _lib = C.CDLL(str(REF_SO))
+def lib(kind: str = "cpu"):
+    so = REF_SO if kind == "cpu" else REF_CUDA_SO
+    if kind not in _libs:
+        if not so.exists():
+            raise FileNotFoundError(f"reference library not built: {so}")
+        _lib = _libs[kind] = C.CDLL(str(so))
         _lib.refh_create.restype = C.c_void_p
         _lib.refh_create.argtypes = [C.POINTER(RefScene)]
         _lib.refh_render.argtypes = [C.c_void_p, C.POINTER(RefFrame)]
@@ -94,14 +97,14 @@ def lib():
         _lib.refh_time_frames.argtypes = [C.c_void_p, C.c_int, C.c_int]
         _lib.refh_num_threads.argtypes = [C.c_void_p]
         _lib.refh_destroy.argtypes = [C.c_void_p]
-    return _lib
+    return _libs[kind]
 
 
 class Reference:
     """A reference CPU-backend viewport holding one scene."""
 
-    def __init__(self, scene, serial: bool = True, workers: int = 0):
-        L = lib()
+    def __init__(self, scene, serial: bool = True, workers: int = 0, backend: str = "cpu"):
+        L = self.L = lib(backend)
         self.scene = scene
         self._keep = []
         meshes = (RefMesh * max(1, len(scene.meshes)))()
@@ -155,6 +158,7 @@ class Reference:
         sc.serial = 1 if serial else 0
         sc.flat = 0 if getattr(scene, "smooth", True) else 1
         sc.workers = int(workers)
+        sc.backend = 0 if backend == "cpu" else BACKEND_CUDA
         self._keep += [meshes, lights, tw, th, td, sc]
         self.h = L.refh_create(C.byref(sc))
         if not self.h:
@@ -174,7 +178,7 @@ class Reference:
         f.color_full = out["color_full"].ctypes.data
         f.depth = out["depth"].ctypes.data
         f.object_id = out["object_id"].ctypes.data
-        rc = lib().refh_render(self.h, C.byref(f))
+        rc = self.L.refh_render(self.h, C.byref(f))
         if rc != 0:
             raise RuntimeError(f"refh_render failed: {rc}")
         out["view"] = np.array(f.view[:], np.float32)
@@ -190,7 +194,7 @@ class Reference:
         ids = np.zeros(n, np.uint32)
         dep = np.zeros(n, np.float32)
         hits = np.zeros(n, np.int32)
-        lib().refh_pick(self.h, n, xy.ctypes.data, ids.ctypes.data, dep.ctypes.data, hits.ctypes.data)
+        self.L.refh_pick(self.h, n, xy.ctypes.data, ids.ctypes.data, dep.ctypes.data, hits.ctypes.data)
         return ids, dep, hits
 
     def env_maps(self):
@@ -198,7 +202,7 @@ class Reference:
         ints = [C.c_int32() for _ in range(7)]
         irr, pf, brdf = ptrs
         iw, ih, pw, ph, lv, bs = ints[:6]
-        rc = lib().refh_env_maps(self.h, C.byref(irr), C.byref(iw), C.byref(ih), C.byref(pf),
+        rc = self.L.refh_env_maps(self.h, C.byref(irr), C.byref(iw), C.byref(ih), C.byref(pf),
                                  C.byref(pw), C.byref(ph), C.byref(lv), C.byref(brdf), C.byref(bs))
         if rc != 0:
             return None
@@ -218,15 +222,15 @@ class Reference:
         }
 
     def time_frames(self, warm: int, frames: int) -> float:
-        return lib().refh_time_frames(self.h, warm, frames)
+        return self.L.refh_time_frames(self.h, warm, frames)
 
     @property
     def threads(self) -> int:
-        return lib().refh_num_threads(self.h)
+        return self.L.refh_num_threads(self.h)
 
     def close(self):
         if self.h:
-            lib().refh_destroy(self.h)
+            self.L.refh_destroy(self.h)
             self.h = None
 
     def __del__(self):

@@ -1,0 +1,108 @@
+"""CPU-side checks of the drop-in boundary (no GPU needed):
+
+* libmopcuda.so loads and exports every function include/mop_cuda.h declares;
+* libmop_rhi_cuda.so exports mop_rhi_backend_cuda (the RHI table);
+* the library's host-side matrices are bit-identical to the reference's
+  (camera chain, mvp products, TRS composition);
+* without a CUDA device, device creation fails loudly (no CPU fallback).
+"""
+import ctypes as C
+import re
+import subprocess
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+import cpu_oracle
+import mopcuda
+import refdrive
+import scenes
+
+ROOT = Path(__file__).resolve().parents[1]
+HEADER = ROOT / "include" / "mop_cuda.h"
+
+
+def declared_functions():
+    text = HEADER.read_text()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(mopcuda_[a-z0-9_]+)\s*\(", text)))
+
+
+def exported(lib_path):
+    out = subprocess.run(["nm", "-D", "--defined-only", str(lib_path)], capture_output=True,
+                         text=True, check=True).stdout
+    return {line.split()[-1] for line in out.splitlines() if " T " in line}
+
+
+def test_header_symbols_exported():
+    names = declared_functions()
+    assert len(names) >= 40
+    have = exported(mopcuda.LIB_PATH)
+    missing = [n for n in names if n not in have]
+    assert not missing, f"declared but not exported: {missing}"
+
+
+def test_binding_covers_header():
+    bound = {s[0] for s in mopcuda.SIGNATURES}
+    assert set(declared_functions()) <= bound
+    mopcuda.lib()  # every signature resolves
+
+
+def test_rhi_table_exported():
+    so = ROOT / "master-of-puppets_b200" / "libmop_rhi_cuda.so"
+    if not so.exists():
+        pytest.skip("RHI table library not built (needs the reference headers)")
+    assert "mop_rhi_backend_cuda" in exported(so)
+
+
+@pytest.mark.parametrize("make", [scenes.config1, lambda: scenes.small_scene(3),
+                                  lambda: scenes.coplanar_scene(),
+                                  lambda: scenes.config2(instances=6, tex_size=8)])
+def test_host_matrices_match_oracle(make):
+    sc = make()
+    v1, p1, e1 = mopcuda.camera_matrices(sc)
+    v2, p2, e2 = cpu_oracle.camera(sc)
+    for a, b in ((v1, v2), (p1, p2), (e1, e2)):
+        assert (a.view(np.uint32) == b.view(np.uint32)).all()
+    for m in sc.meshes:
+        a = mopcuda.mat4_multiply(p1, mopcuda.mat4_multiply(v1, m.transform))
+        b = cpu_oracle.mat4_multiply(p2, cpu_oracle.mat4_multiply(v2, m.transform))
+        assert (a.view(np.uint32) == b.view(np.uint32)).all()
+
+
+@pytest.mark.skipif(not refdrive.available(), reason="reference library not built")
+def test_compose_trs_matches_reference():
+    """mopcuda_mat4_compose_trs vs the reference's own mop_mat4_compose_trs."""
+    ref = refdrive.lib()
+
+    class M4(C.Structure):
+        _fields_ = [("d", C.c_float * 16)]
+
+    class V3(C.Structure):
+        _fields_ = [("x", C.c_float), ("y", C.c_float), ("z", C.c_float)]
+
+    ref.mop_mat4_compose_trs.restype = M4
+    ref.mop_mat4_compose_trs.argtypes = [V3, V3, V3]
+    rng = np.random.default_rng(4)
+    for _ in range(200):
+        p, r, s = (rng.uniform(-5, 5, 3).astype(np.float32) for _ in range(3))
+        want = np.array(ref.mop_mat4_compose_trs(V3(*p), V3(*r), V3(*s)).d[:], np.float32)
+        got = np.zeros(16, np.float32)
+        mopcuda.lib().mopcuda_mat4_compose_trs(p.ctypes.data, r.ctypes.data, s.ctypes.data,
+                                              got.ctypes.data)
+        assert (got.view(np.uint32) == want.view(np.uint32)).all()
+
+
+def _has_gpu():
+    try:
+        import torch
+        return torch.cuda.is_available()
+    except Exception:
+        return False
+
+
+@pytest.mark.skipif(_has_gpu(), reason="a CUDA device is present")
+def test_no_gpu_fails_loudly():
+    with pytest.raises(RuntimeError):
+        mopcuda.Device(0)

@@ -1,0 +1,59 @@
+"""Drop-in check through the reference's own public API.
+
+The unmodified reference viewport core (its compiled objects, with only the
+backend-resolution function swapped so value 4 means the CUDA backend — the
+integration patch in INTEGRATION.md does the same with MOP_BACKEND_CUDA)
+renders each scene twice in one process: once on its CPU backend, once on
+mop_rhi_backend_cuda().  mop_viewport_read_color (SSAA box in the core),
+the object-ID / depth readbacks and mop_viewport_pick must agree: IDs and
+depth bit-exact, colour within the contract tolerance.
+
+Scenes avoid image-based lighting: the unmodified core hands IBL state only
+to its CPU path (reference viewport.c:2692-2706); the CUDA backend receives
+the full IBL state through mopcuda_set_ibl (covered by test_gpu_parity.py).
+"""
+import dataclasses
+
+import numpy as np
+import pytest
+
+import refdrive
+import scenes
+from parity import color_stats, COLOR_MAX_LSB, COLOR_1LSB_FRACTION
+
+pytestmark = pytest.mark.gpu
+
+CASES = {
+    "config1": lambda: scenes.config1(),
+    "mixed": lambda: scenes.small_scene(seed=21, width=240, height=160),
+    "ssaa2": lambda: scenes.small_scene(seed=22, width=160, height=120, ssaa=2),
+    "flat": lambda: dataclasses.replace(scenes.small_scene(seed=23), smooth=False),
+    "coplanar": lambda: scenes.coplanar_scene(seed=24),
+    "config2_reduced_no_ibl": lambda: dataclasses.replace(
+        scenes.config2(width=480, height=270, ssaa=2, instances=48, tex_size=64), env=0),
+}
+
+
+@pytest.mark.parametrize("name", list(CASES))
+def test_viewport_api_cuda_matches_cpu(name):
+    if not refdrive.REF_CUDA_SO.exists():
+        pytest.skip("drop-in harness library not built")
+    sc = CASES[name]()
+    cpu = refdrive.Reference(sc, serial=True)
+    gpu = refdrive.Reference(sc, backend="cuda")
+    try:
+        a = cpu.render()
+        b = gpu.render()
+        assert (a["object_id"] == b["object_id"]).all(), "object IDs differ"
+        assert (a["depth"].view(np.uint32) == b["depth"].view(np.uint32)).all(), "depth differs"
+        for key in ("color", "color_full"):
+            s = color_stats(a[key], b[key])
+            assert s["max"] <= COLOR_MAX_LSB and s["within1"] >= COLOR_1LSB_FRACTION, (key, s)
+        assert a["triangle_count"] == b["triangle_count"]
+        xy = scenes.pick_points(sc, 500)
+        for x, y in zip(cpu.pick(xy), gpu.pick(xy)):
+            assert (np.ascontiguousarray(x).view(np.uint8) ==
+                    np.ascontiguousarray(y).view(np.uint8)).all()
+    finally:
+        gpu.close()
+        cpu.close()
