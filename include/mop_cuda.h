@@ -197,6 +197,26 @@ float mopcuda_pick_read_depth(MopCudaDevice *dev, MopCudaFramebuffer *fb, int x,
 int mopcuda_pick_batch(MopCudaDevice *dev, MopCudaFramebuffer *fb, int ssaa, const int32_t *xy,
                        uint32_t n, uint32_t *ids, float *depths, int32_t *hits);
 
+/* Same results as mopcuda_pick_batch, for callers that cannot allocate at
+ * call time (a fixed memory budget with their own allocator, a thread that
+ * must not call cudaMalloc/cudaFree because they synchronise the device, an
+ * embedder that forbids allocation after start-up).  No counterpart in the
+ * reference: its CPU picks read host arrays directly.
+ *
+ * Nothing is allocated: queries and results are staged in one file-scope
+ * device array of MOPCUDA_NOALLOC_PICK_MAX * 20 bytes (1.25 MiB) that every
+ * GPU loading the library holds until the process exits.  More than
+ * MOPCUDA_NOALLOC_PICK_MAX queries are rejected with MOPCUDA_EINVAL.  xy and
+ * the outputs are host memory.  The frame must be complete
+ * (mopcuda_frame_wait) — completing it here could reallocate.  The first
+ * call on a device resolves the array's device address and creates one
+ * event; make it before any stream capture.  All calls share the array (it
+ * keeps the last call's contents): calls that overlap on the GPU race. */
+#define MOPCUDA_NOALLOC_PICK_MAX 65536u
+int mopcuda_pick_batch_noalloc(MopCudaDevice *dev, MopCudaFramebuffer *fb, int ssaa,
+                               const int32_t *xy, uint32_t n, uint32_t *ids, float *depths,
+                               int32_t *hits);
+
 /* ---- measurement (no reference counterpart: the reference reports only
  *      wall-clock MopFrameStats, include/mop/util/profile.h:51-81) ------- */
 /* Record CUDA events between the frame's stages on the device stream. */

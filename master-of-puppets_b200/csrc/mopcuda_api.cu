@@ -1146,3 +1146,90 @@ extern "C" int mopcuda_measure_fp32_peak(MopCudaDevice *d, double *gops) {
   *gops = best;
   return MOPCUDA_OK;
 }
+
+/* ------------------------------------------------------------------------
+ * Batched pick without any allocation.
+ *
+ * For callers that cannot allocate device or pinned memory at call time —
+ * hosts that run a fixed memory budget with their own allocator, code that
+ * must not call cudaMalloc from a latency-critical thread (cudaMalloc and
+ * cudaFree synchronise the device), or embedders that forbid allocation
+ * after start-up.  The query coordinates and the results are staged in this
+ * file-scope device array instead of per-device arenas.  Every GPU that
+ * loads the library holds it until the process exits.
+ *
+ * Set-up: the first call on a device (with that device current) resolves
+ * the array's device address with cudaGetSymbolAddress — the host-side name
+ * is only a stand-in, not a device address — and creates one event for the
+ * bounded wait.  Make that first call before any stream capture.
+ * All calls share the array and it keeps the last call's contents (every
+ * slot a call reads is written by that call first); calls whose work
+ * overlaps on the GPU race on it, so callers must not overlap them.
+ * ------------------------------------------------------------------------ */
+#define NOALLOC_PICK_BYTES_PER_QUERY 20u /* int2 in, uint32 + float + int32 out */
+static __device__ __align__(256) unsigned char
+    g_pick_scratch[(size_t)MOPCUDA_NOALLOC_PICK_MAX * NOALLOC_PICK_BYTES_PER_QUERY];
+
+#define NOALLOC_MAX_DEVICES 64
+static std::mutex g_noalloc_mu;
+static void *g_noalloc_ptr[NOALLOC_MAX_DEVICES];
+static cudaEvent_t g_noalloc_ev[NOALLOC_MAX_DEVICES];
+
+static int noalloc_setup(int ordinal, unsigned char **scratch, cudaEvent_t *ev) {
+  if (ordinal < 0 || ordinal >= NOALLOC_MAX_DEVICES)
+    return fail(MOPCUDA_EINVAL, "pick_batch_noalloc: device ordinal %d unsupported", ordinal);
+  std::lock_guard<std::mutex> lk(g_noalloc_mu);
+  if (!g_noalloc_ptr[ordinal]) {
+    void *p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_pick_scratch);
+    if (e != cudaSuccess || !p)
+      return fail(MOPCUDA_ECUDA, "pick_batch_noalloc: cudaGetSymbolAddress failed: %s",
+                  cudaGetErrorString(e));
+    cudaEvent_t ev_new;
+    e = cudaEventCreateWithFlags(&ev_new, cudaEventDisableTiming);
+    if (e != cudaSuccess)
+      return fail(MOPCUDA_ECUDA, "pick_batch_noalloc: event creation failed: %s",
+                  cudaGetErrorString(e));
+    g_noalloc_ev[ordinal] = ev_new;
+    g_noalloc_ptr[ordinal] = p;
+  }
+  *scratch = (unsigned char *)g_noalloc_ptr[ordinal];
+  *ev = g_noalloc_ev[ordinal];
+  return MOPCUDA_OK;
+}
+
+extern "C" int mopcuda_pick_batch_noalloc(MopCudaDevice *d, MopCudaFramebuffer *fb, int sf,
+                                          const int32_t *xy, uint32_t n, uint32_t *ids,
+                                          float *depths, int32_t *hits) {
+  if (!d || !fb || sf <= 0 || (n && (!xy || !ids || !depths || !hits)))
+    return fail(MOPCUDA_EINVAL, "pick_batch_noalloc: bad arguments");
+  if (n > MOPCUDA_NOALLOC_PICK_MAX)
+    return fail(MOPCUDA_EINVAL, "pick_batch_noalloc: %u queries exceed the limit of %u", n,
+                (unsigned)MOPCUDA_NOALLOC_PICK_MAX);
+  if (n == 0)
+    return MOPCUDA_OK;
+  std::lock_guard<std::mutex> lk(d->mu);
+  if (d->pending && d->fb == fb)
+    return fail(MOPCUDA_EINVAL, "pick_batch_noalloc: frame still pending; call "
+                                "mopcuda_frame_wait first (completion may reallocate)");
+  CU_TRY(cudaSetDevice(d->ordinal));
+  unsigned char *scratch = nullptr;
+  cudaEvent_t ev = nullptr;
+  int rc = noalloc_setup(d->ordinal, &scratch, &ev);
+  if (rc)
+    return rc;
+  int2 *dxy = (int2 *)scratch;
+  uint32_t *oid = (uint32_t *)(scratch + 8ull * MOPCUDA_NOALLOC_PICK_MAX);
+  float *odp = (float *)(oid + MOPCUDA_NOALLOC_PICK_MAX);
+  int32_t *oht = (int32_t *)(odp + MOPCUDA_NOALLOC_PICK_MAX);
+  cudaStream_t s = d->stream;
+  CU_TRY(cudaMemcpyAsync(dxy, xy, 8ull * n, cudaMemcpyHostToDevice, s));
+  d->launches += (uint64_t)mopcuda_launch_pick(fb->ids.as<uint32_t>(), fb->depth.as<float>(),
+                                               fb->w, fb->h, sf, dxy, n, oid, odp, oht, s);
+  CU_TRY(cudaGetLastError());
+  CU_TRY(cudaMemcpyAsync(ids, oid, 4ull * n, cudaMemcpyDeviceToHost, s));
+  CU_TRY(cudaMemcpyAsync(depths, odp, 4ull * n, cudaMemcpyDeviceToHost, s));
+  CU_TRY(cudaMemcpyAsync(hits, oht, 4ull * n, cudaMemcpyDeviceToHost, s));
+  CU_TRY(cudaEventRecord(ev, s));
+  return bounded_sync(d, ev, FRAME_TIMEOUT_MS);
+}

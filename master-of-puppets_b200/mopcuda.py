@@ -90,6 +90,7 @@ SIGNATURES = [
     ("mopcuda_pick_read_id", C.c_uint32, [_P, _P, C.c_int, C.c_int]),
     ("mopcuda_pick_read_depth", C.c_float, [_P, _P, C.c_int, C.c_int]),
     ("mopcuda_pick_batch", C.c_int, [_P, _P, C.c_int, _P, C.c_uint32, _P, _P, _P]),
+    ("mopcuda_pick_batch_noalloc", C.c_int, [_P, _P, C.c_int, _P, C.c_uint32, _P, _P, _P]),
     ("mopcuda_set_stage_timing", None, [_P, C.c_int]),
     ("mopcuda_stage_times", C.c_int, [_P, _P, C.c_int]),
     ("mopcuda_measure_fp32_peak", C.c_int, [_P, C.POINTER(C.c_double)]),
