@@ -222,8 +222,9 @@ int mopcuda_pick_batch_noalloc(MopCudaDevice *dev, MopCudaFramebuffer *fb, int s
 /* Record CUDA events between the frame's stages on the device stream. */
 void mopcuda_set_stage_timing(MopCudaDevice *dev, int on);
 /* Stage durations of the last completed frame, ms: [0] vertex transform,
- * [1] triangle setup + clipping, [2] binning, [3] tile visibility + shading
- * + resolve, [4] post (FXAA, gamma, SSAA).  `ms` holds >= 5 floats. */
+ * [1] triangle setup + clipping, [2] visibility raster, [3] resolve of
+ * background + compaction, [4] deferred shading + ACES, [5] post (FXAA,
+ * gamma, SSAA).  `ms` holds >= 6 floats. */
 int mopcuda_stage_times(MopCudaDevice *dev, float *ms, int n);
 /* Measured FP32 add/multiply issue rate without FMA, Gop/s: the roofline
  * denominator of the shading stage. */

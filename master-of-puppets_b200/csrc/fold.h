@@ -33,8 +33,10 @@
 
 #if defined(__CUDACC__)
 #define MOPCUDA_HD __host__ __device__ __forceinline__
+#define MOPCUDA_HD_SLOW static __host__ __device__ __noinline__
 #else
 #define MOPCUDA_HD static inline
+#define MOPCUDA_HD_SLOW static
 #include <string.h>
 #endif
 
@@ -68,15 +70,11 @@ MOPCUDA_HD float fold_fadd(float a, float b) {
 #endif
 }
 
-#define FOLD_SERIAL_MAX 8
+#define FOLD_SERIAL_MAX 16
 
-/* w after k >= 0 sequential additions of d. */
-MOPCUDA_HD float fold_add(float w, float d, int k) {
-  if (k <= FOLD_SERIAL_MAX) {
-    for (int i = 0; i < k; i++)
-      w = fold_fadd(w, d);
-    return w;
-  }
+/* The binade-skipping path of fold_add for k > FOLD_SERIAL_MAX (kept out of
+ * line: callers inline only the short serial loop). */
+MOPCUDA_HD_SLOW float fold_add_long(float w, float d, int k) {
   uint32_t db = fold_bits(d);
   /* d = +-0, inf or NaN: after one addition the value is a fixed point. */
   if ((db & 0x7fffffffu) == 0u || (db & 0x7f800000u) == 0x7f800000u)
@@ -119,6 +117,19 @@ MOPCUDA_HD float fold_add(float w, float d, int k) {
     k -= j;
   }
   return w;
+}
+
+/* w after k >= 0 sequential additions of d. */
+MOPCUDA_HD float fold_add(float w, float d, int k) {
+  if (k <= FOLD_SERIAL_MAX) {
+    /* fully unrolled and predicated: no loop and no divergence on k */
+#pragma unroll
+    for (int i = 0; i < FOLD_SERIAL_MAX; i++)
+      if (i < k)
+        w = fold_fadd(w, d);
+    return w;
+  }
+  return fold_add_long(w, d, k);
 }
 
 #endif

@@ -7,10 +7,13 @@
  *   k_setup      cull / trivial accept /  mop_sw_rasterize_triangle_full
  *                screen map / edge setup  rasterizer.c:2458-2612, 1825-1924
  *   k_clip       Sutherland-Hodgman fan   rasterizer.c:514-626
- *   k_bin_*      screen-tile binning      (replaces rasterizer_mt.c binning)
- *   k_tile       visibility (64-bit key   rasterizer.c:1926-1960 coverage +
- *                atomicMin) + deferred    depth; 1961-2108 shading;
- *                shading + ACES resolve   2776-2803 resolve
+ *   k_raster_*   coverage + depth into a  rasterizer.c:1926-1960 (the
+ *                64-bit atomicMin key     incremental edge walk and the
+ *                buffer (small records:   strict depth test; replaces the
+ *                thread each; large:      single-threaded centroid binning
+ *                (row, chunk) items)      of rasterizer_mt.c)
+ *   k_resolve    background + compaction  rasterizer.c:2785-2792
+ *   k_shade      deferred shading + ACES  rasterizer.c:1961-2108, 2776-2803
  *   k_post       FXAA + post + SSAA box   rasterizer.c:2625-2761,
  *                                         postprocess.c:24-116,
  *                                         viewport.c:3385-3411
@@ -22,6 +25,11 @@
 #include "mopcuda_internal.cuh"
 
 #define PI_F 3.14159274f /* (float)M_PI */
+
+/* (uint8_t) of a value already clamped to [0, 255.5] (or NaN): plain
+ * truncation agrees with the x86 conversion there (NaN -> 0 on both after
+ * taking the low byte of INT_MIN / 0). */
+__device__ __forceinline__ uint8_t u8_of(float v) { return (uint8_t)__float2int_rz(v); }
 
 /* ------------------------------------------------------------------------
  * small vector math (reference math.c:17-50, 196-203)
@@ -145,7 +153,7 @@ __global__ void k_vertex(FrameArgs a) {
   }
   a.clip[g] = c;
   a.world[g] = make_float4(w.x, w.y, w.z, 0.0f);
-  a.normal[g] = make_float4(n.x, n.y, n.z, 0.0f);
+  a.normal[g] = make_float4(n.x, n.y, n.z, 1.0f / c.w); /* .w: 1/w for perspective weights */
   a.color[g] = make_float4(col[0], col[1], col[2], col[3]);
 }
 
@@ -167,7 +175,7 @@ __device__ __forceinline__ float falloff_inv_sq(const LightRec &L, float dist) {
 }
 
 __device__ __forceinline__ float spot_cone(const LightRec &L, V3 dir) {
-  V3 sd = norm3(mk3(L.direction[0], L.direction[1], L.direction[2]));
+  V3 sd = mk3(L.ndir[0], L.ndir[1], L.ndir[2]);
   float ca = -dot3(dir, sd);
   if (ca < L.spot_outer_cos)
     return 0.0f;
@@ -181,38 +189,6 @@ __device__ __forceinline__ float spot_cone(const LightRec &L, V3 dir) {
   return 1.0f;
 }
 
-/* compute_multi_light_rgb, rasterizer.c:1596-1688 */
-__device__ void diffuse_rgb(V3 n, V3 wp, const LightRec *Ls, uint32_t cnt, float amb,
-                            float out[3]) {
-  out[0] = out[1] = out[2] = amb;
-  for (uint32_t i = 0; i < cnt; i++) {
-    const LightRec &L = Ls[i];
-    if (!L.active)
-      continue;
-    float ndotl = 0.0f, att = 1.0f, spot = 1.0f;
-    if (L.type == 0) {
-      V3 dir = norm3(mk3(L.direction[0], L.direction[1], L.direction[2]));
-      ndotl = -dot3(n, dir);
-    } else if (L.type == 1 || L.type == 2) {
-      V3 tl = sub3(mk3(L.position[0], L.position[1], L.position[2]), wp);
-      float dist = len3(tl);
-      if (dist < 1e-6f)
-        dist = 1e-6f;
-      V3 dir = scale3(tl, 1.0f / dist);
-      ndotl = dot3(n, dir);
-      if (L.type == 2)
-        spot = spot_cone(L, dir);
-      att = falloff_inv_sq(L, dist);
-    }
-    if (ndotl < 0.0f)
-      ndotl = 0.0f;
-    float contrib = ndotl * L.intensity * att * spot * 1.0f;
-    out[0] += contrib * L.color[0];
-    out[1] += contrib * L.color[1];
-    out[2] += contrib * L.color[2];
-  }
-}
-
 /* compute_multi_light (flat path), rasterizer.c:1497-1588 */
 __device__ float diffuse_flat(V3 n, V3 wp, const LightRec *Ls, uint32_t cnt, float amb) {
   float total = amb;
@@ -222,7 +198,7 @@ __device__ float diffuse_flat(V3 n, V3 wp, const LightRec *Ls, uint32_t cnt, flo
       continue;
     float ndotl = 0.0f, att = 1.0f, spot = 1.0f;
     if (L.type == 0) {
-      V3 dir = norm3(mk3(L.direction[0], L.direction[1], L.direction[2]));
+      V3 dir = mk3(L.ndir[0], L.ndir[1], L.ndir[2]);
       ndotl = -dot3(n, dir);
     } else if (L.type == 1 || L.type == 2) {
       V3 tl = sub3(mk3(L.position[0], L.position[1], L.position[2]), wp);
@@ -253,65 +229,83 @@ __device__ float diffuse_flat(V3 n, V3 wp, const LightRec *Ls, uint32_t cnt, flo
   return clamp01(total);
 }
 
-/* compute_multi_specular_ggx, rasterizer.c:1701-1814 */
-__device__ void specular_ggx(V3 n, V3 wp, V3 vdir, const LightRec *Ls, uint32_t cnt, float rough,
-                             float metal, const float base[3], float out[3]) {
-  out[0] = out[1] = out[2] = 0.0f;
-  float alpha = rough * rough;
-  float alpha2 = alpha * alpha;
-  if (alpha2 < 1e-7f)
-    alpha2 = 1e-7f;
+/* compute_multi_light_rgb (rasterizer.c:1596-1688) and
+ * compute_multi_specular_ggx (1701-1814) evaluated in one pass over the
+ * lights.  For point and spot lights both reference helpers compute the same
+ * to-light vector, distance, direction, N.L and inverse-square / range
+ * falloff from the same operands in the same order, so those values are
+ * computed once here; each helper's own accumulation order is unchanged. */
+__device__ void lights_smooth(V3 n, V3 wp, V3 vdir, const LightRec *Ls, const DrawRec &d,
+                              const float base[3], float lit[3], float spec[3]) {
+  lit[0] = lit[1] = lit[2] = d.ambient;
+  spec[0] = spec[1] = spec[2] = 0.0f;
+  const float alpha2 = d.alpha2, k = d.smith_k, omk = d.one_minus_k;
   float ndotv = dot3(n, vdir);
   if (ndotv < 1e-4f)
     ndotv = 1e-4f;
   float f0[3];
   for (int c = 0; c < 3; c++)
-    f0[c] = 0.04f * (1.0f - metal) + base[c] * metal;
-  float k = alpha * 0.5f;
-  float g1v = ndotv / (ndotv * (1.0f - k) + k);
+    f0[c] = d.f0_dielectric + base[c] * d.metallic;
+  const float g1v = ndotv / (ndotv * omk + k);
+  const uint32_t cnt = d.light_count;
   for (uint32_t i = 0; i < cnt; i++) {
     const LightRec &L = Ls[i];
     if (!L.active)
       continue;
-    V3 ldir = mk3(0.0f, 0.0f, 0.0f);
-    float att = 1.0f;
+    float ndl_d = 0.0f, ndl_s, att = 1.0f, spot = 1.0f;
+    V3 ldir;
     if (L.type == 0) {
-      V3 dd = norm3(mk3(L.direction[0], L.direction[1], L.direction[2]));
-      ldir = mk3(-dd.x, -dd.y, -dd.z);
+      const V3 nd = mk3(L.ndir[0], L.ndir[1], L.ndir[2]);
+      ndl_d = -dot3(n, nd);
+      ldir = mk3(-nd.x, -nd.y, -nd.z);
+      ndl_s = dot3(n, ldir);
     } else if (L.type == 1 || L.type == 2) {
-      V3 tl = sub3(mk3(L.position[0], L.position[1], L.position[2]), wp);
+      const V3 tl = sub3(mk3(L.position[0], L.position[1], L.position[2]), wp);
       float dist = len3(tl);
       if (dist < 1e-6f)
         dist = 1e-6f;
       ldir = scale3(tl, 1.0f / dist);
+      ndl_d = dot3(n, ldir);
+      ndl_s = ndl_d;
+      if (L.type == 2)
+        spot = spot_cone(L, ldir);
       att = falloff_inv_sq(L, dist);
+    } else {
+      ldir = mk3(0.0f, 0.0f, 0.0f);
+      ndl_s = dot3(n, ldir);
     }
-    float ndotl = dot3(n, ldir);
-    if (ndotl <= 0.0f)
+    /* diffuse (rasterizer.c:1673-1687) */
+    float ndotl = ndl_d < 0.0f ? 0.0f : ndl_d;
+    const float contrib = ndotl * L.intensity * att * spot * 1.0f;
+    lit[0] += contrib * L.color[0];
+    lit[1] += contrib * L.color[1];
+    lit[2] += contrib * L.color[2];
+    /* specular (rasterizer.c:1763-1813): spot lights carry no cone factor */
+    if (ndl_s <= 0.0f)
       continue;
-    V3 h = norm3(add3(ldir, vdir));
+    const V3 h = norm3(add3(ldir, vdir));
     float ndoth = dot3(n, h);
     if (ndoth < 0.0f)
       ndoth = 0.0f;
     float vdoth = dot3(vdir, h);
     if (vdoth < 0.0f)
       vdoth = 0.0f;
-    float ndoth2 = ndoth * ndoth;
-    float dd = ndoth2 * (alpha2 - 1.0f) + 1.0f;
-    float D = alpha2 / (PI_F * dd * dd);
-    float g1l = ndotl / (ndotl * (1.0f - k) + k);
-    float G = g1v * g1l;
-    float omv = 1.0f - vdoth;
-    float omv2 = omv * omv;
-    float omv5 = omv2 * omv2 * omv;
-    float den = 4.0f * ndotl * ndotv;
+    const float ndoth2 = ndoth * ndoth;
+    const float dd = ndoth2 * (alpha2 - 1.0f) + 1.0f;
+    const float D = alpha2 / (PI_F * dd * dd);
+    const float g1l = ndl_s / (ndl_s * omk + k);
+    const float G = g1v * g1l;
+    const float omv = 1.0f - vdoth;
+    const float omv2 = omv * omv;
+    const float omv5 = omv2 * omv2 * omv;
+    float den = 4.0f * ndl_s * ndotv;
     if (den < 1e-6f)
       den = 1e-6f;
-    float st = D * G / den;
-    float wgt = st * L.intensity * att * ndotl * 1.0f * PI_F;
+    const float st = D * G / den;
+    const float wgt = st * L.intensity * att * ndl_s * 1.0f * PI_F;
     for (int c = 0; c < 3; c++) {
-      float fr = f0[c] + (1.0f - f0[c]) * omv5;
-      out[c] += wgt * fr * L.color[c];
+      const float fr = f0[c] + (1.0f - f0[c]) * omv5;
+      spec[c] += wgt * fr * L.color[c];
     }
   }
 }
@@ -364,44 +358,30 @@ __device__ void ibl_irr(const FrameArgs &a, V3 n, float out[3]) {
     out[c] *= a.ibl_intensity;
 }
 
-__device__ void ibl_pf(const FrameArgs &a, V3 r, float rough, float out[3]) {
+/* The mip level and its offset/size depend only on the draw's roughness;
+ * the host computes them once per draw (rasterizer.c:243-265). */
+__device__ void ibl_pf(const FrameArgs &a, const DrawRec &d, V3 r, float out[3]) {
   out[0] = out[1] = out[2] = 0.0f;
   float len = sqrtf(r.x * r.x + r.y * r.y + r.z * r.z);
   if (len < 1e-6f)
     return;
-  int level = x86_f2i(rough * (float)(a.pf_levels - 1));
-  if (level >= a.pf_levels)
-    level = a.pf_levels - 1;
-  if (level < 0)
-    level = 0; /* only reachable for roughness < 0, undefined in the reference */
-  size_t off = 0;
-  for (int l = 0; l < level; l++) {
-    int lw = a.pf_w >> l, lh = a.pf_h >> l;
-    off += (size_t)(lw < 1 ? 1 : lw) * (size_t)(lh < 1 ? 1 : lh);
-  }
-  int lw = a.pf_w >> level, lh = a.pf_h >> level;
-  if (lw < 1)
-    lw = 1;
-  if (lh < 1)
-    lh = 1;
   float u, v;
   dir_uv(r.x / len, r.y / len, r.z / len, a.ibl_rotation, &u, &v);
-  ibl_bilinear(a.pf + off * 4, lw, lh, u, v, out);
+  ibl_bilinear(a.pf + (size_t)d.pf_off * 4, d.pf_lw, d.pf_lh, u, v, out);
   for (int c = 0; c < 3; c++)
     out[c] *= a.ibl_intensity;
 }
 
-__device__ __forceinline__ void ibl_lut(const FrameArgs &a, float ndv, float rough, float *sc,
+/* BRDF LUT at (N.V, roughness); the roughness row is per draw, computed on
+ * the host (rasterizer.c:280-291). */
+__device__ __forceinline__ void ibl_lut(const FrameArgs &a, const DrawRec &d, float ndv, float *sc,
                                         float *bi) {
   ndv = ndv < 0.0f ? 0.0f : (ndv > 1.0f ? 1.0f : ndv);
-  rough = rough < 0.0f ? 0.0f : (rough > 1.0f ? 1.0f : rough);
   int n = a.brdf_size;
   int x = (int)(ndv * (float)(n - 1) + 0.5f);
-  int y = (int)(rough * (float)(n - 1) + 0.5f);
+  int y = d.brdf_row;
   if (x >= n)
     x = n - 1;
-  if (y >= n)
-    y = n - 1;
   float4 t = __ldg((const float4 *)a.brdf + ((size_t)y * n + x));
   *sc = t.x;
   *bi = t.y;
@@ -409,11 +389,11 @@ __device__ __forceinline__ void ibl_lut(const FrameArgs &a, float ndv, float rou
 
 /* Per-sample shading of the smooth multi-light path (rasterizer.c:1963-2099)
  * from the normalised perspective-correct weights pc[]. */
-__device__ void shade_smooth(const FrameArgs &a, const DrawRec &d, const uint32_t v[3],
-                             const float pc[3], float out[3]) {
-  float4 N[3], C[3], W[3];
+__device__ void shade_smooth(const FrameArgs &a, const DrawRec &d, const LightRec *Ls,
+                             const uint32_t v[3], const float4 N[3], const float pc[3],
+                             float out[3]) {
+  float4 C[3], W[3];
   for (int k = 0; k < 3; k++) {
-    N[k] = a.normal[v[k]];
     C[k] = a.color[v[k]];
     W[k] = a.world[v[k]];
   }
@@ -429,11 +409,9 @@ __device__ void shade_smooth(const FrameArgs &a, const DrawRec &d, const uint32_
               pc[0] * W[0].y + pc[1] * W[1].y + pc[2] * W[2].y,
               pc[0] * W[0].z + pc[1] * W[1].z + pc[2] * W[2].z);
   V3 vdir = norm3(sub3(mk3(d.cam_eye[0], d.cam_eye[1], d.cam_eye[2]), wp));
-  const LightRec *Ls = a.lights + d.light_off;
   float lit[3], spec[3];
-  diffuse_rgb(n, wp, Ls, d.light_count, d.ambient, lit);
-  specular_ggx(n, wp, vdir, Ls, d.light_count, d.roughness, d.metallic, base, spec);
-  float ds = 1.0f - d.metallic;
+  lights_smooth(n, wp, vdir, Ls, d, base, lit, spec);
+  const float ds = d.diffuse_scale;
   float env[3] = {0.0f, 0.0f, 0.0f}, irr[3] = {0.0f, 0.0f, 0.0f};
   bool has_irr = a.irr != nullptr;
   if (has_irr)
@@ -446,11 +424,11 @@ __device__ void shade_smooth(const FrameArgs &a, const DrawRec &d, const uint32_
       ndv = 0.0f;
     float f0[3];
     for (int c = 0; c < 3; c++)
-      f0[c] = 0.04f * (1.0f - d.metallic) + base[c] * d.metallic;
+      f0[c] = d.f0_dielectric + base[c] * d.metallic;
     if (a.pf != nullptr && a.brdf != nullptr) {
       float pf[3], bs, bb;
-      ibl_pf(a, refl, d.roughness, pf);
-      ibl_lut(a, ndv, d.roughness, &bs, &bb);
+      ibl_pf(a, d, refl, pf);
+      ibl_lut(a, d, ndv, &bs, &bb);
       for (int c = 0; c < 3; c++)
         env[c] = pf[c] * (f0[c] * bs + bb);
     } else if (d.metallic > 0.01f) { /* hemisphere fallback, :2042-2072 */
@@ -655,22 +633,95 @@ __device__ __forceinline__ uint32_t warp_alloc1(uint32_t *counter) {
   return base + (uint32_t)__popc(mask & ((1u << lane) - 1u));
 }
 
+__device__ __forceinline__ bool rec_live(const RasterRec &r, int W, int H) {
+  int y1 = (int)(r.y1 & 0x7fffu);
+  /* live records always lie inside the framebuffer; anything else is dead
+   * or an unwritten slot of an overflowed frame (which the host re-runs) */
+  return (int)r.x0 <= (int)r.x1 && (int)r.y0 <= y1 && (int)r.x1 < W && y1 < H;
+}
+
+__device__ __forceinline__ bool rec_large(const RasterRec &r) {
+  int w = (int)r.x1 - (int)r.x0 + 1, h = (int)(r.y1 & 0x7fffu) - (int)r.y0 + 1;
+  return w > SMALL_MAX_SIDE || h > SMALL_MAX_SIDE || w * h > SMALL_MAX_AREA;
+}
+
+__device__ __forceinline__ uint32_t rec_items(const RasterRec &r) {
+  uint32_t w = (uint32_t)r.x1 - (uint32_t)r.x0 + 1u;
+  uint32_t h = (uint32_t)(r.y1 & 0x7fffu) - (uint32_t)r.y0 + 1u;
+  return h * ((w + RASTER_CHUNK - 1u) / RASTER_CHUNK);
+}
+
+/* Queue a large record for item-parallel rasterisation. */
+__device__ __forceinline__ void push_large(const FrameArgs &a, uint32_t rid, const RasterRec &r) {
+  uint32_t q = atomicAdd(&a.ctr->large_count, 1u);
+  if (q < a.large_cap) {
+    a.large_list[q] = rid;
+    a.large_items[q] = rec_items(r);
+  } else {
+    atomicOr(&a.ctr->overflow, 8u);
+  }
+}
+
+/* Block-aggregated allocation: every thread of the block calls this with
+ * two 0/1 requests; one atomicAdd per counter per block hands out slots in
+ * thread order. */
+__device__ __forceinline__ void block_alloc2(uint32_t *ca, bool fa, uint32_t *cb, bool fb,
+                                             uint32_t &sa, uint32_t &sb) {
+  __shared__ uint32_t wa[32], wb[32], base_a, base_b;
+  const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+  const uint32_t nw = (blockDim.x + 31u) >> 5;
+  const uint32_t ba = __ballot_sync(0xffffffffu, fa), bb = __ballot_sync(0xffffffffu, fb);
+  if (lane == 0) {
+    wa[warp] = (uint32_t)__popc(ba);
+    wb[warp] = (uint32_t)__popc(bb);
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    uint32_t ta = 0, tb = 0;
+    for (uint32_t w = 0; w < nw; w++) {
+      uint32_t x = wa[w], y = wb[w];
+      wa[w] = ta;
+      wb[w] = tb;
+      ta += x;
+      tb += y;
+    }
+    base_a = ta ? atomicAdd(ca, ta) : 0u;
+    base_b = tb ? atomicAdd(cb, tb) : 0u;
+  }
+  __syncthreads();
+  const uint32_t lt = (1u << lane) - 1u;
+  sa = base_a + wa[warp] + (uint32_t)__popc(ba & lt);
+  sb = base_b + wb[warp] + (uint32_t)__popc(bb & lt);
+}
+
+/* Marks slot t dead (or as a redirect to clipped fan records) with one
+ * 16-byte store of the record's tail (inv_area, order, bbox). */
+__device__ __forceinline__ void write_rec_tail(RasterRec *slot, uint32_t order, uint16_t y0) {
+  uint4 tail;
+  tail.x = 0u;                        /* inv_area */
+  tail.y = order;
+  tail.z = 1u | ((uint32_t)y0 << 16); /* x0 = 1, y0 */
+  tail.w = 0u;                        /* x1 = 0 < x0: never rasterised */
+  reinterpret_cast<uint4 *>(slot)[3] = tail;
+}
+
 /* k_setup — one thread per triangle (mop_sw_rasterize_triangle_full
- * rasterizer.c:2458-2530 up to the fan loop). */
-__global__ void k_setup(FrameArgs a) {
-  uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+ * rasterizer.c:2458-2530 up to the fan loop).  Slot t of the record arrays
+ * belongs to triangle t. */
+__global__ void __launch_bounds__(256) k_setup(FrameArgs a) {
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= a.total_tris)
     return;
   const DrawRec &d = a.draws[find_draw_by(a.draws, a.draw_count, t, false)];
-  uint32_t lt = t - d.tbase;
-  uint32_t i0 = __ldg(d.ibuf + 3u * lt), i1 = __ldg(d.ibuf + 3u * lt + 1u),
-           i2 = __ldg(d.ibuf + 3u * lt + 2u);
-  bool alive = !(i0 >= d.vertex_count || i1 >= d.vertex_count || i2 >= d.vertex_count);
+  const uint32_t lt = t - d.tbase;
+  const uint32_t i0 = __ldg(d.ibuf + 3u * lt), i1 = __ldg(d.ibuf + 3u * lt + 1u),
+                 i2 = __ldg(d.ibuf + 3u * lt + 2u);
   int status = 0; /* 0 dead, 1 single fan triangle, 2 needs clipping */
-  uint32_t g[3] = {d.vbase + i0, d.vbase + i1, d.vbase + i2};
-  CV v[3];
-  if (alive) {
-    float4 A = a.clip[g[0]], B = a.clip[g[1]], C = a.clip[g[2]];
+  RasterRec rr;
+  ShadeRec sr;
+  if (!(i0 >= d.vertex_count || i1 >= d.vertex_count || i2 >= d.vertex_count)) {
+    const uint32_t g[3] = {d.vbase + i0, d.vbase + i1, d.vbase + i2};
+    const float4 A = a.clip[g[0]], B = a.clip[g[1]], C = a.clip[g[2]];
     if (!outside_same_plane(A, B, C)) {
       bool culled = false;
       if ((d.flags & DF_CULL) && A.w > 0.0f && B.w > 0.0f && C.w > 0.0f) {
@@ -682,44 +733,38 @@ __global__ void k_setup(FrameArgs a) {
       }
       if (!culled) {
         if (A.w > 0.0f && B.w > 0.0f && C.w > 0.0f && inside_all(A) && inside_all(B) &&
-            inside_all(C))
-          status = 1;
-        else
+            inside_all(C)) {
+          CV v[3];
+          if (d.flags & DF_SMOOTH) { /* smooth records reference the vertex streams */
+            v[0].p = A;
+            v[1].p = B;
+            v[2].p = C;
+          } else { /* flat needs normals, colours and positions for its colour */
+            for (int k = 0; k < 3; k++)
+              v[k] = load_cv(a, g[k]);
+          }
+          status = fan_setup(a, d, v, g, t << ORDER_FAN_BITS, rr, sr) ? 1 : 0;
+        } else {
           status = 2;
+        }
       }
     }
   }
-  RasterRec rr;
-  ShadeRec sr;
   if (status == 1) {
-    for (int k = 0; k < 3; k++)
-      v[k] = load_cv(a, g[k]);
-    if (!fan_setup(a, d, v, g, t << ORDER_FAN_BITS, rr, sr))
-      status = 0;
-  }
-  if (status == 2) {
+    a.rrec[t] = rr;
+    a.srec[t] = sr;
+    if (rec_large(rr))
+      push_large(a, t, rr);
+  } else if (status == 2) {
+    write_rec_tail(&a.rrec[t], 0u, REC_REDIRECT); /* k_clip fills in the target */
     uint32_t q = warp_alloc1(&a.ctr->clip_count);
-    if (q < a.clip_cap) {
+    if (q < a.clip_cap)
       a.clipq[q] = t;
-    } else {
+    else
       atomicOr(&a.ctr->overflow, 4u);
-    }
-    a.rec_base[t] = REC_DEAD; /* k_clip overwrites it */
-    return;
+  } else {
+    write_rec_tail(&a.rrec[t], 0u, 0u);
   }
-  if (status == 1) {
-    uint32_t r = warp_alloc1(&a.ctr->rec_count);
-    if (r < a.rec_cap) {
-      a.rrec[r] = rr;
-      a.srec[r] = sr;
-      a.rec_base[t] = r;
-    } else {
-      atomicOr(&a.ctr->overflow, 1u);
-      a.rec_base[t] = REC_DEAD;
-    }
-    return;
-  }
-  a.rec_base[t] = REC_DEAD;
 }
 
 /* Sutherland-Hodgman (rasterizer.c:514-626) on the triangles queued by
@@ -791,24 +836,21 @@ __global__ void k_clip(FrameArgs a) {
       src = dst;
       dst = tmp;
     }
-    if (cnt < 3) {
-      a.rec_base[t] = REC_DEAD;
-      continue;
-    }
+    if (cnt < 3)
+      continue; /* slot t stays a redirect that no fragment references */
     /* store the polygon's vertices, then one record per fan triangle */
     uint32_t e = atomicAdd(&a.ctr->extra_vertices, (uint32_t)cnt);
     uint32_t nf = (uint32_t)cnt - 2u;
-    uint32_t r = atomicAdd(&a.ctr->rec_count, nf);
+    uint32_t r = a.total_tris + atomicAdd(&a.ctr->rec_count, nf);
     if (a.total_vertices + e + (uint32_t)cnt > a.vertex_cap || r + nf > a.rec_cap) {
       atomicOr(&a.ctr->overflow, (a.total_vertices + e + (uint32_t)cnt > a.vertex_cap) ? 2u : 1u);
-      a.rec_base[t] = REC_DEAD;
       continue;
     }
     uint32_t vs = a.total_vertices + e;
     for (int k = 0; k < cnt; k++) {
       const CV &c = src[k];
       a.clip[vs + k] = c.p;
-      a.normal[vs + k] = make_float4(c.n.x, c.n.y, c.n.z, 0.0f);
+      a.normal[vs + k] = make_float4(c.n.x, c.n.y, c.n.z, 1.0f / c.p.w);
       a.world[vs + k] = make_float4(c.wp.x, c.wp.y, c.wp.z, 0.0f);
       a.color[vs + k] = make_float4(c.c[0], c.c[1], c.c[2], c.c[3]);
     }
@@ -824,54 +866,82 @@ __global__ void k_clip(FrameArgs a) {
       }
       a.rrec[r + i - 1] = rr;
       a.srec[r + i - 1] = sr;
+      if (rec_live(rr, a.width, a.height) && rec_large(rr))
+        push_large(a, r + (uint32_t)i - 1u, rr);
     }
-    a.rec_base[t] = r;
+    write_rec_tail(&a.rrec[t], r, REC_REDIRECT);
   }
 }
 
 /* ------------------------------------------------------------------------
- * screen-tile binning
+ * visibility: every fragment of every live record does a 64-bit atomicMin
+ * of (depth_key << 32 | submission order) into the per-sample key buffer.
+ * The minimum is the fragment the reference keeps: nearest depth, and on an
+ * exact tie the earliest submitted (strict `z < depth`, rasterizer.c:1960).
  * ------------------------------------------------------------------------ */
-__device__ __forceinline__ bool rec_tiles(const FrameArgs &a, const RasterRec &r, int &tx0, int &ty0,
-                                          int &tx1, int &ty1) {
-  int y1 = (int)(r.y1 & 0x7fffu);
-  if ((int)r.x0 > (int)r.x1 || (int)r.y0 > y1)
-    return false;
-  /* live records always lie inside the framebuffer; anything else is an
-   * unwritten slot of an overflowed frame (which the host re-runs) */
-  if ((int)r.x1 >= a.width || y1 >= a.height)
-    return false;
-  tx0 = (int)r.x0 >> a.tile_shift;
-  tx1 = (int)r.x1 >> a.tile_shift;
-  ty0 = (int)r.y0 >> a.tile_shift;
-  ty1 = y1 >> a.tile_shift;
-  return true;
-}
-
-__global__ void k_bin_count(FrameArgs a) {
-  uint32_t n = a.ctr->rec_count;
-  if (n > a.rec_cap)
-    n = a.rec_cap;
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    RasterRec r = a.rrec[i];
-    int tx0, ty0, tx1, ty1;
-    if (!rec_tiles(a, r, tx0, ty0, tx1, ty1))
-      continue;
-    for (int ty = ty0; ty <= ty1; ty++)
-      for (int tx = tx0; tx <= tx1; tx++)
-        atomicAdd(&a.tile_count[ty * a.tiles_x + tx], 1u);
+/* Walk samples [xs, xe] of row y of record r, starting from edge values
+ * w0..w2 (and flat depth z) already folded to (y, xs). */
+__device__ __forceinline__ void raster_span(const FrameArgs &a, const RasterRec &r, bool flat, int y,
+                                            int xs, int xe, float w0, float w1, float w2, float z) {
+  unsigned long long *row = a.keys + (size_t)y * (size_t)a.width;
+  bool seen = false;
+  for (int x = xs; x <= xe; x++) {
+    if (w0 >= 0.0f && w1 >= 0.0f && w2 >= 0.0f) {
+      seen = true;
+      float zz = z;
+      if (!flat) {
+        float b0 = w0 * r.inv_area, b1 = w1 * r.inv_area, b2 = w2 * r.inv_area;
+        zz = b0 * r.zc[0] + b1 * r.zc[1] + b2 * r.zc[2];
+      }
+      if (zz < 1.0f)
+        atomicMin(row + x, ((unsigned long long)depth_key(zz) << 32) | (unsigned long long)r.order);
+    } else if (seen) {
+      break; /* edge values are monotone along a row: coverage has ended */
+    }
+    w0 = __fadd_rn(w0, r.dx[0]);
+    w1 = __fadd_rn(w1, r.dx[1]);
+    w2 = __fadd_rn(w2, r.dx[2]);
+    if (flat)
+      z = __fadd_rn(z, r.zc[1]);
   }
 }
 
-/* Exclusive scan of the per-tile counts; one block of 1024 threads. */
-__global__ void k_bin_scan(FrameArgs a) {
+/* Small records: one thread walks the whole (<= 128-sample) bbox, row by
+ * row, exactly as the reference's loops step (rasterizer.c:1926-2151). */
+__global__ void k_raster_small(FrameArgs a) {
+  uint32_t n = a.total_tris + a.ctr->rec_count;
+  if (n > a.rec_cap)
+    n = a.rec_cap;
+  for (uint32_t rid = blockIdx.x * blockDim.x + threadIdx.x; rid < n;
+       rid += gridDim.x * blockDim.x) {
+    const RasterRec r = a.rrec[rid];
+    if (!rec_live(r, a.width, a.height) || rec_large(r))
+      continue;
+    const bool flat = (r.y1 & REC_FLAT_BIT) != 0;
+    const int y1 = (int)(r.y1 & 0x7fffu);
+    float wr0 = r.w0[0], wr1 = r.w0[1], wr2 = r.w0[2], zr = r.zc[0];
+    for (int y = (int)r.y0; y <= y1; y++) {
+      raster_span(a, r, flat, y, (int)r.x0, (int)r.x1, wr0, wr1, wr2, zr);
+      wr0 = __fadd_rn(wr0, r.dy[0]);
+      wr1 = __fadd_rn(wr1, r.dy[1]);
+      wr2 = __fadd_rn(wr2, r.dy[2]);
+      if (flat)
+        zr = __fadd_rn(zr, r.zc[2]);
+    }
+  }
+}
+
+/* Exclusive scan of the large records' item counts (one block). */
+__global__ void k_large_scan(FrameArgs a) {
   __shared__ uint32_t part[1024];
-  int n = a.tiles_x * a.tiles_y;
-  int per = (n + 1023) / 1024;
-  int b = threadIdx.x * per, e = min(b + per, n);
+  uint32_t n = a.ctr->large_count;
+  if (n > a.large_cap)
+    n = a.large_cap;
+  uint32_t per = (n + 1023u) / 1024u;
+  uint32_t b = threadIdx.x * per, e = min(b + per, n);
   uint32_t s = 0;
-  for (int i = b; i < e; i++)
-    s += a.tile_count[i];
+  for (uint32_t i = b; i < e; i++)
+    s += a.large_items[i];
   part[threadIdx.x] = s;
   __syncthreads();
   for (int o = 1; o < 1024; o <<= 1) {
@@ -881,39 +951,57 @@ __global__ void k_bin_scan(FrameArgs a) {
     __syncthreads();
   }
   uint32_t run = threadIdx.x ? part[threadIdx.x - 1] : 0u;
-  for (int i = b; i < e; i++) {
-    a.tile_off[i] = run;
-    run += a.tile_count[i];
+  for (uint32_t i = b; i < e; i++) {
+    uint32_t c = a.large_items[i];
+    a.large_items[i] = run;
+    run += c;
   }
-  if (threadIdx.x == 1023) {
-    a.ctr->bin_total = part[1023];
-    if (part[1023] > a.bin_cap)
-      atomicOr(&a.ctr->overflow, 8u);
-  }
+  if (threadIdx.x == 1023)
+    a.ctr->large_items = part[1023];
 }
 
-__global__ void k_bin_fill(FrameArgs a) {
-  uint32_t n = a.ctr->rec_count;
-  if (n > a.rec_cap)
-    n = a.rec_cap;
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    RasterRec r = a.rrec[i];
-    int tx0, ty0, tx1, ty1;
-    if (!rec_tiles(a, r, tx0, ty0, tx1, ty1))
+/* Large records: one thread per (row, RASTER_CHUNK-sample chunk); the edge
+ * values at the chunk start come from the exact fold. */
+__global__ void k_raster_large(FrameArgs a) {
+  uint32_t nl = a.ctr->large_count;
+  if (nl > a.large_cap)
+    nl = a.large_cap;
+  const uint32_t total = a.ctr->large_items;
+  for (uint32_t it = blockIdx.x * blockDim.x + threadIdx.x; it < total;
+       it += gridDim.x * blockDim.x) {
+    uint32_t lo = 0, hi = nl; /* last record with offset <= it */
+    while (hi - lo > 1) {
+      uint32_t mid = (lo + hi) >> 1;
+      if (a.large_items[mid] <= it)
+        lo = mid;
+      else
+        hi = mid;
+    }
+    const uint32_t rid = a.large_list[lo];
+    if (rid >= a.rec_cap)
       continue;
-    for (int ty = ty0; ty <= ty1; ty++)
-      for (int tx = tx0; tx <= tx1; tx++) {
-        int tile = ty * a.tiles_x + tx;
-        uint32_t pos = a.tile_off[tile] + atomicAdd(&a.tile_fill[tile], 1u);
-        if (pos < a.bin_cap)
-          a.bins[pos] = i;
-      }
+    const RasterRec r = a.rrec[rid];
+    if (!rec_live(r, a.width, a.height))
+      continue;
+    const bool flat = (r.y1 & REC_FLAT_BIT) != 0;
+    const uint32_t w = (uint32_t)r.x1 - (uint32_t)r.x0 + 1u;
+    const uint32_t chunks = (w + RASTER_CHUNK - 1u) / RASTER_CHUNK;
+    const uint32_t local = it - a.large_items[lo];
+    const int jr = (int)(local / chunks), kc = (int)((local % chunks) * RASTER_CHUNK);
+    const int y = (int)r.y0 + jr;
+    if (y > (int)(r.y1 & 0x7fffu))
+      continue;
+    const int xs = (int)r.x0 + kc, xe = min((int)r.x1, xs + RASTER_CHUNK - 1);
+    float w0 = fold_add(fold_add(r.w0[0], r.dy[0], jr), r.dx[0], kc);
+    float w1 = fold_add(fold_add(r.w0[1], r.dy[1], jr), r.dx[1], kc);
+    float w2 = fold_add(fold_add(r.w0[2], r.dy[2], jr), r.dx[2], kc);
+    float z = flat ? fold_add(fold_add(r.zc[0], r.zc[2], jr), r.zc[1], kc) : 0.0f;
+    raster_span(a, r, flat, y, xs, xe, w0, w1, w2, z);
   }
 }
 
 /* ------------------------------------------------------------------------
- * k_tile — per screen tile: visibility into shared memory, then deferred
- * shading + ACES resolve of every sample of the tile.
+ * resolve and shading
  * ------------------------------------------------------------------------ */
 __device__ __forceinline__ float aces(float x) { /* rasterizer.c:2770-2774 */
   float a = 2.51f, b = 0.03f, c = 2.43f, d = 0.59f, e = 0.14f;
@@ -921,300 +1009,317 @@ __device__ __forceinline__ float aces(float x) { /* rasterizer.c:2770-2774 */
   return m < 0.0f ? 0.0f : (m > 1.0f ? 1.0f : m);
 }
 
-template <int TS>
-__global__ void __launch_bounds__(TS *TS) k_tile(FrameArgs a) {
-  constexpr int NT = TS * TS;
-  __shared__ unsigned long long key[NT];
-  __shared__ uint32_t s_rec[NT];
-  __shared__ uint32_t s_scan[NT + 1];
-  __shared__ uint32_t s_warp[NT / 32];
-  __shared__ int s_tile;
-  const int tid = threadIdx.x;
-  const int ntiles = a.tiles_x * a.tiles_y;
-  for (;;) {
-    if (tid == 0)
-      s_tile = (int)atomicAdd(&a.ctr->tile_cursor, 1u);
-    key[tid] = KEY_EMPTY;
+/* Writes the background (clear colour resolved with id 0 and depth 1,
+ * rasterizer.c:2785-2792) to every sample with 16-byte stores — k_shade
+ * overwrites the covered ones — and queues covered samples for shading in
+ * sample order (each thread owns 8 consecutive samples; one atomicAdd per
+ * block iteration).  Blocks of 256 threads. */
+#define RESOLVE_PER_THREAD 8
+
+__global__ void __launch_bounds__(256) k_resolve(FrameArgs a) {
+  __shared__ uint32_t s_warp[8];
+  __shared__ uint32_t s_base;
+  const uint32_t S = (uint32_t)a.width * (uint32_t)a.height;
+  const uchar4 bg = make_uchar4(x86_f2u8(fminf(a.clear[0], 1.0f) * 255.0f + 0.5f),
+                                x86_f2u8(fminf(a.clear[1], 1.0f) * 255.0f + 0.5f),
+                                x86_f2u8(fminf(a.clear[2], 1.0f) * 255.0f + 0.5f), 255);
+  const uint32_t bgw = (uint32_t)bg.x | ((uint32_t)bg.y << 8) | ((uint32_t)bg.z << 16) |
+                       ((uint32_t)bg.w << 24);
+  const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+  const uint32_t per_iter = 256u * RESOLVE_PER_THREAD;
+  for (uint32_t blk = blockIdx.x * per_iter; blk < S; blk += gridDim.x * per_iter) {
+    const uint32_t i0 = blk + threadIdx.x * RESOLVE_PER_THREAD;
+    uint32_t mask = 0;
+    if (i0 + RESOLVE_PER_THREAD <= S) {
+      const ulonglong2 *kp = reinterpret_cast<const ulonglong2 *>(a.keys + i0);
+#pragma unroll
+      for (int k = 0; k < RESOLVE_PER_THREAD / 2; k++) {
+        const ulonglong2 v = kp[k];
+        if (v.x != KEY_EMPTY)
+          mask |= 1u << (2 * k);
+        if (v.y != KEY_EMPTY)
+          mask |= 1u << (2 * k + 1);
+      }
+      const uint4 c4 = make_uint4(bgw, bgw, bgw, bgw);
+      const float4 d4 = make_float4(1.0f, 1.0f, 1.0f, 1.0f);
+      const uint4 z4 = make_uint4(0u, 0u, 0u, 0u);
+      uint4 *pc = reinterpret_cast<uint4 *>(a.pre + i0);
+      float4 *pd = reinterpret_cast<float4 *>(a.depth + i0);
+      uint4 *pi = reinterpret_cast<uint4 *>(a.ids + i0);
+      pc[0] = c4;
+      pc[1] = c4;
+      pd[0] = d4;
+      pd[1] = d4;
+      pi[0] = z4;
+      pi[1] = z4;
+    } else {
+      for (int k = 0; k < RESOLVE_PER_THREAD; k++) {
+        const uint32_t i = i0 + (uint32_t)k;
+        if (i < S) {
+          if (a.keys[i] != KEY_EMPTY)
+            mask |= 1u << k;
+          a.pre[i] = bg;
+          a.depth[i] = 1.0f;
+          a.ids[i] = 0u;
+        }
+      }
+    }
+    const uint32_t c = (uint32_t)__popc(mask);
+    uint32_t incl = c;
+    for (int o = 1; o < 32; o <<= 1) {
+      uint32_t v = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= (uint32_t)o)
+        incl += v;
+    }
+    if (lane == 31)
+      s_warp[warp] = incl;
     __syncthreads();
-    const int tile = s_tile;
-    if (tile >= ntiles)
-      break;
-    const int tx0 = (tile % a.tiles_x) * TS, ty0 = (tile / a.tiles_x) * TS;
-    uint32_t beg = a.tile_off[tile], cnt = a.tile_count[tile];
-    if (beg >= a.bin_cap)
-      cnt = 0;
-    else if (cnt > a.bin_cap - beg)
-      cnt = a.bin_cap - beg;
-    /* ---- visibility ---- */
-    for (uint32_t base = 0; base < cnt; base += NT) {
-      uint32_t i = base + (uint32_t)tid;
-      uint32_t rows = 0, rid = 0;
-      if (i < cnt) {
-        rid = a.bins[beg + i];
-        if (rid >= a.rec_cap)
-          rid = 0; /* defensive: only reachable in an overflowed frame */
-        const RasterRec &r = a.rrec[rid];
-        int ry0 = max((int)r.y0, ty0), ry1 = min((int)(r.y1 & 0x7fffu), ty0 + TS - 1);
-        int rx0 = max((int)r.x0, tx0), rx1 = min((int)r.x1, tx0 + TS - 1);
-        if (ry0 <= ry1 && rx0 <= rx1)
-          rows = (uint32_t)(ry1 - ry0 + 1);
+    if (threadIdx.x == 0) {
+      uint32_t run = 0;
+      for (int w = 0; w < 8; w++) {
+        uint32_t x = s_warp[w];
+        s_warp[w] = run;
+        run += x;
       }
-      s_rec[tid] = rid;
-      /* block exclusive scan of rows */
-      uint32_t incl = rows;
-      for (int o = 1; o < 32; o <<= 1) {
-        uint32_t v = __shfl_up_sync(0xffffffffu, incl, o);
-        if ((tid & 31) >= o)
-          incl += v;
-      }
-      if ((tid & 31) == 31)
-        s_warp[tid >> 5] = incl;
-      __syncthreads();
-      if (tid < 32) {
-        uint32_t wv = tid < NT / 32 ? s_warp[tid] : 0u;
-        for (int o = 1; o < 32; o <<= 1) {
-          uint32_t v = __shfl_up_sync(0xffffffffu, wv, o);
-          if (tid >= o)
-            wv += v;
-        }
-        if (tid < NT / 32)
-          s_warp[tid] = wv;
-      }
-      __syncthreads();
-      uint32_t excl = incl - rows + ((tid >> 5) ? s_warp[(tid >> 5) - 1] : 0u);
-      s_scan[tid] = excl;
-      if (tid == NT - 1)
-        s_scan[NT] = excl + rows;
-      __syncthreads();
-      const uint32_t total = s_scan[NT];
-      for (uint32_t it = (uint32_t)tid; it < total; it += NT) {
-        /* item -> (record, row): last j with s_scan[j] <= it */
-        int lo = 0, hi = NT;
-        while (hi - lo > 1) {
-          int mid = (lo + hi) >> 1;
-          if (s_scan[mid] <= it)
-            lo = mid;
-          else
-            hi = mid;
-        }
-        const RasterRec r = a.rrec[s_rec[lo]];
-        const bool flat = (r.y1 & REC_FLAT_BIT) != 0;
-        const int ry0 = max((int)r.y0, ty0);
-        const int y = ry0 + (int)(it - s_scan[lo]);
-        const int xs = max((int)r.x0, tx0), xe = min((int)r.x1, tx0 + TS - 1);
-        const int jr = y - (int)r.y0, kc = xs - (int)r.x0;
-        float w0 = fold_add(fold_add(r.w0[0], r.dy[0], jr), r.dx[0], kc);
-        float w1 = fold_add(fold_add(r.w0[1], r.dy[1], jr), r.dx[1], kc);
-        float w2 = fold_add(fold_add(r.w0[2], r.dy[2], jr), r.dx[2], kc);
-        float z = 0.0f;
-        if (flat)
-          z = fold_add(fold_add(r.zc[0], r.zc[2], jr), r.zc[1], kc);
-        bool seen = false;
-        for (int x = xs; x <= xe; x++) {
-          if (w0 >= 0.0f && w1 >= 0.0f && w2 >= 0.0f) {
-            seen = true;
-            float zz = z;
-            if (!flat) {
-              float b0 = w0 * r.inv_area, b1 = w1 * r.inv_area, b2 = w2 * r.inv_area;
-              zz = b0 * r.zc[0] + b1 * r.zc[1] + b2 * r.zc[2];
-            }
-            if (zz < 1.0f) {
-              unsigned long long k =
-                  ((unsigned long long)depth_key(zz) << 32) | (unsigned long long)r.order;
-              atomicMin(&key[(y - ty0) * TS + (x - tx0)], k);
-            }
-          } else if (seen) {
-            break; /* edge values are monotone along a row: coverage ended */
-          }
-          w0 = __fadd_rn(w0, r.dx[0]);
-          w1 = __fadd_rn(w1, r.dx[1]);
-          w2 = __fadd_rn(w2, r.dx[2]);
-          if (flat)
-            z = __fadd_rn(z, r.zc[1]);
-        }
-      }
-      __syncthreads();
+      s_base = run ? atomicAdd(&a.ctr->shade_count, run) : 0u;
     }
-    /* ---- shading + resolve of sample `tid` ---- */
-    const int x = tx0 + (tid % TS), y = ty0 + (tid / TS);
-    if (x < a.width && y < a.height) {
-      const size_t px = (size_t)y * (size_t)a.width + (size_t)x;
-      const unsigned long long k = key[tid];
-      uchar4 out;
-      float depth = 1.0f;
-      uint32_t oid = 0;
-      uint32_t rid = 0xffffffffu;
-      if (k != KEY_EMPTY) {
-        const uint32_t t = (uint32_t)k >> ORDER_FAN_BITS;
-        if (t < a.total_tris) {
-          const uint32_t rb = a.rec_base[t];
-          if (rb != REC_DEAD)
-            rid = rb + ((uint32_t)k & ((1u << ORDER_FAN_BITS) - 1u));
-        }
-        if (rid >= a.rec_cap)
-          rid = 0xffffffffu; /* overflowed frame: the host discards it */
-      }
-      if (rid == 0xffffffffu) {
-        /* background: clear colour, id 0 (rasterizer.c:2785-2792) */
-        out.x = x86_f2u8(fminf(a.clear[0], 1.0f) * 255.0f + 0.5f);
-        out.y = x86_f2u8(fminf(a.clear[1], 1.0f) * 255.0f + 0.5f);
-        out.z = x86_f2u8(fminf(a.clear[2], 1.0f) * 255.0f + 0.5f);
-        out.w = 255;
-      } else {
-        const RasterRec r = a.rrec[rid];
-        const ShadeRec s = a.srec[rid];
-        const DrawRec &d = a.draws[s.draw < a.draw_count ? s.draw : 0];
-        const int jr = y - (int)r.y0, kc = x - (int)r.x0;
-        float hdr[3];
-        if (r.y1 & REC_FLAT_BIT) {
-          depth = fold_add(fold_add(r.zc[0], r.zc[2], jr), r.zc[1], kc);
-          hdr[0] = s.col[0];
-          hdr[1] = s.col[1];
-          hdr[2] = s.col[2];
-        } else if (s.v[0] >= a.vertex_cap || s.v[1] >= a.vertex_cap || s.v[2] >= a.vertex_cap) {
-          hdr[0] = hdr[1] = hdr[2] = 0.0f; /* unreachable for live records */
-        } else {
-          float w[3];
-          for (int e = 0; e < 3; e++)
-            w[e] = fold_add(fold_add(r.w0[e], r.dy[e], jr), r.dx[e], kc);
-          float b0 = w[0] * r.inv_area, b1 = w[1] * r.inv_area, b2 = w[2] * r.inv_area;
-          depth = b0 * r.zc[0] + b1 * r.zc[1] + b2 * r.zc[2];
-          float iw0 = 1.0f / a.clip[s.v[0]].w, iw1 = 1.0f / a.clip[s.v[1]].w,
-                iw2 = 1.0f / a.clip[s.v[2]].w;
-          float pc[3] = {b0 * iw0, b1 * iw1, b2 * iw2};
-          float ip = 1.0f / (pc[0] + pc[1] + pc[2]);
-          pc[0] *= ip;
-          pc[1] *= ip;
-          pc[2] *= ip;
-          shade_smooth(a, d, s.v, pc, hdr);
-        }
-        oid = d.object_id;
-        out.x = x86_f2u8(aces(hdr[0] * a.exposure) * 255.0f + 0.5f);
-        out.y = x86_f2u8(aces(hdr[1] * a.exposure) * 255.0f + 0.5f);
-        out.z = x86_f2u8(aces(hdr[2] * a.exposure) * 255.0f + 0.5f);
-        out.w = x86_f2u8(1.0f * 255.0f + 0.5f);
-      }
-      a.pre[px] = out;
-      a.depth[px] = depth;
-      a.ids[px] = oid;
-    }
+    __syncthreads();
+    uint32_t pos = s_base + s_warp[warp] + incl - c;
+    for (int k = 0; k < RESOLVE_PER_THREAD; k++)
+      if ((mask >> k) & 1u)
+        a.shade_list[pos++] = i0 + (uint32_t)k;
     __syncthreads();
   }
 }
 
-template __global__ void k_tile<16>(FrameArgs);
-template __global__ void k_tile<8>(FrameArgs);
+/* Deferred shading of one covered sample: the winning record's exact edge
+ * values at the sample (fold from the bbox corner), barycentrics, depth,
+ * perspective-correct weights, multi-light + IBL shading (smooth) or the
+ * record's constant colour (flat), then the ACES resolve. */
+#define SHADE_SMEM_LIGHTS 64
+
+/* 4 blocks of 256 per SM (64 registers): the kernel is issue-bound and the
+ * extra warps hide the dependent-latency stalls of the lighting chains. */
+__global__ void __launch_bounds__(256, 4) k_shade(FrameArgs a) {
+  __shared__ LightRec s_lights[SHADE_SMEM_LIGHTS];
+  const bool smem_lights = a.light_total <= SHADE_SMEM_LIGHTS;
+  if (smem_lights) {
+    const uint32_t words = a.light_total * (uint32_t)(sizeof(LightRec) / 4);
+    const uint32_t *src = reinterpret_cast<const uint32_t *>(a.lights);
+    uint32_t *dst = reinterpret_cast<uint32_t *>(s_lights);
+    for (uint32_t i = threadIdx.x; i < words; i += blockDim.x)
+      dst[i] = src[i];
+    __syncthreads();
+  }
+  const uint32_t n = a.ctr->shade_count;
+  for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
+    const uint32_t px = a.shade_list[j];
+    const unsigned long long k = a.keys[px];
+    const uint32_t t = (uint32_t)k >> ORDER_FAN_BITS;
+    const uint32_t fan = (uint32_t)k & ((1u << ORDER_FAN_BITS) - 1u);
+    uint32_t rid = 0xffffffffu;
+    RasterRec r;
+    if (t < a.total_tris) {
+      r = a.rrec[t];
+      if (r.y0 == REC_REDIRECT) {
+        rid = r.order + fan;
+        if (rid < a.rec_cap)
+          r = a.rrec[rid];
+        else
+          rid = 0xffffffffu;
+      } else if (fan == 0u) {
+        rid = t;
+      }
+    }
+    if (rid >= a.rec_cap) { /* overflowed frame: the host re-runs it */
+      a.pre[px] = make_uchar4(0, 0, 0, 255);
+      a.depth[px] = 1.0f;
+      a.ids[px] = 0u;
+      continue;
+    }
+    const int x = (int)(px % (uint32_t)a.width), y = (int)(px / (uint32_t)a.width);
+    const ShadeRec s = a.srec[rid];
+    const DrawRec &d = a.draws[s.draw < a.draw_count ? s.draw : 0];
+    const LightRec *Ls = smem_lights ? s_lights + d.light_off : a.lights + d.light_off;
+    const int jr = y - (int)r.y0, kc = x - (int)r.x0;
+    float hdr[3], depth;
+    if (r.y1 & REC_FLAT_BIT) {
+      depth = fold_add(fold_add(r.zc[0], r.zc[2], jr), r.zc[1], kc);
+      hdr[0] = s.col[0];
+      hdr[1] = s.col[1];
+      hdr[2] = s.col[2];
+    } else {
+      float w[3];
+      for (int e = 0; e < 3; e++)
+        w[e] = fold_add(fold_add(r.w0[e], r.dy[e], jr), r.dx[e], kc);
+      float b0 = w[0] * r.inv_area, b1 = w[1] * r.inv_area, b2 = w[2] * r.inv_area;
+      depth = b0 * r.zc[0] + b1 * r.zc[1] + b2 * r.zc[2];
+      if (s.v[0] >= a.vertex_cap || s.v[1] >= a.vertex_cap || s.v[2] >= a.vertex_cap) {
+        hdr[0] = hdr[1] = hdr[2] = 0.0f; /* unreachable for live records */
+      } else {
+        const float4 N[3] = {a.normal[s.v[0]], a.normal[s.v[1]], a.normal[s.v[2]]};
+        float pc[3] = {b0 * N[0].w, b1 * N[1].w, b2 * N[2].w}; /* .w = 1/clip.w */
+        float ip = 1.0f / (pc[0] + pc[1] + pc[2]);
+        pc[0] *= ip;
+        pc[1] *= ip;
+        pc[2] *= ip;
+        shade_smooth(a, d, Ls, s.v, N, pc, hdr);
+      }
+    }
+    a.pre[px] = make_uchar4(u8_of(aces(hdr[0] * a.exposure) * 255.0f + 0.5f),
+                            u8_of(aces(hdr[1] * a.exposure) * 255.0f + 0.5f),
+                            u8_of(aces(hdr[2] * a.exposure) * 255.0f + 0.5f), 255);
+    a.depth[px] = depth;
+    a.ids[px] = d.object_id;
+  }
+}
 
 /* ------------------------------------------------------------------------
  * k_post — FXAA (rasterizer.c:2625-2761), tonemap/gamma/vignette
- * (postprocess.c:24-116) and the SSAA box (viewport.c:3385-3411); one
- * thread per presented pixel covering its ssaa x ssaa samples.
+ * (postprocess.c:24-116) and the SSAA box (viewport.c:3385-3411).  A block
+ * of 32x8 threads owns 32x8 presented pixels: it stages their samples plus
+ * a one-sample halo (and each sample's luma) in shared memory with
+ * coalesced loads, then each thread filters its ssaa x ssaa samples.
  * ------------------------------------------------------------------------ */
+#define POST_BX 32
+#define POST_BY 8
+
 __device__ __forceinline__ float luma(uchar4 p) {
   return 0.299f * (float)p.x + 0.587f * (float)p.y + 0.114f * (float)p.z;
 }
 
-__device__ uchar4 post_sample(const PostArgs &a, const float *lut, int x, int y) {
-  const int w = a.width, h = a.height;
-  uchar4 c = a.pre[(size_t)y * w + x];
-  if ((a.effects & 16u) && w >= 3 && h >= 3 && x >= 1 && y >= 1 && x < w - 1 && y < h - 1) {
-#define PX(xx, yy) a.pre[(size_t)(yy)*w + (xx)]
-    float lM = luma(c), lN = luma(PX(x, y - 1)), lS = luma(PX(x, y + 1)), lW = luma(PX(x - 1, y)),
-          lE = luma(PX(x + 1, y));
-    float mn = lM, mx = lM;
-    if (lN < mn) mn = lN;
-    if (lS < mn) mn = lS;
-    if (lW < mn) mn = lW;
-    if (lE < mn) mn = lE;
-    if (lN > mx) mx = lN;
-    if (lS > mx) mx = lS;
-    if (lW > mx) mx = lW;
-    if (lE > mx) mx = lE;
-    float range = mx - mn;
-    if (!(range < 0.0625f * mx + 0.004f)) {
-      float lNW = luma(PX(x - 1, y - 1)), lNE = luma(PX(x + 1, y - 1)), lSW = luma(PX(x - 1, y + 1)),
-            lSE = luma(PX(x + 1, y + 1));
-      float avg = (lN + lS + lW + lE) * (2.0f / 12.0f) + (lNW + lNE + lSW + lSE) * (1.0f / 12.0f);
-      float sub = fabsf(avg - lM);
-      sub = sub / range;
-      if (sub > 1.0f)
-        sub = 1.0f;
-      sub = sub * sub * (3.0f - 2.0f * sub);
-      sub *= 0.75f;
-      float eh = fabsf(-2.0f * lW + lNW + lSW) + fabsf(-2.0f * lM + lN + lS) * 2.0f +
-                 fabsf(-2.0f * lE + lNE + lSE);
-      float ev = fabsf(-2.0f * lN + lNW + lNE) + fabsf(-2.0f * lM + lW + lE) * 2.0f +
-                 fabsf(-2.0f * lS + lSW + lSE);
-      bool horiz = eh >= ev;
-      int stx = horiz ? 0 : 1, sty = horiz ? 1 : 0;
-      float lp = horiz ? lS : lE, ln = horiz ? lN : lW;
-      float gp = fabsf(lp - lM), gn = fabsf(ln - lM);
-      int nx = x + (gp >= gn ? stx : -stx), ny = y + (gp >= gn ? sty : -sty);
-      uchar4 nb = PX(nx, ny);
-      float ib = 1.0f - sub;
-      uchar4 o = c;
-      o.x = x86_f2u8((float)c.x * ib + (float)nb.x * sub);
-      o.y = x86_f2u8((float)c.y * ib + (float)nb.y * sub);
-      o.z = x86_f2u8((float)c.z * ib + (float)nb.z * sub);
-      c = o;
-    }
-#undef PX
-  }
-  if (a.effects != 0u) {
-    float v[3] = {lut[c.x], lut[c.y], lut[c.z]};
-    if (a.effects & 4u) {
-      float cx = (float)w * 0.5f, cy = (float)h * 0.5f;
-      float maxd = sqrtf(cx * cx + cy * cy);
-      float dx = (float)x - cx, dy = (float)y - cy;
-      float dist = sqrtf(dx * dx + dy * dy) / maxd;
-      float vg = 1.0f - dist * dist * 0.5f;
-      if (vg < 0.0f)
-        vg = 0.0f;
-      for (int k = 0; k < 3; k++)
-        v[k] *= vg;
-    }
-    for (int k = 0; k < 3; k++) {
-      if (v[k] > 1.0f)
-        v[k] = 1.0f;
-      if (v[k] < 0.0f)
-        v[k] = 0.0f;
-    }
-    c.x = x86_f2u8(v[0] * 255.0f + 0.5f);
-    c.y = x86_f2u8(v[1] * 255.0f + 0.5f);
-    c.z = x86_f2u8(v[2] * 255.0f + 0.5f);
-  }
-  return c;
+/* FXAA of tile sample (i, j) from its 3x3 neighbourhood in the tile. */
+template <int TW>
+__device__ __forceinline__ uchar4 fxaa_tile(const uchar4 (*tc)[TW], const float (*tl)[TW], int i,
+                                            int j) {
+  const uchar4 c = tc[i][j];
+  const float lM = tl[i][j], lN = tl[i - 1][j], lS = tl[i + 1][j], lW = tl[i][j - 1],
+              lE = tl[i][j + 1];
+  float mn = lM, mx = lM;
+  if (lN < mn) mn = lN;
+  if (lS < mn) mn = lS;
+  if (lW < mn) mn = lW;
+  if (lE < mn) mn = lE;
+  if (lN > mx) mx = lN;
+  if (lS > mx) mx = lS;
+  if (lW > mx) mx = lW;
+  if (lE > mx) mx = lE;
+  const float range = mx - mn;
+  if (range < 0.0625f * mx + 0.004f)
+    return c;
+  const float lNW = tl[i - 1][j - 1], lNE = tl[i - 1][j + 1], lSW = tl[i + 1][j - 1],
+              lSE = tl[i + 1][j + 1];
+  const float avg =
+      (lN + lS + lW + lE) * (2.0f / 12.0f) + (lNW + lNE + lSW + lSE) * (1.0f / 12.0f);
+  float sub = fabsf(avg - lM);
+  sub = sub / range;
+  if (sub > 1.0f)
+    sub = 1.0f;
+  sub = sub * sub * (3.0f - 2.0f * sub);
+  sub *= 0.75f;
+  const float eh = fabsf(-2.0f * lW + lNW + lSW) + fabsf(-2.0f * lM + lN + lS) * 2.0f +
+                   fabsf(-2.0f * lE + lNE + lSE);
+  const float ev = fabsf(-2.0f * lN + lNW + lNE) + fabsf(-2.0f * lM + lW + lE) * 2.0f +
+                   fabsf(-2.0f * lS + lSW + lSE);
+  const bool horiz = eh >= ev;
+  const float lp = horiz ? lS : lE, ln = horiz ? lN : lW;
+  const float gp = fabsf(lp - lM), gn = fabsf(ln - lM);
+  const bool pos = gp >= gn;
+  const int ni = horiz ? (pos ? i + 1 : i - 1) : i;
+  const int nj = horiz ? j : (pos ? j + 1 : j - 1);
+  const uchar4 nb = tc[ni][nj];
+  const float ib = 1.0f - sub;
+  uchar4 o = c;
+  o.x = u8_of((float)c.x * ib + (float)nb.x * sub);
+  o.y = u8_of((float)c.y * ib + (float)nb.y * sub);
+  o.z = u8_of((float)c.z * ib + (float)nb.z * sub);
+  return o;
 }
 
-__global__ void k_post(PostArgs a) {
+template <int SF>
+__global__ void __launch_bounds__(POST_BX *POST_BY) k_post(PostArgs a) {
+  constexpr int TW = POST_BX * SF + 2, TH = POST_BY * SF + 2;
+  __shared__ uchar4 s_c[TH][TW];
+  __shared__ float s_l[TH][TW];
   __shared__ float s_lut[256];
-  for (int i = threadIdx.y * blockDim.x + threadIdx.x; i < 256; i += blockDim.x * blockDim.y)
+  __shared__ uint8_t s_lut8[256];
+  const int tid = threadIdx.y * POST_BX + threadIdx.x;
+  for (int i = tid; i < 256; i += POST_BX * POST_BY) {
     s_lut[i] = a.lut[i];
+    s_lut8[i] = a.lut8[i];
+  }
+  const int w = a.width, h = a.height;
+  const int sx0 = (int)blockIdx.x * POST_BX * SF - 1, sy0 = (int)blockIdx.y * POST_BY * SF - 1;
+  for (int i = tid; i < TW * TH; i += POST_BX * POST_BY) {
+    const int ty = i / TW, tx = i % TW;
+    const int sy = min(max(sy0 + ty, 0), h - 1), sx = min(max(sx0 + tx, 0), w - 1);
+    const uchar4 c = a.pre[(size_t)sy * w + sx];
+    s_c[ty][tx] = c;
+    s_l[ty][tx] = luma(c);
+  }
   __syncthreads();
-  const int sf = a.ssaa;
-  const int pw = a.width / sf, ph = a.height / sf;
-  int px = blockIdx.x * blockDim.x + threadIdx.x;
-  int py = blockIdx.y * blockDim.y + threadIdx.y;
+  const int pw = w / SF, ph = h / SF;
+  const int px = (int)blockIdx.x * POST_BX + (int)threadIdx.x;
+  const int py = (int)blockIdx.y * POST_BY + (int)threadIdx.y;
   if (px >= pw || py >= ph)
     return;
+  const bool fx = (a.effects & 16u) && w >= 3 && h >= 3;
   uint32_t acc[4] = {0, 0, 0, 0};
-  for (int dy = 0; dy < sf; dy++)
-    for (int dx = 0; dx < sf; dx++) {
-      int x = px * sf + dx, y = py * sf + dy;
-      uchar4 c = post_sample(a, s_lut, x, y);
-      a.out[(size_t)y * a.width + x] = c;
+#pragma unroll
+  for (int dy = 0; dy < SF; dy++)
+#pragma unroll
+    for (int dx = 0; dx < SF; dx++) {
+      const int x = px * SF + dx, y = py * SF + dy;
+      const int ti = (int)threadIdx.y * SF + dy + 1, tj = (int)threadIdx.x * SF + dx + 1;
+      uchar4 c = s_c[ti][tj];
+      if (fx && x >= 1 && y >= 1 && x < w - 1 && y < h - 1)
+        c = fxaa_tile<TW>(s_c, s_l, ti, tj);
+      if (a.effects != 0u && !(a.effects & 4u)) {
+        /* without vignette the post-process is a fixed byte map */
+        c.x = s_lut8[c.x];
+        c.y = s_lut8[c.y];
+        c.z = s_lut8[c.z];
+      } else if (a.effects != 0u) {
+        float v[3] = {s_lut[c.x], s_lut[c.y], s_lut[c.z]};
+        if (a.effects & 4u) {
+          const float cx = (float)w * 0.5f, cy = (float)h * 0.5f;
+          const float maxd = sqrtf(cx * cx + cy * cy);
+          const float ddx = (float)x - cx, ddy = (float)y - cy;
+          const float dist = sqrtf(ddx * ddx + ddy * ddy) / maxd;
+          float vg = 1.0f - dist * dist * 0.5f;
+          if (vg < 0.0f)
+            vg = 0.0f;
+          for (int k = 0; k < 3; k++)
+            v[k] *= vg;
+        }
+        for (int k = 0; k < 3; k++) {
+          if (v[k] > 1.0f)
+            v[k] = 1.0f;
+          if (v[k] < 0.0f)
+            v[k] = 0.0f;
+        }
+        c.x = u8_of(v[0] * 255.0f + 0.5f);
+        c.y = u8_of(v[1] * 255.0f + 0.5f);
+        c.z = u8_of(v[2] * 255.0f + 0.5f);
+      }
+      a.out[(size_t)y * w + x] = c;
       acc[0] += c.x;
       acc[1] += c.y;
       acc[2] += c.z;
       acc[3] += c.w;
     }
   if (a.presented) {
-    uint32_t n = (uint32_t)(sf * sf);
+    const uint32_t n = (uint32_t)(SF * SF);
     a.presented[(size_t)py * pw + px] =
         make_uchar4((uint8_t)(acc[0] / n), (uint8_t)(acc[1] / n), (uint8_t)(acc[2] / n),
                     (uint8_t)(acc[3] / n));
   }
 }
+
+template __global__ void k_post<1>(PostArgs);
+template __global__ void k_post<2>(PostArgs);
+template __global__ void k_post<3>(PostArgs);
+template __global__ void k_post<4>(PostArgs);
 
 /* SSAA box of an already post-processed buffer (read_color path). */
 __global__ void k_box(const uchar4 *src, int width, int height, int sf, uchar4 *dst) {
@@ -1267,9 +1372,10 @@ __global__ void k_pick(const uint32_t *ids, const float *depth, int width, int h
  * ------------------------------------------------------------------------ */
 static inline unsigned blocks_for(uint32_t n, unsigned bs) { return (n + bs - 1u) / bs; }
 
-int mopcuda_launch_frame(const FrameArgs &a, const PostArgs &p, int tile_size, int grid_tiles,
+int mopcuda_launch_frame(const FrameArgs &a, const PostArgs &p, const LaunchCfg &cfg,
                          cudaStream_t s, cudaEvent_t *ev) {
   int launches = 0;
+  const uint32_t S = (uint32_t)a.width * (uint32_t)a.height;
   if (ev)
     cudaEventRecord(ev[0], s);
   if (a.total_vertices) {
@@ -1285,28 +1391,55 @@ int mopcuda_launch_frame(const FrameArgs &a, const PostArgs &p, int tile_size, i
   }
   if (ev)
     cudaEventRecord(ev[2], s);
-  const uint32_t rec_grid = blocks_for(a.rec_cap < (1u << 22) ? a.rec_cap : (1u << 22), 256);
-  k_bin_count<<<rec_grid, 256, 0, s>>>(a);
-  k_bin_scan<<<1, 1024, 0, s>>>(a);
-  k_bin_fill<<<rec_grid, 256, 0, s>>>(a);
-  launches += 3;
+  cudaMemsetAsync(a.keys, 0xff, sizeof(unsigned long long) * (size_t)S, s);
+  if (a.total_tris) {
+    const int rb = cfg.raster_block > 0 ? cfg.raster_block : 128;
+    const uint32_t rec_grid = blocks_for(a.rec_cap < (1u << 22) ? a.rec_cap : (1u << 22),
+                                         (unsigned)rb);
+    k_raster_small<<<rec_grid, rb, 0, s>>>(a);
+    k_large_scan<<<1, 1024, 0, s>>>(a);
+    k_raster_large<<<cfg.num_sms * 8, 256, 0, s>>>(a);
+    launches += 3;
+  }
   if (ev)
     cudaEventRecord(ev[3], s);
-  if (tile_size == 8)
-    k_tile<8><<<grid_tiles, 64, 0, s>>>(a);
-  else
-    k_tile<16><<<grid_tiles, 256, 0, s>>>(a);
-  launches++;
+  k_resolve<<<cfg.num_sms * 8, 256, 0, s>>>(a);
   if (ev)
     cudaEventRecord(ev[4], s);
-  const int sf = p.ssaa;
-  dim3 pb(16, 16);
-  dim3 pg(blocks_for((uint32_t)(p.width / sf), 16), blocks_for((uint32_t)(p.height / sf), 16));
-  k_post<<<pg, pb, 0, s>>>(p);
-  launches++;
+  const int sb = cfg.shade_block > 0 ? cfg.shade_block : 256;
+  const int waves = cfg.shade_waves > 0 ? cfg.shade_waves : 4;
+  k_shade<<<cfg.num_sms * waves, sb, 0, s>>>(a);
+  launches += 2;
   if (ev)
     cudaEventRecord(ev[5], s);
+  const int sf = p.ssaa;
+  dim3 pb(POST_BX, POST_BY);
+  dim3 pg(blocks_for((uint32_t)(p.width / sf), POST_BX),
+          blocks_for((uint32_t)(p.height / sf), POST_BY));
+  switch (sf) {
+  case 2:
+    k_post<2><<<pg, pb, 0, s>>>(p);
+    break;
+  case 3:
+    k_post<3><<<pg, pb, 0, s>>>(p);
+    break;
+  case 4:
+    k_post<4><<<pg, pb, 0, s>>>(p);
+    break;
+  default:
+    k_post<1><<<pg, pb, 0, s>>>(p);
+    break;
+  }
+  launches++;
+  if (ev)
+    cudaEventRecord(ev[6], s);
   return launches;
+}
+
+int mopcuda_shade_occupancy(int block) {
+  int nb = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_shade, block, 0);
+  return nb > 0 ? nb : 1;
 }
 
 /* FP32 add/multiply issue peak without FMA: the denominator of the shading
@@ -1353,11 +1486,3 @@ int mopcuda_launch_pick(const uint32_t *ids, const float *depth, int width, int 
   return 1;
 }
 
-int mopcuda_tile_occupancy(int tile_size) {
-  int nb = 0;
-  if (tile_size == 8)
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_tile<8>, 64, 0);
-  else
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_tile<16>, 256, 0);
-  return nb > 0 ? nb : 1;
-}

@@ -150,18 +150,18 @@ struct MopCudaDevice {
   float exposure = 1.0f;
   uint32_t post = MOPCUDA_POST_GAMMA | MOPCUDA_POST_FXAA;
   float lut[256];
-  int tile_size = 16;
   /* IBL */
   DevArena irr, pf, brdf;
   int irr_w = 0, irr_h = 0, pf_w = 0, pf_h = 0, pf_levels = 0, brdf_size = 0;
   float ibl_rot = 0.0f, ibl_int = 1.0f;
   bool ibl_on = false;
   /* frame arenas */
-  DevArena d_draws, d_lights, clip, world, normal, color, rec_base, rrec, srec, clipq, tile_count,
-      tile_off, tile_fill, bins, counters, pick_xy, pick_out;
+  DevArena d_draws, d_lights, clip, world, normal, color, rrec, srec, clipq, keys,
+      large_list, large_items, shade_list, counters, pick_xy, pick_out;
   HostArena h_draws, h_lights, h_counters, h_pick;
-  uint32_t vertex_cap = 0, rec_cap = 0, clip_cap = 0, bin_cap = 0;
-  uint32_t extra_hint = 0, rec_hint = 0, clip_hint = 0, bin_hint = 0;
+  uint32_t vertex_cap = 0, rec_cap = 0, clip_cap = 0, large_cap = 0;
+  uint32_t extra_hint = 0, rec_hint = 0, clip_hint = 0, large_hint = 0;
+  LaunchCfg cfg = {148, 128, 256, 4, 32, 4};
   uint64_t launches = 0;
   float last_ms = 0.0f;
   uint64_t io_h2d = 0, io_d2h = 0; /* bytes moved by the last frame launch */
@@ -206,6 +206,7 @@ extern "C" MopCudaDevice *mopcuda_device_create(int ordinal) {
   MopCudaDevice *d = new MopCudaDevice();
   d->ordinal = ordinal;
   cudaDeviceGetAttribute(&d->num_sms, cudaDevAttrMultiProcessorCount, ordinal);
+  d->cfg.num_sms = d->num_sms;
   if (cudaStreamCreateWithFlags(&d->stream, cudaStreamNonBlocking) != cudaSuccess ||
       cudaEventCreate(&d->ev0) != cudaSuccess || cudaEventCreate(&d->ev1) != cudaSuccess) {
     cudaGetLastError();
@@ -251,11 +252,11 @@ extern "C" void mopcuda_device_destroy(MopCudaDevice *d) {
     return;
   cudaSetDevice(d->ordinal);
   stream_sync(d, 10000);
-  DevArena *arenas[] = {&d->irr,       &d->pf,        &d->brdf,       &d->d_draws,  &d->d_lights,
-                        &d->clip,      &d->world,     &d->normal,     &d->color,    &d->rec_base,
-                        &d->rrec,      &d->srec,      &d->clipq,      &d->tile_count,
-                        &d->tile_off,  &d->tile_fill, &d->bins,       &d->counters, &d->pick_xy,
-                        &d->pick_out};
+  DevArena *arenas[] = {&d->irr,      &d->pf,         &d->brdf,        &d->d_draws,
+                        &d->d_lights, &d->clip,       &d->world,       &d->normal,
+                        &d->color,    &d->rrec,       &d->srec,
+                        &d->clipq,    &d->keys,       &d->large_list,  &d->large_items,
+                        &d->shade_list, &d->counters, &d->pick_xy,     &d->pick_out};
   for (DevArena *a : arenas)
     a->release();
   d->h_draws.release();
@@ -620,6 +621,19 @@ static int record_draw(MopCudaDevice *d, const MopCudaDraw *c, const float *mode
   r.metallic = c->metallic;
   r.roughness = c->roughness;
   r.depth_bias = c->depth_bias;
+  {
+    /* per-draw constants the reference recomputes per pixel
+     * (rasterizer.c:1712-1727, 2000, 2030-2032), same operations */
+    float alpha = r.roughness * r.roughness;
+    float alpha2 = alpha * alpha;
+    if (alpha2 < 1e-7f)
+      alpha2 = 1e-7f;
+    r.alpha2 = alpha2;
+    r.smith_k = alpha * 0.5f;
+    r.one_minus_k = 1.0f - r.smith_k;
+    r.f0_dielectric = 0.04f * (1.0f - r.metallic);
+    r.diffuse_scale = 1.0f - r.metallic;
+  }
   memcpy(r.cam_eye, c->cam_eye, sizeof r.cam_eye);
   r.object_id = c->object_id;
   r.vbuf = (const uint8_t *)c->vertex_buffer->d;
@@ -652,6 +666,16 @@ static int record_draw(MopCudaDevice *d, const MopCudaDraw *c, const float *mode
       L.spot_inner_cos = s.spot_inner_cos;
       L.spot_outer_cos = s.spot_outer_cos;
       L.active = s.active;
+      /* mop_vec3_normalize(direction) (math.c:43-50), once per frame */
+      float dl = sqrtf(L.direction[0] * L.direction[0] + L.direction[1] * L.direction[1] +
+                       L.direction[2] * L.direction[2]);
+      if (dl < 1e-8f) {
+        L.ndir[0] = L.ndir[1] = L.ndir[2] = 0.0f;
+      } else {
+        float inv = 1.0f / dl;
+        for (int k = 0; k < 3; k++)
+          L.ndir[k] = L.direction[k] * inv;
+      }
       d->lights.push_back(L);
     }
   }
@@ -714,23 +738,23 @@ static int launch_frame(MopCudaDevice *d) {
   }
   if (T >= (1ull << (32 - ORDER_FAN_BITS)) || V >= (1ull << 31))
     return fail(MOPCUDA_EINVAL, "frame too large: %llu triangles", (unsigned long long)T);
-  const int ts = d->tile_size, shift = ts == 8 ? 3 : 4;
-  const int tiles_x = (fb->w + ts - 1) / ts, tiles_y = (fb->h + ts - 1) / ts;
-  const uint32_t ntiles = (uint32_t)tiles_x * (uint32_t)tiles_y;
+  const size_t S = (size_t)fb->w * (size_t)fb->h;
   /* capacities: grow from the last frame's observed counts */
   uint32_t extra = (uint32_t)(T / 8 + 1024);
   if (extra < d->extra_hint)
     extra = d->extra_hint;
   uint32_t vcap = (uint32_t)V + extra;
-  uint32_t rcap = (uint32_t)(T + T / 4 + 1024);
-  if (rcap < d->rec_hint)
-    rcap = d->rec_hint;
+  /* one record slot per triangle, then the clipped triangles' fans */
+  uint32_t fan_cap = (uint32_t)(T / 8 + 1024);
+  if (fan_cap < d->rec_hint)
+    fan_cap = d->rec_hint;
+  uint32_t rcap = (uint32_t)T + fan_cap;
   uint32_t ccap = (uint32_t)(T / 8 + 1024);
   if (ccap < d->clip_hint)
     ccap = d->clip_hint;
-  uint32_t bcap = rcap * 2u + ntiles;
-  if (bcap < d->bin_hint)
-    bcap = d->bin_hint;
+  uint32_t lcap = (uint32_t)(T / 16 + 1024);
+  if (lcap < d->large_hint)
+    lcap = d->large_hint;
   int rc = 0;
   rc |= d->d_draws.ensure(sizeof(DrawRec) * (nd ? nd : 1));
   rc |= d->d_lights.ensure(sizeof(LightRec) * (d->lights.size() + 1));
@@ -738,14 +762,13 @@ static int launch_frame(MopCudaDevice *d) {
   rc |= d->world.ensure(16ull * vcap);
   rc |= d->normal.ensure(16ull * vcap);
   rc |= d->color.ensure(16ull * vcap);
-  rc |= d->rec_base.ensure(4ull * (T ? T : 1));
   rc |= d->rrec.ensure(sizeof(RasterRec) * (size_t)rcap);
   rc |= d->srec.ensure(sizeof(ShadeRec) * (size_t)rcap);
   rc |= d->clipq.ensure(4ull * ccap);
-  rc |= d->tile_count.ensure(4ull * ntiles);
-  rc |= d->tile_off.ensure(4ull * ntiles);
-  rc |= d->tile_fill.ensure(4ull * ntiles);
-  rc |= d->bins.ensure(4ull * bcap);
+  rc |= d->keys.ensure(8ull * S);
+  rc |= d->large_list.ensure(4ull * lcap);
+  rc |= d->large_items.ensure(4ull * lcap);
+  rc |= d->shade_list.ensure(4ull * S);
   rc |= d->counters.ensure(sizeof(Counters));
   rc |= d->h_draws.ensure(sizeof(DrawRec) * (nd ? nd : 1));
   rc |= d->h_lights.ensure(sizeof(LightRec) * (d->lights.size() + 1));
@@ -755,7 +778,29 @@ static int launch_frame(MopCudaDevice *d) {
   d->vertex_cap = vcap;
   d->rec_cap = rcap;
   d->clip_cap = ccap;
-  d->bin_cap = bcap;
+  d->large_cap = lcap;
+  if (d->ibl_on) {
+    /* per-draw IBL constants (rasterizer.c:243-265, 280-291), x86 float ops */
+    for (uint32_t i = 0; i < nd; i++) {
+      DrawRec &r = d->draws[i];
+      int level = (int)(r.roughness * (float)(d->pf_levels - 1));
+      if (level >= d->pf_levels)
+        level = d->pf_levels - 1;
+      if (level < 0)
+        level = 0; /* roughness < 0: undefined in the reference */
+      size_t off = 0;
+      for (int l = 0; l < level; l++) {
+        int lw = d->pf_w >> l, lh = d->pf_h >> l;
+        off += (size_t)(lw < 1 ? 1 : lw) * (size_t)(lh < 1 ? 1 : lh);
+      }
+      r.pf_off = (uint32_t)off;
+      r.pf_lw = d->pf_w >> level < 1 ? 1 : d->pf_w >> level;
+      r.pf_lh = d->pf_h >> level < 1 ? 1 : d->pf_h >> level;
+      float rough = r.roughness < 0.0f ? 0.0f : (r.roughness > 1.0f ? 1.0f : r.roughness);
+      int row = (int)(rough * (float)(d->brdf_size - 1) + 0.5f);
+      r.brdf_row = row >= d->brdf_size ? d->brdf_size - 1 : row;
+    }
+  }
   if (nd)
     memcpy(d->h_draws.p, d->draws.data(), sizeof(DrawRec) * nd);
   if (!d->lights.empty())
@@ -766,6 +811,7 @@ static int launch_frame(MopCudaDevice *d) {
   a.draws = d->d_draws.as<DrawRec>();
   a.draw_count = nd;
   a.lights = d->d_lights.as<LightRec>();
+  a.light_total = (uint32_t)d->lights.size();
   a.total_vertices = (uint32_t)V;
   a.total_tris = (uint32_t)T;
   a.clip = d->clip.as<float4>();
@@ -773,7 +819,6 @@ static int launch_frame(MopCudaDevice *d) {
   a.normal = d->normal.as<float4>();
   a.color = d->color.as<float4>();
   a.vertex_cap = vcap;
-  a.rec_base = d->rec_base.as<uint32_t>();
   a.rrec = d->rrec.as<RasterRec>();
   a.srec = d->srec.as<ShadeRec>();
   a.rec_cap = rcap;
@@ -781,14 +826,11 @@ static int launch_frame(MopCudaDevice *d) {
   a.clip_cap = ccap;
   a.width = fb->w;
   a.height = fb->h;
-  a.tile_shift = shift;
-  a.tiles_x = tiles_x;
-  a.tiles_y = tiles_y;
-  a.tile_count = d->tile_count.as<uint32_t>();
-  a.tile_off = d->tile_off.as<uint32_t>();
-  a.tile_fill = d->tile_fill.as<uint32_t>();
-  a.bins = d->bins.as<uint32_t>();
-  a.bin_cap = bcap;
+  a.keys = d->keys.as<unsigned long long>();
+  a.large_list = d->large_list.as<uint32_t>();
+  a.large_items = d->large_items.as<uint32_t>();
+  a.large_cap = lcap;
+  a.shade_list = d->shade_list.as<uint32_t>();
   a.ctr = d->counters.as<Counters>();
   memcpy(a.clear, d->clear, sizeof a.clear);
   a.exposure = d->exposure;
@@ -813,7 +855,9 @@ static int launch_frame(MopCudaDevice *d) {
   memset(&p, 0, sizeof p);
   p.pre = fb->pre.as<uchar4>();
   p.out = fb->out.as<uchar4>();
-  int sf = fb->ssaa > 0 && fb->w % fb->ssaa == 0 && fb->h % fb->ssaa == 0 ? fb->ssaa : 1;
+  int sf = fb->ssaa >= 1 && fb->ssaa <= 4 && fb->w % fb->ssaa == 0 && fb->h % fb->ssaa == 0
+               ? fb->ssaa
+               : 1;
   p.presented = sf > 1 ? fb->presented.as<uchar4>() : nullptr;
   p.width = fb->w;
   p.height = fb->h;
@@ -821,6 +865,15 @@ static int launch_frame(MopCudaDevice *d) {
   p.effects = d->post & (MOPCUDA_POST_GAMMA | MOPCUDA_POST_TONEMAP | MOPCUDA_POST_VIGNETTE |
                          MOPCUDA_POST_FXAA);
   memcpy(p.lut, d->lut, sizeof p.lut);
+  for (int i = 0; i < 256; i++) {
+    float v = d->lut[i];
+    if (v > 1.0f)
+      v = 1.0f;
+    if (v < 0.0f)
+      v = 0.0f;
+    volatile float q = v * 255.0f + 0.5f; /* postprocess.c:110-112 */
+    p.lut8[i] = (uint8_t)(int)q;
+  }
 
   cudaStream_t s = d->stream;
   CU_TRY(cudaEventRecord(d->ev0, s));
@@ -831,13 +884,7 @@ static int launch_frame(MopCudaDevice *d) {
     CU_TRY(cudaMemcpyAsync(d->d_lights.p, d->h_lights.p, sizeof(LightRec) * d->lights.size(),
                            cudaMemcpyHostToDevice, s));
   CU_TRY(cudaMemsetAsync(d->counters.p, 0, sizeof(Counters), s));
-  CU_TRY(cudaMemsetAsync(d->tile_count.p, 0, 4ull * ntiles, s));
-  CU_TRY(cudaMemsetAsync(d->tile_fill.p, 0, 4ull * ntiles, s));
-  int occ = mopcuda_tile_occupancy(ts);
-  int grid_tiles = d->num_sms * occ;
-  if ((uint32_t)grid_tiles > ntiles)
-    grid_tiles = (int)ntiles;
-  d->launches += (uint64_t)mopcuda_launch_frame(a, p, ts, grid_tiles, s,
+  d->launches += (uint64_t)mopcuda_launch_frame(a, p, d->cfg, s,
                                                 d->stage_timing ? d->stage_ev : nullptr);
   CU_TRY(cudaGetLastError());
   CU_TRY(cudaMemcpyAsync(d->h_counters.p, d->counters.p, sizeof(Counters), cudaMemcpyDeviceToHost,
@@ -883,7 +930,7 @@ static int finish_frame(MopCudaDevice *d, int timeout_ms) {
     d->rec_hint = c->rec_count + c->rec_count / 4 + 1024;
     d->clip_hint = c->clip_count + c->clip_count / 4 + 1024;
     d->extra_hint = c->extra_vertices + c->extra_vertices / 4 + 1024;
-    d->bin_hint = c->bin_total + c->bin_total / 4 + 1024;
+    d->large_hint = c->large_count + c->large_count / 4 + 1024;
     if (c->overflow & 1u)
       d->rec_hint *= 2;
     if (c->overflow & 2u)
@@ -891,7 +938,7 @@ static int finish_frame(MopCudaDevice *d, int timeout_ms) {
     if (c->overflow & 4u)
       d->clip_hint *= 2;
     if (c->overflow & 8u)
-      d->bin_hint *= 2;
+      d->large_hint *= 2;
     rc = launch_frame(d);
     if (rc)
       return rc;

@@ -54,6 +54,14 @@ struct DrawRec {
   uint32_t stride;
   int16_t off_pos, off_nrm, off_col, off_uv; /* -1 = absent             */
   int8_t n_pos, n_nrm, n_col, n_uv;          /* component counts         */
+  /* per-draw shading constants, computed on the host with the same
+   * operations the reference repeats per pixel (rasterizer.c:1712-1727,
+   * 2000, 2030-2032): alpha^2 (clamped), Smith k, 1-k, 0.04(1-m), 1-m */
+  float alpha2, smith_k, one_minus_k, f0_dielectric, diffuse_scale;
+  /* per-draw IBL lookups (rasterizer.c:243-291): prefiltered mip chosen by
+   * roughness (offset in texels, size) and the BRDF LUT row */
+  uint32_t pf_off;
+  int32_t pf_lw, pf_lh, brdf_row;
 };
 
 struct LightRec {
@@ -66,6 +74,7 @@ struct LightRec {
   float spot_inner_cos;
   float spot_outer_cos;
   int32_t active;
+  float ndir[3]; /* mop_vec3_normalize(direction), computed once per frame */
 };
 
 /* Per fan-triangle raster record, 64 bytes. */
@@ -81,7 +90,10 @@ struct __align__(16) RasterRec {
 
 #define ORDER_FAN_BITS 5
 #define REC_FLAT_BIT 0x8000u
-#define REC_DEAD 0xffffffffu
+/* Record slot t belongs to triangle t.  A clipped triangle's slot holds this
+ * marker in y0 and, in `order`, the slot of its first fan record in the
+ * overflow region that starts at slot total_tris. */
+#define REC_REDIRECT 0xffffu
 
 /* Per fan-triangle shading record, 16 bytes. */
 struct __align__(16) ShadeRec {
@@ -94,20 +106,29 @@ struct __align__(16) ShadeRec {
 
 /* Frame counters and error flags, zeroed at frame start. */
 struct Counters {
-  uint32_t rec_count;
+  uint32_t rec_count;         /* fan records of clipped triangles (overflow region) */
   uint32_t extra_vertices;
   uint32_t clip_count;
-  uint32_t bin_total;
-  uint32_t tile_cursor;
-  uint32_t overflow;     /* bit0 records, bit1 extra vertices, bit2 clip queue, bit3 bins */
-  uint32_t bin_fill_total;
+  uint32_t large_count;       /* records rasterised as (row, chunk) items       */
+  uint32_t large_items;       /* total items of the large records                */
+  uint32_t overflow;          /* bit0 records, bit1 extra vertices, bit2 clip
+                                 queue, bit3 large list                          */
+  uint32_t shade_count;       /* covered samples queued for shading              */
   uint32_t pad;
 };
+
+/* Records whose clamped bbox exceeds these bounds are rasterised as
+ * (row, RASTER_CHUNK-sample) items spread over many threads; smaller ones
+ * by one thread each. */
+#define SMALL_MAX_SIDE 32
+#define SMALL_MAX_AREA 128
+#define RASTER_CHUNK 32
 
 struct FrameArgs {
   const DrawRec *draws;
   uint32_t draw_count;
   const LightRec *lights;
+  uint32_t light_total;   /* records in `lights` (all draws of the frame) */
   uint32_t total_vertices;
   uint32_t total_tris;
   /* vertex streams (total_vertices + extra capacity) */
@@ -116,22 +137,19 @@ struct FrameArgs {
   float4 *normal;
   float4 *color;
   uint32_t vertex_cap;
-  /* triangle -> first record */
-  uint32_t *rec_base;
+  /* records: slot t = triangle t, then the clipped fans' overflow region */
   RasterRec *rrec;
   ShadeRec *srec;
-  uint32_t rec_cap;
+  uint32_t rec_cap;  /* total slots: total_tris + overflow capacity */
   uint32_t *clipq;
   uint32_t clip_cap;
-  /* binning */
-  int width, height;      /* sample resolution */
-  int tile_shift;         /* log2 tile size */
-  int tiles_x, tiles_y;
-  uint32_t *tile_count;
-  uint32_t *tile_off;
-  uint32_t *tile_fill;
-  uint32_t *bins;
-  uint32_t bin_cap;
+  /* visibility */
+  int width, height;                /* sample resolution */
+  unsigned long long *keys;         /* per sample: depth_key << 32 | order */
+  uint32_t *large_list;             /* record ids of large records */
+  uint32_t *large_items;            /* their item counts, then exclusive offsets */
+  uint32_t large_cap;
+  uint32_t *shade_list;             /* covered sample indices */
   Counters *ctr;
   /* resolve */
   float clear[4];
@@ -157,6 +175,7 @@ struct PostArgs {
   int width, height, ssaa;
   uint32_t effects;
   float lut[256];     /* per-byte value after tonemap/gamma */
+  uint8_t lut8[256];  /* the whole per-channel map when vignette is off */
 };
 
 /* ------------------------------------------------------------------------
@@ -186,16 +205,26 @@ __device__ __forceinline__ uint32_t depth_key(float z) {
 #define KEY_EMPTY 0xffffffffffffffffull
 
 /* launchers (kernels.cu); each returns the number of kernels it launched */
-/* ev (optional, 6 events): stage boundaries vertex|setup+clip|bin|tile|post */
-int mopcuda_launch_frame(const FrameArgs &a, const PostArgs &p, int tile_size, int grid_tiles,
+/* Launch shapes of the frame kernels (chosen by the autotuner). */
+struct LaunchCfg {
+  int num_sms;
+  int raster_block;   /* threads per block of the small-record raster     */
+  int shade_block;    /* threads per block of the shading kernel          */
+  int shade_waves;    /* resident blocks per SM targeted by shading       */
+  int post_bx, post_by;
+};
+
+/* ev (optional, 7 events): stage boundaries
+ * vertex | setup+clip | raster | resolve | shade | post */
+int mopcuda_launch_frame(const FrameArgs &a, const PostArgs &p, const LaunchCfg &cfg,
                          cudaStream_t s, cudaEvent_t *ev);
 int mopcuda_launch_fp32_peak(float *out, int blocks, int iters, cudaStream_t s);
-#define MOPCUDA_STAGES 5
+#define MOPCUDA_STAGES 6
 int mopcuda_launch_box(const uchar4 *src, int width, int height, int sf, uchar4 *dst,
                        cudaStream_t s);
 int mopcuda_launch_pick(const uint32_t *ids, const float *depth, int width, int height, int sf,
                         const int2 *xy, uint32_t n, uint32_t *out_id, float *out_depth,
                         int32_t *out_hit, cudaStream_t s);
-int mopcuda_tile_occupancy(int tile_size);
+int mopcuda_shade_occupancy(int block);
 
 #endif

@@ -186,7 +186,7 @@ class Device:
     def launches(self) -> int:
         return int(self.L.mopcuda_launch_count(self.h))
 
-    STAGES = ("vertex", "setup_clip", "bin", "tile_visibility_shade", "post")
+    STAGES = ("vertex", "setup_clip", "raster", "resolve", "shade", "post")
 
     def set_stage_timing(self, on: bool = True):
         self.L.mopcuda_set_stage_timing(self.h, 1 if on else 0)
