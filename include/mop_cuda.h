@@ -233,6 +233,88 @@ int mopcuda_measure_fp32_peak(MopCudaDevice *dev, double *gops);
  * table + light records up; frame counters down), excluding readbacks. */
 int mopcuda_frame_io_bytes(MopCudaDevice *dev, uint64_t *h2d, uint64_t *d2h);
 
+/* ---- batched viewports over a resident scene ---------------------------
+ * No counterpart in the reference, which renders one viewport per
+ * mop_viewport_render (viewport.c:2990-3320).  A scene holds draws recorded
+ * once (buffers, textures, materials, model matrices, lights); a batch binds
+ * a scene to N viewports of their own size, camera and SSAA factor and
+ * renders all of them with one CUDA graph launch.  Every viewport's colour,
+ * depth and object IDs equal what a frame of the same draws through
+ * mopcuda_frame_begin/draw/frame_end gives (draws wholly outside a
+ * viewport's frustum are skipped; they contribute nothing there).  Exposure,
+ * post effects and IBL are the device's at mopcuda_batch_create. */
+typedef struct MopCudaScene MopCudaScene;
+typedef struct MopCudaBatch MopCudaBatch;
+
+typedef struct MopCudaView {
+  float view[16];  /* column-major, as mopcuda_camera_matrices returns */
+  float proj[16];
+  float eye[3];
+  int width, height; /* presented size; the samples are width*ssaa x height*ssaa */
+  int ssaa;          /* 1..4 */
+  float clear[4];
+} MopCudaView;
+
+MopCudaScene *mopcuda_scene_create(MopCudaDevice *dev);
+void mopcuda_scene_destroy(MopCudaScene *scene);
+/* Appends a draw (its mvp and cam_eye are ignored: each viewport supplies
+ * them).  Same state rules and errors as mopcuda_draw.  Returns the draw's
+ * index (>= 0) or an error code. */
+int mopcuda_scene_add_draw(MopCudaScene *scene, const MopCudaDraw *draw);
+/* Replaces draw `index`'s model matrix (TRS update); effective from the next
+ * batch submit. */
+int mopcuda_scene_set_model(MopCudaScene *scene, uint32_t index, const float model[16]);
+uint32_t mopcuda_scene_draw_count(const MopCudaScene *scene);
+/* Triangles submitted by the scene's draws (each viewport processes its
+ * visible subset). */
+uint64_t mopcuda_scene_triangle_count(const MopCudaScene *scene);
+
+/* n in 1..256.  Device memory for every viewport's buffers is allocated
+ * here; the work pools grow on demand (a submit that overflows them is
+ * re-run after growing). */
+MopCudaBatch *mopcuda_batch_create(MopCudaScene *scene, const MopCudaView *views, uint32_t n);
+void mopcuda_batch_destroy(MopCudaBatch *batch);
+/* New cameras/clear colours for the same viewport sizes and SSAA factors. */
+int mopcuda_batch_set_views(MopCudaBatch *batch, const MopCudaView *views, uint32_t n);
+/* Launches the batch (asynchronous); waits for the previous one first. */
+int mopcuda_batch_submit(MopCudaBatch *batch);
+/* Bounded wait for the submitted batch, re-running it if its pools grew. */
+int mopcuda_batch_wait(MopCudaBatch *batch, int timeout_ms);
+/* Device time of the last completed batch launch, ms. */
+float mopcuda_batch_gpu_time_ms(const MopCudaBatch *batch);
+/* Copies one viewport's result into host memory: what = 0 colour at sample
+ * resolution after post effects (RGBA8), 1 presented colour (SSAA box
+ * resolve; = 0 when ssaa is 1), 2 depth (f32, samples), 3 object IDs (u32,
+ * samples).  bytes must equal the buffer's size. */
+#define MOPCUDA_BATCH_COLOR 0
+#define MOPCUDA_BATCH_PRESENTED 1
+#define MOPCUDA_BATCH_DEPTH 2
+#define MOPCUDA_BATCH_IDS 3
+int mopcuda_batch_read(MopCudaBatch *batch, uint32_t view, int what, void *dst, size_t bytes);
+/* Picks on viewport `view` (presented coordinates, top-left sample), as
+ * mopcuda_pick_batch. */
+int mopcuda_batch_pick(MopCudaBatch *batch, uint32_t view, const int32_t *xy, uint32_t n,
+                       uint32_t *ids, float *depths, int32_t *hits);
+
+/* Launch shape of a batch: the small-record limits of the raster (bbox
+ * side, area), block sizes of the vertex / setup / small-raster /
+ * large-raster / shading stages and the persistent-grid multiplier. */
+typedef struct MopCudaBatchConfig {
+  int small_side, small_area;
+  int vertex_block, setup_block, raster_block, large_block, shade_block;
+  int grid_mul;
+} MopCudaBatchConfig;
+int mopcuda_batch_get_config(const MopCudaBatch *batch, MopCudaBatchConfig *cfg);
+/* Validates and applies cfg (the graph is rebuilt at the next submit). */
+int mopcuda_batch_set_config(MopCudaBatch *batch, const MopCudaBatchConfig *cfg);
+/* Autotuner: coordinate search over MopCudaBatchConfig, timing `reps`
+ * launches of the batch per candidate with CUDA events; applies the fastest
+ * and writes a one-line JSON report (candidates and their ms) to report
+ * (may be NULL).  Results do not depend on the configuration. */
+int mopcuda_batch_autotune(MopCudaBatch *batch, int reps, char *report, size_t report_len);
+/* Bytes of device memory the batch holds (buffers + pools). */
+uint64_t mopcuda_batch_device_bytes(const MopCudaBatch *batch);
+
 /* ---- host-side matrices (the device receives finished matrices) ------- */
 /* out = a * b, column-major (mop_mat4_multiply, reference math.c:182-194). */
 void mopcuda_mat4_multiply(const float a[16], const float b[16], float out[16]);

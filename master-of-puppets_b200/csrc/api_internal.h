@@ -1,0 +1,164 @@
+/*
+ * api_internal.h — host-side objects shared by the C-ABI translation units
+ * (mopcuda_api.cu: per-viewport frames; batch_api.cu: batched viewports).
+ */
+#ifndef MOPCUDA_API_INTERNAL_H
+#define MOPCUDA_API_INTERNAL_H
+
+#include "../../include/mop_cuda.h"
+#include "mopcuda_internal.cuh"
+
+#include <mutex>
+#include <vector>
+
+/* Records the message for mopcuda_last_error() and returns code. */
+int mc_fail(int code, const char *fmt, ...);
+#define fail mc_fail
+
+#define CU_TRY(expr)                                                                      \
+  do {                                                                                    \
+    cudaError_t e_ = (expr);                                                              \
+    if (e_ != cudaSuccess)                                                                \
+      return fail(MOPCUDA_ECUDA, "%s: %s (%s:%d)", #expr, cudaGetErrorString(e_), __FILE__, \
+                  __LINE__);                                                              \
+  } while (0)
+
+#define FRAME_TIMEOUT_MS 20000
+
+/* ------------------------------------------------------------------------
+ * objects
+ * ------------------------------------------------------------------------ */
+struct DevArena {
+  void *p = nullptr;
+  size_t cap = 0;
+  int ensure(size_t bytes) {
+    if (bytes <= cap)
+      return 0;
+    size_t n = bytes + bytes / 2 + 4096;
+    if (p)
+      cudaFree(p);
+    p = nullptr;
+    cap = 0;
+    if (cudaMalloc(&p, n) != cudaSuccess) {
+      cudaGetLastError();
+      return fail(MOPCUDA_ENOMEM, "cudaMalloc(%zu) failed", n);
+    }
+    cap = n;
+    return 0;
+  }
+  void release() {
+    if (p)
+      cudaFree(p);
+    p = nullptr;
+    cap = 0;
+  }
+  template <class T> T *as() const { return (T *)p; }
+};
+
+struct HostArena {
+  void *p = nullptr;
+  size_t cap = 0;
+  int ensure(size_t bytes) {
+    if (bytes <= cap)
+      return 0;
+    size_t n = bytes + bytes / 2 + 4096;
+    if (p)
+      cudaFreeHost(p);
+    p = nullptr;
+    cap = 0;
+    if (cudaMallocHost(&p, n) != cudaSuccess) {
+      cudaGetLastError();
+      return fail(MOPCUDA_ENOMEM, "cudaMallocHost(%zu) failed", n);
+    }
+    cap = n;
+    return 0;
+  }
+  void release() {
+    if (p)
+      cudaFreeHost(p);
+    p = nullptr;
+    cap = 0;
+  }
+  template <class T> T *as() const { return (T *)p; }
+};
+
+struct MopCudaBuffer {
+  void *d = nullptr;
+  void *h = nullptr; /* host shadow for buffer_read */
+  size_t size = 0;
+};
+
+struct MopCudaTexture {
+  int w = 0, h = 0;
+  bool hdr = false;
+  void *d = nullptr;
+  void *hcopy = nullptr;
+};
+
+struct MopCudaFramebuffer {
+  int w = 0, h = 0;
+  int ssaa = 1; /* presentation factor when known (fused SSAA output) */
+  DevArena pre, out, depth, ids, presented;
+  HostArena h_color, h_depth, h_ids;
+  bool host_color = false, host_depth = false, host_ids = false;
+  bool presented_valid = false;
+  uint64_t frame_serial = 0;
+};
+
+struct MopCudaDevice {
+  int ordinal = 0;
+  int num_sms = 148;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  cudaEvent_t stage_ev[MOPCUDA_STAGES + 1] = {};
+  bool stage_timing = false;
+  float stage_ms[MOPCUDA_STAGES] = {};
+  std::mutex mu;
+  /* recorded frame */
+  MopCudaFramebuffer *fb = nullptr;
+  float clear[4] = {0, 0, 0, 1};
+  std::vector<DrawRec> draws;
+  std::vector<LightRec> lights;
+  uint32_t unsupported_draws = 0;
+  uint32_t skipped_draws = 0;
+  bool frame_open = false;
+  bool pending = false;
+  int frame_status = 0;
+  /* state */
+  float exposure = 1.0f;
+  uint32_t post = MOPCUDA_POST_GAMMA | MOPCUDA_POST_FXAA;
+  float lut[256];
+  /* IBL */
+  DevArena irr, pf, brdf;
+  int irr_w = 0, irr_h = 0, pf_w = 0, pf_h = 0, pf_levels = 0, brdf_size = 0;
+  float ibl_rot = 0.0f, ibl_int = 1.0f;
+  bool ibl_on = false;
+  /* frame arenas */
+  DevArena d_draws, d_lights, clip, world, normal, color, rrec, srec, clipq, keys,
+      large_list, large_items, shade_list, counters, pick_xy, pick_out;
+  HostArena h_draws, h_lights, h_counters, h_pick;
+  uint32_t vertex_cap = 0, rec_cap = 0, clip_cap = 0, large_cap = 0;
+  uint32_t extra_hint = 0, rec_hint = 0, clip_hint = 0, large_hint = 0;
+  LaunchCfg cfg = {148, SMALL_MAX_SIDE, SMALL_MAX_AREA, 128, 256, 4, 32, 4};
+  uint64_t launches = 0;
+  float last_ms = 0.0f;
+  uint64_t io_h2d = 0, io_d2h = 0; /* bytes moved by the last frame launch */
+};
+
+
+/* Bounded host waits (20 us polls); every device wait of the library. */
+int mc_bounded_sync(MopCudaDevice *d, cudaEvent_t ev, int timeout_ms);
+int mc_stream_sync(MopCudaDevice *d, int timeout_ms);
+/* Builds the device record of one draw (and appends its lights). */
+int mc_build_draw(const MopCudaDraw *c, const float *model, const float *mvp,
+                  std::vector<LightRec> &lights, DrawRec &r, bool &skip);
+/* Per-draw IBL constants for prefiltered maps of pf_w x pf_h with `levels`
+ * levels and a BRDF LUT of brdf_size (no-op when on is false). */
+void mc_ibl_consts(bool on, int pf_w, int pf_h, int levels, int brdf_size, DrawRec *draws,
+                   uint32_t n);
+/* Post-process arguments for the device's current effects. */
+void mc_post_args(const MopCudaDevice *d, PostArgs &p);
+/* mop_mat4_multiply order: running sum from 0.0f, no contraction. */
+void mc_mat4_mul(const float *a, const float *b, float *c);
+
+#endif

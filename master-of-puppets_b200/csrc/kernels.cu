@@ -102,10 +102,7 @@ __device__ __forceinline__ void read_attr(const uint8_t *v, int off, int n, floa
     out[k] = __ldg(f + k);
 }
 
-__global__ void k_vertex(FrameArgs a) {
-  uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
-  if (g >= a.total_vertices)
-    return;
+__device__ __forceinline__ void vertex_item(const FrameArgs &a, uint32_t g) {
   const DrawRec &d = a.draws[find_draw_by(a.draws, a.draw_count, g, true)];
   uint32_t i = g - d.vbase;
   float pos[3], nrm[3], col[4], uv[2];
@@ -155,6 +152,12 @@ __global__ void k_vertex(FrameArgs a) {
   a.world[g] = make_float4(w.x, w.y, w.z, 0.0f);
   a.normal[g] = make_float4(n.x, n.y, n.z, 1.0f / c.w); /* .w: 1/w for perspective weights */
   a.color[g] = make_float4(col[0], col[1], col[2], col[3]);
+}
+
+__global__ void k_vertex(FrameArgs a) {
+  const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g < a.total_vertices)
+    vertex_item(a, g);
 }
 
 /* ------------------------------------------------------------------------
@@ -640,9 +643,11 @@ __device__ __forceinline__ bool rec_live(const RasterRec &r, int W, int H) {
   return (int)r.x0 <= (int)r.x1 && (int)r.y0 <= y1 && (int)r.x1 < W && y1 < H;
 }
 
-__device__ __forceinline__ bool rec_large(const RasterRec &r) {
+/* Records above the small-record limits (bbox side / area, tunable) are
+ * rasterised item-parallel by k_raster_large. */
+__device__ __forceinline__ bool rec_large(const FrameArgs &a, const RasterRec &r) {
   int w = (int)r.x1 - (int)r.x0 + 1, h = (int)(r.y1 & 0x7fffu) - (int)r.y0 + 1;
-  return w > SMALL_MAX_SIDE || h > SMALL_MAX_SIDE || w * h > SMALL_MAX_AREA;
+  return w > a.small_side || h > a.small_side || w * h > a.small_area;
 }
 
 __device__ __forceinline__ uint32_t rec_items(const RasterRec &r) {
@@ -662,38 +667,6 @@ __device__ __forceinline__ void push_large(const FrameArgs &a, uint32_t rid, con
   }
 }
 
-/* Block-aggregated allocation: every thread of the block calls this with
- * two 0/1 requests; one atomicAdd per counter per block hands out slots in
- * thread order. */
-__device__ __forceinline__ void block_alloc2(uint32_t *ca, bool fa, uint32_t *cb, bool fb,
-                                             uint32_t &sa, uint32_t &sb) {
-  __shared__ uint32_t wa[32], wb[32], base_a, base_b;
-  const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
-  const uint32_t nw = (blockDim.x + 31u) >> 5;
-  const uint32_t ba = __ballot_sync(0xffffffffu, fa), bb = __ballot_sync(0xffffffffu, fb);
-  if (lane == 0) {
-    wa[warp] = (uint32_t)__popc(ba);
-    wb[warp] = (uint32_t)__popc(bb);
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    uint32_t ta = 0, tb = 0;
-    for (uint32_t w = 0; w < nw; w++) {
-      uint32_t x = wa[w], y = wb[w];
-      wa[w] = ta;
-      wb[w] = tb;
-      ta += x;
-      tb += y;
-    }
-    base_a = ta ? atomicAdd(ca, ta) : 0u;
-    base_b = tb ? atomicAdd(cb, tb) : 0u;
-  }
-  __syncthreads();
-  const uint32_t lt = (1u << lane) - 1u;
-  sa = base_a + wa[warp] + (uint32_t)__popc(ba & lt);
-  sb = base_b + wb[warp] + (uint32_t)__popc(bb & lt);
-}
-
 /* Marks slot t dead (or as a redirect to clipped fan records) with one
  * 16-byte store of the record's tail (inv_area, order, bbox). */
 __device__ __forceinline__ void write_rec_tail(RasterRec *slot, uint32_t order, uint16_t y0) {
@@ -708,10 +681,7 @@ __device__ __forceinline__ void write_rec_tail(RasterRec *slot, uint32_t order, 
 /* k_setup — one thread per triangle (mop_sw_rasterize_triangle_full
  * rasterizer.c:2458-2530 up to the fan loop).  Slot t of the record arrays
  * belongs to triangle t. */
-__global__ void __launch_bounds__(256) k_setup(FrameArgs a) {
-  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= a.total_tris)
-    return;
+__device__ __forceinline__ void setup_item(const FrameArgs &a, uint32_t t) {
   const DrawRec &d = a.draws[find_draw_by(a.draws, a.draw_count, t, false)];
   const uint32_t lt = t - d.tbase;
   const uint32_t i0 = __ldg(d.ibuf + 3u * lt), i1 = __ldg(d.ibuf + 3u * lt + 1u),
@@ -753,7 +723,7 @@ __global__ void __launch_bounds__(256) k_setup(FrameArgs a) {
   if (status == 1) {
     a.rrec[t] = rr;
     a.srec[t] = sr;
-    if (rec_large(rr))
+    if (rec_large(a, rr))
       push_large(a, t, rr);
   } else if (status == 2) {
     write_rec_tail(&a.rrec[t], 0u, REC_REDIRECT); /* k_clip fills in the target */
@@ -765,6 +735,12 @@ __global__ void __launch_bounds__(256) k_setup(FrameArgs a) {
   } else {
     write_rec_tail(&a.rrec[t], 0u, 0u);
   }
+}
+
+__global__ void __launch_bounds__(256) k_setup(FrameArgs a) {
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < a.total_tris)
+    setup_item(a, t);
 }
 
 /* Sutherland-Hodgman (rasterizer.c:514-626) on the triangles queued by
@@ -794,12 +770,13 @@ __device__ __forceinline__ float plane_dist(int pl, float4 p) {
   return nx[pl] * p.x + ny[pl] * p.y + nz[pl] * p.z + 1.0f * p.w;
 }
 
-__global__ void k_clip(FrameArgs a) {
-  uint32_t n_q = a.ctr->clip_count;
-  if (n_q > a.clip_cap)
-    n_q = a.clip_cap;
-  for (uint32_t qi = blockIdx.x * blockDim.x + threadIdx.x; qi < n_q;
-       qi += gridDim.x * blockDim.x) {
+__device__ __forceinline__ uint32_t clip_items(const FrameArgs &a) {
+  const uint32_t n_q = a.ctr->clip_count;
+  return n_q > a.clip_cap ? a.clip_cap : n_q;
+}
+
+__device__ __forceinline__ void clip_item(const FrameArgs &a, uint32_t qi) {
+  {
     uint32_t t = a.clipq[qi];
     const DrawRec &d = a.draws[find_draw_by(a.draws, a.draw_count, t, false)];
     uint32_t lt = t - d.tbase;
@@ -837,14 +814,14 @@ __global__ void k_clip(FrameArgs a) {
       dst = tmp;
     }
     if (cnt < 3)
-      continue; /* slot t stays a redirect that no fragment references */
+      return; /* slot t stays a redirect that no fragment references */
     /* store the polygon's vertices, then one record per fan triangle */
     uint32_t e = atomicAdd(&a.ctr->extra_vertices, (uint32_t)cnt);
     uint32_t nf = (uint32_t)cnt - 2u;
     uint32_t r = a.total_tris + atomicAdd(&a.ctr->rec_count, nf);
     if (a.total_vertices + e + (uint32_t)cnt > a.vertex_cap || r + nf > a.rec_cap) {
       atomicOr(&a.ctr->overflow, (a.total_vertices + e + (uint32_t)cnt > a.vertex_cap) ? 2u : 1u);
-      continue;
+      return;
     }
     uint32_t vs = a.total_vertices + e;
     for (int k = 0; k < cnt; k++) {
@@ -866,11 +843,18 @@ __global__ void k_clip(FrameArgs a) {
       }
       a.rrec[r + i - 1] = rr;
       a.srec[r + i - 1] = sr;
-      if (rec_live(rr, a.width, a.height) && rec_large(rr))
+      if (rec_live(rr, a.width, a.height) && rec_large(a, rr))
         push_large(a, r + (uint32_t)i - 1u, rr);
     }
     write_rec_tail(&a.rrec[t], r, REC_REDIRECT);
   }
+}
+
+__global__ void k_clip(FrameArgs a) {
+  const uint32_t n_q = clip_items(a);
+  for (uint32_t qi = blockIdx.x * blockDim.x + threadIdx.x; qi < n_q;
+       qi += gridDim.x * blockDim.x)
+    clip_item(a, qi);
 }
 
 /* ------------------------------------------------------------------------
@@ -908,15 +892,16 @@ __device__ __forceinline__ void raster_span(const FrameArgs &a, const RasterRec 
 
 /* Small records: one thread walks the whole (<= 128-sample) bbox, row by
  * row, exactly as the reference's loops step (rasterizer.c:1926-2151). */
-__global__ void k_raster_small(FrameArgs a) {
-  uint32_t n = a.total_tris + a.ctr->rec_count;
-  if (n > a.rec_cap)
-    n = a.rec_cap;
-  for (uint32_t rid = blockIdx.x * blockDim.x + threadIdx.x; rid < n;
-       rid += gridDim.x * blockDim.x) {
+__device__ __forceinline__ uint32_t raster_small_items(const FrameArgs &a) {
+  const uint32_t n = a.total_tris + a.ctr->rec_count;
+  return n > a.rec_cap ? a.rec_cap : n;
+}
+
+__device__ __forceinline__ void raster_small_item(const FrameArgs &a, uint32_t rid) {
+  {
     const RasterRec r = a.rrec[rid];
-    if (!rec_live(r, a.width, a.height) || rec_large(r))
-      continue;
+    if (!rec_live(r, a.width, a.height) || rec_large(a, r))
+      return;
     const bool flat = (r.y1 & REC_FLAT_BIT) != 0;
     const int y1 = (int)(r.y1 & 0x7fffu);
     float wr0 = r.w0[0], wr1 = r.w0[1], wr2 = r.w0[2], zr = r.zc[0];
@@ -931,9 +916,16 @@ __global__ void k_raster_small(FrameArgs a) {
   }
 }
 
+__global__ void k_raster_small(FrameArgs a) {
+  const uint32_t n = raster_small_items(a);
+  for (uint32_t rid = blockIdx.x * blockDim.x + threadIdx.x; rid < n;
+       rid += gridDim.x * blockDim.x)
+    raster_small_item(a, rid);
+}
+
 /* Exclusive scan of the large records' item counts (one block). */
-__global__ void k_large_scan(FrameArgs a) {
-  __shared__ uint32_t part[1024];
+/* Exclusive scan of the large records' item counts by one block of 1024. */
+__device__ __forceinline__ void large_scan_block(const FrameArgs &a, uint32_t *part) {
   uint32_t n = a.ctr->large_count;
   if (n > a.large_cap)
     n = a.large_cap;
@@ -960,15 +952,18 @@ __global__ void k_large_scan(FrameArgs a) {
     a.ctr->large_items = part[1023];
 }
 
+__global__ void __launch_bounds__(1024) k_large_scan(FrameArgs a) {
+  __shared__ uint32_t part[1024];
+  large_scan_block(a, part);
+}
+
 /* Large records: one thread per (row, RASTER_CHUNK-sample chunk); the edge
  * values at the chunk start come from the exact fold. */
-__global__ void k_raster_large(FrameArgs a) {
+__device__ __forceinline__ void raster_large_item(const FrameArgs &a, uint32_t it) {
   uint32_t nl = a.ctr->large_count;
   if (nl > a.large_cap)
     nl = a.large_cap;
-  const uint32_t total = a.ctr->large_items;
-  for (uint32_t it = blockIdx.x * blockDim.x + threadIdx.x; it < total;
-       it += gridDim.x * blockDim.x) {
+  {
     uint32_t lo = 0, hi = nl; /* last record with offset <= it */
     while (hi - lo > 1) {
       uint32_t mid = (lo + hi) >> 1;
@@ -979,10 +974,10 @@ __global__ void k_raster_large(FrameArgs a) {
     }
     const uint32_t rid = a.large_list[lo];
     if (rid >= a.rec_cap)
-      continue;
+      return;
     const RasterRec r = a.rrec[rid];
     if (!rec_live(r, a.width, a.height))
-      continue;
+      return;
     const bool flat = (r.y1 & REC_FLAT_BIT) != 0;
     const uint32_t w = (uint32_t)r.x1 - (uint32_t)r.x0 + 1u;
     const uint32_t chunks = (w + RASTER_CHUNK - 1u) / RASTER_CHUNK;
@@ -990,7 +985,7 @@ __global__ void k_raster_large(FrameArgs a) {
     const int jr = (int)(local / chunks), kc = (int)((local % chunks) * RASTER_CHUNK);
     const int y = (int)r.y0 + jr;
     if (y > (int)(r.y1 & 0x7fffu))
-      continue;
+      return;
     const int xs = (int)r.x0 + kc, xe = min((int)r.x1, xs + RASTER_CHUNK - 1);
     float w0 = fold_add(fold_add(r.w0[0], r.dy[0], jr), r.dx[0], kc);
     float w1 = fold_add(fold_add(r.w0[1], r.dy[1], jr), r.dx[1], kc);
@@ -998,6 +993,13 @@ __global__ void k_raster_large(FrameArgs a) {
     float z = flat ? fold_add(fold_add(r.zc[0], r.zc[2], jr), r.zc[1], kc) : 0.0f;
     raster_span(a, r, flat, y, xs, xe, w0, w1, w2, z);
   }
+}
+
+__global__ void k_raster_large(FrameArgs a) {
+  const uint32_t total = a.ctr->large_items;
+  for (uint32_t it = blockIdx.x * blockDim.x + threadIdx.x; it < total;
+       it += gridDim.x * blockDim.x)
+    raster_large_item(a, it);
 }
 
 /* ------------------------------------------------------------------------
@@ -1016,9 +1018,10 @@ __device__ __forceinline__ float aces(float x) { /* rasterizer.c:2770-2774 */
  * block iteration).  Blocks of 256 threads. */
 #define RESOLVE_PER_THREAD 8
 
-__global__ void __launch_bounds__(256) k_resolve(FrameArgs a) {
-  __shared__ uint32_t s_warp[8];
-  __shared__ uint32_t s_base;
+/* One block iteration of the resolve: samples [blk, blk + 256 * 8). */
+__device__ __forceinline__ void resolve_chunk(const FrameArgs &a, uint32_t blk, uint32_t *s_warp,
+                                              uint32_t *s_base_p) {
+  uint32_t &s_base = *s_base_p;
   const uint32_t S = (uint32_t)a.width * (uint32_t)a.height;
   const uchar4 bg = make_uchar4(x86_f2u8(fminf(a.clear[0], 1.0f) * 255.0f + 0.5f),
                                 x86_f2u8(fminf(a.clear[1], 1.0f) * 255.0f + 0.5f),
@@ -1026,8 +1029,7 @@ __global__ void __launch_bounds__(256) k_resolve(FrameArgs a) {
   const uint32_t bgw = (uint32_t)bg.x | ((uint32_t)bg.y << 8) | ((uint32_t)bg.z << 16) |
                        ((uint32_t)bg.w << 24);
   const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
-  const uint32_t per_iter = 256u * RESOLVE_PER_THREAD;
-  for (uint32_t blk = blockIdx.x * per_iter; blk < S; blk += gridDim.x * per_iter) {
+  {
     const uint32_t i0 = blk + threadIdx.x * RESOLVE_PER_THREAD;
     uint32_t mask = 0;
     if (i0 + RESOLVE_PER_THREAD <= S) {
@@ -1092,27 +1094,38 @@ __global__ void __launch_bounds__(256) k_resolve(FrameArgs a) {
   }
 }
 
+__global__ void __launch_bounds__(256) k_resolve(FrameArgs a) {
+  __shared__ uint32_t s_warp[8];
+  __shared__ uint32_t s_base;
+  const uint32_t S = (uint32_t)a.width * (uint32_t)a.height;
+  const uint32_t per_iter = 256u * RESOLVE_PER_THREAD;
+  for (uint32_t blk = blockIdx.x * per_iter; blk < S; blk += gridDim.x * per_iter)
+    resolve_chunk(a, blk, s_warp, &s_base);
+}
+
 /* Deferred shading of one covered sample: the winning record's exact edge
  * values at the sample (fold from the bbox corner), barycentrics, depth,
  * perspective-correct weights, multi-light + IBL shading (smooth) or the
  * record's constant colour (flat), then the ACES resolve. */
 #define SHADE_SMEM_LIGHTS 64
 
-/* 4 blocks of 256 per SM (64 registers): the kernel is issue-bound and the
- * extra warps hide the dependent-latency stalls of the lighting chains. */
-__global__ void __launch_bounds__(256, 4) k_shade(FrameArgs a) {
-  __shared__ LightRec s_lights[SHADE_SMEM_LIGHTS];
-  const bool smem_lights = a.light_total <= SHADE_SMEM_LIGHTS;
-  if (smem_lights) {
-    const uint32_t words = a.light_total * (uint32_t)(sizeof(LightRec) / 4);
-    const uint32_t *src = reinterpret_cast<const uint32_t *>(a.lights);
-    uint32_t *dst = reinterpret_cast<uint32_t *>(s_lights);
-    for (uint32_t i = threadIdx.x; i < words; i += blockDim.x)
-      dst[i] = src[i];
-    __syncthreads();
-  }
-  const uint32_t n = a.ctr->shade_count;
-  for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
+/* Stages the frame's light records in shared memory when they fit; returns
+ * the array the shading reads. */
+__device__ __forceinline__ const LightRec *stage_lights(const FrameArgs &a, LightRec *s_lights) {
+  if (a.light_total > SHADE_SMEM_LIGHTS)
+    return a.lights;
+  const uint32_t words = a.light_total * (uint32_t)(sizeof(LightRec) / 4);
+  const uint32_t *src = reinterpret_cast<const uint32_t *>(a.lights);
+  uint32_t *dst = reinterpret_cast<uint32_t *>(s_lights);
+  for (uint32_t i = threadIdx.x; i < words; i += blockDim.x)
+    dst[i] = src[i];
+  __syncthreads();
+  return s_lights;
+}
+
+/* Shades covered sample shade_list[j] (lights: the frame's light array). */
+__device__ __forceinline__ void shade_item(const FrameArgs &a, uint32_t j, const LightRec *lights) {
+  {
     const uint32_t px = a.shade_list[j];
     const unsigned long long k = a.keys[px];
     const uint32_t t = (uint32_t)k >> ORDER_FAN_BITS;
@@ -1135,12 +1148,12 @@ __global__ void __launch_bounds__(256, 4) k_shade(FrameArgs a) {
       a.pre[px] = make_uchar4(0, 0, 0, 255);
       a.depth[px] = 1.0f;
       a.ids[px] = 0u;
-      continue;
+      return;
     }
     const int x = (int)(px % (uint32_t)a.width), y = (int)(px / (uint32_t)a.width);
     const ShadeRec s = a.srec[rid];
     const DrawRec &d = a.draws[s.draw < a.draw_count ? s.draw : 0];
-    const LightRec *Ls = smem_lights ? s_lights + d.light_off : a.lights + d.light_off;
+    const LightRec *Ls = lights + d.light_off;
     const int jr = y - (int)r.y0, kc = x - (int)r.x0;
     float hdr[3], depth;
     if (r.y1 & REC_FLAT_BIT) {
@@ -1172,6 +1185,16 @@ __global__ void __launch_bounds__(256, 4) k_shade(FrameArgs a) {
     a.depth[px] = depth;
     a.ids[px] = d.object_id;
   }
+}
+
+/* 4 blocks of 256 per SM (64 registers): the kernel is issue-bound and the
+ * extra warps hide the dependent-latency stalls of the lighting chains. */
+__global__ void __launch_bounds__(256, 4) k_shade(FrameArgs a) {
+  __shared__ LightRec s_lights[SHADE_SMEM_LIGHTS];
+  const LightRec *lights = stage_lights(a, s_lights);
+  const uint32_t n = a.ctr->shade_count;
+  for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x)
+    shade_item(a, j, lights);
 }
 
 /* ------------------------------------------------------------------------
@@ -1236,20 +1259,41 @@ __device__ __forceinline__ uchar4 fxaa_tile(const uchar4 (*tc)[TW], const float 
   return o;
 }
 
+template <int SF> struct PostSmem {
+  static constexpr int TW = POST_BX * SF + 2, TH = POST_BY * SF + 2;
+  uchar4 c[TH][TW];
+  float l[TH][TW];
+  float lut[256];
+  uint8_t lut8[256];
+};
+
 template <int SF>
-__global__ void __launch_bounds__(POST_BX *POST_BY) k_post(PostArgs a) {
-  constexpr int TW = POST_BX * SF + 2, TH = POST_BY * SF + 2;
-  __shared__ uchar4 s_c[TH][TW];
-  __shared__ float s_l[TH][TW];
-  __shared__ float s_lut[256];
-  __shared__ uint8_t s_lut8[256];
+__device__ __forceinline__ void post_load_luts(const PostArgs &a, PostSmem<SF> &sm) {
   const int tid = threadIdx.y * POST_BX + threadIdx.x;
   for (int i = tid; i < 256; i += POST_BX * POST_BY) {
-    s_lut[i] = a.lut[i];
-    s_lut8[i] = a.lut8[i];
+    sm.lut[i] = a.lut[i];
+    sm.lut8[i] = a.lut8[i];
   }
+}
+
+template <int SF, int TW>
+__device__ __forceinline__ void post_pixel(const PostArgs &a, const uchar4 (*s_c)[TW],
+                                           const float (*s_l)[TW], const float *s_lut,
+                                           const uint8_t *s_lut8, int px, int py);
+
+/* One tile of POST_BX x POST_BY presented pixels (bx, by): FXAA, the
+ * tonemap/gamma map and the SSAA box.  Block-uniform; ends with a barrier so
+ * the caller may reuse the shared tile. */
+template <int SF>
+__device__ __forceinline__ void post_tile(const PostArgs &a, PostSmem<SF> &sm, int bx, int by) {
+  constexpr int TW = PostSmem<SF>::TW, TH = PostSmem<SF>::TH;
+  auto &s_c = sm.c;
+  auto &s_l = sm.l;
+  const float *s_lut = sm.lut;
+  const uint8_t *s_lut8 = sm.lut8;
+  const int tid = threadIdx.y * POST_BX + threadIdx.x;
   const int w = a.width, h = a.height;
-  const int sx0 = (int)blockIdx.x * POST_BX * SF - 1, sy0 = (int)blockIdx.y * POST_BY * SF - 1;
+  const int sx0 = bx * POST_BX * SF - 1, sy0 = by * POST_BY * SF - 1;
   for (int i = tid; i < TW * TH; i += POST_BX * POST_BY) {
     const int ty = i / TW, tx = i % TW;
     const int sy = min(max(sy0 + ty, 0), h - 1), sx = min(max(sx0 + tx, 0), w - 1);
@@ -1259,10 +1303,18 @@ __global__ void __launch_bounds__(POST_BX *POST_BY) k_post(PostArgs a) {
   }
   __syncthreads();
   const int pw = w / SF, ph = h / SF;
-  const int px = (int)blockIdx.x * POST_BX + (int)threadIdx.x;
-  const int py = (int)blockIdx.y * POST_BY + (int)threadIdx.y;
-  if (px >= pw || py >= ph)
-    return;
+  const int px = bx * POST_BX + (int)threadIdx.x;
+  const int py = by * POST_BY + (int)threadIdx.y;
+  if (px < pw && py < ph)
+    post_pixel<SF, TW>(a, s_c, s_l, s_lut, s_lut8, px, py);
+  __syncthreads();
+}
+
+template <int SF, int TW>
+__device__ __forceinline__ void post_pixel(const PostArgs &a, const uchar4 (*s_c)[TW],
+                                           const float (*s_l)[TW], const float *s_lut,
+                                           const uint8_t *s_lut8, int px, int py) {
+  const int w = a.width, h = a.height, pw = w / SF;
   const bool fx = (a.effects & 16u) && w >= 3 && h >= 3;
   uint32_t acc[4] = {0, 0, 0, 0};
 #pragma unroll
@@ -1314,6 +1366,13 @@ __global__ void __launch_bounds__(POST_BX *POST_BY) k_post(PostArgs a) {
         make_uchar4((uint8_t)(acc[0] / n), (uint8_t)(acc[1] / n), (uint8_t)(acc[2] / n),
                     (uint8_t)(acc[3] / n));
   }
+}
+
+template <int SF>
+__global__ void __launch_bounds__(POST_BX *POST_BY) k_post(PostArgs a) {
+  __shared__ PostSmem<SF> sm;
+  post_load_luts<SF>(a, sm);
+  post_tile<SF>(a, sm, (int)blockIdx.x, (int)blockIdx.y);
 }
 
 template __global__ void k_post<1>(PostArgs);
@@ -1486,3 +1545,452 @@ int mopcuda_launch_pick(const uint32_t *ids, const float *depth, int width, int 
   return 1;
 }
 
+
+/* ========================================================================
+ * Batched viewports.  One launch per stage covers every viewport of a batch
+ * over one resident scene.  The stage kernels are persistent (a grid of
+ * resident blocks), map each work item to (viewport, local item) through a
+ * per-block prefix of the viewports' item counts, and run the same per-item
+ * code as the single-viewport kernels, so every viewport's result is the
+ * one its own frame would give.
+ * ======================================================================== */
+
+/* mop_mat4_multiply (math.c:182-194) on the device: running sum from 0,
+ * round-to-nearest, no contraction. */
+__device__ void dev_mat4_mul(const float *a, const float *b, float *c) {
+  for (int col = 0; col < 4; col++)
+    for (int row = 0; row < 4; row++) {
+      float s = 0.0f;
+      for (int k = 0; k < 4; k++)
+        s = __fadd_rn(s, __fmul_rn(a[k * 4 + row], b[col * 4 + k]));
+      c[col * 4 + row] = s;
+    }
+}
+
+/* True when every point of the draw's bounding sphere lies outside one
+ * clip plane with a margin far above the rounding of the float clip
+ * transform (xform: four products, three sums), so every triangle of the
+ * draw is trivially rejected by the setup (rasterizer.c:2467-2476) and the
+ * draw contributes nothing.  Planes: x > w, x < -w, y > w, y < -w, and with
+ * zplanes z > w, z < -w. */
+__device__ bool draw_culled(const float *m, const DrawBound &bd, bool zplanes) {
+  const double r = (double)bd.r;
+  if (!(r >= 0.0) || !isfinite(bd.r) || !isfinite(bd.c[0]) || !isfinite(bd.c[1]) ||
+      !isfinite(bd.c[2]))
+    return false;
+  for (int k = 0; k < 16; k++)
+    if (!isfinite(m[k]))
+      return false;
+  const double c[3] = {(double)bd.c[0], (double)bd.c[1], (double)bd.c[2]};
+  for (int axis = 0; axis < (zplanes ? 3 : 2); axis++)
+    for (int sg = -1; sg <= 1; sg += 2) {
+      double q[4], mag = 0.0;
+      for (int j = 0; j < 4; j++) {
+        const double ma = (double)m[j * 4 + axis], mw = (double)m[j * 4 + 3];
+        q[j] = (double)sg * ma - mw;
+        mag += (fabs(ma) + fabs(mw)) * (j < 3 ? fabs(c[j]) + r : 1.0);
+      }
+      const double dist = q[0] * c[0] + q[1] * c[1] + q[2] * c[2] + q[3];
+      const double nrm = sqrt(q[0] * q[0] + q[1] * q[1] + q[2] * q[2]);
+      if (dist - r * nrm > 1e-5 * mag + 1e-30)
+        return true;
+    }
+  return false;
+}
+
+/* Per viewport (one block of 256): mvp = P * (V * M) per scene draw, cull
+ * by bounding sphere, and compact the visible draws in submission order
+ * with their vertex/triangle bases; the triangle order of the survivors is
+ * the scene's, so depth ties resolve as in the full frame. */
+__global__ void __launch_bounds__(256) k_batch_prepare(BatchArgs b) {
+  __shared__ uint32_t s_w[8][3];
+  __shared__ uint32_t s_tot[3];
+  const uint32_t v = blockIdx.x;
+  const ViewRec &vw = b.views[v];
+  DrawRec *out = b.view_draws + (size_t)v * b.nd;
+  const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+  if (threadIdx.x == 0)
+    s_tot[0] = s_tot[1] = s_tot[2] = 0u;
+  __syncthreads();
+  for (uint32_t base = 0; base < b.nd; base += 256u) {
+    const uint32_t i = base + threadIdx.x;
+    float mvp[16];
+    uint32_t x[3] = {0u, 0u, 0u};
+    if (i < b.nd) {
+      const DrawRec &sd = b.scene[i];
+      float vm[16];
+      dev_mat4_mul(vw.view, sd.model, vm);
+      dev_mat4_mul(vw.proj, vm, mvp);
+      const uint32_t tc = sd.index_count / 3u;
+      if (tc > 0u && !draw_culled(mvp, b.bounds[i], sd.depth_bias == 0.0f)) {
+        x[0] = 1u;
+        x[1] = sd.vertex_count;
+        x[2] = tc;
+      }
+    }
+    uint32_t incl[3];
+    for (int k = 0; k < 3; k++) {
+      incl[k] = x[k];
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, incl[k], o);
+        if (lane >= (uint32_t)o)
+          incl[k] += y;
+      }
+      if (lane == 31u)
+        s_w[warp][k] = incl[k];
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      for (int k = 0; k < 3; k++) {
+        uint32_t run = s_tot[k];
+        for (int w = 0; w < 8; w++) {
+          const uint32_t t = s_w[w][k];
+          s_w[w][k] = run;
+          run += t;
+        }
+        s_tot[k] = run;
+      }
+    }
+    __syncthreads();
+    if (x[0]) {
+      DrawRec r = b.scene[i];
+      for (int k = 0; k < 16; k++)
+        r.mvp[k] = mvp[k];
+      r.cam_eye[0] = vw.eye[0];
+      r.cam_eye[1] = vw.eye[1];
+      r.cam_eye[2] = vw.eye[2];
+      r.vbase = s_w[warp][1] + incl[1] - x[1];
+      r.tbase = s_w[warp][2] + incl[2] - x[2];
+      out[s_w[warp][0] + incl[0] - x[0]] = r;
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    FrameArgs a = b.tmpl;
+    a.draws = out;
+    a.draw_count = s_tot[0];
+    a.total_vertices = s_tot[1];
+    a.total_tris = s_tot[2];
+    a.width = vw.width;
+    a.height = vw.height;
+    a.keys = b.keys + vw.sample_off;
+    a.shade_list = b.shade_list + vw.sample_off;
+    a.pre = b.pre + vw.sample_off;
+    a.depth = b.depth + vw.sample_off;
+    a.ids = b.ids + vw.sample_off;
+    for (int k = 0; k < 4; k++)
+      a.clear[k] = vw.clear[k];
+    a.ctr = b.ctr + v;
+    b.frames[v] = a;
+  }
+}
+
+/* One block of 256: carves every viewport's vertex streams, records, clip
+ * queue and large list out of the batch pools (exclusive scans over the
+ * viewports).  A viewport that does not fit renders nothing this time and
+ * the status tells the host how large the pools must grow. */
+__global__ void __launch_bounds__(256) k_batch_alloc(BatchArgs b) {
+  __shared__ unsigned long long s_w[8][4];
+  __shared__ unsigned long long s_tot[4];
+  const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+  const unsigned long long pool[4] = {b.vertex_pool, b.rec_pool, b.clip_pool, b.large_pool};
+  if (threadIdx.x < 4)
+    s_tot[threadIdx.x] = 0ull;
+  __syncthreads();
+  for (uint32_t base = 0; base < b.nv; base += 256u) {
+    const uint32_t v = base + threadIdx.x;
+    unsigned long long need[4] = {0ull, 0ull, 0ull, 0ull};
+    if (v < b.nv) {
+      const FrameArgs &a = b.frames[v];
+      const unsigned long long T = a.total_tris, fan = T * b.fan_num / 8ull + 1024ull;
+      need[0] = (unsigned long long)a.total_vertices + fan;
+      need[1] = T + fan;
+      need[2] = fan;
+      need[3] = T * b.large_num / 16ull + 1024ull;
+    }
+    unsigned long long incl[4];
+    for (int k = 0; k < 4; k++) {
+      incl[k] = need[k];
+      for (int o = 1; o < 32; o <<= 1) {
+        const unsigned long long y = __shfl_up_sync(0xffffffffu, incl[k], o);
+        if (lane >= (uint32_t)o)
+          incl[k] += y;
+      }
+      if (lane == 31u)
+        s_w[warp][k] = incl[k];
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      for (int k = 0; k < 4; k++) {
+        unsigned long long run = s_tot[k];
+        for (int w = 0; w < 8; w++) {
+          const unsigned long long t = s_w[w][k];
+          s_w[w][k] = run;
+          run += t;
+        }
+        s_tot[k] = run;
+      }
+    }
+    __syncthreads();
+    if (v < b.nv) {
+      unsigned long long off[4];
+      bool fits = true;
+      for (int k = 0; k < 4; k++) {
+        off[k] = s_w[warp][k] + incl[k] - need[k];
+        if (off[k] + need[k] > pool[k]) {
+          fits = false;
+          atomicOr(&b.status->overflow, 1u << k);
+        }
+      }
+      FrameArgs &a = b.frames[v];
+      if (!fits) {
+        a.draw_count = 0u;
+        a.total_vertices = 0u;
+        a.total_tris = 0u;
+        for (int k = 0; k < 4; k++)
+          off[k] = 0ull;
+        need[0] = need[1] = need[2] = need[3] = 0ull;
+      }
+      a.clip = b.clip + off[0];
+      a.world = b.world + off[0];
+      a.normal = b.normal + off[0];
+      a.color = b.color + off[0];
+      a.vertex_cap = (uint32_t)need[0];
+      a.rrec = b.rrec + off[1];
+      a.srec = b.srec + off[1];
+      a.rec_cap = (uint32_t)need[1];
+      a.clipq = b.clipq + off[2];
+      a.clip_cap = (uint32_t)need[2];
+      a.large_list = b.large_list + off[3];
+      a.large_items = b.large_items + off[3];
+      a.large_cap = (uint32_t)need[3];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    b.status->need_vertex = s_tot[0];
+    b.status->need_rec = s_tot[1];
+    b.status->need_clip = s_tot[2];
+    b.status->need_large = s_tot[3];
+  }
+}
+
+enum { ST_VERTEX, ST_SETUP, ST_CLIP, ST_RSMALL, ST_RLARGE, ST_SHADE, ST_RESOLVE };
+
+template <int ST> __device__ __forceinline__ uint32_t stage_count(const FrameArgs &a) {
+  switch (ST) {
+  case ST_VERTEX:
+    return a.total_vertices;
+  case ST_SETUP:
+    return a.total_tris;
+  case ST_CLIP:
+    return clip_items(a);
+  case ST_RSMALL:
+    return a.total_tris ? raster_small_items(a) : 0u;
+  case ST_RLARGE:
+    return a.total_tris ? a.ctr->large_items : 0u;
+  case ST_SHADE:
+    return a.ctr->shade_count;
+  default: /* ST_RESOLVE: chunks of 256 x RESOLVE_PER_THREAD samples */
+    return ((uint32_t)a.width * (uint32_t)a.height + 256u * RESOLVE_PER_THREAD - 1u) /
+           (256u * RESOLVE_PER_THREAD);
+  }
+}
+
+/* s_pre[v] = items of viewports before v, s_pre[nv] = total (warp 0). */
+template <int ST>
+__device__ __forceinline__ uint32_t views_prefix(const FrameArgs *__restrict__ fr, uint32_t nv,
+                                                 uint32_t *s_pre) {
+  if (threadIdx.x < 32u) {
+    const uint32_t lane = threadIdx.x;
+    uint32_t run = 0;
+    for (uint32_t base = 0; base < nv; base += 32u) {
+      const uint32_t v = base + lane;
+      const uint32_t c = v < nv ? stage_count<ST>(fr[v]) : 0u;
+      uint32_t incl = c;
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= (uint32_t)o)
+          incl += y;
+      }
+      if (v < nv)
+        s_pre[v] = run + incl - c;
+      run += __shfl_sync(0xffffffffu, incl, 31);
+    }
+    if (lane == 0)
+      s_pre[nv] = run;
+  }
+  __syncthreads();
+  return s_pre[nv];
+}
+
+template <int ST>
+__global__ void __launch_bounds__(256) k_b_items(const FrameArgs *__restrict__ fr, uint32_t nv) {
+  __shared__ uint32_t s_pre[MOPCUDA_MAX_VIEWS + 1];
+  const uint32_t total = views_prefix<ST>(fr, nv, s_pre);
+  uint32_t v = 0;
+  for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < total;
+       g += gridDim.x * blockDim.x) {
+    while (s_pre[v + 1] <= g)
+      v++;
+    const uint32_t i = g - s_pre[v];
+    const FrameArgs &a = fr[v];
+    if (ST == ST_VERTEX)
+      vertex_item(a, i);
+    else if (ST == ST_SETUP)
+      setup_item(a, i);
+    else if (ST == ST_CLIP)
+      clip_item(a, i);
+    else if (ST == ST_RSMALL)
+      raster_small_item(a, i);
+    else
+      raster_large_item(a, i);
+  }
+}
+
+__global__ void __launch_bounds__(1024) k_b_large_scan(const FrameArgs *__restrict__ fr) {
+  __shared__ uint32_t part[1024];
+  if (fr[blockIdx.x].total_tris)
+    large_scan_block(fr[blockIdx.x], part);
+}
+
+__global__ void __launch_bounds__(256) k_b_resolve(const FrameArgs *__restrict__ fr,
+                                                   uint32_t nv) {
+  __shared__ uint32_t s_pre[MOPCUDA_MAX_VIEWS + 1];
+  __shared__ uint32_t s_warp[8];
+  __shared__ uint32_t s_base;
+  const uint32_t total = views_prefix<ST_RESOLVE>(fr, nv, s_pre);
+  uint32_t v = 0;
+  for (uint32_t u = blockIdx.x; u < total; u += gridDim.x) {
+    while (s_pre[v + 1] <= u)
+      v++;
+    resolve_chunk(fr[v], (u - s_pre[v]) * (256u * RESOLVE_PER_THREAD), s_warp, &s_base);
+  }
+}
+
+/* All viewports of a batch share the scene's light array. */
+__global__ void __launch_bounds__(256, 4) k_b_shade(const FrameArgs *__restrict__ fr,
+                                                    uint32_t nv) {
+  __shared__ LightRec s_lights[SHADE_SMEM_LIGHTS];
+  __shared__ uint32_t s_pre[MOPCUDA_MAX_VIEWS + 1];
+  const LightRec *lights = stage_lights(fr[0], s_lights);
+  const uint32_t total = views_prefix<ST_SHADE>(fr, nv, s_pre);
+  uint32_t v = 0;
+  for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < total;
+       g += gridDim.x * blockDim.x) {
+    while (s_pre[v + 1] <= g)
+      v++;
+    shade_item(fr[v], g - s_pre[v], lights);
+  }
+}
+
+template <int SF>
+__device__ __forceinline__ uint32_t post_tiles_of(const PostArgs &p) {
+  const uint32_t pw = (uint32_t)(p.width / SF), ph = (uint32_t)(p.height / SF);
+  return ((pw + POST_BX - 1u) / POST_BX) * ((ph + POST_BY - 1u) / POST_BY);
+}
+
+/* Post tiles of the viewports listed in views (all with ssaa SF). */
+template <int SF>
+__global__ void __launch_bounds__(POST_BX *POST_BY) k_b_post(const PostArgs *__restrict__ posts,
+                                                             const uint32_t *__restrict__ views,
+                                                             uint32_t n) {
+  __shared__ PostSmem<SF> sm;
+  __shared__ uint32_t s_pre[MOPCUDA_MAX_VIEWS + 1];
+  const uint32_t tid = threadIdx.y * POST_BX + threadIdx.x;
+  if (tid < 32u) {
+    uint32_t run = 0;
+    for (uint32_t base = 0; base < n; base += 32u) {
+      const uint32_t k = base + tid;
+      const uint32_t c = k < n ? post_tiles_of<SF>(posts[views[k]]) : 0u;
+      uint32_t incl = c;
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+        if (tid >= (uint32_t)o)
+          incl += y;
+      }
+      if (k < n)
+        s_pre[k] = run + incl - c;
+      run += __shfl_sync(0xffffffffu, incl, 31);
+    }
+    if (tid == 0)
+      s_pre[n] = run;
+  }
+  __syncthreads();
+  const uint32_t total = s_pre[n];
+  uint32_t k = 0;
+  for (uint32_t u = blockIdx.x; u < total; u += gridDim.x) {
+    while (s_pre[k + 1] <= u)
+      k++;
+    const PostArgs &p = posts[views[k]];
+    const uint32_t local = u - s_pre[k];
+    const uint32_t tx = ((uint32_t)(p.width / SF) + POST_BX - 1u) / POST_BX;
+    post_load_luts<SF>(p, sm);
+    post_tile<SF>(p, sm, (int)(local % tx), (int)(local / tx));
+  }
+}
+
+static int resident_blocks(const void *fn, int block) {
+  int nb = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, block, 0) != cudaSuccess) {
+    cudaGetLastError();
+    nb = 1;
+  }
+  return nb > 0 ? nb : 1;
+}
+
+void mopcuda_batch_grids(BatchLaunch &cfg) {
+  const int sms = cfg.num_sms > 0 ? cfg.num_sms : 148;
+  const int gm = cfg.grid_mul > 0 ? cfg.grid_mul : 1;
+  auto grid = [&](const void *fn, int block) { return sms * resident_blocks(fn, block) * gm; };
+  cfg.grid_vertex = grid((const void *)k_b_items<ST_VERTEX>, cfg.vertex_block);
+  cfg.grid_setup = grid((const void *)k_b_items<ST_SETUP>, cfg.setup_block);
+  cfg.grid_clip = grid((const void *)k_b_items<ST_CLIP>, 128);
+  cfg.grid_rsmall = grid((const void *)k_b_items<ST_RSMALL>, cfg.raster_block);
+  cfg.grid_rlarge = grid((const void *)k_b_items<ST_RLARGE>, cfg.large_block);
+  cfg.grid_shade = grid((const void *)k_b_shade, cfg.shade_block);
+}
+
+int mopcuda_launch_batch(const BatchArgs &b, const PostArgs *posts, const uint32_t *post_views[4],
+                         const uint32_t post_count[4], const uint32_t post_tiles[4],
+                         const BatchLaunch &cfg, cudaStream_t s) {
+  if (b.nv == 0)
+    return 0;
+  int launches = 0;
+  const int sms = cfg.num_sms > 0 ? cfg.num_sms : 148;
+  const uint32_t nv = b.nv;
+  const FrameArgs *fr = b.frames;
+  k_batch_prepare<<<nv, 256, 0, s>>>(b);
+  k_batch_alloc<<<1, 256, 0, s>>>(b);
+  k_b_items<ST_VERTEX><<<cfg.grid_vertex, cfg.vertex_block, 0, s>>>(fr, nv);
+  k_b_items<ST_SETUP><<<cfg.grid_setup, cfg.setup_block, 0, s>>>(fr, nv);
+  k_b_items<ST_CLIP><<<cfg.grid_clip, 128, 0, s>>>(fr, nv);
+  k_b_items<ST_RSMALL><<<cfg.grid_rsmall, cfg.raster_block, 0, s>>>(fr, nv);
+  k_b_large_scan<<<nv, 1024, 0, s>>>(fr);
+  k_b_items<ST_RLARGE><<<cfg.grid_rlarge, cfg.large_block, 0, s>>>(fr, nv);
+  k_b_resolve<<<sms * 8, 256, 0, s>>>(fr, nv);
+  k_b_shade<<<cfg.grid_shade, cfg.shade_block, 0, s>>>(fr, nv);
+  launches += 10;
+  dim3 pb(POST_BX, POST_BY);
+  for (int k = 0; k < 4; k++) {
+    if (!post_count[k] || !post_tiles[k])
+      continue;
+    const uint32_t g = post_tiles[k] < (uint32_t)(sms * 16) ? post_tiles[k] : (uint32_t)(sms * 16);
+    switch (k + 1) {
+    case 1:
+      k_b_post<1><<<g, pb, 0, s>>>(posts, post_views[k], post_count[k]);
+      break;
+    case 2:
+      k_b_post<2><<<g, pb, 0, s>>>(posts, post_views[k], post_count[k]);
+      break;
+    case 3:
+      k_b_post<3><<<g, pb, 0, s>>>(posts, post_views[k], post_count[k]);
+      break;
+    default:
+      k_b_post<4><<<g, pb, 0, s>>>(posts, post_views[k], post_count[k]);
+      break;
+    }
+    launches++;
+  }
+  return launches;
+}

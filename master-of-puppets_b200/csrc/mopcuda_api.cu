@@ -9,8 +9,7 @@
  * RHI implementation (src/backend/cpu/cpu_backend.c), with the per-draw
  * software rasterisation replaced by a deferred whole-frame device launch.
  */
-#include "../../include/mop_cuda.h"
-#include "mopcuda_internal.cuh"
+#include "api_internal.h"
 
 #include <math.h>
 #include <stdarg.h>
@@ -27,7 +26,7 @@
  * ------------------------------------------------------------------------ */
 static thread_local char g_err[512] = "";
 
-static int fail(int code, const char *fmt, ...) {
+int mc_fail(int code, const char *fmt, ...) {
   va_list ap;
   va_start(ap, fmt);
   vsnprintf(g_err, sizeof g_err, fmt, ap);
@@ -35,137 +34,7 @@ static int fail(int code, const char *fmt, ...) {
   return code;
 }
 
-#define CU_TRY(expr)                                                                      \
-  do {                                                                                    \
-    cudaError_t e_ = (expr);                                                              \
-    if (e_ != cudaSuccess)                                                                \
-      return fail(MOPCUDA_ECUDA, "%s: %s (%s:%d)", #expr, cudaGetErrorString(e_), __FILE__, \
-                  __LINE__);                                                              \
-  } while (0)
-
 extern "C" const char *mopcuda_last_error(void) { return g_err; }
-
-#define FRAME_TIMEOUT_MS 20000
-
-/* ------------------------------------------------------------------------
- * objects
- * ------------------------------------------------------------------------ */
-struct DevArena {
-  void *p = nullptr;
-  size_t cap = 0;
-  int ensure(size_t bytes) {
-    if (bytes <= cap)
-      return 0;
-    size_t n = bytes + bytes / 2 + 4096;
-    if (p)
-      cudaFree(p);
-    p = nullptr;
-    cap = 0;
-    if (cudaMalloc(&p, n) != cudaSuccess) {
-      cudaGetLastError();
-      return fail(MOPCUDA_ENOMEM, "cudaMalloc(%zu) failed", n);
-    }
-    cap = n;
-    return 0;
-  }
-  void release() {
-    if (p)
-      cudaFree(p);
-    p = nullptr;
-    cap = 0;
-  }
-  template <class T> T *as() const { return (T *)p; }
-};
-
-struct HostArena {
-  void *p = nullptr;
-  size_t cap = 0;
-  int ensure(size_t bytes) {
-    if (bytes <= cap)
-      return 0;
-    size_t n = bytes + bytes / 2 + 4096;
-    if (p)
-      cudaFreeHost(p);
-    p = nullptr;
-    cap = 0;
-    if (cudaMallocHost(&p, n) != cudaSuccess) {
-      cudaGetLastError();
-      return fail(MOPCUDA_ENOMEM, "cudaMallocHost(%zu) failed", n);
-    }
-    cap = n;
-    return 0;
-  }
-  void release() {
-    if (p)
-      cudaFreeHost(p);
-    p = nullptr;
-    cap = 0;
-  }
-  template <class T> T *as() const { return (T *)p; }
-};
-
-struct MopCudaBuffer {
-  void *d = nullptr;
-  void *h = nullptr; /* host shadow for buffer_read */
-  size_t size = 0;
-};
-
-struct MopCudaTexture {
-  int w = 0, h = 0;
-  bool hdr = false;
-  void *d = nullptr;
-  void *hcopy = nullptr;
-};
-
-struct MopCudaFramebuffer {
-  int w = 0, h = 0;
-  int ssaa = 1; /* presentation factor when known (fused SSAA output) */
-  DevArena pre, out, depth, ids, presented;
-  HostArena h_color, h_depth, h_ids;
-  bool host_color = false, host_depth = false, host_ids = false;
-  bool presented_valid = false;
-  uint64_t frame_serial = 0;
-};
-
-struct MopCudaDevice {
-  int ordinal = 0;
-  int num_sms = 148;
-  cudaStream_t stream = nullptr;
-  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-  cudaEvent_t stage_ev[MOPCUDA_STAGES + 1] = {};
-  bool stage_timing = false;
-  float stage_ms[MOPCUDA_STAGES] = {};
-  std::mutex mu;
-  /* recorded frame */
-  MopCudaFramebuffer *fb = nullptr;
-  float clear[4] = {0, 0, 0, 1};
-  std::vector<DrawRec> draws;
-  std::vector<LightRec> lights;
-  uint32_t unsupported_draws = 0;
-  uint32_t skipped_draws = 0;
-  bool frame_open = false;
-  bool pending = false;
-  int frame_status = 0;
-  /* state */
-  float exposure = 1.0f;
-  uint32_t post = MOPCUDA_POST_GAMMA | MOPCUDA_POST_FXAA;
-  float lut[256];
-  /* IBL */
-  DevArena irr, pf, brdf;
-  int irr_w = 0, irr_h = 0, pf_w = 0, pf_h = 0, pf_levels = 0, brdf_size = 0;
-  float ibl_rot = 0.0f, ibl_int = 1.0f;
-  bool ibl_on = false;
-  /* frame arenas */
-  DevArena d_draws, d_lights, clip, world, normal, color, rrec, srec, clipq, keys,
-      large_list, large_items, shade_list, counters, pick_xy, pick_out;
-  HostArena h_draws, h_lights, h_counters, h_pick;
-  uint32_t vertex_cap = 0, rec_cap = 0, clip_cap = 0, large_cap = 0;
-  uint32_t extra_hint = 0, rec_hint = 0, clip_hint = 0, large_hint = 0;
-  LaunchCfg cfg = {148, 128, 256, 4, 32, 4};
-  uint64_t launches = 0;
-  float last_ms = 0.0f;
-  uint64_t io_h2d = 0, io_d2h = 0; /* bytes moved by the last frame launch */
-};
 
 static int finish_frame(MopCudaDevice *d, int timeout_ms);
 
@@ -220,7 +89,7 @@ extern "C" MopCudaDevice *mopcuda_device_create(int ordinal) {
   return d;
 }
 
-static int bounded_sync(MopCudaDevice *d, cudaEvent_t ev, int timeout_ms) {
+int mc_bounded_sync(MopCudaDevice *d, cudaEvent_t ev, int timeout_ms) {
   struct timespec t0, t1;
   clock_gettime(CLOCK_MONOTONIC, &t0);
   for (;;) {
@@ -238,11 +107,11 @@ static int bounded_sync(MopCudaDevice *d, cudaEvent_t ev, int timeout_ms) {
   }
 }
 
-static int stream_sync(MopCudaDevice *d, int timeout_ms) {
+int mc_stream_sync(MopCudaDevice *d, int timeout_ms) {
   cudaEvent_t e;
   CU_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
   cudaEventRecord(e, d->stream);
-  int rc = bounded_sync(d, e, timeout_ms);
+  int rc = mc_bounded_sync(d, e, timeout_ms);
   cudaEventDestroy(e);
   return rc;
 }
@@ -251,7 +120,7 @@ extern "C" void mopcuda_device_destroy(MopCudaDevice *d) {
   if (!d)
     return;
   cudaSetDevice(d->ordinal);
-  stream_sync(d, 10000);
+  mc_stream_sync(d, 10000);
   DevArena *arenas[] = {&d->irr,      &d->pf,         &d->brdf,        &d->d_draws,
                         &d->d_lights, &d->clip,       &d->world,       &d->normal,
                         &d->color,    &d->rrec,       &d->srec,
@@ -314,7 +183,7 @@ extern "C" void mopcuda_buffer_destroy(MopCudaDevice *d, MopCudaBuffer *b) {
     return;
   std::lock_guard<std::mutex> lk(d->mu);
   cudaSetDevice(d->ordinal);
-  stream_sync(d, 10000); /* a launched frame may still read it */
+  mc_stream_sync(d, 10000); /* a launched frame may still read it */
   cudaFree(b->d);
   free(b->h);
   delete b;
@@ -326,7 +195,7 @@ extern "C" int mopcuda_buffer_update(MopCudaDevice *d, MopCudaBuffer *b, const v
     return fail(MOPCUDA_EINVAL, "buffer_update: range outside buffer");
   std::lock_guard<std::mutex> lk(d->mu);
   cudaSetDevice(d->ordinal);
-  int rc = stream_sync(d, 10000);
+  int rc = mc_stream_sync(d, 10000);
   if (rc)
     return rc;
   memcpy((uint8_t *)b->h + offset, data, size);
@@ -388,7 +257,7 @@ extern "C" void mopcuda_texture_destroy(MopCudaDevice *d, MopCudaTexture *t) {
     return;
   std::lock_guard<std::mutex> lk(d->mu);
   cudaSetDevice(d->ordinal);
-  stream_sync(d, 10000);
+  mc_stream_sync(d, 10000);
   cudaFree(t->d);
   free(t->hcopy);
   delete t;
@@ -460,7 +329,7 @@ extern "C" void mopcuda_framebuffer_destroy(MopCudaDevice *d, MopCudaFramebuffer
     return;
   std::lock_guard<std::mutex> lk(d->mu);
   cudaSetDevice(d->ordinal);
-  stream_sync(d, 10000);
+  mc_stream_sync(d, 10000);
   if (d->fb == fb)
     d->fb = nullptr;
   fb_release(fb);
@@ -472,7 +341,7 @@ extern "C" int mopcuda_framebuffer_resize(MopCudaDevice *d, MopCudaFramebuffer *
     return fail(MOPCUDA_EINVAL, "framebuffer_resize: %dx%d out of range", w, h);
   std::lock_guard<std::mutex> lk(d->mu);
   cudaSetDevice(d->ordinal);
-  int rc = stream_sync(d, 10000);
+  int rc = mc_stream_sync(d, 10000);
   if (rc)
     return rc;
   fb_release(fb);
@@ -501,7 +370,7 @@ extern "C" int mopcuda_set_ibl(MopCudaDevice *d, const float *irr, int iw, int i
     return fail(MOPCUDA_EINVAL, "set_ibl: no device");
   std::lock_guard<std::mutex> lk(d->mu);
   cudaSetDevice(d->ordinal);
-  int rc = stream_sync(d, 10000);
+  int rc = mc_stream_sync(d, 10000);
   if (rc)
     return rc;
   if (!irr) {
@@ -565,25 +434,24 @@ static float clamp01f(float x) { return x < 0.0f ? 0.0f : (x > 1.0f ? 1.0f : x);
  * zero-opacity draws are colour no-ops in the reference and are dropped;
  * blended, wireframe, depth-test-off and unlit smooth (edge-AA) draws depend
  * on submission order and are reported as unsupported. */
-static int record_draw(MopCudaDevice *d, const MopCudaDraw *c, const float *model,
-                       const float *mvp) {
+int mc_build_draw(const MopCudaDraw *c, const float *model, const float *mvp,
+                  std::vector<LightRec> &lights, DrawRec &r, bool &skip) {
+  skip = false;
   if (!c->vertex_buffer || !c->index_buffer)
     return fail(MOPCUDA_EINVAL, "draw: missing buffers");
   float op = clamp01f(c->opacity);
   if (op == 0.0f && c->blend_mode != 3) {
-    d->skipped_draws++;
+    skip = true;
     return MOPCUDA_OK;
   }
   bool lit = c->lights && c->light_count > 0;
   if (c->wireframe || !c->depth_test || !c->depth_write || c->blend_mode != 0 || op < 1.0f ||
       (c->smooth && !lit)) {
-    d->unsupported_draws++;
     return fail(MOPCUDA_EUNSUPPORTED,
                 "draw: blended / wireframe / depth-test-off / unlit-smooth state is not on "
                 "the order-independent path");
   }
   uint32_t stride = 48;
-  DrawRec r;
   memset(&r, 0, sizeof r);
   if (c->layout) {
     const MopCudaVertexLayout *L = c->layout;
@@ -652,7 +520,7 @@ static int record_draw(MopCudaDevice *d, const MopCudaDraw *c, const float *mode
     r.flags |= DF_CULL;
   if (lit) {
     r.flags |= DF_LIT;
-    r.light_off = (uint32_t)d->lights.size();
+    r.light_off = (uint32_t)lights.size();
     r.light_count = c->light_count;
     for (uint32_t i = 0; i < c->light_count; i++) {
       const MopCudaLight &s = c->lights[i];
@@ -676,10 +544,25 @@ static int record_draw(MopCudaDevice *d, const MopCudaDraw *c, const float *mode
         for (int k = 0; k < 3; k++)
           L.ndir[k] = L.direction[k] * inv;
       }
-      d->lights.push_back(L);
+      lights.push_back(L);
     }
   }
-  d->draws.push_back(r);
+  return MOPCUDA_OK;
+}
+
+static int record_draw(MopCudaDevice *d, const MopCudaDraw *c, const float *model,
+                       const float *mvp) {
+  DrawRec r;
+  bool skip = false;
+  int rc = mc_build_draw(c, model, mvp, d->lights, r, skip);
+  if (rc == MOPCUDA_EUNSUPPORTED)
+    d->unsupported_draws++;
+  if (rc)
+    return rc;
+  if (skip)
+    d->skipped_draws++;
+  else
+    d->draws.push_back(r);
   return MOPCUDA_OK;
 }
 
@@ -693,7 +576,7 @@ extern "C" int mopcuda_draw(MopCudaDevice *d, MopCudaFramebuffer *fb, const MopC
 }
 
 /* mop_mat4_multiply order (math.c:182-194): running sum from 0.0f. */
-static void mat4_mul(const float *a, const float *b, float *c) {
+void mc_mat4_mul(const float *a, const float *b, float *c) {
   float r[16];
   for (int col = 0; col < 4; col++)
     for (int row = 0; row < 4; row++) {
@@ -717,13 +600,56 @@ extern "C" int mopcuda_draw_instanced(MopCudaDevice *d, MopCudaFramebuffer *fb,
     return fail(MOPCUDA_EINVAL, "draw outside frame_begin/frame_end");
   for (uint32_t i = 0; i < n; i++) {
     float vm[16], mvp[16];
-    mat4_mul(view, inst + 16 * (size_t)i, vm);
-    mat4_mul(proj, vm, mvp);
+    mc_mat4_mul(view, inst + 16 * (size_t)i, vm);
+    mc_mat4_mul(proj, vm, mvp);
     int rc = record_draw(d, c, inst + 16 * (size_t)i, mvp);
     if (rc)
       return rc;
   }
   return MOPCUDA_OK;
+}
+
+
+void mc_ibl_consts(bool on, int pf_w, int pf_h, int pf_levels, int brdf_size, DrawRec *draws,
+                   uint32_t nd) {
+  if (on) {
+    /* per-draw IBL constants (rasterizer.c:243-265, 280-291), x86 float ops */
+    for (uint32_t i = 0; i < nd; i++) {
+      DrawRec &r = draws[i];
+      int level = (int)(r.roughness * (float)(pf_levels - 1));
+      if (level >= pf_levels)
+        level = pf_levels - 1;
+      if (level < 0)
+        level = 0; /* roughness < 0: undefined in the reference */
+      size_t off = 0;
+      for (int l = 0; l < level; l++) {
+        int lw = pf_w >> l, lh = pf_h >> l;
+        off += (size_t)(lw < 1 ? 1 : lw) * (size_t)(lh < 1 ? 1 : lh);
+      }
+      r.pf_off = (uint32_t)off;
+      r.pf_lw = pf_w >> level < 1 ? 1 : pf_w >> level;
+      r.pf_lh = pf_h >> level < 1 ? 1 : pf_h >> level;
+      float rough = r.roughness < 0.0f ? 0.0f : (r.roughness > 1.0f ? 1.0f : r.roughness);
+      int row = (int)(rough * (float)(brdf_size - 1) + 0.5f);
+      r.brdf_row = row >= brdf_size ? brdf_size - 1 : row;
+    }
+  }
+}
+
+void mc_post_args(const MopCudaDevice *d, PostArgs &p) {
+  memset(&p, 0, sizeof p);
+  p.effects = d->post & (MOPCUDA_POST_GAMMA | MOPCUDA_POST_TONEMAP | MOPCUDA_POST_VIGNETTE |
+                         MOPCUDA_POST_FXAA);
+  memcpy(p.lut, d->lut, sizeof p.lut);
+  for (int i = 0; i < 256; i++) {
+    float v = d->lut[i];
+    if (v > 1.0f)
+      v = 1.0f;
+    if (v < 0.0f)
+      v = 0.0f;
+    volatile float q = v * 255.0f + 0.5f; /* postprocess.c:110-112 */
+    p.lut8[i] = (uint8_t)(int)q;
+  }
 }
 
 static int launch_frame(MopCudaDevice *d) {
@@ -779,28 +705,7 @@ static int launch_frame(MopCudaDevice *d) {
   d->rec_cap = rcap;
   d->clip_cap = ccap;
   d->large_cap = lcap;
-  if (d->ibl_on) {
-    /* per-draw IBL constants (rasterizer.c:243-265, 280-291), x86 float ops */
-    for (uint32_t i = 0; i < nd; i++) {
-      DrawRec &r = d->draws[i];
-      int level = (int)(r.roughness * (float)(d->pf_levels - 1));
-      if (level >= d->pf_levels)
-        level = d->pf_levels - 1;
-      if (level < 0)
-        level = 0; /* roughness < 0: undefined in the reference */
-      size_t off = 0;
-      for (int l = 0; l < level; l++) {
-        int lw = d->pf_w >> l, lh = d->pf_h >> l;
-        off += (size_t)(lw < 1 ? 1 : lw) * (size_t)(lh < 1 ? 1 : lh);
-      }
-      r.pf_off = (uint32_t)off;
-      r.pf_lw = d->pf_w >> level < 1 ? 1 : d->pf_w >> level;
-      r.pf_lh = d->pf_h >> level < 1 ? 1 : d->pf_h >> level;
-      float rough = r.roughness < 0.0f ? 0.0f : (r.roughness > 1.0f ? 1.0f : r.roughness);
-      int row = (int)(rough * (float)(d->brdf_size - 1) + 0.5f);
-      r.brdf_row = row >= d->brdf_size ? d->brdf_size - 1 : row;
-    }
-  }
+  mc_ibl_consts(d->ibl_on, d->pf_w, d->pf_h, d->pf_levels, d->brdf_size, d->draws.data(), nd);
   if (nd)
     memcpy(d->h_draws.p, d->draws.data(), sizeof(DrawRec) * nd);
   if (!d->lights.empty())
@@ -850,9 +755,11 @@ static int launch_frame(MopCudaDevice *d) {
   a.pre = fb->pre.as<uchar4>();
   a.depth = fb->depth.as<float>();
   a.ids = fb->ids.as<uint32_t>();
+  a.small_side = d->cfg.small_side;
+  a.small_area = d->cfg.small_area;
 
   PostArgs p;
-  memset(&p, 0, sizeof p);
+  mc_post_args(d, p);
   p.pre = fb->pre.as<uchar4>();
   p.out = fb->out.as<uchar4>();
   int sf = fb->ssaa >= 1 && fb->ssaa <= 4 && fb->w % fb->ssaa == 0 && fb->h % fb->ssaa == 0
@@ -862,18 +769,6 @@ static int launch_frame(MopCudaDevice *d) {
   p.width = fb->w;
   p.height = fb->h;
   p.ssaa = sf;
-  p.effects = d->post & (MOPCUDA_POST_GAMMA | MOPCUDA_POST_TONEMAP | MOPCUDA_POST_VIGNETTE |
-                         MOPCUDA_POST_FXAA);
-  memcpy(p.lut, d->lut, sizeof p.lut);
-  for (int i = 0; i < 256; i++) {
-    float v = d->lut[i];
-    if (v > 1.0f)
-      v = 1.0f;
-    if (v < 0.0f)
-      v = 0.0f;
-    volatile float q = v * 255.0f + 0.5f; /* postprocess.c:110-112 */
-    p.lut8[i] = (uint8_t)(int)q;
-  }
 
   cudaStream_t s = d->stream;
   CU_TRY(cudaEventRecord(d->ev0, s));
@@ -912,7 +807,7 @@ extern "C" int mopcuda_frame_io_bytes(MopCudaDevice *d, uint64_t *h2d, uint64_t 
  * capacity overflowed (the counters say by how much). */
 static int finish_frame(MopCudaDevice *d, int timeout_ms) {
   for (int attempt = 0; d->pending; attempt++) {
-    int rc = bounded_sync(d, d->ev1, timeout_ms);
+    int rc = mc_bounded_sync(d, d->ev1, timeout_ms);
     if (rc) {
       d->pending = false;
       return rc;
@@ -989,7 +884,7 @@ static int fetch(MopCudaDevice *d, DevArena &src, HostArena &dst, size_t bytes, 
   if (valid)
     return MOPCUDA_OK;
   CU_TRY(cudaMemcpyAsync(dst.p, src.p, bytes, cudaMemcpyDeviceToHost, d->stream));
-  int rc = stream_sync(d, FRAME_TIMEOUT_MS);
+  int rc = mc_stream_sync(d, FRAME_TIMEOUT_MS);
   if (rc)
     return rc;
   valid = true;
@@ -1059,7 +954,7 @@ extern "C" int mopcuda_read_color_resolved(MopCudaDevice *d, MopCudaFramebuffer 
     src = fb->presented.p;
   }
   CU_TRY(cudaMemcpyAsync(out, src, need, cudaMemcpyDeviceToHost, d->stream));
-  return stream_sync(d, FRAME_TIMEOUT_MS);
+  return mc_stream_sync(d, FRAME_TIMEOUT_MS);
 }
 
 /* Presentation factor of a framebuffer: lets frame_end fuse the SSAA box
@@ -1135,7 +1030,7 @@ extern "C" int mopcuda_pick_batch(MopCudaDevice *d, MopCudaFramebuffer *fb, int 
   CU_TRY(cudaGetLastError());
   uint8_t *hb = d->h_pick.as<uint8_t>() + in_b;
   CU_TRY(cudaMemcpyAsync(hb, d->pick_out.p, out_b, cudaMemcpyDeviceToHost, s));
-  rc = stream_sync(d, FRAME_TIMEOUT_MS);
+  rc = mc_stream_sync(d, FRAME_TIMEOUT_MS);
   if (rc)
     return rc;
   memcpy(ids, hb, 4ull * n);
@@ -1176,7 +1071,7 @@ extern "C" int mopcuda_measure_fp32_peak(MopCudaDevice *d, double *gops) {
     cudaEventRecord(a, d->stream);
     d->launches += (uint64_t)mopcuda_launch_fp32_peak(tmp, blocks, iters, d->stream);
     cudaEventRecord(b, d->stream);
-    int rc = bounded_sync(d, b, FRAME_TIMEOUT_MS);
+    int rc = mc_bounded_sync(d, b, FRAME_TIMEOUT_MS);
     if (rc) {
       cudaFree(tmp);
       return rc;
@@ -1278,5 +1173,5 @@ extern "C" int mopcuda_pick_batch_noalloc(MopCudaDevice *d, MopCudaFramebuffer *
   CU_TRY(cudaMemcpyAsync(depths, odp, 4ull * n, cudaMemcpyDeviceToHost, s));
   CU_TRY(cudaMemcpyAsync(hits, oht, 4ull * n, cudaMemcpyDeviceToHost, s));
   CU_TRY(cudaEventRecord(ev, s));
-  return bounded_sync(d, ev, FRAME_TIMEOUT_MS);
+  return mc_bounded_sync(d, ev, FRAME_TIMEOUT_MS);
 }

@@ -120,7 +120,7 @@ struct Counters {
 /* Records whose clamped bbox exceeds these bounds are rasterised as
  * (row, RASTER_CHUNK-sample) items spread over many threads; smaller ones
  * by one thread each. */
-#define SMALL_MAX_SIDE 32
+#define SMALL_MAX_SIDE 32  /* default small-record limits */
 #define SMALL_MAX_AREA 128
 #define RASTER_CHUNK 32
 
@@ -166,6 +166,9 @@ struct FrameArgs {
   uchar4 *pre;     /* resolved RGBA8 before post effects */
   float *depth;
   uint32_t *ids;
+  /* small-record limits: bbox side and area (larger records are rasterised
+   * item-parallel) */
+  int small_side, small_area;
 };
 
 struct PostArgs {
@@ -208,11 +211,97 @@ __device__ __forceinline__ uint32_t depth_key(float z) {
 /* Launch shapes of the frame kernels (chosen by the autotuner). */
 struct LaunchCfg {
   int num_sms;
+  int small_side, small_area; /* FrameArgs::small_side / small_area */
   int raster_block;   /* threads per block of the small-record raster     */
   int shade_block;    /* threads per block of the shading kernel          */
   int shade_waves;    /* resident blocks per SM targeted by shading       */
   int post_bx, post_by;
 };
+
+/* ------------------------------------------------------------------------
+ * batched viewports over one resident scene
+ * ------------------------------------------------------------------------ */
+#define MOPCUDA_MAX_VIEWS 256
+
+/* One viewport of a batch: its camera, sample resolution and where its
+ * sample- and pixel-resolution buffers start in the batch pools. */
+struct ViewRec {
+  float view[16], proj[16];
+  float eye[3];
+  float clear[4];
+  int width, height; /* sample resolution */
+  int ssaa;
+  uint32_t pad;
+  unsigned long long sample_off; /* keys, shade list, pre, out, depth, ids */
+  unsigned long long pixel_off;  /* presented */
+};
+
+/* Mesh-local bounding sphere of a draw's vertices; r < 0 (or NaN) means the
+ * draw is never culled. */
+struct DrawBound {
+  float c[3];
+  float r;
+};
+
+/* Pool sizes that the allocation pass found too small; the host grows the
+ * pools to at least these and re-runs the batch. */
+struct BatchStatus {
+  uint32_t overflow; /* bit0 vertex, bit1 records, bit2 clip queue, bit3 large list */
+  uint32_t pad;
+  unsigned long long need_vertex, need_rec, need_clip, need_large;
+};
+
+struct BatchArgs {
+  const DrawRec *scene; /* scene draws: mvp, cam_eye, vbase and tbase unused */
+  const DrawBound *bounds;
+  uint32_t nd;
+  const ViewRec *views;
+  uint32_t nv;
+  FrameArgs *frames;  /* nv, filled by k_batch_prepare / k_batch_alloc */
+  DrawRec *view_draws; /* nv * nd: each viewport's visible draws */
+  Counters *ctr;      /* nv */
+  BatchStatus *status;
+  FrameArgs tmpl;     /* lights, IBL, exposure, small-record limits */
+  /* pools (per-viewport ranges assigned on the device) */
+  float4 *clip, *world, *normal, *color;
+  unsigned long long vertex_pool;
+  RasterRec *rrec;
+  ShadeRec *srec;
+  unsigned long long rec_pool;
+  uint32_t *clipq;
+  unsigned long long clip_pool;
+  uint32_t *large_list, *large_items;
+  unsigned long long large_pool;
+  unsigned long long *keys;
+  uint32_t *shade_list;
+  uchar4 *pre;
+  float *depth;
+  uint32_t *ids;
+  /* per-viewport reserves: clipped fans (records, extra vertices, clip
+   * queue) T * fan_num / 8 + 1024; large list T * large_num / 16 + 1024 */
+  uint32_t fan_num, large_num;
+};
+
+/* Per-stage launch shape of a batch (the autotuner's search space). */
+struct BatchLaunch {
+  int num_sms;
+  int vertex_block, setup_block, raster_block, large_block, shade_block;
+  int grid_mul; /* persistent grids: resident blocks per SM x grid_mul */
+  /* filled by mopcuda_batch_grids (occupancy queries, before any capture) */
+  int grid_vertex, grid_setup, grid_clip, grid_rsmall, grid_rlarge, grid_shade;
+};
+
+/* Computes the persistent grid sizes of cfg from the kernels' occupancy. */
+void mopcuda_batch_grids(BatchLaunch &cfg);
+
+/* Launches the device part of one batch on stream s: prepare, allocate,
+ * vertex, setup, clip, raster, resolve, shade and post (the caller clears
+ * counters and keys first).  post_views[k] lists the viewports with ssaa
+ * k+1 (device array, post_count[k] entries); posts holds each viewport's
+ * PostArgs.  Returns the number of kernels launched. */
+int mopcuda_launch_batch(const BatchArgs &b, const PostArgs *posts, const uint32_t *post_views[4],
+                         const uint32_t post_count[4], const uint32_t post_tiles[4],
+                         const BatchLaunch &cfg, cudaStream_t s);
 
 /* ev (optional, 7 events): stage boundaries
  * vertex | setup+clip | raster | resolve | shade | post */

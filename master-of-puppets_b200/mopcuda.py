@@ -53,6 +53,20 @@ class MopCudaDraw(C.Structure):
                 ("light_count", C.c_uint32), ("layout", C.POINTER(MopCudaVertexLayout))]
 
 
+class MopCudaView(C.Structure):
+    _fields_ = [("view", C.c_float * 16), ("proj", C.c_float * 16), ("eye", C.c_float * 3),
+                ("width", C.c_int), ("height", C.c_int), ("ssaa", C.c_int),
+                ("clear", C.c_float * 4)]
+
+
+class MopCudaBatchConfig(C.Structure):
+    _fields_ = [("small_side", C.c_int), ("small_area", C.c_int), ("vertex_block", C.c_int),
+                ("setup_block", C.c_int), ("raster_block", C.c_int), ("large_block", C.c_int),
+                ("shade_block", C.c_int), ("grid_mul", C.c_int)]
+
+
+BATCH_COLOR, BATCH_PRESENTED, BATCH_DEPTH, BATCH_IDS = 0, 1, 2, 3
+
 # (name, restype, argtypes) for every entry point of include/mop_cuda.h
 _P = C.c_void_p
 SIGNATURES = [
@@ -95,6 +109,24 @@ SIGNATURES = [
     ("mopcuda_stage_times", C.c_int, [_P, _P, C.c_int]),
     ("mopcuda_measure_fp32_peak", C.c_int, [_P, C.POINTER(C.c_double)]),
     ("mopcuda_frame_io_bytes", C.c_int, [_P, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
+    ("mopcuda_scene_create", _P, [_P]),
+    ("mopcuda_scene_destroy", None, [_P]),
+    ("mopcuda_scene_add_draw", C.c_int, [_P, C.POINTER(MopCudaDraw)]),
+    ("mopcuda_scene_set_model", C.c_int, [_P, C.c_uint32, _P]),
+    ("mopcuda_scene_draw_count", C.c_uint32, [_P]),
+    ("mopcuda_scene_triangle_count", C.c_uint64, [_P]),
+    ("mopcuda_batch_create", _P, [_P, C.POINTER(MopCudaView), C.c_uint32]),
+    ("mopcuda_batch_destroy", None, [_P]),
+    ("mopcuda_batch_set_views", C.c_int, [_P, C.POINTER(MopCudaView), C.c_uint32]),
+    ("mopcuda_batch_submit", C.c_int, [_P]),
+    ("mopcuda_batch_wait", C.c_int, [_P, C.c_int]),
+    ("mopcuda_batch_gpu_time_ms", C.c_float, [_P]),
+    ("mopcuda_batch_read", C.c_int, [_P, C.c_uint32, C.c_int, _P, C.c_size_t]),
+    ("mopcuda_batch_pick", C.c_int, [_P, C.c_uint32, _P, C.c_uint32, _P, _P, _P]),
+    ("mopcuda_batch_get_config", C.c_int, [_P, C.POINTER(MopCudaBatchConfig)]),
+    ("mopcuda_batch_set_config", C.c_int, [_P, C.POINTER(MopCudaBatchConfig)]),
+    ("mopcuda_batch_autotune", C.c_int, [_P, C.c_int, C.c_char_p, C.c_size_t]),
+    ("mopcuda_batch_device_bytes", C.c_uint64, [_P]),
     ("mopcuda_mat4_multiply", None, [_P, _P, _P]),
     ("mopcuda_mat4_compose_trs", None, [_P, _P, _P, _P]),
     ("mopcuda_camera_matrices", None, [_P, _P, _P, C.c_float, C.c_float, C.c_float, C.c_int,
@@ -151,6 +183,7 @@ def mat4_multiply(a, b):
 
 
 def camera_matrices(scene):
+    """View, projection and eye of a scene's (or a View's) camera."""
     view = np.zeros(16, np.float32)
     proj = np.zeros(16, np.float32)
     eye = np.zeros(3, np.float32)
@@ -212,8 +245,10 @@ class Device:
             self.h = None
 
 
-class SceneRenderer:
-    """Scene resident on one device; renders frames through the C ABI."""
+class _Resident:
+    """A scene's meshes, textures, lights and device state uploaded through
+    the C ABI (mop_viewport_add_mesh -> buffer_create, create_texture ->
+    texture_create, set_exposure / set_post_effects / set_ibl)."""
 
     def __init__(self, device: Device, scene, ibl=None):
         self.dev = device
@@ -239,11 +274,6 @@ class SceneRenderer:
             if not th:
                 raise RuntimeError(f"texture_create failed: {last_error()}")
             self.textures.append(th)
-        self.sw, self.sh = scene.width * scene.ssaa, scene.height * scene.ssaa
-        self.fb = L.mopcuda_framebuffer_create(d, self.sw, self.sh)
-        if not self.fb:
-            raise RuntimeError(f"framebuffer_create failed: {last_error()}")
-        _check(L.mopcuda_framebuffer_set_ssaa(self.fb, scene.ssaa), "framebuffer_set_ssaa")
         L.mopcuda_set_exposure(d, scene.exposure)
         L.mopcuda_set_post_effects(d, scene.post_effects)
         if ibl is not None:
@@ -253,8 +283,6 @@ class SceneRenderer:
         self.lights = (MopCudaLight * max(1, len(scene.lights)))()
         for k, l in enumerate(scene.lights):
             self.lights[k] = light_struct(l)
-        self.update_camera()
-        self.clear = (C.c_float * 4)(*scene.clear)
 
     def set_ibl(self, ibl):
         self._ibl = [_f32(ibl["irr"]), _f32(ibl["pf"]), _f32(ibl["brdf"])]
@@ -264,34 +292,78 @@ class SceneRenderer:
                                       brdf.ctypes.data, ibl["brdf_size"], ibl["rotation"],
                                       ibl["intensity"]), "set_ibl")
 
-    def update_camera(self):
+    def draw_struct(self, k, view=None, proj=None, eye=None) -> MopCudaDraw:
+        """EMIT_DRAW's draw call for mesh k (mvp = proj * (view * model))."""
         sc = self.scene
-        self.view, self.proj, self.eye = camera_matrices(sc)
-        amb = min(max(sc.ambient, 0.0), 1.0)
-        self.draws = []
-        for (m, vb, ib, vc, ic) in self.meshes:
-            dr = MopCudaDraw()
-            dr.vertex_buffer, dr.index_buffer = vb, ib
-            dr.vertex_count, dr.index_count = vc, ic
-            dr.object_id = m.object_id
-            dr.model[:] = [float(x) for x in m.transform]
-            dr.mvp[:] = [float(x) for x in mat4_multiply(self.proj, mat4_multiply(self.view, m.transform))]
-            dr.light_dir[:] = DEFAULT_LIGHT_DIR
-            dr.ambient = amb
-            dr.opacity = m.opacity
-            dr.metallic = m.metallic if m.has_material else 0.0
-            dr.roughness = m.roughness if m.has_material else 0.5
-            dr.depth_bias = 0.0
-            dr.cam_eye[:] = [float(x) for x in self.eye]
-            dr.smooth = 1 if getattr(sc, "smooth", True) else 0
-            dr.wireframe = 0
-            dr.depth_test = dr.depth_write = dr.backface_cull = 1
-            dr.blend_mode = 0
-            dr.texture = self.textures[m.texture] if m.texture >= 0 else None
-            dr.lights = self.lights
-            dr.light_count = len(sc.lights)
-            dr.layout = None
-            self.draws.append(dr)
+        m, vb, ib, vc, ic = self.meshes[k]
+        dr = MopCudaDraw()
+        dr.vertex_buffer, dr.index_buffer = vb, ib
+        dr.vertex_count, dr.index_count = vc, ic
+        dr.object_id = m.object_id
+        dr.model[:] = [float(x) for x in m.transform]
+        if view is not None:
+            dr.mvp[:] = [float(x) for x in mat4_multiply(proj, mat4_multiply(view, m.transform))]
+            dr.cam_eye[:] = [float(x) for x in eye]
+        dr.light_dir[:] = DEFAULT_LIGHT_DIR
+        dr.ambient = min(max(sc.ambient, 0.0), 1.0)
+        dr.opacity = m.opacity
+        dr.metallic = m.metallic if m.has_material else 0.0
+        dr.roughness = m.roughness if m.has_material else 0.5
+        dr.depth_bias = 0.0
+        dr.smooth = 1 if getattr(sc, "smooth", True) else 0
+        dr.wireframe = 0
+        dr.depth_test = dr.depth_write = dr.backface_cull = 1
+        dr.blend_mode = 0
+        dr.texture = self.textures[m.texture] if m.texture >= 0 else None
+        dr.lights = self.lights
+        dr.light_count = len(sc.lights)
+        dr.layout = None
+        return dr
+
+    def close_resident(self):
+        L, d = self.L, self.dev.h
+        if not d:
+            return
+        for b in self._buffers:
+            L.mopcuda_buffer_destroy(d, b)
+        for t in self.textures:
+            L.mopcuda_texture_destroy(d, t)
+        self._buffers, self.textures = [], []
+
+
+class SceneRenderer(_Resident):
+    """Scene resident on one device; renders frames through the C ABI."""
+
+    def __init__(self, device: Device, scene, ibl=None):
+        super().__init__(device, scene, ibl)
+        L, d = self.L, device.h
+        self.sw, self.sh = scene.width * scene.ssaa, scene.height * scene.ssaa
+        self.fb = L.mopcuda_framebuffer_create(d, self.sw, self.sh)
+        if not self.fb:
+            raise RuntimeError(f"framebuffer_create failed: {last_error()}")
+        _check(L.mopcuda_framebuffer_set_ssaa(self.fb, scene.ssaa), "framebuffer_set_ssaa")
+        self.update_camera()
+        self.clear = (C.c_float * 4)(*scene.clear)
+
+    def set_view(self, v):
+        """Re-targets the frame to a viewport of another size / SSAA / camera
+        (framebuffer_resize, then new per-draw matrices)."""
+        import dataclasses
+        self.scene = dataclasses.replace(self.scene, width=v.width, height=v.height, ssaa=v.ssaa,
+                                         eye=v.eye, target=v.target, up=v.up, fov_deg=v.fov_deg,
+                                         near=v.near, far=v.far, clear=v.clear)
+        sc = self.scene
+        self.sw, self.sh = sc.width * sc.ssaa, sc.height * sc.ssaa
+        _check(self.L.mopcuda_framebuffer_resize(self.dev.h, self.fb, self.sw, self.sh),
+               "framebuffer_resize")
+        _check(self.L.mopcuda_framebuffer_set_ssaa(self.fb, sc.ssaa), "framebuffer_set_ssaa")
+        self.clear = (C.c_float * 4)(*sc.clear)
+        self.update_camera()
+
+    def update_camera(self):
+        self.view, self.proj, self.eye = camera_matrices(self.scene)
+        self.draws = [self.draw_struct(k, self.view, self.proj, self.eye)
+                      for k in range(len(self.meshes))]
 
     def submit(self):
         """Record and launch one frame (asynchronous)."""
@@ -354,10 +426,126 @@ class SceneRenderer:
         L, d = self.L, self.dev.h
         if not d:
             return
-        for b in self._buffers:
-            L.mopcuda_buffer_destroy(d, b)
-        for t in self.textures:
-            L.mopcuda_texture_destroy(d, t)
         if self.fb:
             L.mopcuda_framebuffer_destroy(d, self.fb)
-        self._buffers, self.textures, self.fb = [], [], None
+        self.fb = None
+        self.close_resident()
+
+
+def view_struct(v) -> MopCudaView:
+    """MopCudaView of a scenes.View (camera derived as for a frame)."""
+    s = MopCudaView()
+    view, proj, eye = camera_matrices(v)
+    s.view[:] = [float(x) for x in view]
+    s.proj[:] = [float(x) for x in proj]
+    s.eye[:] = [float(x) for x in eye]
+    s.width, s.height, s.ssaa = v.width, v.height, v.ssaa
+    s.clear[:] = [float(x) for x in v.clear]
+    return s
+
+
+class BatchRenderer(_Resident):
+    """A resident scene rendered into many viewports per graph launch
+    (mopcuda_scene_* / mopcuda_batch_*)."""
+
+    def __init__(self, device: Device, scene, views, ibl=None):
+        super().__init__(device, scene, ibl)
+        L = self.L
+        self.sh_scene = L.mopcuda_scene_create(device.h)
+        if not self.sh_scene:
+            raise RuntimeError(f"scene_create failed: {last_error()}")
+        self._draws = [self.draw_struct(k) for k in range(len(self.meshes))]
+        for dr in self._draws:
+            rc = L.mopcuda_scene_add_draw(self.sh_scene, C.byref(dr))
+            if rc < 0:
+                raise MopCudaError(rc, "scene_add_draw")
+        self.views = list(views)
+        arr = (MopCudaView * len(self.views))(*[view_struct(v) for v in self.views])
+        self.h = L.mopcuda_batch_create(self.sh_scene, arr, len(self.views))
+        if not self.h:
+            raise RuntimeError(f"batch_create failed: {last_error()}")
+
+    @property
+    def samples(self) -> int:
+        return sum(v.samples for v in self.views)
+
+    @property
+    def pixels(self) -> int:
+        return sum(v.pixels for v in self.views)
+
+    def set_views(self, views):
+        views = list(views)
+        arr = (MopCudaView * len(views))(*[view_struct(v) for v in views])
+        _check(self.L.mopcuda_batch_set_views(self.h, arr, len(views)), "batch_set_views")
+        self.views = views
+
+    def set_model(self, k: int, model):
+        m = _f32(model)
+        _check(self.L.mopcuda_scene_set_model(self.sh_scene, k, m.ctypes.data), "scene_set_model")
+
+    def submit(self):
+        _check(self.L.mopcuda_batch_submit(self.h), "batch_submit")
+
+    def wait(self, timeout_ms: int = 20000):
+        _check(self.L.mopcuda_batch_wait(self.h, timeout_ms), "batch_wait")
+
+    def render(self):
+        self.submit()
+        self.wait()
+        return self
+
+    @property
+    def gpu_ms(self) -> float:
+        return float(self.L.mopcuda_batch_gpu_time_ms(self.h))
+
+    def read(self, i: int, what: int, out=None):
+        v = self.views[i]
+        sw, sh = v.width * v.ssaa, v.height * v.ssaa
+        shape, dt = {BATCH_COLOR: ((sh, sw, 4), np.uint8),
+                     BATCH_PRESENTED: ((v.height, v.width, 4), np.uint8),
+                     BATCH_DEPTH: ((sh, sw), np.float32),
+                     BATCH_IDS: ((sh, sw), np.uint32)}[what]
+        if out is None:
+            out = np.empty(shape, dt)
+        _check(self.L.mopcuda_batch_read(self.h, i, what, out.ctypes.data, out.nbytes), "batch_read")
+        return out
+
+    def pick(self, i: int, xy):
+        xy = np.ascontiguousarray(xy, np.int32)
+        n = xy.shape[0]
+        ids = np.zeros(n, np.uint32)
+        dep = np.zeros(n, np.float32)
+        hits = np.zeros(n, np.int32)
+        _check(self.L.mopcuda_batch_pick(self.h, i, xy.ctypes.data, n, ids.ctypes.data,
+                                         dep.ctypes.data, hits.ctypes.data), "batch_pick")
+        return ids, dep, hits
+
+    def config(self) -> dict:
+        c = MopCudaBatchConfig()
+        _check(self.L.mopcuda_batch_get_config(self.h, C.byref(c)), "batch_get_config")
+        return {f: getattr(c, f) for f, _ in MopCudaBatchConfig._fields_}
+
+    def set_config(self, **kw):
+        cur = self.config()
+        cur.update(kw)
+        c = MopCudaBatchConfig(**cur)
+        _check(self.L.mopcuda_batch_set_config(self.h, C.byref(c)), "batch_set_config")
+
+    def autotune(self, reps: int = 5) -> dict:
+        import json
+        buf = C.create_string_buffer(8192)
+        _check(self.L.mopcuda_batch_autotune(self.h, reps, buf, len(buf)), "batch_autotune")
+        return json.loads(buf.value.decode())
+
+    @property
+    def device_bytes(self) -> int:
+        return int(self.L.mopcuda_batch_device_bytes(self.h))
+
+    def close(self):
+        if self.h:
+            self.L.mopcuda_batch_destroy(self.h)
+            self.h = None
+        if self.sh_scene:
+            self.L.mopcuda_scene_destroy(self.sh_scene)
+            self.sh_scene = None
+        self.close_resident()

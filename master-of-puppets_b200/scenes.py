@@ -407,6 +407,59 @@ def coplanar_scene(seed: int = 3, width: int = 192, height: int = 144) -> Scene:
     return sc
 
 
+@dataclasses.dataclass
+class View:
+    """One viewport of a batch: presented size, SSAA factor and camera."""
+    width: int
+    height: int
+    ssaa: int
+    eye: Tuple[float, float, float]
+    target: Tuple[float, float, float]
+    up: Tuple[float, float, float] = (0.0, 1.0, 0.0)
+    fov_deg: float = 50.0
+    near: float = 0.5
+    far: float = 200.0
+    clear: Tuple[float, float, float, float] = (0.12, 0.13, 0.16, 1.0)
+
+    @property
+    def samples(self) -> int:
+        return self.width * self.ssaa * self.height * self.ssaa
+
+    @property
+    def pixels(self) -> int:
+        return self.width * self.height
+
+
+def batch_views(scene: Scene, n: int = 64, seed: int = 4, min_px: int = 128 * 128,
+                max_px: int = 1920 * 1080, radius=(15.0, 40.0)) -> List[View]:
+    """Viewports of the batched workload over `scene`: presented pixel counts
+    log-uniform in [min_px, max_px], aspect ratio log-uniform in [0.5, 2],
+    ssaa 1 or 2, cameras on a sphere of radius U[radius] around the origin
+    looking at a random instance's position."""
+    rng = np.random.default_rng(seed)
+    targets = [tuple(float(x) for x in m.transform[12:15]) for m in scene.meshes] or [(0.0, 0.0, 0.0)]
+    views = []
+    for _ in range(n):
+        px = math.exp(rng.uniform(math.log(min_px), math.log(max_px)))
+        aspect = math.exp(rng.uniform(math.log(0.5), math.log(2.0)))
+        w = max(16, int(round(math.sqrt(px * aspect))))
+        h = max(16, int(round(px / w)))
+        ssaa = int(rng.integers(1, 3))
+        d = rng.normal(size=3)
+        d /= np.linalg.norm(d)
+        eye = tuple(float(x) for x in d * rng.uniform(*radius))
+        tgt = targets[int(rng.integers(0, len(targets)))]
+        views.append(View(w, h, ssaa, eye, tgt, clear=scene.clear))
+    return views
+
+
+def scene_for_view(scene: Scene, v: View) -> Scene:
+    """The single-viewport scene a batch viewport corresponds to."""
+    return dataclasses.replace(scene, width=v.width, height=v.height, ssaa=v.ssaa, eye=v.eye,
+                               target=v.target, up=v.up, fov_deg=v.fov_deg, near=v.near,
+                               far=v.far, clear=v.clear)
+
+
 def procedural_ibl(sun_dir=(0.4, 0.8, 0.35), irr_size=(64, 32), pf_size=(128, 64), levels=5,
                    brdf_size=256, rotation=0.0, intensity=1.0) -> dict:
     """Seedless procedural sky and derived IBL maps with the reference's map

@@ -1,0 +1,160 @@
+"""Batched viewports (mopcuda_scene_* / mopcuda_batch_*): every viewport of a
+batch equals the single-viewport frame of the same draws and camera, byte
+for byte (colour at sample and presented resolution, depth bits, object IDs,
+picks), under any launch configuration, after the autotuner, after TRS
+updates, and when the pools must grow.  One batch is also checked against
+the oracle directly.
+"""
+import dataclasses
+
+import numpy as np
+import pytest
+
+import cpu_oracle
+import mopcuda
+import scenes
+from parity import assert_frame_parity
+
+pytestmark = pytest.mark.gpu
+
+
+def _plain(dev, sc, ibl):
+    r = mopcuda.SceneRenderer(dev, sc, ibl)
+    try:
+        r.render()
+        return {"color_full": r.color_full(), "color": r.color(), "depth": r.depth(),
+                "object_id": r.object_id(), "pick": r.pick(scenes.pick_points(sc, 64, seed=3))}
+    finally:
+        r.close()
+
+
+def _batch_view(b, i):
+    v = b.views[i]
+    sc_pts = scenes.pick_points(dataclasses.replace(b.scene, width=v.width, height=v.height), 64,
+                                seed=3)
+    return {"color_full": b.read(i, mopcuda.BATCH_COLOR),
+            "color": b.read(i, mopcuda.BATCH_PRESENTED),
+            "depth": b.read(i, mopcuda.BATCH_DEPTH),
+            "object_id": b.read(i, mopcuda.BATCH_IDS),
+            "pick": b.pick(i, sc_pts)}
+
+
+def _assert_same(got, want, label):
+    for k in ("color_full", "color", "object_id"):
+        assert got[k].shape == want[k].shape, f"{label}: {k} shape"
+        n = int((got[k] != want[k]).sum())
+        assert n == 0, f"{label}: {k} differs in {n} entries"
+    nd = int((got["depth"].view(np.uint32) != want["depth"].view(np.uint32)).sum())
+    assert nd == 0, f"{label}: depth differs in {nd} samples"
+    for a, b in zip(got["pick"], want["pick"]):
+        assert (np.asarray(a).view(np.uint32) == np.asarray(b).view(np.uint32)).all(), label
+
+
+def _scene(instances=24, tex=64):
+    return scenes.config2(width=320, height=180, ssaa=2, instances=instances, tex_size=tex)
+
+
+def _views(sc, n, seed, max_px=320 * 240):
+    vs = scenes.batch_views(sc, n=n, seed=seed, min_px=24 * 24, max_px=max_px)
+    vs[0] = dataclasses.replace(vs[0], ssaa=3)  # all SSAA templates
+    return vs
+
+
+def _check_batch(dev, b, sc, ibl, label):
+    for i, v in enumerate(b.views):
+        want = _plain(dev, scenes.scene_for_view(sc, v), ibl)
+        _assert_same(_batch_view(b, i), want, f"{label} view {i} ({v.width}x{v.height}x{v.ssaa})")
+
+
+@pytest.fixture(scope="module")
+def ibl():
+    return scenes.procedural_ibl((0.4, 0.8, 0.35), irr_size=(32, 16), pf_size=(64, 32),
+                                 levels=4, brdf_size=64)
+
+
+def test_batch_equals_single_viewport_frames(cuda_device, ibl):
+    sc = _scene()
+    b = mopcuda.BatchRenderer(cuda_device, sc, _views(sc, 10, seed=1), ibl)
+    try:
+        b.render()
+        _check_batch(cuda_device, b, sc, ibl, "batch")
+        # a second launch of the captured graph gives the same bytes
+        first = [_batch_view(b, i) for i in range(len(b.views))]
+        b.render()
+        for i in range(len(b.views)):
+            _assert_same(_batch_view(b, i), first[i], f"replay view {i}")
+    finally:
+        b.close()
+
+
+def test_batch_matches_oracle(cuda_device):
+    sc = scenes.small_scene(seed=4, width=96, height=72)
+    views = [scenes.View(96, 72, 1, sc.eye, sc.target, fov_deg=sc.fov_deg, near=sc.near,
+                         far=sc.far, clear=sc.clear),
+             scenes.View(64, 40, 2, (3.0, 4.0, 6.0), (0.0, 0.3, 0.0), fov_deg=40.0, near=0.1,
+                         far=50.0, clear=sc.clear)]
+    b = mopcuda.BatchRenderer(cuda_device, sc, views)
+    try:
+        b.render()
+        for i, v in enumerate(views):
+            ref = cpu_oracle.render(scenes.scene_for_view(sc, v), None)
+            got = _batch_view(b, i)
+            assert_frame_parity(got, ref, f"oracle view {i}")
+    finally:
+        b.close()
+
+
+def test_batch_launch_configs_and_autotune_do_not_change_results(cuda_device, ibl):
+    sc = _scene(instances=16)
+    b = mopcuda.BatchRenderer(cuda_device, sc, _views(sc, 6, seed=2), ibl)
+    try:
+        b.render()
+        base = [_batch_view(b, i) for i in range(len(b.views))]
+        for cfg in ({"small_side": 8, "small_area": 16, "raster_block": 64},
+                    {"small_side": 64, "small_area": 4096, "shade_block": 128, "grid_mul": 2},
+                    {"setup_block": 128, "vertex_block": 128, "large_block": 128}):
+            b.set_config(**cfg)
+            b.render()
+            for i in range(len(b.views)):
+                _assert_same(_batch_view(b, i), base[i], f"config {cfg} view {i}")
+        rep = b.autotune(reps=2)
+        assert rep["best_ms"] > 0 and len(rep["trials"]) >= 5
+        b.render()
+        for i in range(len(b.views)):
+            _assert_same(_batch_view(b, i), base[i], f"autotuned view {i}")
+    finally:
+        b.close()
+
+
+def test_batch_trs_update_and_camera_change(cuda_device, ibl):
+    sc = _scene(instances=12)
+    views = _views(sc, 4, seed=3)
+    b = mopcuda.BatchRenderer(cuda_device, sc, views, ibl)
+    try:
+        b.render()
+        rng = np.random.default_rng(0)
+        for k in (1, 5):
+            t = sc.meshes[k].transform.copy()
+            t[12:15] += rng.uniform(-2, 2, 3).astype(np.float32)
+            sc.meshes[k] = dataclasses.replace(sc.meshes[k], transform=t)
+            b.set_model(k, t)
+        moved = [dataclasses.replace(v, eye=tuple(np.array(v.eye) * 1.1)) for v in views]
+        b.set_views(moved)
+        b.render()
+        _check_batch(cuda_device, b, sc, ibl, "after update")
+    finally:
+        b.close()
+
+
+def test_batch_pool_growth(cuda_device, ibl):
+    """Views that all see the whole scene need more than the first pools:
+    the batch grows them, re-runs, and still equals the single frames."""
+    sc = _scene(instances=10)
+    v = scenes.View(200, 120, 1, (0.0, 10.0, 60.0), (0.0, 0.0, 0.0), clear=sc.clear)
+    views = [dataclasses.replace(v, eye=(float(x), 10.0, 60.0)) for x in (-6, -2, 2, 6)]
+    b = mopcuda.BatchRenderer(cuda_device, sc, views, ibl)
+    try:
+        b.render()
+        _check_batch(cuda_device, b, sc, ibl, "growth")
+    finally:
+        b.close()
