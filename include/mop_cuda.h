@@ -315,6 +315,74 @@ int mopcuda_batch_autotune(MopCudaBatch *batch, int reps, char *report, size_t r
 /* Bytes of device memory the batch holds (buffers + pools). */
 uint64_t mopcuda_batch_device_bytes(const MopCudaBatch *batch);
 
+/* ---- serving -----------------------------------------------------------
+ * No counterpart in the reference (it renders on the caller's thread).  A
+ * server keeps scenes resident and serves render and pick requests from any
+ * thread with continuous batching: one worker admits queued requests in
+ * arrival order while the estimated device bytes of the work in flight stay
+ * within hbm_budget and a launch slot is free, fuses up to max_views of
+ * them (any mix of scenes) into one launch on the slot's stream, and keeps
+ * admitting new arrivals into the next free slot while earlier launches
+ * run.  A request larger than the budget runs alone.  Results equal the
+ * request's own frame (mopcuda_frame_* of the same draws and camera),
+ * whatever it was batched with.  Scenes added to a server take no further
+ * draws (mopcuda_scene_add_draw fails) until the server is destroyed; model
+ * matrices may change at any time and a request sees them as of its launch. */
+typedef struct MopCudaServer MopCudaServer;
+
+typedef struct MopCudaServerConfig {
+  uint64_t hbm_budget;      /* bytes of in-flight work (framebuffers + pools) */
+  uint32_t max_views;       /* requests fused into one launch, 1..256 */
+  uint32_t max_inflight;    /* launches on the device at once, 1..16 */
+  uint32_t batch_window_us; /* after a launch, wait this long for more arrivals */
+} MopCudaServerConfig;
+
+#define MOPCUDA_REQ_RENDER 0u
+#define MOPCUDA_REQ_PICK 1u
+
+typedef struct MopCudaRequest {
+  uint32_t kind;  /* MOPCUDA_REQ_RENDER or MOPCUDA_REQ_PICK */
+  uint32_t scene; /* id from mopcuda_server_add_scene */
+  MopCudaView view;
+  /* RENDER: presented RGBA8 (width*height*4 bytes) and optionally the
+   * sample-resolution object IDs and depth; NULL skips a buffer.  The
+   * memory must stay valid until mopcuda_server_wait returns. */
+  uint8_t *color;
+  uint32_t *ids;
+  float *depth;
+  /* PICK: pick_n presented-pixel coordinates (copied at submit) and their
+   * results, as mopcuda_pick_batch.  The view is rendered for visibility
+   * only (no shading). */
+  const int32_t *pick_xy;
+  uint32_t pick_n;
+  uint32_t *pick_ids;
+  float *pick_depths;
+  int32_t *pick_hits;
+} MopCudaRequest;
+
+typedef struct MopCudaServerStats {
+  uint64_t submitted, completed, failed;
+  uint64_t launches, launched_views, reruns;
+  uint64_t peak_inflight_bytes; /* estimated bytes admitted at once */
+  uint64_t device_bytes;        /* device memory the launch slots hold now */
+  uint32_t max_views_in_launch;
+  uint32_t pad;
+} MopCudaServerStats;
+
+MopCudaServer *mopcuda_server_create(MopCudaDevice *dev, const MopCudaServerConfig *cfg);
+/* Finishes the queued work, then frees the server (not its scenes). */
+void mopcuda_server_destroy(MopCudaServer *srv);
+/* Returns the scene's id (>= 0) or an error code. */
+int mopcuda_server_add_scene(MopCudaServer *srv, MopCudaScene *scene);
+int mopcuda_server_submit(MopCudaServer *srv, const MopCudaRequest *req, uint64_t *ticket);
+/* Waits up to timeout_ms (0 polls) for a request; on completion returns its
+ * status, writes the arrival-to-result latency and forgets the ticket.
+ * MOPCUDA_ETIMEOUT: still queued or running. */
+int mopcuda_server_wait(MopCudaServer *srv, uint64_t ticket, int timeout_ms, double *latency_ms);
+/* Waits until nothing is queued or running. */
+int mopcuda_server_drain(MopCudaServer *srv, int timeout_ms);
+int mopcuda_server_stats(MopCudaServer *srv, MopCudaServerStats *stats);
+
 /* ---- host-side matrices (the device receives finished matrices) ------- */
 /* out = a * b, column-major (mop_mat4_multiply, reference math.c:182-194). */
 void mopcuda_mat4_multiply(const float a[16], const float b[16], float out[16]);

@@ -1,20 +1,20 @@
 /*
- * batch_api.cu — batched viewports over a resident scene (C ABI in
+ * batch_api.cu — resident scenes and batched viewports (C ABI in
  * include/mop_cuda.h, "batched viewports").
  *
  * A MopCudaScene keeps the draw records of a scene on the host (the same
  * DrawRec the per-viewport path builds, so every per-draw constant is
- * identical).  A MopCudaBatch binds a scene to up to 256 viewports and
- * renders all of them with one CUDA graph: H2D of cameras and draw records,
- * counter/key clears, then one launch per pipeline stage covering every
- * viewport (kernels.cu, "Batched viewports"), and a D2H of the pool status.
- * The graph is captured once per pool layout / launch configuration and
- * replayed per submit.
+ * identical) plus device copies of its draw bounds, lights and IBL maps.  A
+ * LaunchCore renders N viewports over one or more scenes in one stream
+ * sequence: H2D of cameras and draw tables, counter/key clears, one launch
+ * per pipeline stage covering every viewport (kernels.cu, "Batched
+ * viewports") and a D2H of the pool status.  A MopCudaBatch captures that
+ * sequence once as a CUDA graph and replays it per submit.
  *
  * No counterpart in the reference: mop_viewport_render renders one viewport
  * per call (viewport.c:2990-3320).
  */
-#include "api_internal.h"
+#include "batch_internal.h"
 
 #include <math.h>
 #include <stdio.h>
@@ -24,67 +24,65 @@
 #include <string>
 #include <vector>
 
-struct MopCudaScene {
-  MopCudaDevice *dev = nullptr;
-  std::vector<DrawRec> draws;
-  std::vector<LightRec> lights;
-  std::vector<DrawBound> bounds;
-  uint64_t tris = 0, verts = 0;
-  uint64_t version = 0; /* bumps when draws are added */
-  std::mutex mu;
-};
-
-struct MopCudaBatch {
-  MopCudaScene *scene = nullptr;
-  MopCudaDevice *dev = nullptr;
-  uint32_t nv = 0;
-  std::vector<ViewRec> vrec;
-  std::vector<PostArgs> posts;
-  std::vector<uint32_t> post_list[4];
-  uint32_t post_count[4] = {0, 0, 0, 0}, post_tiles[4] = {0, 0, 0, 0};
-  cudaStream_t stream = nullptr;
-  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-  /* per-launch inputs and bookkeeping */
-  DevArena d_views, d_frames, d_view_draws, d_ctr, d_status, d_posts, d_post_views, d_draws,
-      d_lights, d_bounds;
-  HostArena h_views, h_draws, h_status;
-  uint64_t scene_version = ~0ull;
-  uint32_t nd = 0;
-  /* work pools (carved per viewport on the device) */
-  DevArena clip, world, normal, color, rrec, srec, clipq, large_list, large_items;
-  unsigned long long vertex_pool = 0, rec_pool = 0, clip_pool = 0, large_pool = 0;
-  uint32_t fan_num = 1, large_num = 1; /* per-viewport reserve numerators */
-  /* sample / pixel buffers */
-  DevArena keys, shade_list, pre, out, depth, ids, presented, pick_xy, pick_out;
-  DevArena irr, pf, brdf; /* the batch's copy of the device's IBL maps */
-  HostArena h_pick;
-  unsigned long long total_samples = 0, total_pixels = 0;
-  /* launch shape */
-  MopCudaBatchConfig cfg = {SMALL_MAX_SIDE, SMALL_MAX_AREA, 256, 256, 128, 256, 256, 1};
-  FrameArgs tmpl;
-  cudaGraph_t graph = nullptr;
-  cudaGraphExec_t exec = nullptr;
-  bool pending = false;
-  float last_ms = 0.0f;
-  uint64_t launches = 0;
-  std::mutex mu;
-};
-
-
 /* ------------------------------------------------------------------------
  * scene
  * ------------------------------------------------------------------------ */
+static int copy_ibl(MopCudaScene *s, const MopCudaDevice *d) {
+  s->ibl_on = d->ibl_on;
+  if (!d->ibl_on)
+    return MOPCUDA_OK;
+  size_t pf_px = 0;
+  for (int l = 0; l < d->pf_levels; l++) {
+    int lw = d->pf_w >> l, lh = d->pf_h >> l;
+    pf_px += (size_t)(lw < 1 ? 1 : lw) * (size_t)(lh < 1 ? 1 : lh);
+  }
+  const size_t ib = (size_t)d->irr_w * d->irr_h * 16, pb = pf_px * 16,
+               bb = (size_t)d->brdf_size * d->brdf_size * 16;
+  if (s->irr.ensure(ib) || s->pf.ensure(pb) || s->brdf.ensure(bb))
+    return MOPCUDA_ENOMEM;
+  CU_TRY(cudaMemcpy(s->irr.p, d->irr.p, ib, cudaMemcpyDeviceToDevice));
+  CU_TRY(cudaMemcpy(s->pf.p, d->pf.p, pb, cudaMemcpyDeviceToDevice));
+  CU_TRY(cudaMemcpy(s->brdf.p, d->brdf.p, bb, cudaMemcpyDeviceToDevice));
+  s->irr_w = d->irr_w;
+  s->irr_h = d->irr_h;
+  s->pf_w = d->pf_w;
+  s->pf_h = d->pf_h;
+  s->pf_levels = d->pf_levels;
+  s->brdf_size = d->brdf_size;
+  s->ibl_rot = d->ibl_rot;
+  s->ibl_int = d->ibl_int;
+  return MOPCUDA_OK;
+}
+
 extern "C" MopCudaScene *mopcuda_scene_create(MopCudaDevice *dev) {
   if (!dev) {
     fail(MOPCUDA_EINVAL, "scene_create: no device");
     return nullptr;
   }
+  cudaSetDevice(dev->ordinal);
   MopCudaScene *s = new MopCudaScene();
   s->dev = dev;
+  {
+    std::lock_guard<std::mutex> lk(dev->mu);
+    if (mc_stream_sync(dev, 10000) || copy_ibl(s, dev)) {
+      delete s;
+      return nullptr;
+    }
+  }
   return s;
 }
 
-extern "C" void mopcuda_scene_destroy(MopCudaScene *s) { delete s; }
+extern "C" void mopcuda_scene_destroy(MopCudaScene *s) {
+  if (!s)
+    return;
+  cudaSetDevice(s->dev->ordinal);
+  s->d_bounds.release();
+  s->d_lights.release();
+  s->irr.release();
+  s->pf.release();
+  s->brdf.release();
+  delete s;
+}
 
 /* Bounding sphere of the positions the vertex stage reads (read_attrib
  * rules: missing components are 0), in double, then rounded outwards. */
@@ -142,6 +140,8 @@ extern "C" int mopcuda_scene_add_draw(MopCudaScene *s, const MopCudaDraw *c) {
   if (!s || !c)
     return fail(MOPCUDA_EINVAL, "scene_add_draw: bad arguments");
   std::lock_guard<std::mutex> lk(s->mu);
+  if (s->frozen)
+    return fail(MOPCUDA_EINVAL, "scene_add_draw: the scene is held by a server");
   DrawRec r;
   bool skip = false;
   const float ident[16] = {1, 0, 0, 0, 0, 1, 0, 0, 0, 0, 1, 0, 0, 0, 0, 1};
@@ -151,7 +151,7 @@ extern "C" int mopcuda_scene_add_draw(MopCudaScene *s, const MopCudaDraw *c) {
     s->lights.resize(nl);
     return rc;
   }
-  if (skip) { /* zero-opacity: drawn as nothing, keep an empty slot */
+  if (skip) { /* zero opacity: a colour no-op, kept as an empty slot */
     memset(&r, 0, sizeof r);
     memcpy(r.model, c->model, sizeof r.model);
   }
@@ -181,74 +181,244 @@ extern "C" uint32_t mopcuda_scene_draw_count(const MopCudaScene *s) {
 
 extern "C" uint64_t mopcuda_scene_triangle_count(const MopCudaScene *s) { return s ? s->tris : 0; }
 
+int mc_scene_sync(MopCudaScene *s) {
+  std::lock_guard<std::mutex> lk(s->mu);
+  if (s->dev_version == s->version)
+    return MOPCUDA_OK;
+  const size_t nd = s->draws.size();
+  if (s->d_bounds.ensure(sizeof(DrawBound) * (nd ? nd : 1)) ||
+      s->d_lights.ensure(sizeof(LightRec) * (s->lights.size() + 1)))
+    return MOPCUDA_ENOMEM;
+  if (nd)
+    CU_TRY(cudaMemcpy(s->d_bounds.p, s->bounds.data(), sizeof(DrawBound) * nd,
+                      cudaMemcpyHostToDevice));
+  if (!s->lights.empty())
+    CU_TRY(cudaMemcpy(s->d_lights.p, s->lights.data(), sizeof(LightRec) * s->lights.size(),
+                      cudaMemcpyHostToDevice));
+  s->dev_version = s->version;
+  return MOPCUDA_OK;
+}
+
+void mc_scene_snapshot(MopCudaScene *s, DrawRec *dst) {
+  std::lock_guard<std::mutex> lk(s->mu);
+  const uint32_t nd = (uint32_t)s->draws.size();
+  if (nd)
+    memcpy(dst, s->draws.data(), sizeof(DrawRec) * nd);
+  mc_ibl_consts(s->ibl_on, s->pf_w, s->pf_h, s->pf_levels, s->brdf_size, dst, nd);
+}
+
+static void pool_need(uint64_t T, uint64_t V, uint32_t fan_num, uint32_t large_num,
+                      unsigned long long need[4]) {
+  const unsigned long long fan = T * fan_num / 8ull + 1024ull;
+  need[0] = V + fan;
+  need[1] = T + fan;
+  need[2] = fan;
+  need[3] = T * large_num / 16ull + 1024ull;
+}
+
+uint64_t mc_view_bytes(const MopCudaScene *s, uint64_t samples, uint64_t pixels) {
+  unsigned long long need[4];
+  pool_need(s->tris, s->verts, 1, 1, need);
+  const uint64_t pools = 64ull * need[0] + (sizeof(RasterRec) + sizeof(ShadeRec)) * need[1] +
+                         4ull * need[2] + 8ull * need[3];
+  return 28ull * samples + 4ull * pixels + pools / 2 + sizeof(DrawRec) * s->draws.size();
+}
+
 /* ------------------------------------------------------------------------
- * batch
+ * launch core
  * ------------------------------------------------------------------------ */
-static int check_view(const MopCudaView &v) {
+int mc_check_view(const MopCudaView &v) {
   if (v.width <= 0 || v.height <= 0 || v.ssaa < 1 || v.ssaa > 4)
-    return fail(MOPCUDA_EINVAL, "batch view: bad size or ssaa");
+    return fail(MOPCUDA_EINVAL, "view: bad size or ssaa");
   if ((uint64_t)v.width * v.ssaa > 32767u || (uint64_t)v.height * v.ssaa > 32767u)
-    return fail(MOPCUDA_EINVAL, "batch view: %dx%d x%d exceeds 32767 samples per side", v.width,
+    return fail(MOPCUDA_EINVAL, "view: %dx%d x%d exceeds 32767 samples per side", v.width,
                 v.height, v.ssaa);
   return MOPCUDA_OK;
 }
 
-static void set_view(ViewRec &r, const MopCudaView &v) {
+static void set_camera(ViewRec &r, const MopCudaView &v) {
   memcpy(r.view, v.view, sizeof r.view);
   memcpy(r.proj, v.proj, sizeof r.proj);
   memcpy(r.eye, v.eye, sizeof r.eye);
   memcpy(r.clear, v.clear, sizeof r.clear);
 }
 
-static void drop_graph(MopCudaBatch *b) {
-  if (b->exec)
-    cudaGraphExecDestroy(b->exec);
-  if (b->graph)
-    cudaGraphDestroy(b->graph);
-  b->exec = nullptr;
-  b->graph = nullptr;
+int LaunchCore::init(MopCudaDevice *d) {
+  dev = d;
+  if (cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreate(&ev0) != cudaSuccess || cudaEventCreate(&ev1) != cudaSuccess) {
+    cudaGetLastError();
+    return fail(MOPCUDA_ECUDA, "launch: stream/event creation failed");
+  }
+  exposure = d->exposure;
+  post_effects = d->post;
+  memcpy(lut, d->lut, sizeof lut);
+  return MOPCUDA_OK;
 }
 
-static int batch_sync(MopCudaBatch *b, int timeout_ms) {
+int LaunchCore::sync(int timeout_ms) {
   cudaEvent_t e;
   CU_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
-  cudaEventRecord(e, b->stream);
-  int rc = mc_bounded_sync(b->dev, e, timeout_ms);
+  cudaEventRecord(e, stream);
+  int rc = mc_bounded_sync(dev, e, timeout_ms);
   cudaEventDestroy(e);
   return rc;
 }
 
-extern "C" void mopcuda_batch_destroy(MopCudaBatch *b) {
-  if (!b)
-    return;
-  cudaSetDevice(b->dev->ordinal);
-  if (b->stream)
-    batch_sync(b, 10000);
-  drop_graph(b);
-  DevArena *arenas[] = {&b->d_views, &b->d_frames, &b->d_view_draws, &b->d_ctr, &b->d_status,
-                        &b->d_posts, &b->d_post_views, &b->d_draws, &b->d_lights, &b->d_bounds,
-                        &b->clip, &b->world, &b->normal, &b->color, &b->rrec, &b->srec,
-                        &b->clipq, &b->large_list, &b->large_items, &b->keys, &b->shade_list,
-                        &b->pre, &b->out, &b->depth, &b->ids, &b->presented, &b->pick_xy,
-                        &b->pick_out, &b->irr, &b->pf, &b->brdf};
+void LaunchCore::release() {
+  if (stream)
+    sync(10000);
+  DevArena *arenas[] = {&d_views, &d_frames, &d_view_draws, &d_ctr, &d_status, &d_posts,
+                        &d_post_views, &d_draws, &d_scenes, &clip, &world, &normal, &color,
+                        &rrec, &srec, &clipq, &large_list, &large_items, &keys, &shade_list,
+                        &pre, &out, &depth, &ids, &presented};
   for (DevArena *a : arenas)
     a->release();
-  b->h_views.release();
-  b->h_draws.release();
-  b->h_status.release();
-  b->h_pick.release();
-  if (b->ev0)
-    cudaEventDestroy(b->ev0);
-  if (b->ev1)
-    cudaEventDestroy(b->ev1);
-  if (b->stream)
-    cudaStreamDestroy(b->stream);
-  delete b;
+  h_views.release();
+  h_draws.release();
+  h_scenes.release();
+  h_status.release();
+  if (ev0)
+    cudaEventDestroy(ev0);
+  if (ev1)
+    cudaEventDestroy(ev1);
+  if (stream)
+    cudaStreamDestroy(stream);
+  ev0 = ev1 = nullptr;
+  stream = nullptr;
 }
 
-/* Pools for the worst case scaled by `frac` (every draw visible in every
- * viewport is frac = 1). */
-static int size_pools(MopCudaBatch *b, unsigned long long vneed, unsigned long long rneed,
+void LaunchCore::trim() {
+  if (stream)
+    sync(10000);
+  DevArena *arenas[] = {&clip, &world, &normal, &color, &rrec, &srec, &clipq, &large_list,
+                        &large_items, &keys, &shade_list, &pre, &out, &depth, &ids, &presented};
+  for (DevArena *a : arenas)
+    a->release();
+  vertex_pool = rec_pool = clip_pool = large_pool = 0;
+}
+
+uint64_t LaunchCore::device_bytes() const {
+  const DevArena *arenas[] = {&d_views, &d_frames, &d_view_draws, &d_ctr, &d_status, &d_posts,
+                              &d_post_views, &d_draws, &d_scenes, &clip, &world, &normal, &color,
+                              &rrec, &srec, &clipq, &large_list, &large_items, &keys,
+                              &shade_list, &pre, &out, &depth, &ids, &presented};
+  uint64_t t = 0;
+  for (const DevArena *a : arenas)
+    t += a->cap;
+  return t;
+}
+
+int LaunchCore::set_layout(const MopCudaView *views, const uint32_t *scene_of,
+                           const uint8_t *no_color, uint32_t n,
+                           const std::vector<MopCudaScene *> &sc) {
+  if (n == 0 || n > MOPCUDA_MAX_VIEWS)
+    return fail(MOPCUDA_EINVAL, "launch: 1..%d views", MOPCUDA_MAX_VIEWS);
+  for (uint32_t i = 0; i < n; i++) {
+    int rc = mc_check_view(views[i]);
+    if (rc)
+      return rc;
+    if (scene_of[i] >= sc.size())
+      return fail(MOPCUDA_EINVAL, "launch: view %u names scene %u of %zu", i, scene_of[i],
+                  sc.size());
+  }
+  nv = n;
+  scenes = sc;
+  scene_draw_off.assign(sc.size(), 0);
+  total_draws = 0;
+  for (size_t k = 0; k < sc.size(); k++) {
+    scene_draw_off[k] = total_draws;
+    total_draws += sc[k]->draws.size();
+  }
+  vrec.assign(n, ViewRec());
+  posts.assign(n, PostArgs());
+  unsigned long long so = 0, po = 0, dro = 0;
+  for (uint32_t i = 0; i < n; i++) {
+    const MopCudaView &v = views[i];
+    ViewRec &r = vrec[i];
+    memset(&r, 0, sizeof r);
+    set_camera(r, v);
+    r.ssaa = v.ssaa;
+    r.width = v.width * v.ssaa;
+    r.height = v.height * v.ssaa;
+    r.scene = scene_of[i];
+    r.no_color = no_color && no_color[i] ? 1u : 0u;
+    r.sample_off = so;
+    r.pixel_off = po;
+    r.draw_off = dro;
+    /* 16-sample alignment keeps the resolve's vector stores aligned */
+    so += ((unsigned long long)r.width * r.height + 15ull) & ~15ull;
+    po += ((unsigned long long)v.width * v.height + 15ull) & ~15ull;
+    dro += sc[scene_of[i]]->draws.size();
+  }
+  total_samples = so;
+  total_pixels = po;
+  view_draw_total = dro;
+  int rc = 0;
+  rc |= keys.ensure(8ull * so);
+  rc |= shade_list.ensure(4ull * so);
+  rc |= pre.ensure(4ull * so);
+  rc |= out.ensure(4ull * so);
+  rc |= depth.ensure(4ull * so);
+  rc |= ids.ensure(4ull * so);
+  rc |= presented.ensure(4ull * po + 16);
+  rc |= d_views.ensure(sizeof(ViewRec) * n);
+  rc |= h_views.ensure(sizeof(ViewRec) * n);
+  rc |= d_frames.ensure(sizeof(FrameArgs) * n);
+  rc |= d_ctr.ensure(sizeof(Counters) * n);
+  rc |= d_status.ensure(sizeof(BatchStatus));
+  rc |= h_status.ensure(sizeof(BatchStatus) + sizeof(Counters) * n);
+  rc |= d_posts.ensure(sizeof(PostArgs) * n);
+  rc |= d_post_views.ensure(4ull * 4ull * n);
+  rc |= d_view_draws.ensure(sizeof(DrawRec) * (dro ? dro : 1));
+  rc |= d_draws.ensure(sizeof(DrawRec) * (total_draws ? total_draws : 1));
+  rc |= h_draws.ensure(sizeof(DrawRec) * (total_draws ? total_draws : 1));
+  rc |= d_scenes.ensure(sizeof(SceneDesc) * sc.size());
+  rc |= h_scenes.ensure(sizeof(SceneDesc) * sc.size());
+  if (rc)
+    return MOPCUDA_ENOMEM;
+  PostArgs post;
+  memset(&post, 0, sizeof post);
+  post.effects = post_effects & (MOPCUDA_POST_GAMMA | MOPCUDA_POST_TONEMAP |
+                                 MOPCUDA_POST_VIGNETTE | MOPCUDA_POST_FXAA);
+  memcpy(post.lut, lut, sizeof post.lut);
+  for (int i = 0; i < 256; i++) {
+    float v = lut[i];
+    if (v > 1.0f)
+      v = 1.0f;
+    if (v < 0.0f)
+      v = 0.0f;
+    volatile float q = v * 255.0f + 0.5f; /* postprocess.c:110-112 */
+    post.lut8[i] = (uint8_t)(int)q;
+  }
+  std::vector<uint32_t> lists(4ull * n, 0u);
+  for (int k = 0; k < 4; k++)
+    post_count[k] = post_tiles[k] = 0;
+  for (uint32_t i = 0; i < n; i++) {
+    const ViewRec &r = vrec[i];
+    PostArgs p = post;
+    p.pre = pre.as<uchar4>() + r.sample_off;
+    p.out = out.as<uchar4>() + r.sample_off;
+    p.presented = r.ssaa > 1 ? presented.as<uchar4>() + r.pixel_off : nullptr;
+    p.width = r.width;
+    p.height = r.height;
+    p.ssaa = r.ssaa;
+    posts[i] = p;
+    if (r.no_color)
+      continue; /* visibility only: no post effects */
+    const int k = r.ssaa - 1;
+    lists[(size_t)k * n + post_count[k]++] = i;
+    const uint32_t pw = (uint32_t)(r.width / r.ssaa), ph = (uint32_t)(r.height / r.ssaa);
+    post_tiles[k] += ((pw + 31u) / 32u) * ((ph + 7u) / 8u);
+  }
+  CU_TRY(cudaMemcpyAsync(d_posts.p, posts.data(), sizeof(PostArgs) * n, cudaMemcpyHostToDevice,
+                         stream));
+  CU_TRY(cudaMemcpyAsync(d_post_views.p, lists.data(), 4ull * 4ull * n, cudaMemcpyHostToDevice,
+                         stream));
+  return sync(FRAME_TIMEOUT_MS); /* pageable sources: finish before they go */
+}
+
+static int size_pools(LaunchCore *b, unsigned long long vneed, unsigned long long rneed,
                       unsigned long long cneed, unsigned long long lneed) {
   int rc = 0;
   rc |= b->clip.ensure(16ull * vneed);
@@ -271,127 +441,196 @@ static int size_pools(MopCudaBatch *b, unsigned long long vneed, unsigned long l
   return MOPCUDA_OK;
 }
 
-/* Uploads the scene when it changed and refreshes the pinned draw table. */
-static int stage_scene(MopCudaBatch *b) {
-  MopCudaScene *s = b->scene;
-  std::lock_guard<std::mutex> lk(s->mu);
-  const uint32_t nd = (uint32_t)s->draws.size();
-  if (s->version != b->scene_version) {
-    int rc = 0;
-    rc |= b->d_draws.ensure(sizeof(DrawRec) * (nd ? nd : 1));
-    rc |= b->h_draws.ensure(sizeof(DrawRec) * (nd ? nd : 1));
-    rc |= b->d_view_draws.ensure(sizeof(DrawRec) * (size_t)(nd ? nd : 1) * b->nv);
-    rc |= b->d_lights.ensure(sizeof(LightRec) * (s->lights.size() + 1));
-    rc |= b->d_bounds.ensure(sizeof(DrawBound) * (nd ? nd : 1));
+int LaunchCore::stage() {
+  SceneDesc *sd = h_scenes.as<SceneDesc>();
+  DrawRec *hd = h_draws.as<DrawRec>();
+  for (size_t k = 0; k < scenes.size(); k++) {
+    MopCudaScene *s = scenes[k];
+    int rc = mc_scene_sync(s);
     if (rc)
-      return MOPCUDA_ENOMEM;
-    if (!s->lights.empty())
-      CU_TRY(cudaMemcpy(b->d_lights.p, s->lights.data(), sizeof(LightRec) * s->lights.size(),
-                        cudaMemcpyHostToDevice));
-    if (nd)
-      CU_TRY(cudaMemcpy(b->d_bounds.p, s->bounds.data(), sizeof(DrawBound) * nd,
-                        cudaMemcpyHostToDevice));
-    b->tmpl.lights = b->d_lights.as<LightRec>();
-    b->tmpl.light_total = (uint32_t)s->lights.size();
-    b->nd = nd;
-    b->scene_version = s->version;
-    /* first pools: half the worst case (all draws visible everywhere) */
-    const unsigned long long T = s->tris, V = s->verts, fan = T * b->fan_num / 8ull + 1024ull;
-    const unsigned long long half = (b->nv + 1ull) / 2ull;
-    int prc = size_pools(b, half * (V + fan), half * (T + fan), half * fan,
-                         half * (T * b->large_num / 16ull + 1024ull));
-    if (prc)
-      return prc;
-    drop_graph(b);
+      return rc;
+    mc_scene_snapshot(s, hd + scene_draw_off[k]);
+    SceneDesc &d = sd[k];
+    memset(&d, 0, sizeof d);
+    d.draws = d_draws.as<DrawRec>() + scene_draw_off[k];
+    d.bounds = s->d_bounds.as<DrawBound>();
+    d.nd = (uint32_t)s->draws.size();
+    d.lights = s->d_lights.as<LightRec>();
+    d.light_total = (uint32_t)s->lights.size();
+    if (s->ibl_on) {
+      d.irr = s->irr.as<float>();
+      d.irr_w = s->irr_w;
+      d.irr_h = s->irr_h;
+      d.pf = s->pf.as<float>();
+      d.pf_w = s->pf_w;
+      d.pf_h = s->pf_h;
+      d.pf_levels = s->pf_levels;
+      d.brdf = s->brdf.as<float>();
+      d.brdf_size = s->brdf_size;
+      d.ibl_rotation = s->ibl_rot;
+      d.ibl_intensity = s->ibl_int;
+    }
   }
-  DrawRec *h = b->h_draws.as<DrawRec>();
-  if (nd)
-    memcpy(h, s->draws.data(), sizeof(DrawRec) * nd);
-  const FrameArgs &t = b->tmpl;
-  mc_ibl_consts(t.pf != nullptr, t.pf_w, t.pf_h, t.pf_levels, t.brdf_size, h, nd);
+  memcpy(h_views.p, vrec.data(), sizeof(ViewRec) * nv);
+  /* first pools: half the worst case (every draw visible in every view) */
+  unsigned long long want[4] = {0, 0, 0, 0};
+  for (uint32_t i = 0; i < nv; i++) {
+    const MopCudaScene *s = scenes[vrec[i].scene];
+    unsigned long long need[4];
+    pool_need(s->tris, s->verts, fan_num, large_num, need);
+    for (int k = 0; k < 4; k++)
+      want[k] += need[k];
+  }
+  for (int k = 0; k < 4; k++)
+    want[k] = want[k] / 2 + 4096;
+  if (vertex_pool < want[0] || rec_pool < want[1] || clip_pool < want[2] ||
+      large_pool < want[3])
+    return size_pools(this, std::max(want[0], vertex_pool), std::max(want[1], rec_pool),
+                      std::max(want[2], clip_pool), std::max(want[3], large_pool));
   return MOPCUDA_OK;
 }
 
-static int build_graph(MopCudaBatch *b) {
-  drop_graph(b);
+int LaunchCore::enqueue() {
   BatchLaunch L;
   memset(&L, 0, sizeof L);
-  L.num_sms = b->dev->num_sms;
-  L.vertex_block = b->cfg.vertex_block;
-  L.setup_block = b->cfg.setup_block;
-  L.raster_block = b->cfg.raster_block;
-  L.large_block = b->cfg.large_block;
-  L.shade_block = b->cfg.shade_block;
-  L.grid_mul = b->cfg.grid_mul;
+  L.num_sms = dev->num_sms;
+  L.vertex_block = cfg.vertex_block;
+  L.setup_block = cfg.setup_block;
+  L.raster_block = cfg.raster_block;
+  L.large_block = cfg.large_block;
+  L.shade_block = cfg.shade_block;
+  L.grid_mul = cfg.grid_mul;
   mopcuda_batch_grids(L);
-  b->tmpl.small_side = b->cfg.small_side;
-  b->tmpl.small_area = b->cfg.small_area;
 
   BatchArgs a;
   memset(&a, 0, sizeof a);
-  a.scene = b->d_draws.as<DrawRec>();
-  a.bounds = b->d_bounds.as<DrawBound>();
-  a.nd = b->nd;
-  a.views = b->d_views.as<ViewRec>();
-  a.nv = b->nv;
-  a.frames = b->d_frames.as<FrameArgs>();
-  a.view_draws = b->d_view_draws.as<DrawRec>();
-  a.ctr = b->d_ctr.as<Counters>();
-  a.status = b->d_status.as<BatchStatus>();
-  a.tmpl = b->tmpl;
-  a.clip = b->clip.as<float4>();
-  a.world = b->world.as<float4>();
-  a.normal = b->normal.as<float4>();
-  a.color = b->color.as<float4>();
-  a.vertex_pool = b->vertex_pool;
-  a.rrec = b->rrec.as<RasterRec>();
-  a.srec = b->srec.as<ShadeRec>();
-  a.rec_pool = b->rec_pool;
-  a.clipq = b->clipq.as<uint32_t>();
-  a.clip_pool = b->clip_pool;
-  a.large_list = b->large_list.as<uint32_t>();
-  a.large_items = b->large_items.as<uint32_t>();
-  a.large_pool = b->large_pool;
-  a.keys = b->keys.as<unsigned long long>();
-  a.shade_list = b->shade_list.as<uint32_t>();
-  a.pre = b->pre.as<uchar4>();
-  a.depth = b->depth.as<float>();
-  a.ids = b->ids.as<uint32_t>();
-  a.fan_num = b->fan_num;
-  a.large_num = b->large_num;
+  a.scenes = d_scenes.as<SceneDesc>();
+  a.views = d_views.as<ViewRec>();
+  a.nv = nv;
+  a.frames = d_frames.as<FrameArgs>();
+  a.view_draws = d_view_draws.as<DrawRec>();
+  a.ctr = d_ctr.as<Counters>();
+  a.status = d_status.as<BatchStatus>();
+  a.tmpl.exposure = exposure;
+  a.tmpl.small_side = cfg.small_side;
+  a.tmpl.small_area = cfg.small_area;
+  a.clip = clip.as<float4>();
+  a.world = world.as<float4>();
+  a.normal = normal.as<float4>();
+  a.color = color.as<float4>();
+  a.vertex_pool = vertex_pool;
+  a.rrec = rrec.as<RasterRec>();
+  a.srec = srec.as<ShadeRec>();
+  a.rec_pool = rec_pool;
+  a.clipq = clipq.as<uint32_t>();
+  a.clip_pool = clip_pool;
+  a.large_list = large_list.as<uint32_t>();
+  a.large_items = large_items.as<uint32_t>();
+  a.large_pool = large_pool;
+  a.keys = keys.as<unsigned long long>();
+  a.shade_list = shade_list.as<uint32_t>();
+  a.pre = pre.as<uchar4>();
+  a.depth = depth.as<float>();
+  a.ids = ids.as<uint32_t>();
+  a.fan_num = fan_num;
+  a.large_num = large_num;
 
   const uint32_t *pv[4];
   for (int k = 0; k < 4; k++)
-    pv[k] = b->d_post_views.as<uint32_t>() + (size_t)k * b->nv;
-
-  cudaStream_t s = b->stream;
-  CU_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
-  cudaMemcpyAsync(b->d_views.p, b->h_views.p, sizeof(ViewRec) * b->nv, cudaMemcpyHostToDevice, s);
-  if (b->nd)
-    cudaMemcpyAsync(b->d_draws.p, b->h_draws.p, sizeof(DrawRec) * b->nd, cudaMemcpyHostToDevice,
-                    s);
-  cudaMemsetAsync(b->d_ctr.p, 0, sizeof(Counters) * b->nv, s);
-  cudaMemsetAsync(b->d_status.p, 0, sizeof(BatchStatus), s);
-  cudaMemsetAsync(b->keys.p, 0xff, 8ull * b->total_samples, s);
-  int n = mopcuda_launch_batch(a, b->d_posts.as<PostArgs>(), pv, b->post_count, b->post_tiles, L,
-                               s);
-  cudaMemcpyAsync(b->h_status.p, b->d_status.p, sizeof(BatchStatus), cudaMemcpyDeviceToHost, s);
-  cudaMemcpyAsync(b->h_status.as<uint8_t>() + sizeof(BatchStatus), b->d_ctr.p,
-                  sizeof(Counters) * b->nv, cudaMemcpyDeviceToHost, s);
-  cudaError_t e = cudaStreamEndCapture(s, &b->graph);
-  if (e != cudaSuccess) {
-    cudaGetLastError();
-    b->graph = nullptr;
-    return fail(MOPCUDA_ECUDA, "batch graph capture: %s", cudaGetErrorString(e));
-  }
-  e = cudaGraphInstantiate(&b->exec, b->graph, 0);
-  if (e != cudaSuccess) {
-    cudaGetLastError();
-    drop_graph(b);
-    return fail(MOPCUDA_ECUDA, "batch graph instantiate: %s", cudaGetErrorString(e));
-  }
-  b->launches = (uint64_t)n;
+    pv[k] = d_post_views.as<uint32_t>() + (size_t)k * nv;
+  cudaStream_t s = stream;
+  CU_TRY(cudaMemcpyAsync(d_views.p, h_views.p, sizeof(ViewRec) * nv, cudaMemcpyHostToDevice, s));
+  if (total_draws)
+    CU_TRY(cudaMemcpyAsync(d_draws.p, h_draws.p, sizeof(DrawRec) * total_draws,
+                           cudaMemcpyHostToDevice, s));
+  CU_TRY(cudaMemcpyAsync(d_scenes.p, h_scenes.p, sizeof(SceneDesc) * scenes.size(),
+                         cudaMemcpyHostToDevice, s));
+  CU_TRY(cudaMemsetAsync(d_ctr.p, 0, sizeof(Counters) * nv, s));
+  CU_TRY(cudaMemsetAsync(d_status.p, 0, sizeof(BatchStatus), s));
+  CU_TRY(cudaMemsetAsync(keys.p, 0xff, 8ull * total_samples, s));
+  launches = (uint64_t)mopcuda_launch_batch(a, d_posts.as<PostArgs>(), pv, post_count, post_tiles,
+                                            L, scenes.size() == 1, s);
+  CU_TRY(cudaGetLastError());
+  CU_TRY(cudaMemcpyAsync(h_status.p, d_status.p, sizeof(BatchStatus), cudaMemcpyDeviceToHost, s));
+  CU_TRY(cudaMemcpyAsync(h_status.as<uint8_t>() + sizeof(BatchStatus), d_ctr.p,
+                         sizeof(Counters) * nv, cudaMemcpyDeviceToHost, s));
   return MOPCUDA_OK;
+}
+
+int LaunchCore::after(bool *rerun, int attempt) {
+  *rerun = false;
+  const BatchStatus *st = h_status.as<BatchStatus>();
+  const Counters *ctr = (const Counters *)(h_status.as<uint8_t>() + sizeof(BatchStatus));
+  uint32_t view_over = 0;
+  for (uint32_t i = 0; i < nv; i++)
+    view_over |= ctr[i].overflow;
+  if (!st->overflow && !view_over)
+    return MOPCUDA_OK;
+  if (attempt >= 8)
+    return fail(MOPCUDA_ENOMEM, "launch pools overflowed repeatedly (flags %u/%u)", st->overflow,
+                view_over);
+  if (view_over & 7u) { /* a viewport's clipped fans: records, vertices, clip queue */
+    if (fan_num >= 256u)
+      return fail(MOPCUDA_ENOMEM, "launch: clipped-fan reserve exhausted");
+    fan_num *= 2u;
+  }
+  if (view_over & 8u) {
+    if (large_num >= 512u)
+      return fail(MOPCUDA_ENOMEM, "launch: large-record list exhausted");
+    large_num *= 2u;
+  }
+  if (st->overflow) {
+    const unsigned long long need[4] = {st->need_vertex, st->need_rec, st->need_clip,
+                                        st->need_large};
+    unsigned long long cap[4] = {vertex_pool, rec_pool, clip_pool, large_pool};
+    for (int k = 0; k < 4; k++)
+      if (need[k] > cap[k])
+        cap[k] = need[k] + need[k] / 4 + 4096ull;
+    int rc = size_pools(this, cap[0], cap[1], cap[2], cap[3]);
+    if (rc)
+      return rc;
+  }
+  *rerun = true;
+  return MOPCUDA_OK;
+}
+
+/* ------------------------------------------------------------------------
+ * batch: one LaunchCore over one scene, captured as a CUDA graph
+ * ------------------------------------------------------------------------ */
+struct MopCudaBatch {
+  MopCudaScene *scene = nullptr;
+  LaunchCore core;
+  uint64_t scene_version = ~0ull;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  bool pending = false;
+  float last_ms = 0.0f;
+  DevArena pick_xy, pick_out;
+  HostArena h_pick;
+  std::mutex mu;
+};
+
+static void drop_graph(MopCudaBatch *b) {
+  if (b->exec)
+    cudaGraphExecDestroy(b->exec);
+  if (b->graph)
+    cudaGraphDestroy(b->graph);
+  b->exec = nullptr;
+  b->graph = nullptr;
+}
+
+extern "C" void mopcuda_batch_destroy(MopCudaBatch *b) {
+  if (!b)
+    return;
+  cudaSetDevice(b->core.dev->ordinal);
+  if (b->core.stream)
+    b->core.sync(10000);
+  drop_graph(b);
+  b->pick_xy.release();
+  b->pick_out.release();
+  b->h_pick.release();
+  b->core.release();
+  delete b;
 }
 
 extern "C" MopCudaBatch *mopcuda_batch_create(MopCudaScene *scene, const MopCudaView *views,
@@ -400,164 +639,129 @@ extern "C" MopCudaBatch *mopcuda_batch_create(MopCudaScene *scene, const MopCuda
     fail(MOPCUDA_EINVAL, "batch_create: need a scene and 1..%d views", MOPCUDA_MAX_VIEWS);
     return nullptr;
   }
-  for (uint32_t i = 0; i < n; i++)
-    if (check_view(views[i]))
-      return nullptr;
   MopCudaDevice *d = scene->dev;
   cudaSetDevice(d->ordinal);
   MopCudaBatch *b = new MopCudaBatch();
   b->scene = scene;
-  b->dev = d;
-  b->nv = n;
-  if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess ||
-      cudaEventCreate(&b->ev0) != cudaSuccess || cudaEventCreate(&b->ev1) != cudaSuccess) {
-    cudaGetLastError();
-    fail(MOPCUDA_ECUDA, "batch_create: stream/event creation failed");
+  if (b->core.init(d)) {
     mopcuda_batch_destroy(b);
     return nullptr;
   }
-  b->vrec.resize(n);
-  b->posts.resize(n);
-  unsigned long long so = 0, po = 0;
-  PostArgs post;
-  mc_post_args(d, post);
-  for (uint32_t i = 0; i < n; i++) {
-    const MopCudaView &v = views[i];
-    ViewRec &r = b->vrec[i];
-    memset(&r, 0, sizeof r);
-    set_view(r, v);
-    r.ssaa = v.ssaa;
-    r.width = v.width * v.ssaa;
-    r.height = v.height * v.ssaa;
-    r.sample_off = so;
-    r.pixel_off = po;
-    /* 16-sample alignment keeps the resolve's vector stores aligned */
-    so += ((unsigned long long)r.width * r.height + 15ull) & ~15ull;
-    po += ((unsigned long long)v.width * v.height + 15ull) & ~15ull;
-  }
-  b->total_samples = so;
-  b->total_pixels = po;
-  int rc = 0;
-  rc |= b->keys.ensure(8ull * so);
-  rc |= b->shade_list.ensure(4ull * so);
-  rc |= b->pre.ensure(4ull * so);
-  rc |= b->out.ensure(4ull * so);
-  rc |= b->depth.ensure(4ull * so);
-  rc |= b->ids.ensure(4ull * so);
-  rc |= b->presented.ensure(4ull * po + 16);
-  rc |= b->d_views.ensure(sizeof(ViewRec) * n);
-  rc |= b->h_views.ensure(sizeof(ViewRec) * n);
-  rc |= b->d_frames.ensure(sizeof(FrameArgs) * n);
-  rc |= b->d_ctr.ensure(sizeof(Counters) * n);
-  rc |= b->d_status.ensure(sizeof(BatchStatus));
-  rc |= b->h_status.ensure(sizeof(BatchStatus) + sizeof(Counters) * n);
-  rc |= b->d_posts.ensure(sizeof(PostArgs) * n);
-  rc |= b->d_post_views.ensure(4ull * 4ull * n);
-  if (rc) {
+  std::vector<uint32_t> scene_of(n, 0u);
+  std::vector<MopCudaScene *> sc = {scene};
+  if (b->core.set_layout(views, scene_of.data(), nullptr, n, sc)) {
     mopcuda_batch_destroy(b);
     return nullptr;
   }
-  for (uint32_t i = 0; i < n; i++) {
-    const ViewRec &r = b->vrec[i];
-    PostArgs p = post;
-    p.pre = b->pre.as<uchar4>() + r.sample_off;
-    p.out = b->out.as<uchar4>() + r.sample_off;
-    p.presented = r.ssaa > 1 ? b->presented.as<uchar4>() + r.pixel_off : nullptr;
-    p.width = r.width;
-    p.height = r.height;
-    p.ssaa = r.ssaa;
-    b->posts[i] = p;
-    const int k = r.ssaa - 1;
-    b->post_list[k].push_back(i);
-    const uint32_t pw = (uint32_t)(r.width / r.ssaa), ph = (uint32_t)(r.height / r.ssaa);
-    b->post_tiles[k] += ((pw + 31u) / 32u) * ((ph + 7u) / 8u);
-  }
-  std::vector<uint32_t> lists(4ull * n, 0u);
-  for (int k = 0; k < 4; k++) {
-    b->post_count[k] = (uint32_t)b->post_list[k].size();
-    std::copy(b->post_list[k].begin(), b->post_list[k].end(), lists.begin() + (size_t)k * n);
-  }
-  if (cudaMemcpy(b->d_posts.p, b->posts.data(), sizeof(PostArgs) * n, cudaMemcpyHostToDevice) !=
-          cudaSuccess ||
-      cudaMemcpy(b->d_post_views.p, lists.data(), 4ull * 4ull * n, cudaMemcpyHostToDevice) !=
-          cudaSuccess) {
-    cudaGetLastError();
-    fail(MOPCUDA_ECUDA, "batch_create: upload failed");
-    mopcuda_batch_destroy(b);
-    return nullptr;
-  }
-  /* frame state shared by every viewport */
-  FrameArgs &t = b->tmpl;
-  memset(&t, 0, sizeof t);
-  t.exposure = d->exposure;
-  if (d->ibl_on) {
-    /* own copies: later set_ibl calls on the device must not move them */
-    size_t pf_px = 0;
-    for (int l = 0; l < d->pf_levels; l++) {
-      int lw = d->pf_w >> l, lh = d->pf_h >> l;
-      pf_px += (size_t)(lw < 1 ? 1 : lw) * (size_t)(lh < 1 ? 1 : lh);
-    }
-    const size_t ib = (size_t)d->irr_w * d->irr_h * 16, pb = pf_px * 16,
-                 bb = (size_t)d->brdf_size * d->brdf_size * 16;
-    if (b->irr.ensure(ib) || b->pf.ensure(pb) || b->brdf.ensure(bb) ||
-        cudaMemcpy(b->irr.p, d->irr.p, ib, cudaMemcpyDeviceToDevice) != cudaSuccess ||
-        cudaMemcpy(b->pf.p, d->pf.p, pb, cudaMemcpyDeviceToDevice) != cudaSuccess ||
-        cudaMemcpy(b->brdf.p, d->brdf.p, bb, cudaMemcpyDeviceToDevice) != cudaSuccess) {
-      cudaGetLastError();
-      fail(MOPCUDA_ENOMEM, "batch_create: IBL copy failed");
-      mopcuda_batch_destroy(b);
-      return nullptr;
-    }
-    t.irr = b->irr.as<float>();
-    t.irr_w = d->irr_w;
-    t.irr_h = d->irr_h;
-    t.pf = b->pf.as<float>();
-    t.pf_w = d->pf_w;
-    t.pf_h = d->pf_h;
-    t.pf_levels = d->pf_levels;
-    t.brdf = b->brdf.as<float>();
-    t.brdf_size = d->brdf_size;
-    t.ibl_rotation = d->ibl_rot;
-    t.ibl_intensity = d->ibl_int;
-  }
+  b->scene_version = scene->version;
   return b;
 }
 
 extern "C" int mopcuda_batch_set_views(MopCudaBatch *b, const MopCudaView *views, uint32_t n) {
-  if (!b || !views || n != b->nv)
-    return fail(MOPCUDA_EINVAL, "batch_set_views: need %u views", b ? b->nv : 0u);
+  if (!b || !views || n != b->core.nv)
+    return fail(MOPCUDA_EINVAL, "batch_set_views: need %u views", b ? b->core.nv : 0u);
   std::lock_guard<std::mutex> lk(b->mu);
   for (uint32_t i = 0; i < n; i++) {
-    const ViewRec &r = b->vrec[i];
+    const ViewRec &r = b->core.vrec[i];
     if (views[i].ssaa != r.ssaa || views[i].width * views[i].ssaa != r.width ||
         views[i].height * views[i].ssaa != r.height)
       return fail(MOPCUDA_EINVAL, "batch_set_views: view %u changed size or ssaa", i);
   }
   for (uint32_t i = 0; i < n; i++)
-    set_view(b->vrec[i], views[i]);
+    set_camera(b->core.vrec[i], views[i]);
+  return MOPCUDA_OK;
+}
+
+static int build_graph(MopCudaBatch *b) {
+  drop_graph(b);
+  LaunchCore &c = b->core;
+  CU_TRY(cudaStreamBeginCapture(c.stream, cudaStreamCaptureModeThreadLocal));
+  int rc = c.enqueue();
+  cudaError_t e = cudaStreamEndCapture(c.stream, &b->graph);
+  if (rc || e != cudaSuccess) {
+    cudaGetLastError();
+    if (b->graph)
+      cudaGraphDestroy(b->graph);
+    b->graph = nullptr;
+    return rc ? rc : fail(MOPCUDA_ECUDA, "batch graph capture: %s", cudaGetErrorString(e));
+  }
+  e = cudaGraphInstantiate(&b->exec, b->graph, 0);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    drop_graph(b);
+    return fail(MOPCUDA_ECUDA, "batch graph instantiate: %s", cudaGetErrorString(e));
+  }
   return MOPCUDA_OK;
 }
 
 static int launch_graph(MopCudaBatch *b) {
-  cudaStream_t s = b->stream;
-  CU_TRY(cudaEventRecord(b->ev0, s));
+  cudaStream_t s = b->core.stream;
+  CU_TRY(cudaEventRecord(b->core.ev0, s));
   CU_TRY(cudaGraphLaunch(b->exec, s));
-  CU_TRY(cudaEventRecord(b->ev1, s));
+  CU_TRY(cudaEventRecord(b->core.ev1, s));
   b->pending = true;
   return MOPCUDA_OK;
 }
 
-static int finish_batch(MopCudaBatch *b, int timeout_ms);
+/* Waits; re-runs after growing a viewport's reserves or the pools. */
+static int finish_batch(MopCudaBatch *b, int timeout_ms) {
+  for (int attempt = 0; b->pending; attempt++) {
+    int rc = mc_bounded_sync(b->core.dev, b->core.ev1, timeout_ms);
+    b->pending = false;
+    if (rc)
+      return rc;
+    cudaEventElapsedTime(&b->last_ms, b->core.ev0, b->core.ev1);
+    bool rerun = false;
+    rc = b->core.after(&rerun, attempt);
+    if (rc)
+      return rc;
+    if (!rerun)
+      break;
+    rc = build_graph(b);
+    if (rc)
+      return rc;
+    rc = launch_graph(b);
+    if (rc)
+      return rc;
+  }
+  return MOPCUDA_OK;
+}
 
 static int submit_locked(MopCudaBatch *b) {
-  cudaSetDevice(b->dev->ordinal);
+  cudaSetDevice(b->core.dev->ordinal);
   int rc = finish_batch(b, FRAME_TIMEOUT_MS);
   if (rc)
     return rc;
-  rc = stage_scene(b);
+  if (b->scene->version != b->scene_version) { /* draws were added: new table sizes */
+    LaunchCore &c = b->core;
+    std::vector<uint32_t> scene_of(c.nv, 0u);
+    std::vector<MopCudaView> views(c.nv);
+    for (uint32_t i = 0; i < c.nv; i++) {
+      const ViewRec &r = c.vrec[i];
+      MopCudaView &v = views[i];
+      memcpy(v.view, r.view, sizeof v.view);
+      memcpy(v.proj, r.proj, sizeof v.proj);
+      memcpy(v.eye, r.eye, sizeof v.eye);
+      memcpy(v.clear, r.clear, sizeof v.clear);
+      v.width = r.width / r.ssaa;
+      v.height = r.height / r.ssaa;
+      v.ssaa = r.ssaa;
+    }
+    std::vector<MopCudaScene *> sc = {b->scene};
+    rc = c.set_layout(views.data(), scene_of.data(), nullptr, c.nv, sc);
+    if (rc)
+      return rc;
+    b->scene_version = b->scene->version;
+    drop_graph(b);
+  }
+  const unsigned long long pools[4] = {b->core.vertex_pool, b->core.rec_pool, b->core.clip_pool,
+                                       b->core.large_pool};
+  rc = b->core.stage();
   if (rc)
     return rc;
-  memcpy(b->h_views.p, b->vrec.data(), sizeof(ViewRec) * b->nv);
+  if (pools[0] != b->core.vertex_pool || pools[1] != b->core.rec_pool ||
+      pools[2] != b->core.clip_pool || pools[3] != b->core.large_pool)
+    drop_graph(b); /* the pools moved */
   if (!b->exec) {
     rc = build_graph(b);
     if (rc)
@@ -573,62 +777,11 @@ extern "C" int mopcuda_batch_submit(MopCudaBatch *b) {
   return submit_locked(b);
 }
 
-/* Waits; re-runs after growing the per-viewport reserves (a viewport's
- * counters overflowed) or the pools (the allocation pass found them short;
- * the status holds the exact totals). */
-static int finish_batch(MopCudaBatch *b, int timeout_ms) {
-  for (int attempt = 0; b->pending; attempt++) {
-    int rc = mc_bounded_sync(b->dev, b->ev1, timeout_ms);
-    b->pending = false;
-    if (rc)
-      return rc;
-    cudaEventElapsedTime(&b->last_ms, b->ev0, b->ev1);
-    const BatchStatus *st = b->h_status.as<BatchStatus>();
-    const Counters *ctr = (const Counters *)(b->h_status.as<uint8_t>() + sizeof(BatchStatus));
-    uint32_t view_over = 0;
-    for (uint32_t i = 0; i < b->nv; i++)
-      view_over |= ctr[i].overflow;
-    if (!st->overflow && !view_over)
-      break;
-    if (attempt >= 8)
-      return fail(MOPCUDA_ENOMEM, "batch pools overflowed repeatedly (flags %u/%u)",
-                  st->overflow, view_over);
-    if (view_over & 7u) { /* clipped fans: records, extra vertices or clip queue */
-      if (b->fan_num >= 256u)
-        return fail(MOPCUDA_ENOMEM, "batch: clipped-fan reserve exhausted");
-      b->fan_num *= 2u;
-    }
-    if (view_over & 8u) {
-      if (b->large_num >= 512u)
-        return fail(MOPCUDA_ENOMEM, "batch: large-record list exhausted");
-      b->large_num *= 2u;
-    }
-    if (st->overflow) {
-      const unsigned long long need[4] = {st->need_vertex, st->need_rec, st->need_clip,
-                                          st->need_large};
-      unsigned long long cap[4] = {b->vertex_pool, b->rec_pool, b->clip_pool, b->large_pool};
-      for (int k = 0; k < 4; k++)
-        if (need[k] > cap[k])
-          cap[k] = need[k] + need[k] / 4 + 4096ull;
-      rc = size_pools(b, cap[0], cap[1], cap[2], cap[3]);
-      if (rc)
-        return rc;
-    }
-    rc = build_graph(b);
-    if (rc)
-      return rc;
-    rc = launch_graph(b);
-    if (rc)
-      return rc;
-  }
-  return MOPCUDA_OK;
-}
-
 extern "C" int mopcuda_batch_wait(MopCudaBatch *b, int timeout_ms) {
   if (!b)
     return fail(MOPCUDA_EINVAL, "batch_wait: no batch");
   std::lock_guard<std::mutex> lk(b->mu);
-  cudaSetDevice(b->dev->ordinal);
+  cudaSetDevice(b->core.dev->ordinal);
   return finish_batch(b, timeout_ms);
 }
 
@@ -636,34 +789,35 @@ extern "C" float mopcuda_batch_gpu_time_ms(const MopCudaBatch *b) { return b ? b
 
 extern "C" int mopcuda_batch_read(MopCudaBatch *b, uint32_t view, int what, void *dst,
                                   size_t bytes) {
-  if (!b || !dst || view >= b->nv)
+  if (!b || !dst || view >= b->core.nv)
     return fail(MOPCUDA_EINVAL, "batch_read: bad arguments");
   std::lock_guard<std::mutex> lk(b->mu);
-  cudaSetDevice(b->dev->ordinal);
+  cudaSetDevice(b->core.dev->ordinal);
   int rc = finish_batch(b, FRAME_TIMEOUT_MS);
   if (rc)
     return rc;
-  const ViewRec &r = b->vrec[view];
+  const LaunchCore &c = b->core;
+  const ViewRec &r = c.vrec[view];
   const size_t S = (size_t)r.width * r.height;
   const size_t P = (size_t)(r.width / r.ssaa) * (r.height / r.ssaa);
   const void *src = nullptr;
   size_t n = 0;
   switch (what) {
   case MOPCUDA_BATCH_COLOR:
-    src = b->out.as<uchar4>() + r.sample_off;
+    src = c.out.as<uchar4>() + r.sample_off;
     n = 4 * S;
     break;
   case MOPCUDA_BATCH_PRESENTED:
-    src = r.ssaa > 1 ? (const void *)(b->presented.as<uchar4>() + r.pixel_off)
-                     : (const void *)(b->out.as<uchar4>() + r.sample_off);
+    src = r.ssaa > 1 ? (const void *)(c.presented.as<uchar4>() + r.pixel_off)
+                     : (const void *)(c.out.as<uchar4>() + r.sample_off);
     n = 4 * P;
     break;
   case MOPCUDA_BATCH_DEPTH:
-    src = b->depth.as<float>() + r.sample_off;
+    src = c.depth.as<float>() + r.sample_off;
     n = 4 * S;
     break;
   case MOPCUDA_BATCH_IDS:
-    src = b->ids.as<uint32_t>() + r.sample_off;
+    src = c.ids.as<uint32_t>() + r.sample_off;
     n = 4 * S;
     break;
   default:
@@ -671,18 +825,18 @@ extern "C" int mopcuda_batch_read(MopCudaBatch *b, uint32_t view, int what, void
   }
   if (bytes != n)
     return fail(MOPCUDA_EINVAL, "batch_read: buffer is %zu bytes, not %zu", n, bytes);
-  CU_TRY(cudaMemcpyAsync(dst, src, n, cudaMemcpyDeviceToHost, b->stream));
-  return batch_sync(b, FRAME_TIMEOUT_MS);
+  CU_TRY(cudaMemcpyAsync(dst, src, n, cudaMemcpyDeviceToHost, c.stream));
+  return b->core.sync(FRAME_TIMEOUT_MS);
 }
 
 extern "C" int mopcuda_batch_pick(MopCudaBatch *b, uint32_t view, const int32_t *xy, uint32_t n,
                                   uint32_t *ids, float *depths, int32_t *hits) {
-  if (!b || view >= b->nv || (n && (!xy || !ids || !depths || !hits)))
+  if (!b || view >= b->core.nv || (n && (!xy || !ids || !depths || !hits)))
     return fail(MOPCUDA_EINVAL, "batch_pick: bad arguments");
   if (n == 0)
     return MOPCUDA_OK;
   std::lock_guard<std::mutex> lk(b->mu);
-  cudaSetDevice(b->dev->ordinal);
+  cudaSetDevice(b->core.dev->ordinal);
   int rc = finish_batch(b, FRAME_TIMEOUT_MS);
   if (rc)
     return rc;
@@ -690,18 +844,19 @@ extern "C" int mopcuda_batch_pick(MopCudaBatch *b, uint32_t view, const int32_t 
   if (b->pick_xy.ensure(in_b) || b->pick_out.ensure(out_b) || b->h_pick.ensure(in_b + out_b))
     return MOPCUDA_ENOMEM;
   memcpy(b->h_pick.p, xy, in_b);
-  cudaStream_t s = b->stream;
+  LaunchCore &c = b->core;
+  cudaStream_t s = c.stream;
   CU_TRY(cudaMemcpyAsync(b->pick_xy.p, b->h_pick.p, in_b, cudaMemcpyHostToDevice, s));
   uint32_t *oid = b->pick_out.as<uint32_t>();
   float *odp = (float *)(oid + n);
   int32_t *oht = (int32_t *)(odp + n);
-  const ViewRec &r = b->vrec[view];
-  mopcuda_launch_pick(b->ids.as<uint32_t>() + r.sample_off, b->depth.as<float>() + r.sample_off,
+  const ViewRec &r = c.vrec[view];
+  mopcuda_launch_pick(c.ids.as<uint32_t>() + r.sample_off, c.depth.as<float>() + r.sample_off,
                       r.width, r.height, r.ssaa, b->pick_xy.as<int2>(), n, oid, odp, oht, s);
   CU_TRY(cudaGetLastError());
   uint8_t *hb = b->h_pick.as<uint8_t>() + in_b;
   CU_TRY(cudaMemcpyAsync(hb, b->pick_out.p, out_b, cudaMemcpyDeviceToHost, s));
-  rc = batch_sync(b, FRAME_TIMEOUT_MS);
+  rc = c.sync(FRAME_TIMEOUT_MS);
   if (rc)
     return rc;
   memcpy(ids, hb, 4ull * n);
@@ -716,26 +871,31 @@ extern "C" int mopcuda_batch_pick(MopCudaBatch *b, uint32_t view, const int32_t 
 extern "C" int mopcuda_batch_get_config(const MopCudaBatch *b, MopCudaBatchConfig *cfg) {
   if (!b || !cfg)
     return fail(MOPCUDA_EINVAL, "batch_get_config: bad arguments");
-  *cfg = b->cfg;
+  *cfg = b->core.cfg;
   return MOPCUDA_OK;
 }
 
-static bool block_ok(int n) { return n >= 32 && n <= 256 && n % 32 == 0; }
+static int config_ok(const MopCudaBatchConfig *c) {
+  if (c->small_side < 1 || c->small_side > 256 || c->small_area < 1 ||
+      c->small_area > 65536 || !mc_block_ok(c->vertex_block) || !mc_block_ok(c->setup_block) ||
+      !mc_block_ok(c->raster_block) || !mc_block_ok(c->large_block) ||
+      !mc_block_ok(c->shade_block) || c->grid_mul < 1 || c->grid_mul > 8)
+    return fail(MOPCUDA_EINVAL, "batch config: value out of range");
+  return MOPCUDA_OK;
+}
 
 extern "C" int mopcuda_batch_set_config(MopCudaBatch *b, const MopCudaBatchConfig *c) {
   if (!b || !c)
     return fail(MOPCUDA_EINVAL, "batch_set_config: bad arguments");
-  if (c->small_side < 1 || c->small_side > 256 || c->small_area < 1 ||
-      c->small_area > 65536 || !block_ok(c->vertex_block) || !block_ok(c->setup_block) ||
-      !block_ok(c->raster_block) || !block_ok(c->large_block) || !block_ok(c->shade_block) ||
-      c->grid_mul < 1 || c->grid_mul > 8)
-    return fail(MOPCUDA_EINVAL, "batch_set_config: value out of range");
-  std::lock_guard<std::mutex> lk(b->mu);
-  cudaSetDevice(b->dev->ordinal);
-  int rc = finish_batch(b, FRAME_TIMEOUT_MS);
+  int rc = config_ok(c);
   if (rc)
     return rc;
-  b->cfg = *c;
+  std::lock_guard<std::mutex> lk(b->mu);
+  cudaSetDevice(b->core.dev->ordinal);
+  rc = finish_batch(b, FRAME_TIMEOUT_MS);
+  if (rc)
+    return rc;
+  b->core.cfg = *c;
   drop_graph(b);
   return MOPCUDA_OK;
 }
@@ -764,8 +924,8 @@ extern "C" int mopcuda_batch_autotune(MopCudaBatch *b, int reps, char *report,
   if (!b || reps < 1)
     return fail(MOPCUDA_EINVAL, "batch_autotune: bad arguments");
   std::lock_guard<std::mutex> lk(b->mu);
-  cudaSetDevice(b->dev->ordinal);
-  MopCudaBatchConfig best = b->cfg;
+  cudaSetDevice(b->core.dev->ordinal);
+  MopCudaBatchConfig best = b->core.cfg;
   float best_ms = 0.0f;
   int rc = time_config(b, reps, &best_ms);
   if (rc)
@@ -788,7 +948,7 @@ extern "C" int mopcuda_batch_autotune(MopCudaBatch *b, int reps, char *report,
   for (const Axis &ax : axes)
     for (const auto &val : ax.values) {
       MopCudaBatchConfig c = best;
-      std::string nm = ax.name;
+      const std::string nm = ax.name;
       if (nm == "small") {
         c.small_side = val.first;
         c.small_area = val.second;
@@ -807,7 +967,7 @@ extern "C" int mopcuda_batch_autotune(MopCudaBatch *b, int reps, char *report,
       }
       if (memcmp(&c, &best, sizeof c) == 0)
         continue;
-      b->cfg = c;
+      b->core.cfg = c;
       drop_graph(b);
       float ms = 0.0f;
       rc = time_config(b, reps, &ms);
@@ -823,9 +983,9 @@ extern "C" int mopcuda_batch_autotune(MopCudaBatch *b, int reps, char *report,
         best_ms = ms;
       }
     }
-  b->cfg = best;
+  b->core.cfg = best;
   drop_graph(b);
-  char tail[256];
+  char tail[320];
   snprintf(tail, sizeof tail,
            "], \"best_ms\": %.4f, \"best\": {\"small_side\": %d, \"small_area\": %d, "
            "\"vertex_block\": %d, \"setup_block\": %d, \"raster_block\": %d, "
@@ -841,17 +1001,5 @@ extern "C" int mopcuda_batch_autotune(MopCudaBatch *b, int reps, char *report,
 }
 
 extern "C" uint64_t mopcuda_batch_device_bytes(const MopCudaBatch *b) {
-  if (!b)
-    return 0;
-  const DevArena *arenas[] = {&b->d_views, &b->d_frames, &b->d_view_draws, &b->d_ctr,
-                              &b->d_status, &b->d_posts, &b->d_post_views, &b->d_draws,
-                              &b->d_lights, &b->d_bounds, &b->clip, &b->world, &b->normal,
-                              &b->color, &b->rrec, &b->srec, &b->clipq, &b->large_list,
-                              &b->large_items, &b->keys, &b->shade_list, &b->pre, &b->out,
-                              &b->depth, &b->ids, &b->presented, &b->pick_xy, &b->pick_out,
-                              &b->irr, &b->pf, &b->brdf};
-  uint64_t t = 0;
-  for (const DevArena *a : arenas)
-    t += a->cap;
-  return t;
+  return b ? b->core.device_bytes() + b->pick_xy.cap + b->pick_out.cap : 0;
 }

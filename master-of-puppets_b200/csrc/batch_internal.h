@@ -1,0 +1,90 @@
+/*
+ * batch_internal.h — resident scenes and the launch machinery shared by the
+ * batch API (batch_api.cu) and the request server (server.cu).
+ */
+#ifndef MOPCUDA_BATCH_INTERNAL_H
+#define MOPCUDA_BATCH_INTERNAL_H
+
+#include "api_internal.h"
+
+struct MopCudaScene {
+  MopCudaDevice *dev = nullptr;
+  std::vector<DrawRec> draws; /* host records; mvp / cam_eye come per viewport */
+  std::vector<LightRec> lights;
+  std::vector<DrawBound> bounds;
+  uint64_t tris = 0, verts = 0;
+  uint64_t version = 0;     /* bumps when draws are added */
+  bool frozen = false;      /* held by a server: no more draws */
+  /* device copies of the immutable parts, uploaded when version changes */
+  DevArena d_bounds, d_lights;
+  uint64_t dev_version = ~0ull;
+  /* IBL maps captured from the device at scene creation */
+  DevArena irr, pf, brdf;
+  bool ibl_on = false;
+  int irr_w = 0, irr_h = 0, pf_w = 0, pf_h = 0, pf_levels = 0, brdf_size = 0;
+  float ibl_rot = 0.0f, ibl_int = 1.0f;
+  std::mutex mu;
+};
+
+/* Uploads bounds and lights when the draw list changed (synchronous). */
+int mc_scene_sync(MopCudaScene *s);
+/* The scene's draw table as of now, with its per-draw IBL constants. */
+void mc_scene_snapshot(MopCudaScene *s, DrawRec *dst);
+/* Estimated device bytes of one viewport of `samples` samples over scene s
+ * (sample buffers plus half the worst-case work pools). */
+uint64_t mc_view_bytes(const MopCudaScene *s, uint64_t samples, uint64_t pixels);
+
+/* One launch of N viewports over one or more resident scenes: its device
+ * buffers and work pools, and the stream it runs on. */
+struct LaunchCore {
+  MopCudaDevice *dev = nullptr;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  /* layout */
+  uint32_t nv = 0;
+  std::vector<ViewRec> vrec;
+  std::vector<MopCudaScene *> scenes; /* distinct scenes, index = ViewRec::scene */
+  std::vector<uint64_t> scene_draw_off;
+  uint64_t total_draws = 0, view_draw_total = 0;
+  std::vector<PostArgs> posts;
+  uint32_t post_count[4] = {0, 0, 0, 0}, post_tiles[4] = {0, 0, 0, 0};
+  unsigned long long total_samples = 0, total_pixels = 0;
+  /* inputs */
+  DevArena d_views, d_frames, d_view_draws, d_ctr, d_status, d_posts, d_post_views, d_draws,
+      d_scenes;
+  HostArena h_views, h_draws, h_scenes, h_status;
+  /* work pools */
+  DevArena clip, world, normal, color, rrec, srec, clipq, large_list, large_items;
+  unsigned long long vertex_pool = 0, rec_pool = 0, clip_pool = 0, large_pool = 0;
+  uint32_t fan_num = 1, large_num = 1;
+  /* sample / pixel buffers */
+  DevArena keys, shade_list, pre, out, depth, ids, presented;
+  /* launch shape */
+  MopCudaBatchConfig cfg = {SMALL_MAX_SIDE, SMALL_MAX_AREA, 256, 256, 128, 256, 256, 1};
+  float exposure = 1.0f;
+  uint32_t post_effects = 0;
+  float lut[256];
+  uint64_t launches = 0;
+
+  int init(MopCudaDevice *d);
+  void release();
+  /* views[i] renders scene scene_of[i] (index into sc); no_color[i] (may be
+   * null) marks visibility-only viewports. */
+  int set_layout(const MopCudaView *views, const uint32_t *scene_of, const uint8_t *no_color,
+                 uint32_t n, const std::vector<MopCudaScene *> &sc);
+  /* Snapshots the scenes' draw tables into pinned memory; sizes the pools. */
+  int stage();
+  /* Enqueues the whole launch on `stream` (capturable). */
+  int enqueue();
+  /* After ev1: true when the launch must run again (reserves or pools grew). */
+  int after(bool *rerun, int attempt);
+  uint64_t device_bytes() const;
+  int sync(int timeout_ms);
+  /* Frees the pools and sample buffers (they grow back on the next use). */
+  void trim();
+};
+
+static inline bool mc_block_ok(int n) { return n >= 32 && n <= 256 && n % 32 == 0; }
+int mc_check_view(const MopCudaView &v);
+
+#endif

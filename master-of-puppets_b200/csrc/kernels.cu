@@ -1167,8 +1167,10 @@ __device__ __forceinline__ void shade_item(const FrameArgs &a, uint32_t j, const
         w[e] = fold_add(fold_add(r.w0[e], r.dy[e], jr), r.dx[e], kc);
       float b0 = w[0] * r.inv_area, b1 = w[1] * r.inv_area, b2 = w[2] * r.inv_area;
       depth = b0 * r.zc[0] + b1 * r.zc[1] + b2 * r.zc[2];
-      if (s.v[0] >= a.vertex_cap || s.v[1] >= a.vertex_cap || s.v[2] >= a.vertex_cap) {
-        hdr[0] = hdr[1] = hdr[2] = 0.0f; /* unreachable for live records */
+      if (a.no_color || s.v[0] >= a.vertex_cap || s.v[1] >= a.vertex_cap ||
+          s.v[2] >= a.vertex_cap) {
+        hdr[0] = hdr[1] = hdr[2] = 0.0f; /* visibility-only view (bad vertex slots are
+                                           unreachable for live records) */
       } else {
         const float4 N[3] = {a.normal[s.v[0]], a.normal[s.v[1]], a.normal[s.v[2]]};
         float pc[3] = {b0 * N[0].w, b1 * N[1].w, b2 * N[2].w}; /* .w = 1/clip.w */
@@ -1607,22 +1609,23 @@ __global__ void __launch_bounds__(256) k_batch_prepare(BatchArgs b) {
   __shared__ uint32_t s_tot[3];
   const uint32_t v = blockIdx.x;
   const ViewRec &vw = b.views[v];
-  DrawRec *out = b.view_draws + (size_t)v * b.nd;
+  const SceneDesc &sc = b.scenes[vw.scene];
+  DrawRec *out = b.view_draws + vw.draw_off;
   const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
   if (threadIdx.x == 0)
     s_tot[0] = s_tot[1] = s_tot[2] = 0u;
   __syncthreads();
-  for (uint32_t base = 0; base < b.nd; base += 256u) {
+  for (uint32_t base = 0; base < sc.nd; base += 256u) {
     const uint32_t i = base + threadIdx.x;
     float mvp[16];
     uint32_t x[3] = {0u, 0u, 0u};
-    if (i < b.nd) {
-      const DrawRec &sd = b.scene[i];
+    if (i < sc.nd) {
+      const DrawRec &sd = sc.draws[i];
       float vm[16];
       dev_mat4_mul(vw.view, sd.model, vm);
       dev_mat4_mul(vw.proj, vm, mvp);
       const uint32_t tc = sd.index_count / 3u;
-      if (tc > 0u && !draw_culled(mvp, b.bounds[i], sd.depth_bias == 0.0f)) {
+      if (tc > 0u && !draw_culled(mvp, sc.bounds[i], sd.depth_bias == 0.0f)) {
         x[0] = 1u;
         x[1] = sd.vertex_count;
         x[2] = tc;
@@ -1653,7 +1656,7 @@ __global__ void __launch_bounds__(256) k_batch_prepare(BatchArgs b) {
     }
     __syncthreads();
     if (x[0]) {
-      DrawRec r = b.scene[i];
+      DrawRec r = sc.draws[i];
       for (int k = 0; k < 16; k++)
         r.mvp[k] = mvp[k];
       r.cam_eye[0] = vw.eye[0];
@@ -1667,6 +1670,20 @@ __global__ void __launch_bounds__(256) k_batch_prepare(BatchArgs b) {
   }
   if (threadIdx.x == 0) {
     FrameArgs a = b.tmpl;
+    a.lights = sc.lights;
+    a.light_total = sc.light_total;
+    a.irr = sc.irr;
+    a.irr_w = sc.irr_w;
+    a.irr_h = sc.irr_h;
+    a.pf = sc.pf;
+    a.pf_w = sc.pf_w;
+    a.pf_h = sc.pf_h;
+    a.pf_levels = sc.pf_levels;
+    a.brdf = sc.brdf;
+    a.brdf_size = sc.brdf_size;
+    a.ibl_rotation = sc.ibl_rotation;
+    a.ibl_intensity = sc.ibl_intensity;
+    a.no_color = (int)vw.no_color;
     a.draws = out;
     a.draw_count = s_tot[0];
     a.total_vertices = s_tot[1];
@@ -1868,19 +1885,21 @@ __global__ void __launch_bounds__(256) k_b_resolve(const FrameArgs *__restrict__
   }
 }
 
-/* All viewports of a batch share the scene's light array. */
+/* shared_lights: every viewport of the launch reads one light array (one
+ * scene), staged in shared memory; otherwise each reads its own. */
 __global__ void __launch_bounds__(256, 4) k_b_shade(const FrameArgs *__restrict__ fr,
-                                                    uint32_t nv) {
+                                                    uint32_t nv, int shared_lights) {
   __shared__ LightRec s_lights[SHADE_SMEM_LIGHTS];
   __shared__ uint32_t s_pre[MOPCUDA_MAX_VIEWS + 1];
-  const LightRec *lights = stage_lights(fr[0], s_lights);
+  const LightRec *lights = shared_lights ? stage_lights(fr[0], s_lights) : nullptr;
   const uint32_t total = views_prefix<ST_SHADE>(fr, nv, s_pre);
   uint32_t v = 0;
   for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < total;
        g += gridDim.x * blockDim.x) {
     while (s_pre[v + 1] <= g)
       v++;
-    shade_item(fr[v], g - s_pre[v], lights);
+    const FrameArgs &a = fr[v];
+    shade_item(a, g - s_pre[v], lights ? lights : a.lights);
   }
 }
 
@@ -1953,7 +1972,7 @@ void mopcuda_batch_grids(BatchLaunch &cfg) {
 
 int mopcuda_launch_batch(const BatchArgs &b, const PostArgs *posts, const uint32_t *post_views[4],
                          const uint32_t post_count[4], const uint32_t post_tiles[4],
-                         const BatchLaunch &cfg, cudaStream_t s) {
+                         const BatchLaunch &cfg, bool shared_lights, cudaStream_t s) {
   if (b.nv == 0)
     return 0;
   int launches = 0;
@@ -1969,7 +1988,7 @@ int mopcuda_launch_batch(const BatchArgs &b, const PostArgs *posts, const uint32
   k_b_large_scan<<<nv, 1024, 0, s>>>(fr);
   k_b_items<ST_RLARGE><<<cfg.grid_rlarge, cfg.large_block, 0, s>>>(fr, nv);
   k_b_resolve<<<sms * 8, 256, 0, s>>>(fr, nv);
-  k_b_shade<<<cfg.grid_shade, cfg.shade_block, 0, s>>>(fr, nv);
+  k_b_shade<<<cfg.grid_shade, cfg.shade_block, 0, s>>>(fr, nv, shared_lights ? 1 : 0);
   launches += 10;
   dim3 pb(POST_BX, POST_BY);
   for (int k = 0; k < 4; k++) {

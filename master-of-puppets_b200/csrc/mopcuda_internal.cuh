@@ -169,6 +169,8 @@ struct FrameArgs {
   /* small-record limits: bbox side and area (larger records are rasterised
    * item-parallel) */
   int small_side, small_area;
+  /* visibility only: shading writes depth and IDs but no colour */
+  int no_color;
 };
 
 struct PostArgs {
@@ -231,9 +233,25 @@ struct ViewRec {
   float clear[4];
   int width, height; /* sample resolution */
   int ssaa;
+  uint32_t scene;    /* index into BatchArgs::scenes */
+  uint32_t no_color; /* visibility only (picks): depth and IDs, no shading */
   uint32_t pad;
   unsigned long long sample_off; /* keys, shade list, pre, out, depth, ids */
   unsigned long long pixel_off;  /* presented */
+  unsigned long long draw_off;   /* first of the scene's nd slots in view_draws */
+};
+
+/* One resident scene of a batch: its draw table for this launch, bounds,
+ * lights and IBL maps. */
+struct SceneDesc {
+  const DrawRec *draws; /* mvp, cam_eye, vbase and tbase unused */
+  const struct DrawBound *bounds;
+  uint32_t nd;
+  uint32_t light_total;
+  const LightRec *lights;
+  const float *irr, *pf, *brdf;
+  int irr_w, irr_h, pf_w, pf_h, pf_levels, brdf_size;
+  float ibl_rotation, ibl_intensity;
 };
 
 /* Mesh-local bounding sphere of a draw's vertices; r < 0 (or NaN) means the
@@ -252,16 +270,14 @@ struct BatchStatus {
 };
 
 struct BatchArgs {
-  const DrawRec *scene; /* scene draws: mvp, cam_eye, vbase and tbase unused */
-  const DrawBound *bounds;
-  uint32_t nd;
+  const SceneDesc *scenes;
   const ViewRec *views;
   uint32_t nv;
-  FrameArgs *frames;  /* nv, filled by k_batch_prepare / k_batch_alloc */
-  DrawRec *view_draws; /* nv * nd: each viewport's visible draws */
-  Counters *ctr;      /* nv */
+  FrameArgs *frames;   /* nv, filled by k_batch_prepare / k_batch_alloc */
+  DrawRec *view_draws; /* per viewport its scene's nd slots: the visible draws */
+  Counters *ctr;       /* nv */
   BatchStatus *status;
-  FrameArgs tmpl;     /* lights, IBL, exposure, small-record limits */
+  FrameArgs tmpl;      /* exposure and small-record limits */
   /* pools (per-viewport ranges assigned on the device) */
   float4 *clip, *world, *normal, *color;
   unsigned long long vertex_pool;
@@ -301,7 +317,7 @@ void mopcuda_batch_grids(BatchLaunch &cfg);
  * PostArgs.  Returns the number of kernels launched. */
 int mopcuda_launch_batch(const BatchArgs &b, const PostArgs *posts, const uint32_t *post_views[4],
                          const uint32_t post_count[4], const uint32_t post_tiles[4],
-                         const BatchLaunch &cfg, cudaStream_t s);
+                         const BatchLaunch &cfg, bool shared_lights, cudaStream_t s);
 
 /* ev (optional, 7 events): stage boundaries
  * vertex | setup+clip | raster | resolve | shade | post */

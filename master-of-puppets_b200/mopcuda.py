@@ -66,6 +66,27 @@ class MopCudaBatchConfig(C.Structure):
 
 
 BATCH_COLOR, BATCH_PRESENTED, BATCH_DEPTH, BATCH_IDS = 0, 1, 2, 3
+REQ_RENDER, REQ_PICK = 0, 1
+
+
+class MopCudaServerConfig(C.Structure):
+    _fields_ = [("hbm_budget", C.c_uint64), ("max_views", C.c_uint32),
+                ("max_inflight", C.c_uint32), ("batch_window_us", C.c_uint32)]
+
+
+class MopCudaRequest(C.Structure):
+    _fields_ = [("kind", C.c_uint32), ("scene", C.c_uint32), ("view", MopCudaView),
+                ("color", C.c_void_p), ("ids", C.c_void_p), ("depth", C.c_void_p),
+                ("pick_xy", C.c_void_p), ("pick_n", C.c_uint32), ("pick_ids", C.c_void_p),
+                ("pick_depths", C.c_void_p), ("pick_hits", C.c_void_p)]
+
+
+class MopCudaServerStats(C.Structure):
+    _fields_ = [("submitted", C.c_uint64), ("completed", C.c_uint64), ("failed", C.c_uint64),
+                ("launches", C.c_uint64), ("launched_views", C.c_uint64),
+                ("reruns", C.c_uint64), ("peak_inflight_bytes", C.c_uint64),
+                ("device_bytes", C.c_uint64), ("max_views_in_launch", C.c_uint32),
+                ("pad", C.c_uint32)]
 
 # (name, restype, argtypes) for every entry point of include/mop_cuda.h
 _P = C.c_void_p
@@ -127,6 +148,13 @@ SIGNATURES = [
     ("mopcuda_batch_set_config", C.c_int, [_P, C.POINTER(MopCudaBatchConfig)]),
     ("mopcuda_batch_autotune", C.c_int, [_P, C.c_int, C.c_char_p, C.c_size_t]),
     ("mopcuda_batch_device_bytes", C.c_uint64, [_P]),
+    ("mopcuda_server_create", _P, [_P, C.POINTER(MopCudaServerConfig)]),
+    ("mopcuda_server_destroy", None, [_P]),
+    ("mopcuda_server_add_scene", C.c_int, [_P, _P]),
+    ("mopcuda_server_submit", C.c_int, [_P, C.POINTER(MopCudaRequest), C.POINTER(C.c_uint64)]),
+    ("mopcuda_server_wait", C.c_int, [_P, C.c_uint64, C.c_int, C.POINTER(C.c_double)]),
+    ("mopcuda_server_drain", C.c_int, [_P, C.c_int]),
+    ("mopcuda_server_stats", C.c_int, [_P, C.POINTER(MopCudaServerStats)]),
     ("mopcuda_mat4_multiply", None, [_P, _P, _P]),
     ("mopcuda_mat4_compose_trs", None, [_P, _P, _P, _P]),
     ("mopcuda_camera_matrices", None, [_P, _P, _P, C.c_float, C.c_float, C.c_float, C.c_int,
@@ -444,11 +472,11 @@ def view_struct(v) -> MopCudaView:
     return s
 
 
-class BatchRenderer(_Resident):
-    """A resident scene rendered into many viewports per graph launch
-    (mopcuda_scene_* / mopcuda_batch_*)."""
+class ResidentScene(_Resident):
+    """A scene uploaded once and recorded as a MopCudaScene (one draw per
+    mesh, in mesh order) for batches and servers."""
 
-    def __init__(self, device: Device, scene, views, ibl=None):
+    def __init__(self, device: Device, scene, ibl=None):
         super().__init__(device, scene, ibl)
         L = self.L
         self.sh_scene = L.mopcuda_scene_create(device.h)
@@ -459,6 +487,29 @@ class BatchRenderer(_Resident):
             rc = L.mopcuda_scene_add_draw(self.sh_scene, C.byref(dr))
             if rc < 0:
                 raise MopCudaError(rc, "scene_add_draw")
+
+    def set_model(self, k: int, model):
+        m = _f32(model)
+        _check(self.L.mopcuda_scene_set_model(self.sh_scene, k, m.ctypes.data), "scene_set_model")
+
+    @property
+    def triangles(self) -> int:
+        return int(self.L.mopcuda_scene_triangle_count(self.sh_scene))
+
+    def close(self):
+        if getattr(self, "sh_scene", None):
+            self.L.mopcuda_scene_destroy(self.sh_scene)
+            self.sh_scene = None
+        self.close_resident()
+
+
+class BatchRenderer(ResidentScene):
+    """A resident scene rendered into many viewports per graph launch
+    (mopcuda_scene_* / mopcuda_batch_*)."""
+
+    def __init__(self, device: Device, scene, views, ibl=None):
+        super().__init__(device, scene, ibl)
+        L = self.L
         self.views = list(views)
         arr = (MopCudaView * len(self.views))(*[view_struct(v) for v in self.views])
         self.h = L.mopcuda_batch_create(self.sh_scene, arr, len(self.views))
@@ -478,10 +529,6 @@ class BatchRenderer(_Resident):
         arr = (MopCudaView * len(views))(*[view_struct(v) for v in views])
         _check(self.L.mopcuda_batch_set_views(self.h, arr, len(views)), "batch_set_views")
         self.views = views
-
-    def set_model(self, k: int, model):
-        m = _f32(model)
-        _check(self.L.mopcuda_scene_set_model(self.sh_scene, k, m.ctypes.data), "scene_set_model")
 
     def submit(self):
         _check(self.L.mopcuda_batch_submit(self.h), "batch_submit")
@@ -545,7 +592,85 @@ class BatchRenderer(_Resident):
         if self.h:
             self.L.mopcuda_batch_destroy(self.h)
             self.h = None
-        if self.sh_scene:
-            self.L.mopcuda_scene_destroy(self.sh_scene)
-            self.sh_scene = None
-        self.close_resident()
+        super().close()
+
+
+class Ticket:
+    """An in-flight server request and the host buffers it fills."""
+
+    def __init__(self, req, kind, view, color=None, ids=None, depth=None, xy=None):
+        self.req, self.kind, self.view = req, kind, view
+        self.color, self.ids, self.depth, self.xy = color, ids, depth, xy
+        self.pick = None
+        self.id = 0
+        self.latency_ms = None
+
+
+class Server:
+    """Continuous-batching request server over resident scenes
+    (mopcuda_server_*)."""
+
+    def __init__(self, device: Device, hbm_budget: int, max_views: int = 64,
+                 max_inflight: int = 3, batch_window_us: int = 0):
+        self.dev = device
+        self.L = device.L
+        cfg = MopCudaServerConfig(hbm_budget, max_views, max_inflight, batch_window_us)
+        self.h = self.L.mopcuda_server_create(device.h, C.byref(cfg))
+        if not self.h:
+            raise RuntimeError(f"server_create failed: {last_error()}")
+        self.scenes = []
+
+    def add_scene(self, rs: ResidentScene) -> int:
+        rc = self.L.mopcuda_server_add_scene(self.h, rs.sh_scene)
+        if rc < 0:
+            raise MopCudaError(rc, "server_add_scene")
+        self.scenes.append(rs)
+        return rc
+
+    def _submit(self, t: Ticket) -> Ticket:
+        tid = C.c_uint64()
+        _check(self.L.mopcuda_server_submit(self.h, C.byref(t.req), C.byref(tid)), "server_submit")
+        t.id = tid.value
+        return t
+
+    def submit_render(self, scene_id: int, view, want_ids=False, want_depth=False) -> Ticket:
+        r = MopCudaRequest()
+        r.kind, r.scene, r.view = REQ_RENDER, scene_id, view_struct(view)
+        sw, sh = view.width * view.ssaa, view.height * view.ssaa
+        color = np.empty((view.height, view.width, 4), np.uint8)
+        ids = np.empty((sh, sw), np.uint32) if want_ids else None
+        dep = np.empty((sh, sw), np.float32) if want_depth else None
+        r.color = color.ctypes.data
+        r.ids = ids.ctypes.data if ids is not None else None
+        r.depth = dep.ctypes.data if dep is not None else None
+        return self._submit(Ticket(r, REQ_RENDER, view, color, ids, dep))
+
+    def submit_pick(self, scene_id: int, view, xy) -> Ticket:
+        xy = np.ascontiguousarray(xy, np.int32)
+        n = xy.shape[0]
+        r = MopCudaRequest()
+        r.kind, r.scene, r.view = REQ_PICK, scene_id, view_struct(view)
+        t = Ticket(r, REQ_PICK, view, xy=xy)
+        t.pick = (np.zeros(n, np.uint32), np.zeros(n, np.float32), np.zeros(n, np.int32))
+        r.pick_xy, r.pick_n = xy.ctypes.data, n
+        r.pick_ids, r.pick_depths, r.pick_hits = [a.ctypes.data for a in t.pick]
+        return self._submit(t)
+
+    def wait(self, t: Ticket, timeout_ms: int = 20000) -> float:
+        lat = C.c_double()
+        _check(self.L.mopcuda_server_wait(self.h, t.id, timeout_ms, C.byref(lat)), "server_wait")
+        t.latency_ms = float(lat.value)
+        return t.latency_ms
+
+    def drain(self, timeout_ms: int = 60000):
+        _check(self.L.mopcuda_server_drain(self.h, timeout_ms), "server_drain")
+
+    def stats(self) -> dict:
+        st = MopCudaServerStats()
+        _check(self.L.mopcuda_server_stats(self.h, C.byref(st)), "server_stats")
+        return {f: getattr(st, f) for f, _ in MopCudaServerStats._fields_ if f != "pad"}
+
+    def close(self):
+        if self.h:
+            self.L.mopcuda_server_destroy(self.h)
+            self.h = None

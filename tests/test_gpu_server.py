@@ -1,0 +1,141 @@
+"""Request server (mopcuda_server_*): continuous batching over resident
+scenes.  A request's result is the same alone and in a mix of other scenes,
+sizes, SSAA factors and pick requests, and equals the single-viewport frame
+of the same draws and camera; admission respects the HBM budget (a budget
+too small for two requests runs them one launch at a time, same results).
+"""
+import dataclasses
+
+import numpy as np
+import pytest
+
+import mopcuda
+import scenes
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def world(cuda_device):
+    ibl = scenes.procedural_ibl((0.4, 0.8, 0.35), irr_size=(32, 16), pf_size=(64, 32),
+                                levels=4, brdf_size=64)
+    scs = [scenes.config2(seed=s, width=160, height=90, ssaa=1, instances=n, tex_size=64)
+           for s, n in ((11, 10), (12, 16), (13, 6))]
+    rss = [mopcuda.ResidentScene(cuda_device, sc, ibl) for sc in scs]
+    yield scs, rss, ibl
+    for rs in rss:
+        rs.close()
+
+
+def _views(sc, n, seed):
+    return scenes.batch_views(sc, n=n, seed=seed, min_px=32 * 32, max_px=240 * 160)
+
+
+def _plain(dev, sc, v, ibl, xy=None):
+    r = mopcuda.SceneRenderer(dev, scenes.scene_for_view(sc, v), ibl)
+    try:
+        r.render()
+        out = {"color": r.color(), "ids": r.object_id(), "depth": r.depth()}
+        if xy is not None:
+            out["pick"] = r.pick(xy)
+        return out
+    finally:
+        r.close()
+
+
+def _same_render(t, want, label):
+    assert (t.color == want["color"]).all(), f"{label}: colour differs"
+    assert (t.ids == want["ids"]).all(), f"{label}: IDs differ"
+    assert (t.depth.view(np.uint32) == want["depth"].view(np.uint32)).all(), f"{label}: depth"
+
+
+def _same_pick(got, want, label):
+    for a, b in zip(got, want):
+        assert (np.asarray(a).view(np.uint32) == np.asarray(b).view(np.uint32)).all(), label
+
+
+def test_server_alone_equals_mix_equals_frame(cuda_device, world):
+    scs, rss, ibl = world
+    srv = mopcuda.Server(cuda_device, hbm_budget=8 << 30, max_views=16, max_inflight=2)
+    try:
+        sid = [srv.add_scene(rs) for rs in rss]
+        probe_v = dataclasses.replace(_views(scs[1], 1, seed=5)[0], ssaa=2)
+        pick_v = _views(scs[2], 1, seed=6)[0]
+        xy = scenes.pick_points(dataclasses.replace(scs[2], width=pick_v.width,
+                                                    height=pick_v.height), 48, seed=2)
+        # alone
+        a = srv.submit_render(sid[1], probe_v, want_ids=True, want_depth=True)
+        srv.wait(a)
+        ap = srv.submit_pick(sid[2], pick_v, xy)
+        srv.wait(ap)
+        # in a mix: 40 requests over all scenes, the probes in the middle
+        rng = np.random.default_rng(9)
+        mix = []
+        for k in range(40):
+            s = int(rng.integers(0, 3))
+            v = _views(scs[s], 1, seed=100 + k)[0]
+            if k % 7 == 3:
+                pts = scenes.pick_points(dataclasses.replace(scs[s], width=v.width,
+                                                             height=v.height), 16, seed=k)
+                mix.append(srv.submit_pick(sid[s], v, pts))
+            else:
+                mix.append(srv.submit_render(sid[s], v))
+            if k == 20:
+                b = srv.submit_render(sid[1], probe_v, want_ids=True, want_depth=True)
+                bp = srv.submit_pick(sid[2], pick_v, xy)
+        for t in mix + [b, bp]:
+            srv.wait(t)
+        assert (a.color == b.color).all() and (a.ids == b.ids).all()
+        assert (a.depth.view(np.uint32) == b.depth.view(np.uint32)).all()
+        _same_pick(ap.pick, bp.pick, "pick alone vs mix")
+        st = srv.stats()
+        assert st["completed"] == 44 and st["failed"] == 0
+        assert st["launches"] < st["completed"] and st["max_views_in_launch"] > 1, st
+        # and both equal the request's own frame
+        want = _plain(cuda_device, scs[1], probe_v, ibl)
+        _same_render(b, want, "probe vs frame")
+        wantp = _plain(cuda_device, scs[2], pick_v, ibl, xy)
+        _same_pick(bp.pick, wantp["pick"], "pick vs frame")
+        for t in mix[:12]:
+            if t.kind == mopcuda.REQ_RENDER:
+                w = _plain(cuda_device, scs[sid.index(t.req.scene)], t.view, ibl)
+                assert (t.color == w["color"]).all(), "mix render vs frame"
+    finally:
+        srv.close()
+
+
+def test_server_budget_admission(cuda_device, world):
+    scs, rss, ibl = world
+    srv = mopcuda.Server(cuda_device, hbm_budget=1, max_views=16, max_inflight=2)
+    try:
+        sid = srv.add_scene(rss[0])
+        views = _views(scs[0], 6, seed=7)
+        ts = [srv.submit_render(sid, v, want_ids=True, want_depth=True) for v in views]
+        for t in ts:
+            srv.wait(t)
+        st = srv.stats()
+        assert st["max_views_in_launch"] == 1 and st["launches"] == 6, st
+        for t, v in zip(ts, views):
+            _same_render(t, _plain(cuda_device, scs[0], v, ibl), "budget-limited")
+    finally:
+        srv.close()
+
+
+def test_server_trs_update_between_requests(cuda_device, world):
+    scs, rss, ibl = world
+    srv = mopcuda.Server(cuda_device, hbm_budget=8 << 30, max_views=8, max_inflight=2)
+    try:
+        sid = srv.add_scene(rss[2])
+        v = _views(scs[2], 1, seed=8)[0]
+        sc = scs[2]
+        m = sc.meshes[0].transform.copy()
+        m[12:15] += np.float32(0.75)
+        rss[2].set_model(0, m)
+        t = srv.submit_render(sid, v, want_ids=True, want_depth=True)
+        srv.wait(t)
+        moved = dataclasses.replace(sc, meshes=[dataclasses.replace(sc.meshes[0], transform=m)]
+                                    + sc.meshes[1:])
+        _same_render(t, _plain(cuda_device, moved, v, ibl), "after TRS update")
+        rss[2].set_model(0, sc.meshes[0].transform)
+    finally:
+        srv.close()
