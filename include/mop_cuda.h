@@ -166,6 +166,11 @@ int mopcuda_set_ibl(MopCudaDevice *dev, const float *irradiance, int iw, int ih,
  *      (rhi.h:160-175, 214-218), cpu_backend.c:197-211, 528-657 -------- */
 int mopcuda_frame_begin(MopCudaDevice *dev, MopCudaFramebuffer *fb, const float clear_rgba[4]);
 int mopcuda_draw(MopCudaDevice *dev, MopCudaFramebuffer *fb, const MopCudaDraw *draw);
+/* n draws in array order, exactly as n mopcuda_draw calls (no reference
+ * counterpart: a convenience for hosts that keep their draw calls in an
+ * array; stops at the first draw that fails). */
+int mopcuda_draw_list(MopCudaDevice *dev, MopCudaFramebuffer *fb, const MopCudaDraw *draws,
+                      uint32_t n);
 /* view/projection multiply per instance as cpu_draw_instanced does
  * (mvp = P * (V * instance), cpu_backend.c:638-657). */
 int mopcuda_draw_instanced(MopCudaDevice *dev, MopCudaFramebuffer *fb, const MopCudaDraw *draw,
@@ -327,7 +332,8 @@ uint64_t mopcuda_batch_device_bytes(const MopCudaBatch *batch);
  * request's own frame (mopcuda_frame_* of the same draws and camera),
  * whatever it was batched with.  Scenes added to a server take no further
  * draws (mopcuda_scene_add_draw fails) until the server is destroyed; model
- * matrices may change at any time and a request sees them as of its launch. */
+ * matrices may change at any time and a request renders them as they were
+ * when it was submitted. */
 typedef struct MopCudaServer MopCudaServer;
 
 typedef struct MopCudaServerConfig {
@@ -346,7 +352,9 @@ typedef struct MopCudaRequest {
   MopCudaView view;
   /* RENDER: presented RGBA8 (width*height*4 bytes) and optionally the
    * sample-resolution object IDs and depth; NULL skips a buffer.  The
-   * memory must stay valid until mopcuda_server_wait returns. */
+   * memory must stay valid until mopcuda_server_wait returns.  Page-locked
+   * buffers (mopcuda_host_alloc) receive the device copy directly; others
+   * are staged and copied by the server's worker thread. */
   uint8_t *color;
   uint32_t *ids;
   float *depth;
@@ -382,6 +390,9 @@ int mopcuda_server_wait(MopCudaServer *srv, uint64_t ticket, int timeout_ms, dou
 /* Waits until nothing is queued or running. */
 int mopcuda_server_drain(MopCudaServer *srv, int timeout_ms);
 int mopcuda_server_stats(MopCudaServer *srv, MopCudaServerStats *stats);
+/* Page-locked host memory (cudaMallocHost) for request buffers. */
+void *mopcuda_host_alloc(size_t bytes);
+void mopcuda_host_free(void *p);
 
 /* ---- host-side matrices (the device receives finished matrices) ------- */
 /* out = a * b, column-major (mop_mat4_multiply, reference math.c:182-194). */

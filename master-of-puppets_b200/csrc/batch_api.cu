@@ -172,6 +172,7 @@ extern "C" int mopcuda_scene_set_model(MopCudaScene *s, uint32_t index, const fl
   if (index >= s->draws.size())
     return fail(MOPCUDA_EINVAL, "scene_set_model: index %u out of range", index);
   memcpy(s->draws[index].model, model, sizeof s->draws[index].model);
+  s->gen++;
   return MOPCUDA_OK;
 }
 
@@ -199,12 +200,27 @@ int mc_scene_sync(MopCudaScene *s) {
   return MOPCUDA_OK;
 }
 
-void mc_scene_snapshot(MopCudaScene *s, DrawRec *dst) {
+void mc_scene_snapshot(MopCudaScene *s, DrawRec *dst, const std::vector<float> *models) {
   std::lock_guard<std::mutex> lk(s->mu);
   const uint32_t nd = (uint32_t)s->draws.size();
   if (nd)
     memcpy(dst, s->draws.data(), sizeof(DrawRec) * nd);
+  if (models && models->size() == 16ull * nd)
+    for (uint32_t i = 0; i < nd; i++)
+      memcpy(dst[i].model, models->data() + 16ull * i, sizeof dst[i].model);
   mc_ibl_consts(s->ibl_on, s->pf_w, s->pf_h, s->pf_levels, s->brdf_size, dst, nd);
+}
+
+std::shared_ptr<const std::vector<float>> mc_scene_models(MopCudaScene *s) {
+  std::lock_guard<std::mutex> lk(s->mu);
+  if (!s->models || s->models_gen != s->gen || s->models->size() != 16ull * s->draws.size()) {
+    auto m = std::make_shared<std::vector<float>>(16ull * s->draws.size());
+    for (size_t i = 0; i < s->draws.size(); i++)
+      memcpy(m->data() + 16 * i, s->draws[i].model, 16 * sizeof(float));
+    s->models = m;
+    s->models_gen = s->gen;
+  }
+  return s->models;
 }
 
 static void pool_need(uint64_t T, uint64_t V, uint32_t fan_num, uint32_t large_num,
@@ -311,7 +327,8 @@ uint64_t LaunchCore::device_bytes() const {
 
 int LaunchCore::set_layout(const MopCudaView *views, const uint32_t *scene_of,
                            const uint8_t *no_color, uint32_t n,
-                           const std::vector<MopCudaScene *> &sc) {
+                           const std::vector<MopCudaScene *> &sc,
+                           const std::vector<std::shared_ptr<const std::vector<float>>> *models) {
   if (n == 0 || n > MOPCUDA_MAX_VIEWS)
     return fail(MOPCUDA_EINVAL, "launch: 1..%d views", MOPCUDA_MAX_VIEWS);
   for (uint32_t i = 0; i < n; i++) {
@@ -324,6 +341,10 @@ int LaunchCore::set_layout(const MopCudaView *views, const uint32_t *scene_of,
   }
   nv = n;
   scenes = sc;
+  if (models)
+    scene_models = *models;
+  else
+    scene_models.assign(sc.size(), nullptr);
   scene_draw_off.assign(sc.size(), 0);
   total_draws = 0;
   for (size_t k = 0; k < sc.size(); k++) {
@@ -449,7 +470,7 @@ int LaunchCore::stage() {
     int rc = mc_scene_sync(s);
     if (rc)
       return rc;
-    mc_scene_snapshot(s, hd + scene_draw_off[k]);
+    mc_scene_snapshot(s, hd + scene_draw_off[k], scene_models[k].get());
     SceneDesc &d = sd[k];
     memset(&d, 0, sizeof d);
     d.draws = d_draws.as<DrawRec>() + scene_draw_off[k];

@@ -7,6 +7,8 @@
 
 #include "api_internal.h"
 
+#include <memory>
+
 struct MopCudaScene {
   MopCudaDevice *dev = nullptr;
   std::vector<DrawRec> draws; /* host records; mvp / cam_eye come per viewport */
@@ -14,6 +16,9 @@ struct MopCudaScene {
   std::vector<DrawBound> bounds;
   uint64_t tris = 0, verts = 0;
   uint64_t version = 0;     /* bumps when draws are added */
+  uint64_t gen = 0;         /* bumps when a model matrix changes */
+  std::shared_ptr<const std::vector<float>> models; /* models as of models_gen */
+  uint64_t models_gen = ~0ull;
   bool frozen = false;      /* held by a server: no more draws */
   /* device copies of the immutable parts, uploaded when version changes */
   DevArena d_bounds, d_lights;
@@ -28,8 +33,11 @@ struct MopCudaScene {
 
 /* Uploads bounds and lights when the draw list changed (synchronous). */
 int mc_scene_sync(MopCudaScene *s);
-/* The scene's draw table as of now, with its per-draw IBL constants. */
-void mc_scene_snapshot(MopCudaScene *s, DrawRec *dst);
+/* The scene's draw table as of now, with its per-draw IBL constants; with
+ * models (nd x 16 floats) the model matrices are taken from there. */
+void mc_scene_snapshot(MopCudaScene *s, DrawRec *dst, const std::vector<float> *models);
+/* The scene's model matrices now (shared until the next change). */
+std::shared_ptr<const std::vector<float>> mc_scene_models(MopCudaScene *s);
 /* Estimated device bytes of one viewport of `samples` samples over scene s
  * (sample buffers plus half the worst-case work pools). */
 uint64_t mc_view_bytes(const MopCudaScene *s, uint64_t samples, uint64_t pixels);
@@ -43,7 +51,9 @@ struct LaunchCore {
   /* layout */
   uint32_t nv = 0;
   std::vector<ViewRec> vrec;
-  std::vector<MopCudaScene *> scenes; /* distinct scenes, index = ViewRec::scene */
+  std::vector<MopCudaScene *> scenes; /* scene entries, index = ViewRec::scene */
+  /* per entry: model matrices to render with (null: the scene's current) */
+  std::vector<std::shared_ptr<const std::vector<float>>> scene_models;
   std::vector<uint64_t> scene_draw_off;
   uint64_t total_draws = 0, view_draw_total = 0;
   std::vector<PostArgs> posts;
@@ -71,7 +81,8 @@ struct LaunchCore {
   /* views[i] renders scene scene_of[i] (index into sc); no_color[i] (may be
    * null) marks visibility-only viewports. */
   int set_layout(const MopCudaView *views, const uint32_t *scene_of, const uint8_t *no_color,
-                 uint32_t n, const std::vector<MopCudaScene *> &sc);
+                 uint32_t n, const std::vector<MopCudaScene *> &sc,
+                 const std::vector<std::shared_ptr<const std::vector<float>>> *models = nullptr);
   /* Snapshots the scenes' draw tables into pinned memory; sizes the pools. */
   int stage();
   /* Enqueues the whole launch on `stream` (capturable). */

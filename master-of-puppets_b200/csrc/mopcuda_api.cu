@@ -36,6 +36,21 @@ int mc_fail(int code, const char *fmt, ...) {
 
 extern "C" const char *mopcuda_last_error(void) { return g_err; }
 
+extern "C" void *mopcuda_host_alloc(size_t bytes) {
+  void *p = nullptr;
+  if (cudaMallocHost(&p, bytes ? bytes : 1) != cudaSuccess) {
+    cudaGetLastError();
+    fail(MOPCUDA_ENOMEM, "cudaMallocHost(%zu) failed", bytes);
+    return nullptr;
+  }
+  return p;
+}
+
+extern "C" void mopcuda_host_free(void *p) {
+  if (p)
+    cudaFreeHost(p);
+}
+
 static int finish_frame(MopCudaDevice *d, int timeout_ms);
 
 /* float x86-compatible evaluation of the post-process byte map
@@ -573,6 +588,21 @@ extern "C" int mopcuda_draw(MopCudaDevice *d, MopCudaFramebuffer *fb, const MopC
   if (!d->frame_open || d->fb != fb)
     return fail(MOPCUDA_EINVAL, "draw outside frame_begin/frame_end");
   return record_draw(d, c, c->model, c->mvp);
+}
+
+extern "C" int mopcuda_draw_list(MopCudaDevice *d, MopCudaFramebuffer *fb, const MopCudaDraw *c,
+                                 uint32_t n) {
+  if (!d || !fb || (n && !c))
+    return fail(MOPCUDA_EINVAL, "draw_list: bad arguments");
+  std::lock_guard<std::mutex> lk(d->mu);
+  if (!d->frame_open || d->fb != fb)
+    return fail(MOPCUDA_EINVAL, "draw outside frame_begin/frame_end");
+  for (uint32_t i = 0; i < n; i++) {
+    int rc = record_draw(d, c + i, c[i].model, c[i].mvp);
+    if (rc)
+      return rc;
+  }
+  return MOPCUDA_OK;
 }
 
 /* mop_mat4_multiply order (math.c:182-194): running sum from 0.0f. */

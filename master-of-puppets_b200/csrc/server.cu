@@ -34,12 +34,15 @@ using Clock = std::chrono::steady_clock;
 struct SrvRequest {
   uint64_t ticket = 0;
   MopCudaRequest req;
+  std::shared_ptr<const std::vector<float>> models; /* the scene's models at submit */
   std::vector<int32_t> pick_xy;
   Clock::time_point t_submit, t_done;
   int status = 0; /* 0 queued, 1 running, 2 done, < 0 error */
   uint64_t est_bytes = 0;
   /* result staging offsets in the slot's pinned buffer */
   size_t off_color = 0, off_ids = 0, off_depth = 0, off_pick = 0;
+  /* client buffers in page-locked memory receive their DMA directly */
+  bool direct_color = false, direct_ids = false, direct_depth = false;
 };
 
 struct SrvSlot {
@@ -69,6 +72,18 @@ struct MopCudaServer {
   MopCudaServerStats st;
 };
 
+/* True for page-locked host memory (cudaHostAlloc / cudaHostRegister). */
+static bool pinned(const void *p) {
+  if (!p)
+    return false;
+  cudaPointerAttributes at;
+  if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return at.type == cudaMemoryTypeHost;
+}
+
 static double ms_between(Clock::time_point a, Clock::time_point b) {
   return std::chrono::duration<double, std::milli>(b - a).count();
 }
@@ -95,14 +110,19 @@ static int srv_enqueue(MopCudaServer *s, SrvSlot *sl) {
       if (r->req.color) {
         const void *src = v.ssaa > 1 ? (const void *)(c.presented.as<uchar4>() + v.pixel_off)
                                      : (const void *)(c.out.as<uchar4>() + v.sample_off);
-        CU_TRY(cudaMemcpyAsync(out + r->off_color, src, 4 * P, cudaMemcpyDeviceToHost, st));
+        void *dst = r->direct_color ? (void *)r->req.color : (void *)(out + r->off_color);
+        CU_TRY(cudaMemcpyAsync(dst, src, 4 * P, cudaMemcpyDeviceToHost, st));
       }
-      if (r->req.ids)
-        CU_TRY(cudaMemcpyAsync(out + r->off_ids, c.ids.as<uint32_t>() + v.sample_off, 4 * S,
+      if (r->req.ids) {
+        void *dst = r->direct_ids ? (void *)r->req.ids : (void *)(out + r->off_ids);
+        CU_TRY(cudaMemcpyAsync(dst, c.ids.as<uint32_t>() + v.sample_off, 4 * S,
                                cudaMemcpyDeviceToHost, st));
-      if (r->req.depth)
-        CU_TRY(cudaMemcpyAsync(out + r->off_depth, c.depth.as<float>() + v.sample_off, 4 * S,
+      }
+      if (r->req.depth) {
+        void *dst = r->direct_depth ? (void *)r->req.depth : (void *)(out + r->off_depth);
+        CU_TRY(cudaMemcpyAsync(dst, c.depth.as<float>() + v.sample_off, 4 * S,
                                cudaMemcpyDeviceToHost, st));
+      }
     } else if (r->req.pick_n) {
       const uint32_t n = r->req.pick_n;
       uint32_t *oid = (uint32_t *)(sl->d_pick_out.as<uint8_t>() + pick_out);
@@ -126,17 +146,24 @@ static int srv_launch(MopCudaServer *s, SrvSlot *sl) {
   LaunchCore &c = sl->core;
   const uint32_t n = (uint32_t)sl->reqs.size();
   std::vector<MopCudaScene *> sc;
+  std::vector<std::shared_ptr<const std::vector<float>>> sm;
   std::vector<uint32_t> scene_of(n);
   std::vector<uint8_t> no_color(n);
   std::vector<MopCudaView> views(n);
   size_t in_b = 0, out_b = 0;
   for (uint32_t i = 0; i < n; i++) {
     SrvRequest *r = sl->reqs[i];
+    /* one scene entry per (scene, model state): requests see their scene as
+     * it was when they were submitted */
     MopCudaScene *scene = s->scenes[r->req.scene];
-    auto it = std::find(sc.begin(), sc.end(), scene);
-    scene_of[i] = (uint32_t)(it - sc.begin());
-    if (it == sc.end())
+    uint32_t e = 0;
+    while (e < sc.size() && !(sc[e] == scene && sm[e] == r->models))
+      e++;
+    if (e == sc.size()) {
       sc.push_back(scene);
+      sm.push_back(r->models);
+    }
+    scene_of[i] = e;
     views[i] = r->req.view;
     no_color[i] = r->req.kind == MOPCUDA_REQ_PICK ? 1 : 0;
     const MopCudaView &v = r->req.view;
@@ -148,11 +175,11 @@ static int srv_launch(MopCudaServer *s, SrvSlot *sl) {
       return o;
     };
     if (r->req.kind == MOPCUDA_REQ_RENDER) {
-      if (r->req.color)
+      if (r->req.color && !r->direct_color)
         r->off_color = take(4 * P);
-      if (r->req.ids)
+      if (r->req.ids && !r->direct_ids)
         r->off_ids = take(4 * S);
-      if (r->req.depth)
+      if (r->req.depth && !r->direct_depth)
         r->off_depth = take(4 * S);
     } else {
       r->off_pick = take(12ull * r->req.pick_n);
@@ -171,7 +198,7 @@ static int srv_launch(MopCudaServer *s, SrvSlot *sl) {
       memcpy(sl->h_io.as<uint8_t>() + o, r->pick_xy.data(), 8ull * r->req.pick_n);
       o += 8ull * r->req.pick_n;
     }
-  int rc = c.set_layout(views.data(), scene_of.data(), no_color.data(), n, sc);
+  int rc = c.set_layout(views.data(), scene_of.data(), no_color.data(), n, sc, &sm);
   if (!rc)
     rc = c.stage();
   if (!rc)
@@ -189,11 +216,11 @@ static void srv_deliver(SrvSlot *sl) {
     const size_t S = (size_t)v.width * v.height;
     const size_t P = (size_t)(v.width / v.ssaa) * (v.height / v.ssaa);
     if (r->req.kind == MOPCUDA_REQ_RENDER) {
-      if (r->req.color)
+      if (r->req.color && !r->direct_color)
         memcpy(r->req.color, out + r->off_color, 4 * P);
-      if (r->req.ids)
+      if (r->req.ids && !r->direct_ids)
         memcpy(r->req.ids, out + r->off_ids, 4 * S);
-      if (r->req.depth)
+      if (r->req.depth && !r->direct_depth)
         memcpy(r->req.depth, out + r->off_depth, 4 * S);
     } else if (r->req.pick_n) {
       const uint32_t n = r->req.pick_n;
@@ -412,6 +439,9 @@ extern "C" int mopcuda_server_submit(MopCudaServer *s, const MopCudaRequest *req
     return fail(MOPCUDA_EINVAL, "server_submit: pick buffers missing");
   SrvRequest *r = new SrvRequest();
   r->req = *req;
+  r->direct_color = pinned(req->color);
+  r->direct_ids = pinned(req->ids);
+  r->direct_depth = pinned(req->depth);
   if (req->kind == MOPCUDA_REQ_PICK && req->pick_n)
     r->pick_xy.assign(req->pick_xy, req->pick_xy + 2ull * req->pick_n);
   r->t_submit = Clock::now();
@@ -425,6 +455,7 @@ extern "C" int mopcuda_server_submit(MopCudaServer *s, const MopCudaRequest *req
     const uint64_t S = (uint64_t)v.width * v.ssaa * v.height * v.ssaa;
     const uint64_t P = (uint64_t)v.width * v.height;
     r->est_bytes = mc_view_bytes(s->scenes[req->scene], S, P);
+    r->models = mc_scene_models(s->scenes[req->scene]);
     r->ticket = s->next_ticket++;
     s->reqs[r->ticket] = r;
     s->pending.push_back(r);

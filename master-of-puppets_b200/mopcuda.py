@@ -114,6 +114,7 @@ SIGNATURES = [
                                   C.c_int, C.c_float, C.c_float]),
     ("mopcuda_frame_begin", C.c_int, [_P, _P, _P]),
     ("mopcuda_draw", C.c_int, [_P, _P, C.POINTER(MopCudaDraw)]),
+    ("mopcuda_draw_list", C.c_int, [_P, _P, _P, C.c_uint32]),
     ("mopcuda_draw_instanced", C.c_int, [_P, _P, C.POINTER(MopCudaDraw), _P, _P, _P, C.c_uint32]),
     ("mopcuda_frame_end", C.c_int, [_P, _P]),
     ("mopcuda_frame_wait", C.c_int, [_P, C.c_int]),
@@ -155,6 +156,8 @@ SIGNATURES = [
     ("mopcuda_server_wait", C.c_int, [_P, C.c_uint64, C.c_int, C.POINTER(C.c_double)]),
     ("mopcuda_server_drain", C.c_int, [_P, C.c_int]),
     ("mopcuda_server_stats", C.c_int, [_P, C.POINTER(MopCudaServerStats)]),
+    ("mopcuda_host_alloc", _P, [C.c_size_t]),
+    ("mopcuda_host_free", None, [_P]),
     ("mopcuda_mat4_multiply", None, [_P, _P, _P]),
     ("mopcuda_mat4_compose_trs", None, [_P, _P, _P, _P]),
     ("mopcuda_camera_matrices", None, [_P, _P, _P, C.c_float, C.c_float, C.c_float, C.c_int,
@@ -595,6 +598,26 @@ class BatchRenderer(ResidentScene):
         super().close()
 
 
+class HostArray:
+    """A numpy array over page-locked host memory (mopcuda_host_alloc)."""
+
+    def __init__(self, shape, dtype):
+        self.L = lib()
+        n = int(np.prod(shape)) * np.dtype(dtype).itemsize
+        self.p = self.L.mopcuda_host_alloc(n)
+        if not self.p:
+            raise RuntimeError(f"host_alloc failed: {last_error()}")
+        buf = (C.c_uint8 * n).from_address(self.p)
+        self.a = np.frombuffer(buf, dtype=dtype).reshape(shape)
+        self.a.fill(0)
+
+    def close(self):
+        if self.p:
+            self.a = None
+            self.L.mopcuda_host_free(self.p)
+            self.p = None
+
+
 class Ticket:
     """An in-flight server request and the host buffers it fills."""
 
@@ -633,11 +656,14 @@ class Server:
         t.id = tid.value
         return t
 
-    def submit_render(self, scene_id: int, view, want_ids=False, want_depth=False) -> Ticket:
+    def submit_render(self, scene_id: int, view, want_ids=False, want_depth=False,
+                      out=None) -> Ticket:
+        """out: optional (h, w, 4) uint8 destination (page-locked memory
+        receives the device copy directly)."""
         r = MopCudaRequest()
         r.kind, r.scene, r.view = REQ_RENDER, scene_id, view_struct(view)
         sw, sh = view.width * view.ssaa, view.height * view.ssaa
-        color = np.empty((view.height, view.width, 4), np.uint8)
+        color = out if out is not None else np.empty((view.height, view.width, 4), np.uint8)
         ids = np.empty((sh, sw), np.uint32) if want_ids else None
         dep = np.empty((sh, sw), np.float32) if want_depth else None
         r.color = color.ctypes.data

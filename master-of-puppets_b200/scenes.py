@@ -333,6 +333,46 @@ def config2(seed: int = 2, width: int = 1920, height: int = 1080, ssaa: int = 2,
     return sc
 
 
+def served_scene(seed: int, target_tris: int, tex_size: int = 1024, n_textures: int = 4,
+                 width: int = 1280, height: int = 720) -> Scene:
+    """A config-2-style scene of about target_tris triangles: the config-2
+    lights, textures and materials over instances drawn 80% subdiv-4
+    icospheres, 10% tori 64x128, 8% subdiv-5 and 2% subdiv-6 icospheres,
+    added until the triangle count reaches the target."""
+    rng = np.random.default_rng(seed)
+    base = config2(seed=seed, width=width, height=height, ssaa=1, instances=0,
+                   tex_size=tex_size, n_textures=n_textures)
+    proto = {}
+    tris = 0
+    n = 0
+    while tris < target_tris:
+        u = rng.random()
+        k = "s4" if u < 0.8 else ("torus" if u < 0.9 else ("s5" if u < 0.98 else "s6"))
+        if k not in proto:
+            proto[k] = torus(64, 128, 1.0, 0.35, (1, 1, 1, 1)) if k == "torus" else \
+                icosphere(int(k[1]), 1.0, (1, 1, 1, 1))
+        v, i = proto[k]
+        v = v.copy()
+        v[:, 6:10] = _color(rng)
+        metallic, rough = _mat_rand(rng)
+        t = rng.uniform(-20, 20, 3)
+        sc = float(math.exp(rng.uniform(math.log(0.2), math.log(3.0))))
+        m = mat_trs(t, random_rotation(rng), (sc, sc, sc))
+        base.meshes.append(Mesh(v, i, n + 1, m, metallic, rough,
+                                texture=int(rng.integers(0, n_textures))))
+        tris += i.size // 3
+        n += 1
+    base.name = f"served{seed}"
+    return base
+
+
+def served_triangle_counts(n: int = 32, seed: int = 5, lo: int = 50_000, hi: int = 2_000_000):
+    """Log-normal scene sizes clipped to [lo, hi] (median ~300k)."""
+    rng = np.random.default_rng(seed)
+    return [int(min(max(math.exp(rng.normal(math.log(300_000), 0.9)), lo), hi))
+            for _ in range(n)]
+
+
 def small_scene(seed: int = 7, width: int = 160, height: int = 120, ssaa: int = 1,
                 n_meshes: int = 6, lights: str = "mixed", textured: bool = True,
                 env: int = 0) -> Scene:
