@@ -28,6 +28,7 @@ int mc_fail(int code, const char *fmt, ...);
 /* ------------------------------------------------------------------------
  * objects
  * ------------------------------------------------------------------------ */
+/* Grow-only device buffer. */
 struct DevArena {
   void *p = nullptr;
   size_t cap = 0;
@@ -35,12 +36,10 @@ struct DevArena {
     if (bytes <= cap)
       return 0;
     size_t n = bytes + bytes / 2 + 4096;
-    if (p)
-      cudaFree(p);
-    p = nullptr;
-    cap = 0;
+    release();
     if (cudaMalloc(&p, n) != cudaSuccess) {
       cudaGetLastError();
+      p = nullptr;
       return fail(MOPCUDA_ENOMEM, "cudaMalloc(%zu) failed", n);
     }
     cap = n;

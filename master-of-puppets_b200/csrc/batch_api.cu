@@ -223,8 +223,8 @@ std::shared_ptr<const std::vector<float>> mc_scene_models(MopCudaScene *s) {
   return s->models;
 }
 
-static void pool_need(uint64_t T, uint64_t V, uint32_t fan_num, uint32_t large_num,
-                      unsigned long long need[4]) {
+void mc_pool_need(uint64_t T, uint64_t V, uint32_t fan_num, uint32_t large_num,
+                  unsigned long long need[4]) {
   const unsigned long long fan = T * fan_num / 8ull + 1024ull;
   need[0] = V + fan;
   need[1] = T + fan;
@@ -234,7 +234,7 @@ static void pool_need(uint64_t T, uint64_t V, uint32_t fan_num, uint32_t large_n
 
 uint64_t mc_view_bytes(const MopCudaScene *s, uint64_t samples, uint64_t pixels) {
   unsigned long long need[4];
-  pool_need(s->tris, s->verts, 1, 1, need);
+  mc_pool_need(s->tris, s->verts, 1, 1, need);
   const uint64_t pools = 64ull * need[0] + (sizeof(RasterRec) + sizeof(ShadeRec)) * need[1] +
                          4ull * need[2] + 8ull * need[3];
   return 28ull * samples + 4ull * pixels + pools / 2 + sizeof(DrawRec) * s->draws.size();
@@ -498,12 +498,12 @@ int LaunchCore::stage() {
   for (uint32_t i = 0; i < nv; i++) {
     const MopCudaScene *s = scenes[vrec[i].scene];
     unsigned long long need[4];
-    pool_need(s->tris, s->verts, fan_num, large_num, need);
+    mc_pool_need(s->tris, s->verts, fan_num, large_num, need);
     for (int k = 0; k < 4; k++)
       want[k] += need[k];
   }
   for (int k = 0; k < 4; k++)
-    want[k] = want[k] / 2 + 4096;
+    want[k] = std::max(want[k] / 2 + 4096, pool_floor[k]);
   if (vertex_pool < want[0] || rec_pool < want[1] || clip_pool < want[2] ||
       large_pool < want[3])
     return size_pools(this, std::max(want[0], vertex_pool), std::max(want[1], rec_pool),

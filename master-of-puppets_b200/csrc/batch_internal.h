@@ -67,6 +67,9 @@ struct LaunchCore {
   DevArena clip, world, normal, color, rrec, srec, clipq, large_list, large_items;
   unsigned long long vertex_pool = 0, rec_pool = 0, clip_pool = 0, large_pool = 0;
   uint32_t fan_num = 1, large_num = 1;
+  /* pool sizes below which stage() does not go (a server sizes its slots
+   * once for its largest launch, so they do not reallocate while serving) */
+  unsigned long long pool_floor[4] = {0, 0, 0, 0};
   /* sample / pixel buffers */
   DevArena keys, shade_list, pre, out, depth, ids, presented;
   /* launch shape */
@@ -97,5 +100,9 @@ struct LaunchCore {
 
 static inline bool mc_block_ok(int n) { return n >= 32 && n <= 256 && n % 32 == 0; }
 int mc_check_view(const MopCudaView &v);
+/* Work-pool entries one viewport of a scene of T triangles and V vertices
+ * may need: vertices, records, clip queue, large list. */
+void mc_pool_need(uint64_t T, uint64_t V, uint32_t fan_num, uint32_t large_num,
+                  unsigned long long need[4]);
 
 #endif

@@ -422,6 +422,14 @@ extern "C" int mopcuda_server_add_scene(MopCudaServer *s, MopCudaScene *scene) {
     return rc;
   std::lock_guard<std::mutex> lk(s->mu);
   s->scenes.push_back(scene);
+  /* slot pools: half the worst case of a full launch of the largest scene,
+   * so serving does not stop to reallocate them */
+  unsigned long long need[4];
+  mc_pool_need(scene->tris, scene->verts, 1, 1, need);
+  for (SrvSlot *sl : s->slots)
+    for (int k = 0; k < 4; k++)
+      sl->core.pool_floor[k] =
+          std::max(sl->core.pool_floor[k], need[k] * s->cfg.max_views / 2 + 4096ull);
   return (int)(s->scenes.size() - 1);
 }
 

@@ -128,55 +128,63 @@ class _Ring:
 
 def run_server(dev, rss, trace: List[Request], hbm_budget: int, max_views: int = 64,
                max_inflight: int = 3, batch_window_us: int = 0, keep_every: int = 0,
-               ring: int = 64) -> dict:
-    """Serve the trace.  Render results land in rings of page-locked buffers
-    per resolution (reused once their request completed); keep_every > 0
-    also keeps every k-th render's IDs and depth (for the exactness check)
-    under "kept"."""
+               ring: int = 64, warmup: Optional[List[Request]] = None) -> dict:
+    """Serve the trace (after serving `warmup`, untimed, on the same server).
+    Render results land in rings of page-locked buffers per resolution
+    (reused once their request completed); keep_every > 0 also keeps every
+    k-th render's IDs and depth (for the exactness check) under "kept"."""
     srv = mopcuda.Server(dev, hbm_budget, max_views, max_inflight, batch_window_us)
     rings = {(w, h): _Ring((h, w, 4), ring) for w, h in RESOLUTIONS}
     try:
         ids = [srv.add_scene(rs) for rs in rss]
-        tickets = [None] * len(trace)
-        slots = [None] * len(trace)
-        done = threading.Event()
-        lat = [0.0] * len(trace)
 
-        def collector():
-            for i in range(len(trace)):
-                while tickets[i] is None:
-                    time.sleep(0.0001)
-                lat[i] = srv.wait(tickets[i], 60000)
-                if slots[i] is not None:
-                    rg, k = slots[i]
-                    rg.free[k].set()
-            done.set()
+        def serve(tr, keep_every):
+            tickets = [None] * len(tr)
+            slots = [None] * len(tr)
+            lat = [0.0] * len(tr)
 
-        th = threading.Thread(target=collector, daemon=True)
-        t0 = time.perf_counter()
-        th.start()
-        for i, r in enumerate(trace):
-            _sleep_until(t0 + r.t)
-            for k, m in r.moves:
-                rss[r.scene].set_model(k, m)
-            keep = keep_every and i % keep_every == 0 and r.kind == mopcuda.REQ_RENDER
-            if r.kind == mopcuda.REQ_RENDER:
-                out = None
-                if not keep:
-                    rg = rings[(r.view.width, r.view.height)]
-                    k, out = rg.take()
-                    slots[i] = (rg, k)
-                tickets[i] = srv.submit_render(ids[r.scene], r.view, want_ids=bool(keep),
-                                               want_depth=bool(keep), out=out)
-            else:
-                tickets[i] = srv.submit_pick(ids[r.scene], r.view, r.xy)
-        done.wait()
-        wall = time.perf_counter() - t0
-        th.join()
+            def collector():
+                for i in range(len(tr)):
+                    while tickets[i] is None:
+                        time.sleep(0.0001)
+                    lat[i] = srv.wait(tickets[i], 60000)
+                    if slots[i] is not None:
+                        rg, k = slots[i]
+                        rg.free[k].set()
+
+            th = threading.Thread(target=collector, daemon=True)
+            t0 = time.perf_counter()
+            th.start()
+            for i, r in enumerate(tr):
+                _sleep_until(t0 + r.t)
+                for k, m in r.moves:
+                    rss[r.scene].set_model(k, m)
+                keep = keep_every and i % keep_every == 0 and r.kind == mopcuda.REQ_RENDER
+                if r.kind == mopcuda.REQ_RENDER:
+                    out = None
+                    if not keep:
+                        rg = rings[(r.view.width, r.view.height)]
+                        k, out = rg.take()
+                        slots[i] = (rg, k)
+                    tickets[i] = srv.submit_render(ids[r.scene], r.view, want_ids=bool(keep),
+                                                   want_depth=bool(keep), out=out)
+                else:
+                    tickets[i] = srv.submit_pick(ids[r.scene], r.view, r.xy)
+            th.join()
+            wall = time.perf_counter() - t0
+            kept = {i: tickets[i] for i in range(len(tr))
+                    if keep_every and i % keep_every == 0 and tr[i].kind == mopcuda.REQ_RENDER}
+            return lat, wall, kept
+
+        if warmup:
+            serve(warmup, 0)
+        s0 = srv.stats()
+        lat, wall, kept = serve(trace, keep_every)
+        st = srv.stats()
+        for k in ("submitted", "completed", "failed", "launches", "launched_views", "reruns"):
+            st[k] -= s0[k]
         pixels = sum(r.pixels for r in trace)
-        kept = {i: tickets[i] for i in range(len(trace))
-                if keep_every and i % keep_every == 0 and trace[i].kind == mopcuda.REQ_RENDER}
-        return _summary(lat, pixels, wall, {"stats": srv.stats(), "kept": kept})
+        return _summary(lat, pixels, wall, {"stats": st, "kept": kept})
     finally:
         srv.close()
         for rg in rings.values():
@@ -263,7 +271,7 @@ def check_kept(dev, rss, trace: List[Request], kept: dict) -> dict:
             "id_mismatches": bad_ids, "depth_mismatches": bad_depth}
 
 
-def run_plain(dev, rss, trace: List[Request]) -> dict:
+def run_plain(dev, rss, trace: List[Request], warmup: Optional[List[Request]] = None) -> dict:
     L, d = dev.L, dev.h
     plains = [PlainScene(rs) for rs in rss]
     fbs = {}
@@ -274,6 +282,10 @@ def run_plain(dev, rss, trace: List[Request]) -> dict:
     outs = {k: np.zeros((k[1], k[0], 4), np.uint8) for k in fbs}
     lat = []
     try:
+        for r in warmup or []:  # untimed: first-use allocations of every frame size
+            ps = plains[r.scene]
+            ps.set_camera(r.view)
+            ps.frame(dev, fbs[(r.view.width, r.view.height)], r.view)
         t0 = time.perf_counter()
         for r in trace:
             _sleep_until(t0 + r.t)
