@@ -48,6 +48,10 @@ def parse():
     ap.add_argument("--config", choices=["config2", "config1"], default="config2")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--flush-mb", type=int, default=256)
+    ap.add_argument("--no-forms", action="store_true",
+                    help="skip the batched (64 viewports) and served (32 scenes) forms")
+    ap.add_argument("--forms-only", action="store_true",
+                    help="run only the batched and served forms (one JSON line)")
     return ap.parse_args()
 
 
@@ -333,6 +337,8 @@ def run_cuda(args):
             line["cpu_baseline"] = {"value": None, "unit": "Mpix/s", "error": str(e)[:200]}
     r.close()
     dev.close()
+    if rank == 0 and world == 1 and not args.no_forms:
+        line.update(forms_subprocess())
     if rank == 0:
         emit(line)
     if dist is not None:
@@ -340,8 +346,146 @@ def run_cuda(args):
     return 0
 
 
+def run_batched(dev, steps=10, warm=3, n_views=64):
+    """64 viewports of uneven size, camera and SSAA over the large static
+    scene in one CUDA-graph launch, against the plain per-viewport frames of
+    the same viewports (both read every presented image back to host)."""
+    import ctypes as C
+    import numpy as np
+    import mopcuda
+    import scenes
+    import serving
+    sc = scenes.config2()
+    ibl = scenes.procedural_ibl(sc.sun_dir)
+    views = scenes.batch_views(sc, n=n_views, seed=4)
+    pixels = sum(v.pixels for v in views)
+    b = mopcuda.BatchRenderer(dev, sc, views, ibl)
+    outs = [mopcuda.HostArray((v.height, v.width, 4), np.uint8) for v in views]
+    try:
+        for _ in range(warm):
+            b.render()
+        gms, t0 = [], time.perf_counter()
+        for _ in range(steps):
+            b.render()
+            gms.append(b.gpu_ms)
+            for i, o in enumerate(outs):
+                b.read(i, mopcuda.BATCH_PRESENTED, o.a)
+        wall_b = (time.perf_counter() - t0) / steps
+        cfg = b.config()
+        # plain: one frame per viewport through the per-viewport C ABI
+        L, d = dev.L, dev.h
+        ps = serving.PlainScene(b)
+        fbs = []
+        for v in views:
+            fb = L.mopcuda_framebuffer_create(d, v.width * v.ssaa, v.height * v.ssaa)
+            L.mopcuda_framebuffer_set_ssaa(fb, v.ssaa)
+            fbs.append(fb)
+
+        def plain_pass():
+            g = 0.0
+            for v, fb, o in zip(views, fbs, outs):
+                ps.set_camera(v)
+                ps.frame(dev, fb, v)
+                g += L.mopcuda_frame_gpu_time_ms(d)
+                L.mopcuda_read_color_resolved(d, fb, v.ssaa, C.c_void_p(o.p), o.a.nbytes)
+            return g
+        plain_pass()
+        t0 = time.perf_counter()
+        g_plain = sum(plain_pass() for _ in range(2)) / 2
+        wall_p = (time.perf_counter() - t0) / 2
+        for fb in fbs:
+            L.mopcuda_framebuffer_destroy(d, fb)
+    finally:
+        for o in outs:
+            o.close()
+        b.close()
+    gmed = float(np.median(gms))
+    return {"workload": f"{n_views} viewports (log-uniform 128^2..1920x1080, aspect 0.5-2, "
+                        "ssaa 1|2, cameras r=15-40) over the 1,470,464-tri scene, one CUDA graph",
+            "pixels": pixels, "samples": sum(v.samples for v in views),
+            "batch_ms": round(wall_b * 1e3, 3), "batch_gpu_ms": round(gmed, 3),
+            "batch_mpix_s": round(pixels / (wall_b * 1e6), 1),
+            "plain_ms": round(wall_p * 1e3, 3), "plain_gpu_ms": round(g_plain, 3),
+            "plain_mpix_s": round(pixels / (wall_p * 1e6), 1),
+            "speedup_vs_plain": round(wall_p / wall_b, 2), "launch_config": cfg,
+            "note": "wall time per pass including every presented image read to host"}
+
+
+def run_served(dev, rates=(2000.0, 4000.0), duration=2.0, n_scenes=32):
+    """Served mix: resident scenes of log-normal size, Poisson render/pick
+    requests; p50/p99 arrival-to-result latency and Mpix/s of the
+    continuous-batching server and of the plain per-viewport path on the
+    same trace; IDs/depth of a 1% sample checked bit-exact against the
+    request's own frame."""
+    import mopcuda
+    import scenes
+    import serving
+    counts = scenes.served_triangle_counts(n_scenes)
+    scs = [scenes.served_scene(100 + i, c, tex_size=256) for i, c in enumerate(counts)]
+    ibl = scenes.procedural_ibl(scs[0].sun_dir)
+    rss = [mopcuda.ResidentScene(dev, sc, ibl) for sc in scs]
+    out = {"workload": f"{n_scenes} resident scenes ({sum(counts):,} tris, 50k-2M log-normal), "
+                       "Poisson arrivals, 85% renders at 256^2/720p/1080p/1440p, 15% pick "
+                       "batches of 1-64, 1% of a scene's instances moved per request",
+           "server_config": {"max_views": 32, "max_inflight": 3, "hbm_budget_gib": 100},
+           "rates": []}
+    try:
+        for rate in rates:
+            warm = serving.make_trace(scs, rate, 0.5, seed=7 + int(rate))
+            for r in warm:
+                r.moves = []
+            trace = serving.make_trace(scs, rate, duration, seed=int(rate))
+            serving.reset_models(rss, scs)
+            s = serving.run_server(dev, rss, trace, hbm_budget=100 << 30, max_views=32,
+                                   max_inflight=3, keep_every=100, warmup=warm)
+            chk = serving.check_kept(dev, rss, trace, s.pop("kept"))
+            p = serving.run_plain(dev, rss, trace, warmup=warm[:40])
+            st = s.pop("stats")
+            out["rates"].append({
+                "req_per_s": rate, "requests": s["requests"],
+                "server": {k: round(s[k], 3) for k in ("p50_ms", "p99_ms", "mpix_s")},
+                "plain": {k: round(p[k], 3) for k in ("p50_ms", "p99_ms", "mpix_s")},
+                "server_launches": st["launches"], "max_views_in_launch": st["max_views_in_launch"],
+                "exact_check": chk})
+    finally:
+        for rs in rss:
+            rs.close()
+    return out
+
+
+def forms_subprocess(timeout_s=900):
+    """The batched and served forms in a fresh process on the same GPU, so
+    their device and host state starts clean."""
+    try:
+        p = subprocess.run([sys.executable, str(Path(__file__).resolve()), "--forms-only"],
+                           capture_output=True, text=True, timeout=timeout_s)
+        for ln in reversed(p.stdout.strip().splitlines()):
+            if ln.startswith("{"):
+                return json.loads(ln)
+        return {"batched": {"error": (p.stderr or "no output")[-300:]}}
+    except Exception as e:
+        return {"batched": {"error": str(e)[:300]}}
+
+
+def run_forms():
+    import mopcuda
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dev = mopcuda.Device(local)
+    out = {}
+    for key, fn in (("batched", run_batched), ("served", run_served)):
+        try:
+            out[key] = fn(dev)
+        except Exception as e:  # report, do not lose the other form
+            out[key] = {"error": str(e)[:300]}
+    dev.close()
+    emit(out)
+    return 0
+
+
 def main():
     args = parse()
+    if args.forms_only:
+        return run_forms()
     if args.impl == "reference":
         return run_reference(args)
     return run_cuda(args)

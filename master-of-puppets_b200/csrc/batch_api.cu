@@ -376,13 +376,14 @@ int LaunchCore::set_layout(const MopCudaView *views, const uint32_t *scene_of,
   total_pixels = po;
   view_draw_total = dro;
   int rc = 0;
-  rc |= keys.ensure(8ull * so);
-  rc |= shade_list.ensure(4ull * so);
-  rc |= pre.ensure(4ull * so);
-  rc |= out.ensure(4ull * so);
-  rc |= depth.ensure(4ull * so);
-  rc |= ids.ensure(4ull * so);
-  rc |= presented.ensure(4ull * po + 16);
+  const unsigned long long sa = std::max(so, sample_floor), pa = std::max(po, pixel_floor);
+  rc |= keys.ensure(8ull * sa);
+  rc |= shade_list.ensure(4ull * sa);
+  rc |= pre.ensure(4ull * sa);
+  rc |= out.ensure(4ull * sa);
+  rc |= depth.ensure(4ull * sa);
+  rc |= ids.ensure(4ull * sa);
+  rc |= presented.ensure(4ull * pa + 16);
   rc |= d_views.ensure(sizeof(ViewRec) * n);
   rc |= h_views.ensure(sizeof(ViewRec) * n);
   rc |= d_frames.ensure(sizeof(FrameArgs) * n);

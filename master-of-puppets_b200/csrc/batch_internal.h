@@ -70,6 +70,8 @@ struct LaunchCore {
   /* pool sizes below which stage() does not go (a server sizes its slots
    * once for its largest launch, so they do not reallocate while serving) */
   unsigned long long pool_floor[4] = {0, 0, 0, 0};
+  /* likewise for the sample- and pixel-resolution buffers */
+  unsigned long long sample_floor = 0, pixel_floor = 0;
   /* sample / pixel buffers */
   DevArena keys, shade_list, pre, out, depth, ids, presented;
   /* launch shape */

@@ -69,6 +69,7 @@ struct MopCudaServer {
   bool stop = false;
   uint64_t next_ticket = 1;
   uint64_t inflight_bytes = 0;
+  uint64_t max_view_samples = 0, max_view_pixels = 0; /* largest request so far */
   MopCudaServerStats st;
 };
 
@@ -318,6 +319,10 @@ static void srv_loop(MopCudaServer *s) {
         break;
       for (SrvRequest *r : group)
         r->status = 1;
+      /* size the slot's buffers for a full launch of the largest request
+       * seen, so later launches do not stop to reallocate */
+      sl->core.sample_floor = s->max_view_samples * s->cfg.max_views;
+      sl->core.pixel_floor = s->max_view_pixels * s->cfg.max_views;
       sl->reqs = group;
       sl->busy = true;
       sl->attempt = 0;
@@ -463,6 +468,8 @@ extern "C" int mopcuda_server_submit(MopCudaServer *s, const MopCudaRequest *req
     const uint64_t S = (uint64_t)v.width * v.ssaa * v.height * v.ssaa;
     const uint64_t P = (uint64_t)v.width * v.height;
     r->est_bytes = mc_view_bytes(s->scenes[req->scene], S, P);
+    s->max_view_samples = std::max<uint64_t>(s->max_view_samples, (S + 15) & ~(uint64_t)15);
+    s->max_view_pixels = std::max<uint64_t>(s->max_view_pixels, (P + 15) & ~(uint64_t)15);
     r->models = mc_scene_models(s->scenes[req->scene]);
     r->ticket = s->next_ticket++;
     s->reqs[r->ticket] = r;
