@@ -52,6 +52,8 @@ def parse():
                     help="skip the batched (64 viewports) and served (32 scenes) forms")
     ap.add_argument("--forms-only", action="store_true",
                     help="run only the batched and served forms (one JSON line)")
+    ap.add_argument("--form", choices=["both", "batched", "served"], default="both",
+                    help="with --forms-only: which form to run")
     return ap.parse_args()
 
 
@@ -134,6 +136,17 @@ class ClockSampler:
         s = sorted(self.samples)
         return {"sm_mhz": s[len(s) // 2] if s else None, "sm_max_mhz": self.max_mhz,
                 "reasons": sorted(self.reasons), "samples": len(s)}
+
+
+def pair_traffic():
+    """DRAM bytes (read + write) of one k_resolve + k_shade frame from the
+    committed ncu capture summary, or None."""
+    try:
+        t = json.loads((ROOT / "profiles" / "traffic_config2.json").read_text())["per_launch"]
+        mb = sum(t[k]["dram_read_mb"] + t[k]["dram_write_mb"] for k in ("k_resolve", "k_shade"))
+        return round(mb * 1e6)
+    except Exception:
+        return None
 
 
 def dist_setup(args):
@@ -315,7 +328,7 @@ def run_cuda(args):
             "roofline": {"bound": "hbm", "kernel": "k_resolve + k_shade (deferred shading + ACES)",
                          "achieved": round(achieved, 1), "peak": hbm_peak,
                          "unit": "GB/s", "frac": round(achieved / hbm_peak, 4),
-                         "peak_source": peak_kind, "traffic": None,
+                         "peak_source": peak_kind, "traffic": pair_traffic(),
                          "alu": {"achieved": round(alu_achieved, 1), "peak": round(fp32_peak, 1),
                                  "unit": "Gop/s (fp32 add/mul, no FMA)",
                                  "frac": round(alu_achieved / fp32_peak, 4) if fp32_peak else None,
@@ -467,12 +480,14 @@ def forms_subprocess(timeout_s=900):
         return {"batched": {"error": str(e)[:300]}}
 
 
-def run_forms():
+def run_forms(which="both"):
     import mopcuda
     local = int(os.environ.get("LOCAL_RANK", "0"))
     dev = mopcuda.Device(local)
     out = {}
     for key, fn in (("batched", run_batched), ("served", run_served)):
+        if which not in ("both", key):
+            continue
         try:
             out[key] = fn(dev)
         except Exception as e:  # report, do not lose the other form
@@ -485,7 +500,7 @@ def run_forms():
 def main():
     args = parse()
     if args.forms_only:
-        return run_forms()
+        return run_forms(args.form)
     if args.impl == "reference":
         return run_reference(args)
     return run_cuda(args)

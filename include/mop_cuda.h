@@ -11,13 +11,14 @@
  * master-of-puppets_b200/host/mop_rhi_cuda.c on top of these calls.
  *
  * Execution model.  Draws are recorded on the host between frame_begin and
- * frame_end; frame_end (or the first readback that needs the frame) runs the
- * whole frame on the device as a fixed sequence of kernels: vertex
- * transform, triangle setup + clipping, screen-tile binning, per-tile
- * visibility (64-bit atomicMin on depth|submission order) fused with deferred
- * shading and the ACES resolve, then FXAA + gamma + SSAA box.  Results are
- * order-independent and deterministic; object IDs and depth are bit-exact to
- * the reference CPU backend.
+ * frame_end; frame_end runs the whole frame on the device as a fixed
+ * sequence of kernels: vertex transform, triangle setup + clipping,
+ * rasterisation of every triangle record into a per-sample visibility key
+ * (64-bit atomicMin on depth|submission order), resolve of the background and
+ * compaction of covered samples, deferred shading with the ACES resolve, then
+ * FXAA + gamma + SSAA box.  Results are order-independent and deterministic;
+ * object IDs and depth are bit-exact to the reference CPU backend.  Batches
+ * and the server (further down) run the same kernels over many viewports.
  *
  * Errors: create calls return NULL; int-returning calls return MOPCUDA_OK
  * (0) or a negative MOPCUDA_E* code; mopcuda_last_error() gives text.
