@@ -737,7 +737,9 @@ __device__ __forceinline__ void setup_item(const FrameArgs &a, uint32_t t) {
   }
 }
 
-__global__ void __launch_bounds__(256) k_setup(FrameArgs a) {
+/* 5 blocks of 256 per SM (48 registers): the setup waits on vertex gathers
+ * and more resident warps hide them. */
+__global__ void __launch_bounds__(256, 5) k_setup(FrameArgs a) {
   const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t < a.total_tris)
     setup_item(a, t);
@@ -786,6 +788,13 @@ __device__ __forceinline__ void clip_item(const FrameArgs &a, uint32_t qi) {
     CV *src = buf0, *dst = buf1;
     int cnt = 3;
     for (int pl = 0; pl < 6 && cnt > 0; pl++) {
+      /* a plane every vertex is inside of returns the polygon unchanged (same
+       * vertices, same order): skip its copy */
+      bool all_in = true;
+      for (int i = 0; i < cnt; i++)
+        all_in &= plane_dist(pl, src[i].p) >= 0.0f;
+      if (all_in)
+        continue;
       int m = 0;
       CV prev = src[cnt - 1];
       float dp = plane_dist(pl, prev.p);
@@ -923,33 +932,69 @@ __global__ void k_raster_small(FrameArgs a) {
     raster_small_item(a, rid);
 }
 
-/* Exclusive scan of the large records' item counts (one block). */
-/* Exclusive scan of the large records' item counts by one block of 1024. */
+/* Exclusive scan of the large records' item counts by one block of 1024:
+ * tiles of 4096 counts (4 consecutive per thread), warp-shuffle scans, the
+ * next tile's counts loaded before the current one is scanned; part holds
+ * >= 32 words. */
+#define LARGE_SCAN_PER 4
 __device__ __forceinline__ void large_scan_block(const FrameArgs &a, uint32_t *part) {
   uint32_t n = a.ctr->large_count;
   if (n > a.large_cap)
     n = a.large_cap;
-  uint32_t per = (n + 1023u) / 1024u;
-  uint32_t b = threadIdx.x * per, e = min(b + per, n);
-  uint32_t s = 0;
-  for (uint32_t i = b; i < e; i++)
-    s += a.large_items[i];
-  part[threadIdx.x] = s;
-  __syncthreads();
-  for (int o = 1; o < 1024; o <<= 1) {
-    uint32_t v = threadIdx.x >= (unsigned)o ? part[threadIdx.x - o] : 0u;
-    __syncthreads();
-    part[threadIdx.x] += v;
-    __syncthreads();
+  const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
+  const uint32_t tile = 1024u * LARGE_SCAN_PER;
+  uint32_t nxt[LARGE_SCAN_PER];
+#pragma unroll
+  for (int k = 0; k < LARGE_SCAN_PER; k++) {
+    const uint32_t i = tid * LARGE_SCAN_PER + (uint32_t)k;
+    nxt[k] = i < n ? a.large_items[i] : 0u;
   }
-  uint32_t run = threadIdx.x ? part[threadIdx.x - 1] : 0u;
-  for (uint32_t i = b; i < e; i++) {
-    uint32_t c = a.large_items[i];
-    a.large_items[i] = run;
-    run += c;
+  uint32_t carry = 0;
+  for (uint32_t base = 0; base < n; base += tile) {
+    uint32_t v[LARGE_SCAN_PER];
+    uint32_t sum = 0;
+#pragma unroll
+    for (int k = 0; k < LARGE_SCAN_PER; k++) {
+      v[k] = nxt[k];
+      sum += v[k];
+      const uint32_t j = base + tile + tid * LARGE_SCAN_PER + (uint32_t)k;
+      nxt[k] = j < n ? a.large_items[j] : 0u;
+    }
+    uint32_t x = sum; /* inclusive scan of the per-thread sums within the warp */
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= (uint32_t)o)
+        x += y;
+    }
+    if (lane == 31u)
+      part[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+      uint32_t w = part[lane];
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, w, o);
+        if (lane >= (uint32_t)o)
+          w += y;
+      }
+      part[lane] = w;
+    }
+    __syncthreads();
+    uint32_t run = carry + (warp ? part[warp - 1] : 0u) + x - sum;
+    const uint32_t total = part[31];
+#pragma unroll
+    for (int k = 0; k < LARGE_SCAN_PER; k++) {
+      const uint32_t i = base + tid * LARGE_SCAN_PER + (uint32_t)k;
+      if (i < n)
+        a.large_items[i] = run;
+      run += v[k];
+    }
+    carry += total;
+    __syncthreads(); /* part is reused by the next tile */
   }
-  if (threadIdx.x == 1023)
-    a.ctr->large_items = part[1023];
+  if (tid == 0)
+    a.ctr->large_items = carry;
 }
 
 __global__ void __launch_bounds__(1024) k_large_scan(FrameArgs a) {

@@ -447,6 +447,150 @@ def coplanar_scene(seed: int = 3, width: int = 192, height: int = 144) -> Scene:
     return sc
 
 
+def skin_vertices(verts: np.ndarray, joints: np.ndarray, weights: np.ndarray,
+                  mats: np.ndarray) -> np.ndarray:
+    """Linear blend skinning on the host, as the core does before
+    buffer_update (mop_skin_apply, reference viewport.c:1572-1680): position
+    = sum over the 4 influences of w * (M_j * p); normal = sum of w * (M_j's
+    3x3 * n), then normalised.  verts [V, 12] float32, joints [V, 4] int,
+    weights [V, 4] float32 (sum 1), mats [J, 16] column-major float32."""
+    out = verts.copy()
+    p = verts[:, 0:3].astype(np.float32)
+    n = verts[:, 3:6].astype(np.float32)
+    pos = np.zeros_like(p)
+    nrm = np.zeros_like(n)
+    for b in range(4):
+        m = mats[joints[:, b]].reshape(-1, 4, 4).transpose(0, 2, 1)  # row-major per vertex
+        w = weights[:, b:b + 1].astype(np.float32)
+        tp = np.einsum("vij,vj->vi", m[:, :3, :3], p) + m[:, :3, 3]
+        tn = np.einsum("vij,vj->vi", m[:, :3, :3], n)
+        pos += w * tp.astype(np.float32)
+        nrm += w * tn.astype(np.float32)
+    ln = np.linalg.norm(nrm, axis=1, keepdims=True)
+    nrm = np.where(ln > 1e-8, nrm / np.maximum(ln, 1e-30), nrm)
+    out[:, 0:3] = pos
+    out[:, 3:6] = nrm
+    return out
+
+
+def config3(seed: int = 3, width: int = 1920, height: int = 1080, n_tris: int = 2_000_000,
+            tris_per_mesh: int = 2000) -> Scene:
+    """Clipping and depth stress: n_tris triangles with screen-space edge
+    length log-uniform 0.1-8 px; 10 % straddle the near plane, 5 % lie
+    outside the frustum, 20 % come in coplanar pairs (the same triangle in two
+    meshes with different object IDs, so draw order decides the tie); 5 % are
+    joint-skinned tubes (4 influences, 64 joints, weights normalised to 1,
+    skinned on the host).  Camera at (0, 0, 10) looking at the origin."""
+    rng = np.random.default_rng(seed)
+    fov, near, far = 50.0, 0.5, 100.0
+    sc = Scene("config3", width, height, 1, eye=(0.0, 0.0, 10.0), target=(0.0, 0.0, 0.0),
+               fov_deg=fov, near=near, far=far)
+    sc.lights.append(Light(LIGHT_DIRECTIONAL, direction=(-0.3, -0.6, -1.0), intensity=2.5))
+    sc.lights.append(Light(LIGHT_POINT, position=(2.0, 3.0, 6.0), intensity=40.0))
+    t = math.tan(math.radians(fov) * 0.5)
+    aspect = width / height
+    eye = np.array([0.0, 0.0, 10.0])
+
+    def place(ndc_x, ndc_y, depth):
+        return eye + depth[:, None] * np.stack([ndc_x * t * aspect, ndc_y * t,
+                                                -np.ones_like(depth)], 1)
+
+    def tris(n, kind):
+        if kind == "straddle":
+            d = np.full(n, near)
+            x, y = rng.uniform(-0.95, 0.95, n), rng.uniform(-0.95, 0.95, n)
+        elif kind == "outside":
+            d = np.exp(rng.uniform(math.log(2.0), math.log(60.0), n))
+            x = rng.choice([-1, 1], n) * rng.uniform(1.3, 3.0, n)
+            y = rng.uniform(-2.0, 2.0, n)
+        else:
+            d = np.exp(rng.uniform(math.log(1.0), math.log(80.0), n))
+            x, y = rng.uniform(-1.05, 1.05, n), rng.uniform(-1.05, 1.05, n)
+        c = place(x, y, d)
+        px = np.exp(rng.uniform(math.log(0.1), math.log(8.0), n))
+        size = px * 2.0 * d * t / height
+        a = rng.normal(size=(n, 3))
+        a /= np.linalg.norm(a, axis=1, keepdims=True)
+        b = rng.normal(size=(n, 3))
+        b -= (b * a).sum(1, keepdims=True) * a
+        b /= np.linalg.norm(b, axis=1, keepdims=True)
+        ang = rng.uniform(0, 2 * math.pi, (n, 3)) + np.array([0, 2.1, 4.2])
+        v = c[:, None, :] + size[:, None, None] * (np.cos(ang)[..., None] * a[:, None, :]
+                                                   + np.sin(ang)[..., None] * b[:, None, :])
+        if kind == "straddle":  # one vertex in front of, one behind the near plane
+            v[:, 0, 2] = eye[2] - (near - 0.6 * size)
+            v[:, 1, 2] = eye[2] - (near + 0.6 * size)
+        nrm = np.cross(v[:, 1] - v[:, 0], v[:, 2] - v[:, 0])
+        nrm /= np.maximum(np.linalg.norm(nrm, axis=1, keepdims=True), 1e-20)
+        return v.astype(np.float32), nrm.astype(np.float32)
+
+    def add_mesh(v, nrm, oid):
+        nt = v.shape[0]
+        pos = v.reshape(-1, 3)
+        nn = np.repeat(nrm, 3, axis=0)
+        col = np.repeat(rng.uniform(0.2, 1.0, (nt, 4)).astype(np.float32), 3, axis=0)
+        col[:, 3] = 1.0
+        uv = np.zeros((3 * nt, 2), np.float32)
+        verts = _pack(pos, nn, col, uv)
+        idx = np.arange(3 * nt, dtype=np.uint32)
+        m, r = _mat_rand(rng)
+        sc.meshes.append(Mesh(verts, idx, oid, mat_identity(), m, r))
+
+    oid = 1
+    counts = {"plain": int(n_tris * 0.60), "pair": int(n_tris * 0.10),
+              "straddle": int(n_tris * 0.10), "outside": int(n_tris * 0.05)}
+    for kind in ("plain", "straddle", "outside"):
+        v, nrm = tris(counts[kind], kind)
+        for s0 in range(0, v.shape[0], tris_per_mesh):
+            add_mesh(v[s0:s0 + tris_per_mesh], nrm[s0:s0 + tris_per_mesh], oid)
+            oid += 1
+    v, nrm = tris(counts["pair"], "plain")          # coplanar pairs: same triangles twice
+    for s0 in range(0, v.shape[0], tris_per_mesh):
+        for _ in range(2):
+            add_mesh(v[s0:s0 + tris_per_mesh], nrm[s0:s0 + tris_per_mesh], oid)
+            oid += 1
+    # joint-skinned tubes: 64 joints along each tube, 4 influences per vertex
+    skinned = n_tris - sum(counts.values()) - counts["pair"]
+    seg, ring = 64, 16
+    per_tube = 2 * seg * ring
+    for _ in range(max(1, skinned // per_tube)):
+        z = np.linspace(0.0, 1.0, seg + 1)
+        a = np.linspace(0.0, 2 * math.pi, ring, endpoint=False)
+        Z, A = np.meshgrid(z, a, indexing="ij")
+        rad = 0.15
+        pos = np.stack([rad * np.cos(A), rad * np.sin(A), Z * 4.0], -1).reshape(-1, 3)
+        nrm = np.stack([np.cos(A), np.sin(A), np.zeros_like(A)], -1).reshape(-1, 3)
+        col = np.tile(rng.uniform(0.2, 1.0, 4).astype(np.float32), (pos.shape[0], 1))
+        col[:, 3] = 1.0
+        verts = _pack(pos.astype(np.float32), nrm.astype(np.float32), col,
+                      np.zeros((pos.shape[0], 2), np.float32))
+        jpos = np.clip((Z.reshape(-1) * 63.0), 0, 63)
+        j0 = np.floor(jpos).astype(np.int64)
+        joints = np.clip(np.stack([j0 - 1, j0, j0 + 1, j0 + 2], 1), 0, 63)
+        w = rng.uniform(0.05, 1.0, (pos.shape[0], 4)).astype(np.float32)
+        w /= w.sum(1, keepdims=True)
+        mats = []
+        base = rng.uniform(-3, 3, 3) + np.array([0.0, 0.0, -5.0])
+        for j in range(64):
+            ang = 0.6 * math.sin(j / 64.0 * math.pi * rng.uniform(0.5, 2.0))
+            rot = np.array([[math.cos(ang), -math.sin(ang), 0], [math.sin(ang), math.cos(ang), 0],
+                            [0, 0, 1]])
+            mats.append(mat_trs(base + np.array([0.0, 0.02 * j, 0.0]), rot, (1.0, 1.0, 1.0)))
+        verts = skin_vertices(verts, joints, w, np.asarray(mats, np.float32))
+        idx = []
+        for s_ in range(seg):
+            for r_ in range(ring):
+                i0 = s_ * ring + r_
+                i1 = s_ * ring + (r_ + 1) % ring
+                i2 = i0 + ring
+                i3 = i1 + ring
+                idx += [i0, i1, i3, i0, i3, i2]
+        m, r = _mat_rand(rng)
+        sc.meshes.append(Mesh(verts, np.asarray(idx, np.uint32), oid, mat_identity(), m, r))
+        oid += 1
+    return sc
+
+
 @dataclasses.dataclass
 class View:
     """One viewport of a batch: presented size, SSAA factor and camera."""

@@ -5,7 +5,8 @@ IDs and depth must match bit for bit; colour within the contract tolerance
 (tests/parity.py).  Scenes cover: multi-light smooth GGX (directional,
 point, spot, ranged, inactive lights), textures, SSAA 2, IBL, flat shading
 (lit and unlit), near-plane clipping (the config-1 ground plane passes
-behind the camera), coplanar draw-order ties, and picks.
+behind the camera), coplanar draw-order ties, the clipping/depth stress scene
+(near-plane straddlers, coplanar pairs, host-skinned meshes), and picks.
 """
 import dataclasses
 
@@ -53,6 +54,10 @@ CASES = {
     "coplanar_ties": lambda: scenes.coplanar_scene(),
     "config2_reduced": lambda: scenes.config2(width=320, height=180, ssaa=2, instances=24,
                                               tex_size=64),
+    # clipping / depth stress: near-plane straddlers, out-of-frustum triangles, coplanar pairs
+    # in separate meshes, host-skinned tubes, 0.1-8 px triangles
+    "config3_reduced": lambda: scenes.config3(n_tris=80_000, width=480, height=270),
+    "config3_medium": lambda: scenes.config3(seed=4, n_tris=400_000, width=960, height=540),
 }
 
 
