@@ -1063,9 +1063,25 @@ __device__ __forceinline__ float aces(float x) { /* rasterizer.c:2770-2774 */
  * block iteration).  Blocks of 256 threads. */
 #define RESOLVE_PER_THREAD 8
 
-/* One block iteration of the resolve: samples [blk, blk + 256 * 8). */
-__device__ __forceinline__ void resolve_chunk(const FrameArgs &a, uint32_t blk, uint32_t *s_warp,
-                                              uint32_t *s_base_p) {
+/* This thread's 8 keys of the chunk at blk (full chunks only; the ragged
+ * tail is read sample by sample). */
+__device__ __forceinline__ void resolve_load_keys(const FrameArgs &a, uint32_t blk,
+                                                  ulonglong2 kk[RESOLVE_PER_THREAD / 2]) {
+  const uint32_t S = (uint32_t)a.width * (uint32_t)a.height;
+  const uint32_t i0 = blk + threadIdx.x * RESOLVE_PER_THREAD;
+  if (i0 + RESOLVE_PER_THREAD <= S) {
+    const ulonglong2 *kp = reinterpret_cast<const ulonglong2 *>(a.keys + i0);
+#pragma unroll
+    for (int k = 0; k < RESOLVE_PER_THREAD / 2; k++)
+      kk[k] = kp[k];
+  }
+}
+
+/* One block iteration of the resolve: samples [blk, blk + 256 * 8), with
+ * this thread's keys already loaded (resolve_load_keys). */
+__device__ __forceinline__ void resolve_chunk_keys(const FrameArgs &a, uint32_t blk,
+                                                   const ulonglong2 kk[RESOLVE_PER_THREAD / 2],
+                                                   uint32_t *s_warp, uint32_t *s_base_p) {
   uint32_t &s_base = *s_base_p;
   const uint32_t S = (uint32_t)a.width * (uint32_t)a.height;
   const uchar4 bg = make_uchar4(x86_f2u8(fminf(a.clear[0], 1.0f) * 255.0f + 0.5f),
@@ -1078,10 +1094,9 @@ __device__ __forceinline__ void resolve_chunk(const FrameArgs &a, uint32_t blk, 
     const uint32_t i0 = blk + threadIdx.x * RESOLVE_PER_THREAD;
     uint32_t mask = 0;
     if (i0 + RESOLVE_PER_THREAD <= S) {
-      const ulonglong2 *kp = reinterpret_cast<const ulonglong2 *>(a.keys + i0);
 #pragma unroll
       for (int k = 0; k < RESOLVE_PER_THREAD / 2; k++) {
-        const ulonglong2 v = kp[k];
+        const ulonglong2 v = kk[k];
         if (v.x != KEY_EMPTY)
           mask |= 1u << (2 * k);
         if (v.y != KEY_EMPTY)
@@ -1139,13 +1154,33 @@ __device__ __forceinline__ void resolve_chunk(const FrameArgs &a, uint32_t blk, 
   }
 }
 
+__device__ __forceinline__ void resolve_chunk(const FrameArgs &a, uint32_t blk, uint32_t *s_warp,
+                                              uint32_t *s_base_p) {
+  ulonglong2 kk[RESOLVE_PER_THREAD / 2];
+  resolve_load_keys(a, blk, kk);
+  resolve_chunk_keys(a, blk, kk, s_warp, s_base_p);
+}
+
+/* The next chunk's keys are loaded before this chunk's barriers and
+ * compaction atomic, so they are in flight while the block waits. */
 __global__ void __launch_bounds__(256) k_resolve(FrameArgs a) {
   __shared__ uint32_t s_warp[8];
   __shared__ uint32_t s_base;
   const uint32_t S = (uint32_t)a.width * (uint32_t)a.height;
-  const uint32_t per_iter = 256u * RESOLVE_PER_THREAD;
-  for (uint32_t blk = blockIdx.x * per_iter; blk < S; blk += gridDim.x * per_iter)
-    resolve_chunk(a, blk, s_warp, &s_base);
+  const uint32_t per_iter = 256u * RESOLVE_PER_THREAD, stride = gridDim.x * per_iter;
+  ulonglong2 nk[RESOLVE_PER_THREAD / 2];
+  uint32_t blk = blockIdx.x * per_iter;
+  if (blk < S)
+    resolve_load_keys(a, blk, nk);
+  for (; blk < S; blk += stride) {
+    ulonglong2 ck[RESOLVE_PER_THREAD / 2];
+#pragma unroll
+    for (int k = 0; k < RESOLVE_PER_THREAD / 2; k++)
+      ck[k] = nk[k];
+    if (blk + stride < S)
+      resolve_load_keys(a, blk + stride, nk);
+    resolve_chunk_keys(a, blk, ck, s_warp, &s_base);
+  }
 }
 
 /* Deferred shading of one covered sample: the winning record's exact edge

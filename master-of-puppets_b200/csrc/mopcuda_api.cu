@@ -535,11 +535,19 @@ int mc_build_draw(const MopCudaDraw *c, const float *model, const float *mvp,
     r.flags |= DF_CULL;
   if (lit) {
     r.flags |= DF_LIT;
-    r.light_off = (uint32_t)lights.size();
-    r.light_count = c->light_count;
+    /* the draw's active lights (inactive ones contribute nothing: the
+     * reference skips them, rasterizer.c:1504, 1605, 1729); a block equal to the
+     * previous draw's is shared, so a frame's draws usually share one list */
+    LightRec blk[64];
+    std::vector<LightRec> big;
+    LightRec *b = c->light_count <= 64 ? blk : (big.resize(c->light_count), big.data());
+    uint32_t n = 0;
     for (uint32_t i = 0; i < c->light_count; i++) {
       const MopCudaLight &s = c->lights[i];
+      if (!s.active)
+        continue;
       LightRec L;
+      memset(&L, 0, sizeof L);
       L.type = s.type;
       memcpy(L.position, s.position, sizeof L.position);
       memcpy(L.direction, s.direction, sizeof L.direction);
@@ -559,7 +567,15 @@ int mc_build_draw(const MopCudaDraw *c, const float *model, const float *mvp,
         for (int k = 0; k < 3; k++)
           L.ndir[k] = L.direction[k] * inv;
       }
-      lights.push_back(L);
+      b[n++] = L;
+    }
+    r.light_count = n;
+    if (n && lights.size() >= n &&
+        memcmp(lights.data() + (lights.size() - n), b, sizeof(LightRec) * n) == 0) {
+      r.light_off = (uint32_t)(lights.size() - n);
+    } else {
+      r.light_off = (uint32_t)lights.size();
+      lights.insert(lights.end(), b, b + n);
     }
   }
   return MOPCUDA_OK;
