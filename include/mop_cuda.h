@@ -149,6 +149,32 @@ int mopcuda_framebuffer_resize(MopCudaDevice *dev, MopCudaFramebuffer *fb, int w
  * (viewport.c:3385-3411) into its post pass. */
 int mopcuda_framebuffer_set_ssaa(MopCudaFramebuffer *fb, int ssaa);
 
+/* ---- vertex deformation: the core's mop_skin_apply / mop_morph_apply
+ *      (reference src/core/viewport.c:1572-1680, 1763-1804) on the device.
+ *      The core keeps the bind pose and morph targets in backend buffers and
+ *      calls these instead of deforming on the host and re-uploading; dst's
+ *      host shadow (mopcuda_buffer_read) is refreshed, as the core reads
+ *      deformed vertices back for bounds. ------------------------------- */
+typedef struct MopCudaDeformLayout {
+  uint32_t stride;         /* bytes per vertex, multiple of 4                */
+  int32_t position_offset; /* float3                                         */
+  int32_t normal_offset;   /* float3, -1 when absent                         */
+  int32_t joints_offset;   /* ubyte4 bone indices (skinning only)            */
+  int32_t weights_offset;  /* float4 bone weights (skinning only)            */
+} MopCudaDeformLayout;
+/* dst = bind pose with positions (and normals, renormalised) skinned by up
+ * to 4 weighted bones each; bones: bone_count column-major 4x4 (host). */
+int mopcuda_skin_apply(MopCudaDevice *dev, MopCudaBuffer *dst, const MopCudaBuffer *bind,
+                       uint32_t vertex_count, const MopCudaDeformLayout *layout,
+                       const float *bones, uint32_t bone_count);
+/* dst = bind pose with positions += weight_t * delta_t over the targets in
+ * order (zero weights skipped); targets: target_count x vertex_count x 3
+ * floats in a device buffer; weights: host array. */
+int mopcuda_morph_apply(MopCudaDevice *dev, MopCudaBuffer *dst, const MopCudaBuffer *bind,
+                        uint32_t vertex_count, const MopCudaDeformLayout *layout,
+                        const MopCudaBuffer *targets, const float *weights,
+                        uint32_t target_count);
+
 /* ---- frame state ------------------------------------------------------ */
 /* set_exposure (rhi.h:244): exposure for the ACES resolve
  * (reference mop_sw_hdr_resolve, rasterizer.c:2776). */

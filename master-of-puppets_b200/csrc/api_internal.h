@@ -136,6 +136,8 @@ struct MopCudaDevice {
   DevArena d_draws, d_lights, clip, world, normal, color, rrec, srec, clipq, keys,
       large_list, large_items, shade_list, counters, pick_xy, pick_out;
   HostArena h_draws, h_lights, h_counters, h_pick;
+  DevArena deform_params; /* bone matrices / morph weights of a deform call */
+  HostArena h_deform;
   uint32_t vertex_cap = 0, rec_cap = 0, clip_cap = 0, large_cap = 0;
   uint32_t extra_hint = 0, rec_hint = 0, clip_hint = 0, large_hint = 0;
   LaunchCfg cfg = {148, SMALL_MAX_SIDE, SMALL_MAX_AREA, 128, 256, 4, 32, 4};

@@ -2093,3 +2093,140 @@ int mopcuda_launch_batch(const BatchArgs &b, const PostArgs *posts, const uint32
   }
   return launches;
 }
+
+/* ========================================================================
+ * Vertex deformation: mop_skin_apply / mop_morph_apply on the device
+ * (reference src/core/viewport.c:1572-1680, 1763-1804).  One thread per
+ * vertex copies the bind-pose vertex and rewrites position (and normal), in
+ * the reference's operation order.
+ * ======================================================================== */
+__device__ __forceinline__ void copy_vertex(const uint8_t *src, uint8_t *dst, uint32_t stride) {
+  const uint32_t *s = reinterpret_cast<const uint32_t *>(src);
+  uint32_t *d = reinterpret_cast<uint32_t *>(dst);
+  for (uint32_t k = 0; k < stride / 4u; k++)
+    d[k] = s[k];
+}
+
+#define SKIN_SMEM_BONES 256
+
+__global__ void __launch_bounds__(256) k_skin(const uint8_t *bind, uint8_t *dst, uint32_t vc,
+                                              DeformLayout l, const float *bones,
+                                              uint32_t bone_count) {
+  __shared__ float s_b[SKIN_SMEM_BONES * 16];
+  const bool in_smem = bone_count <= SKIN_SMEM_BONES;
+  if (in_smem) {
+    for (uint32_t i = threadIdx.x; i < bone_count * 16u; i += blockDim.x)
+      s_b[i] = bones[i];
+    __syncthreads();
+  }
+  const float *B = in_smem ? s_b : bones;
+  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < vc; v += gridDim.x * blockDim.x) {
+    const uint8_t *vert = bind + (size_t)v * l.stride;
+    uint8_t *out = dst + (size_t)v * l.stride;
+    copy_vertex(vert, out, l.stride);
+    const uint8_t *jd = vert + l.joints_offset;
+    const uint8_t j[4] = {jd[0], jd[1], jd[2], jd[3]};
+    const float *wd = reinterpret_cast<const float *>(vert + l.weights_offset);
+    const float w[4] = {wd[0], wd[1], wd[2], wd[3]};
+    const float *pd = reinterpret_cast<const float *>(vert + l.position_offset);
+    const float px = pd[0], py = pd[1], pz = pd[2];
+    float sx = 0.0f, sy = 0.0f, sz = 0.0f;
+    for (int b = 0; b < 4; b++) {
+      if (w[b] <= 0.0f || j[b] >= bone_count)
+        continue;
+      const float *m = B + 16u * j[b];
+      const float rx = m[0] * px + m[4] * py + m[8] * pz + m[12];
+      const float ry = m[1] * px + m[5] * py + m[9] * pz + m[13];
+      const float rz = m[2] * px + m[6] * py + m[10] * pz + m[14];
+      sx += w[b] * rx;
+      sy += w[b] * ry;
+      sz += w[b] * rz;
+    }
+    float *op = reinterpret_cast<float *>(out + l.position_offset);
+    op[0] = sx;
+    op[1] = sy;
+    op[2] = sz;
+    if (l.normal_offset >= 0) {
+      const float *nd = reinterpret_cast<const float *>(vert + l.normal_offset);
+      const float nx = nd[0], ny = nd[1], nz = nd[2];
+      float snx = 0.0f, sny = 0.0f, snz = 0.0f;
+      for (int b = 0; b < 4; b++) {
+        if (w[b] <= 0.0f || j[b] >= bone_count)
+          continue;
+        const float *m = B + 16u * j[b];
+        const float rx = m[0] * nx + m[4] * ny + m[8] * nz;
+        const float ry = m[1] * nx + m[5] * ny + m[9] * nz;
+        const float rz = m[2] * nx + m[6] * ny + m[10] * nz;
+        snx += w[b] * rx;
+        sny += w[b] * ry;
+        snz += w[b] * rz;
+      }
+      const float len = sqrtf(snx * snx + sny * sny + snz * snz);
+      if (len > 1e-8f) {
+        snx /= len;
+        sny /= len;
+        snz /= len;
+      }
+      float *on = reinterpret_cast<float *>(out + l.normal_offset);
+      on[0] = snx;
+      on[1] = sny;
+      on[2] = snz;
+    }
+  }
+}
+
+#define MORPH_SMEM_WEIGHTS 1024
+
+__global__ void __launch_bounds__(256) k_morph(const uint8_t *bind, uint8_t *dst, uint32_t vc,
+                                               DeformLayout l, const float *targets,
+                                               const float *weights, uint32_t tc) {
+  __shared__ float s_w[MORPH_SMEM_WEIGHTS];
+  const bool in_smem = tc <= MORPH_SMEM_WEIGHTS;
+  if (in_smem) {
+    for (uint32_t i = threadIdx.x; i < tc; i += blockDim.x)
+      s_w[i] = weights[i];
+    __syncthreads();
+  }
+  const float *W = in_smem ? s_w : weights;
+  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < vc; v += gridDim.x * blockDim.x) {
+    const uint8_t *vert = bind + (size_t)v * l.stride;
+    uint8_t *out = dst + (size_t)v * l.stride;
+    copy_vertex(vert, out, l.stride);
+    const float *pd = reinterpret_cast<const float *>(vert + l.position_offset);
+    float p0 = pd[0], p1 = pd[1], p2 = pd[2];
+    for (uint32_t t = 0; t < tc; t++) { /* targets in order, as the reference's outer loop */
+      const float w = W[t];
+      if (w == 0.0f)
+        continue;
+      const float *d = targets + ((size_t)t * vc + v) * 3u;
+      p0 += w * d[0];
+      p1 += w * d[1];
+      p2 += w * d[2];
+    }
+    float *op = reinterpret_cast<float *>(out + l.position_offset);
+    op[0] = p0;
+    op[1] = p1;
+    op[2] = p2;
+  }
+}
+
+int mopcuda_launch_skin(const uint8_t *bind, uint8_t *dst, uint32_t vc, const DeformLayout &l,
+                        const float *bones, uint32_t bone_count, int num_sms, cudaStream_t s) {
+  if (!vc)
+    return 0;
+  const uint32_t g = blocks_for(vc, 256);
+  const uint32_t cap = (uint32_t)num_sms * 8u;
+  k_skin<<<g < cap ? g : cap, 256, 0, s>>>(bind, dst, vc, l, bones, bone_count);
+  return 1;
+}
+
+int mopcuda_launch_morph(const uint8_t *bind, uint8_t *dst, uint32_t vc, const DeformLayout &l,
+                         const float *targets, const float *weights, uint32_t tc, int num_sms,
+                         cudaStream_t s) {
+  if (!vc)
+    return 0;
+  const uint32_t g = blocks_for(vc, 256);
+  const uint32_t cap = (uint32_t)num_sms * 8u;
+  k_morph<<<g < cap ? g : cap, 256, 0, s>>>(bind, dst, vc, l, targets, weights, tc);
+  return 1;
+}

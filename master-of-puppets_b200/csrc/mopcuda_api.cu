@@ -140,13 +140,15 @@ extern "C" void mopcuda_device_destroy(MopCudaDevice *d) {
                         &d->d_lights, &d->clip,       &d->world,       &d->normal,
                         &d->color,    &d->rrec,       &d->srec,
                         &d->clipq,    &d->keys,       &d->large_list,  &d->large_items,
-                        &d->shade_list, &d->counters, &d->pick_xy,     &d->pick_out};
+                        &d->shade_list, &d->counters, &d->pick_xy,     &d->pick_out,
+                        &d->deform_params};
   for (DevArena *a : arenas)
     a->release();
   d->h_draws.release();
   d->h_lights.release();
   d->h_counters.release();
   d->h_pick.release();
+  d->h_deform.release();
   cudaEventDestroy(d->ev0);
   cudaEventDestroy(d->ev1);
   for (int i = 0; i <= MOPCUDA_STAGES; i++)
@@ -420,6 +422,94 @@ extern "C" int mopcuda_set_ibl(MopCudaDevice *d, const float *irr, int iw, int i
 /* ------------------------------------------------------------------------
  * frame commands
  * ------------------------------------------------------------------------ */
+/* ------------------------------------------------------------------------
+ * vertex deformation (mop_skin_apply / mop_morph_apply on the device)
+ * ------------------------------------------------------------------------ */
+static int deform_check(const MopCudaBuffer *dst, const MopCudaBuffer *bind, uint32_t vc,
+                        const MopCudaDeformLayout *l, bool skin) {
+  if (!dst || !bind || !l || l->stride == 0 || l->stride % 4 || l->position_offset < 0 ||
+      l->position_offset % 4 || (uint32_t)l->position_offset + 12u > l->stride)
+    return fail(MOPCUDA_EINVAL, "deform: bad layout");
+  if (l->normal_offset >= 0 && (l->normal_offset % 4 || (uint32_t)l->normal_offset + 12u > l->stride))
+    return fail(MOPCUDA_EINVAL, "deform: bad normal offset");
+  if (skin && (l->joints_offset < 0 || (uint32_t)l->joints_offset + 4u > l->stride ||
+               l->weights_offset < 0 || l->weights_offset % 4 ||
+               (uint32_t)l->weights_offset + 16u > l->stride))
+    return fail(MOPCUDA_EINVAL, "deform: skinning needs joints (ubyte4) and weights (float4)");
+  const size_t need = (size_t)vc * l->stride;
+  if (need > bind->size || need > dst->size)
+    return fail(MOPCUDA_EINVAL, "deform: %u vertices exceed a buffer", vc);
+  return MOPCUDA_OK;
+}
+
+/* Runs the launch on the device stream, then refreshes dst's host shadow (the
+ * core reads deformed vertices back for bounds). */
+static int deform_finish(MopCudaDevice *d, MopCudaBuffer *dst, size_t bytes) {
+  CU_TRY(cudaGetLastError());
+  CU_TRY(cudaMemcpyAsync(dst->h, dst->d, bytes, cudaMemcpyDeviceToHost, d->stream));
+  return mc_stream_sync(d, FRAME_TIMEOUT_MS);
+}
+
+extern "C" int mopcuda_skin_apply(MopCudaDevice *d, MopCudaBuffer *dst, const MopCudaBuffer *bind,
+                                  uint32_t vc, const MopCudaDeformLayout *l, const float *bones,
+                                  uint32_t bone_count) {
+  if (!d || (bone_count && !bones))
+    return fail(MOPCUDA_EINVAL, "skin_apply: bad arguments");
+  int rc = deform_check(dst, bind, vc, l, true);
+  if (rc)
+    return rc;
+  std::lock_guard<std::mutex> lk(d->mu);
+  cudaSetDevice(d->ordinal);
+  if (d->pending && (rc = finish_frame(d, FRAME_TIMEOUT_MS)))
+    return rc; /* the last frame may still read dst */
+  const size_t bb = 64ull * bone_count;
+  if (d->deform_params.ensure(bb + 16) || d->h_deform.ensure(bb + 16))
+    return MOPCUDA_ENOMEM;
+  if (bb) {
+    memcpy(d->h_deform.p, bones, bb);
+    CU_TRY(cudaMemcpyAsync(d->deform_params.p, d->h_deform.p, bb, cudaMemcpyHostToDevice,
+                           d->stream));
+  }
+  DeformLayout dl = {l->stride, l->position_offset, l->normal_offset, l->joints_offset,
+                     l->weights_offset};
+  d->launches += (uint64_t)mopcuda_launch_skin((const uint8_t *)bind->d, (uint8_t *)dst->d, vc,
+                                               dl, d->deform_params.as<float>(), bone_count,
+                                               d->num_sms, d->stream);
+  return deform_finish(d, dst, (size_t)vc * l->stride);
+}
+
+extern "C" int mopcuda_morph_apply(MopCudaDevice *d, MopCudaBuffer *dst,
+                                   const MopCudaBuffer *bind, uint32_t vc,
+                                   const MopCudaDeformLayout *l, const MopCudaBuffer *targets,
+                                   const float *weights, uint32_t target_count) {
+  if (!d || (target_count && (!weights || !targets)))
+    return fail(MOPCUDA_EINVAL, "morph_apply: bad arguments");
+  int rc = deform_check(dst, bind, vc, l, false);
+  if (rc)
+    return rc;
+  if (target_count && (size_t)target_count * vc * 12u > targets->size)
+    return fail(MOPCUDA_EINVAL, "morph_apply: targets buffer holds fewer than %u targets",
+                target_count);
+  std::lock_guard<std::mutex> lk(d->mu);
+  cudaSetDevice(d->ordinal);
+  if (d->pending && (rc = finish_frame(d, FRAME_TIMEOUT_MS)))
+    return rc;
+  const size_t wb = 4ull * target_count;
+  if (d->deform_params.ensure(wb + 16) || d->h_deform.ensure(wb + 16))
+    return MOPCUDA_ENOMEM;
+  if (wb) {
+    memcpy(d->h_deform.p, weights, wb);
+    CU_TRY(cudaMemcpyAsync(d->deform_params.p, d->h_deform.p, wb, cudaMemcpyHostToDevice,
+                           d->stream));
+  }
+  DeformLayout dl = {l->stride, l->position_offset, l->normal_offset, -1, -1};
+  d->launches += (uint64_t)mopcuda_launch_morph(
+      (const uint8_t *)bind->d, (uint8_t *)dst->d, vc, dl,
+      target_count ? (const float *)targets->d : nullptr, d->deform_params.as<float>(),
+      target_count, d->num_sms, d->stream);
+  return deform_finish(d, dst, (size_t)vc * l->stride);
+}
+
 extern "C" int mopcuda_frame_begin(MopCudaDevice *d, MopCudaFramebuffer *fb, const float clear[4]) {
   if (!d || !fb)
     return fail(MOPCUDA_EINVAL, "frame_begin: bad arguments");

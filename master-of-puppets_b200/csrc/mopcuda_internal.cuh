@@ -220,6 +220,19 @@ struct LaunchCfg {
   int post_bx, post_by;
 };
 
+/* Byte layout of a deformed vertex: stride and offsets (-1: no normal). */
+struct DeformLayout {
+  uint32_t stride;
+  int32_t position_offset, normal_offset, joints_offset, weights_offset;
+};
+
+/* Skinning / morph of vc vertices from bind into dst (device pointers). */
+int mopcuda_launch_skin(const uint8_t *bind, uint8_t *dst, uint32_t vc, const DeformLayout &l,
+                        const float *bones, uint32_t bone_count, int num_sms, cudaStream_t s);
+int mopcuda_launch_morph(const uint8_t *bind, uint8_t *dst, uint32_t vc, const DeformLayout &l,
+                         const float *targets, const float *weights, uint32_t tc, int num_sms,
+                         cudaStream_t s);
+
 /* ------------------------------------------------------------------------
  * batched viewports over one resident scene
  * ------------------------------------------------------------------------ */

@@ -53,6 +53,12 @@ class MopCudaDraw(C.Structure):
                 ("light_count", C.c_uint32), ("layout", C.POINTER(MopCudaVertexLayout))]
 
 
+class MopCudaDeformLayout(C.Structure):
+    _fields_ = [("stride", C.c_uint32), ("position_offset", C.c_int32),
+                ("normal_offset", C.c_int32), ("joints_offset", C.c_int32),
+                ("weights_offset", C.c_int32)]
+
+
 class MopCudaView(C.Structure):
     _fields_ = [("view", C.c_float * 16), ("proj", C.c_float * 16), ("eye", C.c_float * 3),
                 ("width", C.c_int), ("height", C.c_int), ("ssaa", C.c_int),
@@ -112,6 +118,10 @@ SIGNATURES = [
     ("mopcuda_set_post_effects", None, [_P, C.c_uint32]),
     ("mopcuda_set_ibl", C.c_int, [_P, _P, C.c_int, C.c_int, _P, C.c_int, C.c_int, C.c_int, _P,
                                   C.c_int, C.c_float, C.c_float]),
+    ("mopcuda_skin_apply", C.c_int, [_P, _P, _P, C.c_uint32, C.POINTER(MopCudaDeformLayout),
+                                     _P, C.c_uint32]),
+    ("mopcuda_morph_apply", C.c_int, [_P, _P, _P, C.c_uint32, C.POINTER(MopCudaDeformLayout),
+                                      _P, _P, C.c_uint32]),
     ("mopcuda_frame_begin", C.c_int, [_P, _P, _P]),
     ("mopcuda_draw", C.c_int, [_P, _P, C.POINTER(MopCudaDraw)]),
     ("mopcuda_draw_list", C.c_int, [_P, _P, _P, C.c_uint32]),
@@ -700,3 +710,33 @@ class Server:
         if self.h:
             self.L.mopcuda_server_destroy(self.h)
             self.h = None
+
+
+def deform(dev: Device, bind_bytes, vertex_count: int, layout, bones=None, targets=None,
+           weights=None) -> np.ndarray:
+    """Skinning (bones) or morph (targets + weights) of a vertex buffer on the
+    device through the C ABI; returns the deformed bytes (the host shadow
+    mopcuda_buffer_read gives after the call)."""
+    L, d = dev.L, dev.h
+    b = np.ascontiguousarray(bind_bytes, np.uint8)
+    bind = L.mopcuda_buffer_create(d, b.ctypes.data, b.nbytes)
+    dst = L.mopcuda_buffer_create(d, b.ctypes.data, b.nbytes)
+    tb = None
+    try:
+        lay = MopCudaDeformLayout(*layout)
+        if bones is not None:
+            m = _f32(bones).reshape(-1)
+            _check(L.mopcuda_skin_apply(d, dst, bind, vertex_count, C.byref(lay), m.ctypes.data,
+                                        m.size // 16), "skin_apply")
+        else:
+            t = _f32(targets).reshape(-1)
+            w = _f32(weights)
+            tb = L.mopcuda_buffer_create(d, t.ctypes.data, t.nbytes)
+            _check(L.mopcuda_morph_apply(d, dst, bind, vertex_count, C.byref(lay), tb,
+                                         w.ctypes.data, w.size), "morph_apply")
+        p = L.mopcuda_buffer_read(dst)
+        return np.ctypeslib.as_array(C.cast(p, C.POINTER(C.c_uint8)), shape=(b.nbytes,)).copy()
+    finally:
+        for h in (bind, dst, tb):
+            if h:
+                L.mopcuda_buffer_destroy(d, h)

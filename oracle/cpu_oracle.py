@@ -58,6 +58,36 @@ class OrFrame(C.Structure):
 _lib = None
 
 
+class OrDeformLayout(C.Structure):
+    _fields_ = [("stride", C.c_uint32), ("position_offset", C.c_int32),
+                ("normal_offset", C.c_int32), ("joints_offset", C.c_int32),
+                ("weights_offset", C.c_int32)]
+
+
+def skin(layout, bind: np.ndarray, vertex_count: int, bones: np.ndarray) -> np.ndarray:
+    """mop_skin_apply restated (bytes in, bytes out)."""
+    L = OrDeformLayout(*layout)
+    b = np.ascontiguousarray(bind, np.uint8)
+    m = np.ascontiguousarray(bones, np.float32).reshape(-1)
+    out = np.empty_like(b)
+    lib().oracle_skin_apply(C.byref(L), b.ctypes.data, vertex_count, m.ctypes.data,
+                            m.size // 16, out.ctypes.data)
+    return out
+
+
+def morph(layout, bind: np.ndarray, vertex_count: int, targets: np.ndarray,
+          weights: np.ndarray) -> np.ndarray:
+    """mop_morph_apply restated (bytes in, bytes out)."""
+    L = OrDeformLayout(*layout)
+    b = np.ascontiguousarray(bind, np.uint8)
+    t = np.ascontiguousarray(targets, np.float32).reshape(-1)
+    w = np.ascontiguousarray(weights, np.float32)
+    out = np.empty_like(b)
+    lib().oracle_morph_apply(C.byref(L), b.ctypes.data, vertex_count, t.ctypes.data,
+                             w.ctypes.data, w.size, out.ctypes.data)
+    return out
+
+
 def lib():
     global _lib
     if _lib is None:
@@ -70,6 +100,10 @@ def lib():
         _lib.oracle_pick.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int,
                                      C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
         _lib.oracle_gamma_lut.argtypes = [C.c_void_p]
+        _lib.oracle_skin_apply.argtypes = [C.POINTER(OrDeformLayout), C.c_void_p, C.c_uint32,
+                                           C.c_void_p, C.c_uint32, C.c_void_p]
+        _lib.oracle_morph_apply.argtypes = [C.POINTER(OrDeformLayout), C.c_void_p, C.c_uint32,
+                                            C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p]
     return _lib
 
 

@@ -1273,3 +1273,77 @@ void oracle_pick(const uint32_t *object_id, const float *depth, int width, int h
     }
   }
 }
+
+/* ------------------------------------------------------------------------
+ * vertex deformation (reference src/core/viewport.c:1572-1680, 1763-1804)
+ * ------------------------------------------------------------------------ */
+void oracle_skin_apply(const OrDeformLayout *l, const uint8_t *bind, uint32_t vc,
+                       const float *bones, uint32_t bone_count, uint8_t *dst) {
+  memcpy(dst, bind, (size_t)vc * l->stride);
+  for (uint32_t v = 0; v < vc; v++) {
+    const uint8_t *vert = bind + (size_t)v * l->stride;
+    uint8_t *out = dst + (size_t)v * l->stride;
+    const uint8_t *jd = vert + l->joints_offset;
+    float w[4], p[3];
+    memcpy(w, vert + l->weights_offset, sizeof w);
+    memcpy(p, vert + l->position_offset, sizeof p);
+    float sx = 0, sy = 0, sz = 0;
+    for (int b = 0; b < 4; b++) {
+      if (w[b] <= 0.0f || jd[b] >= bone_count)
+        continue;
+      const float *m = bones + 16 * (size_t)jd[b];
+      float rx = m[0] * p[0] + m[4] * p[1] + m[8] * p[2] + m[12];
+      float ry = m[1] * p[0] + m[5] * p[1] + m[9] * p[2] + m[13];
+      float rz = m[2] * p[0] + m[6] * p[1] + m[10] * p[2] + m[14];
+      sx += w[b] * rx;
+      sy += w[b] * ry;
+      sz += w[b] * rz;
+    }
+    float o[3] = {sx, sy, sz};
+    memcpy(out + l->position_offset, o, sizeof o);
+    if (l->normal_offset >= 0) {
+      float n[3];
+      memcpy(n, vert + l->normal_offset, sizeof n);
+      float nx = 0, ny = 0, nz = 0;
+      for (int b = 0; b < 4; b++) {
+        if (w[b] <= 0.0f || jd[b] >= bone_count)
+          continue;
+        const float *m = bones + 16 * (size_t)jd[b];
+        float rx = m[0] * n[0] + m[4] * n[1] + m[8] * n[2];
+        float ry = m[1] * n[0] + m[5] * n[1] + m[9] * n[2];
+        float rz = m[2] * n[0] + m[6] * n[1] + m[10] * n[2];
+        nx += w[b] * rx;
+        ny += w[b] * ry;
+        nz += w[b] * rz;
+      }
+      float len = sqrtf(nx * nx + ny * ny + nz * nz);
+      if (len > 1e-8f) {
+        nx /= len;
+        ny /= len;
+        nz /= len;
+      }
+      float on[3] = {nx, ny, nz};
+      memcpy(out + l->normal_offset, on, sizeof on);
+    }
+  }
+}
+
+void oracle_morph_apply(const OrDeformLayout *l, const uint8_t *bind, uint32_t vc,
+                        const float *targets, const float *weights, uint32_t tc, uint8_t *dst) {
+  memcpy(dst, bind, (size_t)vc * l->stride);
+  for (uint32_t t = 0; t < tc; t++) {
+    float w = weights[t];
+    if (w == 0.0f)
+      continue;
+    const float *d = targets + (size_t)t * vc * 3;
+    for (uint32_t v = 0; v < vc; v++) {
+      float pos[3];
+      uint8_t *q = dst + (size_t)v * l->stride + l->position_offset;
+      memcpy(pos, q, sizeof pos);
+      pos[0] += w * d[v * 3 + 0];
+      pos[1] += w * d[v * 3 + 1];
+      pos[2] += w * d[v * 3 + 2];
+      memcpy(q, pos, sizeof pos);
+    }
+  }
+}

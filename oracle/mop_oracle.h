@@ -114,6 +114,24 @@ void oracle_pick(const uint32_t *object_id, const float *depth, int width,
 /* sRGB gamma byte map used by the post-process (postprocess.c:75-82). */
 void oracle_gamma_lut(uint8_t lut[256]);
 
+/* Vertex deformation the core runs before buffer_update: byte layout of one
+ * vertex (stride; offsets of position float3, normal float3 or -1, joints
+ * ubyte4, weights float4). */
+typedef struct OrDeformLayout {
+  uint32_t stride;
+  int32_t position_offset, normal_offset, joints_offset, weights_offset;
+} OrDeformLayout;
+
+/* mop_skin_apply (reference src/core/viewport.c:1572-1680): dst = bind pose
+ * with positions and normals skinned by the bone matrices (column-major). */
+void oracle_skin_apply(const OrDeformLayout *l, const uint8_t *bind, uint32_t vertex_count,
+                       const float *bones, uint32_t bone_count, uint8_t *dst);
+/* mop_morph_apply (viewport.c:1763-1804): dst = bind pose with positions
+ * plus the weighted deltas of every target (targets * vertices * 3 floats). */
+void oracle_morph_apply(const OrDeformLayout *l, const uint8_t *bind, uint32_t vertex_count,
+                        const float *targets, const float *weights, uint32_t target_count,
+                        uint8_t *dst);
+
 #ifdef __cplusplus
 }
 #endif

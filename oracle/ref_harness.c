@@ -274,3 +274,42 @@ void refh_destroy(void *hp) {
   mop_viewport_destroy(h->vp);
   free(h);
 }
+
+int refh_deform_probe(const uint8_t *vertices, uint32_t vertex_count, const float *bones,
+                      uint32_t bone_count, const float *targets, const float *weights,
+                      uint32_t target_count, uint8_t *out) {
+  if (!vertices || vertex_count < 3 || !out)
+    return -1;
+  MopViewportDesc desc = {.width = 16, .height = 16, .backend = MOP_BACKEND_CPU, .ssaa_factor = 1};
+  MopViewport *vp = mop_viewport_create(&desc);
+  if (!vp)
+    return -1;
+  mop_viewport_set_chrome(vp, false);
+  MopVertexFormat fmt;
+  memset(&fmt, 0, sizeof fmt);
+  fmt.attribs[0] = (MopVertexAttrib){MOP_ATTRIB_POSITION, MOP_FORMAT_FLOAT3, 0};
+  fmt.attribs[1] = (MopVertexAttrib){MOP_ATTRIB_NORMAL, MOP_FORMAT_FLOAT3, 12};
+  fmt.attribs[2] = (MopVertexAttrib){MOP_ATTRIB_JOINTS, MOP_FORMAT_UBYTE4, 24};
+  fmt.attribs[3] = (MopVertexAttrib){MOP_ATTRIB_WEIGHTS, MOP_FORMAT_FLOAT4, 28};
+  fmt.attrib_count = 4;
+  fmt.stride = 44;
+  const uint32_t idx[3] = {0, 1, 2};
+  MopMeshDescEx md = {.vertex_data = vertices, .vertex_count = vertex_count, .indices = idx,
+                      .index_count = 3, .object_id = 1, .vertex_format = &fmt};
+  MopMesh *m = mop_viewport_add_mesh_ex(vp, &md);
+  int rc = -1;
+  if (m) {
+    if (target_count && targets && weights)
+      mop_mesh_set_morph_targets(m, vp, targets, weights, target_count);
+    if (bone_count && bones)
+      mop_mesh_set_bone_matrices(m, vp, (const MopMat4 *)bones, bone_count);
+    mop_viewport_render(vp);
+    const void *raw = vp->rhi->buffer_read(m->vertex_buffer);
+    if (raw) {
+      memcpy(out, raw, (size_t)vertex_count * 44u);
+      rc = 0;
+    }
+  }
+  mop_viewport_destroy(vp);
+  return rc;
+}

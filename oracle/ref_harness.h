@@ -97,6 +97,16 @@ double refh_time_frames(void *h, int warm, int frames);
 int refh_num_threads(void *h);
 void refh_destroy(void *h);
 
+/* Deformation probe: one mesh of vertex layout position float3 @0, normal
+ * float3 @12, joints ubyte4 @24, weights float4 @28 (stride 44) added with
+ * mop_viewport_add_mesh_ex; bone matrices (mop_mesh_set_bone_matrices) and/or
+ * morph targets (mop_mesh_set_morph_targets) set; one render on the CPU
+ * backend; the vertex buffer the core uploaded is copied to out
+ * (vertex_count * 44 bytes).  Returns 0 on success. */
+int refh_deform_probe(const uint8_t *vertices, uint32_t vertex_count, const float *bones,
+                      uint32_t bone_count, const float *targets, const float *weights,
+                      uint32_t target_count, uint8_t *out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -97,6 +97,9 @@ def lib(kind: str = "cpu"):
         _lib.refh_time_frames.argtypes = [C.c_void_p, C.c_int, C.c_int]
         _lib.refh_num_threads.argtypes = [C.c_void_p]
         _lib.refh_destroy.argtypes = [C.c_void_p]
+        if hasattr(_lib, "refh_deform_probe"):
+            _lib.refh_deform_probe.argtypes = [C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint32,
+                                               C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p]
     return _libs[kind]
 
 
@@ -238,3 +241,25 @@ class Reference:
             self.close()
         except Exception:
             pass
+
+
+def deform_probe(vertices: np.ndarray, vertex_count: int, bones=None, targets=None,
+                 weights=None) -> np.ndarray:
+    """The reference core's own skinning / morph of one mesh (layout: position
+    @0, normal @12, joints ubyte4 @24, weights float4 @28, stride 44), read
+    back from the CPU backend's vertex buffer."""
+    L = lib()
+    v = np.ascontiguousarray(vertices, np.uint8)
+    out = np.zeros(vertex_count * 44, np.uint8)
+    b = None if bones is None else np.ascontiguousarray(bones, np.float32).reshape(-1)
+    t = None if targets is None else np.ascontiguousarray(targets, np.float32).reshape(-1)
+    w = None if weights is None else np.ascontiguousarray(weights, np.float32)
+    rc = L.refh_deform_probe(v.ctypes.data, vertex_count,
+                             b.ctypes.data if b is not None else None,
+                             b.size // 16 if b is not None else 0,
+                             t.ctypes.data if t is not None else None,
+                             w.ctypes.data if w is not None else None,
+                             w.size if w is not None else 0, out.ctypes.data)
+    if rc != 0:
+        raise RuntimeError("refh_deform_probe failed")
+    return out

@@ -29,3 +29,34 @@ def assert_frame_parity(got, ref, label=""):
         s = color_stats(got[key], ref[key])
         assert s["max"] <= COLOR_MAX_LSB, f"{label}: {key} max diff {s}"
         assert s["within1"] >= COLOR_1LSB_FRACTION, f"{label}: {key} {s}"
+
+
+def deform_case(seed: int, vertex_count: int, bone_count: int = 64, stride: int = 44):
+    """Seeded skinning input in the layout position float3 @0, normal float3
+    @12, joints ubyte4 @24, weights float4 @28 (+ padding to `stride`):
+    weights of both signs (non-positive ones are skipped), joint indices
+    beyond bone_count (skipped), zero normals (not renormalised), and random
+    affine bones (column-major)."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    vc = vertex_count
+    raw = np.zeros((vc, stride), np.uint8)
+    f = np.zeros((vc, 11), np.float32)
+    f[:, 0:3] = rng.uniform(-3, 3, (vc, 3))
+    n = rng.normal(size=(vc, 3))
+    n /= np.linalg.norm(n, axis=1, keepdims=True)
+    n[::17] = 0.0
+    f[:, 3:6] = n
+    w = rng.uniform(-0.2, 1.0, (vc, 4)).astype(np.float32)
+    w /= np.abs(w).sum(1, keepdims=True)
+    f[:, 7:11] = w
+    raw[:, :44] = f.view(np.uint8).reshape(vc, 44)
+    raw[:, 24:28] = rng.integers(0, min(255, bone_count + 8), (vc, 4)).astype(np.uint8)
+    bones = np.zeros((bone_count, 16), np.float32)
+    for k in range(bone_count):
+        q, _ = np.linalg.qr(rng.normal(size=(3, 3)))
+        m = np.eye(4)
+        m[:3, :3] = q * rng.uniform(0.5, 2.0)
+        m[:3, 3] = rng.uniform(-1, 1, 3)
+        bones[k] = m.T.reshape(-1)
+    return raw.reshape(-1), bones

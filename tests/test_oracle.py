@@ -93,3 +93,25 @@ def test_gamma_lut_matches_formula():
     lut = cpu_oracle.gamma_lut()
     assert lut[0] == 0 and lut[255] == 255
     assert (np.diff(lut.astype(int)) >= 0).all()
+
+
+@pytest.mark.skipif(not refdrive.available(), reason="reference library not built")
+def test_deform_oracle_matches_reference():
+    """Skinning and morph restated in the oracle equal the reference core's
+    own mop_skin_apply / mop_morph_apply, read back from its CPU backend."""
+    from parity import deform_case
+    lay = (44, 0, 12, 24, 28)
+    for seed, vc in ((1, 500), (2, 2048)):
+        raw, bones = deform_case(seed, vc)
+        got = cpu_oracle.skin(lay, raw, vc, bones)
+        ref = refdrive.deform_probe(raw, vc, bones=bones)
+        assert (got == ref).all(), f"skin seed {seed}"
+        rng = np.random.default_rng(seed)
+        targets = rng.normal(size=(4, vc, 3)).astype(np.float32)
+        weights = np.array([0.5, 0.0, -0.25, 1.5], np.float32)
+        got = cpu_oracle.morph(lay, raw, vc, targets, weights)
+        ref = refdrive.deform_probe(raw, vc, targets=targets, weights=weights)
+        assert (got == ref).all(), f"morph seed {seed}"
+        # both set: the core morphs, then skins from the bind pose again
+        ref = refdrive.deform_probe(raw, vc, bones=bones, targets=targets, weights=weights)
+        assert (cpu_oracle.skin(lay, raw, vc, bones) == ref).all(), f"skin+morph seed {seed}"
