@@ -44,6 +44,7 @@ class Mesh:
     has_material: bool = True
     texture: int = -1
     opacity: float = 1.0
+    blend_mode: int = 0           # MopBlendMode set explicitly (0: opaque unless opacity < 1)
 
     @property
     def triangle_count(self) -> int:
@@ -587,6 +588,64 @@ def config3(seed: int = 3, width: int = 1920, height: int = 1080, n_tris: int = 
                 idx += [i0, i1, i3, i0, i3, i2]
         m, r = _mat_rand(rng)
         sc.meshes.append(Mesh(verts, np.asarray(idx, np.uint32), oid, mat_identity(), m, r))
+        oid += 1
+    return sc
+
+
+BLEND_OPAQUE, BLEND_ALPHA, BLEND_ADDITIVE, BLEND_MULTIPLY = 0, 1, 2, 3
+
+
+def effective_blend(m: Mesh) -> int:
+    """The mesh's blend mode as the core holds it: mop_mesh_set_opacity
+    promotes an opaque mesh to alpha blending below opacity 1
+    (reference viewport.c:1815-1829)."""
+    if m.blend_mode:
+        return m.blend_mode
+    return BLEND_ALPHA if m.opacity < 1.0 else BLEND_OPAQUE
+
+
+def draw_order(scene: Scene, eye) -> List[int]:
+    """Mesh indices in the core's draw order (viewport.c:2449-2553): opaque
+    meshes in scene order, then blended meshes back to front by the float32
+    squared distance of their translation to the eye (the core's insertion
+    sort: farthest first, ties keep scene order)."""
+    opaque = [k for k, m in enumerate(scene.meshes) if effective_blend(m) == BLEND_OPAQUE]
+    trans = [k for k, m in enumerate(scene.meshes) if effective_blend(m) != BLEND_OPAQUE]
+    e = np.asarray(eye, np.float32)
+    dist = []
+    for k in trans:
+        t = np.asarray(scene.meshes[k].transform, np.float32)
+        dx, dy, dz = t[12] - e[0], t[13] - e[1], t[14] - e[2]
+        dist.append(np.float32(np.float32(dx * dx + dy * dy) + dz * dz))
+    idx = list(trans)
+    for j in range(1, len(idx)):
+        ki, kd = idx[j], dist[j]
+        i = j - 1
+        while i >= 0 and dist[i] < kd:
+            idx[i + 1], dist[i + 1] = idx[i], dist[i]
+            i -= 1
+        idx[i + 1], dist[i + 1] = ki, kd
+    return opaque + idx
+
+
+def transparent_scene(seed: int = 12, width: int = 160, height: int = 120, ssaa: int = 1,
+                      env: int = 0) -> Scene:
+    """small_scene plus overlapping blended meshes: alpha (opacity 0.2-0.9),
+    additive and multiply spheres and quads in front of and behind the opaque
+    ones, so blended fragments stack, pass and fail the depth test, and write
+    depth and IDs when their alpha exceeds 0.5."""
+    sc = small_scene(seed=seed, width=width, height=height, ssaa=ssaa, env=env)
+    rng = np.random.default_rng(seed + 100)
+    oid = max(m.object_id for m in sc.meshes) + 1
+    modes = [BLEND_OPAQUE, BLEND_OPAQUE, BLEND_ALPHA, BLEND_ADDITIVE, BLEND_MULTIPLY, BLEND_OPAQUE]
+    for k, mode in enumerate(modes):
+        v, i = uv_sphere(24, 12, float(rng.uniform(0.4, 0.9)), _color(rng))
+        t = rng.uniform(-1.2, 1.2, 3)
+        m = mat_trs(t, random_rotation(rng), (1.0, 1.0, 1.0))
+        mt, r = _mat_rand(rng)
+        op = float(rng.uniform(0.2, 0.9)) if mode in (BLEND_OPAQUE, BLEND_ALPHA) else \
+            float(rng.uniform(0.3, 1.0))
+        sc.meshes.append(Mesh(v, i, oid, m, mt, r, opacity=op, blend_mode=mode))
         oid += 1
     return sc
 

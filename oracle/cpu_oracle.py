@@ -11,6 +11,8 @@ from pathlib import Path
 
 import numpy as np
 
+import scenes
+
 HERE = Path(__file__).resolve().parent
 ORACLE_SO = HERE / "liboracle.so"
 
@@ -162,7 +164,8 @@ def render(scene, ibl=None, want_hdr=False):
     texs = [np.ascontiguousarray(t, np.uint8) for t in scene.textures]
     draws = (OrDraw * max(1, len(scene.meshes)))()
     amb = min(max(scene.ambient, 0.0), 1.0)
-    for k, m in enumerate(scene.meshes):
+    for k, mi in enumerate(scenes.draw_order(scene, eye)):
+        m = scene.meshes[mi]
         v = _f32(m.vertices)
         i = np.ascontiguousarray(m.indices, np.uint32)
         keep += [v, i]
@@ -180,7 +183,8 @@ def render(scene, ibl=None, want_hdr=False):
         d.depth_bias = 0.0
         d.cam_eye[:] = [float(x) for x in eye]
         d.smooth = 1 if getattr(scene, "smooth", True) else 0
-        d.depth_test, d.backface_cull, d.blend_mode = 1, 1, 0
+        d.depth_test, d.backface_cull = 1, 1
+        d.blend_mode = scenes.effective_blend(m)
         d.lights = lights
         d.light_count = len(scene.lights)
         if m.texture >= 0:

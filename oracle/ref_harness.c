@@ -146,6 +146,8 @@ void *refh_create(const RefScene *sc) {
     }
     if (rm->texture >= 0 && (uint32_t)rm->texture < h->texture_count)
       mop_mesh_set_texture(mesh, h->textures[rm->texture]);
+    if (rm->blend_mode > 0)
+      mop_mesh_set_blend_mode(mesh, (MopBlendMode)rm->blend_mode);
     if (rm->opacity != 1.0f)
       mop_mesh_set_opacity(mesh, rm->opacity);
   }

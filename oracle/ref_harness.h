@@ -31,6 +31,7 @@ typedef struct RefMesh {
   int32_t has_material;     /* 0: reference defaults (metallic 0, rough .5) */
   int32_t texture;          /* index into RefScene textures, -1 = none      */
   float opacity;
+  int32_t blend_mode;       /* > 0: mop_mesh_set_blend_mode before opacity  */
 } RefMesh;
 
 typedef struct RefLight {

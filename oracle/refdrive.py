@@ -22,7 +22,7 @@ class RefMesh(C.Structure):
                 ("object_id", C.c_uint32), ("transform", C.c_float * 16),
                 ("metallic", C.c_float), ("roughness", C.c_float),
                 ("has_material", C.c_int32), ("texture", C.c_int32),
-                ("opacity", C.c_float)]
+                ("opacity", C.c_float), ("blend_mode", C.c_int32)]
 
 
 class RefLight(C.Structure):
@@ -127,6 +127,7 @@ class Reference:
             rm.has_material = 1 if m.has_material else 0
             rm.texture = m.texture
             rm.opacity = m.opacity
+            rm.blend_mode = getattr(m, "blend_mode", 0)
         lights = (RefLight * max(1, len(scene.lights)))()
         for k, l in enumerate(scene.lights):
             lights[k] = light_struct(l)

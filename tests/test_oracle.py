@@ -64,6 +64,10 @@ LIVE = {
     "coplanar": lambda: scenes.coplanar_scene(seed=16),
     "config2_reduced": lambda: scenes.config2(width=256, height=144, ssaa=2, instances=16,
                                               tex_size=32),
+    # blended meshes (alpha / additive / multiply) in the core's transparent pass order
+    "transparent": lambda: scenes.transparent_scene(seed=17),
+    "transparent_ssaa2_ibl": lambda: scenes.transparent_scene(seed=18, ssaa=2, env=1),
+    "config3_small": lambda: scenes.config3(seed=19, n_tris=30_000, width=320, height=180),
 }
 
 
