@@ -120,6 +120,7 @@ struct MopCudaDevice {
   std::vector<LightRec> lights;
   uint32_t unsupported_draws = 0;
   uint32_t skipped_draws = 0;
+  uint32_t ordered_from = UINT32_MAX; /* first draw of the blended suffix */
   bool frame_open = false;
   bool pending = false;
   int frame_status = 0;
@@ -137,6 +138,8 @@ struct MopCudaDevice {
       large_list, large_items, shade_list, counters, pick_xy, pick_out;
   HostArena h_draws, h_lights, h_counters, h_pick;
   DevArena deform_params; /* bone matrices / morph weights of a deform call */
+  DevArena hdr, frag_head, frags, touched, olist, olist_items; /* blended suffix */
+  uint32_t frag_hint = 0, olist_hint = 0;
   HostArena h_deform;
   uint32_t vertex_cap = 0, rec_cap = 0, clip_cap = 0, large_cap = 0;
   uint32_t extra_hint = 0, rec_hint = 0, clip_hint = 0, large_hint = 0;

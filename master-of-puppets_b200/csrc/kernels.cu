@@ -643,6 +643,12 @@ __device__ __forceinline__ bool rec_live(const RasterRec &r, int W, int H) {
   return (int)r.x0 <= (int)r.x1 && (int)r.y0 <= y1 && (int)r.x1 < W && y1 < H;
 }
 
+/* Records of the ordered suffix (a blended draw and all after it) are
+ * composited per sample in submission order instead. */
+__device__ __forceinline__ bool rec_ordered(const FrameArgs &a, const RasterRec &r) {
+  return a.hdr != nullptr && (r.order >> ORDER_FAN_BITS) >= a.t_split;
+}
+
 /* Records above the small-record limits (bbox side / area, tunable) are
  * rasterised item-parallel by k_raster_large. */
 __device__ __forceinline__ bool rec_large(const FrameArgs &a, const RasterRec &r) {
@@ -909,7 +915,7 @@ __device__ __forceinline__ uint32_t raster_small_items(const FrameArgs &a) {
 __device__ __forceinline__ void raster_small_item(const FrameArgs &a, uint32_t rid) {
   {
     const RasterRec r = a.rrec[rid];
-    if (!rec_live(r, a.width, a.height) || rec_large(a, r))
+    if (!rec_live(r, a.width, a.height) || rec_large(a, r) || rec_ordered(a, r))
       return;
     const bool flat = (r.y1 & REC_FLAT_BIT) != 0;
     const int y1 = (int)(r.y1 & 0x7fffu);
@@ -937,17 +943,15 @@ __global__ void k_raster_small(FrameArgs a) {
  * next tile's counts loaded before the current one is scanned; part holds
  * >= 32 words. */
 #define LARGE_SCAN_PER 4
-__device__ __forceinline__ void large_scan_block(const FrameArgs &a, uint32_t *part) {
-  uint32_t n = a.ctr->large_count;
-  if (n > a.large_cap)
-    n = a.large_cap;
+__device__ __forceinline__ void items_scan_block(uint32_t *items, uint32_t n, uint32_t *total_out,
+                                                 uint32_t *part) {
   const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
   const uint32_t tile = 1024u * LARGE_SCAN_PER;
   uint32_t nxt[LARGE_SCAN_PER];
 #pragma unroll
   for (int k = 0; k < LARGE_SCAN_PER; k++) {
     const uint32_t i = tid * LARGE_SCAN_PER + (uint32_t)k;
-    nxt[k] = i < n ? a.large_items[i] : 0u;
+    nxt[k] = i < n ? items[i] : 0u;
   }
   uint32_t carry = 0;
   for (uint32_t base = 0; base < n; base += tile) {
@@ -958,7 +962,7 @@ __device__ __forceinline__ void large_scan_block(const FrameArgs &a, uint32_t *p
       v[k] = nxt[k];
       sum += v[k];
       const uint32_t j = base + tile + tid * LARGE_SCAN_PER + (uint32_t)k;
-      nxt[k] = j < n ? a.large_items[j] : 0u;
+      nxt[k] = j < n ? items[j] : 0u;
     }
     uint32_t x = sum; /* inclusive scan of the per-thread sums within the warp */
 #pragma unroll
@@ -987,14 +991,21 @@ __device__ __forceinline__ void large_scan_block(const FrameArgs &a, uint32_t *p
     for (int k = 0; k < LARGE_SCAN_PER; k++) {
       const uint32_t i = base + tid * LARGE_SCAN_PER + (uint32_t)k;
       if (i < n)
-        a.large_items[i] = run;
+        items[i] = run;
       run += v[k];
     }
     carry += total;
     __syncthreads(); /* part is reused by the next tile */
   }
   if (tid == 0)
-    a.ctr->large_items = carry;
+    *total_out = carry;
+}
+
+__device__ __forceinline__ void large_scan_block(const FrameArgs &a, uint32_t *part) {
+  uint32_t n = a.ctr->large_count;
+  if (n > a.large_cap)
+    n = a.large_cap;
+  items_scan_block(a.large_items, n, &a.ctr->large_items, part);
 }
 
 __global__ void __launch_bounds__(1024) k_large_scan(FrameArgs a) {
@@ -1021,7 +1032,7 @@ __device__ __forceinline__ void raster_large_item(const FrameArgs &a, uint32_t i
     if (rid >= a.rec_cap)
       return;
     const RasterRec r = a.rrec[rid];
-    if (!rec_live(r, a.width, a.height))
+    if (!rec_live(r, a.width, a.height) || rec_ordered(a, r))
       return;
     const bool flat = (r.y1 & REC_FLAT_BIT) != 0;
     const uint32_t w = (uint32_t)r.x1 - (uint32_t)r.x0 + 1u;
@@ -1266,6 +1277,8 @@ __device__ __forceinline__ void shade_item(const FrameArgs &a, uint32_t j, const
                             u8_of(aces(hdr[2] * a.exposure) * 255.0f + 0.5f), 255);
     a.depth[px] = depth;
     a.ids[px] = d.object_id;
+    if (a.hdr) /* the blended suffix composites over this colour */
+      a.hdr[px] = make_float4(hdr[0], hdr[1], hdr[2], 1.0f);
   }
 }
 
@@ -1513,6 +1526,11 @@ __global__ void k_pick(const uint32_t *ids, const float *depth, int width, int h
  * ------------------------------------------------------------------------ */
 static inline unsigned blocks_for(uint32_t n, unsigned bs) { return (n + bs - 1u) / bs; }
 
+__global__ void k_ocount(FrameArgs a);
+__global__ void k_oscan(FrameArgs a);
+__global__ void k_oraster(FrameArgs a);
+__global__ void k_ofold(FrameArgs a);
+
 int mopcuda_launch_frame(const FrameArgs &a, const PostArgs &p, const LaunchCfg &cfg,
                          cudaStream_t s, cudaEvent_t *ev) {
   int launches = 0;
@@ -1551,6 +1569,15 @@ int mopcuda_launch_frame(const FrameArgs &a, const PostArgs &p, const LaunchCfg 
   const int waves = cfg.shade_waves > 0 ? cfg.shade_waves : 4;
   k_shade<<<cfg.num_sms * waves, sb, 0, s>>>(a);
   launches += 2;
+  if (a.hdr) { /* blended suffix, composited in submission order */
+    cudaMemsetAsync(a.frag_head, 0xff, sizeof(uint32_t) * (size_t)S, s);
+    const uint32_t nrec = a.rec_cap < (1u << 22) ? a.rec_cap : (1u << 22);
+    k_ocount<<<blocks_for(nrec, 256), 256, 0, s>>>(a);
+    k_oscan<<<1, 1024, 0, s>>>(a);
+    k_oraster<<<cfg.num_sms * 8, 256, 0, s>>>(a);
+    k_ofold<<<cfg.num_sms * 8, 128, 0, s>>>(a);
+    launches += 4;
+  }
   if (ev)
     cudaEventRecord(ev[5], s);
   const int sf = p.ssaa;
@@ -1627,6 +1654,248 @@ int mopcuda_launch_pick(const uint32_t *ids, const float *depth, int width, int 
   return 1;
 }
 
+
+/* ========================================================================
+ * Ordered suffix: blended draws (and every draw after the first one) in
+ * submission order per sample — mop_sw_rasterize_triangle_smooth_ml's
+ * blended branch (rasterizer.c:2094-2140) and the flat opaque path
+ * (:890-1024), which read and write the colour, depth and ID the earlier
+ * fragments left.  The records are rasterised into per-sample fragment
+ * lists (fragments at or behind the opaque pass's depth can never pass: the
+ * depth only decreases), each sample sorts its list by submission order and
+ * folds it sequentially.
+ * ======================================================================== */
+__device__ __forceinline__ uint32_t ordered_record_items(const FrameArgs &a) {
+  return raster_small_items(a);
+}
+
+/* Queue the live records of the suffix with their (row, chunk) counts. */
+__global__ void __launch_bounds__(256) k_ocount(FrameArgs a) {
+  const uint32_t n = ordered_record_items(a);
+  for (uint32_t rid = blockIdx.x * blockDim.x + threadIdx.x; rid < n;
+       rid += gridDim.x * blockDim.x) {
+    const RasterRec r = a.rrec[rid];
+    if (!rec_live(r, a.width, a.height) || !rec_ordered(a, r))
+      continue;
+    const uint32_t q = atomicAdd(&a.ctr->olist_count, 1u);
+    if (q < a.olist_cap) {
+      a.olist[q] = rid;
+      a.olist_items[q] = rec_items(r);
+    } else {
+      atomicOr(&a.ctr->overflow, 32u);
+    }
+  }
+}
+
+__global__ void __launch_bounds__(1024) k_oscan(FrameArgs a) {
+  __shared__ uint32_t part[32];
+  uint32_t n = a.ctr->olist_count;
+  if (n > a.olist_cap)
+    n = a.olist_cap;
+  items_scan_block(a.olist_items, n, &a.ctr->olist_items, part);
+}
+
+__device__ __forceinline__ void push_fragment(const FrameArgs &a, uint32_t px, uint32_t order) {
+  const uint32_t node = atomicAdd(&a.ctr->frag_count, 1u);
+  if (node >= a.frag_cap) {
+    atomicOr(&a.ctr->overflow, 16u);
+    return;
+  }
+  const uint32_t prev = atomicExch(&a.frag_head[px], node);
+  a.frags[node] = make_uint2(prev, order);
+  if (prev == 0xffffffffu) /* first fragment of this sample */
+    a.touched[atomicAdd(&a.ctr->touched_count, 1u)] = px;
+}
+
+/* One (row, 32-sample chunk) item of a suffix record: the reference's edge
+ * walk from the folded chunk start; covered samples in front of the opaque
+ * depth get a fragment. */
+__global__ void __launch_bounds__(256) k_oraster(FrameArgs a) {
+  uint32_t nl = a.ctr->olist_count;
+  if (nl > a.olist_cap)
+    nl = a.olist_cap;
+  const uint32_t total = a.ctr->olist_items;
+  for (uint32_t it = blockIdx.x * blockDim.x + threadIdx.x; it < total;
+       it += gridDim.x * blockDim.x) {
+    uint32_t lo = 0, hi = nl;
+    while (hi - lo > 1) {
+      const uint32_t mid = (lo + hi) >> 1;
+      if (a.olist_items[mid] <= it)
+        lo = mid;
+      else
+        hi = mid;
+    }
+    const uint32_t rid = a.olist[lo];
+    if (rid >= a.rec_cap)
+      continue;
+    const RasterRec r = a.rrec[rid];
+    const bool flat = (r.y1 & REC_FLAT_BIT) != 0;
+    const uint32_t wd = (uint32_t)r.x1 - (uint32_t)r.x0 + 1u;
+    const uint32_t chunks = (wd + RASTER_CHUNK - 1u) / RASTER_CHUNK;
+    const uint32_t local = it - a.olist_items[lo];
+    const int jr = (int)(local / chunks), kc = (int)((local % chunks) * RASTER_CHUNK);
+    const int y = (int)r.y0 + jr;
+    if (y > (int)(r.y1 & 0x7fffu))
+      continue;
+    const int xs = (int)r.x0 + kc, xe = min((int)r.x1, xs + RASTER_CHUNK - 1);
+    float w0 = fold_add(fold_add(r.w0[0], r.dy[0], jr), r.dx[0], kc);
+    float w1 = fold_add(fold_add(r.w0[1], r.dy[1], jr), r.dx[1], kc);
+    float w2 = fold_add(fold_add(r.w0[2], r.dy[2], jr), r.dx[2], kc);
+    float z = flat ? fold_add(fold_add(r.zc[0], r.zc[2], jr), r.zc[1], kc) : 0.0f;
+    const uint32_t rowbase = (uint32_t)y * (uint32_t)a.width;
+    for (int x = xs; x <= xe; x++) {
+      if (w0 >= 0.0f && w1 >= 0.0f && w2 >= 0.0f) {
+        float zz = z;
+        if (!flat) {
+          const float b0 = w0 * r.inv_area, b1 = w1 * r.inv_area, b2 = w2 * r.inv_area;
+          zz = b0 * r.zc[0] + b1 * r.zc[1] + b2 * r.zc[2];
+        }
+        const uint32_t px = rowbase + (uint32_t)x;
+        if (zz < a.depth[px])
+          push_fragment(a, px, r.order);
+      }
+      w0 = __fadd_rn(w0, r.dx[0]);
+      w1 = __fadd_rn(w1, r.dx[1]);
+      w2 = __fadd_rn(w2, r.dx[2]);
+      if (flat)
+        z = __fadd_rn(z, r.zc[1]);
+    }
+  }
+}
+
+/* The record behind an order (triangle << 5 | fan), as shade_item finds it. */
+__device__ __forceinline__ uint32_t record_of(const FrameArgs &a, uint32_t order) {
+  const uint32_t t = order >> ORDER_FAN_BITS, fan = order & ((1u << ORDER_FAN_BITS) - 1u);
+  if (t >= a.total_tris)
+    return 0xffffffffu;
+  const RasterRec r = a.rrec[t];
+  if (r.y0 == REC_REDIRECT)
+    return r.order + fan;
+  return fan == 0u ? t : 0xffffffffu;
+}
+
+__global__ void __launch_bounds__(128) k_ofold(FrameArgs a) {
+  const uint32_t n = a.ctr->touched_count;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const uint32_t px = a.touched[i];
+    uint32_t ord[ORDERED_MAX_FRAGS];
+    uint32_t cnt = 0, total = 0;
+    for (uint32_t node = a.frag_head[px]; node != 0xffffffffu && node < a.frag_cap;
+         node = a.frags[node].x) {
+      if (cnt < ORDERED_MAX_FRAGS)
+        ord[cnt++] = a.frags[node].y;
+      if (++total > a.frag_cap)
+        break;
+    }
+    if (total > ORDERED_MAX_FRAGS)
+      atomicOr(&a.ctr->overflow, 64u); /* the frame is reported unsupported */
+    for (uint32_t k = 1; k < cnt; k++) { /* submission order */
+      const uint32_t v = ord[k];
+      uint32_t j = k;
+      while (j > 0 && ord[j - 1] > v) {
+        ord[j] = ord[j - 1];
+        j--;
+      }
+      ord[j] = v;
+    }
+    const int x = (int)(px % (uint32_t)a.width), y = (int)(px / (uint32_t)a.width);
+    const bool covered = a.keys[px] != KEY_EMPTY;
+    float hdr[3];
+    if (covered) {
+      const float4 h = a.hdr[px];
+      hdr[0] = h.x;
+      hdr[1] = h.y;
+      hdr[2] = h.z;
+    } else {
+      hdr[0] = a.clear[0];
+      hdr[1] = a.clear[1];
+      hdr[2] = a.clear[2];
+    }
+    float depth = a.depth[px];
+    uint32_t id = a.ids[px];
+    for (uint32_t k = 0; k < cnt; k++) {
+      const uint32_t rid = record_of(a, ord[k]);
+      if (rid >= a.rec_cap)
+        continue;
+      const RasterRec r = a.rrec[rid];
+      const ShadeRec s = a.srec[rid];
+      const DrawRec &d = a.draws[s.draw < a.draw_count ? s.draw : 0];
+      const int jr = y - (int)r.y0, kc = x - (int)r.x0;
+      if (r.y1 & REC_FLAT_BIT) { /* flat: opaque only */
+        const float z = fold_add(fold_add(r.zc[0], r.zc[2], jr), r.zc[1], kc);
+        if (z < depth) {
+          hdr[0] = s.col[0];
+          hdr[1] = s.col[1];
+          hdr[2] = s.col[2];
+          depth = z;
+          id = d.object_id;
+        }
+        continue;
+      }
+      float w[3];
+      for (int e = 0; e < 3; e++)
+        w[e] = fold_add(fold_add(r.w0[e], r.dy[e], jr), r.dx[e], kc);
+      const float b0 = w[0] * r.inv_area, b1 = w[1] * r.inv_area, b2 = w[2] * r.inv_area;
+      const float z = b0 * r.zc[0] + b1 * r.zc[1] + b2 * r.zc[2];
+      if (!(z < depth))
+        continue;
+      if (s.v[0] >= a.vertex_cap || s.v[1] >= a.vertex_cap || s.v[2] >= a.vertex_cap)
+        continue;
+      const float4 N[3] = {a.normal[s.v[0]], a.normal[s.v[1]], a.normal[s.v[2]]};
+      float pc[3] = {b0 * N[0].w, b1 * N[1].w, b2 * N[2].w};
+      const float ip = 1.0f / (pc[0] + pc[1] + pc[2]);
+      pc[0] *= ip;
+      pc[1] *= ip;
+      pc[2] *= ip;
+      float p[3];
+      shade_smooth(a, d, a.lights + d.light_off, s.v, N, pc, p);
+      /* edge-distance coverage (rasterizer.c:1899-1938) */
+      float min_d = 0.0f;
+      for (int e = 0; e < 3; e++) {
+        const float len = sqrtf(r.dx[e] * r.dx[e] + r.dy[e] * r.dy[e]);
+        const float inv = len > 1e-6f ? 1.0f / len : 0.0f;
+        const float de = w[e] * inv;
+        if (e == 0 || de < min_d)
+          min_d = de;
+      }
+      const float op = d.opacity < 0.0f ? 0.0f : (d.opacity > 1.0f ? 1.0f : d.opacity);
+      const float cov = (min_d < 1.0f && d.blend_mode != 0) ? min_d : 1.0f;
+      const float fa = op * cov;
+      if (d.blend_mode == 0 && fa >= 1.0f) {
+        hdr[0] = p[0];
+        hdr[1] = p[1];
+        hdr[2] = p[2];
+        depth = z;
+        id = d.object_id;
+      } else {
+        const float inv = 1.0f - fa;
+        for (int c = 0; c < 3; c++) {
+          if (d.blend_mode == 2)
+            hdr[c] = hdr[c] + p[c] * fa;
+          else if (d.blend_mode == 3)
+            hdr[c] = hdr[c] * p[c];
+          else
+            hdr[c] = p[c] * fa + hdr[c] * inv;
+        }
+        if (fa > 0.5f) {
+          depth = z;
+          id = d.object_id;
+        }
+      }
+    }
+    /* mop_sw_hdr_resolve (rasterizer.c:2776-2803) of the composited sample */
+    if (id == 0u)
+      a.pre[px] = make_uchar4(x86_f2u8(fminf(hdr[0], 1.0f) * 255.0f + 0.5f),
+                              x86_f2u8(fminf(hdr[1], 1.0f) * 255.0f + 0.5f),
+                              x86_f2u8(fminf(hdr[2], 1.0f) * 255.0f + 0.5f), 255);
+    else
+      a.pre[px] = make_uchar4(u8_of(aces(hdr[0] * a.exposure) * 255.0f + 0.5f),
+                              u8_of(aces(hdr[1] * a.exposure) * 255.0f + 0.5f),
+                              u8_of(aces(hdr[2] * a.exposure) * 255.0f + 0.5f), 255);
+    a.depth[px] = depth;
+    a.ids[px] = id;
+  }
+}
 
 /* ========================================================================
  * Batched viewports.  One launch per stage covers every viewport of a batch

@@ -18,6 +18,7 @@
 #include <string.h>
 #include <time.h>
 
+#include <algorithm>
 #include <mutex>
 #include <vector>
 
@@ -141,7 +142,8 @@ extern "C" void mopcuda_device_destroy(MopCudaDevice *d) {
                         &d->color,    &d->rrec,       &d->srec,
                         &d->clipq,    &d->keys,       &d->large_list,  &d->large_items,
                         &d->shade_list, &d->counters, &d->pick_xy,     &d->pick_out,
-                        &d->deform_params};
+                        &d->deform_params, &d->hdr, &d->frag_head, &d->frags, &d->touched,
+                        &d->olist, &d->olist_items};
   for (DevArena *a : arenas)
     a->release();
   d->h_draws.release();
@@ -529,6 +531,7 @@ extern "C" int mopcuda_frame_begin(MopCudaDevice *d, MopCudaFramebuffer *fb, con
   d->lights.clear();
   d->unsupported_draws = 0;
   d->skipped_draws = 0;
+  d->ordered_from = UINT32_MAX;
   d->frame_open = true;
   return MOPCUDA_OK;
 }
@@ -550,11 +553,15 @@ int mc_build_draw(const MopCudaDraw *c, const float *model, const float *mvp,
     return MOPCUDA_OK;
   }
   bool lit = c->lights && c->light_count > 0;
-  if (c->wireframe || !c->depth_test || !c->depth_write || c->blend_mode != 0 || op < 1.0f ||
-      (c->smooth && !lit)) {
+  /* Supported: opaque draws (order-independent) and blended lit smooth
+   * draws (composited per sample in submission order).  Wireframe lines,
+   * depth test or write off, unlit smooth (edge-AA) and blended flat draws
+   * are not built. */
+  if (c->wireframe || !c->depth_test || !c->depth_write || (c->smooth && !lit) ||
+      (!c->smooth && (c->blend_mode != 0 || op < 1.0f))) {
     return fail(MOPCUDA_EUNSUPPORTED,
-                "draw: blended / wireframe / depth-test-off / unlit-smooth state is not on "
-                "the order-independent path");
+                "draw: wireframe / depth-test-off / depth-write-off / unlit-smooth / blended "
+                "flat state is not implemented");
   }
   uint32_t stride = 48;
   memset(&r, 0, sizeof r);
@@ -588,6 +595,7 @@ int mc_build_draw(const MopCudaDraw *c, const float *model, const float *mvp,
     return fail(MOPCUDA_EINVAL, "draw: index_count exceeds the index buffer");
   memcpy(r.mvp, mvp, sizeof r.mvp);
   memcpy(r.model, model, sizeof r.model);
+  r.blend_mode = c->blend_mode;
   memcpy(r.light_dir, c->light_dir, sizeof r.light_dir);
   r.ambient = c->ambient;
   r.opacity = c->opacity;
@@ -680,10 +688,14 @@ static int record_draw(MopCudaDevice *d, const MopCudaDraw *c, const float *mode
     d->unsupported_draws++;
   if (rc)
     return rc;
-  if (skip)
+  if (skip) {
     d->skipped_draws++;
-  else
-    d->draws.push_back(r);
+    return MOPCUDA_OK;
+  }
+  /* the first blended draw starts the ordered suffix of the frame */
+  if ((r.blend_mode != 0 || clamp01f(r.opacity) < 1.0f) && d->ordered_from == UINT32_MAX)
+    d->ordered_from = (uint32_t)d->draws.size();
+  d->draws.push_back(r);
   return MOPCUDA_OK;
 }
 
@@ -835,6 +847,20 @@ static int launch_frame(MopCudaDevice *d) {
   rc |= d->h_draws.ensure(sizeof(DrawRec) * (nd ? nd : 1));
   rc |= d->h_lights.ensure(sizeof(LightRec) * (d->lights.size() + 1));
   rc |= d->h_counters.ensure(sizeof(Counters));
+  /* blended suffix: per-sample composition buffers and fragment lists */
+  const bool ordered = d->ordered_from < nd;
+  const uint32_t t_split = ordered ? d->draws[d->ordered_from].tbase : (uint32_t)T;
+  uint32_t fcap = 0, ocap = 0;
+  if (ordered) {
+    fcap = (uint32_t)std::min<size_t>(std::max<size_t>(d->frag_hint, S + 65536), 0xfffffff0u);
+    ocap = std::max<uint32_t>(d->olist_hint, (uint32_t)(T - t_split) + fan_cap);
+    rc |= d->hdr.ensure(16ull * S);
+    rc |= d->frag_head.ensure(4ull * S);
+    rc |= d->touched.ensure(4ull * S);
+    rc |= d->frags.ensure(8ull * fcap);
+    rc |= d->olist.ensure(4ull * ocap);
+    rc |= d->olist_items.ensure(4ull * ocap);
+  }
   if (rc)
     return MOPCUDA_ENOMEM;
   d->vertex_cap = vcap;
@@ -893,6 +919,17 @@ static int launch_frame(MopCudaDevice *d) {
   a.ids = fb->ids.as<uint32_t>();
   a.small_side = d->cfg.small_side;
   a.small_area = d->cfg.small_area;
+  if (ordered) {
+    a.t_split = t_split;
+    a.hdr = d->hdr.as<float4>();
+    a.frag_head = d->frag_head.as<uint32_t>();
+    a.frags = d->frags.as<uint2>();
+    a.frag_cap = fcap;
+    a.touched = d->touched.as<uint32_t>();
+    a.olist = d->olist.as<uint32_t>();
+    a.olist_items = d->olist_items.as<uint32_t>();
+    a.olist_cap = ocap;
+  }
 
   PostArgs p;
   mc_post_args(d, p);
@@ -962,6 +999,13 @@ static int finish_frame(MopCudaDevice *d, int timeout_ms) {
     d->clip_hint = c->clip_count + c->clip_count / 4 + 1024;
     d->extra_hint = c->extra_vertices + c->extra_vertices / 4 + 1024;
     d->large_hint = c->large_count + c->large_count / 4 + 1024;
+    if (c->overflow & 64u)
+      return fail(MOPCUDA_EUNSUPPORTED, "frame: more than %d blended fragments on one sample",
+                  ORDERED_MAX_FRAGS);
+    if (c->overflow & 16u)
+      d->frag_hint = c->frag_count + c->frag_count / 4 + 65536;
+    if (c->overflow & 32u)
+      d->olist_hint = c->olist_count + c->olist_count / 4 + 1024;
     if (c->overflow & 1u)
       d->rec_hint *= 2;
     if (c->overflow & 2u)

@@ -62,6 +62,7 @@ struct DrawRec {
    * roughness (offset in texels, size) and the BRDF LUT row */
   uint32_t pf_off;
   int32_t pf_lw, pf_lh, brdf_row;
+  int32_t blend_mode; /* MopBlendMode: 0 opaque, 1 alpha, 2 additive, 3 multiply */
 };
 
 struct LightRec {
@@ -114,8 +115,15 @@ struct Counters {
   uint32_t overflow;          /* bit0 records, bit1 extra vertices, bit2 clip
                                  queue, bit3 large list                          */
   uint32_t shade_count;       /* covered samples queued for shading              */
+  /* ordered (blended) suffix of the frame; overflow bit4 fragment pool,
+   * bit5 ordered-record list, bit6 more than ORDERED_MAX_FRAGS fragments on
+   * one sample */
+  uint32_t frag_count, touched_count, olist_count, olist_items;
   uint32_t pad;
 };
+
+/* Blended fragments one sample may receive in a frame. */
+#define ORDERED_MAX_FRAGS 48
 
 /* Records whose clamped bbox exceeds these bounds are rasterised as
  * (row, RASTER_CHUNK-sample) items spread over many threads; smaller ones
@@ -171,6 +179,18 @@ struct FrameArgs {
   int small_side, small_area;
   /* visibility only: shading writes depth and IDs but no colour */
   int no_color;
+  /* ordered suffix: triangles t >= t_split (a blended draw and everything
+   * after it) are composited per sample in submission order instead of
+   * entering the visibility keys; hdr != null when the frame has one */
+  uint32_t t_split;
+  float4 *hdr;            /* per sample: the opaque pass's colour before ACES */
+  uint32_t *frag_head;    /* per sample: first fragment, 0xffffffff = none      */
+  uint2 *frags;           /* fragment: (next, order)                            */
+  uint32_t frag_cap;
+  uint32_t *touched;      /* samples that received a fragment                   */
+  uint32_t *olist;        /* live records of the suffix                          */
+  uint32_t *olist_items;  /* their (row, chunk) item counts, then offsets        */
+  uint32_t olist_cap;
 };
 
 struct PostArgs {

@@ -354,7 +354,7 @@ class _Resident:
         dr.smooth = 1 if getattr(sc, "smooth", True) else 0
         dr.wireframe = 0
         dr.depth_test = dr.depth_write = dr.backface_cull = 1
-        dr.blend_mode = 0
+        dr.blend_mode = getattr(m, "blend_mode", 0) or (1 if m.opacity < 1.0 else 0)
         dr.texture = self.textures[m.texture] if m.texture >= 0 else None
         dr.lights = self.lights
         dr.light_count = len(sc.lights)
@@ -402,9 +402,11 @@ class SceneRenderer(_Resident):
         self.update_camera()
 
     def update_camera(self):
+        import scenes
         self.view, self.proj, self.eye = camera_matrices(self.scene)
+        # the core's pass order: opaque meshes, then blended ones back to front
         self.draws = [self.draw_struct(k, self.view, self.proj, self.eye)
-                      for k in range(len(self.meshes))]
+                      for k in scenes.draw_order(self.scene, self.eye)]
 
     def submit(self):
         """Record and launch one frame (asynchronous)."""

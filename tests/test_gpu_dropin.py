@@ -29,6 +29,9 @@ CASES = {
     "ssaa2": lambda: scenes.small_scene(seed=22, width=160, height=120, ssaa=2),
     "flat": lambda: dataclasses.replace(scenes.small_scene(seed=23), smooth=False),
     "coplanar": lambda: scenes.coplanar_scene(seed=24),
+    # blended meshes: the core's own transparent pass drives the ordered path
+    "transparent": lambda: scenes.transparent_scene(seed=25),
+    "transparent_ssaa2": lambda: scenes.transparent_scene(seed=26, width=128, height=96, ssaa=2),
     "config2_reduced_no_ibl": lambda: dataclasses.replace(
         scenes.config2(width=480, height=270, ssaa=2, instances=48, tex_size=64), env=0),
 }

@@ -6,7 +6,8 @@ IDs and depth must match bit for bit; colour within the contract tolerance
 point, spot, ranged, inactive lights), textures, SSAA 2, IBL, flat shading
 (lit and unlit), near-plane clipping (the config-1 ground plane passes
 behind the camera), coplanar draw-order ties, the clipping/depth stress scene
-(near-plane straddlers, coplanar pairs, host-skinned meshes), and picks.
+(near-plane straddlers, coplanar pairs, host-skinned meshes), blended meshes
+(alpha, additive, multiply) in the core's transparent-pass order, and picks.
 """
 import dataclasses
 
@@ -58,7 +59,19 @@ CASES = {
     # in separate meshes, host-skinned tubes, 0.1-8 px triangles
     "config3_reduced": lambda: scenes.config3(n_tris=80_000, width=480, height=270),
     "config3_medium": lambda: scenes.config3(seed=4, n_tris=400_000, width=960, height=540),
+    # blended meshes (alpha / additive / multiply), composited in submission order
+    "transparent": lambda: scenes.transparent_scene(seed=21),
+    "transparent_ssaa2_ibl": lambda: scenes.transparent_scene(seed=22, ssaa=2, env=1),
+    "transparent_config2": lambda: _transparent_config2(),
 }
+
+
+def _transparent_config2():
+    sc = scenes.config2(width=320, height=180, ssaa=2, instances=32, tex_size=64)
+    for k in range(0, len(sc.meshes), 3):  # every third instance blended
+        sc.meshes[k] = dataclasses.replace(sc.meshes[k], opacity=0.35 + 0.1 * (k % 5),
+                                           blend_mode=(1, 2, 3, 1)[k % 4])
+    return sc
 
 
 @pytest.mark.parametrize("name", list(CASES))
