@@ -189,6 +189,28 @@ int mopcuda_set_ibl(MopCudaDevice *dev, const float *irradiance, int iw, int ih,
                     const float *prefiltered, int pw, int ph, int levels,
                     const float *brdf_lut, int brdf_size, float rotation, float intensity);
 
+/* ---- shadow map (pass_shadow, viewport.c:2288-2442, which the core runs
+ *      for its CPU backend only; mop_sw_shadow_render_mesh,
+ *      rasterizer.c:357-493; mop_sw_shadow_set / _clear, rasterizer.c:146-157)
+ *
+ * shadow_begin opens a pass of a size x size depth map (the core uses 1024)
+ * for the light view-projection light_vp; shadow_draw adds one caster (the
+ * core passes every active opaque mesh below the chrome IDs, in mesh order:
+ * its vertex buffer with positions as float3 at offset 0 of each `stride`-
+ * byte vertex, 48 for MopVertex, its index buffer and world transform);
+ * shadow_end rasterises the casters on the device stream and binds the map
+ * for this device's later frames, where every directional light's diffuse
+ * and specular terms take the 3x3 PCF factor (rasterizer.c:303-348,
+ * 1580-1583, 1677-1680, 1802-1805) until shadow_clear. */
+int mopcuda_shadow_begin(MopCudaDevice *dev, int size, const float light_vp[16]);
+int mopcuda_shadow_draw(MopCudaDevice *dev, const MopCudaBuffer *vertices, uint32_t vertex_count,
+                        uint32_t stride, const MopCudaBuffer *indices, uint32_t index_count,
+                        const float model[16]);
+int mopcuda_shadow_end(MopCudaDevice *dev);
+int mopcuda_shadow_clear(MopCudaDevice *dev);
+/* The bound map as depth values (size * size floats, row-major). */
+int mopcuda_shadow_read(MopCudaDevice *dev, float *depth, size_t bytes);
+
 /* ---- frame commands: frame_begin/end/submit, draw, draw_instanced
  *      (rhi.h:160-175, 214-218), cpu_backend.c:197-211, 528-657 -------- */
 int mopcuda_frame_begin(MopCudaDevice *dev, MopCudaFramebuffer *fb, const float clear_rgba[4]);
@@ -433,6 +455,13 @@ void mopcuda_mat4_compose_trs(const float position[3], const float rotation[3],
 void mopcuda_camera_matrices(const float eye[3], const float target[3], const float up[3],
                              float fov_deg, float near_plane, float far_plane, int width,
                              int height, float view[16], float proj[16], float eye_out[3]);
+/* The shadow pass's light view-projection (viewport.c:2303-2427): a scene
+ * box from the casters' world transforms (translation +- 1.5 x the largest
+ * column length), an orthographic light camera looking along `direction`
+ * from twice the box radius.  Returns 0 (and leaves light_vp alone) when
+ * count is 0, 1 otherwise. */
+int mopcuda_shadow_light_vp(const float *models, uint32_t count, const float direction[3],
+                            float light_vp[16]);
 
 #ifdef __cplusplus
 }

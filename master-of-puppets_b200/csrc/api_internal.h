@@ -141,6 +141,16 @@ struct MopCudaDevice {
   DevArena hdr, frag_head, frags, touched, olist, olist_items; /* blended suffix */
   uint32_t frag_hint = 0, olist_hint = 0;
   HostArena h_deform;
+  /* shadow pass: casters recorded between shadow_begin and shadow_end; the
+   * map then stays bound for the device's frames until shadow_clear */
+  std::vector<ShadowDraw> sh_draws;
+  bool sh_open = false, sh_bound = false;
+  int sh_rec_size = 0, sh_size = 0;
+  float sh_rec_vp[16] = {};
+  DevArena sh_map, sh_d_draws, sh_recs, sh_items, sh_ctr;
+  HostArena sh_h_draws;
+  cudaEvent_t sh_ev = nullptr; /* after the caster table's upload */
+  bool sh_ev_live = false;
   uint32_t vertex_cap = 0, rec_cap = 0, clip_cap = 0, large_cap = 0;
   uint32_t extra_hint = 0, rec_hint = 0, clip_hint = 0, large_hint = 0;
   LaunchCfg cfg = {148, SMALL_MAX_SIDE, SMALL_MAX_AREA, 128, 256, 4, 32, 4};

@@ -10,6 +10,7 @@
  *   camera chain                 mop_viewport_set_camera viewport.c:1058-1093,
  *                                orbit re-application each frame
  *                                camera.c:35-63 -> viewport.c:1095-1128
+ *   ortho, shadow light camera   math.c:93-109, pass_shadow viewport.c:2303-2427
  * sinf/cosf/tanf/atan2f/asinf are the host C library's, as in the reference.
  * Compiled with -ffp-contract=off (no FMA contraction).
  */
@@ -97,6 +98,26 @@ static v3 cross(v3 a, v3 b) {
   return r;
 }
 
+/* mop_mat4_look_at, math.c:111-130 */
+static void look_at(v3 e, v3 t, v3 u, float view[16]) {
+  v3 f = unit((v3){t.x - e.x, t.y - e.y, t.z - e.z});
+  v3 s = unit(cross(f, u));
+  v3 uu = cross(s, f);
+  ident(view);
+  E(view, 0, 0) = s.x;
+  E(view, 0, 1) = s.y;
+  E(view, 0, 2) = s.z;
+  E(view, 1, 0) = uu.x;
+  E(view, 1, 1) = uu.y;
+  E(view, 1, 2) = uu.z;
+  E(view, 2, 0) = -f.x;
+  E(view, 2, 1) = -f.y;
+  E(view, 2, 2) = -f.z;
+  E(view, 0, 3) = -dot(s, e);
+  E(view, 1, 3) = -dot(uu, e);
+  E(view, 2, 3) = dot(f, e);
+}
+
 void mopcuda_camera_matrices(const float eye[3], const float target[3], const float up[3],
                              float fov_deg, float near_plane, float far_plane, int width,
                              int height, float view[16], float proj[16], float eye_out[3]) {
@@ -116,22 +137,7 @@ void mopcuda_camera_matrices(const float eye[3], const float target[3], const fl
              t.z + dist * cp2 * cosf(yaw)};
     e = oe;
   }
-  v3 f = unit((v3){t.x - e.x, t.y - e.y, t.z - e.z});
-  v3 s = unit(cross(f, u));
-  v3 uu = cross(s, f);
-  ident(view);
-  E(view, 0, 0) = s.x;
-  E(view, 0, 1) = s.y;
-  E(view, 0, 2) = s.z;
-  E(view, 1, 0) = uu.x;
-  E(view, 1, 1) = uu.y;
-  E(view, 1, 2) = uu.z;
-  E(view, 2, 0) = -f.x;
-  E(view, 2, 1) = -f.y;
-  E(view, 2, 2) = -f.z;
-  E(view, 0, 3) = -dot(s, e);
-  E(view, 1, 3) = -dot(uu, e);
-  E(view, 2, 3) = dot(f, e);
+  look_at(e, t, u, view);
   float fov = fov_deg * (3.14159265358979323846f / 180.0f);
   float aspect = (float)width / (float)height;
   float th = tanf(fov * 0.5f);
@@ -144,4 +150,63 @@ void mopcuda_camera_matrices(const float eye[3], const float target[3], const fl
   eye_out[0] = e.x;
   eye_out[1] = e.y;
   eye_out[2] = e.z;
+}
+
+/* mop_mat4_ortho, math.c:93-109 */
+static void ortho(float l, float r, float b, float t, float n, float f, float m[16]) {
+  float rl = r - l, tb = t - b, fn = f - n;
+  if (fabsf(rl) < 1e-9f || fabsf(tb) < 1e-9f || fabsf(fn) < 1e-9f) {
+    ident(m);
+    return;
+  }
+  memset(m, 0, 16 * sizeof(float));
+  E(m, 0, 0) = 2.0f / rl;
+  E(m, 1, 1) = 2.0f / tb;
+  E(m, 2, 2) = -2.0f / fn;
+  E(m, 0, 3) = -(r + l) / rl;
+  E(m, 1, 3) = -(t + b) / tb;
+  E(m, 2, 3) = -(f + n) / fn;
+  E(m, 3, 3) = 1.0f;
+}
+
+/* pass_shadow's light camera, viewport.c:2303-2427 */
+int mopcuda_shadow_light_vp(const float *models, uint32_t count, const float direction[3],
+                            float light_vp[16]) {
+  if (!models || !direction || !light_vp || count == 0)
+    return 0;
+  float lo[3] = {1e9f, 1e9f, 1e9f}, hi[3] = {-1e9f, -1e9f, -1e9f};
+  for (uint32_t i = 0; i < count; i++) {
+    const float *m = models + 16 * (size_t)i;
+    const float c[3] = {m[12], m[13], m[14]};
+    float sx = sqrtf(m[0] * m[0] + m[1] * m[1] + m[2] * m[2]);
+    float sy = sqrtf(m[4] * m[4] + m[5] * m[5] + m[6] * m[6]);
+    float sz = sqrtf(m[8] * m[8] + m[9] * m[9] + m[10] * m[10]);
+    float r = sx > sy ? sx : sy;
+    if (sz > r)
+      r = sz;
+    r *= 1.5f;
+    for (int k = 0; k < 3; k++)
+      if (c[k] - r < lo[k])
+        lo[k] = c[k] - r;
+    for (int k = 0; k < 3; k++)
+      if (c[k] + r > hi[k])
+        hi[k] = c[k] + r;
+  }
+  v3 d = unit((v3){direction[0], direction[1], direction[2]});
+  v3 ctr = {(lo[0] + hi[0]) * 0.5f, (lo[1] + hi[1]) * 0.5f, (lo[2] + hi[2]) * 0.5f};
+  float dx = hi[0] - lo[0], dy = hi[1] - lo[1], dz = hi[2] - lo[2];
+  float radius = sqrtf(dx * dx + dy * dy + dz * dz) * 0.5f;
+  if (radius < 1.0f)
+    radius = 1.0f;
+  v3 eye = {ctr.x - d.x * radius * 2.0f, ctr.y - d.y * radius * 2.0f,
+            ctr.z - d.z * radius * 2.0f};
+  v3 up = {0.0f, 1.0f, 0.0f};
+  if (fabsf(dot(d, up)) > 0.99f)
+    up = (v3){1.0f, 0.0f, 0.0f};
+  float view[16], proj[16];
+  look_at(eye, ctr, up, view);
+  float size = radius * 1.2f;
+  ortho(-size, size, -size, size, 0.1f, radius * 4.0f, proj);
+  mopcuda_mat4_multiply(proj, view, light_vp);
+  return 1;
 }

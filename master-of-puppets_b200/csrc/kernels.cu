@@ -192,8 +192,60 @@ __device__ __forceinline__ float spot_cone(const LightRec &L, V3 dir) {
   return 1.0f;
 }
 
-/* compute_multi_light (flat path), rasterizer.c:1497-1588 */
-__device__ float diffuse_flat(V3 n, V3 wp, const LightRec *Ls, uint32_t cnt, float amb) {
+/* Shadow-map texel from its key: 0xffffffff is the cleared value 1.0,
+ * otherwise the inverse of depth_key. */
+__device__ __forceinline__ float shadow_texel(uint32_t k) {
+  if (k == 0xffffffffu)
+    return 1.0f;
+  return __uint_as_float((k & 0x80000000u) ? (k & 0x7fffffffu) : ~k);
+}
+
+/* shadow_test_pcf, rasterizer.c:303-348: the world position through the
+ * light's view-projection, 3x3 texels around the truncated texel coordinate
+ * (out-of-map texels count as lit), lit when ndc z <= texel + 0.005; the
+ * result is lit / 9.  The texel coordinate converts as the x86 build does
+ * (cvttss2si); the neighbour offsets are taken in 64 bits so INT_MIN +- 1
+ * stays out of the map. */
+__device__ __noinline__ float shadow_pcf_at(const uint32_t *__restrict__ keys,
+                                           const float *__restrict__ vp, int sw, int sh,
+                                           float px, float py, float pz) {
+  const float4 lp = xform(vp, px, py, pz, 1.0f);
+  if (lp.w <= 0.0f)
+    return 1.0f;
+  const float inv_w = 1.0f / lp.w;
+  const float ndcx = lp.x * inv_w;
+  const float ndcy = lp.y * inv_w;
+  const float ndcz = (lp.z * inv_w + 1.0f) * 0.5f;
+  const float u = (ndcx + 1.0f) * 0.5f * (float)sw;
+  const float v = (1.0f - ndcy) * 0.5f * (float)sh;
+  const long long cx = x86_f2i(u), cy = x86_f2i(v);
+  int lit = 0;
+  for (int dy = -1; dy <= 1; dy++) {
+    for (int dx = -1; dx <= 1; dx++) {
+      const long long sx = cx + dx, sy = cy + dy;
+      if (sx < 0 || sx >= sw || sy < 0 || sy >= sh) {
+        lit++;
+        continue;
+      }
+      const float sz = shadow_texel(__ldg(keys + (size_t)sy * (size_t)sw + sx));
+      if (ndcz <= sz + 0.005f)
+        lit++;
+    }
+  }
+  return (float)lit / 9.0f;
+}
+
+/* Kept out of line: frames without a shadow map never call it, and the
+ * shading loops keep their registers. */
+__device__ __forceinline__ float shadow_pcf(const FrameArgs &a, V3 wp) {
+  return shadow_pcf_at(a.shadow_keys, a.shadow_vp, a.shadow_w, a.shadow_h, wp.x, wp.y, wp.z);
+}
+
+/* compute_multi_light (flat path), rasterizer.c:1497-1588; directional
+ * lights are shadowed when a shadow map is bound (:1580-1583). */
+template <bool SH>
+__device__ float diffuse_flat(const FrameArgs &a, V3 n, V3 wp, const LightRec *Ls, uint32_t cnt,
+                              float amb) {
   float total = amb;
   for (uint32_t i = 0; i < cnt; i++) {
     const LightRec &L = Ls[i];
@@ -227,7 +279,8 @@ __device__ float diffuse_flat(V3 n, V3 wp, const LightRec *Ls, uint32_t cnt, flo
     }
     if (ndotl < 0.0f)
       ndotl = 0.0f;
-    total += ndotl * L.intensity * att * spot * 1.0f;
+    const float shadow = (SH && L.type == 0) ? shadow_pcf(a, wp) : 1.0f;
+    total += ndotl * L.intensity * att * spot * shadow;
   }
   return clamp01(total);
 }
@@ -238,8 +291,10 @@ __device__ float diffuse_flat(V3 n, V3 wp, const LightRec *Ls, uint32_t cnt, flo
  * to-light vector, distance, direction, N.L and inverse-square / range
  * falloff from the same operands in the same order, so those values are
  * computed once here; each helper's own accumulation order is unchanged. */
-__device__ void lights_smooth(V3 n, V3 wp, V3 vdir, const LightRec *Ls, const DrawRec &d,
-                              const float base[3], float lit[3], float spec[3]) {
+template <bool SH>
+__device__ void lights_smooth(const FrameArgs &a, V3 n, V3 wp, V3 vdir, const LightRec *Ls,
+                              const DrawRec &d, const float base[3], float lit[3],
+                              float spec[3]) {
   lit[0] = lit[1] = lit[2] = d.ambient;
   spec[0] = spec[1] = spec[2] = 0.0f;
   const float alpha2 = d.alpha2, k = d.smith_k, omk = d.one_minus_k;
@@ -277,9 +332,12 @@ __device__ void lights_smooth(V3 n, V3 wp, V3 vdir, const LightRec *Ls, const Dr
       ldir = mk3(0.0f, 0.0f, 0.0f);
       ndl_s = dot3(n, ldir);
     }
+    /* both helpers shadow directional lights from the same world position
+     * when a shadow map is bound (rasterizer.c:1677-1680, 1802-1805) */
+    const float shadow = (SH && L.type == 0) ? shadow_pcf(a, wp) : 1.0f;
     /* diffuse (rasterizer.c:1673-1687) */
     float ndotl = ndl_d < 0.0f ? 0.0f : ndl_d;
-    const float contrib = ndotl * L.intensity * att * spot * 1.0f;
+    const float contrib = ndotl * L.intensity * att * spot * shadow;
     lit[0] += contrib * L.color[0];
     lit[1] += contrib * L.color[1];
     lit[2] += contrib * L.color[2];
@@ -305,7 +363,7 @@ __device__ void lights_smooth(V3 n, V3 wp, V3 vdir, const LightRec *Ls, const Dr
     if (den < 1e-6f)
       den = 1e-6f;
     const float st = D * G / den;
-    const float wgt = st * L.intensity * att * ndl_s * 1.0f * PI_F;
+    const float wgt = st * L.intensity * att * ndl_s * shadow * PI_F;
     for (int c = 0; c < 3; c++) {
       const float fr = f0[c] + (1.0f - f0[c]) * omv5;
       spec[c] += wgt * fr * L.color[c];
@@ -392,6 +450,7 @@ __device__ __forceinline__ void ibl_lut(const FrameArgs &a, const DrawRec &d, fl
 
 /* Per-sample shading of the smooth multi-light path (rasterizer.c:1963-2099)
  * from the normalised perspective-correct weights pc[]. */
+template <bool SH>
 __device__ void shade_smooth(const FrameArgs &a, const DrawRec &d, const LightRec *Ls,
                              const uint32_t v[3], const float4 N[3], const float pc[3],
                              float out[3]) {
@@ -413,7 +472,7 @@ __device__ void shade_smooth(const FrameArgs &a, const DrawRec &d, const LightRe
               pc[0] * W[0].z + pc[1] * W[1].z + pc[2] * W[2].z);
   V3 vdir = norm3(sub3(mk3(d.cam_eye[0], d.cam_eye[1], d.cam_eye[2]), wp));
   float lit[3], spec[3];
-  lights_smooth(n, wp, vdir, Ls, d, base, lit, spec);
+  lights_smooth<SH>(a, n, wp, vdir, Ls, d, base, lit, spec);
   const float ds = d.diffuse_scale;
   float env[3] = {0.0f, 0.0f, 0.0f}, irr[3] = {0.0f, 0.0f, 0.0f};
   bool has_irr = a.irr != nullptr;
@@ -551,6 +610,7 @@ __device__ __forceinline__ void mark_dead(RasterRec &r) {
 /* Screen mapping, cull and edge setup of one fan triangle (the body of the
  * fan loop, rasterizer.c:2532-2609).  Fills `rr`/`sr`; returns false if the
  * reference would draw nothing for it. */
+template <bool SH>
 __device__ bool fan_setup(const FrameArgs &a, const DrawRec &d, const CV v[3], const uint32_t slot[3],
                           uint32_t order, RasterRec &rr, ShadeRec &sr) {
   if (fabsf(v[0].p.w) < 1e-7f || fabsf(v[1].p.w) < 1e-7f || fabsf(v[2].p.w) < 1e-7f)
@@ -594,7 +654,7 @@ __device__ bool fan_setup(const FrameArgs &a, const DrawRec &d, const CV v[3], c
   if (d.flags & DF_LIT) {
     V3 wp = mk3((v[0].wp.x + v[1].wp.x + v[2].wp.x) / 3.0f, (v[0].wp.y + v[1].wp.y + v[2].wp.y) / 3.0f,
                 (v[0].wp.z + v[1].wp.z + v[2].wp.z) / 3.0f);
-    float lighting = diffuse_flat(fn, wp, a.lights + d.light_off, d.light_count, d.ambient);
+    float lighting = diffuse_flat<SH>(a, fn, wp, a.lights + d.light_off, d.light_count, d.ambient);
     float ds = 1.0f - d.metallic;
     float env_flat = d.ambient * d.metallic * 0.3f;
     for (int k = 0; k < 3; k++)
@@ -687,6 +747,7 @@ __device__ __forceinline__ void write_rec_tail(RasterRec *slot, uint32_t order, 
 /* k_setup — one thread per triangle (mop_sw_rasterize_triangle_full
  * rasterizer.c:2458-2530 up to the fan loop).  Slot t of the record arrays
  * belongs to triangle t. */
+template <bool SH>
 __device__ __forceinline__ void setup_item(const FrameArgs &a, uint32_t t) {
   const DrawRec &d = a.draws[find_draw_by(a.draws, a.draw_count, t, false)];
   const uint32_t lt = t - d.tbase;
@@ -719,7 +780,7 @@ __device__ __forceinline__ void setup_item(const FrameArgs &a, uint32_t t) {
             for (int k = 0; k < 3; k++)
               v[k] = load_cv(a, g[k]);
           }
-          status = fan_setup(a, d, v, g, t << ORDER_FAN_BITS, rr, sr) ? 1 : 0;
+          status = fan_setup<SH>(a, d, v, g, t << ORDER_FAN_BITS, rr, sr) ? 1 : 0;
         } else {
           status = 2;
         }
@@ -745,10 +806,11 @@ __device__ __forceinline__ void setup_item(const FrameArgs &a, uint32_t t) {
 
 /* 5 blocks of 256 per SM (48 registers): the setup waits on vertex gathers
  * and more resident warps hide them. */
+template <bool SH>
 __global__ void __launch_bounds__(256, 5) k_setup(FrameArgs a) {
   const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t < a.total_tris)
-    setup_item(a, t);
+    setup_item<SH>(a, t);
 }
 
 /* Sutherland-Hodgman (rasterizer.c:514-626) on the triangles queued by
@@ -783,6 +845,7 @@ __device__ __forceinline__ uint32_t clip_items(const FrameArgs &a) {
   return n_q > a.clip_cap ? a.clip_cap : n_q;
 }
 
+template <bool SH>
 __device__ __forceinline__ void clip_item(const FrameArgs &a, uint32_t qi) {
   {
     uint32_t t = a.clipq[qi];
@@ -851,7 +914,7 @@ __device__ __forceinline__ void clip_item(const FrameArgs &a, uint32_t qi) {
       uint32_t slot[3] = {vs, vs + (uint32_t)i, vs + (uint32_t)i + 1u};
       RasterRec rr;
       ShadeRec sr;
-      if (!fan_setup(a, d, fv, slot, (t << ORDER_FAN_BITS) | (uint32_t)(i - 1), rr, sr)) {
+      if (!fan_setup<SH>(a, d, fv, slot, (t << ORDER_FAN_BITS) | (uint32_t)(i - 1), rr, sr)) {
         mark_dead(rr);
         rr.order = (t << ORDER_FAN_BITS) | (uint32_t)(i - 1);
         sr.draw = (uint32_t)(&d - a.draws);
@@ -865,11 +928,12 @@ __device__ __forceinline__ void clip_item(const FrameArgs &a, uint32_t qi) {
   }
 }
 
+template <bool SH>
 __global__ void k_clip(FrameArgs a) {
   const uint32_t n_q = clip_items(a);
   for (uint32_t qi = blockIdx.x * blockDim.x + threadIdx.x; qi < n_q;
        qi += gridDim.x * blockDim.x)
-    clip_item(a, qi);
+    clip_item<SH>(a, qi);
 }
 
 /* ------------------------------------------------------------------------
@@ -943,31 +1007,31 @@ __global__ void k_raster_small(FrameArgs a) {
  * next tile's counts loaded before the current one is scanned; part holds
  * >= 32 words. */
 #define LARGE_SCAN_PER 4
-__device__ __forceinline__ void items_scan_block(uint32_t *items, uint32_t n, uint32_t *total_out,
-                                                 uint32_t *part) {
+template <typename T>
+__device__ __forceinline__ void items_scan_block(T *items, uint32_t n, T *total_out, T *part) {
   const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
   const uint32_t tile = 1024u * LARGE_SCAN_PER;
-  uint32_t nxt[LARGE_SCAN_PER];
+  T nxt[LARGE_SCAN_PER];
 #pragma unroll
   for (int k = 0; k < LARGE_SCAN_PER; k++) {
     const uint32_t i = tid * LARGE_SCAN_PER + (uint32_t)k;
-    nxt[k] = i < n ? items[i] : 0u;
+    nxt[k] = i < n ? items[i] : (T)0;
   }
-  uint32_t carry = 0;
+  T carry = 0;
   for (uint32_t base = 0; base < n; base += tile) {
-    uint32_t v[LARGE_SCAN_PER];
-    uint32_t sum = 0;
+    T v[LARGE_SCAN_PER];
+    T sum = 0;
 #pragma unroll
     for (int k = 0; k < LARGE_SCAN_PER; k++) {
       v[k] = nxt[k];
       sum += v[k];
       const uint32_t j = base + tile + tid * LARGE_SCAN_PER + (uint32_t)k;
-      nxt[k] = j < n ? items[j] : 0u;
+      nxt[k] = j < n ? items[j] : (T)0;
     }
-    uint32_t x = sum; /* inclusive scan of the per-thread sums within the warp */
+    T x = sum; /* inclusive scan of the per-thread sums within the warp */
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
-      const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+      const T y = __shfl_up_sync(0xffffffffu, x, o);
       if (lane >= (uint32_t)o)
         x += y;
     }
@@ -975,18 +1039,18 @@ __device__ __forceinline__ void items_scan_block(uint32_t *items, uint32_t n, ui
       part[warp] = x;
     __syncthreads();
     if (warp == 0) {
-      uint32_t w = part[lane];
+      T w = part[lane];
 #pragma unroll
       for (int o = 1; o < 32; o <<= 1) {
-        const uint32_t y = __shfl_up_sync(0xffffffffu, w, o);
+        const T y = __shfl_up_sync(0xffffffffu, w, o);
         if (lane >= (uint32_t)o)
           w += y;
       }
       part[lane] = w;
     }
     __syncthreads();
-    uint32_t run = carry + (warp ? part[warp - 1] : 0u) + x - sum;
-    const uint32_t total = part[31];
+    T run = carry + (warp ? part[warp - 1] : (T)0) + x - sum;
+    const T total = part[31];
 #pragma unroll
     for (int k = 0; k < LARGE_SCAN_PER; k++) {
       const uint32_t i = base + tid * LARGE_SCAN_PER + (uint32_t)k;
@@ -1215,6 +1279,7 @@ __device__ __forceinline__ const LightRec *stage_lights(const FrameArgs &a, Ligh
 }
 
 /* Shades covered sample shade_list[j] (lights: the frame's light array). */
+template <bool SH>
 __device__ __forceinline__ void shade_item(const FrameArgs &a, uint32_t j, const LightRec *lights) {
   {
     const uint32_t px = a.shade_list[j];
@@ -1269,7 +1334,7 @@ __device__ __forceinline__ void shade_item(const FrameArgs &a, uint32_t j, const
         pc[0] *= ip;
         pc[1] *= ip;
         pc[2] *= ip;
-        shade_smooth(a, d, Ls, s.v, N, pc, hdr);
+        shade_smooth<SH>(a, d, Ls, s.v, N, pc, hdr);
       }
     }
     a.pre[px] = make_uchar4(u8_of(aces(hdr[0] * a.exposure) * 255.0f + 0.5f),
@@ -1284,12 +1349,13 @@ __device__ __forceinline__ void shade_item(const FrameArgs &a, uint32_t j, const
 
 /* 4 blocks of 256 per SM (64 registers): the kernel is issue-bound and the
  * extra warps hide the dependent-latency stalls of the lighting chains. */
+template <bool SH>
 __global__ void __launch_bounds__(256, 4) k_shade(FrameArgs a) {
   __shared__ LightRec s_lights[SHADE_SMEM_LIGHTS];
   const LightRec *lights = stage_lights(a, s_lights);
   const uint32_t n = a.ctr->shade_count;
   for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x)
-    shade_item(a, j, lights);
+    shade_item<SH>(a, j, lights);
 }
 
 /* ------------------------------------------------------------------------
@@ -1529,7 +1595,7 @@ static inline unsigned blocks_for(uint32_t n, unsigned bs) { return (n + bs - 1u
 __global__ void k_ocount(FrameArgs a);
 __global__ void k_oscan(FrameArgs a);
 __global__ void k_oraster(FrameArgs a);
-__global__ void k_ofold(FrameArgs a);
+template <bool SH> __global__ void k_ofold(FrameArgs a);
 
 int mopcuda_launch_frame(const FrameArgs &a, const PostArgs &p, const LaunchCfg &cfg,
                          cudaStream_t s, cudaEvent_t *ev) {
@@ -1544,8 +1610,14 @@ int mopcuda_launch_frame(const FrameArgs &a, const PostArgs &p, const LaunchCfg 
   if (ev)
     cudaEventRecord(ev[1], s);
   if (a.total_tris) {
-    k_setup<<<blocks_for(a.total_tris, 256), 256, 0, s>>>(a);
-    k_clip<<<blocks_for(a.clip_cap < 65536u ? a.clip_cap : 65536u, 128), 128, 0, s>>>(a);
+    const unsigned cg = blocks_for(a.clip_cap < 65536u ? a.clip_cap : 65536u, 128);
+    if (a.shadow_keys) {
+      k_setup<true><<<blocks_for(a.total_tris, 256), 256, 0, s>>>(a);
+      k_clip<true><<<cg, 128, 0, s>>>(a);
+    } else {
+      k_setup<false><<<blocks_for(a.total_tris, 256), 256, 0, s>>>(a);
+      k_clip<false><<<cg, 128, 0, s>>>(a);
+    }
     launches += 2;
   }
   if (ev)
@@ -1567,7 +1639,10 @@ int mopcuda_launch_frame(const FrameArgs &a, const PostArgs &p, const LaunchCfg 
     cudaEventRecord(ev[4], s);
   const int sb = cfg.shade_block > 0 ? cfg.shade_block : 256;
   const int waves = cfg.shade_waves > 0 ? cfg.shade_waves : 4;
-  k_shade<<<cfg.num_sms * waves, sb, 0, s>>>(a);
+  if (a.shadow_keys)
+    k_shade<true><<<cfg.num_sms * waves, sb, 0, s>>>(a);
+  else
+    k_shade<false><<<cfg.num_sms * waves, sb, 0, s>>>(a);
   launches += 2;
   if (a.hdr) { /* blended suffix, composited in submission order */
     cudaMemsetAsync(a.frag_head, 0xff, sizeof(uint32_t) * (size_t)S, s);
@@ -1575,7 +1650,10 @@ int mopcuda_launch_frame(const FrameArgs &a, const PostArgs &p, const LaunchCfg 
     k_ocount<<<blocks_for(nrec, 256), 256, 0, s>>>(a);
     k_oscan<<<1, 1024, 0, s>>>(a);
     k_oraster<<<cfg.num_sms * 8, 256, 0, s>>>(a);
-    k_ofold<<<cfg.num_sms * 8, 128, 0, s>>>(a);
+    if (a.shadow_keys)
+      k_ofold<true><<<cfg.num_sms * 8, 128, 0, s>>>(a);
+    else
+      k_ofold<false><<<cfg.num_sms * 8, 128, 0, s>>>(a);
     launches += 4;
   }
   if (ev)
@@ -1606,7 +1684,7 @@ int mopcuda_launch_frame(const FrameArgs &a, const PostArgs &p, const LaunchCfg 
 
 int mopcuda_shade_occupancy(int block) {
   int nb = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_shade, block, 0);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_shade<false>, block, 0);
   return nb > 0 ? nb : 1;
 }
 
@@ -1774,6 +1852,7 @@ __device__ __forceinline__ uint32_t record_of(const FrameArgs &a, uint32_t order
   return fan == 0u ? t : 0xffffffffu;
 }
 
+template <bool SH>
 __global__ void __launch_bounds__(128) k_ofold(FrameArgs a) {
   const uint32_t n = a.ctr->touched_count;
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
@@ -1848,7 +1927,7 @@ __global__ void __launch_bounds__(128) k_ofold(FrameArgs a) {
       pc[1] *= ip;
       pc[2] *= ip;
       float p[3];
-      shade_smooth(a, d, a.lights + d.light_off, s.v, N, pc, p);
+      shade_smooth<SH>(a, d, a.lights + d.light_off, s.v, N, pc, p);
       /* edge-distance coverage (rasterizer.c:1899-1938) */
       float min_d = 0.0f;
       for (int e = 0; e < 3; e++) {
@@ -2204,9 +2283,9 @@ __global__ void __launch_bounds__(256) k_b_items(const FrameArgs *__restrict__ f
     if (ST == ST_VERTEX)
       vertex_item(a, i);
     else if (ST == ST_SETUP)
-      setup_item(a, i);
+      setup_item<false>(a, i);
     else if (ST == ST_CLIP)
-      clip_item(a, i);
+      clip_item<false>(a, i);
     else if (ST == ST_RSMALL)
       raster_small_item(a, i);
     else
@@ -2248,7 +2327,7 @@ __global__ void __launch_bounds__(256, 4) k_b_shade(const FrameArgs *__restrict_
     while (s_pre[v + 1] <= g)
       v++;
     const FrameArgs &a = fr[v];
-    shade_item(a, g - s_pre[v], lights ? lights : a.lights);
+    shade_item<false>(a, g - s_pre[v], lights ? lights : a.lights);
   }
 }
 
@@ -2498,4 +2577,203 @@ int mopcuda_launch_morph(const uint8_t *bind, uint8_t *dst, uint32_t vc, const D
   const uint32_t cap = (uint32_t)num_sms * 8u;
   k_morph<<<g < cap ? g : cap, 256, 0, s>>>(bind, dst, vc, l, targets, weights, tc);
   return 1;
+}
+
+/* ------------------------------------------------------------------------
+ * shadow pass: depth-only raster of the casters from the light
+ * (mop_sw_shadow_render_mesh, rasterizer.c:357-493).  The reference keeps
+ * `z < depth ? z : depth` per texel over all triangles in submission order,
+ * which is the minimum whatever the order, so texels take an atomicMin of
+ * depth_key(z).  The map starts at 0xffffffff (read as 1.0) and only z < 1
+ * is written, as the test against a map cleared to 1.0 keeps; -0 and +0
+ * share a key and compare equal after the lookup's bias anyway.
+ * ------------------------------------------------------------------------ */
+#define SHADOW_BLOCK 256
+
+/* Texels [xs, xe] of row y from edge values already stepped to (xs, y).  A
+ * plain read first: the map only decreases, so a key not below a (possibly
+ * stale) read value cannot lower the texel and needs no atomic. */
+__device__ __forceinline__ void shadow_walk(uint32_t *map, int size, const ShadowRec &r, int y,
+                                            int xs, int xe, float w0, float w1, float w2) {
+  uint32_t *row = map + (size_t)y * (size_t)size;
+  bool seen = false;
+  for (int x = xs; x <= xe; x++) {
+    if (w0 >= 0.0f && w1 >= 0.0f && w2 >= 0.0f) {
+      seen = true;
+      const float b0 = w0 * r.inv_area, b1 = w1 * r.inv_area, b2 = w2 * r.inv_area;
+      const float z = b0 * r.sz[0] + b1 * r.sz[1] + b2 * r.sz[2];
+      if (z < 1.0f) {
+        const uint32_t k = depth_key(z);
+        if (k < row[x])
+          atomicMin(row + x, k);
+      }
+    } else if (seen) {
+      break; /* edge values are monotone along a row: coverage has ended */
+    }
+    w0 = __fadd_rn(w0, r.dx[0]);
+    w1 = __fadd_rn(w1, r.dx[1]);
+    w2 = __fadd_rn(w2, r.dx[2]);
+  }
+}
+
+/* One thread per caster triangle: the reference's per-triangle front end
+ * (trivial reject, w guard, divide, window map, clamped bbox, area, edges
+ * flipped to positive winding, values at the bbox corner), then either the
+ * whole bbox walked here (at most small_area texels) or a record queued for
+ * the item-parallel walk. */
+__global__ void __launch_bounds__(SHADOW_BLOCK) k_shadow_tri(ShadowArgs s) {
+  const float half = (float)s.size * 0.5f;
+  for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < s.tri_total;
+       t += gridDim.x * blockDim.x) {
+    uint32_t lo = 0, hi = s.draw_count; /* last caster with tri_off <= t */
+    while (hi - lo > 1) {
+      const uint32_t mid = (lo + hi) >> 1;
+      if (s.draws[mid].tri_off <= t)
+        lo = mid;
+      else
+        hi = mid;
+    }
+    const ShadowDraw &d = s.draws[lo];
+    const size_t i3 = 3u * (size_t)(t - d.tri_off);
+    const uint32_t i0 = d.idx[i3], i1 = d.idx[i3 + 1], i2 = d.idx[i3 + 2];
+    if (i0 >= d.vertex_count || i1 >= d.vertex_count || i2 >= d.vertex_count)
+      continue;
+    const float *p0 = reinterpret_cast<const float *>(d.verts + (size_t)i0 * d.stride);
+    const float *p1 = reinterpret_cast<const float *>(d.verts + (size_t)i1 * d.stride);
+    const float *p2 = reinterpret_cast<const float *>(d.verts + (size_t)i2 * d.stride);
+    const float4 c0 = xform(d.mvp, p0[0], p0[1], p0[2], 1.0f);
+    const float4 c1 = xform(d.mvp, p1[0], p1[1], p1[2], 1.0f);
+    const float4 c2 = xform(d.mvp, p2[0], p2[1], p2[2], 1.0f);
+    if ((c0.x < -c0.w && c1.x < -c1.w && c2.x < -c2.w) ||
+        (c0.x > c0.w && c1.x > c1.w && c2.x > c2.w) ||
+        (c0.y < -c0.w && c1.y < -c1.w && c2.y < -c2.w) ||
+        (c0.y > c0.w && c1.y > c1.w && c2.y > c2.w) ||
+        (c0.z < -c0.w && c1.z < -c1.w && c2.z < -c2.w) ||
+        (c0.z > c0.w && c1.z > c1.w && c2.z > c2.w))
+      continue;
+    if (c0.w <= 1e-6f || c1.w <= 1e-6f || c2.w <= 1e-6f)
+      continue;
+    const float inv0 = 1.0f / c0.w, inv1 = 1.0f / c1.w, inv2 = 1.0f / c2.w;
+    const float sx0 = (c0.x * inv0 + 1.0f) * half, sy0 = (1.0f - c0.y * inv0) * half;
+    const float sx1 = (c1.x * inv1 + 1.0f) * half, sy1 = (1.0f - c1.y * inv1) * half;
+    const float sx2 = (c2.x * inv2 + 1.0f) * half, sy2 = (1.0f - c2.y * inv2) * half;
+    ShadowRec r;
+    r.sz[0] = (c0.z * inv0 + 1.0f) * 0.5f;
+    r.sz[1] = (c1.z * inv1 + 1.0f) * 0.5f;
+    r.sz[2] = (c2.z * inv2 + 1.0f) * 0.5f;
+    /* bbox by the reference's compare-and-replace sequence (NaN keeps the
+     * first operand, unlike fminf) */
+    float fmin_x = sx0, fmin_y = sy0, fmax_x = sx0, fmax_y = sy0;
+    if (sx1 < fmin_x)
+      fmin_x = sx1;
+    if (sx1 > fmax_x)
+      fmax_x = sx1;
+    if (sx2 < fmin_x)
+      fmin_x = sx2;
+    if (sx2 > fmax_x)
+      fmax_x = sx2;
+    if (sy1 < fmin_y)
+      fmin_y = sy1;
+    if (sy1 > fmax_y)
+      fmax_y = sy1;
+    if (sy2 < fmin_y)
+      fmin_y = sy2;
+    if (sy2 > fmax_y)
+      fmax_y = sy2;
+    int min_x = x86_f2i(floorf(fmin_x)), min_y = x86_f2i(floorf(fmin_y));
+    int max_x = x86_f2i(ceilf(fmax_x)), max_y = x86_f2i(ceilf(fmax_y));
+    if (min_x < 0)
+      min_x = 0;
+    if (min_y < 0)
+      min_y = 0;
+    if (max_x >= s.size)
+      max_x = s.size - 1;
+    if (max_y >= s.size)
+      max_y = s.size - 1;
+    if (min_x > max_x || min_y > max_y)
+      continue;
+    const float area = (sx1 - sx0) * (sy2 - sy0) - (sx2 - sx0) * (sy1 - sy0);
+    if (fabsf(area) < 1e-6f)
+      continue;
+    r.inv_area = 1.0f / fabsf(area);
+    r.dx[0] = sy1 - sy2;
+    r.dy[0] = sx2 - sx1;
+    r.dx[1] = sy2 - sy0;
+    r.dy[1] = sx0 - sx2;
+    r.dx[2] = sy0 - sy1;
+    r.dy[2] = sx1 - sx0;
+    const float px0 = (float)min_x + 0.5f, py0 = (float)min_y + 0.5f;
+    r.w[0] = (sx2 - sx1) * (py0 - sy1) - (sy2 - sy1) * (px0 - sx1);
+    r.w[1] = (sx0 - sx2) * (py0 - sy2) - (sy0 - sy2) * (px0 - sx2);
+    r.w[2] = (sx1 - sx0) * (py0 - sy0) - (sy1 - sy0) * (px0 - sx0);
+    if (area < 0.0f) {
+      for (int k = 0; k < 3; k++) {
+        r.dx[k] = -r.dx[k];
+        r.dy[k] = -r.dy[k];
+        r.w[k] = -r.w[k];
+      }
+    }
+    const uint32_t bw = (uint32_t)(max_x - min_x + 1), bh = (uint32_t)(max_y - min_y + 1);
+    if (bw * bh <= (uint32_t)s.small_area) {
+      float w0 = r.w[0], w1 = r.w[1], w2 = r.w[2];
+      for (int y = min_y; y <= max_y; y++) {
+        shadow_walk(s.map, s.size, r, y, min_x, max_x, w0, w1, w2);
+        w0 = __fadd_rn(w0, r.dy[0]);
+        w1 = __fadd_rn(w1, r.dy[1]);
+        w2 = __fadd_rn(w2, r.dy[2]);
+      }
+    } else {
+      r.x0y0 = (uint32_t)min_x | ((uint32_t)min_y << 16);
+      r.x1y1 = (uint32_t)max_x | ((uint32_t)max_y << 16);
+      r.pad = 0;
+      const uint32_t slot = atomicAdd(&s.ctr->recs, 1u); /* < tri_total: one per triangle */
+      s.recs[slot] = r;
+      s.items[slot] = (unsigned long long)bh * ((bw + RASTER_CHUNK - 1u) / RASTER_CHUNK);
+    }
+  }
+}
+
+__global__ void __launch_bounds__(1024) k_shadow_scan(ShadowArgs s) {
+  __shared__ unsigned long long part[32];
+  items_scan_block(s.items, s.ctr->recs, &s.ctr->items, part);
+}
+
+/* One thread per (row, RASTER_CHUNK-texel chunk) of the queued records; the
+ * edge values at the chunk start come from the exact folds. */
+__global__ void __launch_bounds__(SHADOW_BLOCK) k_shadow_large(ShadowArgs s) {
+  const unsigned long long total = s.ctr->items;
+  const uint32_t n = s.ctr->recs;
+  for (unsigned long long it = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
+       it < total; it += (unsigned long long)gridDim.x * blockDim.x) {
+    uint32_t lo = 0, hi = n; /* last record with offset <= it */
+    while (hi - lo > 1) {
+      const uint32_t mid = (lo + hi) >> 1;
+      if (s.items[mid] <= it)
+        lo = mid;
+      else
+        hi = mid;
+    }
+    const ShadowRec r = s.recs[lo];
+    const int x0 = (int)(r.x0y0 & 0xffffu), y0 = (int)(r.x0y0 >> 16);
+    const int x1 = (int)(r.x1y1 & 0xffffu);
+    const uint32_t chunks = ((uint32_t)(x1 - x0) + RASTER_CHUNK) / RASTER_CHUNK;
+    const unsigned long long local = it - s.items[lo];
+    const int jr = (int)(local / chunks), kc = (int)(local % chunks) * RASTER_CHUNK;
+    const int xs = x0 + kc, xe = min(x1, xs + RASTER_CHUNK - 1);
+    const float w0 = fold_add(fold_add(r.w[0], r.dy[0], jr), r.dx[0], kc);
+    const float w1 = fold_add(fold_add(r.w[1], r.dy[1], jr), r.dx[1], kc);
+    const float w2 = fold_add(fold_add(r.w[2], r.dy[2], jr), r.dx[2], kc);
+    shadow_walk(s.map, s.size, r, y0 + jr, xs, xe, w0, w1, w2);
+  }
+}
+
+int mopcuda_launch_shadow(const ShadowArgs &s, cudaStream_t st) {
+  if (!s.tri_total)
+    return 0;
+  const uint32_t cap = (uint32_t)s.num_sms * 8u;
+  const uint32_t g = blocks_for(s.tri_total, SHADOW_BLOCK);
+  k_shadow_tri<<<g < cap ? g : cap, SHADOW_BLOCK, 0, st>>>(s);
+  k_shadow_scan<<<1, 1024, 0, st>>>(s);
+  k_shadow_large<<<cap, SHADOW_BLOCK, 0, st>>>(s);
+  return 3;
 }

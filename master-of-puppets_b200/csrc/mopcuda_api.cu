@@ -143,9 +143,13 @@ extern "C" void mopcuda_device_destroy(MopCudaDevice *d) {
                         &d->clipq,    &d->keys,       &d->large_list,  &d->large_items,
                         &d->shade_list, &d->counters, &d->pick_xy,     &d->pick_out,
                         &d->deform_params, &d->hdr, &d->frag_head, &d->frags, &d->touched,
-                        &d->olist, &d->olist_items};
+                        &d->olist, &d->olist_items, &d->sh_map, &d->sh_d_draws,
+                        &d->sh_recs, &d->sh_items, &d->sh_ctr};
   for (DevArena *a : arenas)
     a->release();
+  d->sh_h_draws.release();
+  if (d->sh_ev)
+    cudaEventDestroy(d->sh_ev);
   d->h_draws.release();
   d->h_lights.release();
   d->h_counters.release();
@@ -931,6 +935,12 @@ static int launch_frame(MopCudaDevice *d) {
     a.olist_cap = ocap;
   }
 
+  if (d->sh_bound) {
+    a.shadow_keys = d->sh_map.as<uint32_t>();
+    a.shadow_vp = (const float *)(d->sh_map.as<uint8_t>() + 4 * (size_t)d->sh_size * d->sh_size);
+    a.shadow_w = a.shadow_h = d->sh_size;
+  }
+
   PostArgs p;
   mc_post_args(d, p);
   p.pre = fb->pre.as<uchar4>();
@@ -1047,6 +1057,153 @@ extern "C" int mopcuda_frame_wait(MopCudaDevice *d, int timeout_ms) {
 }
 
 extern "C" float mopcuda_frame_gpu_time_ms(MopCudaDevice *d) { return d ? d->last_ms : 0.0f; }
+
+/* ------------------------------------------------------------------------
+ * shadow pass (pass_shadow, viewport.c:2288-2442: casters rasterised into a
+ * depth map from the light, then bound for the frame's shading)
+ * ------------------------------------------------------------------------ */
+extern "C" int mopcuda_shadow_begin(MopCudaDevice *d, int size, const float light_vp[16]) {
+  if (!d || !light_vp || size <= 0 || size > 16384)
+    return fail(MOPCUDA_EINVAL, "shadow_begin: bad arguments (size %d)", size);
+  std::lock_guard<std::mutex> lk(d->mu);
+  d->sh_draws.clear();
+  d->sh_open = true;
+  d->sh_rec_size = size;
+  memcpy(d->sh_rec_vp, light_vp, sizeof d->sh_rec_vp);
+  return MOPCUDA_OK;
+}
+
+extern "C" int mopcuda_shadow_draw(MopCudaDevice *d, const MopCudaBuffer *vertices,
+                                   uint32_t vertex_count, uint32_t stride,
+                                   const MopCudaBuffer *indices, uint32_t index_count,
+                                   const float model[16]) {
+  if (!d || !vertices || !indices || !model)
+    return fail(MOPCUDA_EINVAL, "shadow_draw: bad arguments");
+  std::lock_guard<std::mutex> lk(d->mu);
+  if (!d->sh_open)
+    return fail(MOPCUDA_EINVAL, "shadow_draw outside shadow_begin/shadow_end");
+  if (stride < 12 || stride % 4 != 0)
+    return fail(MOPCUDA_EINVAL, "shadow_draw: stride %u (needs >= 12, a multiple of 4)", stride);
+  if ((uint64_t)vertex_count * stride > vertices->size ||
+      (uint64_t)index_count * 4u > indices->size)
+    return fail(MOPCUDA_EINVAL, "shadow_draw: %u vertices / %u indices exceed the buffers",
+                vertex_count, index_count);
+  ShadowDraw s;
+  s.verts = (const uint8_t *)vertices->d;
+  s.idx = (const uint32_t *)indices->d;
+  s.vertex_count = vertex_count;
+  s.stride = stride;
+  s.tri_count = index_count / 3u;
+  s.tri_off = 0;
+  mc_mat4_mul(d->sh_rec_vp, model, s.mvp); /* mop_mat4_multiply(light_vp, model) */
+  if (s.tri_count)
+    d->sh_draws.push_back(s);
+  return MOPCUDA_OK;
+}
+
+extern "C" int mopcuda_shadow_end(MopCudaDevice *d) {
+  if (!d)
+    return fail(MOPCUDA_EINVAL, "shadow_end: no device");
+  std::lock_guard<std::mutex> lk(d->mu);
+  if (!d->sh_open)
+    return fail(MOPCUDA_EINVAL, "shadow_end without shadow_begin");
+  d->sh_open = false;
+  cudaSetDevice(d->ordinal);
+  int rc;
+  /* a frame still in flight reads the map this pass rewrites */
+  if (d->pending && (rc = finish_frame(d, FRAME_TIMEOUT_MS)))
+    return rc;
+  if (!d->sh_ev)
+    CU_TRY(cudaEventCreateWithFlags(&d->sh_ev, cudaEventDisableTiming));
+  if (d->sh_ev_live && (rc = mc_bounded_sync(d, d->sh_ev, FRAME_TIMEOUT_MS)))
+    return rc;
+  const uint32_t n = (uint32_t)d->sh_draws.size();
+  uint64_t T = 0;
+  for (ShadowDraw &s : d->sh_draws) {
+    s.tri_off = (uint32_t)T;
+    T += s.tri_count;
+  }
+  if (T >= (1ull << 31))
+    return fail(MOPCUDA_EINVAL, "shadow pass too large: %llu triangles", (unsigned long long)T);
+  const size_t S = (size_t)d->sh_rec_size;
+  rc = 0;
+  rc |= d->sh_map.ensure(4 * S * S + 64); /* texels, then the light's view-projection */
+  rc |= d->sh_d_draws.ensure(sizeof(ShadowDraw) * (n ? n : 1));
+  rc |= d->sh_h_draws.ensure(sizeof(ShadowDraw) * n + 64);
+  rc |= d->sh_recs.ensure(sizeof(ShadowRec) * (size_t)(T ? T : 1));
+  rc |= d->sh_items.ensure(8 * (size_t)(T ? T : 1));
+  rc |= d->sh_ctr.ensure(sizeof(ShadowCounters));
+  if (rc)
+    return MOPCUDA_ENOMEM;
+  cudaStream_t st = d->stream;
+  /* page-locked staging: the caster table, then the view-projection */
+  uint8_t *hp = d->sh_h_draws.as<uint8_t>();
+  const size_t db = sizeof(ShadowDraw) * n;
+  if (n)
+    memcpy(hp, d->sh_draws.data(), db);
+  memcpy(hp + db, d->sh_rec_vp, 64);
+  if (n)
+    CU_TRY(cudaMemcpyAsync(d->sh_d_draws.p, hp, db, cudaMemcpyHostToDevice, st));
+  CU_TRY(cudaMemcpyAsync(d->sh_map.as<uint8_t>() + 4 * S * S, hp + db, 64,
+                         cudaMemcpyHostToDevice, st));
+  CU_TRY(cudaEventRecord(d->sh_ev, st));
+  d->sh_ev_live = true;
+  /* cleared to 1.0 (viewport.c:2370-2373): the key 0xffffffff */
+  CU_TRY(cudaMemsetAsync(d->sh_map.p, 0xff, 4 * S * S, st));
+  CU_TRY(cudaMemsetAsync(d->sh_ctr.p, 0, sizeof(ShadowCounters), st));
+  ShadowArgs a;
+  a.draws = d->sh_d_draws.as<ShadowDraw>();
+  a.draw_count = n;
+  a.tri_total = (uint32_t)T;
+  a.map = d->sh_map.as<uint32_t>();
+  a.size = (int)S;
+  a.small_area = d->cfg.small_area;
+  a.recs = d->sh_recs.as<ShadowRec>();
+  a.items = d->sh_items.as<unsigned long long>();
+  a.ctr = d->sh_ctr.as<ShadowCounters>();
+  a.num_sms = d->num_sms;
+  d->launches += (uint64_t)mopcuda_launch_shadow(a, st);
+  CU_TRY(cudaGetLastError());
+  d->sh_size = (int)S;
+  d->sh_bound = true;
+  return MOPCUDA_OK;
+}
+
+extern "C" int mopcuda_shadow_clear(MopCudaDevice *d) {
+  if (!d)
+    return fail(MOPCUDA_EINVAL, "shadow_clear: no device");
+  std::lock_guard<std::mutex> lk(d->mu);
+  cudaSetDevice(d->ordinal);
+  int rc;
+  if (d->pending && (rc = finish_frame(d, FRAME_TIMEOUT_MS)))
+    return rc;
+  d->sh_bound = false;
+  d->sh_open = false;
+  return MOPCUDA_OK;
+}
+
+extern "C" int mopcuda_shadow_read(MopCudaDevice *d, float *out, size_t out_bytes) {
+  if (!d || !out)
+    return fail(MOPCUDA_EINVAL, "shadow_read: bad arguments");
+  std::lock_guard<std::mutex> lk(d->mu);
+  if (!d->sh_bound)
+    return fail(MOPCUDA_EINVAL, "shadow_read: no shadow map bound");
+  const size_t n = (size_t)d->sh_size * (size_t)d->sh_size;
+  if (out_bytes < 4 * n)
+    return fail(MOPCUDA_EINVAL, "shadow_read: %zu bytes, %zu needed", out_bytes, 4 * n);
+  cudaSetDevice(d->ordinal);
+  int rc = mc_stream_sync(d, FRAME_TIMEOUT_MS);
+  if (rc)
+    return rc;
+  CU_TRY(cudaMemcpy(out, d->sh_map.p, 4 * n, cudaMemcpyDeviceToHost));
+  uint32_t *k = (uint32_t *)out;
+  for (size_t i = 0; i < n; i++) { /* keys -> depth values, in place */
+    uint32_t b = k[i];
+    b = b == 0xffffffffu ? 0x3f800000u : ((b & 0x80000000u) ? (b & 0x7fffffffu) : ~b);
+    k[i] = b;
+  }
+  return MOPCUDA_OK;
+}
 
 /* ------------------------------------------------------------------------
  * readbacks

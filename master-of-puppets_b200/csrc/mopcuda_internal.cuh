@@ -191,7 +191,61 @@ struct FrameArgs {
   uint32_t *olist;        /* live records of the suffix                          */
   uint32_t *olist_items;  /* their (row, chunk) item counts, then offsets        */
   uint32_t olist_cap;
+  /* shadow map bound for directional lights (the rasteriser's shadow state,
+   * rasterizer.c:141-157): shadow_w x shadow_h texel keys (shadow_texel),
+   * null when none is bound; shadow_vp: the light's view-projection, 16
+   * floats in device memory */
+  const uint32_t *shadow_keys;
+  const float *shadow_vp;
+  int shadow_w, shadow_h;
 };
+
+/* ------------------------------------------------------------------------
+ * shadow pass: depth-only raster of the casters from the light
+ * (mop_sw_shadow_render_mesh, rasterizer.c:357-493)
+ * ------------------------------------------------------------------------ */
+/* One caster mesh; its triangles are [tri_off, tri_off + tri_count) of the
+ * pass.  Positions are float3 at offset 0 of each `stride`-byte vertex. */
+struct ShadowDraw {
+  const uint8_t *verts;
+  const uint32_t *idx;
+  uint32_t vertex_count, stride, tri_count, tri_off;
+  float mvp[16]; /* light view-projection * model (mop_mat4_multiply, on the host) */
+};
+
+/* A triangle whose bbox exceeds the small-walk area, rasterised by
+ * (row, RASTER_CHUNK-texel) items from the exact folds; 64 bytes. */
+struct __align__(16) ShadowRec {
+  float w[3];  /* edge values at (x0 + .5, y0 + .5), winding already flipped */
+  float dx[3]; /* per-texel increments */
+  float dy[3]; /* per-row increments   */
+  float sz[3]; /* window depth of the three vertices */
+  float inv_area;
+  uint32_t x0y0, x1y1; /* bbox corners, x | y << 16 */
+  uint32_t pad;
+};
+
+struct ShadowCounters {
+  uint32_t recs;           /* large records written */
+  uint32_t pad;
+  unsigned long long items; /* (row, chunk) items of all large records */
+};
+
+struct ShadowArgs {
+  const ShadowDraw *draws;
+  uint32_t draw_count, tri_total;
+  uint32_t *map; /* size x size keys; 0xffffffff (cleared) = depth 1.0 */
+  int size;
+  int small_area;
+  ShadowRec *recs;            /* capacity tri_total */
+  unsigned long long *items;  /* per record: item count, then exclusive offsets */
+  ShadowCounters *ctr;
+  int num_sms;
+};
+
+/* Rasterises the pass into s.map (already cleared, counters zeroed); returns
+ * the number of kernels launched. */
+int mopcuda_launch_shadow(const ShadowArgs &s, cudaStream_t st);
 
 struct PostArgs {
   const uchar4 *pre;

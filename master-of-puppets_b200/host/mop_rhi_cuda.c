@@ -51,6 +51,10 @@ static MopRhiDevice *cu_device_create(void) {
   return d;
 }
 
+/* The C-ABI device behind an RHI device: the core's CPU-only hooks
+ * (shadow pass, IBL maps, post effects) call the C ABI with it. */
+MopCudaDevice *mop_rhi_cuda_device(MopRhiDevice *d) { return d ? d->cu : NULL; }
+
 static void cu_device_destroy(MopRhiDevice *d) {
   if (!d)
     return;

@@ -122,6 +122,11 @@ SIGNATURES = [
                                      _P, C.c_uint32]),
     ("mopcuda_morph_apply", C.c_int, [_P, _P, _P, C.c_uint32, C.POINTER(MopCudaDeformLayout),
                                       _P, _P, C.c_uint32]),
+    ("mopcuda_shadow_begin", C.c_int, [_P, C.c_int, _P]),
+    ("mopcuda_shadow_draw", C.c_int, [_P, _P, C.c_uint32, C.c_uint32, _P, C.c_uint32, _P]),
+    ("mopcuda_shadow_end", C.c_int, [_P]),
+    ("mopcuda_shadow_clear", C.c_int, [_P]),
+    ("mopcuda_shadow_read", C.c_int, [_P, _P, C.c_size_t]),
     ("mopcuda_frame_begin", C.c_int, [_P, _P, _P]),
     ("mopcuda_draw", C.c_int, [_P, _P, C.POINTER(MopCudaDraw)]),
     ("mopcuda_draw_list", C.c_int, [_P, _P, _P, C.c_uint32]),
@@ -172,6 +177,7 @@ SIGNATURES = [
     ("mopcuda_mat4_compose_trs", None, [_P, _P, _P, _P]),
     ("mopcuda_camera_matrices", None, [_P, _P, _P, C.c_float, C.c_float, C.c_float, C.c_int,
                                        C.c_int, _P, _P, _P]),
+    ("mopcuda_shadow_light_vp", C.c_int, [_P, C.c_uint32, _P, _P]),
 ]
 
 _lib = None
@@ -324,6 +330,9 @@ class _Resident:
         self.lights = (MopCudaLight * max(1, len(scene.lights)))()
         for k, l in enumerate(scene.lights):
             self.lights[k] = light_struct(l)
+        # the device's shadow binding outlives a scene: start unbound
+        _check(L.mopcuda_shadow_clear(d), "shadow_clear")
+        self._shadow_bound = False
 
     def set_ibl(self, ibl):
         self._ibl = [_f32(ibl["irr"]), _f32(ibl["pf"]), _f32(ibl["brdf"])]
@@ -408,9 +417,47 @@ class SceneRenderer(_Resident):
         self.draws = [self.draw_struct(k, self.view, self.proj, self.eye)
                       for k in scenes.draw_order(self.scene, self.eye)]
 
+    def shadow_pass(self) -> bool:
+        """pass_shadow through the C ABI (reference viewport.c:2288-2442):
+        the light camera from the casters' world transforms, every caster
+        rasterised into the map, the map bound for the following frames.
+        Without a casting directional light or a caster the map is unbound."""
+        import scenes
+        L, d, sc = self.L, self.dev.h, self.scene
+        light = scenes.shadow_light(sc)
+        casters = scenes.shadow_casters(sc)
+        if light is None or not casters:
+            if self._shadow_bound:
+                _check(L.mopcuda_shadow_clear(d), "shadow_clear")
+                self._shadow_bound = False
+            return False
+        models = np.concatenate([_f32(sc.meshes[k].transform) for k in casters])
+        vp = np.zeros(16, np.float32)
+        dr = _f32(light.direction)
+        L.mopcuda_shadow_light_vp(models.ctypes.data, len(casters), dr.ctypes.data,
+                                  vp.ctypes.data)
+        _check(L.mopcuda_shadow_begin(d, scenes.SHADOW_MAP_SIZE, vp.ctypes.data), "shadow_begin")
+        for j, k in enumerate(casters):
+            _, vb, ib, vc, ic = self.meshes[k]
+            _check(L.mopcuda_shadow_draw(d, vb, vc, 48, ib, ic, models[16 * j:].ctypes.data),
+                   "shadow_draw")
+        _check(L.mopcuda_shadow_end(d), "shadow_end")
+        self._shadow_bound = True
+        return True
+
+    def shadow_map(self):
+        """The bound shadow map as float32 [size, size]."""
+        import scenes
+        n = scenes.SHADOW_MAP_SIZE
+        out = np.zeros((n, n), np.float32)
+        _check(self.L.mopcuda_shadow_read(self.dev.h, out.ctypes.data, out.nbytes), "shadow_read")
+        return out
+
     def submit(self):
-        """Record and launch one frame (asynchronous)."""
+        """Record and launch one frame (asynchronous); the shadow pass first
+        when a directional light casts shadows."""
         L, d, fb = self.L, self.dev.h, self.fb
+        self.shadow_pass()
         _check(L.mopcuda_frame_begin(d, fb, self.clear), "frame_begin")
         for dr in self.draws:
             _check(L.mopcuda_draw(d, fb, C.byref(dr)), "draw")

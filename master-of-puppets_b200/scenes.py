@@ -62,6 +62,7 @@ class Light:
     spot_inner_cos: float = 0.95
     spot_outer_cos: float = 0.85
     active: bool = True
+    cast_shadows: bool = False    # MopLight.cast_shadows (drives the shadow pass)
 
 
 @dataclasses.dataclass
@@ -647,6 +648,43 @@ def transparent_scene(seed: int = 12, width: int = 160, height: int = 120, ssaa:
             float(rng.uniform(0.3, 1.0))
         sc.meshes.append(Mesh(v, i, oid, m, mt, r, opacity=op, blend_mode=mode))
         oid += 1
+    return sc
+
+
+SHADOW_MAP_SIZE = 1024          # MOP_SHADOW_MAP_SIZE, reference viewport.c:2286
+CHROME_ID_FLOOR = 0xFFFD0000    # object IDs at or above it are editor chrome
+
+
+def shadow_light(scene: Scene):
+    """The light pass_shadow renders from: the first active directional light
+    with cast_shadows (reference viewport.c:2293-2300), or None."""
+    for l in scene.lights:
+        if l.active and l.type == LIGHT_DIRECTIONAL and l.cast_shadows:
+            return l
+    return None
+
+
+def shadow_casters(scene: Scene) -> List[int]:
+    """Mesh indices pass_shadow rasterises, in mesh order: active opaque
+    meshes below the chrome IDs (viewport.c:2310-2315, 2405-2410)."""
+    return [k for k, m in enumerate(scene.meshes)
+            if m.object_id < CHROME_ID_FLOOR and effective_blend(m) == BLEND_OPAQUE]
+
+
+def shadow_scene(seed: int = 31, width: int = 192, height: int = 144, ssaa: int = 1,
+                 env: int = 0, transparent: bool = False) -> Scene:
+    """small_scene (or transparent_scene) with its directional light casting
+    shadows onto the ground plane, plus a second directional light that does
+    not cast: the bound map shadows every directional light's diffuse and
+    specular terms (reference rasterizer.c:1580-1583, 1677-1680, 1802-1805)."""
+    if transparent:
+        sc = transparent_scene(seed=seed, width=width, height=height, ssaa=ssaa, env=env)
+    else:
+        sc = small_scene(seed=seed, width=width, height=height, ssaa=ssaa, env=env)
+    sc.name = f"shadow{seed}"
+    sc.lights[0].cast_shadows = True
+    sc.lights.append(Light(LIGHT_DIRECTIONAL, direction=(0.5, -0.8, 0.2), intensity=0.8,
+                           color=(0.9, 0.9, 1.0, 1.0)))
     return sc
 
 

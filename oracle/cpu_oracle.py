@@ -48,13 +48,24 @@ class OrIBL(C.Structure):
                 ("rotation", C.c_float), ("intensity", C.c_float)]
 
 
+class OrShadow(C.Structure):
+    _fields_ = [("depth", C.c_void_p), ("w", C.c_int32), ("h", C.c_int32),
+                ("vp", C.c_float * 16)]
+
+
+class OrShadowMesh(C.Structure):
+    _fields_ = [("vertices", C.c_void_p), ("vertex_count", C.c_uint32),
+                ("indices", C.c_void_p), ("index_count", C.c_uint32),
+                ("model", C.c_float * 16)]
+
+
 class OrFrame(C.Structure):
     _fields_ = [("width", C.c_int32), ("height", C.c_int32), ("ssaa", C.c_int32),
                 ("clear", C.c_float * 4), ("exposure", C.c_float),
                 ("post_effects", C.c_uint32), ("ibl", C.POINTER(OrIBL)),
                 ("color_full", C.c_void_p), ("depth", C.c_void_p),
                 ("object_id", C.c_void_p), ("color_presented", C.c_void_p),
-                ("hdr", C.c_void_p)]
+                ("hdr", C.c_void_p), ("shadow", C.POINTER(OrShadow))]
 
 
 _lib = None
@@ -106,6 +117,9 @@ def lib():
                                            C.c_void_p, C.c_uint32, C.c_void_p]
         _lib.oracle_morph_apply.argtypes = [C.POINTER(OrDeformLayout), C.c_void_p, C.c_uint32,
                                             C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p]
+        _lib.oracle_shadow_matrix.argtypes = [C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p]
+        _lib.oracle_shadow_render.argtypes = [C.POINTER(OrShadowMesh), C.c_uint32, C.c_int,
+                                              C.c_void_p, C.c_void_p]
     return _lib
 
 
@@ -150,6 +164,34 @@ def _light(l):
     s.spot_outer_cos = l.spot_outer_cos
     s.active = 1 if l.active else 0
     return s
+
+
+def shadow_map(scene):
+    """pass_shadow restated (reference viewport.c:2288-2442): None when no
+    active directional light casts or no mesh casts, else the bound map
+    {"depth": float32 [size, size], "vp": float32 [16], "size": size}."""
+    light = scenes.shadow_light(scene)
+    casters = scenes.shadow_casters(scene)
+    if light is None or not casters:
+        return None
+    models = np.concatenate([_f32(scene.meshes[k].transform) for k in casters])
+    vp = np.zeros(16, np.float32)
+    d = _f32(light.direction)
+    lib().oracle_shadow_matrix(models.ctypes.data, len(casters), d.ctypes.data, vp.ctypes.data)
+    keep = []
+    ms = (OrShadowMesh * len(casters))()
+    for j, k in enumerate(casters):
+        m = scene.meshes[k]
+        v = _f32(m.vertices)
+        i = np.ascontiguousarray(m.indices, np.uint32)
+        keep += [v, i]
+        ms[j].vertices, ms[j].vertex_count = v.ctypes.data, v.shape[0]
+        ms[j].indices, ms[j].index_count = i.ctypes.data, i.size
+        ms[j].model[:] = [float(x) for x in m.transform]
+    n = scenes.SHADOW_MAP_SIZE
+    depth = np.zeros((n, n), np.float32)
+    lib().oracle_shadow_render(ms, len(casters), n, vp.ctypes.data, depth.ctypes.data)
+    return {"depth": depth, "vp": vp, "size": n}
 
 
 def render(scene, ibl=None, want_hdr=False):
@@ -220,6 +262,14 @@ def render(scene, ibl=None, want_hdr=False):
     if want_hdr:
         out["hdr"] = np.zeros((sh, sw, 4), np.float32)
         f.hdr = out["hdr"].ctypes.data
+    shadow = shadow_map(scene)
+    if shadow is not None:
+        so = OrShadow()
+        so.depth, so.w, so.h = shadow["depth"].ctypes.data, shadow["size"], shadow["size"]
+        so.vp[:] = [float(x) for x in shadow["vp"]]
+        keep += [shadow, so]
+        f.shadow = C.pointer(so)
+        out["shadow"] = shadow
     rc = L.oracle_render(C.byref(f), draws, len(scene.meshes))
     if rc != 0:
         raise RuntimeError(f"oracle_render failed: {rc}")

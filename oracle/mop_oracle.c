@@ -410,7 +410,228 @@ static float spot_cone(const OrLight *L, V3 dir) {
   return 1.0f;
 }
 
-/* compute_multi_light_rgb, rasterizer.c:1596-1688 (no shadow map bound). */
+/* ------------------------------------------------------------------------
+ * shadow map: the rasteriser's bound map (rasterizer.c:141-157), the 3x3 PCF
+ * test (rasterizer.c:303-348), the depth-only caster raster (:357-493) and
+ * pass_shadow's light camera (viewport.c:2288-2442)
+ * ------------------------------------------------------------------------ */
+static const OrShadow *g_shadow; /* bound for the frame oracle_render draws */
+
+/* (int) of a float as the x86-64 build converts it (cvttss2si): INT_MIN
+ * for NaN and out-of-range values. */
+static int x86_f2i(float f) {
+  if (!(f >= -2147483648.0f && f < 2147483648.0f))
+    return INT32_MIN;
+  return (int)f;
+}
+
+static float shadow_test_pcf(V3 wp) {
+  const OrShadow *s = g_shadow;
+  if (!s || !s->depth)
+    return 1.0f;
+  V4 p = {wp.x, wp.y, wp.z, 1.0f};
+  V4 lp = m4_xform(s->vp, p);
+  if (lp.w <= 0.0f)
+    return 1.0f;
+  float inv_w = 1.0f / lp.w;
+  float ndcx = lp.x * inv_w;
+  float ndcy = lp.y * inv_w;
+  float ndcz = (lp.z * inv_w + 1.0f) * 0.5f;
+  float u = (ndcx + 1.0f) * 0.5f * (float)s->w;
+  float v = (1.0f - ndcy) * 0.5f * (float)s->h;
+  int64_t cx = x86_f2i(u), cy = x86_f2i(v);
+  float bias = 0.005f;
+  int lit = 0, total = 0;
+  for (int dy = -1; dy <= 1; dy++) {
+    for (int dx = -1; dx <= 1; dx++) {
+      int64_t sx = cx + dx, sy = cy + dy;
+      if (sx < 0 || sx >= s->w || sy < 0 || sy >= s->h) {
+        lit++;
+        total++;
+        continue;
+      }
+      float shadow_z = s->depth[sy * (int64_t)s->w + sx];
+      if (ndcz <= shadow_z + bias)
+        lit++;
+      total++;
+    }
+  }
+  return (float)lit / (float)total;
+}
+
+static float light_shadow(const OrLight *L, V3 wp) {
+  return (L->type == 0 && g_shadow && g_shadow->depth) ? shadow_test_pcf(wp) : 1.0f;
+}
+
+/* mop_mat4_ortho, math.c:93-109 */
+static void m4_ortho(float l, float r, float b, float t, float n, float f, float *m) {
+  float rl = r - l, tb = t - b, fn = f - n;
+  memset(m, 0, 16 * sizeof(float));
+  if (fabsf(rl) < 1e-9f || fabsf(tb) < 1e-9f || fabsf(fn) < 1e-9f) {
+    m[0] = m[5] = m[10] = m[15] = 1.0f;
+    return;
+  }
+  MAT(m, 0, 0) = 2.0f / rl;
+  MAT(m, 1, 1) = 2.0f / tb;
+  MAT(m, 2, 2) = -2.0f / fn;
+  MAT(m, 0, 3) = -(r + l) / rl;
+  MAT(m, 1, 3) = -(t + b) / tb;
+  MAT(m, 2, 3) = -(f + n) / fn;
+  MAT(m, 3, 3) = 1.0f;
+}
+
+int oracle_shadow_matrix(const float *models, uint32_t count, const float dir[3],
+                         float vp[16]) {
+  if (count == 0)
+    return 0;
+  float smin[3] = {1e9f, 1e9f, 1e9f}, smax[3] = {-1e9f, -1e9f, -1e9f};
+  for (uint32_t i = 0; i < count; i++) {
+    const float *m = models + 16 * (size_t)i;
+    float cx = m[12], cy = m[13], cz = m[14];
+    float sx = sqrtf(m[0] * m[0] + m[1] * m[1] + m[2] * m[2]);
+    float sy = sqrtf(m[4] * m[4] + m[5] * m[5] + m[6] * m[6]);
+    float sz = sqrtf(m[8] * m[8] + m[9] * m[9] + m[10] * m[10]);
+    float r = sx > sy ? sx : sy;
+    if (sz > r)
+      r = sz;
+    r *= 1.5f;
+    if (cx - r < smin[0])
+      smin[0] = cx - r;
+    if (cy - r < smin[1])
+      smin[1] = cy - r;
+    if (cz - r < smin[2])
+      smin[2] = cz - r;
+    if (cx + r > smax[0])
+      smax[0] = cx + r;
+    if (cy + r > smax[1])
+      smax[1] = cy + r;
+    if (cz + r > smax[2])
+      smax[2] = cz + r;
+  }
+  V3 ld = v3_norm(v3(dir[0], dir[1], dir[2]));
+  float ctx = (smin[0] + smax[0]) * 0.5f;
+  float cty = (smin[1] + smax[1]) * 0.5f;
+  float ctz = (smin[2] + smax[2]) * 0.5f;
+  float dx = smax[0] - smin[0], dy = smax[1] - smin[1], dz = smax[2] - smin[2];
+  float radius = sqrtf(dx * dx + dy * dy + dz * dz) * 0.5f;
+  if (radius < 1.0f)
+    radius = 1.0f;
+  V3 eye = v3(ctx - ld.x * radius * 2.0f, cty - ld.y * radius * 2.0f,
+              ctz - ld.z * radius * 2.0f);
+  V3 up = v3(0.0f, 1.0f, 0.0f);
+  if (fabsf(v3_dot(ld, up)) > 0.99f)
+    up = v3(1.0f, 0.0f, 0.0f);
+  float view[16], proj[16];
+  m4_look_at(eye, v3(ctx, cty, ctz), up, view);
+  float os = radius * 1.2f;
+  m4_ortho(-os, os, -os, os, 0.1f, radius * 4.0f, proj);
+  oracle_mat4_multiply(proj, view, vp);
+  return 1;
+}
+
+static void shadow_mesh(const OrShadowMesh *me, const float *light_vp, int size, float *depth) {
+  float mvp[16];
+  oracle_mat4_multiply(light_vp, me->model, mvp);
+  float half_w = (float)size * 0.5f;
+  float half_h = (float)size * 0.5f;
+  for (uint32_t i = 0; i + 2 < me->index_count; i += 3) {
+    uint32_t ix[3] = {me->indices[i], me->indices[i + 1], me->indices[i + 2]};
+    if (ix[0] >= me->vertex_count || ix[1] >= me->vertex_count || ix[2] >= me->vertex_count)
+      continue;
+    V4 c[3];
+    for (int k = 0; k < 3; k++) {
+      const float *p = me->vertices + (size_t)ix[k] * 12;
+      V4 pos = {p[0], p[1], p[2], 1.0f};
+      c[k] = m4_xform(mvp, pos);
+    }
+    if ((c[0].x < -c[0].w && c[1].x < -c[1].w && c[2].x < -c[2].w) ||
+        (c[0].x > c[0].w && c[1].x > c[1].w && c[2].x > c[2].w) ||
+        (c[0].y < -c[0].w && c[1].y < -c[1].w && c[2].y < -c[2].w) ||
+        (c[0].y > c[0].w && c[1].y > c[1].w && c[2].y > c[2].w) ||
+        (c[0].z < -c[0].w && c[1].z < -c[1].w && c[2].z < -c[2].w) ||
+        (c[0].z > c[0].w && c[1].z > c[1].w && c[2].z > c[2].w))
+      continue;
+    if (c[0].w <= 1e-6f || c[1].w <= 1e-6f || c[2].w <= 1e-6f)
+      continue;
+    float sx[3], sy[3], sz[3];
+    for (int k = 0; k < 3; k++) {
+      float inv = 1.0f / c[k].w;
+      sx[k] = (c[k].x * inv + 1.0f) * half_w;
+      sy[k] = (1.0f - c[k].y * inv) * half_h;
+      sz[k] = (c[k].z * inv + 1.0f) * 0.5f;
+    }
+    float fmin_x = sx[0], fmin_y = sy[0], fmax_x = sx[0], fmax_y = sy[0];
+    for (int k = 1; k < 3; k++) {
+      if (sx[k] < fmin_x)
+        fmin_x = sx[k];
+      if (sx[k] > fmax_x)
+        fmax_x = sx[k];
+    }
+    for (int k = 1; k < 3; k++) {
+      if (sy[k] < fmin_y)
+        fmin_y = sy[k];
+      if (sy[k] > fmax_y)
+        fmax_y = sy[k];
+    }
+    int min_x = x86_f2i(floorf(fmin_x)), min_y = x86_f2i(floorf(fmin_y));
+    int max_x = x86_f2i(ceilf(fmax_x)), max_y = x86_f2i(ceilf(fmax_y));
+    if (min_x < 0)
+      min_x = 0;
+    if (min_y < 0)
+      min_y = 0;
+    if (max_x >= size)
+      max_x = size - 1;
+    if (max_y >= size)
+      max_y = size - 1;
+    if (min_x > max_x || min_y > max_y)
+      continue;
+    float area = (sx[1] - sx[0]) * (sy[2] - sy[0]) - (sx[2] - sx[0]) * (sy[1] - sy[0]);
+    if (fabsf(area) < 1e-6f)
+      continue;
+    float inv_area = 1.0f / fabsf(area);
+    float edx[3] = {sy[1] - sy[2], sy[2] - sy[0], sy[0] - sy[1]};
+    float edy[3] = {sx[2] - sx[1], sx[0] - sx[2], sx[1] - sx[0]};
+    float px0 = (float)min_x + 0.5f, py0 = (float)min_y + 0.5f;
+    float wr[3] = {(sx[2] - sx[1]) * (py0 - sy[1]) - (sy[2] - sy[1]) * (px0 - sx[1]),
+                   (sx[0] - sx[2]) * (py0 - sy[2]) - (sy[0] - sy[2]) * (px0 - sx[2]),
+                   (sx[1] - sx[0]) * (py0 - sy[0]) - (sy[1] - sy[0]) * (px0 - sx[0])};
+    if (area < 0.0f) {
+      for (int k = 0; k < 3; k++) {
+        edx[k] = -edx[k];
+        edy[k] = -edy[k];
+        wr[k] = -wr[k];
+      }
+    }
+    for (int y = min_y; y <= max_y; y++) {
+      float w0 = wr[0], w1 = wr[1], w2 = wr[2];
+      for (int x = min_x; x <= max_x; x++) {
+        if (w0 >= 0.0f && w1 >= 0.0f && w2 >= 0.0f) {
+          float b0 = w0 * inv_area, b1 = w1 * inv_area, b2 = w2 * inv_area;
+          float z = b0 * sz[0] + b1 * sz[1] + b2 * sz[2];
+          size_t idx = (size_t)y * (size_t)size + (size_t)x;
+          if (z < depth[idx])
+            depth[idx] = z;
+        }
+        w0 += edx[0];
+        w1 += edx[1];
+        w2 += edx[2];
+      }
+      wr[0] += edy[0];
+      wr[1] += edy[1];
+      wr[2] += edy[2];
+    }
+  }
+}
+
+void oracle_shadow_render(const OrShadowMesh *meshes, uint32_t count, int size,
+                          const float vp[16], float *depth) {
+  for (size_t p = 0; p < (size_t)size * (size_t)size; p++)
+    depth[p] = 1.0f;
+  for (uint32_t i = 0; i < count; i++)
+    shadow_mesh(&meshes[i], vp, size, depth);
+}
+
+/* compute_multi_light_rgb, rasterizer.c:1596-1688. */
 static void diffuse_rgb(V3 n, V3 wp, const OrLight *Ls, uint32_t cnt, float amb,
                         float out[3]) {
   out[0] = out[1] = out[2] = amb;
@@ -435,7 +656,7 @@ static void diffuse_rgb(V3 n, V3 wp, const OrLight *Ls, uint32_t cnt, float amb,
     }
     if (ndotl < 0.0f)
       ndotl = 0.0f;
-    float shadow = 1.0f;
+    float shadow = light_shadow(L, wp);
     float contrib = ndotl * L->intensity * att * spot * shadow;
     out[0] += contrib * L->color[0];
     out[1] += contrib * L->color[1];
@@ -480,7 +701,7 @@ static float diffuse_flat(V3 n, V3 wp, const OrLight *Ls, uint32_t cnt, float am
     }
     if (ndotl < 0.0f)
       ndotl = 0.0f;
-    float shadow = 1.0f;
+    float shadow = light_shadow(L, wp);
     total += ndotl * L->intensity * att * spot * shadow;
   }
   return clamp01(total);
@@ -545,7 +766,7 @@ static void specular_ggx(V3 n, V3 wp, V3 vdir, const OrLight *Ls, uint32_t cnt,
     if (den < 1e-6f)
       den = 1e-6f;
     float st = D * G / den;
-    float shadow = 1.0f;
+    float shadow = light_shadow(L, wp);
     float wgt = st * L->intensity * att * ndotl * shadow * OR_PI_F;
     for (int c = 0; c < 3; c++)
       out[c] += wgt * fr[c] * L->color[c];
@@ -1197,6 +1418,7 @@ int oracle_render(OrFrame *f, const OrDraw *draws, uint32_t n) {
     free(fb.color);
     return -2;
   }
+  g_shadow = f->shadow;
   /* mop_sw_framebuffer_clear, rasterizer.c:114-134 */
   for (size_t i = 0; i < px; i++) {
     for (int c = 0; c < 4; c++) {
@@ -1248,6 +1470,7 @@ int oracle_render(OrFrame *f, const OrDraw *draws, uint32_t n) {
   free(fb.depth);
   free(fb.id);
   free(fb.color);
+  g_shadow = NULL;
   return 0;
 }
 

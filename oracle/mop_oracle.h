@@ -76,6 +76,14 @@ typedef struct OrIBL {
   float intensity;
 } OrIBL;
 
+/* A bound shadow map (mop_sw_shadow_set, reference rasterizer.c:146-151):
+ * w x h depth values and the light's view-projection. */
+typedef struct OrShadow {
+  const float *depth;
+  int32_t w, h;
+  float vp[16];
+} OrShadow;
+
 typedef struct OrFrame {
   int32_t width, height; /* sample resolution (presented * ssaa) */
   int32_t ssaa;
@@ -89,6 +97,7 @@ typedef struct OrFrame {
   uint32_t *object_id;      /* width*height */
   uint8_t *color_presented; /* (width/ssaa)*(height/ssaa)*4 */
   float *hdr;               /* width*height*4, before resolve */
+  const OrShadow *shadow;   /* NULL = no shadow map bound */
 } OrFrame;
 
 /* Render one frame of draws in submission order.  Returns 0 on success. */
@@ -113,6 +122,26 @@ void oracle_pick(const uint32_t *object_id, const float *depth, int width,
 
 /* sRGB gamma byte map used by the post-process (postprocess.c:75-82). */
 void oracle_gamma_lut(uint8_t lut[256]);
+
+/* One shadow caster: MopVertex array, indices, world transform. */
+typedef struct OrShadowMesh {
+  const float *vertices; /* vertex_count * 12 floats */
+  uint32_t vertex_count;
+  const uint32_t *indices;
+  uint32_t index_count;
+  float model[16];
+} OrShadowMesh;
+
+/* The light view-projection of pass_shadow (viewport.c:2303-2427) from the
+ * casters' world transforms (count x 16 floats) and the light direction.
+ * Returns 0 when count is 0. */
+int oracle_shadow_matrix(const float *models, uint32_t count, const float dir[3],
+                         float vp[16]);
+/* The shadow map of pass_shadow: size x size cleared to 1.0 (viewport.c:
+ * 2370-2373), then mop_sw_shadow_render_mesh (rasterizer.c:357-493) for
+ * every caster in order. */
+void oracle_shadow_render(const OrShadowMesh *meshes, uint32_t count, int size,
+                          const float vp[16], float *depth);
 
 /* Vertex deformation the core runs before buffer_update: byte layout of one
  * vertex (stride; offsets of position float3, normal float3 or -1, joints

@@ -6,9 +6,9 @@
  *   - chrome off (mop_viewport_set_chrome, reference viewport.c:3934-3942) so
  *     no gradient quad / grid draws are issued;
  *   - the always-on outline overlay disabled (viewport.c:745);
- *   - lights cleared, then the scene's lights added with cast_shadows=false
- *     (the default sun would otherwise drive the shadow pass,
- *     viewport.c:683-692, 2288-2442);
+ *   - lights cleared (the default sun would otherwise drive the shadow pass,
+ *     viewport.c:683-692, 2288-2442), then the scene's lights added with their
+ *     own cast_shadows flags;
  *   - base colour baked into vertex colours by the caller (CPU shading reads
  *     vertex colour only); metallic/roughness through mop_mesh_set_material.
  * Serial mode nulls the CPU device's tile pool so cpu_draw takes its
@@ -38,6 +38,54 @@ static double now_ms(void) {
   clock_gettime(CLOCK_MONOTONIC, &ts);
   return (double)ts.tv_sec * 1e3 + (double)ts.tv_nsec * 1e-6;
 }
+
+#ifdef REFH_CUDA_HOOKS
+#include "mop_cuda.h"
+
+MopCudaDevice *mop_rhi_cuda_device(MopRhiDevice *d);
+
+/* The integration patch's shadow pass for the CUDA backend, run as a
+ * MOP_STAGE_PRE_SCENE hook (the core gates its own pass_shadow to the CPU
+ * backend, viewport.c:3224, and keeps it static): the casters the core would
+ * select (active, below the chrome IDs, opaque; viewport.c:2310-2315), the
+ * light camera from mopcuda_shadow_light_vp, every caster's RHI buffers
+ * rasterised by the C ABI, the map bound for the frame's draws. */
+static void cuda_shadow_hook(MopViewport *vp, void *ud) {
+  (void)ud;
+  MopCudaDevice *cu = mop_rhi_cuda_device(vp->device);
+  const MopLight *sun = NULL;
+  for (uint32_t i = 0; i < vp->light_count && !sun; i++)
+    if (vp->lights[i].active && vp->lights[i].type == MOP_LIGHT_DIRECTIONAL &&
+        vp->lights[i].cast_shadows)
+      sun = &vp->lights[i];
+  uint32_t n = 0;
+  float *models = malloc(sizeof(float) * 16 * (vp->mesh_count ? vp->mesh_count : 1));
+  struct MopMesh **casters = malloc(sizeof(*casters) * (vp->mesh_count ? vp->mesh_count : 1));
+  for (uint32_t i = 0; sun && models && casters && i < vp->mesh_count; i++) {
+    struct MopMesh *m = vp->meshes[i];
+    if (!m->active || m->object_id >= 0xFFFD0000u || m->blend_mode != MOP_BLEND_OPAQUE)
+      continue;
+    memcpy(models + 16 * n, m->world_transform.d, sizeof(float) * 16);
+    casters[n++] = m;
+  }
+  float light_vp[16];
+  const float dir[3] = {sun ? sun->direction.x : 0.0f, sun ? sun->direction.y : 0.0f,
+                        sun ? sun->direction.z : 0.0f};
+  if (!n || !mopcuda_shadow_light_vp(models, n, dir, light_vp)) {
+    mopcuda_shadow_clear(cu);
+  } else {
+    mopcuda_shadow_begin(cu, 1024, light_vp);
+    for (uint32_t k = 0; k < n; k++)
+      mopcuda_shadow_draw(cu, (MopCudaBuffer *)casters[k]->vertex_buffer,
+                          casters[k]->vertex_count, (uint32_t)sizeof(MopVertex),
+                          (MopCudaBuffer *)casters[k]->index_buffer, casters[k]->index_count,
+                          models + 16 * k);
+    mopcuda_shadow_end(cu);
+  }
+  free(models);
+  free(casters);
+}
+#endif
 
 void *refh_create(const RefScene *sc) {
   if (!sc || sc->width <= 0 || sc->height <= 0)
@@ -80,6 +128,10 @@ void *refh_create(const RefScene *sc) {
     h->threads = sc->workers + 1; /* workers + the calling thread */
   }
 
+#ifdef REFH_CUDA_HOOKS
+  if (!cpu)
+    mop_viewport_add_hook(vp, MOP_STAGE_PRE_SCENE, cuda_shadow_hook, NULL);
+#endif
   mop_viewport_set_chrome(vp, false);
   mop_viewport_set_overlay_enabled(vp, MOP_OVERLAY_OUTLINE, false);
   mop_viewport_set_clear_color(
@@ -109,7 +161,7 @@ void *refh_create(const RefScene *sc) {
         .spot_inner_cos = L->spot_inner_cos,
         .spot_outer_cos = L->spot_outer_cos,
         .active = L->active != 0,
-        .cast_shadows = false,
+        .cast_shadows = L->cast_shadows != 0,
     };
     MopLight *slot = mop_viewport_add_light(vp, &d);
     /* add_light always activates its slot (reference light.c:26-71). */

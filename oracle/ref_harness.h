@@ -44,6 +44,7 @@ typedef struct RefLight {
   float spot_inner_cos;
   float spot_outer_cos;
   int32_t active;
+  int32_t cast_shadows;     /* MopLight.cast_shadows                         */
 } RefLight;
 
 typedef struct RefScene {

@@ -30,7 +30,7 @@ class RefLight(C.Structure):
                 ("direction", C.c_float * 3), ("color", C.c_float * 4),
                 ("intensity", C.c_float), ("range", C.c_float),
                 ("spot_inner_cos", C.c_float), ("spot_outer_cos", C.c_float),
-                ("active", C.c_int32)]
+                ("active", C.c_int32), ("cast_shadows", C.c_int32)]
 
 
 class RefScene(C.Structure):
@@ -70,6 +70,7 @@ def light_struct(L, cls=RefLight):
     s.spot_inner_cos = L.spot_inner_cos
     s.spot_outer_cos = L.spot_outer_cos
     s.active = 1 if L.active else 0
+    s.cast_shadows = 1 if getattr(L, "cast_shadows", False) else 0
     return s
 
 

@@ -7,7 +7,7 @@ colour, depth and object-ID buffers and 200 pick results.  The oracle's
 tests compare against these files, so the oracle stays pinned even where
 the reference library is not available.
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py [name ...]
 """
 import dataclasses
 import sys
@@ -33,11 +33,17 @@ GOLDEN = {
         scenes.small_scene(seed=8, width=96, height=72, lights="none"), smooth=False),
     "small_unlit_smooth": lambda: scenes.small_scene(seed=4, width=96, height=72, lights="none"),
     "coplanar": lambda: scenes.coplanar_scene(width=96, height=72),
+    # the core's transparent pass: alpha / additive / multiply meshes back to front
+    "transparent": lambda: scenes.transparent_scene(seed=41, width=96, height=72),
+    # a directional light casting shadows: pass_shadow + 3x3 PCF on the CPU backend
+    "shadow": lambda: scenes.shadow_scene(seed=42, width=96, height=72),
 }
 
 
-def main():
+def main(names=None):
     for name, make in GOLDEN.items():
+        if names and name not in names:
+            continue
         sc = make()
         r = refdrive.Reference(sc, serial=True)
         out = r.render()
@@ -56,4 +62,4 @@ def main():
 
 
 if __name__ == "__main__":
-    main()
+    main(sys.argv[1:])

@@ -71,6 +71,33 @@ def test_host_matrices_match_oracle(make):
         assert (a.view(np.uint32) == b.view(np.uint32)).all()
 
 
+def test_shadow_light_vp_matches_oracle():
+    """mopcuda_shadow_light_vp (the product's pass_shadow light camera) vs
+    the oracle's restatement, on random caster sets and light directions,
+    including directions within the up-vector switch and scenes small enough
+    for the radius clamp."""
+    rng = np.random.default_rng(6)
+    dirs = [(0.0, -1.0, 0.0), (0.05, -1.0, 0.02), (-0.4, -0.9, -0.3), (1.0, 0.0, 0.0),
+            (0.0, 0.0, 0.0)]
+    dirs += [tuple(rng.normal(size=3)) for _ in range(40)]
+    for k, dr in enumerate(dirs):
+        n = int(rng.integers(1, 12))
+        scale = 0.05 if k % 5 == 0 else 2.0
+        models = np.concatenate([
+            scenes.mat_trs(rng.uniform(-8, 8, 3), scenes.random_rotation(rng),
+                           rng.uniform(0.1, 1.0, 3) * scale) for _ in range(n)]).astype(np.float32)
+        d = np.asarray(dr, np.float32)
+        a = np.zeros(16, np.float32)
+        b = np.zeros(16, np.float32)
+        assert mopcuda.lib().mopcuda_shadow_light_vp(models.ctypes.data, n, d.ctypes.data,
+                                                    a.ctypes.data) == 1
+        assert cpu_oracle.lib().oracle_shadow_matrix(models.ctypes.data, n, d.ctypes.data,
+                                                     b.ctypes.data) == 1
+        assert (a.view(np.uint32) == b.view(np.uint32)).all(), dr
+    assert mopcuda.lib().mopcuda_shadow_light_vp(models.ctypes.data, 0, d.ctypes.data,
+                                                a.ctypes.data) == 0
+
+
 @pytest.mark.skipif(not refdrive.available(), reason="reference library not built")
 def test_compose_trs_matches_reference():
     """mopcuda_mat4_compose_trs vs the reference's own mop_mat4_compose_trs."""

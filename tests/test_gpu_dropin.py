@@ -11,6 +11,10 @@ depth bit-exact, colour within the contract tolerance.
 Scenes avoid image-based lighting: the unmodified core hands IBL state only
 to its CPU path (reference viewport.c:2692-2706); the CUDA backend receives
 the full IBL state through mopcuda_set_ibl (covered by test_gpu_parity.py).
+The shadow scenes run the core's own pass_shadow on the CPU side; on the
+CUDA side the harness registers the integration patch's shadow pass as a
+MOP_STAGE_PRE_SCENE hook (the core runs pass_shadow for its CPU backend
+only, viewport.c:3224).
 """
 import dataclasses
 
@@ -32,6 +36,10 @@ CASES = {
     # blended meshes: the core's own transparent pass drives the ordered path
     "transparent": lambda: scenes.transparent_scene(seed=25),
     "transparent_ssaa2": lambda: scenes.transparent_scene(seed=26, width=128, height=96, ssaa=2),
+    # directional-light shadows: the core's pass_shadow vs the C-ABI shadow pass
+    "shadow": lambda: scenes.shadow_scene(seed=27, width=192, height=144),
+    "shadow_ssaa2_transparent": lambda: scenes.shadow_scene(seed=28, width=128, height=96,
+                                                            ssaa=2, transparent=True),
     "config2_reduced_no_ibl": lambda: dataclasses.replace(
         scenes.config2(width=480, height=270, ssaa=2, instances=48, tex_size=64), env=0),
 }

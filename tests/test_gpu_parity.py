@@ -7,7 +7,9 @@ point, spot, ranged, inactive lights), textures, SSAA 2, IBL, flat shading
 (lit and unlit), near-plane clipping (the config-1 ground plane passes
 behind the camera), coplanar draw-order ties, the clipping/depth stress scene
 (near-plane straddlers, coplanar pairs, host-skinned meshes), blended meshes
-(alpha, additive, multiply) in the core's transparent-pass order, and picks.
+(alpha, additive, multiply) in the core's transparent-pass order, directional
+lights shadowed through the shadow pass (the shadow map itself compared
+texel for texel), and picks.
 """
 import dataclasses
 
@@ -18,7 +20,7 @@ import cpu_oracle
 import mopcuda
 import refdrive
 import scenes
-from parity import assert_frame_parity
+from parity import assert_frame_parity, color_stats, COLOR_MAX_LSB, COLOR_1LSB_FRACTION
 
 pytestmark = pytest.mark.gpu
 
@@ -63,7 +65,28 @@ CASES = {
     "transparent": lambda: scenes.transparent_scene(seed=21),
     "transparent_ssaa2_ibl": lambda: scenes.transparent_scene(seed=22, ssaa=2, env=1),
     "transparent_config2": lambda: _transparent_config2(),
+    # shadow pass + 3x3 PCF on every directional light (one casting, one not)
+    "shadow": lambda: scenes.shadow_scene(seed=51),
+    "shadow_flat": lambda: dataclasses.replace(scenes.shadow_scene(seed=52), smooth=False),
+    "shadow_ssaa2_ibl": lambda: scenes.shadow_scene(seed=53, ssaa=2, env=1),
+    "shadow_transparent": lambda: scenes.shadow_scene(seed=54, transparent=True),
+    "shadow_config2": lambda: _with_shadow(scenes.config2(width=320, height=180, ssaa=2,
+                                                          instances=24, tex_size=64)),
+    "shadow_config3": lambda: _with_shadow(scenes.config3(seed=5, n_tris=80_000, width=480,
+                                                          height=270)),
 }
+
+
+def _with_shadow(sc):
+    """The scene with its first directional light casting shadows (one is
+    added when the scene has none)."""
+    for k, l in enumerate(sc.lights):
+        if l.type == scenes.LIGHT_DIRECTIONAL and l.active:
+            sc.lights[k] = dataclasses.replace(l, cast_shadows=True)
+            return sc
+    sc.lights.insert(0, scenes.Light(scenes.LIGHT_DIRECTIONAL, direction=(-0.3, -0.9, -0.2),
+                                     intensity=1.5, cast_shadows=True))
+    return sc
 
 
 def _transparent_config2():
@@ -102,5 +125,41 @@ def test_repeat_frames_identical(cuda_device):
         b = (r.render().color_full(), r.depth(), r.object_id())
         for x, y in zip(a, b):
             assert x.tobytes() == y.tobytes()
+    finally:
+        r.close()
+
+
+@pytest.mark.parametrize("name", ["shadow", "shadow_config3"])
+def test_shadow_map_matches_oracle(cuda_device, name):
+    """The device shadow pass (depth-only raster of the casters from the
+    light) equals pass_shadow's map texel for texel (-0 and +0 count as one
+    value: the lookup compares after adding the bias)."""
+    sc = CASES[name]()
+    want = cpu_oracle.shadow_map(sc)
+    r = mopcuda.SceneRenderer(cuda_device, sc)
+    try:
+        assert r.shadow_pass()
+        got = r.shadow_map()
+        assert ((got + 0.0).view(np.uint32) == (want["depth"] + 0.0).view(np.uint32)).all(), \
+            int(((got + 0.0).view(np.uint32) != (want["depth"] + 0.0).view(np.uint32)).sum())
+        assert (want["depth"] < 1.0).mean() > 0.05  # the casters cover part of the map
+    finally:
+        r.close()
+
+
+def test_shadow_clear_unbinds(cuda_device):
+    """Once the casting light is switched off, frames render as without a
+    shadow map (mop_sw_shadow_clear)."""
+    sc = scenes.shadow_scene(seed=55)
+    r = mopcuda.SceneRenderer(cuda_device, sc)
+    try:
+        shadowed = r.render().color_full()
+        sc.lights[0] = dataclasses.replace(sc.lights[0], cast_shadows=False)
+        plain = r.render().color_full()
+        ref = cpu_oracle.render(sc)
+        assert "shadow" not in ref
+        st = color_stats(plain, ref["color_full"])
+        assert st["max"] <= COLOR_MAX_LSB and st["within1"] >= COLOR_1LSB_FRACTION, st
+        assert (plain != shadowed).any()
     finally:
         r.close()

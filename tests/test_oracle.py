@@ -68,6 +68,11 @@ LIVE = {
     "transparent": lambda: scenes.transparent_scene(seed=17),
     "transparent_ssaa2_ibl": lambda: scenes.transparent_scene(seed=18, ssaa=2, env=1),
     "config3_small": lambda: scenes.config3(seed=19, n_tris=30_000, width=320, height=180),
+    # pass_shadow + PCF: smooth, flat, SSAA 2 with IBL, with the transparent pass
+    "shadow": lambda: scenes.shadow_scene(seed=31),
+    "shadow_flat": lambda: dataclasses.replace(scenes.shadow_scene(seed=32), smooth=False),
+    "shadow_ssaa2_ibl": lambda: scenes.shadow_scene(seed=33, ssaa=2, env=1),
+    "shadow_transparent": lambda: scenes.shadow_scene(seed=34, transparent=True),
 }
 
 
