@@ -52,7 +52,7 @@ def parse():
                     help="skip the batched (64 viewports) and served (32 scenes) forms")
     ap.add_argument("--forms-only", action="store_true",
                     help="run only the batched and served forms (one JSON line)")
-    ap.add_argument("--form", choices=["both", "batched", "served"], default="both",
+    ap.add_argument("--form", choices=["all", "batched", "served", "shadowed"], default="all",
                     help="with --forms-only: which form to run")
     return ap.parse_args()
 
@@ -466,6 +466,44 @@ def run_served(dev, rates=(2000.0, 4000.0), duration=2.0, n_scenes=32):
     return out
 
 
+def run_shadowed(dev, steps=20, warm=3):
+    """The config-2 frame with its directional light casting shadows: the
+    shadow pass (1024^2 map, every opaque mesh a caster) runs before each
+    frame and every directional light takes the 3x3 PCF factor."""
+    import dataclasses
+    import numpy as np
+    import mopcuda
+    import scenes
+    sc, _ = workload("config2")
+    k = next(i for i, l in enumerate(sc.lights) if l.type == scenes.LIGHT_DIRECTIONAL)
+    sc.lights[k] = dataclasses.replace(sc.lights[k], cast_shadows=True)
+    ibl = scenes.procedural_ibl(sc.sun_dir) if sc.env else None
+    r = mopcuda.SceneRenderer(dev, sc, ibl)
+    try:
+        for _ in range(warm):
+            r.render()
+        frame, shadow, wall = [], [], []
+        for _ in range(steps):
+            t0 = time.perf_counter()
+            r.render()
+            wall.append((time.perf_counter() - t0) * 1e3)
+            frame.append(r.gpu_ms)
+            shadow.append(r.shadow_gpu_ms)
+        ids = r.object_id()
+        fm, sm = float(np.median(frame)), float(np.median(shadow))
+        return {"scene": "config2 with its directional light casting shadows",
+                "casters": len(scenes.shadow_casters(sc)),
+                "caster_triangles": int(sum(sc.meshes[i].indices.size // 3
+                                            for i in scenes.shadow_casters(sc))),
+                "shadow_map": scenes.SHADOW_MAP_SIZE, "steps": steps,
+                "frame_ms": round(fm, 4), "shadow_pass_ms": round(sm, 4),
+                "mpix_s": round(sc.pixels / ((fm + sm) * 1e3), 1),
+                "wall_ms_per_frame": round(float(np.median(wall)), 4),
+                "covered_samples": int((ids != 0).sum())}
+    finally:
+        r.close()
+
+
 def forms_subprocess(timeout_s=900):
     """The batched and served forms in a fresh process on the same GPU, so
     their device and host state starts clean."""
@@ -480,13 +518,14 @@ def forms_subprocess(timeout_s=900):
         return {"batched": {"error": str(e)[:300]}}
 
 
-def run_forms(which="both"):
+def run_forms(which="all"):
     import mopcuda
     local = int(os.environ.get("LOCAL_RANK", "0"))
     dev = mopcuda.Device(local)
     out = {}
-    for key, fn in (("batched", run_batched), ("served", run_served)):
-        if which not in ("both", key):
+    for key, fn in (("batched", run_batched), ("served", run_served),
+                    ("shadowed", run_shadowed)):
+        if which not in ("all", key):
             continue
         try:
             out[key] = fn(dev)

@@ -208,6 +208,9 @@ int mopcuda_shadow_draw(MopCudaDevice *dev, const MopCudaBuffer *vertices, uint3
                         const float model[16]);
 int mopcuda_shadow_end(MopCudaDevice *dev);
 int mopcuda_shadow_clear(MopCudaDevice *dev);
+/* Device time of the last shadow pass (map clear + raster), waiting for it
+ * (bounded); 0 before the first pass (no reference counterpart). */
+float mopcuda_shadow_gpu_time_ms(MopCudaDevice *dev);
 /* The bound map as depth values (size * size floats, row-major). */
 int mopcuda_shadow_read(MopCudaDevice *dev, float *depth, size_t bytes);
 

@@ -151,6 +151,7 @@ struct MopCudaDevice {
   HostArena sh_h_draws;
   cudaEvent_t sh_ev = nullptr; /* after the caster table's upload */
   bool sh_ev_live = false;
+  cudaEvent_t sh_t0 = nullptr, sh_t1 = nullptr; /* around the pass's clear and kernels */
   uint32_t vertex_cap = 0, rec_cap = 0, clip_cap = 0, large_cap = 0;
   uint32_t extra_hint = 0, rec_hint = 0, clip_hint = 0, large_hint = 0;
   LaunchCfg cfg = {148, SMALL_MAX_SIDE, SMALL_MAX_AREA, 128, 256, 4, 32, 4};

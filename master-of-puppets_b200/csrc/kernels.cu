@@ -2590,9 +2590,8 @@ int mopcuda_launch_morph(const uint8_t *bind, uint8_t *dst, uint32_t vc, const D
  * ------------------------------------------------------------------------ */
 #define SHADOW_BLOCK 256
 
-/* Texels [xs, xe] of row y from edge values already stepped to (xs, y).  A
- * plain read first: the map only decreases, so a key not below a (possibly
- * stale) read value cannot lower the texel and needs no atomic. */
+/* Texels [xs, xe] of row y from edge values already stepped to (xs, y).
+ * The atomics' results are unused (reductions the thread does not wait on). */
 __device__ __forceinline__ void shadow_walk(uint32_t *map, int size, const ShadowRec &r, int y,
                                             int xs, int xe, float w0, float w1, float w2) {
   uint32_t *row = map + (size_t)y * (size_t)size;
@@ -2602,11 +2601,8 @@ __device__ __forceinline__ void shadow_walk(uint32_t *map, int size, const Shado
       seen = true;
       const float b0 = w0 * r.inv_area, b1 = w1 * r.inv_area, b2 = w2 * r.inv_area;
       const float z = b0 * r.sz[0] + b1 * r.sz[1] + b2 * r.sz[2];
-      if (z < 1.0f) {
-        const uint32_t k = depth_key(z);
-        if (k < row[x])
-          atomicMin(row + x, k);
-      }
+      if (z < 1.0f)
+        atomicMin(row + x, depth_key(z));
     } else if (seen) {
       break; /* edge values are monotone along a row: coverage has ended */
     }
@@ -2728,7 +2724,7 @@ __global__ void __launch_bounds__(SHADOW_BLOCK) k_shadow_tri(ShadowArgs s) {
       r.pad = 0;
       const uint32_t slot = atomicAdd(&s.ctr->recs, 1u); /* < tri_total: one per triangle */
       s.recs[slot] = r;
-      s.items[slot] = (unsigned long long)bh * ((bw + RASTER_CHUNK - 1u) / RASTER_CHUNK);
+      s.items[slot] = bw <= (uint32_t)SHADOW_SEG ? (bh + 31u) / 32u : bh;
     }
   }
 }
@@ -2738,32 +2734,95 @@ __global__ void __launch_bounds__(1024) k_shadow_scan(ShadowArgs s) {
   items_scan_block(s.items, s.ctr->recs, &s.ctr->items, part);
 }
 
-/* One thread per (row, RASTER_CHUNK-texel chunk) of the queued records; the
- * edge values at the chunk start come from the exact folds. */
+/* The queued records, one warp per item, in two shapes:
+ *  - narrow records (bbox at most SHADOW_SEG texels wide): an item is a band
+ *    of 32 rows, one lane per row; lanes 0-2 fold one edge each to the band's
+ *    first row (the long folds, once per band), every lane folds on to its
+ *    own row (at most 16 + 15 predicated additions) and walks it texel by
+ *    texel exactly as the reference's row loop steps;
+ *  - wide records: an item is one row; lanes 0-2 fold one edge each to the
+ *    row start and step along the row as the reference does, keeping the
+ *    value at every 32-texel chunk start in shared memory (32 chunks at a
+ *    time); each lane then walks one chunk from its start.
+ * A walk ends where its coverage ends. */
+__device__ __forceinline__ void shadow_span(uint32_t *row, const ShadowRec &r, int xs, int xe,
+                                            float w0, float w1, float w2) {
+  bool seen = false;
+  for (int x = xs; x <= xe; x++) {
+    if (w0 >= 0.0f && w1 >= 0.0f && w2 >= 0.0f) {
+      seen = true;
+      const float b0 = w0 * r.inv_area, b1 = w1 * r.inv_area, b2 = w2 * r.inv_area;
+      const float z = b0 * r.sz[0] + b1 * r.sz[1] + b2 * r.sz[2];
+      if (z < 1.0f)
+        atomicMin(row + x, depth_key(z));
+    } else if (seen) {
+      break; /* edge values are monotone along a row: coverage has ended */
+    }
+    w0 = __fadd_rn(w0, r.dx[0]);
+    w1 = __fadd_rn(w1, r.dx[1]);
+    w2 = __fadd_rn(w2, r.dx[2]);
+  }
+}
+
 __global__ void __launch_bounds__(SHADOW_BLOCK) k_shadow_large(ShadowArgs s) {
+  __shared__ float s_cs[SHADOW_BLOCK / 32][3][32];
   const unsigned long long total = s.ctr->items;
   const uint32_t n = s.ctr->recs;
-  for (unsigned long long it = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
-       it < total; it += (unsigned long long)gridDim.x * blockDim.x) {
-    uint32_t lo = 0, hi = n; /* last record with offset <= it */
+  const uint32_t lane = threadIdx.x & 31u;
+  float(*cs)[32] = s_cs[threadIdx.x >> 5];
+  const int k1 = lane < 16u ? (int)lane : 16, k2 = (int)lane - k1;
+  const unsigned long long wpb = blockDim.x >> 5;
+  for (unsigned long long it = blockIdx.x * wpb + (threadIdx.x >> 5); it < total;
+       it += gridDim.x * wpb) {
+    /* last record with offset <= it: a 32-way search, one candidate per lane
+     * (the offsets increase strictly, so the lanes that pass form a prefix) */
+    uint32_t lo = 0, hi = n;
     while (hi - lo > 1) {
-      const uint32_t mid = (lo + hi) >> 1;
-      if (s.items[mid] <= it)
-        lo = mid;
-      else
-        hi = mid;
+      const uint32_t step = (hi - lo + 31u) >> 5;
+      const uint32_t cand = lo + lane * step;
+      const bool le = cand < hi && s.items[cand] <= it;
+      const uint32_t pass = __ballot_sync(0xffffffffu, le);
+      lo += (uint32_t)(31 - __clz(pass)) * step;
+      hi = min(hi, lo + step);
     }
     const ShadowRec r = s.recs[lo];
     const int x0 = (int)(r.x0y0 & 0xffffu), y0 = (int)(r.x0y0 >> 16);
-    const int x1 = (int)(r.x1y1 & 0xffffu);
-    const uint32_t chunks = ((uint32_t)(x1 - x0) + RASTER_CHUNK) / RASTER_CHUNK;
-    const unsigned long long local = it - s.items[lo];
-    const int jr = (int)(local / chunks), kc = (int)(local % chunks) * RASTER_CHUNK;
-    const int xs = x0 + kc, xe = min(x1, xs + RASTER_CHUNK - 1);
-    const float w0 = fold_add(fold_add(r.w[0], r.dy[0], jr), r.dx[0], kc);
-    const float w1 = fold_add(fold_add(r.w[1], r.dy[1], jr), r.dx[1], kc);
-    const float w2 = fold_add(fold_add(r.w[2], r.dy[2], jr), r.dx[2], kc);
-    shadow_walk(s.map, s.size, r, y0 + jr, xs, xe, w0, w1, w2);
+    const int x1 = (int)(r.x1y1 & 0xffffu), y1 = (int)(r.x1y1 >> 16);
+    const int local = (int)(it - s.items[lo]);
+    const float e_w = lane == 0u ? r.w[0] : (lane == 1u ? r.w[1] : r.w[2]);
+    const float e_dx = lane == 0u ? r.dx[0] : (lane == 1u ? r.dx[1] : r.dx[2]);
+    const float e_dy = lane == 0u ? r.dy[0] : (lane == 1u ? r.dy[1] : r.dy[2]);
+    if (x1 - x0 < SHADOW_SEG) {
+      const int band = local * 32;
+      const float wb = lane < 3u ? fold_add(e_w, e_dy, band) : 0.0f;
+      float w[3];
+      for (int e = 0; e < 3; e++) {
+        w[e] = __shfl_sync(0xffffffffu, wb, e);
+        w[e] = fold_add(fold_add(w[e], r.dy[e], k1), r.dy[e], k2);
+      }
+      const int y = y0 + band + (int)lane;
+      if (y <= y1)
+        shadow_span(s.map + (size_t)y * (size_t)s.size, r, x0, x1, w[0], w[1], w[2]);
+    } else {
+      uint32_t *row = s.map + (size_t)(y0 + local) * (size_t)s.size;
+      float v = lane < 3u ? fold_add(e_w, e_dy, local) : 0.0f;
+      for (int xw = x0; xw <= x1; xw += 32 * RASTER_CHUNK) { /* 32 chunks per window */
+        if (lane < 3u) {
+          for (int c = 0; c < 32; c++) {
+            cs[lane][c] = v;
+#pragma unroll
+            for (int k = 0; k < RASTER_CHUNK; k++)
+              v = __fadd_rn(v, e_dx);
+          }
+        }
+        __syncwarp();
+        const int xs = xw + (int)lane * RASTER_CHUNK;
+        if (xs <= x1)
+          shadow_span(row, r, xs, min(x1, xs + RASTER_CHUNK - 1), cs[0][lane], cs[1][lane],
+                      cs[2][lane]);
+        __syncwarp(); /* starts read before lanes 0-2 write the next window */
+      }
+    }
   }
 }
 

@@ -148,8 +148,11 @@ extern "C" void mopcuda_device_destroy(MopCudaDevice *d) {
   for (DevArena *a : arenas)
     a->release();
   d->sh_h_draws.release();
-  if (d->sh_ev)
+  if (d->sh_ev) {
     cudaEventDestroy(d->sh_ev);
+    cudaEventDestroy(d->sh_t0);
+    cudaEventDestroy(d->sh_t1);
+  }
   d->h_draws.release();
   d->h_lights.release();
   d->h_counters.release();
@@ -1113,8 +1116,11 @@ extern "C" int mopcuda_shadow_end(MopCudaDevice *d) {
   /* a frame still in flight reads the map this pass rewrites */
   if (d->pending && (rc = finish_frame(d, FRAME_TIMEOUT_MS)))
     return rc;
-  if (!d->sh_ev)
+  if (!d->sh_ev) {
     CU_TRY(cudaEventCreateWithFlags(&d->sh_ev, cudaEventDisableTiming));
+    CU_TRY(cudaEventCreate(&d->sh_t0));
+    CU_TRY(cudaEventCreate(&d->sh_t1));
+  }
   if (d->sh_ev_live && (rc = mc_bounded_sync(d, d->sh_ev, FRAME_TIMEOUT_MS)))
     return rc;
   const uint32_t n = (uint32_t)d->sh_draws.size();
@@ -1148,6 +1154,7 @@ extern "C" int mopcuda_shadow_end(MopCudaDevice *d) {
                          cudaMemcpyHostToDevice, st));
   CU_TRY(cudaEventRecord(d->sh_ev, st));
   d->sh_ev_live = true;
+  CU_TRY(cudaEventRecord(d->sh_t0, st));
   /* cleared to 1.0 (viewport.c:2370-2373): the key 0xffffffff */
   CU_TRY(cudaMemsetAsync(d->sh_map.p, 0xff, 4 * S * S, st));
   CU_TRY(cudaMemsetAsync(d->sh_ctr.p, 0, sizeof(ShadowCounters), st));
@@ -1157,16 +1164,29 @@ extern "C" int mopcuda_shadow_end(MopCudaDevice *d) {
   a.tri_total = (uint32_t)T;
   a.map = d->sh_map.as<uint32_t>();
   a.size = (int)S;
-  a.small_area = d->cfg.small_area;
+  a.small_area = SHADOW_SMALL_AREA;
   a.recs = d->sh_recs.as<ShadowRec>();
   a.items = d->sh_items.as<unsigned long long>();
   a.ctr = d->sh_ctr.as<ShadowCounters>();
   a.num_sms = d->num_sms;
   d->launches += (uint64_t)mopcuda_launch_shadow(a, st);
   CU_TRY(cudaGetLastError());
+  CU_TRY(cudaEventRecord(d->sh_t1, st));
   d->sh_size = (int)S;
   d->sh_bound = true;
   return MOPCUDA_OK;
+}
+
+extern "C" float mopcuda_shadow_gpu_time_ms(MopCudaDevice *d) {
+  if (!d || !d->sh_t1)
+    return 0.0f;
+  std::lock_guard<std::mutex> lk(d->mu);
+  cudaSetDevice(d->ordinal);
+  if (mc_bounded_sync(d, d->sh_t1, FRAME_TIMEOUT_MS))
+    return 0.0f;
+  float ms = 0.0f;
+  cudaEventElapsedTime(&ms, d->sh_t0, d->sh_t1);
+  return ms;
 }
 
 extern "C" int mopcuda_shadow_clear(MopCudaDevice *d) {

@@ -213,8 +213,8 @@ struct ShadowDraw {
   float mvp[16]; /* light view-projection * model (mop_mat4_multiply, on the host) */
 };
 
-/* A triangle whose bbox exceeds the small-walk area, rasterised by
- * (row, RASTER_CHUNK-texel) items from the exact folds; 64 bytes. */
+/* A triangle whose bbox exceeds SHADOW_SMALL_AREA, rasterised by
+ * 32-row bands (narrow bboxes) or rows (wide ones); 64 bytes. */
 struct __align__(16) ShadowRec {
   float w[3];  /* edge values at (x0 + .5, y0 + .5), winding already flipped */
   float dx[3]; /* per-texel increments */
@@ -228,8 +228,15 @@ struct __align__(16) ShadowRec {
 struct ShadowCounters {
   uint32_t recs;           /* large records written */
   uint32_t pad;
-  unsigned long long items; /* (row, chunk) items of all large records */
+  unsigned long long items; /* band / row items of all large records */
 };
+
+/* Caster bboxes of at most this many texels are walked by their triangle's
+ * thread; larger ones go to the warp-per-chunk raster. */
+#define SHADOW_SMALL_AREA 32
+/* Large casters up to this bbox width are walked a 32-row band per warp
+ * (one row per lane); wider ones a row per warp (one chunk per lane). */
+#define SHADOW_SEG 128
 
 struct ShadowArgs {
   const ShadowDraw *draws;

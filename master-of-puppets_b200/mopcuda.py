@@ -126,6 +126,7 @@ SIGNATURES = [
     ("mopcuda_shadow_draw", C.c_int, [_P, _P, C.c_uint32, C.c_uint32, _P, C.c_uint32, _P]),
     ("mopcuda_shadow_end", C.c_int, [_P]),
     ("mopcuda_shadow_clear", C.c_int, [_P]),
+    ("mopcuda_shadow_gpu_time_ms", C.c_float, [_P]),
     ("mopcuda_shadow_read", C.c_int, [_P, _P, C.c_size_t]),
     ("mopcuda_frame_begin", C.c_int, [_P, _P, _P]),
     ("mopcuda_draw", C.c_int, [_P, _P, C.POINTER(MopCudaDraw)]),
@@ -444,6 +445,11 @@ class SceneRenderer(_Resident):
         _check(L.mopcuda_shadow_end(d), "shadow_end")
         self._shadow_bound = True
         return True
+
+    @property
+    def shadow_gpu_ms(self) -> float:
+        """Device time of the last shadow pass."""
+        return float(self.L.mopcuda_shadow_gpu_time_ms(self.dev.h))
 
     def shadow_map(self):
         """The bound shadow map as float32 [size, size]."""
