@@ -52,7 +52,7 @@ def parse():
                     help="skip the batched (64 viewports) and served (32 scenes) forms")
     ap.add_argument("--forms-only", action="store_true",
                     help="run only the batched and served forms (one JSON line)")
-    ap.add_argument("--form", choices=["all", "batched", "served", "shadowed"], default="all",
+    ap.add_argument("--form", choices=["all", "batched", "served", "shadowed", "ibl"], default="all",
                     help="with --forms-only: which form to run")
     return ap.parse_args()
 
@@ -504,6 +504,40 @@ def run_shadowed(dev, steps=20, warm=3):
         r.close()
 
 
+def run_ibl(dev, steps=20, warm=3):
+    """Environment admission: the config-2 procedural sky and its IBL maps
+    (sky 512x256, irradiance 64x32, prefiltered 128x64x5, BRDF LUT 256^2)
+    computed on the device; the reference core's own serial
+    mop_viewport_set_environment for the same sky timed on the host beside
+    it (oracle/_ref, in a subprocess)."""
+    import numpy as np
+    sc, _ = workload("config2")
+    args = (sc.sun_dir, sc.turbidity, sc.ground_albedo, sc.env_rotation, sc.env_intensity)
+    for _ in range(warm):
+        dev.ibl_procedural_sky(*args)
+    gpu, wall = [], []
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        dev.ibl_procedural_sky(*args)
+        wall.append((time.perf_counter() - t0) * 1e3)
+        gpu.append(dev.ibl_gpu_ms)
+    out = {"scene": "config2 procedural sky (sun %s, turbidity %g)" % (tuple(sc.sun_dir),
+                                                                      sc.turbidity),
+           "steps": steps, "gpu_ms": round(float(np.median(gpu)), 4),
+           "wall_ms": round(float(np.median(wall)), 4)}
+    cmd = [sys.executable, str(ROOT / "oracle" / "time_reference.py"), "--config", "config2",
+           "--environment", "--frames", "3"]
+    try:
+        p = subprocess.run(cmd, capture_output=True, text=True, timeout=300)
+        t = json.loads(p.stdout.strip().splitlines()[-1])
+        out["cpu_baseline"] = {"value": round(t["ms"], 3), "unit": "ms", "cores": t["threads"],
+                               "kind": "reference",
+                               "sample": f"{t['reps']} x mop_viewport_set_environment"}
+    except Exception as e:  # report, do not fail the device measurement
+        out["cpu_baseline"] = {"value": None, "error": str(e)[:200]}
+    return out
+
+
 def forms_subprocess(timeout_s=900):
     """The batched and served forms in a fresh process on the same GPU, so
     their device and host state starts clean."""
@@ -524,7 +558,7 @@ def run_forms(which="all"):
     dev = mopcuda.Device(local)
     out = {}
     for key, fn in (("batched", run_batched), ("served", run_served),
-                    ("shadowed", run_shadowed)):
+                    ("shadowed", run_shadowed), ("ibl", run_ibl)):
         if which not in ("all", key):
             continue
         try:

@@ -189,6 +189,29 @@ int mopcuda_set_ibl(MopCudaDevice *dev, const float *irradiance, int iw, int ih,
                     const float *prefiltered, int pw, int ph, int levels,
                     const float *brdf_lut, int brdf_size, float rotation, float intensity);
 
+/* ---- IBL precompute on the device (environment.c:111-484, 493-620)
+ *
+ * ibl_from_env computes from an RGBA32F equirectangular environment (w x h,
+ * what the core loads for MOP_ENV_HDRI) the maps precompute_irradiance,
+ * precompute_prefiltered and precompute_brdf_lut make — irradiance 64x32,
+ * prefiltered 128x64 in 5 levels, BRDF LUT 256x256 — and binds them as
+ * mopcuda_set_ibl does; ibl_procedural_sky first generates the 512x256
+ * Preetham sky of generate_procedural_sky (MOP_ENV_PROCEDURAL_SKY) on the
+ * device.  The BRDF LUT is bit-exact; the sky and the two environment
+ * convolutions use CUDA's atan2f/asinf/acosf/cosf/expf per sample, so they
+ * agree with the core's to float rounding. */
+int mopcuda_ibl_from_env(MopCudaDevice *dev, const float *env_rgba, int w, int h, float rotation,
+                         float intensity);
+int mopcuda_ibl_procedural_sky(MopCudaDevice *dev, const float sun_direction[3], float turbidity,
+                               float ground_albedo, float rotation, float intensity);
+/* Device time of the last precompute (table upload, sky, three maps). */
+float mopcuda_ibl_gpu_time_ms(MopCudaDevice *dev);
+/* Copies of the bound maps (any pointer may be NULL); env is the
+ * environment the last precompute read (the generated sky included). */
+int mopcuda_ibl_read(MopCudaDevice *dev, float *irradiance, size_t irradiance_bytes,
+                     float *prefiltered, size_t prefiltered_bytes, float *brdf_lut,
+                     size_t brdf_lut_bytes, float *env, size_t env_bytes);
+
 /* ---- shadow map (pass_shadow, viewport.c:2288-2442, which the core runs
  *      for its CPU backend only; mop_sw_shadow_render_mesh,
  *      rasterizer.c:357-493; mop_sw_shadow_set / _clear, rasterizer.c:146-157)

@@ -8,6 +8,7 @@
 #include "../../include/mop_cuda.h"
 #include "mopcuda_internal.cuh"
 
+#include <algorithm>
 #include <mutex>
 #include <vector>
 
@@ -131,6 +132,10 @@ struct MopCudaDevice {
   /* IBL */
   DevArena irr, pf, brdf;
   int irr_w = 0, irr_h = 0, pf_w = 0, pf_h = 0, pf_levels = 0, brdf_size = 0;
+  DevArena env, ibl_tab; /* device precompute: the environment map and host tables */
+  HostArena h_ibl;
+  int env_w = 0, env_h = 0;
+  cudaEvent_t ibl_t0 = nullptr, ibl_t1 = nullptr;
   float ibl_rot = 0.0f, ibl_int = 1.0f;
   bool ibl_on = false;
   /* frame arenas */
@@ -164,6 +169,9 @@ struct MopCudaDevice {
 /* Bounded host waits (20 us polls); every device wait of the library. */
 int mc_bounded_sync(MopCudaDevice *d, cudaEvent_t ev, int timeout_ms);
 int mc_stream_sync(MopCudaDevice *d, int timeout_ms);
+/* Completes a launched frame (re-running it on overflow) before state it
+ * reads changes. */
+int mc_finish_pending(MopCudaDevice *d);
 /* Builds the device record of one draw (and appends its lights). */
 int mc_build_draw(const MopCudaDraw *c, const float *model, const float *mvp,
                   std::vector<LightRec> &lights, DrawRec &r, bool &skip);

@@ -132,6 +132,10 @@ int mc_stream_sync(MopCudaDevice *d, int timeout_ms) {
   return rc;
 }
 
+int mc_finish_pending(MopCudaDevice *d) {
+  return d->pending ? finish_frame(d, FRAME_TIMEOUT_MS) : MOPCUDA_OK;
+}
+
 extern "C" void mopcuda_device_destroy(MopCudaDevice *d) {
   if (!d)
     return;
@@ -144,9 +148,14 @@ extern "C" void mopcuda_device_destroy(MopCudaDevice *d) {
                         &d->shade_list, &d->counters, &d->pick_xy,     &d->pick_out,
                         &d->deform_params, &d->hdr, &d->frag_head, &d->frags, &d->touched,
                         &d->olist, &d->olist_items, &d->sh_map, &d->sh_d_draws,
-                        &d->sh_recs, &d->sh_items, &d->sh_ctr};
+                        &d->sh_recs, &d->sh_items, &d->sh_ctr, &d->env, &d->ibl_tab};
   for (DevArena *a : arenas)
     a->release();
+  d->h_ibl.release();
+  if (d->ibl_t0) {
+    cudaEventDestroy(d->ibl_t0);
+    cudaEventDestroy(d->ibl_t1);
+  }
   d->sh_h_draws.release();
   if (d->sh_ev) {
     cudaEventDestroy(d->sh_ev);
@@ -396,7 +405,9 @@ extern "C" int mopcuda_set_ibl(MopCudaDevice *d, const float *irr, int iw, int i
     return fail(MOPCUDA_EINVAL, "set_ibl: no device");
   std::lock_guard<std::mutex> lk(d->mu);
   cudaSetDevice(d->ordinal);
-  int rc = mc_stream_sync(d, 10000);
+  int rc = mc_finish_pending(d);
+  if (!rc)
+    rc = mc_stream_sync(d, 10000);
   if (rc)
     return rc;
   if (!irr) {

@@ -122,6 +122,12 @@ SIGNATURES = [
                                      _P, C.c_uint32]),
     ("mopcuda_morph_apply", C.c_int, [_P, _P, _P, C.c_uint32, C.POINTER(MopCudaDeformLayout),
                                       _P, _P, C.c_uint32]),
+    ("mopcuda_ibl_from_env", C.c_int, [_P, _P, C.c_int, C.c_int, C.c_float, C.c_float]),
+    ("mopcuda_ibl_procedural_sky", C.c_int, [_P, _P, C.c_float, C.c_float, C.c_float,
+                                             C.c_float]),
+    ("mopcuda_ibl_gpu_time_ms", C.c_float, [_P]),
+    ("mopcuda_ibl_read", C.c_int, [_P, _P, C.c_size_t, _P, C.c_size_t, _P, C.c_size_t, _P,
+                                   C.c_size_t]),
     ("mopcuda_shadow_begin", C.c_int, [_P, C.c_int, _P]),
     ("mopcuda_shadow_draw", C.c_int, [_P, _P, C.c_uint32, C.c_uint32, _P, C.c_uint32, _P]),
     ("mopcuda_shadow_end", C.c_int, [_P]),
@@ -286,6 +292,43 @@ class Device:
         g = C.c_double()
         _check(self.L.mopcuda_measure_fp32_peak(self.h, C.byref(g)), "measure_fp32_peak")
         return float(g.value)
+
+    def ibl_procedural_sky(self, sun_dir, turbidity, ground_albedo, rotation=0.0,
+                           intensity=1.0):
+        """The procedural sky and its IBL maps computed on the device and
+        bound (mop_viewport_set_procedural_sky + set_environment)."""
+        sd = (C.c_float * 3)(*sun_dir)
+        _check(self.L.mopcuda_ibl_procedural_sky(self.h, sd, turbidity, ground_albedo, rotation,
+                                                 intensity), "ibl_procedural_sky")
+
+    def ibl_from_env(self, env, rotation=0.0, intensity=1.0):
+        """IBL maps computed on the device from an RGBA32F equirect map
+        [h, w, 4] and bound."""
+        env = np.ascontiguousarray(env, np.float32)
+        _check(self.L.mopcuda_ibl_from_env(self.h, env.ctypes.data, env.shape[1], env.shape[0],
+                                           rotation, intensity), "ibl_from_env")
+
+    @property
+    def ibl_gpu_ms(self) -> float:
+        return float(self.L.mopcuda_ibl_gpu_time_ms(self.h))
+
+    def ibl_maps(self, env_shape=None):
+        """The bound maps in the dictionary form of set_ibl's arguments (and
+        the environment map when env_shape = (h, w) is given)."""
+        irr = np.zeros((32, 64, 4), np.float32)
+        n_pf = sum(max(1, 128 >> l) * max(1, 64 >> l) for l in range(5))
+        pf = np.zeros(n_pf * 4, np.float32)
+        brdf = np.zeros((256, 256, 4), np.float32)
+        env = np.zeros(tuple(env_shape) + (4,), np.float32) if env_shape else None
+        _check(self.L.mopcuda_ibl_read(self.h, irr.ctypes.data, irr.nbytes, pf.ctypes.data,
+                                       pf.nbytes, brdf.ctypes.data, brdf.nbytes,
+                                       env.ctypes.data if env is not None else None,
+                                       env.nbytes if env is not None else 0), "ibl_read")
+        out = {"irr": irr.reshape(-1), "irr_w": 64, "irr_h": 32, "pf": pf, "pf_w": 128,
+               "pf_h": 64, "pf_levels": 5, "brdf": brdf.reshape(-1), "brdf_size": 256}
+        if env is not None:
+            out["env"] = env
+        return out
 
     def close(self):
         if self.h:

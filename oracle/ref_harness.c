@@ -288,6 +288,16 @@ int refh_env_maps(void *hp, const float **irr, int32_t *iw, int32_t *ih,
   return 0;
 }
 
+int refh_env_hdr(void *hp, const float **hdr, int32_t *w, int32_t *h) {
+  RefH *rh = hp;
+  if (!rh || !rh->vp->env_hdr_data)
+    return -1;
+  *hdr = rh->vp->env_hdr_data;
+  *w = rh->vp->env_width;
+  *h = rh->vp->env_height;
+  return 0;
+}
+
 static int cmp_double(const void *a, const void *b) {
   double x = *(const double *)a, y = *(const double *)b;
   return (x > y) - (x < y);
@@ -310,6 +320,26 @@ double refh_time_frames(void *hp, int warm, int frames) {
   }
   qsort(t, (size_t)frames, sizeof(double), cmp_double);
   double med = t[frames / 2];
+  free(t);
+  return med;
+}
+
+double refh_time_environment(void *hp, int reps) {
+  RefH *h = hp;
+  if (!h || reps <= 0)
+    return -1.0;
+  MopViewport *vp = h->vp;
+  MopEnvironmentDesc env = {.type = MOP_ENV_PROCEDURAL_SKY,
+                            .rotation = vp->env_rotation,
+                            .intensity = vp->env_intensity};
+  double *t = malloc(sizeof(double) * (size_t)reps);
+  for (int i = 0; i < reps; i++) {
+    double t0 = now_ms();
+    mop_viewport_set_environment(vp, &env); /* sky + the three precomputes */
+    t[i] = now_ms() - t0;
+  }
+  qsort(t, (size_t)reps, sizeof(double), cmp_double);
+  double med = t[reps / 2];
   free(t);
   return med;
 }

@@ -94,8 +94,14 @@ int refh_pick(void *h, int n, const int32_t *xy, uint32_t *ids, float *depths,
 int refh_env_maps(void *h, const float **irr, int32_t *iw, int32_t *ih,
                   const float **pf, int32_t *pw, int32_t *ph, int32_t *levels,
                   const float **brdf, int32_t *brdf_size);
+/* The environment map the maps were computed from (the generated sky for
+ * env == 1): RGBA32F, w x h. */
+int refh_env_hdr(void *h, const float **hdr, int32_t *w, int32_t *hh);
 /* Median wall time (ms) of render + read_color over `frames` after `warm`. */
 double refh_time_frames(void *h, int warm, int frames);
+/* Median ms of mop_viewport_set_environment with the scene's procedural sky
+ * (sky generation + the three IBL precomputes, serial on the host). */
+double refh_time_environment(void *h, int reps);
 int refh_num_threads(void *h);
 void refh_destroy(void *h);
 

@@ -94,8 +94,11 @@ def lib(kind: str = "cpu"):
         _lib.refh_render.argtypes = [C.c_void_p, C.POINTER(RefFrame)]
         _lib.refh_pick.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
         _lib.refh_env_maps.argtypes = [C.c_void_p] + [C.c_void_p] * 9
+        _lib.refh_env_hdr.argtypes = [C.c_void_p] * 4
         _lib.refh_time_frames.restype = C.c_double
         _lib.refh_time_frames.argtypes = [C.c_void_p, C.c_int, C.c_int]
+        _lib.refh_time_environment.restype = C.c_double
+        _lib.refh_time_environment.argtypes = [C.c_void_p, C.c_int]
         _lib.refh_num_threads.argtypes = [C.c_void_p]
         _lib.refh_destroy.argtypes = [C.c_void_p]
         if hasattr(_lib, "refh_deform_probe"):
@@ -225,6 +228,19 @@ class Reference:
             "rotation": self.scene.env_rotation,
             "intensity": self.scene.env_intensity if self.scene.env_intensity > 0 else 1.0,
         }
+
+    def env_hdr(self):
+        """The environment map the reference computed its IBL maps from
+        (float32 [h, w, 4]), or None."""
+        p, w, h = C.c_void_p(), C.c_int32(), C.c_int32()
+        if self.L.refh_env_hdr(self.h, C.byref(p), C.byref(w), C.byref(h)) != 0:
+            return None
+        n = w.value * h.value * 4
+        a = np.ctypeslib.as_array(C.cast(p, C.POINTER(C.c_float)), shape=(n,)).copy()
+        return a.reshape(h.value, w.value, 4)
+
+    def time_environment(self, reps: int) -> float:
+        return self.L.refh_time_environment(self.h, reps)
 
     def time_frames(self, warm: int, frames: int) -> float:
         return self.L.refh_time_frames(self.h, warm, frames)

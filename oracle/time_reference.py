@@ -7,7 +7,8 @@ thread pool can be killed by a timeout):
 
 --workers 0 selects the reference's serial path (tile pool removed);
 --workers N replaces the tile pool with N worker threads (+ the caller).
-Prints one JSON object: median ms of mop_viewport_render + read_color.
+Prints one JSON object: median ms of mop_viewport_render + read_color
+(--environment: of mop_viewport_set_environment with the workload's sky).
 """
 import argparse
 import json
@@ -27,10 +28,21 @@ def main():
     ap.add_argument("--warm", type=int, default=1)
     ap.add_argument("--frames", type=int, default=2)
     ap.add_argument("--budget-s", type=float, default=60.0)
+    ap.add_argument("--environment", action="store_true",
+                    help="time mop_viewport_set_environment (procedural sky + IBL "
+                         "precompute) instead of frames")
     a = ap.parse_args()
+    import dataclasses
     import refdrive
     import scenes
     sc = scenes.config1() if a.config == "config1" else scenes.config2()
+    if a.environment:  # the environment only: no meshes, a small viewport
+        sc = dataclasses.replace(sc, width=64, height=36, ssaa=1, meshes=[], textures=[])
+        r = refdrive.Reference(sc, serial=True)
+        print(json.dumps({"ms": r.time_environment(max(1, a.frames)), "reps": max(1, a.frames),
+                          "threads": 1, "mode": "serial (the core runs it on the caller)"}))
+        r.close()
+        return
     r = refdrive.Reference(sc, serial=(a.workers == 0), workers=max(0, a.workers))
     t0 = time.perf_counter()
     first = r.time_frames(a.warm, 1)
