@@ -52,7 +52,8 @@ def parse():
                     help="skip the batched (64 viewports) and served (32 scenes) forms")
     ap.add_argument("--forms-only", action="store_true",
                     help="run only the batched and served forms (one JSON line)")
-    ap.add_argument("--form", choices=["all", "batched", "served", "shadowed", "ibl"], default="all",
+    ap.add_argument("--form", choices=["all", "batched", "served", "shadowed", "ibl",
+                                           "scene_load"], default="all",
                     help="with --forms-only: which form to run")
     return ap.parse_args()
 
@@ -538,6 +539,54 @@ def run_ibl(dev, steps=20, warm=3):
     return out
 
 
+def run_scene_load(dev, steps=5):
+    """Scene admission from a .mop v2 file: the config-2 scene with 240 of
+    its 256 instances (the format holds at most 256 sections: meshes, lights
+    and the camera) written with quantized vertices, every mesh read
+    straight into device buffers (stored bytes over PCIe, decoded on the
+    device); the reference's own mop_scene_load + mop_scene_get_mesh host
+    decode of the same file timed beside it (oracle/_ref, in a subprocess)."""
+    import tempfile
+    import numpy as np
+    import scene_file
+    import scenes
+    sc = scenes.config2(instances=240)
+    tmp = tempfile.mkdtemp()
+    path = os.path.join(tmp, "config2_quantized.mop")
+    scene_file.save(sc, path, True)
+    raw_bytes = sum(48 * m.vertices.shape[0] + 4 * m.indices.size for m in sc.meshes)
+    out = {"scene": "config2 (240 instances), quantized .mop v2",
+           "triangles": int(sum(m.indices.size // 3 for m in sc.meshes)),
+           "file_bytes": os.path.getsize(path),
+           "decoded_bytes": raw_bytes, "meshes": len(sc.meshes), "steps": steps}
+    for key, fn in (("device_load_ms", scene_file.upload_all),
+                    ("device_load_per_mesh_ms", scene_file.upload)):
+        wall = []
+        for s in range(steps + 1):
+            t0 = time.perf_counter()
+            bufs = fn(dev, path)
+            t1 = time.perf_counter()
+            for b in bufs:
+                dev.L.mopcuda_buffer_destroy(dev.h, b["vertices"])
+                dev.L.mopcuda_buffer_destroy(dev.h, b["indices"])
+            if s:  # the first pass warms the page cache and the staging buffers
+                wall.append((t1 - t0) * 1e3)
+        out[key] = round(float(np.median(wall)), 3)
+    cmd = [sys.executable, str(ROOT / "oracle" / "time_reference.py"), "--scene-file", path,
+           "--frames", "3"]
+    try:
+        p = subprocess.run(cmd, capture_output=True, text=True, timeout=300)
+        t = json.loads(p.stdout.strip().splitlines()[-1])
+        out["cpu_baseline"] = {"value": round(t["ms"], 3), "unit": "ms", "cores": t["threads"],
+                               "kind": "reference",
+                               "sample": f"{t['reps']} x mop_scene_load + every get_mesh"}
+    except Exception as e:
+        out["cpu_baseline"] = {"value": None, "error": str(e)[:200]}
+    os.remove(path)
+    os.rmdir(tmp)
+    return out
+
+
 def forms_subprocess(timeout_s=900):
     """The batched and served forms in a fresh process on the same GPU, so
     their device and host state starts clean."""
@@ -558,7 +607,8 @@ def run_forms(which="all"):
     dev = mopcuda.Device(local)
     out = {}
     for key, fn in (("batched", run_batched), ("served", run_served),
-                    ("shadowed", run_shadowed), ("ibl", run_ibl)):
+                    ("shadowed", run_shadowed), ("ibl", run_ibl),
+                    ("scene_load", run_scene_load)):
         if which not in ("all", key):
             continue
         try:

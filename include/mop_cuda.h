@@ -125,6 +125,11 @@ int mopcuda_buffer_update(MopCudaDevice *dev, MopCudaBuffer *buf, const void *da
                           size_t offset, size_t size);
 /* Host shadow of the buffer contents (the core reads vertex data back). */
 const void *mopcuda_buffer_read(const MopCudaBuffer *buf);
+/* The device bytes [offset, offset + size) of a buffer (no reference
+ * counterpart: the device copy, for buffers made on the device without a
+ * host copy). */
+int mopcuda_buffer_copy_to_host(MopCudaDevice *dev, const MopCudaBuffer *buf, size_t offset,
+                                void *dst, size_t size);
 size_t mopcuda_buffer_size(const MopCudaBuffer *buf);
 
 /* ---- textures: texture_create/_hdr/destroy (rhi.h:197-211),
@@ -211,6 +216,45 @@ float mopcuda_ibl_gpu_time_ms(MopCudaDevice *dev);
 int mopcuda_ibl_read(MopCudaDevice *dev, float *irradiance, size_t irradiance_bytes,
                      float *prefiltered, size_t prefiltered_bytes, float *brdf_lut,
                      size_t brdf_lut_bytes, float *env, size_t env_bytes);
+
+/* ---- .mop v2 scene files straight to device memory (reference
+ *      src/loader/mop_scene.c, include/mop/loader/mop_scene.h)
+ *
+ * scene_file_open maps the file and checks it as mop_scene_load does (magic
+ * 0x4D4F5002, version 2, at most 256 sections, the table of contents inside
+ * the file); NULL on failure.  The counts and the camera are
+ * mop_scene_mesh_count / _light_count / _get_camera; scene_file_light reads
+ * light section idx (no reference getter).  scene_file_upload_mesh is
+ * mop_scene_get_mesh into device buffers: the section's stored bytes
+ * (quantized 18-byte or raw 48-byte vertices, 16- or 32-bit indices) cross
+ * PCIe as they are and are decoded on the device into MopVertex and 32-bit
+ * index buffers byte-identical to mop_scene_get_mesh's arrays.  With
+ * MOPCUDA_LOAD_HOST_SHADOW the buffers also keep the host copy
+ * mopcuda_buffer_read returns (the core reads vertices back); otherwise
+ * mopcuda_buffer_read returns NULL for them. */
+typedef struct MopCudaSceneFile MopCudaSceneFile;
+#define MOPCUDA_LOAD_HOST_SHADOW 1u
+MopCudaSceneFile *mopcuda_scene_file_open(const char *path);
+void mopcuda_scene_file_close(MopCudaSceneFile *file);
+uint32_t mopcuda_scene_file_mesh_count(const MopCudaSceneFile *file);
+uint32_t mopcuda_scene_file_light_count(const MopCudaSceneFile *file);
+int mopcuda_scene_file_camera(const MopCudaSceneFile *file, float eye[3], float target[3],
+                              float up[3], float *fov_radians, float *near_plane,
+                              float *far_plane);
+int mopcuda_scene_file_light(const MopCudaSceneFile *file, uint32_t idx, MopCudaLight *out);
+int mopcuda_scene_file_upload_mesh(MopCudaDevice *dev, const MopCudaSceneFile *file, uint32_t idx,
+                                   uint32_t flags, MopCudaBuffer **vertices,
+                                   MopCudaBuffer **indices, uint32_t *vertex_count,
+                                   uint32_t *index_count, float bbox_min[3], float bbox_max[3]);
+/* Every mesh of the file in one pass: one host-to-device copy of all stored
+ * mesh sections, one decode launch for the vertices and one for the
+ * indices, the buffers carved from one device allocation (each still
+ * released with mopcuda_buffer_destroy; the allocation goes with the last).
+ * vertices / indices receive mesh_count handles; the count arrays may be
+ * NULL. */
+int mopcuda_scene_file_upload_all(MopCudaDevice *dev, const MopCudaSceneFile *file, uint32_t flags,
+                                  MopCudaBuffer **vertices, MopCudaBuffer **indices,
+                                  uint32_t *vertex_counts, uint32_t *index_counts);
 
 /* ---- shadow map (pass_shadow, viewport.c:2288-2442, which the core runs
  *      for its CPU backend only; mop_sw_shadow_render_mesh,

@@ -82,10 +82,18 @@ struct HostArena {
   template <class T> T *as() const { return (T *)p; }
 };
 
+/* One device allocation shared by several buffers (a scene file's meshes);
+ * freed with the last of them. */
+struct BufferSlab {
+  void *d = nullptr;
+  uint32_t refs = 0;
+};
+
 struct MopCudaBuffer {
   void *d = nullptr;
-  void *h = nullptr; /* host shadow for buffer_read */
+  void *h = nullptr; /* host shadow for buffer_read (null for buffers made on the device) */
   size_t size = 0;
+  BufferSlab *slab = nullptr; /* d lies inside slab->d when set */
 };
 
 struct MopCudaTexture {
@@ -136,6 +144,9 @@ struct MopCudaDevice {
   HostArena h_ibl;
   int env_w = 0, env_h = 0;
   cudaEvent_t ibl_t0 = nullptr, ibl_t1 = nullptr;
+  /* scene-file uploads: page-locked and device staging of a mesh section */
+  HostArena h_load;
+  DevArena load_stage;
   float ibl_rot = 0.0f, ibl_int = 1.0f;
   bool ibl_on = false;
   /* frame arenas */

@@ -152,6 +152,8 @@ extern "C" void mopcuda_device_destroy(MopCudaDevice *d) {
   for (DevArena *a : arenas)
     a->release();
   d->h_ibl.release();
+  d->h_load.release();
+  d->load_stage.release();
   if (d->ibl_t0) {
     cudaEventDestroy(d->ibl_t0);
     cudaEventDestroy(d->ibl_t1);
@@ -219,7 +221,14 @@ extern "C" void mopcuda_buffer_destroy(MopCudaDevice *d, MopCudaBuffer *b) {
   std::lock_guard<std::mutex> lk(d->mu);
   cudaSetDevice(d->ordinal);
   mc_stream_sync(d, 10000); /* a launched frame may still read it */
-  cudaFree(b->d);
+  if (b->slab) {
+    if (--b->slab->refs == 0) {
+      cudaFree(b->slab->d);
+      delete b->slab;
+    }
+  } else {
+    cudaFree(b->d);
+  }
   free(b->h);
   delete b;
 }
@@ -233,12 +242,27 @@ extern "C" int mopcuda_buffer_update(MopCudaDevice *d, MopCudaBuffer *b, const v
   int rc = mc_stream_sync(d, 10000);
   if (rc)
     return rc;
-  memcpy((uint8_t *)b->h + offset, data, size);
+  if (b->h)
+    memcpy((uint8_t *)b->h + offset, data, size);
   CU_TRY(cudaMemcpy((uint8_t *)b->d + offset, data, size, cudaMemcpyHostToDevice));
   return MOPCUDA_OK;
 }
 
 extern "C" const void *mopcuda_buffer_read(const MopCudaBuffer *b) { return b ? b->h : nullptr; }
+
+extern "C" int mopcuda_buffer_copy_to_host(MopCudaDevice *d, const MopCudaBuffer *b,
+                                           size_t offset, void *dst, size_t size) {
+  if (!d || !b || (!dst && size) || offset > b->size || size > b->size - offset)
+    return fail(MOPCUDA_EINVAL, "buffer_copy_to_host: range outside buffer");
+  std::lock_guard<std::mutex> lk(d->mu);
+  cudaSetDevice(d->ordinal);
+  int rc = mc_stream_sync(d, FRAME_TIMEOUT_MS);
+  if (rc)
+    return rc;
+  if (size)
+    CU_TRY(cudaMemcpy(dst, (const uint8_t *)b->d + offset, size, cudaMemcpyDeviceToHost));
+  return MOPCUDA_OK;
+}
 extern "C" size_t mopcuda_buffer_size(const MopCudaBuffer *b) { return b ? b->size : 0; }
 
 /* ------------------------------------------------------------------------
@@ -466,7 +490,8 @@ static int deform_check(const MopCudaBuffer *dst, const MopCudaBuffer *bind, uin
  * core reads deformed vertices back for bounds). */
 static int deform_finish(MopCudaDevice *d, MopCudaBuffer *dst, size_t bytes) {
   CU_TRY(cudaGetLastError());
-  CU_TRY(cudaMemcpyAsync(dst->h, dst->d, bytes, cudaMemcpyDeviceToHost, d->stream));
+  if (dst->h)
+    CU_TRY(cudaMemcpyAsync(dst->h, dst->d, bytes, cudaMemcpyDeviceToHost, d->stream));
   return mc_stream_sync(d, FRAME_TIMEOUT_MS);
 }
 

@@ -105,6 +105,7 @@ SIGNATURES = [
     ("mopcuda_buffer_destroy", None, [_P, _P]),
     ("mopcuda_buffer_update", C.c_int, [_P, _P, _P, C.c_size_t, C.c_size_t]),
     ("mopcuda_buffer_read", _P, [_P]),
+    ("mopcuda_buffer_copy_to_host", C.c_int, [_P, _P, C.c_size_t, _P, C.c_size_t]),
     ("mopcuda_buffer_size", C.c_size_t, [_P]),
     ("mopcuda_texture_create", _P, [_P, C.c_int, C.c_int, _P]),
     ("mopcuda_texture_create_hdr", _P, [_P, C.c_int, C.c_int, _P]),
@@ -128,6 +129,17 @@ SIGNATURES = [
     ("mopcuda_ibl_gpu_time_ms", C.c_float, [_P]),
     ("mopcuda_ibl_read", C.c_int, [_P, _P, C.c_size_t, _P, C.c_size_t, _P, C.c_size_t, _P,
                                    C.c_size_t]),
+    ("mopcuda_scene_file_open", _P, [C.c_char_p]),
+    ("mopcuda_scene_file_close", None, [_P]),
+    ("mopcuda_scene_file_mesh_count", C.c_uint32, [_P]),
+    ("mopcuda_scene_file_light_count", C.c_uint32, [_P]),
+    ("mopcuda_scene_file_camera", C.c_int, [_P, _P, _P, _P, _P, _P, _P]),
+    ("mopcuda_scene_file_light", C.c_int, [_P, C.c_uint32, C.POINTER(MopCudaLight)]),
+    ("mopcuda_scene_file_upload_mesh", C.c_int, [_P, _P, C.c_uint32, C.c_uint32,
+                                                 C.POINTER(_P), C.POINTER(_P),
+                                                 C.POINTER(C.c_uint32), C.POINTER(C.c_uint32),
+                                                 _P, _P]),
+    ("mopcuda_scene_file_upload_all", C.c_int, [_P, _P, C.c_uint32, _P, _P, _P, _P]),
     ("mopcuda_shadow_begin", C.c_int, [_P, C.c_int, _P]),
     ("mopcuda_shadow_draw", C.c_int, [_P, _P, C.c_uint32, C.c_uint32, _P, C.c_uint32, _P]),
     ("mopcuda_shadow_end", C.c_int, [_P]),
@@ -341,7 +353,10 @@ class _Resident:
     the C ABI (mop_viewport_add_mesh -> buffer_create, create_texture ->
     texture_create, set_exposure / set_post_effects / set_ibl)."""
 
-    def __init__(self, device: Device, scene, ibl=None):
+    def __init__(self, device: Device, scene, ibl=None, preloaded=None):
+        """preloaded: the meshes' device buffers already made (one
+        scene_file.upload entry per mesh, in mesh order) instead of uploading
+        scene.meshes' arrays."""
         self.dev = device
         self.scene = scene
         L = device.L
@@ -349,15 +364,20 @@ class _Resident:
         self.L = L
         self._buffers = []
         self.meshes = []
-        for m in scene.meshes:
-            v = _f32(m.vertices)
-            i = np.ascontiguousarray(m.indices, np.uint32)
-            vb = L.mopcuda_buffer_create(d, v.ctypes.data, v.nbytes)
-            ib = L.mopcuda_buffer_create(d, i.ctypes.data, i.nbytes)
-            if not vb or not ib:
-                raise RuntimeError(f"buffer_create failed: {last_error()}")
+        for k, m in enumerate(scene.meshes):
+            if preloaded is not None:
+                p = preloaded[k]
+                vb, ib, vc, ic = p["vertices"], p["indices"], p["vertex_count"], p["index_count"]
+            else:
+                v = _f32(m.vertices)
+                i = np.ascontiguousarray(m.indices, np.uint32)
+                vb = L.mopcuda_buffer_create(d, v.ctypes.data, v.nbytes)
+                ib = L.mopcuda_buffer_create(d, i.ctypes.data, i.nbytes)
+                if not vb or not ib:
+                    raise RuntimeError(f"buffer_create failed: {last_error()}")
+                vc, ic = v.shape[0], i.size
             self._buffers += [vb, ib]
-            self.meshes.append((m, vb, ib, v.shape[0], i.size))
+            self.meshes.append((m, vb, ib, vc, ic))
         self.textures = []
         for t in scene.textures:
             t = np.ascontiguousarray(t, np.uint8)
@@ -428,8 +448,8 @@ class _Resident:
 class SceneRenderer(_Resident):
     """Scene resident on one device; renders frames through the C ABI."""
 
-    def __init__(self, device: Device, scene, ibl=None):
-        super().__init__(device, scene, ibl)
+    def __init__(self, device: Device, scene, ibl=None, preloaded=None):
+        super().__init__(device, scene, ibl, preloaded)
         L, d = self.L, device.h
         self.sw, self.sh = scene.width * scene.ssaa, scene.height * scene.ssaa
         self.fb = L.mopcuda_framebuffer_create(d, self.sw, self.sh)

@@ -117,6 +117,7 @@ def lib():
                                            C.c_void_p, C.c_uint32, C.c_void_p]
         _lib.oracle_morph_apply.argtypes = [C.POINTER(OrDeformLayout), C.c_void_p, C.c_uint32,
                                             C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p]
+        _lib.oracle_mop_decode_mesh.argtypes = [C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p]
         _lib.oracle_shadow_matrix.argtypes = [C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p]
         _lib.oracle_shadow_render.argtypes = [C.POINTER(OrShadowMesh), C.c_uint32, C.c_int,
                                               C.c_void_p, C.c_void_p]
@@ -287,3 +288,28 @@ def pick(scene, frame, xy):
     lib().oracle_pick(oid.ctypes.data, d.ctypes.data, scene.width, scene.height, scene.ssaa, n,
                       xy.ctypes.data, ids.ctypes.data, dep.ctypes.data, hits.ctypes.data)
     return ids, dep, hits
+
+
+def scene_file_meshes(path):
+    """Every mesh section of a .mop v2 file decoded as mop_scene_get_mesh
+    does: a list of (vertices float32 [V, 12], indices uint32, bbox [6])."""
+    import struct
+    data = open(path, "rb").read()
+    magic, version, nsec, _ = struct.unpack_from("<IIII", data, 0)
+    if magic != 0x4D4F5002 or version != 2 or nsec > 256:
+        raise ValueError("not a .mop v2 file")
+    buf = np.frombuffer(data, np.uint8)
+    out = []
+    for k in range(nsec):
+        kind, _, off, size = struct.unpack_from("<IIQQ", data, 64 + 24 * k)
+        if kind != 1:
+            continue
+        vc, ic = struct.unpack_from("<II", data, off)
+        bbox = np.frombuffer(data, np.float32, 6, off + 16).copy()
+        v = np.zeros((vc, 12), np.float32)
+        i = np.zeros(ic, np.uint32)
+        sec = np.ascontiguousarray(buf[off:off + size])
+        if lib().oracle_mop_decode_mesh(sec.ctypes.data, size, v.ctypes.data, i.ctypes.data):
+            raise ValueError(f"mesh section {k} shorter than its counts")
+        out.append((v, i, bbox))
+    return out

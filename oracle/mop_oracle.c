@@ -1570,3 +1570,70 @@ void oracle_morph_apply(const OrDeformLayout *l, const uint8_t *bind, uint32_t v
     }
   }
 }
+
+/* ------------------------------------------------------------------------
+ * .mop v2 mesh section decode, mop_scene.c:142-223, 397-486
+ * ------------------------------------------------------------------------ */
+int oracle_mop_decode_mesh(const uint8_t *sec, uint64_t size, float *out_v, uint32_t *out_i) {
+  if (size < 48)
+    return -1;
+  uint32_t h[4];
+  float bmin[3], bmax[3];
+  memcpy(h, sec, 16);
+  memcpy(bmin, sec + 16, 12);
+  memcpy(bmax, sec + 28, 12);
+  const uint32_t vc = h[0], ic = h[1];
+  const int quant = h[2] == 1, idx16 = h[3] == 2;
+  const uint64_t vb = (uint64_t)vc * (quant ? 18u : 48u), ib = (uint64_t)ic * (idx16 ? 2u : 4u);
+  const uint64_t vb8 = (vb + 7u) & ~(uint64_t)7u;
+  if (48 + vb8 + ib > size)
+    return -1;
+  const uint8_t *vd = sec + 48, *id = sec + 48 + vb8;
+  for (uint32_t k = 0; k < vc; k++) {
+    float *o = out_v + (size_t)k * 12;
+    if (!quant) {
+      memcpy(o, vd + (size_t)k * 48, 48);
+      continue;
+    }
+    uint16_t q[9];
+    memcpy(q, vd + (size_t)k * 18, 18);
+    for (int i = 0; i < 3; i++) {
+      float range = bmax[i] - bmin[i];
+      o[i] = bmin[i] + ((float)q[i] / 65535.0f) * range;
+    }
+    float ox = (float)(int16_t)q[3] / 32767.0f, oy = (float)(int16_t)q[4] / 32767.0f;
+    float nz = 1.0f - fabsf(ox) - fabsf(oy);
+    if (nz < 0.0f) {
+      float tx = (1.0f - fabsf(oy)) * (ox >= 0.0f ? 1.0f : -1.0f);
+      float ty = (1.0f - fabsf(ox)) * (oy >= 0.0f ? 1.0f : -1.0f);
+      ox = tx;
+      oy = ty;
+    }
+    float nx = ox, ny = oy;
+    float len = sqrtf(nx * nx + ny * ny + nz * nz);
+    if (len > 1e-8f) {
+      nx /= len;
+      ny /= len;
+      nz /= len;
+    }
+    o[3] = nx;
+    o[4] = ny;
+    o[5] = nz;
+    o[6] = (float)(q[5] & 0xffu) / 255.0f;
+    o[7] = (float)(q[5] >> 8) / 255.0f;
+    o[8] = (float)(q[6] & 0xffu) / 255.0f;
+    o[9] = (float)(q[6] >> 8) / 255.0f;
+    o[10] = (float)q[7] / 65535.0f;
+    o[11] = (float)q[8] / 65535.0f;
+  }
+  for (uint32_t k = 0; k < ic; k++) {
+    if (idx16) {
+      uint16_t x;
+      memcpy(&x, id + (size_t)k * 2, 2);
+      out_i[k] = x;
+    } else {
+      memcpy(&out_i[k], id + (size_t)k * 4, 4);
+    }
+  }
+  return 0;
+}

@@ -143,6 +143,14 @@ int oracle_shadow_matrix(const float *models, uint32_t count, const float dir[3]
 void oracle_shadow_render(const OrShadowMesh *meshes, uint32_t count, int size,
                           const float vp[16], float *depth);
 
+/* mop_scene_get_mesh's decode of one .mop v2 mesh section (reference
+ * src/loader/mop_scene.c:397-486, dequantize_vertex / oct_decode :142-223):
+ * section points at the 48-byte section header; vertices receives
+ * vertex_count x 12 floats, indices index_count words.  Returns 0, or -1
+ * when the section is shorter than its counts. */
+int oracle_mop_decode_mesh(const uint8_t *section, uint64_t size, float *vertices,
+                           uint32_t *indices);
+
 /* Vertex deformation the core runs before buffer_update: byte layout of one
  * vertex (stride; offsets of position float3, normal float3 or -1, joints
  * ubyte4, weights float4). */

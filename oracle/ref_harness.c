@@ -19,6 +19,8 @@
 #include "core/viewport_internal.h"
 #include "rasterizer/rasterizer_mt.h"
 
+#include <mop/loader/loader.h>
+#include <mop/loader/mop_scene.h>
 #include <mop/mop.h>
 #include <stdlib.h>
 #include <string.h>
@@ -32,6 +34,8 @@ typedef struct RefH {
   int w, h, ssaa;
   int threads;
 } RefH;
+
+static int cmp_double(const void *a, const void *b);
 
 static double now_ms(void) {
   struct timespec ts;
@@ -286,6 +290,67 @@ int refh_env_maps(void *hp, const float **irr, int32_t *iw, int32_t *ih,
   *brdf = vp->env_brdf_lut_data;
   *brdf_size = 256; /* BRDF_LUT_SIZE, reference viewport.c:2702 */
   return 0;
+}
+
+int refh_scene_save(void *hp, const char *path, uint32_t flags) {
+  RefH *h = hp;
+  return h ? mop_scene_save(h->vp, path, flags) : -1;
+}
+
+int refh_scene_file_mesh(const char *path, uint32_t idx, float *vertices, uint32_t vcap,
+                         uint32_t *indices, uint32_t icap, uint32_t *vc, uint32_t *ic,
+                         float bbox[6]) {
+  MopSceneFile *f = mop_scene_load(path);
+  if (!f)
+    return -1;
+  MopLoadedMesh m;
+  int rc = -2;
+  if (mop_scene_get_mesh(f, idx, &m)) {
+    rc = -3;
+    if (m.vertex_count <= vcap && m.index_count <= icap) {
+      memcpy(vertices, m.vertices, (size_t)m.vertex_count * sizeof(MopVertex));
+      memcpy(indices, m.indices, (size_t)m.index_count * sizeof(uint32_t));
+      *vc = m.vertex_count;
+      *ic = m.index_count;
+      bbox[0] = m.bbox_min.x;
+      bbox[1] = m.bbox_min.y;
+      bbox[2] = m.bbox_min.z;
+      bbox[3] = m.bbox_max.x;
+      bbox[4] = m.bbox_max.y;
+      bbox[5] = m.bbox_max.z;
+      rc = 0;
+    }
+    free(m.vertices);
+    free(m.indices);
+  }
+  mop_scene_free(f);
+  return rc;
+}
+
+double refh_time_scene_file(const char *path, int reps) {
+  double *t = malloc(sizeof(double) * (size_t)(reps > 0 ? reps : 1));
+  for (int r = 0; r < reps; r++) {
+    double t0 = now_ms();
+    MopSceneFile *f = mop_scene_load(path);
+    if (!f) {
+      free(t);
+      return -1.0;
+    }
+    uint32_t n = mop_scene_mesh_count(f);
+    for (uint32_t k = 0; k < n; k++) {
+      MopLoadedMesh m;
+      if (mop_scene_get_mesh(f, k, &m)) {
+        free(m.vertices);
+        free(m.indices);
+      }
+    }
+    mop_scene_free(f);
+    t[r] = now_ms() - t0;
+  }
+  qsort(t, (size_t)reps, sizeof(double), cmp_double);
+  double med = t[reps / 2];
+  free(t);
+  return med;
 }
 
 int refh_env_hdr(void *hp, const float **hdr, int32_t *w, int32_t *h) {

@@ -94,6 +94,15 @@ int refh_pick(void *h, int n, const int32_t *xy, uint32_t *ids, float *depths,
 int refh_env_maps(void *h, const float **irr, int32_t *iw, int32_t *ih,
                   const float **pf, int32_t *pw, int32_t *ph, int32_t *levels,
                   const float **brdf, int32_t *brdf_size);
+/* mop_scene_save of the harness's viewport (flags: MOP_SAVE_QUANTIZE = 1). */
+int refh_scene_save(void *h, const char *path, uint32_t flags);
+/* mop_scene_load + mop_scene_get_mesh(idx): the decoded vertices (12 floats
+ * each) and 32-bit indices, and the section's bbox (min, max). */
+int refh_scene_file_mesh(const char *path, uint32_t idx, float *vertices, uint32_t vcap,
+                         uint32_t *indices, uint32_t icap, uint32_t *vc, uint32_t *ic,
+                         float bbox[6]);
+/* Median ms of mop_scene_load + mop_scene_get_mesh of every mesh + frees. */
+double refh_time_scene_file(const char *path, int reps);
 /* The environment map the maps were computed from (the generated sky for
  * env == 1): RGBA32F, w x h. */
 int refh_env_hdr(void *h, const float **hdr, int32_t *w, int32_t *hh);

@@ -95,6 +95,12 @@ def lib(kind: str = "cpu"):
         _lib.refh_pick.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
         _lib.refh_env_maps.argtypes = [C.c_void_p] + [C.c_void_p] * 9
         _lib.refh_env_hdr.argtypes = [C.c_void_p] * 4
+        _lib.refh_scene_save.argtypes = [C.c_void_p, C.c_char_p, C.c_uint32]
+        _lib.refh_scene_file_mesh.argtypes = [C.c_char_p, C.c_uint32, C.c_void_p, C.c_uint32,
+                                              C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p,
+                                              C.c_void_p]
+        _lib.refh_time_scene_file.restype = C.c_double
+        _lib.refh_time_scene_file.argtypes = [C.c_char_p, C.c_int]
         _lib.refh_time_frames.restype = C.c_double
         _lib.refh_time_frames.argtypes = [C.c_void_p, C.c_int, C.c_int]
         _lib.refh_time_environment.restype = C.c_double
@@ -229,6 +235,11 @@ class Reference:
             "intensity": self.scene.env_intensity if self.scene.env_intensity > 0 else 1.0,
         }
 
+    def save_scene(self, path, quantize: bool) -> None:
+        """mop_scene_save of this viewport."""
+        if self.L.refh_scene_save(self.h, str(path).encode(), 1 if quantize else 0) != 0:
+            raise RuntimeError("mop_scene_save failed")
+
     def env_hdr(self):
         """The environment map the reference computed its IBL maps from
         (float32 [h, w, 4]), or None."""
@@ -281,3 +292,22 @@ def deform_probe(vertices: np.ndarray, vertex_count: int, bones=None, targets=No
     if rc != 0:
         raise RuntimeError("refh_deform_probe failed")
     return out
+
+
+def scene_file_mesh(path, idx: int, vcap: int = 1 << 22, icap: int = 1 << 24):
+    """mop_scene_load + mop_scene_get_mesh(idx) of the reference: (vertices
+    float32 [V, 12], indices uint32, bbox float32 [6])."""
+    v = np.zeros((vcap, 12), np.float32)
+    i = np.zeros(icap, np.uint32)
+    vc, ic = C.c_uint32(), C.c_uint32()
+    bb = np.zeros(6, np.float32)
+    rc = lib().refh_scene_file_mesh(str(path).encode(), idx, v.ctypes.data, vcap, i.ctypes.data,
+                                    icap, C.byref(vc), C.byref(ic), bb.ctypes.data)
+    if rc != 0:
+        raise RuntimeError(f"reference mop_scene_get_mesh failed ({rc})")
+    return v[:vc.value].copy(), i[:ic.value].copy(), bb
+
+
+def time_scene_file(path, reps: int = 3) -> float:
+    """Median ms of the reference's mop_scene_load + every mop_scene_get_mesh."""
+    return lib().refh_time_scene_file(str(path).encode(), reps)

@@ -28,6 +28,9 @@ def main():
     ap.add_argument("--warm", type=int, default=1)
     ap.add_argument("--frames", type=int, default=2)
     ap.add_argument("--budget-s", type=float, default=60.0)
+    ap.add_argument("--scene-file", default=None,
+                    help="time mop_scene_load + mop_scene_get_mesh of every mesh of this "
+                         ".mop v2 file instead of frames")
     ap.add_argument("--environment", action="store_true",
                     help="time mop_viewport_set_environment (procedural sky + IBL "
                          "precompute) instead of frames")
@@ -36,6 +39,11 @@ def main():
     import refdrive
     import scenes
     sc = scenes.config1() if a.config == "config1" else scenes.config2()
+    if a.scene_file:
+        ms = refdrive.time_scene_file(a.scene_file, max(1, a.frames))
+        print(json.dumps({"ms": ms, "reps": max(1, a.frames), "threads": 1,
+                          "mode": "serial (the loader runs on the caller)"}))
+        return
     if a.environment:  # the environment only: no meshes, a small viewport
         sc = dataclasses.replace(sc, width=64, height=36, ssaa=1, meshes=[], textures=[])
         r = refdrive.Reference(sc, serial=True)

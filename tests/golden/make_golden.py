@@ -8,6 +8,7 @@ tests compare against these files, so the oracle stays pinned even where
 the reference library is not available.
 
     python tests/golden/make_golden.py [name ...]
+    python tests/golden/make_golden.py scene_files
 """
 import dataclasses
 import sys
@@ -40,7 +41,33 @@ GOLDEN = {
 }
 
 
+# .mop v2 scene files written by the reference's mop_scene_save, with the
+# reference's mop_scene_get_mesh decode of every mesh
+SCENE_FILES = {
+    "scene_small_quant": (lambda: scenes.small_scene(seed=3), True),
+    "scene_coplanar_raw": (lambda: scenes.coplanar_scene(), False),
+}
+
+
+def make_scene_files():
+    for name, (make, quant) in SCENE_FILES.items():
+        sc = make()
+        path = HERE / f"{name}.mop"
+        r = refdrive.Reference(sc, serial=True)
+        r.save_scene(path, quant)
+        r.close()
+        n = sum(1 for m in sc.meshes if m.object_id != 0)
+        arrays = {}
+        for k in range(n):
+            v, i, bb = refdrive.scene_file_mesh(path, k)
+            arrays[f"v{k}"], arrays[f"i{k}"], arrays[f"b{k}"] = v, i, bb
+        np.savez_compressed(HERE / f"{name}_decoded.npz", **arrays)
+        print(name, path.stat().st_size, "bytes")
+
+
 def main(names=None):
+    if names and "scene_files" in names:
+        return make_scene_files()
     for name, make in GOLDEN.items():
         if names and name not in names:
             continue
