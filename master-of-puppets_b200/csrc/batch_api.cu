@@ -151,9 +151,11 @@ extern "C" int mopcuda_scene_add_draw(MopCudaScene *s, const MopCudaDraw *c) {
     s->lights.resize(nl);
     return rc;
   }
-  if (!skip && (r.blend_mode != 0 || r.opacity < 1.0f)) {
+  if (!skip && (r.blend_mode != 0 || r.opacity < 1.0f ||
+                ((r.flags & DF_SMOOTH) && !(r.flags & DF_LIT)))) {
     s->lights.resize(nl);
-    return fail(MOPCUDA_EUNSUPPORTED, "scene_add_draw: batches render opaque draws only");
+    return fail(MOPCUDA_EUNSUPPORTED,
+                "scene_add_draw: batches render opaque lit or flat draws only");
   }
   if (skip) { /* zero opacity: a colour no-op, kept as an empty slot */
     memset(&r, 0, sizeof r);

@@ -1597,6 +1597,39 @@ __global__ void k_oscan(FrameArgs a);
 __global__ void k_oraster(FrameArgs a);
 template <bool SH> __global__ void k_ofold(FrameArgs a);
 
+/* The legacy smooth path's shading (mop_sw_rasterize_triangle_smooth,
+ * rasterizer.c:1371-1420): interpolated normal and vertex colour, one
+ * directional light (light_dir) with ambient, a view-independent Blinn-Phong
+ * term of power 32 and weight 0.25, clamped at zero. */
+__device__ void shade_legacy(const FrameArgs &a, const DrawRec &d, const uint32_t v[3],
+                             const float4 N[3], const float pc[3], float out[3]) {
+  const float4 C0 = a.color[v[0]], C1 = a.color[v[1]], C2 = a.color[v[2]];
+  const V3 n = norm3(mk3(pc[0] * N[0].x + pc[1] * N[1].x + pc[2] * N[2].x,
+                         pc[0] * N[0].y + pc[1] * N[1].y + pc[2] * N[2].y,
+                         pc[0] * N[0].z + pc[1] * N[1].z + pc[2] * N[2].z));
+  const float fr = pc[0] * C0.x + pc[1] * C1.x + pc[2] * C2.x;
+  const float fg = pc[0] * C0.y + pc[1] * C1.y + pc[2] * C2.y;
+  const float fb = pc[0] * C0.z + pc[1] * C1.z + pc[2] * C2.z;
+  const V3 nl = norm3(mk3(d.light_dir[0], d.light_dir[1], d.light_dir[2]));
+  float ndotl = dot3(n, nl);
+  if (ndotl < 0.0f)
+    ndotl = 0.0f;
+  const float lit = d.ambient + (1.0f - d.ambient) * ndotl;
+  const V3 hv = norm3(mk3(nl.x, nl.y + 1.0f, nl.z));
+  float ndoth = dot3(n, hv);
+  if (ndoth < 0.0f)
+    ndoth = 0.0f;
+  float spec = ndoth * ndoth;
+  spec *= spec;
+  spec *= spec;
+  spec *= spec;
+  spec *= spec;
+  spec *= 0.25f;
+  const float p[3] = {fr * lit + spec, fg * lit + spec, fb * lit + spec};
+  for (int c = 0; c < 3; c++)
+    out[c] = p[c] < 0.0f ? 0.0f : p[c];
+}
+
 int mopcuda_launch_frame(const FrameArgs &a, const PostArgs &p, const LaunchCfg &cfg,
                          cudaStream_t s, cudaEvent_t *ev) {
   int launches = 0;
@@ -1926,9 +1959,7 @@ __global__ void __launch_bounds__(128) k_ofold(FrameArgs a) {
       pc[0] *= ip;
       pc[1] *= ip;
       pc[2] *= ip;
-      float p[3];
-      shade_smooth<SH>(a, d, a.lights + d.light_off, s.v, N, pc, p);
-      /* edge-distance coverage (rasterizer.c:1899-1938) */
+      /* edge-distance coverage (rasterizer.c:1899-1938, 1320-1361) */
       float min_d = 0.0f;
       for (int e = 0; e < 3; e++) {
         const float len = sqrtf(r.dx[e] * r.dx[e] + r.dy[e] * r.dy[e]);
@@ -1937,8 +1968,21 @@ __global__ void __launch_bounds__(128) k_ofold(FrameArgs a) {
         if (e == 0 || de < min_d)
           min_d = de;
       }
+      const bool legacy = !(d.flags & DF_LIT);
+      if (legacy && !(min_d >= 0.0f))
+        continue;
+      float p[3];
+      if (legacy)
+        shade_legacy(a, d, s.v, N, pc, p);
+      else
+        shade_smooth<SH>(a, d, a.lights + d.light_off, s.v, N, pc, p);
       const float op = d.opacity < 0.0f ? 0.0f : (d.opacity > 1.0f ? 1.0f : d.opacity);
-      const float cov = (min_d < 1.0f && d.blend_mode != 0) ? min_d : 1.0f;
+      /* the legacy path blends at silhouettes only: where the sample's depth
+       * so far lies clearly behind the fragment (rasterizer.c:1425-1429);
+       * the multi-light path blends at every edge of a non-opaque draw
+       * (rasterizer.c:2097-2100) */
+      const float cov = legacy ? ((min_d < 1.0f && (depth - z) > 0.005f) ? min_d : 1.0f)
+                               : ((min_d < 1.0f && d.blend_mode != 0) ? min_d : 1.0f);
       const float fa = op * cov;
       if (d.blend_mode == 0 && fa >= 1.0f) {
         hdr[0] = p[0];

@@ -581,10 +581,12 @@ extern "C" int mopcuda_frame_begin(MopCudaDevice *d, MopCudaFramebuffer *fb, con
 
 static float clamp01f(float x) { return x < 0.0f ? 0.0f : (x > 1.0f ? 1.0f : x); }
 
-/* Records one draw.  Order-independent opaque state is rendered exactly;
- * zero-opacity draws are colour no-ops in the reference and are dropped;
- * blended, wireframe, depth-test-off and unlit smooth (edge-AA) draws depend
- * on submission order and are reported as unsupported. */
+/* Records one draw.  Opaque lit draws and flat draws are order-independent;
+ * blended lit smooth draws and unlit smooth draws (the legacy path with
+ * silhouette edge AA) depend on submission order and start the frame's
+ * ordered suffix; zero-opacity draws are colour no-ops in the reference and
+ * are dropped; wireframe, depth-test-off, depth-write-off and blended flat
+ * draws are reported as unsupported. */
 int mc_build_draw(const MopCudaDraw *c, const float *model, const float *mvp,
                   std::vector<LightRec> &lights, DrawRec &r, bool &skip) {
   skip = false;
@@ -596,15 +598,11 @@ int mc_build_draw(const MopCudaDraw *c, const float *model, const float *mvp,
     return MOPCUDA_OK;
   }
   bool lit = c->lights && c->light_count > 0;
-  /* Supported: opaque draws (order-independent) and blended lit smooth
-   * draws (composited per sample in submission order).  Wireframe lines,
-   * depth test or write off, unlit smooth (edge-AA) and blended flat draws
-   * are not built. */
-  if (c->wireframe || !c->depth_test || !c->depth_write || (c->smooth && !lit) ||
+  if (c->wireframe || !c->depth_test || !c->depth_write ||
       (!c->smooth && (c->blend_mode != 0 || op < 1.0f))) {
     return fail(MOPCUDA_EUNSUPPORTED,
-                "draw: wireframe / depth-test-off / depth-write-off / unlit-smooth / blended "
-                "flat state is not implemented");
+                "draw: wireframe / depth-test-off / depth-write-off / blended flat state is not "
+                "implemented");
   }
   uint32_t stride = 48;
   memset(&r, 0, sizeof r);
@@ -735,8 +733,10 @@ static int record_draw(MopCudaDevice *d, const MopCudaDraw *c, const float *mode
     d->skipped_draws++;
     return MOPCUDA_OK;
   }
-  /* the first blended draw starts the ordered suffix of the frame */
-  if ((r.blend_mode != 0 || clamp01f(r.opacity) < 1.0f) && d->ordered_from == UINT32_MAX)
+  /* the first blended or unlit smooth draw starts the ordered suffix */
+  const bool legacy = (r.flags & DF_SMOOTH) && !(r.flags & DF_LIT);
+  if ((r.blend_mode != 0 || clamp01f(r.opacity) < 1.0f || legacy) &&
+      d->ordered_from == UINT32_MAX)
     d->ordered_from = (uint32_t)d->draws.size();
   d->draws.push_back(r);
   return MOPCUDA_OK;

@@ -7,7 +7,8 @@ point, spot, ranged, inactive lights), textures, SSAA 2, IBL, flat shading
 (lit and unlit), near-plane clipping (the config-1 ground plane passes
 behind the camera), coplanar draw-order ties, the clipping/depth stress scene
 (near-plane straddlers, coplanar pairs, host-skinned meshes), blended meshes
-(alpha, additive, multiply) in the core's transparent-pass order, directional
+(alpha, additive, multiply) in the core's transparent-pass order, unlit
+smooth draws (the legacy path's silhouette edge AA), directional
 lights shadowed through the shadow pass (the shadow map itself compared
 texel for texel), and picks.
 """
@@ -65,6 +66,11 @@ CASES = {
     "transparent": lambda: scenes.transparent_scene(seed=21),
     "transparent_ssaa2_ibl": lambda: scenes.transparent_scene(seed=22, ssaa=2, env=1),
     "transparent_config2": lambda: _transparent_config2(),
+    # no lights: the legacy smooth path with silhouette edge AA (order-dependent)
+    "unlit_smooth": lambda: scenes.small_scene(seed=56, lights="none"),
+    "unlit_smooth_ssaa2": lambda: scenes.small_scene(seed=57, lights="none", ssaa=2),
+    "unlit_transparent": lambda: dataclasses.replace(scenes.transparent_scene(seed=58),
+                                                     lights=[]),
     # shadow pass + 3x3 PCF on every directional light (one casting, one not)
     "shadow": lambda: scenes.shadow_scene(seed=51),
     "shadow_flat": lambda: dataclasses.replace(scenes.shadow_scene(seed=52), smooth=False),
