@@ -314,6 +314,16 @@ const float *mopcuda_read_depth(MopCudaDevice *dev, MopCudaFramebuffer *fb, int 
  * viewport.c:3385-3411) into a caller buffer of (w/ssaa)*(h/ssaa)*4 bytes. */
 int mopcuda_read_color_resolved(MopCudaDevice *dev, MopCudaFramebuffer *fb, int ssaa,
                                 uint8_t *out, size_t out_size);
+/* The same image, read asynchronously (no reference counterpart): the copy
+ * into `out` (page-locked memory for a true overlap, mopcuda_host_alloc)
+ * starts on a separate copy stream when the frame completes, overlapping the
+ * next frame's work; ssaa must be 1 or the framebuffer's presentation
+ * factor.  mopcuda_readback_wait returns once the framebuffer's last
+ * requested image is in host memory (it completes the frame first when it
+ * is still pending). */
+int mopcuda_read_color_resolved_async(MopCudaDevice *dev, MopCudaFramebuffer *fb, int ssaa,
+                                      void *out, size_t out_size);
+int mopcuda_readback_wait(MopCudaDevice *dev, MopCudaFramebuffer *fb, int timeout_ms);
 uint32_t mopcuda_pick_read_id(MopCudaDevice *dev, MopCudaFramebuffer *fb, int x, int y);
 float mopcuda_pick_read_depth(MopCudaDevice *dev, MopCudaFramebuffer *fb, int x, int y);
 /* Batched pick at presentation pixels (mop_viewport_pick, viewport.c:3687):

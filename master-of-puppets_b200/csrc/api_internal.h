@@ -111,25 +111,40 @@ struct MopCudaFramebuffer {
   bool host_color = false, host_depth = false, host_ids = false;
   bool presented_valid = false;
   uint64_t frame_serial = 0;
+  /* asynchronous presented-colour readback: requested for the pending frame
+   * (issued once it completes) or in flight on the device's copy stream */
+  cudaEvent_t rb_done = nullptr;
+  bool rb_requested = false, rb_live = false;
+  void *rb_dst = nullptr;
+  size_t rb_size = 0;
+  int rb_ssaa = 1;
 };
 
 struct MopCudaDevice {
   int ordinal = 0;
   int num_sms = 148;
   cudaStream_t stream = nullptr;
+  cudaStream_t copy_stream = nullptr; /* asynchronous readbacks */
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   cudaEvent_t stage_ev[MOPCUDA_STAGES + 1] = {};
   bool stage_timing = false;
   float stage_ms[MOPCUDA_STAGES] = {};
   std::mutex mu;
-  /* recorded frame */
+  /* the launched frame (kept for a re-run after an overflow) */
   MopCudaFramebuffer *fb = nullptr;
   float clear[4] = {0, 0, 0, 1};
   std::vector<DrawRec> draws;
   std::vector<LightRec> lights;
   uint32_t unsupported_draws = 0;
   uint32_t skipped_draws = 0;
-  uint32_t ordered_from = UINT32_MAX; /* first draw of the blended suffix */
+  uint32_t ordered_from = UINT32_MAX; /* first draw of the ordered suffix */
+  /* the frame being recorded (frame_begin .. frame_end), while the previous
+   * one may still run on the device */
+  MopCudaFramebuffer *rec_fb = nullptr;
+  float rec_clear[4] = {0, 0, 0, 1};
+  std::vector<DrawRec> rec_draws;
+  std::vector<LightRec> rec_lights;
+  uint32_t rec_unsupported = 0, rec_skipped = 0, rec_ordered_from = UINT32_MAX;
   bool frame_open = false;
   bool pending = false;
   int frame_status = 0;

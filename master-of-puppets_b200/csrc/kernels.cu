@@ -1631,7 +1631,7 @@ __device__ void shade_legacy(const FrameArgs &a, const DrawRec &d, const uint32_
 }
 
 int mopcuda_launch_frame(const FrameArgs &a, const PostArgs &p, const LaunchCfg &cfg,
-                         cudaStream_t s, cudaEvent_t *ev) {
+                         cudaStream_t s, cudaEvent_t *ev, cudaEvent_t post_wait) {
   int launches = 0;
   const uint32_t S = (uint32_t)a.width * (uint32_t)a.height;
   if (ev)
@@ -1691,6 +1691,8 @@ int mopcuda_launch_frame(const FrameArgs &a, const PostArgs &p, const LaunchCfg 
   }
   if (ev)
     cudaEventRecord(ev[5], s);
+  if (post_wait) /* the previous frame's image may still be on its way to the host */
+    cudaStreamWaitEvent(s, post_wait, 0);
   const int sf = p.ssaa;
   dim3 pb(POST_BX, POST_BY);
   dim3 pg(blocks_for((uint32_t)(p.width / sf), POST_BX),

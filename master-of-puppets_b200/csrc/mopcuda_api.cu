@@ -53,6 +53,7 @@ extern "C" void mopcuda_host_free(void *p) {
 }
 
 static int finish_frame(MopCudaDevice *d, int timeout_ms);
+static int issue_readback(MopCudaDevice *d, MopCudaFramebuffer *fb);
 
 /* float x86-compatible evaluation of the post-process byte map
  * (postprocess.c:43-86 for one channel value) */
@@ -93,6 +94,7 @@ extern "C" MopCudaDevice *mopcuda_device_create(int ordinal) {
   cudaDeviceGetAttribute(&d->num_sms, cudaDevAttrMultiProcessorCount, ordinal);
   d->cfg.num_sms = d->num_sms;
   if (cudaStreamCreateWithFlags(&d->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&d->copy_stream, cudaStreamNonBlocking) != cudaSuccess ||
       cudaEventCreate(&d->ev0) != cudaSuccess || cudaEventCreate(&d->ev1) != cudaSuccess) {
     cudaGetLastError();
     fail(MOPCUDA_ECUDA, "stream/event creation failed");
@@ -105,6 +107,9 @@ extern "C" MopCudaDevice *mopcuda_device_create(int ordinal) {
   return d;
 }
 
+/* Polls the event: back to back for the first 2 ms (a frame usually ends
+ * within that, and a sleep would add the scheduler's wake-up latency to
+ * every frame), then every 20 us until the timeout. */
 int mc_bounded_sync(MopCudaDevice *d, cudaEvent_t ev, int timeout_ms) {
   struct timespec t0, t1;
   clock_gettime(CLOCK_MONOTONIC, &t0);
@@ -118,8 +123,10 @@ int mc_bounded_sync(MopCudaDevice *d, cudaEvent_t ev, int timeout_ms) {
     double ms = (t1.tv_sec - t0.tv_sec) * 1e3 + (t1.tv_nsec - t0.tv_nsec) * 1e-6;
     if (timeout_ms >= 0 && ms > (double)timeout_ms)
       return fail(MOPCUDA_ETIMEOUT, "frame did not complete within %d ms", timeout_ms);
-    struct timespec nap = {0, 20000};
-    nanosleep(&nap, nullptr);
+    if (ms > 2.0) {
+      struct timespec nap = {0, 20000};
+      nanosleep(&nap, nullptr);
+    }
   }
 }
 
@@ -174,6 +181,8 @@ extern "C" void mopcuda_device_destroy(MopCudaDevice *d) {
   for (int i = 0; i <= MOPCUDA_STAGES; i++)
     if (d->stage_ev[i])
       cudaEventDestroy(d->stage_ev[i]);
+  cudaStreamSynchronize(d->copy_stream);
+  cudaStreamDestroy(d->copy_stream);
   cudaStreamDestroy(d->stream);
   delete d;
 }
@@ -220,7 +229,8 @@ extern "C" void mopcuda_buffer_destroy(MopCudaDevice *d, MopCudaBuffer *b) {
     return;
   std::lock_guard<std::mutex> lk(d->mu);
   cudaSetDevice(d->ordinal);
-  mc_stream_sync(d, 10000); /* a launched frame may still read it */
+  mc_finish_pending(d);     /* a launched frame may still read it, or re-run */
+  mc_stream_sync(d, 10000);
   if (b->slab) {
     if (--b->slab->refs == 0) {
       cudaFree(b->slab->d);
@@ -239,7 +249,9 @@ extern "C" int mopcuda_buffer_update(MopCudaDevice *d, MopCudaBuffer *b, const v
     return fail(MOPCUDA_EINVAL, "buffer_update: range outside buffer");
   std::lock_guard<std::mutex> lk(d->mu);
   cudaSetDevice(d->ordinal);
-  int rc = mc_stream_sync(d, 10000);
+  int rc = mc_finish_pending(d); /* the launched frame reads the old contents */
+  if (!rc)
+    rc = mc_stream_sync(d, 10000);
   if (rc)
     return rc;
   if (b->h)
@@ -391,6 +403,14 @@ extern "C" void mopcuda_framebuffer_destroy(MopCudaDevice *d, MopCudaFramebuffer
   mc_stream_sync(d, 10000);
   if (d->fb == fb)
     d->fb = nullptr;
+  if (d->rec_fb == fb) {
+    d->rec_fb = nullptr;
+    d->frame_open = false;
+  }
+  if (fb->rb_live)
+    mc_bounded_sync(d, fb->rb_done, 10000);
+  if (fb->rb_done)
+    cudaEventDestroy(fb->rb_done);
   fb_release(fb);
   delete fb;
 }
@@ -560,21 +580,17 @@ extern "C" int mopcuda_frame_begin(MopCudaDevice *d, MopCudaFramebuffer *fb, con
     return fail(MOPCUDA_EINVAL, "frame_begin: bad arguments");
   std::lock_guard<std::mutex> lk(d->mu);
   cudaSetDevice(d->ordinal);
-  /* The previous frame must be complete (or re-run after an overflow) before
-   * its recorded draws and pinned staging are reused. */
-  if (d->pending) {
-    int rc = finish_frame(d, FRAME_TIMEOUT_MS);
-    if (rc)
-      return rc;
-  }
-  d->fb = fb;
+  /* Recording goes to its own lists: the previous frame may still run (its
+   * lists stay for a re-run after an overflow) and is completed at
+   * frame_end, so the host records while the device renders. */
+  d->rec_fb = fb;
   for (int k = 0; k < 4; k++)
-    d->clear[k] = clear ? clear[k] : 0.0f;
-  d->draws.clear();
-  d->lights.clear();
-  d->unsupported_draws = 0;
-  d->skipped_draws = 0;
-  d->ordered_from = UINT32_MAX;
+    d->rec_clear[k] = clear ? clear[k] : 0.0f;
+  d->rec_draws.clear();
+  d->rec_lights.clear();
+  d->rec_unsupported = 0;
+  d->rec_skipped = 0;
+  d->rec_ordered_from = UINT32_MAX;
   d->frame_open = true;
   return MOPCUDA_OK;
 }
@@ -724,21 +740,21 @@ static int record_draw(MopCudaDevice *d, const MopCudaDraw *c, const float *mode
                        const float *mvp) {
   DrawRec r;
   bool skip = false;
-  int rc = mc_build_draw(c, model, mvp, d->lights, r, skip);
+  int rc = mc_build_draw(c, model, mvp, d->rec_lights, r, skip);
   if (rc == MOPCUDA_EUNSUPPORTED)
-    d->unsupported_draws++;
+    d->rec_unsupported++;
   if (rc)
     return rc;
   if (skip) {
-    d->skipped_draws++;
+    d->rec_skipped++;
     return MOPCUDA_OK;
   }
   /* the first blended or unlit smooth draw starts the ordered suffix */
   const bool legacy = (r.flags & DF_SMOOTH) && !(r.flags & DF_LIT);
   if ((r.blend_mode != 0 || clamp01f(r.opacity) < 1.0f || legacy) &&
-      d->ordered_from == UINT32_MAX)
-    d->ordered_from = (uint32_t)d->draws.size();
-  d->draws.push_back(r);
+      d->rec_ordered_from == UINT32_MAX)
+    d->rec_ordered_from = (uint32_t)d->rec_draws.size();
+  d->rec_draws.push_back(r);
   return MOPCUDA_OK;
 }
 
@@ -746,7 +762,7 @@ extern "C" int mopcuda_draw(MopCudaDevice *d, MopCudaFramebuffer *fb, const MopC
   if (!d || !fb || !c)
     return fail(MOPCUDA_EINVAL, "draw: bad arguments");
   std::lock_guard<std::mutex> lk(d->mu);
-  if (!d->frame_open || d->fb != fb)
+  if (!d->frame_open || d->rec_fb != fb)
     return fail(MOPCUDA_EINVAL, "draw outside frame_begin/frame_end");
   return record_draw(d, c, c->model, c->mvp);
 }
@@ -756,7 +772,7 @@ extern "C" int mopcuda_draw_list(MopCudaDevice *d, MopCudaFramebuffer *fb, const
   if (!d || !fb || (n && !c))
     return fail(MOPCUDA_EINVAL, "draw_list: bad arguments");
   std::lock_guard<std::mutex> lk(d->mu);
-  if (!d->frame_open || d->fb != fb)
+  if (!d->frame_open || d->rec_fb != fb)
     return fail(MOPCUDA_EINVAL, "draw outside frame_begin/frame_end");
   for (uint32_t i = 0; i < n; i++) {
     int rc = record_draw(d, c + i, c[i].model, c[i].mvp);
@@ -787,7 +803,7 @@ extern "C" int mopcuda_draw_instanced(MopCudaDevice *d, MopCudaFramebuffer *fb,
   if (!d || !fb || !c || !view || !proj || (!inst && n))
     return fail(MOPCUDA_EINVAL, "draw_instanced: bad arguments");
   std::lock_guard<std::mutex> lk(d->mu);
-  if (!d->frame_open || d->fb != fb)
+  if (!d->frame_open || d->rec_fb != fb)
     return fail(MOPCUDA_EINVAL, "draw outside frame_begin/frame_end");
   for (uint32_t i = 0; i < n; i++) {
     float vm[16], mvp[16];
@@ -1002,7 +1018,8 @@ static int launch_frame(MopCudaDevice *d) {
                            cudaMemcpyHostToDevice, s));
   CU_TRY(cudaMemsetAsync(d->counters.p, 0, sizeof(Counters), s));
   d->launches += (uint64_t)mopcuda_launch_frame(a, p, d->cfg, s,
-                                                d->stage_timing ? d->stage_ev : nullptr);
+                                                d->stage_timing ? d->stage_ev : nullptr,
+                                                fb->rb_live ? fb->rb_done : nullptr);
   CU_TRY(cudaGetLastError());
   CU_TRY(cudaMemcpyAsync(d->h_counters.p, d->counters.p, sizeof(Counters), cudaMemcpyDeviceToHost,
                          s));
@@ -1040,8 +1057,11 @@ static int finish_frame(MopCudaDevice *d, int timeout_ms) {
       for (int i = 0; i < MOPCUDA_STAGES; i++)
         cudaEventElapsedTime(&d->stage_ms[i], d->stage_ev[i], d->stage_ev[i + 1]);
     const Counters *c = d->h_counters.as<Counters>();
-    if (!c->overflow)
+    if (!c->overflow) {
+      if (d->fb && d->fb->rb_requested)
+        return issue_readback(d, d->fb);
       break;
+    }
     if (attempt >= 4)
       return fail(MOPCUDA_ENOMEM, "frame arenas overflowed repeatedly (flags %u)", c->overflow);
     d->rec_hint = c->rec_count + c->rec_count / 4 + 1024;
@@ -1074,11 +1094,23 @@ extern "C" int mopcuda_frame_end(MopCudaDevice *d, MopCudaFramebuffer *fb) {
   if (!d || !fb)
     return fail(MOPCUDA_EINVAL, "frame_end: bad arguments");
   std::lock_guard<std::mutex> lk(d->mu);
-  if (!d->frame_open || d->fb != fb)
+  if (!d->frame_open || d->rec_fb != fb)
     return fail(MOPCUDA_EINVAL, "frame_end without frame_begin");
   d->frame_open = false;
   cudaSetDevice(d->ordinal);
-  int rc = launch_frame(d);
+  /* the previous frame completes (or re-runs) with its own lists before its
+   * pinned staging is reused */
+  int rc;
+  if (d->pending && (rc = finish_frame(d, FRAME_TIMEOUT_MS)))
+    return rc;
+  d->fb = d->rec_fb;
+  memcpy(d->clear, d->rec_clear, sizeof d->clear);
+  d->draws.swap(d->rec_draws);
+  d->lights.swap(d->rec_lights);
+  d->unsupported_draws = d->rec_unsupported;
+  d->skipped_draws = d->rec_skipped;
+  d->ordered_from = d->rec_ordered_from;
+  rc = launch_frame(d);
   if (rc)
     return rc;
   if (d->unsupported_draws)
@@ -1348,6 +1380,57 @@ extern "C" int mopcuda_read_color_resolved(MopCudaDevice *d, MopCudaFramebuffer 
   }
   CU_TRY(cudaMemcpyAsync(out, src, need, cudaMemcpyDeviceToHost, d->stream));
   return mc_stream_sync(d, FRAME_TIMEOUT_MS);
+}
+
+/* Asynchronous readback of the presented image (no reference counterpart:
+ * the synchronous read is mop_viewport_read_color).  The copy runs on the
+ * device's copy stream once the frame has completed, so it overlaps the next
+ * frame's work; the next frame's post pass, which overwrites the image,
+ * waits for it. */
+static int issue_readback(MopCudaDevice *d, MopCudaFramebuffer *fb) {
+  fb->rb_requested = false;
+  if (!fb->rb_done)
+    CU_TRY(cudaEventCreateWithFlags(&fb->rb_done, cudaEventDisableTiming));
+  const void *src = fb->rb_ssaa > 1 ? fb->presented.p : fb->out.p;
+  CU_TRY(cudaStreamWaitEvent(d->copy_stream, d->ev1, 0));
+  CU_TRY(cudaMemcpyAsync(fb->rb_dst, src, fb->rb_size, cudaMemcpyDeviceToHost, d->copy_stream));
+  CU_TRY(cudaEventRecord(fb->rb_done, d->copy_stream));
+  fb->rb_live = true;
+  return MOPCUDA_OK;
+}
+
+extern "C" int mopcuda_read_color_resolved_async(MopCudaDevice *d, MopCudaFramebuffer *fb,
+                                                 int sf, void *out, size_t out_size) {
+  if (!d || !fb || !out || sf <= 0 || fb->w % sf || fb->h % sf)
+    return fail(MOPCUDA_EINVAL, "read_color_resolved_async: bad arguments");
+  std::lock_guard<std::mutex> lk(d->mu);
+  cudaSetDevice(d->ordinal);
+  if (sf > 1 && fb->ssaa != sf)
+    return fail(MOPCUDA_EINVAL, "read_color_resolved_async: SSAA %d is not the framebuffer's "
+                                "presentation factor %d", sf, fb->ssaa);
+  const size_t need = (size_t)(fb->w / sf) * (size_t)(fb->h / sf) * 4;
+  if (out_size < need)
+    return fail(MOPCUDA_EINVAL, "read_color_resolved_async: buffer too small");
+  fb->rb_dst = out;
+  fb->rb_size = need;
+  fb->rb_ssaa = sf;
+  fb->rb_requested = true;
+  if (d->fb == fb && d->pending)
+    return MOPCUDA_OK; /* issued when the frame completes */
+  return issue_readback(d, fb);
+}
+
+extern "C" int mopcuda_readback_wait(MopCudaDevice *d, MopCudaFramebuffer *fb, int timeout_ms) {
+  if (!d || !fb)
+    return fail(MOPCUDA_EINVAL, "readback_wait: bad arguments");
+  std::lock_guard<std::mutex> lk(d->mu);
+  cudaSetDevice(d->ordinal);
+  int rc;
+  if (fb->rb_requested && d->fb == fb && d->pending && (rc = finish_frame(d, timeout_ms)))
+    return rc;
+  if (!fb->rb_live)
+    return MOPCUDA_OK;
+  return mc_bounded_sync(d, fb->rb_done, timeout_ms);
 }
 
 /* Presentation factor of a framebuffer: lets frame_end fuse the SSAA box

@@ -157,6 +157,8 @@ SIGNATURES = [
     ("mopcuda_read_object_id", _P, [_P, _P, _P, _P]),
     ("mopcuda_read_depth", _P, [_P, _P, _P, _P]),
     ("mopcuda_read_color_resolved", C.c_int, [_P, _P, C.c_int, _P, C.c_size_t]),
+    ("mopcuda_read_color_resolved_async", C.c_int, [_P, _P, C.c_int, _P, C.c_size_t]),
+    ("mopcuda_readback_wait", C.c_int, [_P, _P, C.c_int]),
     ("mopcuda_pick_read_id", C.c_uint32, [_P, _P, C.c_int, C.c_int]),
     ("mopcuda_pick_read_depth", C.c_float, [_P, _P, C.c_int, C.c_int]),
     ("mopcuda_pick_batch", C.c_int, [_P, _P, C.c_int, _P, C.c_uint32, _P, _P, _P]),
@@ -480,6 +482,7 @@ class SceneRenderer(_Resident):
         # the core's pass order: opaque meshes, then blended ones back to front
         self.draws = [self.draw_struct(k, self.view, self.proj, self.eye)
                       for k in scenes.draw_order(self.scene, self.eye)]
+        self.draw_array = (MopCudaDraw * max(1, len(self.draws)))(*self.draws)
 
     def shadow_pass(self) -> bool:
         """pass_shadow through the C ABI (reference viewport.c:2288-2442):
@@ -489,7 +492,7 @@ class SceneRenderer(_Resident):
         import scenes
         L, d, sc = self.L, self.dev.h, self.scene
         light = scenes.shadow_light(sc)
-        casters = scenes.shadow_casters(sc)
+        casters = scenes.shadow_casters(sc) if light is not None else []
         if light is None or not casters:
             if self._shadow_bound:
                 _check(L.mopcuda_shadow_clear(d), "shadow_clear")
@@ -528,8 +531,7 @@ class SceneRenderer(_Resident):
         L, d, fb = self.L, self.dev.h, self.fb
         self.shadow_pass()
         _check(L.mopcuda_frame_begin(d, fb, self.clear), "frame_begin")
-        for dr in self.draws:
-            _check(L.mopcuda_draw(d, fb, C.byref(dr)), "draw")
+        _check(L.mopcuda_draw_list(d, fb, self.draw_array, len(self.draws)), "draw_list")
         _check(L.mopcuda_frame_end(d, fb), "frame_end")
 
     def wait(self, timeout_ms: int = 20000):
@@ -569,6 +571,18 @@ class SceneRenderer(_Resident):
         _check(self.L.mopcuda_read_color_resolved(self.dev.h, self.fb, sc.ssaa, out.ctypes.data,
                                                   out.nbytes), "read_color_resolved")
         return out
+
+    def color_async(self, out):
+        """Requests the presented image into `out` (a page-locked uint8
+        [height, width, 4] array for a true overlap); it is copied on the
+        copy stream once the frame completes, overlapping the next frame."""
+        sc = self.scene
+        _check(self.L.mopcuda_read_color_resolved_async(self.dev.h, self.fb, sc.ssaa,
+                                                        out.ctypes.data, out.nbytes),
+               "read_color_resolved_async")
+
+    def wait_readback(self, timeout_ms: int = 20000):
+        _check(self.L.mopcuda_readback_wait(self.dev.h, self.fb, timeout_ms), "readback_wait")
 
     def pick(self, xy):
         xy = np.ascontiguousarray(xy, np.int32)

@@ -169,3 +169,33 @@ def test_shadow_clear_unbinds(cuda_device):
         assert (plain != shadowed).any()
     finally:
         r.close()
+
+
+@pytest.mark.parametrize("ssaa", [1, 2])
+def test_async_readback_matches_sync(cuda_device, ssaa):
+    """mopcuda_read_color_resolved_async: frames submitted back to back with
+    their images requested asynchronously (each copy overlapping the next
+    frame) equal the synchronous reads of the same frames."""
+    sc = scenes.small_scene(seed=59, ssaa=ssaa)
+    eyes = [(4.0, 3.0, 7.0), (-5.0, 2.0, 5.0), (2.0, 6.0, -6.0), (6.0, 1.5, 1.0)]
+    r = mopcuda.SceneRenderer(cuda_device, sc)
+    bufs = [mopcuda.HostArray((sc.height, sc.width, 4), np.uint8) for _ in eyes]
+    try:
+        want = []
+        for e in eyes:
+            sc.eye = e
+            r.update_camera()
+            r.render()
+            want.append(r.color())
+        for k, e in enumerate(eyes):
+            sc.eye = e
+            r.update_camera()
+            r.submit()
+            r.color_async(bufs[k].a)
+        r.wait_readback()
+        for k in range(len(eyes)):
+            assert (bufs[k].a == want[k]).all(), f"frame {k}"
+    finally:
+        for b in bufs:
+            b.close()
+        r.close()
