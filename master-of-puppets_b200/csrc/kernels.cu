@@ -1935,14 +1935,27 @@ __global__ void __launch_bounds__(128) k_ofold(FrameArgs a) {
       const ShadeRec s = a.srec[rid];
       const DrawRec &d = a.draws[s.draw < a.draw_count ? s.draw : 0];
       const int jr = y - (int)r.y0, kc = x - (int)r.x0;
-      if (r.y1 & REC_FLAT_BIT) { /* flat: opaque only */
+      if (r.y1 & REC_FLAT_BIT) { /* rasterize_filled_triangle, rasterizer.c:1000-1083 */
         const float z = fold_add(fold_add(r.zc[0], r.zc[2], jr), r.zc[1], kc);
         if (z < depth) {
-          hdr[0] = s.col[0];
-          hdr[1] = s.col[1];
-          hdr[2] = s.col[2];
-          depth = z;
-          id = d.object_id;
+          const float ca = d.opacity < 0.0f ? 0.0f : (d.opacity > 1.0f ? 1.0f : d.opacity);
+          if (d.blend_mode == 0 && ca >= 1.0f) {
+            hdr[0] = s.col[0];
+            hdr[1] = s.col[1];
+            hdr[2] = s.col[2];
+            depth = z;
+            id = d.object_id;
+          } else { /* blended: colour only, no depth or ID write */
+            const float inv_a = 1.0f - ca;
+            for (int c = 0; c < 3; c++) {
+              if (d.blend_mode == 2)
+                hdr[c] = hdr[c] + s.col[c] * ca;
+              else if (d.blend_mode == 3)
+                hdr[c] = hdr[c] * s.col[c];
+              else
+                hdr[c] = s.col[c] * ca + hdr[c] * inv_a;
+            }
+          }
         }
         continue;
       }

@@ -597,12 +597,12 @@ extern "C" int mopcuda_frame_begin(MopCudaDevice *d, MopCudaFramebuffer *fb, con
 
 static float clamp01f(float x) { return x < 0.0f ? 0.0f : (x > 1.0f ? 1.0f : x); }
 
-/* Records one draw.  Opaque lit draws and flat draws are order-independent;
- * blended lit smooth draws and unlit smooth draws (the legacy path with
- * silhouette edge AA) depend on submission order and start the frame's
+/* Records one draw.  Opaque lit and opaque flat draws are order-independent;
+ * blended draws (smooth or flat) and unlit smooth draws (the legacy path
+ * with silhouette edge AA) depend on submission order and start the frame's
  * ordered suffix; zero-opacity draws are colour no-ops in the reference and
- * are dropped; wireframe, depth-test-off, depth-write-off and blended flat
- * draws are reported as unsupported. */
+ * are dropped; wireframe, depth-test-off and depth-write-off draws are
+ * reported as unsupported. */
 int mc_build_draw(const MopCudaDraw *c, const float *model, const float *mvp,
                   std::vector<LightRec> &lights, DrawRec &r, bool &skip) {
   skip = false;
@@ -614,11 +614,9 @@ int mc_build_draw(const MopCudaDraw *c, const float *model, const float *mvp,
     return MOPCUDA_OK;
   }
   bool lit = c->lights && c->light_count > 0;
-  if (c->wireframe || !c->depth_test || !c->depth_write ||
-      (!c->smooth && (c->blend_mode != 0 || op < 1.0f))) {
+  if (c->wireframe || !c->depth_test || !c->depth_write) {
     return fail(MOPCUDA_EUNSUPPORTED,
-                "draw: wireframe / depth-test-off / depth-write-off / blended flat state is not "
-                "implemented");
+                "draw: wireframe / depth-test-off / depth-write-off state is not implemented");
   }
   uint32_t stride = 48;
   memset(&r, 0, sizeof r);

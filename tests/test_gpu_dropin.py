@@ -36,6 +36,8 @@ CASES = {
     # blended meshes: the core's own transparent pass drives the ordered path
     "transparent": lambda: scenes.transparent_scene(seed=25),
     "transparent_ssaa2": lambda: scenes.transparent_scene(seed=26, width=128, height=96, ssaa=2),
+    "transparent_flat": lambda: dataclasses.replace(
+        scenes.transparent_scene(seed=62, width=128, height=96, ssaa=2), smooth=False),
     # no lights: the core's legacy smooth rasteriser (silhouette edge AA)
     "unlit_smooth": lambda: scenes.small_scene(seed=29, lights="none", width=192, height=144),
     # directional-light shadows: the core's pass_shadow vs the C-ABI shadow pass

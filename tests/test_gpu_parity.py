@@ -66,6 +66,9 @@ CASES = {
     "transparent": lambda: scenes.transparent_scene(seed=21),
     "transparent_ssaa2_ibl": lambda: scenes.transparent_scene(seed=22, ssaa=2, env=1),
     "transparent_config2": lambda: _transparent_config2(),
+    # blended flat draws (colour only, no depth or ID writes) in the transparent pass
+    "transparent_flat": lambda: dataclasses.replace(scenes.transparent_scene(seed=60),
+                                                    smooth=False),
     # no lights: the legacy smooth path with silhouette edge AA (order-dependent)
     "unlit_smooth": lambda: scenes.small_scene(seed=56, lights="none"),
     "unlit_smooth_ssaa2": lambda: scenes.small_scene(seed=57, lights="none", ssaa=2),

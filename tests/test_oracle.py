@@ -73,6 +73,8 @@ LIVE = {
     "shadow_flat": lambda: dataclasses.replace(scenes.shadow_scene(seed=32), smooth=False),
     "shadow_ssaa2_ibl": lambda: scenes.shadow_scene(seed=33, ssaa=2, env=1),
     "shadow_transparent": lambda: scenes.shadow_scene(seed=34, transparent=True),
+    "transparent_flat": lambda: dataclasses.replace(scenes.transparent_scene(seed=36),
+                                                    smooth=False),
     # no lights: legacy smooth path (silhouette edge AA) with blended meshes
     "unlit_transparent": lambda: dataclasses.replace(scenes.transparent_scene(seed=35),
                                                      lights=[]),
