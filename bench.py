@@ -441,12 +441,16 @@ def run_batched(dev, steps=10, warm=3, n_views=64):
             "note": "wall time per pass including every presented image read to host"}
 
 
-def run_served(dev, rates=(2000.0, 4000.0), duration=2.0, n_scenes=32):
+CAP_SAMPLES = 24 << 20  # samples per server launch (about two 1080p SSAA-2 views)
+
+
+def run_served(dev, rates=(2000.0, 4000.0, 6000.0), duration=2.0, n_scenes=32):
     """Served mix: resident scenes of log-normal size, Poisson render/pick
     requests; p50/p99 arrival-to-result latency and Mpix/s of the
-    continuous-batching server and of the plain per-viewport path on the
-    same trace; IDs/depth of a 1% sample checked bit-exact against the
-    request's own frame."""
+    continuous-batching server (and with launches capped at CAP_SAMPLES
+    samples) and of the plain per-viewport path on the same trace; IDs/depth
+    of a 1% sample checked bit-exact against the request's own frame in a
+    separate, untimed run of the same trace."""
     import mopcuda
     import scenes
     import serving
@@ -458,24 +462,38 @@ def run_served(dev, rates=(2000.0, 4000.0), duration=2.0, n_scenes=32):
                        "Poisson arrivals, 85% renders at 256^2/720p/1080p/1440p, 15% pick "
                        "batches of 1-64, 1% of a scene's instances moved per request",
            "server_config": {"max_views": 32, "max_inflight": 3, "hbm_budget_gib": 100},
+           "capped_config": {"max_launch_samples": CAP_SAMPLES},
            "rates": []}
+    keys = ("p50_ms", "p99_ms", "mpix_s")
     try:
         for rate in rates:
             warm = serving.make_trace(scs, rate, 0.5, seed=7 + int(rate))
             for r in warm:
                 r.moves = []
             trace = serving.make_trace(scs, rate, duration, seed=int(rate))
+            # timed runs keep no results for checking: copying a kept request's
+            # sample-resolution IDs and depth into pageable memory stalls the
+            # server's worker and would dominate the tail
+            runs = {}
+            for name, cap in (("server", 0), ("server_capped", CAP_SAMPLES)):
+                serving.reset_models(rss, scs)
+                r_ = serving.run_server(dev, rss, trace, hbm_budget=100 << 30, max_views=32,
+                                        max_inflight=3, warmup=warm, max_launch_samples=cap)
+                r_.pop("kept", None)
+                st = r_.pop("stats")
+                runs[name] = dict({k: round(r_[k], 3) for k in keys}, launches=st["launches"],
+                                  reruns=st["reruns"],
+                                  max_views_in_launch=st["max_views_in_launch"])
+            # exactness: the same trace again, every 100th render's IDs and depth kept
             serving.reset_models(rss, scs)
-            s = serving.run_server(dev, rss, trace, hbm_budget=100 << 30, max_views=32,
-                                   max_inflight=3, keep_every=100, warmup=warm)
-            chk = serving.check_kept(dev, rss, trace, s.pop("kept"))
+            k_ = serving.run_server(dev, rss, trace, hbm_budget=100 << 30, max_views=32,
+                                    max_inflight=3, keep_every=100, warmup=warm)
+            chk = serving.check_kept(dev, rss, trace, k_.pop("kept"))
+            serving.reset_models(rss, scs)
             p = serving.run_plain(dev, rss, trace, warmup=warm[:40])
-            st = s.pop("stats")
             out["rates"].append({
-                "req_per_s": rate, "requests": s["requests"],
-                "server": {k: round(s[k], 3) for k in ("p50_ms", "p99_ms", "mpix_s")},
-                "plain": {k: round(p[k], 3) for k in ("p50_ms", "p99_ms", "mpix_s")},
-                "server_launches": st["launches"], "max_views_in_launch": st["max_views_in_launch"],
+                "req_per_s": rate, "requests": len(trace), **runs,
+                "plain": {k: round(p[k], 3) for k in keys},
                 "exact_check": chk})
     finally:
         for rs in rss:

@@ -470,6 +470,9 @@ typedef struct MopCudaServerConfig {
   uint32_t max_views;       /* requests fused into one launch, 1..256 */
   uint32_t max_inflight;    /* launches on the device at once, 1..16 */
   uint32_t batch_window_us; /* after a launch, wait this long for more arrivals */
+  uint64_t max_launch_samples; /* samples of one launch at most (a larger request still runs,
+                                  alone); 0 = no limit.  Smaller launches finish sooner and
+                                  shorten the latency tail at some cost in throughput */
 } MopCudaServerConfig;
 
 #define MOPCUDA_REQ_RENDER 0u

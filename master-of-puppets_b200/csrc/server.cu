@@ -39,6 +39,7 @@ struct SrvRequest {
   Clock::time_point t_submit, t_done;
   int status = 0; /* 0 queued, 1 running, 2 done, < 0 error */
   uint64_t est_bytes = 0;
+  uint64_t samples = 0; /* width * height * ssaa^2 of the view */
   /* result staging offsets in the slot's pinned buffer */
   size_t off_color = 0, off_ids = 0, off_depth = 0, off_pick = 0;
   /* client buffers in page-locked memory receive their DMA directly */
@@ -304,15 +305,19 @@ static void srv_loop(MopCudaServer *s) {
       if (sl->busy || s->pending.empty())
         continue;
       std::vector<SrvRequest *> group;
-      uint64_t bytes = 0;
+      uint64_t bytes = 0, samples = 0;
       while (!s->pending.empty() && group.size() < s->cfg.max_views) {
         SrvRequest *r = s->pending.front();
         const bool fits = s->inflight_bytes + bytes + r->est_bytes <= s->cfg.hbm_budget;
         const bool alone = s->inflight_bytes == 0 && group.empty(); /* oversize: run it alone */
         if (!fits && !alone)
           break;
+        if (s->cfg.max_launch_samples && !group.empty() &&
+            samples + r->samples > s->cfg.max_launch_samples)
+          break; /* the launch is full: the rest wait for the next slot */
         group.push_back(r);
         bytes += r->est_bytes;
+        samples += r->samples;
         s->pending.pop_front();
       }
       if (group.empty())
@@ -468,6 +473,7 @@ extern "C" int mopcuda_server_submit(MopCudaServer *s, const MopCudaRequest *req
     const uint64_t S = (uint64_t)v.width * v.ssaa * v.height * v.ssaa;
     const uint64_t P = (uint64_t)v.width * v.height;
     r->est_bytes = mc_view_bytes(s->scenes[req->scene], S, P);
+    r->samples = S;
     s->max_view_samples = std::max<uint64_t>(s->max_view_samples, (S + 15) & ~(uint64_t)15);
     s->max_view_pixels = std::max<uint64_t>(s->max_view_pixels, (P + 15) & ~(uint64_t)15);
     r->models = mc_scene_models(s->scenes[req->scene]);

@@ -77,7 +77,8 @@ REQ_RENDER, REQ_PICK = 0, 1
 
 class MopCudaServerConfig(C.Structure):
     _fields_ = [("hbm_budget", C.c_uint64), ("max_views", C.c_uint32),
-                ("max_inflight", C.c_uint32), ("batch_window_us", C.c_uint32)]
+                ("max_inflight", C.c_uint32), ("batch_window_us", C.c_uint32),
+                ("max_launch_samples", C.c_uint64)]
 
 
 class MopCudaRequest(C.Structure):
@@ -776,10 +777,11 @@ class Server:
     (mopcuda_server_*)."""
 
     def __init__(self, device: Device, hbm_budget: int, max_views: int = 64,
-                 max_inflight: int = 3, batch_window_us: int = 0):
+                 max_inflight: int = 3, batch_window_us: int = 0, max_launch_samples: int = 0):
         self.dev = device
         self.L = device.L
-        cfg = MopCudaServerConfig(hbm_budget, max_views, max_inflight, batch_window_us)
+        cfg = MopCudaServerConfig(hbm_budget, max_views, max_inflight, batch_window_us,
+                                  max_launch_samples)
         self.h = self.L.mopcuda_server_create(device.h, C.byref(cfg))
         if not self.h:
             raise RuntimeError(f"server_create failed: {last_error()}")

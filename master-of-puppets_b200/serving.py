@@ -128,12 +128,14 @@ class _Ring:
 
 def run_server(dev, rss, trace: List[Request], hbm_budget: int, max_views: int = 64,
                max_inflight: int = 3, batch_window_us: int = 0, keep_every: int = 0,
-               ring: int = 64, warmup: Optional[List[Request]] = None) -> dict:
+               ring: int = 64, warmup: Optional[List[Request]] = None,
+               max_launch_samples: int = 0) -> dict:
     """Serve the trace (after serving `warmup`, untimed, on the same server).
     Render results land in rings of page-locked buffers per resolution
     (reused once their request completed); keep_every > 0 also keeps every
     k-th render's IDs and depth (for the exactness check) under "kept"."""
-    srv = mopcuda.Server(dev, hbm_budget, max_views, max_inflight, batch_window_us)
+    srv = mopcuda.Server(dev, hbm_budget, max_views, max_inflight, batch_window_us,
+                         max_launch_samples)
     rings = {(w, h): _Ring((h, w, 4), ring) for w, h in RESOLUTIONS}
     try:
         ids = [srv.add_scene(rs) for rs in rss]
