@@ -147,6 +147,11 @@ struct MopCudaDevice {
   uint32_t rec_unsupported = 0, rec_skipped = 0, rec_ordered_from = UINT32_MAX;
   bool frame_open = false;
   bool pending = false;
+  /* the completed frame whose readback frame_end issues inside the next
+   * launch, once that launch's upload and kernels up to shading are queued
+   * (issued earlier, the image copy delays the next frame's start) */
+  MopCudaFramebuffer *rb_defer = nullptr;
+  int rb_defer_rc = 0;
   int frame_status = 0;
   /* state */
   float exposure = 1.0f;

@@ -1631,7 +1631,8 @@ __device__ void shade_legacy(const FrameArgs &a, const DrawRec &d, const uint32_
 }
 
 int mopcuda_launch_frame(const FrameArgs &a, const PostArgs &p, const LaunchCfg &cfg,
-                         cudaStream_t s, cudaEvent_t *ev, cudaEvent_t post_wait) {
+                         cudaStream_t s, cudaEvent_t *ev, PrePostHook before_post,
+                         void *hook_ctx) {
   int launches = 0;
   const uint32_t S = (uint32_t)a.width * (uint32_t)a.height;
   if (ev)
@@ -1691,7 +1692,9 @@ int mopcuda_launch_frame(const FrameArgs &a, const PostArgs &p, const LaunchCfg 
   }
   if (ev)
     cudaEventRecord(ev[5], s);
-  if (post_wait) /* the previous frame's image may still be on its way to the host */
+  /* the previous frame's image may still be on its way to the host */
+  cudaEvent_t post_wait = before_post ? before_post(hook_ctx) : nullptr;
+  if (post_wait)
     cudaStreamWaitEvent(s, post_wait, 0);
   const int sf = p.ssaa;
   dim3 pb(POST_BX, POST_BY);

@@ -52,7 +52,7 @@ extern "C" void mopcuda_host_free(void *p) {
     cudaFreeHost(p);
 }
 
-static int finish_frame(MopCudaDevice *d, int timeout_ms);
+static int finish_frame(MopCudaDevice *d, int timeout_ms, bool defer_readback = false);
 static int issue_readback(MopCudaDevice *d, MopCudaFramebuffer *fb);
 
 /* float x86-compatible evaluation of the post-process byte map
@@ -857,6 +857,19 @@ void mc_post_args(const MopCudaDevice *d, PostArgs &p) {
   }
 }
 
+/* Runs between a launch's shading and its post pass: issues the previous
+ * frame's deferred readback, then names the readback the post pass must wait
+ * for (this framebuffer's image may still be on its way to the host). */
+static cudaEvent_t frame_pre_post(void *ctx) {
+  MopCudaDevice *d = (MopCudaDevice *)ctx;
+  if (d->rb_defer) {
+    MopCudaFramebuffer *prev = d->rb_defer;
+    d->rb_defer = nullptr;
+    d->rb_defer_rc = issue_readback(d, prev);
+  }
+  return d->fb->rb_live ? d->fb->rb_done : nullptr;
+}
+
 static int launch_frame(MopCudaDevice *d) {
   MopCudaFramebuffer *fb = d->fb;
   const uint32_t nd = (uint32_t)d->draws.size();
@@ -1015,9 +1028,10 @@ static int launch_frame(MopCudaDevice *d) {
     CU_TRY(cudaMemcpyAsync(d->d_lights.p, d->h_lights.p, sizeof(LightRec) * d->lights.size(),
                            cudaMemcpyHostToDevice, s));
   CU_TRY(cudaMemsetAsync(d->counters.p, 0, sizeof(Counters), s));
+  d->rb_defer_rc = MOPCUDA_OK;
   d->launches += (uint64_t)mopcuda_launch_frame(a, p, d->cfg, s,
                                                 d->stage_timing ? d->stage_ev : nullptr,
-                                                fb->rb_live ? fb->rb_done : nullptr);
+                                                frame_pre_post, d);
   CU_TRY(cudaGetLastError());
   CU_TRY(cudaMemcpyAsync(d->h_counters.p, d->counters.p, sizeof(Counters), cudaMemcpyDeviceToHost,
                          s));
@@ -1028,7 +1042,7 @@ static int launch_frame(MopCudaDevice *d) {
   d->pending = true;
   d->io_h2d = sizeof(DrawRec) * (uint64_t)nd + sizeof(LightRec) * (uint64_t)d->lights.size();
   d->io_d2h = sizeof(Counters);
-  return MOPCUDA_OK;
+  return d->rb_defer_rc; /* the previous frame's readback, issued by the hook */
 }
 
 extern "C" int mopcuda_frame_io_bytes(MopCudaDevice *d, uint64_t *h2d, uint64_t *d2h) {
@@ -1042,7 +1056,7 @@ extern "C" int mopcuda_frame_io_bytes(MopCudaDevice *d, uint64_t *h2d, uint64_t 
 
 /* Waits for the launched frame; re-runs it with larger arenas if any
  * capacity overflowed (the counters say by how much). */
-static int finish_frame(MopCudaDevice *d, int timeout_ms) {
+static int finish_frame(MopCudaDevice *d, int timeout_ms, bool defer_readback) {
   for (int attempt = 0; d->pending; attempt++) {
     int rc = mc_bounded_sync(d, d->ev1, timeout_ms);
     if (rc) {
@@ -1056,8 +1070,13 @@ static int finish_frame(MopCudaDevice *d, int timeout_ms) {
         cudaEventElapsedTime(&d->stage_ms[i], d->stage_ev[i], d->stage_ev[i + 1]);
     const Counters *c = d->h_counters.as<Counters>();
     if (!c->overflow) {
-      if (d->fb && d->fb->rb_requested)
+      if (d->fb && d->fb->rb_requested) {
+        if (defer_readback) {
+          d->rb_defer = d->fb; /* issued inside the caller's next launch */
+          return MOPCUDA_OK;
+        }
         return issue_readback(d, d->fb);
+      }
       break;
     }
     if (attempt >= 4)
@@ -1099,7 +1118,7 @@ extern "C" int mopcuda_frame_end(MopCudaDevice *d, MopCudaFramebuffer *fb) {
   /* the previous frame completes (or re-runs) with its own lists before its
    * pinned staging is reused */
   int rc;
-  if (d->pending && (rc = finish_frame(d, FRAME_TIMEOUT_MS)))
+  if (d->pending && (rc = finish_frame(d, FRAME_TIMEOUT_MS, true)))
     return rc;
   d->fb = d->rec_fb;
   memcpy(d->clear, d->rec_clear, sizeof d->clear);
@@ -1109,6 +1128,13 @@ extern "C" int mopcuda_frame_end(MopCudaDevice *d, MopCudaFramebuffer *fb) {
   d->skipped_draws = d->rec_skipped;
   d->ordered_from = d->rec_ordered_from;
   rc = launch_frame(d);
+  if (d->rb_defer) { /* the launch stopped before its post pass */
+    MopCudaFramebuffer *prev = d->rb_defer;
+    d->rb_defer = nullptr;
+    int rrc = issue_readback(d, prev);
+    if (!rc)
+      rc = rrc;
+  }
   if (rc)
     return rc;
   if (d->unsupported_draws)

@@ -415,10 +415,13 @@ int mopcuda_launch_batch(const BatchArgs &b, const PostArgs *posts, const uint32
 
 /* ev (optional, 7 events): stage boundaries
  * vertex | setup+clip | raster | resolve | shade | post */
-/* post_wait: an event the post pass waits for (the previous readback of the
- * framebuffer it overwrites), or null. */
+/* before_post (optional): called on the host once the kernels up to shading
+ * are queued, before the post pass is; returns an event the post pass waits
+ * for (the readback of the image it overwrites), or null. */
+typedef cudaEvent_t (*PrePostHook)(void *ctx);
 int mopcuda_launch_frame(const FrameArgs &a, const PostArgs &p, const LaunchCfg &cfg,
-                         cudaStream_t s, cudaEvent_t *ev, cudaEvent_t post_wait = nullptr);
+                         cudaStream_t s, cudaEvent_t *ev, PrePostHook before_post = nullptr,
+                         void *hook_ctx = nullptr);
 int mopcuda_launch_fp32_peak(float *out, int blocks, int iters, cudaStream_t s);
 #define MOPCUDA_STAGES 6
 int mopcuda_launch_box(const uchar4 *src, int width, int height, int sf, uchar4 *dst,

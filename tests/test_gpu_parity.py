@@ -174,13 +174,17 @@ def test_shadow_clear_unbinds(cuda_device):
         r.close()
 
 
-@pytest.mark.parametrize("ssaa", [1, 2])
-def test_async_readback_matches_sync(cuda_device, ssaa):
+@pytest.mark.parametrize("ssaa,width,height", [(1, 160, 120), (2, 160, 120),
+                                               (2, 1920, 1080)])
+def test_async_readback_matches_sync(cuda_device, ssaa, width, height):
     """mopcuda_read_color_resolved_async: frames submitted back to back with
-    their images requested asynchronously (each copy overlapping the next
-    frame) equal the synchronous reads of the same frames."""
-    sc = scenes.small_scene(seed=59, ssaa=ssaa)
-    eyes = [(4.0, 3.0, 7.0), (-5.0, 2.0, 5.0), (2.0, 6.0, -6.0), (6.0, 1.5, 1.0)]
+    their images requested asynchronously (each copy issued inside the next
+    frame's launch and overlapping it) equal the synchronous reads of the
+    same frames.  At 1920x1080 an image copy outlasts the next frame's work
+    up to its post pass, which must wait for it."""
+    sc = scenes.small_scene(seed=59, ssaa=ssaa, width=width, height=height)
+    eyes = [(4.0, 3.0, 7.0), (-5.0, 2.0, 5.0), (2.0, 6.0, -6.0), (6.0, 1.5, 1.0),
+            (-3.0, 4.0, -5.0), (5.0, 5.0, 3.0)]
     r = mopcuda.SceneRenderer(cuda_device, sc)
     bufs = [mopcuda.HostArray((sc.height, sc.width, 4), np.uint8) for _ in eyes]
     try:
