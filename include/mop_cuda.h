@@ -268,11 +268,25 @@ int mopcuda_scene_file_upload_all(MopCudaDevice *dev, const MopCudaSceneFile *fi
  * shadow_end rasterises the casters on the device stream and binds the map
  * for this device's later frames, where every directional light's diffuse
  * and specular terms take the 3x3 PCF factor (rasterizer.c:303-348,
- * 1580-1583, 1677-1680, 1802-1805) until shadow_clear. */
+ * 1580-1583, 1677-1680, 1802-1805) until shadow_clear.  A frame keeps the
+ * map bound at its frame_end; two maps alternate, so a pass recorded while
+ * that frame runs does not wait for it. */
 int mopcuda_shadow_begin(MopCudaDevice *dev, int size, const float light_vp[16]);
 int mopcuda_shadow_draw(MopCudaDevice *dev, const MopCudaBuffer *vertices, uint32_t vertex_count,
                         uint32_t stride, const MopCudaBuffer *indices, uint32_t index_count,
                         const float model[16]);
+/* n casters in array order, exactly as n shadow_draw calls (no reference
+ * counterpart: for hosts that keep their casters in an array; stops at the
+ * first caster that fails). */
+typedef struct MopCudaShadowCaster {
+  const MopCudaBuffer *vertices;
+  uint32_t vertex_count;
+  uint32_t stride;
+  const MopCudaBuffer *indices;
+  uint32_t index_count;
+  float model[16];
+} MopCudaShadowCaster;
+int mopcuda_shadow_draw_list(MopCudaDevice *dev, const MopCudaShadowCaster *casters, uint32_t n);
 int mopcuda_shadow_end(MopCudaDevice *dev);
 int mopcuda_shadow_clear(MopCudaDevice *dev);
 /* Device time of the last shadow pass (map clear + raster), waiting for it

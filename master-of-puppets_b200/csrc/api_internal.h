@@ -178,12 +178,16 @@ struct MopCudaDevice {
   uint32_t frag_hint = 0, olist_hint = 0;
   HostArena h_deform;
   /* shadow pass: casters recorded between shadow_begin and shadow_end; the
-   * map then stays bound for the device's frames until shadow_clear */
+   * map then stays bound for the device's frames until shadow_clear.  Two
+   * maps alternate, so a pass does not wait for the frame in flight, which
+   * (or its re-run) reads the other one: fr_sh is the map a launched frame
+   * was bound to at its frame_end (-1: none) and fr_sh_size its size. */
   std::vector<ShadowDraw> sh_draws;
   bool sh_open = false, sh_bound = false;
-  int sh_rec_size = 0, sh_size = 0;
+  int sh_rec_size = 0, sh_size = 0, sh_cur = 0;
+  int fr_sh = -1, fr_sh_size = 0;
   float sh_rec_vp[16] = {};
-  DevArena sh_map, sh_d_draws, sh_recs, sh_items, sh_ctr;
+  DevArena sh_map[2], sh_d_draws, sh_recs, sh_items, sh_ctr;
   HostArena sh_h_draws;
   cudaEvent_t sh_ev = nullptr; /* after the caster table's upload */
   bool sh_ev_live = false;

@@ -154,7 +154,7 @@ extern "C" void mopcuda_device_destroy(MopCudaDevice *d) {
                         &d->clipq,    &d->keys,       &d->large_list,  &d->large_items,
                         &d->shade_list, &d->counters, &d->pick_xy,     &d->pick_out,
                         &d->deform_params, &d->hdr, &d->frag_head, &d->frags, &d->touched,
-                        &d->olist, &d->olist_items, &d->sh_map, &d->sh_d_draws,
+                        &d->olist, &d->olist_items, &d->sh_map[0], &d->sh_map[1], &d->sh_d_draws,
                         &d->sh_recs, &d->sh_items, &d->sh_ctr, &d->env, &d->ibl_tab};
   for (DevArena *a : arenas)
     a->release();
@@ -1001,10 +1001,11 @@ static int launch_frame(MopCudaDevice *d) {
     a.olist_cap = ocap;
   }
 
-  if (d->sh_bound) {
-    a.shadow_keys = d->sh_map.as<uint32_t>();
-    a.shadow_vp = (const float *)(d->sh_map.as<uint8_t>() + 4 * (size_t)d->sh_size * d->sh_size);
-    a.shadow_w = a.shadow_h = d->sh_size;
+  if (d->fr_sh >= 0) { /* the map bound at this frame's frame_end */
+    const DevArena &m = d->sh_map[d->fr_sh];
+    a.shadow_keys = m.as<uint32_t>();
+    a.shadow_vp = (const float *)(m.as<uint8_t>() + 4 * (size_t)d->fr_sh_size * d->fr_sh_size);
+    a.shadow_w = a.shadow_h = d->fr_sh_size;
   }
 
   PostArgs p;
@@ -1127,6 +1128,8 @@ extern "C" int mopcuda_frame_end(MopCudaDevice *d, MopCudaFramebuffer *fb) {
   d->unsupported_draws = d->rec_unsupported;
   d->skipped_draws = d->rec_skipped;
   d->ordered_from = d->rec_ordered_from;
+  d->fr_sh = d->sh_bound ? d->sh_cur : -1;
+  d->fr_sh_size = d->sh_size;
   rc = launch_frame(d);
   if (d->rb_defer) { /* the launch stopped before its post pass */
     MopCudaFramebuffer *prev = d->rb_defer;
@@ -1168,15 +1171,12 @@ extern "C" int mopcuda_shadow_begin(MopCudaDevice *d, int size, const float ligh
   return MOPCUDA_OK;
 }
 
-extern "C" int mopcuda_shadow_draw(MopCudaDevice *d, const MopCudaBuffer *vertices,
-                                   uint32_t vertex_count, uint32_t stride,
-                                   const MopCudaBuffer *indices, uint32_t index_count,
-                                   const float model[16]) {
-  if (!d || !vertices || !indices || !model)
+/* One caster of the open pass (the device lock held). */
+static int add_caster(MopCudaDevice *d, const MopCudaBuffer *vertices, uint32_t vertex_count,
+                      uint32_t stride, const MopCudaBuffer *indices, uint32_t index_count,
+                      const float model[16]) {
+  if (!vertices || !indices)
     return fail(MOPCUDA_EINVAL, "shadow_draw: bad arguments");
-  std::lock_guard<std::mutex> lk(d->mu);
-  if (!d->sh_open)
-    return fail(MOPCUDA_EINVAL, "shadow_draw outside shadow_begin/shadow_end");
   if (stride < 12 || stride % 4 != 0)
     return fail(MOPCUDA_EINVAL, "shadow_draw: stride %u (needs >= 12, a multiple of 4)", stride);
   if ((uint64_t)vertex_count * stride > vertices->size ||
@@ -1196,6 +1196,34 @@ extern "C" int mopcuda_shadow_draw(MopCudaDevice *d, const MopCudaBuffer *vertic
   return MOPCUDA_OK;
 }
 
+extern "C" int mopcuda_shadow_draw(MopCudaDevice *d, const MopCudaBuffer *vertices,
+                                   uint32_t vertex_count, uint32_t stride,
+                                   const MopCudaBuffer *indices, uint32_t index_count,
+                                   const float model[16]) {
+  if (!d || !model)
+    return fail(MOPCUDA_EINVAL, "shadow_draw: bad arguments");
+  std::lock_guard<std::mutex> lk(d->mu);
+  if (!d->sh_open)
+    return fail(MOPCUDA_EINVAL, "shadow_draw outside shadow_begin/shadow_end");
+  return add_caster(d, vertices, vertex_count, stride, indices, index_count, model);
+}
+
+extern "C" int mopcuda_shadow_draw_list(MopCudaDevice *d, const MopCudaShadowCaster *c,
+                                        uint32_t n) {
+  if (!d || (n && !c))
+    return fail(MOPCUDA_EINVAL, "shadow_draw_list: bad arguments");
+  std::lock_guard<std::mutex> lk(d->mu);
+  if (!d->sh_open)
+    return fail(MOPCUDA_EINVAL, "shadow_draw outside shadow_begin/shadow_end");
+  for (uint32_t i = 0; i < n; i++) {
+    int rc = add_caster(d, c[i].vertices, c[i].vertex_count, c[i].stride, c[i].indices,
+                        c[i].index_count, c[i].model);
+    if (rc)
+      return rc;
+  }
+  return MOPCUDA_OK;
+}
+
 extern "C" int mopcuda_shadow_end(MopCudaDevice *d) {
   if (!d)
     return fail(MOPCUDA_EINVAL, "shadow_end: no device");
@@ -1205,8 +1233,10 @@ extern "C" int mopcuda_shadow_end(MopCudaDevice *d) {
   d->sh_open = false;
   cudaSetDevice(d->ordinal);
   int rc;
-  /* a frame still in flight reads the map this pass rewrites */
-  if (d->pending && (rc = finish_frame(d, FRAME_TIMEOUT_MS)))
+  /* the pass writes the map the last one did not; only a frame in flight
+   * bound to that map (an older pass's) has to complete first */
+  const int t = 1 - d->sh_cur;
+  if (d->pending && d->fr_sh == t && (rc = finish_frame(d, FRAME_TIMEOUT_MS)))
     return rc;
   if (!d->sh_ev) {
     CU_TRY(cudaEventCreateWithFlags(&d->sh_ev, cudaEventDisableTiming));
@@ -1225,7 +1255,7 @@ extern "C" int mopcuda_shadow_end(MopCudaDevice *d) {
     return fail(MOPCUDA_EINVAL, "shadow pass too large: %llu triangles", (unsigned long long)T);
   const size_t S = (size_t)d->sh_rec_size;
   rc = 0;
-  rc |= d->sh_map.ensure(4 * S * S + 64); /* texels, then the light's view-projection */
+  rc |= d->sh_map[t].ensure(4 * S * S + 64); /* texels, then the light's view-projection */
   rc |= d->sh_d_draws.ensure(sizeof(ShadowDraw) * (n ? n : 1));
   rc |= d->sh_h_draws.ensure(sizeof(ShadowDraw) * n + 64);
   rc |= d->sh_recs.ensure(sizeof(ShadowRec) * (size_t)(T ? T : 1));
@@ -1242,19 +1272,19 @@ extern "C" int mopcuda_shadow_end(MopCudaDevice *d) {
   memcpy(hp + db, d->sh_rec_vp, 64);
   if (n)
     CU_TRY(cudaMemcpyAsync(d->sh_d_draws.p, hp, db, cudaMemcpyHostToDevice, st));
-  CU_TRY(cudaMemcpyAsync(d->sh_map.as<uint8_t>() + 4 * S * S, hp + db, 64,
+  CU_TRY(cudaMemcpyAsync(d->sh_map[t].as<uint8_t>() + 4 * S * S, hp + db, 64,
                          cudaMemcpyHostToDevice, st));
   CU_TRY(cudaEventRecord(d->sh_ev, st));
   d->sh_ev_live = true;
   CU_TRY(cudaEventRecord(d->sh_t0, st));
   /* cleared to 1.0 (viewport.c:2370-2373): the key 0xffffffff */
-  CU_TRY(cudaMemsetAsync(d->sh_map.p, 0xff, 4 * S * S, st));
+  CU_TRY(cudaMemsetAsync(d->sh_map[t].p, 0xff, 4 * S * S, st));
   CU_TRY(cudaMemsetAsync(d->sh_ctr.p, 0, sizeof(ShadowCounters), st));
   ShadowArgs a;
   a.draws = d->sh_d_draws.as<ShadowDraw>();
   a.draw_count = n;
   a.tri_total = (uint32_t)T;
-  a.map = d->sh_map.as<uint32_t>();
+  a.map = d->sh_map[t].as<uint32_t>();
   a.size = (int)S;
   a.small_area = SHADOW_SMALL_AREA;
   a.recs = d->sh_recs.as<ShadowRec>();
@@ -1265,6 +1295,7 @@ extern "C" int mopcuda_shadow_end(MopCudaDevice *d) {
   CU_TRY(cudaGetLastError());
   CU_TRY(cudaEventRecord(d->sh_t1, st));
   d->sh_size = (int)S;
+  d->sh_cur = t;
   d->sh_bound = true;
   return MOPCUDA_OK;
 }
@@ -1307,7 +1338,7 @@ extern "C" int mopcuda_shadow_read(MopCudaDevice *d, float *out, size_t out_byte
   int rc = mc_stream_sync(d, FRAME_TIMEOUT_MS);
   if (rc)
     return rc;
-  CU_TRY(cudaMemcpy(out, d->sh_map.p, 4 * n, cudaMemcpyDeviceToHost));
+  CU_TRY(cudaMemcpy(out, d->sh_map[d->sh_cur].p, 4 * n, cudaMemcpyDeviceToHost));
   uint32_t *k = (uint32_t *)out;
   for (size_t i = 0; i < n; i++) { /* keys -> depth values, in place */
     uint32_t b = k[i];

@@ -53,6 +53,17 @@ class MopCudaDraw(C.Structure):
                 ("light_count", C.c_uint32), ("layout", C.POINTER(MopCudaVertexLayout))]
 
 
+class MopCudaShadowCaster(C.Structure):
+    _fields_ = [("vertices", C.c_void_p), ("vertex_count", C.c_uint32), ("stride", C.c_uint32),
+                ("indices", C.c_void_p), ("index_count", C.c_uint32), ("model", C.c_float * 16)]
+
+
+# the model matrices of a MopCudaShadowCaster array, as a numpy view
+_CASTER_MODELS = np.dtype({"names": ["model"], "formats": [(np.float32, 16)],
+                           "offsets": [MopCudaShadowCaster.model.offset],
+                           "itemsize": C.sizeof(MopCudaShadowCaster)})
+
+
 class MopCudaDeformLayout(C.Structure):
     _fields_ = [("stride", C.c_uint32), ("position_offset", C.c_int32),
                 ("normal_offset", C.c_int32), ("joints_offset", C.c_int32),
@@ -143,6 +154,7 @@ SIGNATURES = [
     ("mopcuda_scene_file_upload_all", C.c_int, [_P, _P, C.c_uint32, _P, _P, _P, _P]),
     ("mopcuda_shadow_begin", C.c_int, [_P, C.c_int, _P]),
     ("mopcuda_shadow_draw", C.c_int, [_P, _P, C.c_uint32, C.c_uint32, _P, C.c_uint32, _P]),
+    ("mopcuda_shadow_draw_list", C.c_int, [_P, C.POINTER(MopCudaShadowCaster), C.c_uint32]),
     ("mopcuda_shadow_end", C.c_int, [_P]),
     ("mopcuda_shadow_clear", C.c_int, [_P]),
     ("mopcuda_shadow_gpu_time_ms", C.c_float, [_P]),
@@ -400,6 +412,7 @@ class _Resident:
         # the device's shadow binding outlives a scene: start unbound
         _check(L.mopcuda_shadow_clear(d), "shadow_clear")
         self._shadow_bound = False
+        self._caster_key, self._caster_arr, self._caster_models = None, None, None
 
     def set_ibl(self, ibl):
         self._ibl = [_f32(ibl["irr"]), _f32(ibl["pf"]), _f32(ibl["brdf"])]
@@ -504,11 +517,18 @@ class SceneRenderer(_Resident):
         dr = _f32(light.direction)
         L.mopcuda_shadow_light_vp(models.ctypes.data, len(casters), dr.ctypes.data,
                                   vp.ctypes.data)
+        key = tuple(casters)
+        if self._caster_key != key:  # the caster array is rebuilt when the set changes
+            arr = (MopCudaShadowCaster * len(casters))()
+            for j, k in enumerate(casters):
+                _, vb, ib, vc, ic = self.meshes[k]
+                arr[j].vertices, arr[j].indices = vb, ib
+                arr[j].vertex_count, arr[j].index_count, arr[j].stride = vc, ic, 48
+            self._caster_arr, self._caster_key = arr, key
+            self._caster_models = np.frombuffer(arr, _CASTER_MODELS)["model"]
+        self._caster_models[:] = models.reshape(-1, 16)
         _check(L.mopcuda_shadow_begin(d, scenes.SHADOW_MAP_SIZE, vp.ctypes.data), "shadow_begin")
-        for j, k in enumerate(casters):
-            _, vb, ib, vc, ic = self.meshes[k]
-            _check(L.mopcuda_shadow_draw(d, vb, vc, 48, ib, ic, models[16 * j:].ctypes.data),
-                   "shadow_draw")
+        _check(L.mopcuda_shadow_draw_list(d, self._caster_arr, len(casters)), "shadow_draw_list")
         _check(L.mopcuda_shadow_end(d), "shadow_end")
         self._shadow_bound = True
         return True

@@ -156,6 +156,81 @@ def test_shadow_map_matches_oracle(cuda_device, name):
         r.close()
 
 
+def test_shadow_draw_list_equals_single_draws(cuda_device):
+    """mopcuda_shadow_draw_list (the renderer's path) builds the same map as
+    one mopcuda_shadow_draw call per caster, and rejects a caster whose
+    counts exceed its buffers as the single call does."""
+    sc = scenes.shadow_scene(seed=57)
+    r = mopcuda.SceneRenderer(cuda_device, sc)
+    L, d = mopcuda.lib(), cuda_device.h
+    try:
+        assert r.shadow_pass()
+        by_list = r.shadow_map()
+        casters = scenes.shadow_casters(sc)
+        vp = np.zeros(16, np.float32)
+        models = np.concatenate([mopcuda._f32(sc.meshes[k].transform) for k in casters])
+        dr = mopcuda._f32(scenes.shadow_light(sc).direction)
+        L.mopcuda_shadow_light_vp(models.ctypes.data, len(casters), dr.ctypes.data, vp.ctypes.data)
+        assert L.mopcuda_shadow_begin(d, scenes.SHADOW_MAP_SIZE, vp.ctypes.data) == 0
+        for j, k in enumerate(casters):
+            _, vb, ib, vc, ic = r.meshes[k]
+            assert L.mopcuda_shadow_draw(d, vb, vc, 48, ib, ic, models[16 * j:].ctypes.data) == 0
+        assert L.mopcuda_shadow_end(d) == 0
+        one_by_one = r.shadow_map()
+        assert (by_list.view(np.uint32) == one_by_one.view(np.uint32)).all()
+        bad = (mopcuda.MopCudaShadowCaster * 1)()
+        _, vb, ib, vc, ic = r.meshes[casters[0]]
+        bad[0].vertices, bad[0].indices, bad[0].stride = vb, ib, 48
+        bad[0].vertex_count, bad[0].index_count = vc + 1000000, ic
+        assert L.mopcuda_shadow_begin(d, scenes.SHADOW_MAP_SIZE, vp.ctypes.data) == 0
+        assert L.mopcuda_shadow_draw_list(d, bad, 1) != 0
+        assert "exceed the buffers" in mopcuda.last_error()
+        assert L.mopcuda_shadow_end(d) == 0
+    finally:
+        r.close()
+
+
+def test_shadow_pipelined_frames_match_sync(cuda_device):
+    """Shadowed frames submitted back to back (each shadow pass recorded
+    while the previous frame runs, into the map that frame does not read)
+    with a caster moving every frame and the images read asynchronously
+    equal the same frames rendered one at a time."""
+    sc = scenes.shadow_scene(seed=61)
+    r = mopcuda.SceneRenderer(cuda_device, sc)
+    casters = scenes.shadow_casters(sc)
+    mover = sc.meshes[casters[-1]]
+    base = mover.transform.copy()
+    steps = [(0.0, 0.0), (0.35, 0.0), (0.35, 0.3), (-0.3, 0.1), (0.0, -0.25)]
+    bufs = [mopcuda.HostArray((sc.height, sc.width, 4), np.uint8) for _ in steps]
+
+    def place(dx, dz):
+        mover.transform[:] = base
+        mover.transform[12] += dx
+        mover.transform[14] += dz
+        r.update_camera()
+
+    try:
+        want, maps = [], []
+        for dx, dz in steps:
+            place(dx, dz)
+            r.render()
+            want.append(r.color())
+            maps.append(r.shadow_map())
+        assert all((maps[k] != maps[k + 1]).any() for k in range(len(steps) - 1))
+        for k, (dx, dz) in enumerate(steps):
+            place(dx, dz)
+            r.submit()
+            r.color_async(bufs[k].a)
+        r.wait_readback()
+        for k in range(len(steps)):
+            assert (bufs[k].a == want[k]).all(), f"frame {k}"
+        assert (r.shadow_map().view(np.uint32) == maps[-1].view(np.uint32)).all()
+    finally:
+        for b in bufs:
+            b.close()
+        r.close()
+
+
 def test_shadow_clear_unbinds(cuda_device):
     """Once the casting light is switched off, frames render as without a
     shadow map (mop_sw_shadow_clear)."""
