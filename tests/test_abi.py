@@ -4,10 +4,13 @@
 * libmop_rhi_cuda.so exports mop_rhi_backend_cuda (the RHI table);
 * the library's host-side matrices are bit-identical to the reference's
   (camera chain, mvp products, TRS composition);
+* the ctypes structures of the Python binding have the header's sizes and
+  field offsets (a C probe compiled against include/mop_cuda.h);
 * without a CUDA device, device creation fails loudly (no CPU fallback).
 """
 import ctypes as C
 import re
+import shutil
 import subprocess
 from pathlib import Path
 
@@ -133,3 +136,42 @@ def _has_gpu():
 def test_no_gpu_fails_loudly():
     with pytest.raises(RuntimeError):
         mopcuda.Device(0)
+
+
+PUBLIC_STRUCTS = [mopcuda.MopCudaLight, mopcuda.MopCudaVertexLayout, mopcuda.MopCudaDraw,
+                  mopcuda.MopCudaShadowCaster, mopcuda.MopCudaDeformLayout, mopcuda.MopCudaView,
+                  mopcuda.MopCudaBatchConfig, mopcuda.MopCudaServerConfig,
+                  mopcuda.MopCudaRequest, mopcuda.MopCudaServerStats]
+
+
+@pytest.mark.skipif(shutil.which("cc") is None, reason="no C compiler")
+def test_struct_layouts_match_header(tmp_path):
+    """Every public struct of mop_cuda.h has a ctypes mirror of the same size
+    whose fields sit at the C offsets (a field missing from the header fails
+    the compile)."""
+    text = HEADER.read_text()
+    declared = set(re.findall(r"\}\s*(MopCuda[A-Za-z]+)\s*;", text))
+    assert declared == {c.__name__ for c in PUBLIC_STRUCTS}, declared
+    lines = ["#include <stddef.h>", "#include <stdio.h>", '#include "mop_cuda.h"',
+             "int main(void) {"]
+    for cls in PUBLIC_STRUCTS:
+        t = cls.__name__
+        lines.append(f'  printf("{t} sizeof %zu\\n", sizeof({t}));')
+        for name, *_ in cls._fields_:
+            lines.append(f'  printf("{t} {name} %zu\\n", offsetof({t}, {name}));')
+    lines += ["  return 0;", "}"]
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines) + "\n")
+    exe = tmp_path / "layout"
+    subprocess.run(["cc", "-std=c11", "-I", str(HEADER.parent), str(src), "-o", str(exe)],
+                   check=True, capture_output=True)
+    got = {}
+    for line in subprocess.run([str(exe)], capture_output=True, text=True,
+                               check=True).stdout.splitlines():
+        t, name, v = line.split()
+        got[(t, name)] = int(v)
+    for cls in PUBLIC_STRUCTS:
+        t = cls.__name__
+        assert got[(t, "sizeof")] == C.sizeof(cls), t
+        for name, *_ in cls._fields_:
+            assert got[(t, name)] == getattr(cls, name).offset, f"{t}.{name}"
