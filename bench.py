@@ -166,7 +166,7 @@ def cpu_reference_time(config, budget_s=45.0, warm=1, frames=3):
     attempt is reported with the thread count it used."""
     ncpu = len(os.sched_getaffinity(0))
     attempts = [max(1, ncpu // 2 - 1), 0]
-    best = None
+    best, modes = None, {}
     for workers in attempts:
         cmd = [sys.executable, str(ROOT / "oracle" / "time_reference.py"), "--config", config,
                "--workers", str(workers), "--warm", str(warm), "--frames", str(frames),
@@ -178,12 +178,13 @@ def cpu_reference_time(config, budget_s=45.0, warm=1, frames=3):
             t = json.loads(p.stdout.strip().splitlines()[-1])
         except (subprocess.TimeoutExpired, ValueError, IndexError):
             continue
+        modes[t["mode"]] = {"ms": round(t["ms"], 3), "threads": t["threads"]}
         if best is None or t["ms"] < best["ms"]:
             best = t
     if best is None:
         raise RuntimeError("reference CPU backend did not complete a frame in time")
     return {"ms": best["ms"], "frames": best["frames"], "cores": best["threads"],
-            "kind": "reference", "mode": best["mode"]}
+            "kind": "reference", "mode": best["mode"], "modes": modes}
 
 
 def emit(line):
@@ -226,7 +227,8 @@ def run_reference(args):
             "cpu_baseline": {"value": round(mpix, 4), "unit": "Mpix/s", "cores": t["cores"],
                              "kind": t["kind"],
                              "sample": f"{t['frames']} full frame(s) ({t['mode']}), median wall "
-                                       "time of mop_viewport_render + mop_viewport_read_color"},
+                                       "time of mop_viewport_render + mop_viewport_read_color",
+                             "modes": t["modes"]},
             "e2e": {"value": round(mpix, 4), "unit": "Mpix/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     emit(line)
@@ -362,7 +364,8 @@ def run_cuda(args):
                 "value": round(sc.pixels / (t["ms"] * 1e3), 4), "unit": "Mpix/s",
                 "cores": t["cores"], "kind": t["kind"],
                 "sample": f"{t['frames']} full frame(s) of the same scene ({t['mode']}, "
-                          "median of mop_viewport_render + read_color)"}
+                          "median of mop_viewport_render + read_color)",
+                "modes": t["modes"]}  # the tile pool and the serial path (the parity reference)
         except Exception as e:  # report, do not fail the GPU measurement
             line["cpu_baseline"] = {"value": None, "unit": "Mpix/s", "error": str(e)[:200]}
     r.close()
