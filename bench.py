@@ -401,8 +401,7 @@ def run_batched(dev, steps=10, warm=3, n_views=64):
         for _ in range(steps):
             b.render()
             gms.append(b.gpu_ms)
-            for i, o in enumerate(outs):
-                b.read(i, mopcuda.BATCH_PRESENTED, o.a)
+            b.read_all(mopcuda.BATCH_PRESENTED, [o.a for o in outs])
         wall_b = (time.perf_counter() - t0) / steps
         cfg = b.config()
         # plain: one frame per viewport through the per-viewport C ABI

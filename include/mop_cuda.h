@@ -439,6 +439,11 @@ float mopcuda_batch_gpu_time_ms(const MopCudaBatch *batch);
 #define MOPCUDA_BATCH_DEPTH 2
 #define MOPCUDA_BATCH_IDS 3
 int mopcuda_batch_read(MopCudaBatch *batch, uint32_t view, int what, void *dst, size_t bytes);
+/* The same buffer of views first .. first+count-1 in one call: dsts[i] and
+ * bytes[i] for view first+i, every size checked before any copy, one wait
+ * for all the copies. */
+int mopcuda_batch_read_views(MopCudaBatch *batch, uint32_t first, uint32_t count, int what,
+                             void *const *dsts, const size_t *bytes);
 /* Picks on viewport `view` (presented coordinates, top-left sample), as
  * mopcuda_pick_batch. */
 int mopcuda_batch_pick(MopCudaBatch *batch, uint32_t view, const int32_t *xy, uint32_t n,

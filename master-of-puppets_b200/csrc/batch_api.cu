@@ -815,45 +815,69 @@ extern "C" int mopcuda_batch_wait(MopCudaBatch *b, int timeout_ms) {
 
 extern "C" float mopcuda_batch_gpu_time_ms(const MopCudaBatch *b) { return b ? b->last_ms : 0.0f; }
 
+/* Where viewport `view`'s buffer `what` lives on the device, and its size. */
+static int view_buffer(const LaunchCore &c, uint32_t view, int what, const void **src,
+                       size_t *n) {
+  const ViewRec &r = c.vrec[view];
+  const size_t S = (size_t)r.width * r.height;
+  const size_t P = (size_t)(r.width / r.ssaa) * (r.height / r.ssaa);
+  switch (what) {
+  case MOPCUDA_BATCH_COLOR:
+    *src = c.out.as<uchar4>() + r.sample_off;
+    *n = 4 * S;
+    return MOPCUDA_OK;
+  case MOPCUDA_BATCH_PRESENTED:
+    *src = r.ssaa > 1 ? (const void *)(c.presented.as<uchar4>() + r.pixel_off)
+                      : (const void *)(c.out.as<uchar4>() + r.sample_off);
+    *n = 4 * P;
+    return MOPCUDA_OK;
+  case MOPCUDA_BATCH_DEPTH:
+    *src = c.depth.as<float>() + r.sample_off;
+    *n = 4 * S;
+    return MOPCUDA_OK;
+  case MOPCUDA_BATCH_IDS:
+    *src = c.ids.as<uint32_t>() + r.sample_off;
+    *n = 4 * S;
+    return MOPCUDA_OK;
+  default:
+    return fail(MOPCUDA_EINVAL, "batch_read: unknown buffer %d", what);
+  }
+}
+
 extern "C" int mopcuda_batch_read(MopCudaBatch *b, uint32_t view, int what, void *dst,
                                   size_t bytes) {
-  if (!b || !dst || view >= b->core.nv)
+  return mopcuda_batch_read_views(b, view, 1, what, &dst, &bytes);
+}
+
+extern "C" int mopcuda_batch_read_views(MopCudaBatch *b, uint32_t first, uint32_t count,
+                                        int what, void *const *dsts, const size_t *bytes) {
+  if (!b || !dsts || !bytes || count == 0 || first >= b->core.nv ||
+      count > b->core.nv - first)
     return fail(MOPCUDA_EINVAL, "batch_read: bad arguments");
+  for (uint32_t i = 0; i < count; i++)
+    if (!dsts[i])
+      return fail(MOPCUDA_EINVAL, "batch_read: bad arguments");
   std::lock_guard<std::mutex> lk(b->mu);
   cudaSetDevice(b->core.dev->ordinal);
   int rc = finish_batch(b, FRAME_TIMEOUT_MS);
   if (rc)
     return rc;
   const LaunchCore &c = b->core;
-  const ViewRec &r = c.vrec[view];
-  const size_t S = (size_t)r.width * r.height;
-  const size_t P = (size_t)(r.width / r.ssaa) * (r.height / r.ssaa);
-  const void *src = nullptr;
-  size_t n = 0;
-  switch (what) {
-  case MOPCUDA_BATCH_COLOR:
-    src = c.out.as<uchar4>() + r.sample_off;
-    n = 4 * S;
-    break;
-  case MOPCUDA_BATCH_PRESENTED:
-    src = r.ssaa > 1 ? (const void *)(c.presented.as<uchar4>() + r.pixel_off)
-                     : (const void *)(c.out.as<uchar4>() + r.sample_off);
-    n = 4 * P;
-    break;
-  case MOPCUDA_BATCH_DEPTH:
-    src = c.depth.as<float>() + r.sample_off;
-    n = 4 * S;
-    break;
-  case MOPCUDA_BATCH_IDS:
-    src = c.ids.as<uint32_t>() + r.sample_off;
-    n = 4 * S;
-    break;
-  default:
-    return fail(MOPCUDA_EINVAL, "batch_read: unknown buffer %d", what);
+  /* every size is checked before the first copy is queued */
+  for (uint32_t i = 0; i < count; i++) {
+    const void *src;
+    size_t n;
+    if ((rc = view_buffer(c, first + i, what, &src, &n)))
+      return rc;
+    if (bytes[i] != n)
+      return fail(MOPCUDA_EINVAL, "batch_read: buffer is %zu bytes, not %zu", n, bytes[i]);
   }
-  if (bytes != n)
-    return fail(MOPCUDA_EINVAL, "batch_read: buffer is %zu bytes, not %zu", n, bytes);
-  CU_TRY(cudaMemcpyAsync(dst, src, n, cudaMemcpyDeviceToHost, c.stream));
+  for (uint32_t i = 0; i < count; i++) {
+    const void *src;
+    size_t n;
+    view_buffer(c, first + i, what, &src, &n);
+    CU_TRY(cudaMemcpyAsync(dsts[i], src, n, cudaMemcpyDeviceToHost, c.stream));
+  }
   return b->core.sync(FRAME_TIMEOUT_MS);
 }
 

@@ -193,6 +193,8 @@ SIGNATURES = [
     ("mopcuda_batch_wait", C.c_int, [_P, C.c_int]),
     ("mopcuda_batch_gpu_time_ms", C.c_float, [_P]),
     ("mopcuda_batch_read", C.c_int, [_P, C.c_uint32, C.c_int, _P, C.c_size_t]),
+    ("mopcuda_batch_read_views", C.c_int, [_P, C.c_uint32, C.c_uint32, C.c_int,
+                                           C.POINTER(C.c_void_p), C.POINTER(C.c_size_t)]),
     ("mopcuda_batch_pick", C.c_int, [_P, C.c_uint32, _P, C.c_uint32, _P, _P, _P]),
     ("mopcuda_batch_get_config", C.c_int, [_P, C.POINTER(MopCudaBatchConfig)]),
     ("mopcuda_batch_set_config", C.c_int, [_P, C.POINTER(MopCudaBatchConfig)]),
@@ -722,6 +724,15 @@ class BatchRenderer(ResidentScene):
             out = np.empty(shape, dt)
         _check(self.L.mopcuda_batch_read(self.h, i, what, out.ctypes.data, out.nbytes), "batch_read")
         return out
+
+    def read_all(self, what: int, outs):
+        """Buffer `what` of every viewport into outs[i] (arrays of the sizes
+        read() gives), in one call."""
+        n = len(self.views)
+        ptrs = (C.c_void_p * n)(*[o.ctypes.data for o in outs])
+        sizes = (C.c_size_t * n)(*[o.nbytes for o in outs])
+        _check(self.L.mopcuda_batch_read_views(self.h, 0, n, what, ptrs, sizes), "batch_read_views")
+        return outs
 
     def pick(self, i: int, xy):
         xy = np.ascontiguousarray(xy, np.int32)

@@ -87,6 +87,34 @@ def test_batch_equals_single_viewport_frames(cuda_device, ibl):
         b.close()
 
 
+def test_batch_read_views_equals_single_reads(cuda_device, ibl):
+    """mopcuda_batch_read_views (every view's buffer in one call) returns the
+    bytes of one mopcuda_batch_read per view, for each buffer, and rejects a
+    wrong size or range before copying anything."""
+    import ctypes as C
+    sc = _scene()
+    b = mopcuda.BatchRenderer(cuda_device, sc, _views(sc, 6, seed=5), ibl)
+    try:
+        b.render()
+        for what in (mopcuda.BATCH_COLOR, mopcuda.BATCH_PRESENTED, mopcuda.BATCH_DEPTH,
+                     mopcuda.BATCH_IDS):
+            one = [b.read(i, what) for i in range(len(b.views))]
+            every = b.read_all(what, [np.zeros_like(x) for x in one])
+            for i, (x, y) in enumerate(zip(one, every)):
+                assert x.tobytes() == y.tobytes(), f"buffer {what} view {i}"
+        outs = [np.full_like(b.read(i, mopcuda.BATCH_IDS), 7) for i in range(len(b.views))]
+        ptrs = (C.c_void_p * len(outs))(*[o.ctypes.data for o in outs])
+        sizes = (C.c_size_t * len(outs))(*[o.nbytes for o in outs])
+        sizes[-1] -= 4
+        L = mopcuda.lib()
+        assert L.mopcuda_batch_read_views(b.h, 0, len(outs), mopcuda.BATCH_IDS, ptrs, sizes) != 0
+        assert all((o == 7).all() for o in outs)  # nothing copied
+        sizes[-1] += 4
+        assert L.mopcuda_batch_read_views(b.h, 1, len(outs), mopcuda.BATCH_IDS, ptrs, sizes) != 0
+    finally:
+        b.close()
+
+
 def test_batch_matches_oracle(cuda_device):
     sc = scenes.small_scene(seed=4, width=96, height=72)
     views = [scenes.View(96, 72, 1, sc.eye, sc.target, fov_deg=sc.fov_deg, near=sc.near,
