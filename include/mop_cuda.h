@@ -444,6 +444,16 @@ int mopcuda_batch_read(MopCudaBatch *batch, uint32_t view, int what, void *dst, 
  * for all the copies. */
 int mopcuda_batch_read_views(MopCudaBatch *batch, uint32_t first, uint32_t count, int what,
                              void *const *dsts, const size_t *bytes);
+/* Asynchronous form for the colour buffers (MOPCUDA_BATCH_COLOR or
+ * _PRESENTED) of the last submitted launch, which it waits for: the copies
+ * are queued once the next submit has queued its stages up to shading, and
+ * run while that launch renders (its post passes, which rewrite the images,
+ * wait for them); without a next submit, readback_wait queues them.  dsts
+ * stay the caller's and should be page-locked; the copies are complete when
+ * mopcuda_batch_readback_wait returns 0. */
+int mopcuda_batch_read_views_async(MopCudaBatch *batch, uint32_t first, uint32_t count, int what,
+                                   void *const *dsts, const size_t *bytes);
+int mopcuda_batch_readback_wait(MopCudaBatch *batch, int timeout_ms);
 /* Picks on viewport `view` (presented coordinates, top-left sample), as
  * mopcuda_pick_batch. */
 int mopcuda_batch_pick(MopCudaBatch *batch, uint32_t view, const int32_t *xy, uint32_t n,

@@ -518,7 +518,7 @@ int LaunchCore::stage() {
   return MOPCUDA_OK;
 }
 
-int LaunchCore::enqueue() {
+int LaunchCore::enqueue(int parts) {
   BatchLaunch L;
   memset(&L, 0, sizeof L);
   L.num_sms = dev->num_sms;
@@ -567,21 +567,27 @@ int LaunchCore::enqueue() {
   for (int k = 0; k < 4; k++)
     pv[k] = d_post_views.as<uint32_t>() + (size_t)k * nv;
   cudaStream_t s = stream;
-  CU_TRY(cudaMemcpyAsync(d_views.p, h_views.p, sizeof(ViewRec) * nv, cudaMemcpyHostToDevice, s));
-  if (total_draws)
-    CU_TRY(cudaMemcpyAsync(d_draws.p, h_draws.p, sizeof(DrawRec) * total_draws,
+  if (parts & BATCH_PART_MAIN) {
+    CU_TRY(cudaMemcpyAsync(d_views.p, h_views.p, sizeof(ViewRec) * nv, cudaMemcpyHostToDevice,
+                           s));
+    if (total_draws)
+      CU_TRY(cudaMemcpyAsync(d_draws.p, h_draws.p, sizeof(DrawRec) * total_draws,
+                             cudaMemcpyHostToDevice, s));
+    CU_TRY(cudaMemcpyAsync(d_scenes.p, h_scenes.p, sizeof(SceneDesc) * scenes.size(),
                            cudaMemcpyHostToDevice, s));
-  CU_TRY(cudaMemcpyAsync(d_scenes.p, h_scenes.p, sizeof(SceneDesc) * scenes.size(),
-                         cudaMemcpyHostToDevice, s));
-  CU_TRY(cudaMemsetAsync(d_ctr.p, 0, sizeof(Counters) * nv, s));
-  CU_TRY(cudaMemsetAsync(d_status.p, 0, sizeof(BatchStatus), s));
-  CU_TRY(cudaMemsetAsync(keys.p, 0xff, 8ull * total_samples, s));
+    CU_TRY(cudaMemsetAsync(d_ctr.p, 0, sizeof(Counters) * nv, s));
+    CU_TRY(cudaMemsetAsync(d_status.p, 0, sizeof(BatchStatus), s));
+    CU_TRY(cudaMemsetAsync(keys.p, 0xff, 8ull * total_samples, s));
+  }
   launches = (uint64_t)mopcuda_launch_batch(a, d_posts.as<PostArgs>(), pv, post_count, post_tiles,
-                                            L, scenes.size() == 1, s);
+                                            L, scenes.size() == 1, s, parts);
   CU_TRY(cudaGetLastError());
-  CU_TRY(cudaMemcpyAsync(h_status.p, d_status.p, sizeof(BatchStatus), cudaMemcpyDeviceToHost, s));
-  CU_TRY(cudaMemcpyAsync(h_status.as<uint8_t>() + sizeof(BatchStatus), d_ctr.p,
-                         sizeof(Counters) * nv, cudaMemcpyDeviceToHost, s));
+  if (parts & BATCH_PART_POST) { /* status after the last kernel: read at completion */
+    CU_TRY(cudaMemcpyAsync(h_status.p, d_status.p, sizeof(BatchStatus), cudaMemcpyDeviceToHost,
+                           s));
+    CU_TRY(cudaMemcpyAsync(h_status.as<uint8_t>() + sizeof(BatchStatus), d_ctr.p,
+                           sizeof(Counters) * nv, cudaMemcpyDeviceToHost, s));
+  }
   return MOPCUDA_OK;
 }
 
@@ -625,13 +631,30 @@ int LaunchCore::after(bool *rerun, int attempt) {
 /* ------------------------------------------------------------------------
  * batch: one LaunchCore over one scene, captured as a CUDA graph
  * ------------------------------------------------------------------------ */
+/* One device-to-host copy of an asynchronous colour readback. */
+struct RbCopy {
+  void *dst;
+  const void *src;
+  size_t n;
+};
+
 struct MopCudaBatch {
   MopCudaScene *scene = nullptr;
   LaunchCore core;
   uint64_t scene_version = ~0ull;
-  cudaGraph_t graph = nullptr;
-  cudaGraphExec_t exec = nullptr;
+  /* a launch is two graphs: every stage up to shading, then the post passes
+   * (which write the colour images) and the status copies */
+  cudaGraph_t graph = nullptr, graph_post = nullptr;
+  cudaGraphExec_t exec = nullptr, exec_post = nullptr;
   bool pending = false;
+  /* asynchronous colour readback of the last completed launch: the copies
+   * wait in rb_copies until the next launch's first graph is queued (queued
+   * before it, they held back its uploads), run on copy_stream, and that
+   * launch's post graph waits for rb_done */
+  std::vector<RbCopy> rb_copies;
+  cudaStream_t copy_stream = nullptr;
+  cudaEvent_t rb_done = nullptr;
+  bool rb_live = false;
   float last_ms = 0.0f;
   DevArena pick_xy, pick_out;
   HostArena h_pick;
@@ -643,8 +666,44 @@ static void drop_graph(MopCudaBatch *b) {
     cudaGraphExecDestroy(b->exec);
   if (b->graph)
     cudaGraphDestroy(b->graph);
-  b->exec = nullptr;
-  b->graph = nullptr;
+  if (b->exec_post)
+    cudaGraphExecDestroy(b->exec_post);
+  if (b->graph_post)
+    cudaGraphDestroy(b->graph_post);
+  b->exec = b->exec_post = nullptr;
+  b->graph = b->graph_post = nullptr;
+}
+
+/* Queues the recorded readback copies on the copy stream (the launch they
+ * read has completed). */
+static int issue_readback(MopCudaBatch *b) {
+  if (b->rb_copies.empty())
+    return MOPCUDA_OK;
+  if (!b->copy_stream) {
+    CU_TRY(cudaStreamCreateWithFlags(&b->copy_stream, cudaStreamNonBlocking));
+    CU_TRY(cudaEventCreateWithFlags(&b->rb_done, cudaEventDisableTiming));
+  }
+  std::vector<RbCopy> copies;
+  copies.swap(b->rb_copies);
+  for (const RbCopy &c : copies)
+    CU_TRY(cudaMemcpyAsync(c.dst, c.src, c.n, cudaMemcpyDeviceToHost, b->copy_stream));
+  CU_TRY(cudaEventRecord(b->rb_done, b->copy_stream));
+  b->rb_live = true;
+  return MOPCUDA_OK;
+}
+
+/* The readback queued and complete (before the images' memory is freed or
+ * moved). */
+static int drain_readback(MopCudaBatch *b, int timeout_ms) {
+  int rc = issue_readback(b);
+  if (rc)
+    return rc;
+  if (!b->rb_live)
+    return MOPCUDA_OK;
+  rc = mc_bounded_sync(b->core.dev, b->rb_done, timeout_ms);
+  if (!rc)
+    b->rb_live = false;
+  return rc;
 }
 
 extern "C" void mopcuda_batch_destroy(MopCudaBatch *b) {
@@ -653,6 +712,13 @@ extern "C" void mopcuda_batch_destroy(MopCudaBatch *b) {
   cudaSetDevice(b->core.dev->ordinal);
   if (b->core.stream)
     b->core.sync(10000);
+  b->rb_copies.clear();
+  if (b->copy_stream) {
+    if (b->rb_live)
+      mc_bounded_sync(b->core.dev, b->rb_done, 10000);
+    cudaEventDestroy(b->rb_done);
+    cudaStreamDestroy(b->copy_stream);
+  }
   drop_graph(b);
   b->pick_xy.release();
   b->pick_out.release();
@@ -700,25 +766,39 @@ extern "C" int mopcuda_batch_set_views(MopCudaBatch *b, const MopCudaView *views
   return MOPCUDA_OK;
 }
 
-static int build_graph(MopCudaBatch *b) {
-  drop_graph(b);
+static int capture_part(MopCudaBatch *b, int part, cudaGraph_t *graph, cudaGraphExec_t *exec,
+                        uint64_t *launches) {
   LaunchCore &c = b->core;
   CU_TRY(cudaStreamBeginCapture(c.stream, cudaStreamCaptureModeThreadLocal));
-  int rc = c.enqueue();
-  cudaError_t e = cudaStreamEndCapture(c.stream, &b->graph);
+  int rc = c.enqueue(part);
+  cudaError_t e = cudaStreamEndCapture(c.stream, graph);
   if (rc || e != cudaSuccess) {
     cudaGetLastError();
-    if (b->graph)
-      cudaGraphDestroy(b->graph);
-    b->graph = nullptr;
+    if (*graph)
+      cudaGraphDestroy(*graph);
+    *graph = nullptr;
     return rc ? rc : fail(MOPCUDA_ECUDA, "batch graph capture: %s", cudaGetErrorString(e));
   }
-  e = cudaGraphInstantiate(&b->exec, b->graph, 0);
+  e = cudaGraphInstantiate(exec, *graph, 0);
   if (e != cudaSuccess) {
     cudaGetLastError();
-    drop_graph(b);
     return fail(MOPCUDA_ECUDA, "batch graph instantiate: %s", cudaGetErrorString(e));
   }
+  *launches += c.launches;
+  return MOPCUDA_OK;
+}
+
+static int build_graph(MopCudaBatch *b) {
+  drop_graph(b);
+  uint64_t launches = 0;
+  int rc = capture_part(b, BATCH_PART_MAIN, &b->graph, &b->exec, &launches);
+  if (!rc)
+    rc = capture_part(b, BATCH_PART_POST, &b->graph_post, &b->exec_post, &launches);
+  if (rc) {
+    drop_graph(b);
+    return rc;
+  }
+  b->core.launches = launches;
   return MOPCUDA_OK;
 }
 
@@ -726,9 +806,15 @@ static int launch_graph(MopCudaBatch *b) {
   cudaStream_t s = b->core.stream;
   CU_TRY(cudaEventRecord(b->core.ev0, s));
   CU_TRY(cudaGraphLaunch(b->exec, s));
+  /* the previous launch's images go to the host while this one renders;
+   * its post passes overwrite them only once they are there */
+  const int rrc = issue_readback(b);
+  if (b->rb_live)
+    CU_TRY(cudaStreamWaitEvent(s, b->rb_done, 0));
+  CU_TRY(cudaGraphLaunch(b->exec_post, s));
   CU_TRY(cudaEventRecord(b->core.ev1, s));
   b->pending = true;
-  return MOPCUDA_OK;
+  return rrc;
 }
 
 /* Waits; re-runs after growing a viewport's reserves or the pools. */
@@ -761,6 +847,9 @@ static int submit_locked(MopCudaBatch *b) {
   if (rc)
     return rc;
   if (b->scene->version != b->scene_version) { /* draws were added: new table sizes */
+    /* the buffers may move: a pending readback runs to completion first */
+    if ((rc = drain_readback(b, FRAME_TIMEOUT_MS)))
+      return rc;
     LaunchCore &c = b->core;
     std::vector<uint32_t> scene_of(c.nv, 0u);
     std::vector<MopCudaView> views(c.nv);
@@ -879,6 +968,47 @@ extern "C" int mopcuda_batch_read_views(MopCudaBatch *b, uint32_t first, uint32_
     CU_TRY(cudaMemcpyAsync(dsts[i], src, n, cudaMemcpyDeviceToHost, c.stream));
   }
   return b->core.sync(FRAME_TIMEOUT_MS);
+}
+
+extern "C" int mopcuda_batch_read_views_async(MopCudaBatch *b, uint32_t first, uint32_t count,
+                                              int what, void *const *dsts,
+                                              const size_t *bytes) {
+  if (!b || !dsts || !bytes || count == 0 || first >= b->core.nv ||
+      count > b->core.nv - first)
+    return fail(MOPCUDA_EINVAL, "batch_read_views_async: bad arguments");
+  if (what != MOPCUDA_BATCH_COLOR && what != MOPCUDA_BATCH_PRESENTED)
+    return fail(MOPCUDA_EINVAL, "batch_read_views_async: colour buffers only (got %d)", what);
+  for (uint32_t i = 0; i < count; i++)
+    if (!dsts[i])
+      return fail(MOPCUDA_EINVAL, "batch_read_views_async: bad arguments");
+  std::lock_guard<std::mutex> lk(b->mu);
+  cudaSetDevice(b->core.dev->ordinal);
+  int rc = finish_batch(b, FRAME_TIMEOUT_MS);
+  if (rc)
+    return rc;
+  const LaunchCore &c = b->core;
+  std::vector<RbCopy> copies(count);
+  for (uint32_t i = 0; i < count; i++) {
+    if ((rc = view_buffer(c, first + i, what, &copies[i].src, &copies[i].n)))
+      return rc;
+    if (bytes[i] != copies[i].n)
+      return fail(MOPCUDA_EINVAL, "batch_read_views_async: buffer is %zu bytes, not %zu",
+                  copies[i].n, bytes[i]);
+    copies[i].dst = dsts[i];
+  }
+  /* copies recorded earlier for this launch go first */
+  if ((rc = issue_readback(b)))
+    return rc;
+  b->rb_copies.swap(copies);
+  return MOPCUDA_OK;
+}
+
+extern "C" int mopcuda_batch_readback_wait(MopCudaBatch *b, int timeout_ms) {
+  if (!b)
+    return fail(MOPCUDA_EINVAL, "batch_readback_wait: no batch");
+  std::lock_guard<std::mutex> lk(b->mu);
+  cudaSetDevice(b->core.dev->ordinal);
+  return drain_readback(b, timeout_ms);
 }
 
 extern "C" int mopcuda_batch_pick(MopCudaBatch *b, uint32_t view, const int32_t *xy, uint32_t n,

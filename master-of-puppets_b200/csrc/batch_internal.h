@@ -90,8 +90,11 @@ struct LaunchCore {
                  const std::vector<std::shared_ptr<const std::vector<float>>> *models = nullptr);
   /* Snapshots the scenes' draw tables into pinned memory; sizes the pools. */
   int stage();
-  /* Enqueues the whole launch on `stream` (capturable). */
-  int enqueue();
+  /* Enqueues the launch on `stream` (capturable): parts = BATCH_PART_MAIN
+   * (uploads, clears, every stage up to shading) and/or BATCH_PART_POST (the
+   * post passes, then the status copies the host reads at completion);
+   * `launches` counts the kernels of the parts enqueued. */
+  int enqueue(int parts = BATCH_PART_MAIN | BATCH_PART_POST);
   /* After ev1: true when the launch must run again (reserves or pools grew). */
   int after(bool *rerun, int attempt);
   uint64_t device_bytes() const;

@@ -2462,24 +2462,28 @@ void mopcuda_batch_grids(BatchLaunch &cfg) {
 
 int mopcuda_launch_batch(const BatchArgs &b, const PostArgs *posts, const uint32_t *post_views[4],
                          const uint32_t post_count[4], const uint32_t post_tiles[4],
-                         const BatchLaunch &cfg, bool shared_lights, cudaStream_t s) {
+                         const BatchLaunch &cfg, bool shared_lights, cudaStream_t s, int parts) {
   if (b.nv == 0)
     return 0;
   int launches = 0;
   const int sms = cfg.num_sms > 0 ? cfg.num_sms : 148;
   const uint32_t nv = b.nv;
   const FrameArgs *fr = b.frames;
-  k_batch_prepare<<<nv, 256, 0, s>>>(b);
-  k_batch_alloc<<<1, 256, 0, s>>>(b);
-  k_b_items<ST_VERTEX><<<cfg.grid_vertex, cfg.vertex_block, 0, s>>>(fr, nv);
-  k_b_items<ST_SETUP><<<cfg.grid_setup, cfg.setup_block, 0, s>>>(fr, nv);
-  k_b_items<ST_CLIP><<<cfg.grid_clip, 128, 0, s>>>(fr, nv);
-  k_b_items<ST_RSMALL><<<cfg.grid_rsmall, cfg.raster_block, 0, s>>>(fr, nv);
-  k_b_large_scan<<<nv, 1024, 0, s>>>(fr);
-  k_b_items<ST_RLARGE><<<cfg.grid_rlarge, cfg.large_block, 0, s>>>(fr, nv);
-  k_b_resolve<<<sms * 8, 256, 0, s>>>(fr, nv);
-  k_b_shade<<<cfg.grid_shade, cfg.shade_block, 0, s>>>(fr, nv, shared_lights ? 1 : 0);
-  launches += 10;
+  if (parts & BATCH_PART_MAIN) {
+    k_batch_prepare<<<nv, 256, 0, s>>>(b);
+    k_batch_alloc<<<1, 256, 0, s>>>(b);
+    k_b_items<ST_VERTEX><<<cfg.grid_vertex, cfg.vertex_block, 0, s>>>(fr, nv);
+    k_b_items<ST_SETUP><<<cfg.grid_setup, cfg.setup_block, 0, s>>>(fr, nv);
+    k_b_items<ST_CLIP><<<cfg.grid_clip, 128, 0, s>>>(fr, nv);
+    k_b_items<ST_RSMALL><<<cfg.grid_rsmall, cfg.raster_block, 0, s>>>(fr, nv);
+    k_b_large_scan<<<nv, 1024, 0, s>>>(fr);
+    k_b_items<ST_RLARGE><<<cfg.grid_rlarge, cfg.large_block, 0, s>>>(fr, nv);
+    k_b_resolve<<<sms * 8, 256, 0, s>>>(fr, nv);
+    k_b_shade<<<cfg.grid_shade, cfg.shade_block, 0, s>>>(fr, nv, shared_lights ? 1 : 0);
+    launches += 10;
+  }
+  if (!(parts & BATCH_PART_POST))
+    return launches;
   dim3 pb(POST_BX, POST_BY);
   for (int k = 0; k < 4; k++) {
     if (!post_count[k] || !post_tiles[k])

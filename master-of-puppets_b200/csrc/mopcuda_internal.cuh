@@ -409,9 +409,15 @@ void mopcuda_batch_grids(BatchLaunch &cfg);
  * counters and keys first).  post_views[k] lists the viewports with ssaa
  * k+1 (device array, post_count[k] entries); posts holds each viewport's
  * PostArgs.  Returns the number of kernels launched. */
+/* parts: which of the launch to enqueue, BATCH_PART_MAIN (uploads done by
+ * the caller, then every stage up to shading) and/or BATCH_PART_POST (the
+ * post passes, which write the colour images). */
+#define BATCH_PART_MAIN 1
+#define BATCH_PART_POST 2
 int mopcuda_launch_batch(const BatchArgs &b, const PostArgs *posts, const uint32_t *post_views[4],
                          const uint32_t post_count[4], const uint32_t post_tiles[4],
-                         const BatchLaunch &cfg, bool shared_lights, cudaStream_t s);
+                         const BatchLaunch &cfg, bool shared_lights, cudaStream_t s,
+                         int parts = BATCH_PART_MAIN | BATCH_PART_POST);
 
 /* ev (optional, 7 events): stage boundaries
  * vertex | setup+clip | raster | resolve | shade | post */

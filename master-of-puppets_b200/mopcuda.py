@@ -195,6 +195,9 @@ SIGNATURES = [
     ("mopcuda_batch_read", C.c_int, [_P, C.c_uint32, C.c_int, _P, C.c_size_t]),
     ("mopcuda_batch_read_views", C.c_int, [_P, C.c_uint32, C.c_uint32, C.c_int,
                                            C.POINTER(C.c_void_p), C.POINTER(C.c_size_t)]),
+    ("mopcuda_batch_read_views_async", C.c_int, [_P, C.c_uint32, C.c_uint32, C.c_int,
+                                                 C.POINTER(C.c_void_p), C.POINTER(C.c_size_t)]),
+    ("mopcuda_batch_readback_wait", C.c_int, [_P, C.c_int]),
     ("mopcuda_batch_pick", C.c_int, [_P, C.c_uint32, _P, C.c_uint32, _P, _P, _P]),
     ("mopcuda_batch_get_config", C.c_int, [_P, C.POINTER(MopCudaBatchConfig)]),
     ("mopcuda_batch_set_config", C.c_int, [_P, C.POINTER(MopCudaBatchConfig)]),
@@ -733,6 +736,20 @@ class BatchRenderer(ResidentScene):
         sizes = (C.c_size_t * n)(*[o.nbytes for o in outs])
         _check(self.L.mopcuda_batch_read_views(self.h, 0, n, what, ptrs, sizes), "batch_read_views")
         return outs
+
+    def read_all_async(self, what: int, outs):
+        """Colour buffer `what` of every viewport of the last submitted
+        launch into outs[i] (page-locked arrays), copied while the next
+        submitted launch renders; complete after wait_readback()."""
+        n = len(self.views)
+        ptrs = (C.c_void_p * n)(*[o.ctypes.data for o in outs])
+        sizes = (C.c_size_t * n)(*[o.nbytes for o in outs])
+        _check(self.L.mopcuda_batch_read_views_async(self.h, 0, n, what, ptrs, sizes),
+               "batch_read_views_async")
+        return outs
+
+    def wait_readback(self, timeout_ms: int = 20000):
+        _check(self.L.mopcuda_batch_readback_wait(self.h, timeout_ms), "batch_readback_wait")
 
     def pick(self, i: int, xy):
         xy = np.ascontiguousarray(xy, np.int32)

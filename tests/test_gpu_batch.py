@@ -115,6 +115,51 @@ def test_batch_read_views_equals_single_reads(cuda_device, ibl):
         b.close()
 
 
+def test_batch_async_readback_matches_sync(cuda_device, ibl):
+    """mopcuda_batch_read_views_async: launches submitted back to back with
+    new cameras, each launch's images copied while the next one renders (its
+    post passes wait for the copies), equal the synchronous reads of the same
+    launches; with no next submit, readback_wait issues the copies.  Depth
+    and IDs are refused (they are rewritten before the post passes)."""
+    sc = _scene()
+    views0 = _views(sc, 8, seed=7)
+    steps = [scenes.batch_views(sc, n=8, seed=7 + k, min_px=24 * 24, max_px=320 * 240)
+             for k in range(4)]
+    # same sizes and SSAA as the batch, new cameras
+    steps = [[dataclasses.replace(v0, eye=v.eye, target=v.target) for v0, v in zip(views0, vs)]
+             for vs in steps]
+    b = mopcuda.BatchRenderer(cuda_device, sc, views0, ibl)
+    host = []
+    try:
+        want = []
+        for vs in steps:
+            b.set_views(vs)
+            b.render()
+            want.append([b.read(i, w) for w in (mopcuda.BATCH_PRESENTED, mopcuda.BATCH_COLOR)
+                         for i in range(len(vs))])
+        assert any((want[0][i] != want[1][i]).any() for i in range(len(views0)))
+        for k, vs in enumerate(steps):
+            bufs = [mopcuda.HostArray(x.shape, x.dtype) for x in want[k]]
+            host.append(bufs)
+            b.set_views(vs)
+            b.submit()
+            n = len(vs)
+            b.read_all_async(mopcuda.BATCH_PRESENTED, [h.a for h in bufs[:n]])
+            b.read_all_async(mopcuda.BATCH_COLOR, [h.a for h in bufs[n:]])
+        b.wait_readback()
+        for k in range(len(steps)):
+            for i, (h, x) in enumerate(zip(host[k], want[k])):
+                assert h.a.tobytes() == x.tobytes(), f"launch {k} buffer {i}"
+        ids = [np.zeros_like(b.read(i, mopcuda.BATCH_IDS)) for i in range(len(views0))]
+        with pytest.raises(RuntimeError):
+            b.read_all_async(mopcuda.BATCH_IDS, ids)
+    finally:
+        for bufs in host:
+            for h in bufs:
+                h.close()
+        b.close()
+
+
 def test_batch_matches_oracle(cuda_device):
     sc = scenes.small_scene(seed=4, width=96, height=72)
     views = [scenes.View(96, 72, 1, sc.eye, sc.target, fov_deg=sc.fov_deg, near=sc.near,
