@@ -22,6 +22,8 @@
 #define E(m, r, c) ((m)[(c)*4 + (r)])
 
 void mopcuda_mat4_multiply(const float a[16], const float b[16], float out[16]) {
+  if (!a || !b || !out)
+    return;
   float r[16];
   for (int c = 0; c < 4; c++)
     for (int row = 0; row < 4; row++) {
@@ -40,6 +42,8 @@ static void ident(float m[16]) {
 
 void mopcuda_mat4_compose_trs(const float pos[3], const float rot[3], const float scl[3],
                               float out[16]) {
+  if (!pos || !rot || !scl || !out)
+    return;
   float s[16], rx[16], ry[16], rz[16], t[16], m1[16], m2[16], m3[16];
   memset(s, 0, sizeof s);
   E(s, 0, 0) = scl[0];
@@ -121,6 +125,8 @@ static void look_at(v3 e, v3 t, v3 u, float view[16]) {
 void mopcuda_camera_matrices(const float eye[3], const float target[3], const float up[3],
                              float fov_deg, float near_plane, float far_plane, int width,
                              int height, float view[16], float proj[16], float eye_out[3]) {
+  if (!eye || !target || !up || !view || !proj || !eye_out)
+    return;
   v3 e = {eye[0], eye[1], eye[2]}, t = {target[0], target[1], target[2]};
   v3 u = {up[0], up[1], up[2]};
   v3 off = {e.x - t.x, e.y - t.y, e.z - t.z};

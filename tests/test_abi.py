@@ -6,12 +6,16 @@
   (camera chain, mvp products, TRS composition);
 * the ctypes structures of the Python binding have the header's sizes and
   field offsets (a C probe compiled against include/mop_cuda.h);
+* every entry point given null handles and pointers returns an error or a
+  neutral value (NULL, 0, "no hit") instead of crashing;
 * without a CUDA device, device creation fails loudly (no CPU fallback).
 """
 import ctypes as C
+import json
 import re
 import shutil
 import subprocess
+import sys
 from pathlib import Path
 
 import numpy as np
@@ -175,3 +179,41 @@ def test_struct_layouts_match_header(tmp_path):
         assert got[(t, "sizeof")] == C.sizeof(cls), t
         for name, *_ in cls._fields_:
             assert got[(t, name)] == getattr(cls, name).offset, f"{t}.{name}"
+
+
+_NULL_SWEEP = r"""
+import ctypes as C, json, sys
+sys.path[:0] = [sys.argv[1]]
+import mopcuda
+L = mopcuda.lib()
+out = {}
+for name, res, argtypes in mopcuda.SIGNATURES:
+    print(name, flush=True)
+    args = [0.0 if t in (C.c_float, C.c_double) else
+            (0 if t in (C.c_int, C.c_uint32, C.c_uint64, C.c_size_t, C.c_int32) else None)
+            for t in argtypes]
+    r = getattr(L, name)(*args)
+    out[name] = r if isinstance(r, (int, float)) or r is None else str(r)
+print(json.dumps(out))
+"""
+
+# int results that are counts, sizes or "nothing there" rather than status codes
+NEUTRAL_INT = {"mopcuda_scene_file_mesh_count", "mopcuda_scene_file_light_count",
+               "mopcuda_shadow_light_vp"}
+
+
+def test_null_arguments_fail_cleanly():
+    """Every C entry point called with null handles and pointers (and zero
+    sizes) returns instead of crashing: status calls return an error code,
+    creates return NULL, counts and sizes 0.  Run in a child process so a
+    crash names the function."""
+    p = subprocess.run([sys.executable, "-c", _NULL_SWEEP, str(ROOT / "master-of-puppets_b200")],
+                       capture_output=True, text=True, timeout=300)
+    lines = p.stdout.strip().splitlines()
+    assert p.returncode == 0, f"crashed in {lines[-1] if lines else '?'} (rc {p.returncode})"
+    got = json.loads(lines[-1])
+    for name, res, _ in mopcuda.SIGNATURES:
+        if res is C.c_int and name not in NEUTRAL_INT:
+            assert got[name] != 0, f"{name} accepted null arguments"
+        elif res is mopcuda._P:
+            assert got[name] is None, f"{name} returned a handle for null arguments"
