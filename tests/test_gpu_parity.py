@@ -62,6 +62,10 @@ CASES = {
     # in separate meshes, host-skinned tubes, 0.1-8 px triangles
     "config3_reduced": lambda: scenes.config3(n_tris=80_000, width=480, height=270),
     "config3_medium": lambda: scenes.config3(seed=4, n_tris=400_000, width=960, height=540),
+    # the benchmark workloads at full size: 1920x1080 SSAA 2 with 1.47 M triangles, 7 lights,
+    # 1024^2 textures and IBL; 1920x1080 with 2 M clipping / coplanar / skinned triangles
+    "config2_full": lambda: scenes.config2(),
+    "config3_full": lambda: scenes.config3(),
     # blended meshes (alpha / additive / multiply), composited in submission order
     "transparent": lambda: scenes.transparent_scene(seed=21),
     "transparent_ssaa2_ibl": lambda: scenes.transparent_scene(seed=22, ssaa=2, env=1),
