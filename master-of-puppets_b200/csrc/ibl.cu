@@ -290,25 +290,37 @@ struct IblDev {
   SkyArgs sky_args;
 };
 
+/* Both convolutions run a warp per texel: each lane evaluates one of 32
+ * consecutive samples (direction, equirect coordinates, bilinear fetch),
+ * then the warp adds the 32 values one lane at a time in sample order, so
+ * every sum is accumulated in exactly the order of the serial loop. */
+static_assert(IRR_SAMPLES % 32 == 0 && PF_SAMPLES % 32 == 0, "samples in whole warps");
+
 __global__ void __launch_bounds__(128) k_ibl_irradiance(IblDev a) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5); /* warp-uniform */
+  const int lane = (int)(threadIdx.x & 31u);
   if (i >= IRR_W * IRR_H)
     return;
   const float4 *fr = a.tab + a.L.irr_basis / 4 + (size_t)i * 3;
   const float4 T = fr[0], N = fr[1], B = fr[2];
   const float4 *dirs = a.tab + a.L.irr_dirs / 4;
   float acc0 = 0.0f, acc1 = 0.0f, acc2 = 0.0f, total = 0.0f;
-  for (int s = 0; s < IRR_SAMPLES; s++) {
-    const float4 l = dirs[s];
+  for (int s0 = 0; s0 < IRR_SAMPLES; s0 += 32) {
+    const float4 l = dirs[s0 + lane];
     const float wx = T.x * l.x + N.x * l.y + B.x * l.z;
     const float wy = T.y * l.x + N.y * l.y + B.y * l.z;
     const float wz = T.z * l.x + N.z * l.y + B.z * l.z;
     const float4 c = env_dir(a.env, a.env_w, a.env_h, wx, wy, wz);
-    acc0 += c.x;
-    acc1 += c.y;
-    acc2 += c.z;
-    total += 1.0f;
+#pragma unroll 8
+    for (int j = 0; j < 32; j++) {
+      acc0 += __shfl_sync(0xffffffffu, c.x, j);
+      acc1 += __shfl_sync(0xffffffffu, c.y, j);
+      acc2 += __shfl_sync(0xffffffffu, c.z, j);
+      total += 1.0f;
+    }
   }
+  if (lane != 0)
+    return;
   float4 o = make_float4(0.0f, 0.0f, 0.0f, 1.0f);
   if (total > 0.0f) {
     o.x = acc0 / total;
@@ -319,7 +331,8 @@ __global__ void __launch_bounds__(128) k_ibl_irradiance(IblDev a) {
 }
 
 __global__ void __launch_bounds__(128) k_ibl_prefilter(IblDev a) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5); /* warp-uniform */
+  const int lane = (int)(threadIdx.x & 31u);
   if (i >= a.pf_texels)
     return;
   int l = 0, base = 0;
@@ -334,8 +347,8 @@ __global__ void __launch_bounds__(128) k_ibl_prefilter(IblDev a) {
   const float vx = N.x, vy = N.y, vz = N.z;
   const float4 *dirs = a.tab + a.L.pf_dirs / 4 + (size_t)l * PF_SAMPLES;
   float acc0 = 0.0f, acc1 = 0.0f, acc2 = 0.0f, total = 0.0f;
-  for (int s = 0; s < PF_SAMPLES; s++) {
-    const float4 h = dirs[s];
+  for (int s0 = 0; s0 < PF_SAMPLES; s0 += 32) {
+    const float4 h = dirs[s0 + lane];
     const float hx = T.x * h.x + N.x * h.y + B.x * h.z;
     const float hy = T.y * h.x + N.y * h.y + B.y * h.z;
     const float hz = T.z * h.x + N.z * h.y + B.z * h.z;
@@ -344,14 +357,31 @@ __global__ void __launch_bounds__(128) k_ibl_prefilter(IblDev a) {
     const float ly = 2.0f * vdh * hy - vy;
     const float lz = 2.0f * vdh * hz - vz;
     const float ndl = N.x * lx + N.y * ly + N.z * lz;
-    if (ndl <= 0.0f)
-      continue;
-    const float4 c = env_dir(a.env, a.env_w, a.env_h, lx, ly, lz);
-    acc0 += c.x * ndl;
-    acc1 += c.y * ndl;
-    acc2 += c.z * ndl;
-    total += ndl;
+    const bool use = !(ndl <= 0.0f); /* the serial loop skips ndl <= 0 */
+    float px = 0.0f, py = 0.0f, pz = 0.0f;
+    if (use) {
+      const float4 c = env_dir(a.env, a.env_w, a.env_h, lx, ly, lz);
+      px = c.x * ndl;
+      py = c.y * ndl;
+      pz = c.z * ndl;
+    }
+    const unsigned m = __ballot_sync(0xffffffffu, use);
+#pragma unroll 8
+    for (int j = 0; j < 32; j++) {
+      const float qx = __shfl_sync(0xffffffffu, px, j);
+      const float qy = __shfl_sync(0xffffffffu, py, j);
+      const float qz = __shfl_sync(0xffffffffu, pz, j);
+      const float qn = __shfl_sync(0xffffffffu, ndl, j);
+      if ((m >> j) & 1u) {
+        acc0 += qx;
+        acc1 += qy;
+        acc2 += qz;
+        total += qn;
+      }
+    }
   }
+  if (lane != 0)
+    return;
   float4 o = make_float4(0.0f, 0.0f, 0.0f, 1.0f);
   if (total > 0.0f) {
     o.x = acc0 / total;
@@ -505,8 +535,8 @@ int run_precompute(MopCudaDevice *d, const float *env_host, int env_w, int env_h
     k_ibl_sky<<<(SKY_W * SKY_H + 255) / 256, 256, 0, st>>>(a);
     launches++;
   }
-  k_ibl_irradiance<<<(IRR_W * IRR_H + 127) / 128, 128, 0, st>>>(a);
-  k_ibl_prefilter<<<(npf + 127) / 128, 128, 0, st>>>(a);
+  k_ibl_irradiance<<<(IRR_W * IRR_H * 32 + 127) / 128, 128, 0, st>>>(a); /* a warp per texel */
+  k_ibl_prefilter<<<(npf * 32 + 127) / 128, 128, 0, st>>>(a);
   k_ibl_brdf<<<(BRDF_SIZE * BRDF_SIZE + 255) / 256, 256, 0, st>>>(a);
   launches += 3;
   CU_TRY(cudaGetLastError());
