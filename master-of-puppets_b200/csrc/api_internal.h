@@ -88,6 +88,14 @@ struct BufferSlab {
   void *d = nullptr;
   uint32_t refs = 0;
 };
+/* Drops one reference; frees the allocation with the last (device lock
+ * held, nothing in flight reads it). */
+static inline void mc_slab_release(BufferSlab *s) {
+  if (s && --s->refs == 0) {
+    cudaFree(s->d);
+    delete s;
+  }
+}
 
 struct MopCudaBuffer {
   void *d = nullptr;
@@ -164,9 +172,13 @@ struct MopCudaDevice {
   HostArena h_ibl;
   int env_w = 0, env_h = 0;
   cudaEvent_t ibl_t0 = nullptr, ibl_t1 = nullptr;
-  /* scene-file uploads: page-locked and device staging of a mesh section */
+  /* scene-file uploads: page-locked and device staging of a mesh section;
+   * per-mesh uploads carve their buffers from load_chunk (the device holds
+   * one reference on it while it is the current chunk) */
   HostArena h_load;
   DevArena load_stage;
+  BufferSlab *load_chunk = nullptr;
+  size_t load_chunk_used = 0;
   float ibl_rot = 0.0f, ibl_int = 1.0f;
   bool ibl_on = false;
   /* frame arenas */

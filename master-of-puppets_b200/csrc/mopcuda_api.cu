@@ -161,6 +161,8 @@ extern "C" void mopcuda_device_destroy(MopCudaDevice *d) {
   d->h_ibl.release();
   d->h_load.release();
   d->load_stage.release();
+  mc_slab_release(d->load_chunk); /* buffers still carved from it keep it */
+  d->load_chunk = nullptr;
   if (d->ibl_t0) {
     cudaEventDestroy(d->ibl_t0);
     cudaEventDestroy(d->ibl_t1);
@@ -231,14 +233,10 @@ extern "C" void mopcuda_buffer_destroy(MopCudaDevice *d, MopCudaBuffer *b) {
   cudaSetDevice(d->ordinal);
   mc_finish_pending(d);     /* a launched frame may still read it, or re-run */
   mc_stream_sync(d, 10000);
-  if (b->slab) {
-    if (--b->slab->refs == 0) {
-      cudaFree(b->slab->d);
-      delete b->slab;
-    }
-  } else {
+  if (b->slab)
+    mc_slab_release(b->slab);
+  else
     cudaFree(b->d);
-  }
   free(b->h);
   delete b;
 }

@@ -62,6 +62,7 @@ struct LightSection { /* MopLightSection, 64 bytes */
 };
 
 uint64_t align8(uint64_t v) { return (v + 7u) & ~(uint64_t)7u; }
+uint64_t align256(uint64_t v) { return (v + 255u) & ~(uint64_t)255u; }
 
 /* dequantize_vertex + oct_decode, mop_scene.c:142-223: one thread per
  * vertex; q holds 18-byte records (9 halfwords: position x3, octahedral
@@ -344,6 +345,37 @@ extern "C" int mopcuda_scene_file_light(const MopCudaSceneFile *f, uint32_t idx,
   return MOPCUDA_OK;
 }
 
+/* Per-mesh uploads carve their two buffers from 64 MiB device chunks: one
+ * allocation serves many meshes (a cudaMalloc per buffer took most of a
+ * mesh's upload).  A chunk is freed with the last buffer carved from it once
+ * a newer chunk has replaced it; a mesh larger than a chunk gets an
+ * allocation of its own.  Device lock held. */
+constexpr size_t LOAD_CHUNK = 64ull << 20;
+
+static BufferSlab *carve_load(MopCudaDevice *d, size_t bytes, size_t *off) {
+  BufferSlab *s = nullptr;
+  if (bytes > LOAD_CHUNK || !d->load_chunk || d->load_chunk_used + bytes > LOAD_CHUNK) {
+    s = new BufferSlab();
+    const size_t n = bytes > LOAD_CHUNK ? bytes : LOAD_CHUNK;
+    if (cudaMalloc(&s->d, n) != cudaSuccess) {
+      cudaGetLastError();
+      delete s;
+      return nullptr;
+    }
+    if (bytes > LOAD_CHUNK) {
+      *off = 0;
+      return s; /* refs come from its two buffers */
+    }
+    s->refs = 1; /* the device's hold while it is the current chunk */
+    mc_slab_release(d->load_chunk);
+    d->load_chunk = s;
+    d->load_chunk_used = 0;
+  }
+  *off = d->load_chunk_used;
+  d->load_chunk_used += bytes;
+  return d->load_chunk;
+}
+
 extern "C" int mopcuda_scene_file_upload_mesh(MopCudaDevice *d, const MopCudaSceneFile *f,
                                               uint32_t idx, uint32_t flags,
                                               MopCudaBuffer **vertices, MopCudaBuffer **indices,
@@ -381,12 +413,21 @@ extern "C" int mopcuda_scene_file_upload_mesh(MopCudaDevice *d, const MopCudaSce
   vb->size = out_v;
   ib->size = out_i;
   const bool shadow = (flags & MOPCUDA_LOAD_HOST_SHADOW) != 0;
-  if (cudaMalloc(&vb->d, out_v ? out_v : 16) != cudaSuccess ||
-      cudaMalloc(&ib->d, out_i ? out_i : 16) != cudaSuccess ||
+  const size_t span_v = align256(out_v ? out_v : 1), span_i = align256(out_i ? out_i : 1);
+  size_t off = 0;
+  BufferSlab *slab = carve_load(d, span_v + span_i, &off);
+  if (slab) {
+    vb->slab = ib->slab = slab;
+    slab->refs += 2;
+    vb->d = (uint8_t *)slab->d + off;
+    ib->d = (uint8_t *)slab->d + off + span_v;
+  }
+  if (!slab ||
       (shadow && (!(vb->h = malloc(out_v ? out_v : 16)) || !(ib->h = malloc(out_i ? out_i : 16))))) {
-    cudaGetLastError();
-    cudaFree(vb->d);
-    cudaFree(ib->d);
+    if (slab) {
+      mc_slab_release(slab);
+      mc_slab_release(slab);
+    }
     free(vb->h);
     free(ib->h);
     delete vb;
@@ -441,8 +482,8 @@ extern "C" int mopcuda_scene_file_upload_mesh(MopCudaDevice *d, const MopCudaSce
   } while (0);
   const cudaError_t ce = cudaGetLastError();
   mc_stream_sync(d, FRAME_TIMEOUT_MS);
-  cudaFree(vb->d);
-  cudaFree(ib->d);
+  mc_slab_release(slab);
+  mc_slab_release(slab);
   free(vb->h);
   free(ib->h);
   delete vb;

@@ -91,6 +91,57 @@ def test_device_decode_wide_mesh(cuda_device, tmp_path, quant):
     _same(_device_meshes(cuda_device, path, False, whole_file=True), want)
 
 
+def test_per_mesh_buffers_across_chunks(cuda_device, tmp_path):
+    """Per-mesh uploads carve their buffers from 64 MiB device chunks: uploads
+    that fill several chunks, a mesh larger than a chunk (an allocation of
+    its own), buffers destroyed out of order while others stay live, and
+    uploads after that all keep every buffer's bytes equal to the oracle's
+    decode."""
+    big_v, big_i = scenes.uv_sphere(1200, 1200, 1.0, (0.8, 0.3, 0.2, 1.0))  # 1.45 M vertices
+    sc = scenes.small_scene(seed=9, n_meshes=1)
+    v, i = scenes.uv_sphere(300, 240, 1.1, (0.2, 0.5, 0.9, 1.0))  # 3.5 MB decoded
+    sc.meshes = [scenes.Mesh(v, i, 11, scenes.mat_identity())]
+    path = tmp_path / "mid.mop"
+    scene_file.save(sc, path, True)
+    want = cpu_oracle.scene_file_meshes(path)[0]
+    sc_big = scenes.small_scene(seed=9, n_meshes=1)
+    sc_big.meshes = [scenes.Mesh(big_v, big_i, 12, scenes.mat_identity())]
+    big_path = tmp_path / "big.mop"
+    scene_file.save(sc_big, big_path, True)
+    want_big = cpu_oracle.scene_file_meshes(big_path)[0]
+    assert want_big[0].nbytes > 64 << 20
+    L = cuda_device.L
+    live = []
+
+    def check(b, w):
+        v = np.zeros((b["vertex_count"], 12), np.float32)
+        i = np.zeros(b["index_count"], np.uint32)
+        _read_device(cuda_device, b, v, i)
+        assert v.tobytes() == w[0].tobytes() and (i == w[1]).all()
+
+    def drop(b):
+        L.mopcuda_buffer_destroy(cuda_device.h, b["vertices"])
+        L.mopcuda_buffer_destroy(cuda_device.h, b["indices"])
+
+    try:
+        for _ in range(40):  # about 140 MB: three chunks
+            live.append((scene_file.upload(cuda_device, path)[0], want))
+        live.append((scene_file.upload(cuda_device, big_path)[0], want_big))
+        for b, w in live:
+            check(b, w)
+        for k in sorted(range(len(live)), key=lambda k: (k * 7) % 11)[:25]:
+            drop(live[k][0])
+            live[k] = None
+        live = [x for x in live if x is not None]
+        for _ in range(20):
+            live.append((scene_file.upload(cuda_device, path)[0], want))
+        for b, w in live:
+            check(b, w)
+    finally:
+        for x in live:
+            drop(x[0])
+
+
 def test_truncated_section_rejected(cuda_device, tmp_path):
     data = bytearray((GOLDEN / "scene_coplanar_raw.mop").read_bytes())
     kind, _, off, size = struct.unpack_from("<IIQQ", data, 64 + 24 * 10)  # a mesh entry
