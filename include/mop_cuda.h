@@ -330,8 +330,9 @@ int mopcuda_read_color_resolved(MopCudaDevice *dev, MopCudaFramebuffer *fb, int 
                                 uint8_t *out, size_t out_size);
 /* The same image, read asynchronously (no reference counterpart): the copy
  * into `out` (page-locked memory for a true overlap, mopcuda_host_alloc)
- * starts on a separate copy stream when the frame completes, overlapping the
- * next frame's work; ssaa must be 1 or the framebuffer's presentation
+ * starts on a separate copy stream when the frame completes, queued inside
+ * the next frame's launch when mopcuda_frame_end follows, and overlaps that
+ * frame's work; ssaa must be 1 or the framebuffer's presentation
  * factor.  mopcuda_readback_wait returns once the framebuffer's last
  * requested image is in host memory (it completes the frame first when it
  * is still pending). */

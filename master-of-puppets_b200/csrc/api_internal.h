@@ -120,7 +120,8 @@ struct MopCudaFramebuffer {
   bool presented_valid = false;
   uint64_t frame_serial = 0;
   /* asynchronous presented-colour readback: requested for the pending frame
-   * (issued once it completes) or in flight on the device's copy stream */
+   * (issued once it completes, inside the next launch when frame_end follows)
+   * or in flight on the device's copy stream */
   cudaEvent_t rb_done = nullptr;
   bool rb_requested = false, rb_live = false;
   void *rb_dst = nullptr;

@@ -1437,9 +1437,10 @@ extern "C" int mopcuda_read_color_resolved(MopCudaDevice *d, MopCudaFramebuffer 
 
 /* Asynchronous readback of the presented image (no reference counterpart:
  * the synchronous read is mop_viewport_read_color).  The copy runs on the
- * device's copy stream once the frame has completed, so it overlaps the next
- * frame's work; the next frame's post pass, which overwrites the image,
- * waits for it. */
+ * device's copy stream once the frame has completed; when frame_end launches
+ * the next frame, it is queued inside that launch (frame_pre_post), after
+ * the frame's upload and kernels up to shading, so it overlaps their work;
+ * the next frame's post pass, which overwrites the image, waits for it. */
 static int issue_readback(MopCudaDevice *d, MopCudaFramebuffer *fb) {
   fb->rb_requested = false;
   if (!fb->rb_done)
@@ -1469,7 +1470,7 @@ extern "C" int mopcuda_read_color_resolved_async(MopCudaDevice *d, MopCudaFrameb
   fb->rb_ssaa = sf;
   fb->rb_requested = true;
   if (d->fb == fb && d->pending)
-    return MOPCUDA_OK; /* issued when the frame completes */
+    return MOPCUDA_OK; /* issued when the frame completes (inside the next launch) */
   return issue_readback(d, fb);
 }
 
