@@ -2,7 +2,8 @@
 scenes.  A request's result is the same alone and in a mix of other scenes,
 sizes, SSAA factors and pick requests, and equals the single-viewport frame
 of the same draws and camera; admission respects the HBM budget (a budget
-too small for two requests runs them one launch at a time, same results).
+too small for two requests runs them one launch at a time, same results)
+and the per-launch sample cap.
 """
 import dataclasses
 
@@ -117,6 +118,33 @@ def test_server_budget_admission(cuda_device, world):
         assert st["max_views_in_launch"] == 1 and st["launches"] == 6, st
         for t, v in zip(ts, views):
             _same_render(t, _plain(cuda_device, scs[0], v, ibl), "budget-limited")
+    finally:
+        srv.close()
+
+
+def test_server_launch_sample_cap(cuda_device, world):
+    """max_launch_samples: a launch takes requests only while their samples
+    fit the cap (three 64x64 views here), a request larger than the cap
+    still runs, alone, and every result equals the request's own frame."""
+    scs, rss, ibl = world
+    side = 64
+    cap = 3 * side * side
+    srv = mopcuda.Server(cuda_device, hbm_budget=8 << 30, max_views=16, max_inflight=2,
+                         max_launch_samples=cap)
+    try:
+        sid = srv.add_scene(rss[1])
+        views = [dataclasses.replace(v, width=side, height=side, ssaa=1)
+                 for v in _views(scs[1], 12, seed=21)]
+        big = dataclasses.replace(views[0], width=2 * side, height=2 * side, ssaa=1)
+        ts = [srv.submit_render(sid, v, want_ids=True, want_depth=True) for v in views]
+        tb = srv.submit_render(sid, big, want_ids=True, want_depth=True)
+        for t in ts + [tb]:
+            srv.wait(t)
+        st = srv.stats()
+        assert st["completed"] == 13 and st["failed"] == 0, st
+        assert st["max_views_in_launch"] <= 3 and st["launches"] >= 5, st
+        for t, v in zip(ts + [tb], views + [big]):
+            _same_render(t, _plain(cuda_device, scs[1], v, ibl), f"capped {v.width}x{v.height}")
     finally:
         srv.close()
 
