@@ -11,8 +11,8 @@ depth bit-exact, colour within the contract tolerance.
 Scenes avoid image-based lighting: the unmodified core hands IBL state only
 to its CPU path (reference viewport.c:2692-2706); the CUDA backend receives
 the full IBL state through mopcuda_set_ibl (covered by test_gpu_parity.py).
-The reference's own picking and depth test programs also run unmodified on
-the CUDA backend (a link-time wrapper of mop_viewport_create selects it).
+Twelve of the reference's own test programs also run unmodified on the
+CUDA backend (a link-time wrapper of mop_viewport_create selects it).
 The shadow scenes run the core's own pass_shadow on the CPU side; on the
 CUDA side the harness registers the integration patch's shadow pass as a
 MOP_STAGE_PRE_SCENE hook (the core runs pass_shadow for its CPU backend
@@ -78,21 +78,30 @@ def test_viewport_api_cuda_matches_cpu(name):
         cpu.close()
 
 
-TORTURE = Path(__file__).resolve().parents[1] / "oracle" / "_ref"
+REFTESTS = Path(__file__).resolve().parents[1] / "oracle" / "_ref" / "tests"
+
+# the reference's own test programs that drive the public viewport API, with
+# their check counts (each passes them all on the reference's CPU backend)
+REFERENCE_SUITES = {"test_torture_picking": 10, "test_torture_depth": 8,
+                    "test_torture_golden": 6, "test_torture_geometry": 12,
+                    "test_torture_lighting": 8, "test_torture_hierarchy": 9,
+                    "test_torture_camera": 10, "test_exposure": 3, "test_skinning": 8,
+                    "test_morph_targets": 7, "test_procedural_sky": 4,
+                    "test_ortho_camera": 6}
 
 
-@pytest.mark.parametrize("suite,count", [("picking", 10), ("depth", 8)])
-def test_reference_torture_suite_on_cuda_backend(suite, count):
-    """The reference's own tests/test_torture_<suite>.c, compiled unmodified
-    and linked with the drop-in objects (oracle/Makefile `torture`): every
-    viewport it creates runs on the CUDA backend, and all its known-answer
-    checks (corner, boundary, out-of-range, overlapping, hierarchy, SSAA,
-    transparent and replay picks; depth order, near/far planes, gradient,
-    large coordinates, clear value) pass."""
-    exe = TORTURE / f"torture_{suite}"
+@pytest.mark.parametrize("suite", list(REFERENCE_SUITES))
+def test_reference_suite_on_cuda_backend(suite):
+    """The reference's own tests/<suite>.c, compiled unmodified and linked
+    with the drop-in objects (oracle/Makefile `reftests`): every viewport it
+    creates runs on the CUDA backend and all of its checks pass (picks at
+    corners, boundaries, out of range, through hierarchies, with SSAA and
+    transparency; depth order and planes; golden determinism; geometry,
+    lighting, camera, exposure, skinning, morph and sky cases)."""
+    exe = REFTESTS / f"{suite}_cuda"
     if not exe.exists():
-        pytest.skip("torture programs not built (reference tree absent at build time)")
+        pytest.skip("reference test programs not built (reference tree absent at build time)")
     p = subprocess.run([str(exe)], capture_output=True, text=True, timeout=300)
     out = p.stdout
     assert p.returncode == 0, out[-3000:] + p.stderr[-2000:]
-    assert f"Passed: {count}" in out and "FAIL" not in out, out[-3000:]
+    assert f"Passed: {REFERENCE_SUITES[suite]}" in out and "FAIL" not in out, out[-3000:]
