@@ -7,6 +7,7 @@ reference: bit-exact on colour, depth, object IDs, camera matrices and picks.
   larger seeded scenes, when that library has been built.
 """
 import dataclasses
+import subprocess
 from pathlib import Path
 
 import numpy as np
@@ -129,3 +130,24 @@ def test_deform_oracle_matches_reference():
         # both set: the core morphs, then skins from the bind pose again
         ref = refdrive.deform_probe(raw, vc, bones=bones, targets=targets, weights=weights)
         assert (cpu_oracle.skin(lay, raw, vc, bones) == ref).all(), f"skin+morph seed {seed}"
+
+
+REFTESTS = Path(__file__).resolve().parents[1] / "oracle" / "_ref" / "tests"
+
+
+@pytest.mark.parametrize("suite", ["test_torture_picking", "test_torture_depth",
+                                   "test_torture_golden", "test_torture_geometry",
+                                   "test_torture_lighting", "test_torture_hierarchy",
+                                   "test_torture_camera", "test_exposure", "test_skinning",
+                                   "test_morph_targets", "test_procedural_sky",
+                                   "test_ortho_camera"])
+def test_reference_suite_on_its_cpu_backend(suite):
+    """The reference's own test program, built by oracle/Makefile `reftests`
+    from the unmodified sources, passes on the reference's CPU backend: the
+    baseline for the same programs linked to the CUDA backend
+    (test_gpu_dropin.py)."""
+    exe = REFTESTS / f"{suite}_cpu"
+    if not exe.exists():
+        pytest.skip("reference test programs not built (reference tree absent at build time)")
+    p = subprocess.run([str(exe)], capture_output=True, text=True, timeout=300)
+    assert p.returncode == 0 and "FAIL" not in p.stdout, p.stdout[-3000:]
