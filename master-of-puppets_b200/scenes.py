@@ -91,6 +91,8 @@ class Scene:
     env_rotation: float = 0.0
     env_intensity: float = 1.0
     smooth: bool = True           # MOP_SHADING_SMOOTH (viewport default)
+    # MopFogParams ((r, g, b, a), near, far) for the MOP_POST_FOG bit; None: not set
+    fog: Optional[Tuple[Tuple[float, float, float, float], float, float]] = None
 
     @property
     def samples(self) -> int:

@@ -65,7 +65,9 @@ class OrFrame(C.Structure):
                 ("post_effects", C.c_uint32), ("ibl", C.POINTER(OrIBL)),
                 ("color_full", C.c_void_p), ("depth", C.c_void_p),
                 ("object_id", C.c_void_p), ("color_presented", C.c_void_p),
-                ("hdr", C.c_void_p), ("shadow", C.POINTER(OrShadow))]
+                ("hdr", C.c_void_p), ("shadow", C.POINTER(OrShadow)),
+                ("fog_on", C.c_int32), ("fog_color", C.c_float * 4),
+                ("fog_near", C.c_float), ("fog_far", C.c_float)]
 
 
 _lib = None
@@ -246,6 +248,11 @@ def render(scene, ibl=None, want_hdr=False):
     f.clear[:] = scene.clear
     f.exposure = scene.exposure
     f.post_effects = scene.post_effects
+    fog = getattr(scene, "fog", None)
+    if fog is not None:
+        f.fog_on = 1
+        f.fog_color[:] = fog[0]
+        f.fog_near, f.fog_far = fog[1], fog[2]
     if ibl is not None:
         arrs = [_f32(ibl["irr"]), _f32(ibl["pf"]), _f32(ibl["brdf"])]
         keep += arrs

@@ -1362,9 +1362,10 @@ void oracle_gamma_lut(uint8_t lut[256]) {
   }
 }
 
-/* mop_postprocess_apply, postprocess.c:24-116 (fog parameters are not part
- * of this path's inputs; a FOG bit is ignored). */
-static void postprocess(FB *fb, uint32_t fx) {
+/* mop_postprocess_apply, postprocess.c:24-116: FXAA, then per sample fog
+ * (from the sample's depth value, :51-65), Reinhard tonemap, sRGB gamma and
+ * vignette, clamped and rounded to bytes. */
+static void postprocess(FB *fb, uint32_t fx, const OrFrame *f) {
   if (fx == 0)
     return;
   if (fx & 16u)
@@ -1378,6 +1379,20 @@ static void postprocess(FB *fb, uint32_t fx) {
       float c[3];
       for (int k = 0; k < 3; k++)
         c[k] = (float)p[k] / 255.0f;
+      if ((fx & 8u) && f->fog_on) {
+        const float depth = fb->depth[(size_t)y * w + x];
+        const float range = f->fog_far - f->fog_near;
+        float factor = 0.0f;
+        if (range > 0.0f) {
+          factor = (depth - f->fog_near) / range;
+          if (factor < 0.0f)
+            factor = 0.0f;
+          if (factor > 1.0f)
+            factor = 1.0f;
+        }
+        for (int k = 0; k < 3; k++)
+          c[k] = c[k] + (f->fog_color[k] - c[k]) * factor;
+      }
       if (fx & 2u)
         for (int k = 0; k < 3; k++)
           c[k] = c[k] / (c[k] + 1.0f);
@@ -1443,7 +1458,7 @@ int oracle_render(OrFrame *f, const OrDraw *draws, uint32_t n) {
   if (f->hdr)
     memcpy(f->hdr, fb.hdr, px * 16);
   hdr_resolve(&fb, f->exposure);
-  postprocess(&fb, f->post_effects);
+  postprocess(&fb, f->post_effects, f);
   if (f->color_full)
     memcpy(f->color_full, fb.color, px * 4);
   if (f->depth)

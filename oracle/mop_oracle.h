@@ -98,6 +98,10 @@ typedef struct OrFrame {
   uint8_t *color_presented; /* (width/ssaa)*(height/ssaa)*4 */
   float *hdr;               /* width*height*4, before resolve */
   const OrShadow *shadow;   /* NULL = no shadow map bound */
+  /* MopFogParams, applied when post_effects has MOP_POST_FOG (fog_on) */
+  int32_t fog_on;
+  float fog_color[4];
+  float fog_near, fog_far;
 } OrFrame;
 
 /* Render one frame of draws in submission order.  Returns 0 on success. */

@@ -144,6 +144,11 @@ void *refh_create(const RefScene *sc) {
   mop_viewport_set_ambient(vp, sc->ambient);
   mop_viewport_set_exposure(vp, sc->exposure);
   mop_viewport_set_post_effects(vp, sc->post_effects);
+  if (sc->fog_on) {
+    MopFogParams fog = {{sc->fog_color[0], sc->fog_color[1], sc->fog_color[2], sc->fog_color[3]},
+                        sc->fog_near, sc->fog_far};
+    mop_viewport_set_fog(vp, &fog);
+  }
   if (sc->flat)
     mop_viewport_set_shading(vp, MOP_SHADING_FLAT);
   mop_viewport_set_camera(

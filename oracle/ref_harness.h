@@ -73,6 +73,9 @@ typedef struct RefScene {
                                worker threads (default: nproc-1)           */
   int32_t backend;          /* 0: MOP_BACKEND_CPU; 4: the CUDA backend
                                (only in the drop-in harness library)       */
+  int32_t fog_on;           /* 1: mop_viewport_set_fog with the values below */
+  float fog_color[4];
+  float fog_near, fog_far;
 } RefScene;
 
 typedef struct RefFrame {

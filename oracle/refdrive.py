@@ -48,7 +48,9 @@ class RefScene(C.Structure):
                 ("ground_albedo", C.c_float), ("env_rotation", C.c_float),
                 ("env_intensity", C.c_float), ("serial", C.c_int32),
                 ("flat", C.c_int32), ("workers", C.c_int32),
-                ("backend", C.c_int32)]
+                ("backend", C.c_int32), ("fog_on", C.c_int32),
+                ("fog_color", C.c_float * 4), ("fog_near", C.c_float),
+                ("fog_far", C.c_float)]
 
 
 class RefFrame(C.Structure):
@@ -173,6 +175,11 @@ class Reference:
         sc.flat = 0 if getattr(scene, "smooth", True) else 1
         sc.workers = int(workers)
         sc.backend = 0 if backend == "cpu" else BACKEND_CUDA
+        fog = getattr(scene, "fog", None)
+        if fog is not None:
+            sc.fog_on = 1
+            sc.fog_color[:] = fog[0]
+            sc.fog_near, sc.fog_far = fog[1], fog[2]
         self._keep += [meshes, lights, tw, th, td, sc]
         self.h = L.refh_create(C.byref(sc))
         if not self.h:

@@ -79,6 +79,19 @@ LIVE = {
     # no lights: legacy smooth path (silhouette edge AA) with blended meshes
     "unlit_transparent": lambda: dataclasses.replace(scenes.transparent_scene(seed=35),
                                                      lights=[]),
+    # MOP_POST_FOG (mop_viewport_set_fog): colour blended towards the fog colour by each
+    # sample's depth value, before tonemap / gamma / vignette; a zero range leaves it off
+    "fog": lambda: dataclasses.replace(
+        scenes.small_scene(seed=41), post_effects=scenes.DEFAULT_POST | scenes.POST_FOG,
+        fog=((0.6, 0.65, 0.7, 1.0), 0.85, 0.99)),
+    "fog_all_effects_ssaa2": lambda: dataclasses.replace(
+        scenes.small_scene(seed=42, ssaa=2),
+        post_effects=(scenes.POST_GAMMA | scenes.POST_TONEMAP | scenes.POST_VIGNETTE
+                      | scenes.POST_FOG | scenes.POST_FXAA),
+        fog=((0.2, 0.3, 0.5, 1.0), 0.9, 0.995)),
+    "fog_zero_range": lambda: dataclasses.replace(
+        scenes.small_scene(seed=43), post_effects=scenes.DEFAULT_POST | scenes.POST_FOG,
+        fog=((1.0, 0.0, 0.0, 1.0), 0.95, 0.95)),
 }
 
 
