@@ -3,8 +3,9 @@
  *
  * Linked in place of the reference's src/rhi/rhi.c (same three functions,
  * rhi.c:15-72) so that the UNMODIFIED reference viewport core resolves
- * backend value 4 — MOP_BACKEND_CUDA in the integration patch described in
- * INTEGRATION.md — to mop_rhi_backend_cuda().  Everything else in the core is
+ * backend value 4 — MOP_BACKEND_CUDA in the integration patch (a new
+ * enumerator after MOP_BACKEND_VULKAN, backend.h:24-30) — to
+ * mop_rhi_backend_cuda().  Everything else in the core is
  * the reference's own object code.
  */
 #include "rhi/rhi.h"

@@ -2,7 +2,7 @@
 
 The unmodified reference viewport core (its compiled objects, with only the
 backend-resolution function swapped so value 4 means the CUDA backend — the
-integration patch in INTEGRATION.md does the same with MOP_BACKEND_CUDA)
+integration patch does the same with a MOP_BACKEND_CUDA enumerator)
 renders each scene twice in one process: once on its CPU backend, once on
 mop_rhi_backend_cuda().  mop_viewport_read_color (SSAA box in the core),
 the object-ID / depth readbacks and mop_viewport_pick must agree: IDs and
