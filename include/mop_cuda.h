@@ -44,6 +44,7 @@ extern "C" {
 #define MOPCUDA_POST_GAMMA (1u << 0)
 #define MOPCUDA_POST_TONEMAP (1u << 1)
 #define MOPCUDA_POST_VIGNETTE (1u << 2)
+#define MOPCUDA_POST_FOG (1u << 3)
 #define MOPCUDA_POST_FXAA (1u << 4)
 
 typedef struct MopCudaDevice MopCudaDevice;
@@ -185,8 +186,17 @@ int mopcuda_morph_apply(MopCudaDevice *dev, MopCudaBuffer *dst, const MopCudaBuf
  * (reference mop_sw_hdr_resolve, rasterizer.c:2776). */
 void mopcuda_set_exposure(MopCudaDevice *dev, float exposure);
 /* Post-effect bits applied after the resolve (mop_postprocess_apply,
- * postprocess.c:24); default GAMMA|FXAA as the viewport sets it. */
+ * postprocess.c:24); default GAMMA|FXAA as the viewport sets it.  FOG,
+ * TONEMAP, GAMMA and VIGNETTE run per sample in the reference's order; the
+ * other bits (bloom, SSAO, ...) belong to GPU effect hooks the CPU path
+ * ignores, and are ignored here too. */
 void mopcuda_set_post_effects(MopCudaDevice *dev, uint32_t effects);
+/* mop_viewport_set_fog (postprocess.c:170-175): the MopFogParams the FOG bit
+ * uses (colour RGBA, only RGB read; near and far distances compared with each
+ * sample's depth value, postprocess.c:51-65).  A device starts with all zero,
+ * as a new viewport does: factor 0, colours unchanged.  Returns EINVAL for a
+ * null device or colour. */
+int mopcuda_set_fog(MopCudaDevice *dev, const float color[4], float near_dist, float far_dist);
 /* IBL maps, as mop_sw_ibl_set (rasterizer.h:212-215): irradiance RGBA32F
  * iw x ih, prefiltered RGBA32F mip chain concatenated (levels), BRDF LUT
  * RGBA32F size x size.  Copied to the device.  NULL irradiance clears. */
@@ -312,7 +322,9 @@ int mopcuda_draw_instanced(MopCudaDevice *dev, MopCudaFramebuffer *fb, const Mop
 /* Launch the recorded frame (asynchronous; returns after enqueueing). */
 int mopcuda_frame_end(MopCudaDevice *dev, MopCudaFramebuffer *fb);
 /* Bounded wait for the last launched frame; MOPCUDA_ETIMEOUT after
- * timeout_ms (the frame's result is then undefined). */
+ * timeout_ms, with the frame still pending: a later wait (or any call that
+ * completes the frame first) resumes waiting for it.  A device error
+ * (MOPCUDA_ECUDA) ends the frame with its result undefined. */
 int mopcuda_frame_wait(MopCudaDevice *dev, int timeout_ms);
 /* Device time of the last completed frame (frame_gpu_time_ms, rhi.h:240). */
 float mopcuda_frame_gpu_time_ms(MopCudaDevice *dev);
@@ -358,9 +370,14 @@ int mopcuda_pick_batch(MopCudaDevice *dev, MopCudaFramebuffer *fb, int ssaa, con
  * MOPCUDA_NOALLOC_PICK_MAX queries are rejected with MOPCUDA_EINVAL.  xy and
  * the outputs are host memory.  The frame must be complete
  * (mopcuda_frame_wait) — completing it here could reallocate.  The first
- * call on a device resolves the array's device address and creates one
- * event; make it before any stream capture.  All calls share the array (it
- * keeps the last call's contents): calls that overlap on the GPU race. */
+ * call on a device resolves the array's device address; make it before any
+ * stream capture.  All calls share the array (it keeps the last call's
+ * contents): calls that overlap on the GPU race.  The results are copied
+ * straight into the caller's arrays, so the 20 s wait bounds the call only
+ * when ids, depths and hits are page-locked (mopcuda_host_alloc): a copy
+ * into pageable memory holds the host until the pick kernel ends.  After
+ * MOPCUDA_ETIMEOUT the copies are still queued: xy and the outputs stay in
+ * use until the device is synchronised or destroyed. */
 #define MOPCUDA_NOALLOC_PICK_MAX 65536u
 int mopcuda_pick_batch_noalloc(MopCudaDevice *dev, MopCudaFramebuffer *fb, int ssaa,
                                const int32_t *xy, uint32_t n, uint32_t *ids, float *depths,

@@ -135,6 +135,7 @@ struct MopCudaDevice {
   cudaStream_t stream = nullptr;
   cudaStream_t copy_stream = nullptr; /* asynchronous readbacks */
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  cudaEvent_t pick_ev = nullptr; /* the allocation-free pick's bounded wait */
   cudaEvent_t stage_ev[MOPCUDA_STAGES + 1] = {};
   bool stage_timing = false;
   float stage_ms[MOPCUDA_STAGES] = {};
@@ -166,6 +167,7 @@ struct MopCudaDevice {
   float exposure = 1.0f;
   uint32_t post = MOPCUDA_POST_GAMMA | MOPCUDA_POST_FXAA;
   float lut[256];
+  float fog[6] = {0, 0, 0, 0, 0, 0}; /* MopFogParams: colour RGBA, near, far */
   /* IBL */
   DevArena irr, pf, brdf;
   int irr_w = 0, irr_h = 0, pf_w = 0, pf_h = 0, pf_levels = 0, brdf_size = 0;
@@ -229,6 +231,10 @@ void mc_ibl_consts(bool on, int pf_w, int pf_h, int levels, int brdf_size, DrawR
                    uint32_t n);
 /* Post-process arguments for the device's current effects. */
 void mc_post_args(const MopCudaDevice *d, PostArgs &p);
+/* Post-process arguments for effect bits `fx` with the per-byte values `lut`
+ * (build_lut of fx) and fog parameters `fog` (colour RGBA, near, far); the
+ * buffer pointers and sizes are left to the caller. */
+void mc_post_template(uint32_t fx, const float lut[256], const float fog[6], PostArgs &p);
 /* mop_mat4_multiply order: running sum from 0.0f, no contraction. */
 void mc_mat4_mul(const float *a, const float *b, float *c);
 

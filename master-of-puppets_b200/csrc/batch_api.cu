@@ -152,7 +152,8 @@ extern "C" int mopcuda_scene_add_draw(MopCudaScene *s, const MopCudaDraw *c) {
     return rc;
   }
   if (!skip && (r.blend_mode != 0 || r.opacity < 1.0f ||
-                ((r.flags & DF_SMOOTH) && !(r.flags & DF_LIT)))) {
+                ((r.flags & DF_SMOOTH) && !(r.flags & DF_LIT)) ||
+                (r.flags & (DF_NO_DEPTH_WRITE | DF_NO_DEPTH_TEST)))) {
     s->lights.resize(nl);
     return fail(MOPCUDA_EUNSUPPORTED,
                 "scene_add_draw: batches render opaque lit or flat draws only");
@@ -275,6 +276,7 @@ int LaunchCore::init(MopCudaDevice *d) {
   exposure = d->exposure;
   post_effects = d->post;
   memcpy(lut, d->lut, sizeof lut);
+  memcpy(fog, d->fog, sizeof fog);
   return MOPCUDA_OK;
 }
 
@@ -406,19 +408,7 @@ int LaunchCore::set_layout(const MopCudaView *views, const uint32_t *scene_of,
   if (rc)
     return MOPCUDA_ENOMEM;
   PostArgs post;
-  memset(&post, 0, sizeof post);
-  post.effects = post_effects & (MOPCUDA_POST_GAMMA | MOPCUDA_POST_TONEMAP |
-                                 MOPCUDA_POST_VIGNETTE | MOPCUDA_POST_FXAA);
-  memcpy(post.lut, lut, sizeof post.lut);
-  for (int i = 0; i < 256; i++) {
-    float v = lut[i];
-    if (v > 1.0f)
-      v = 1.0f;
-    if (v < 0.0f)
-      v = 0.0f;
-    volatile float q = v * 255.0f + 0.5f; /* postprocess.c:110-112 */
-    post.lut8[i] = (uint8_t)(int)q;
-  }
+  mc_post_template(post_effects, lut, fog, post);
   std::vector<uint32_t> lists(4ull * n, 0u);
   for (int k = 0; k < 4; k++)
     post_count[k] = post_tiles[k] = 0;
@@ -428,6 +418,7 @@ int LaunchCore::set_layout(const MopCudaView *views, const uint32_t *scene_of,
     p.pre = pre.as<uchar4>() + r.sample_off;
     p.out = out.as<uchar4>() + r.sample_off;
     p.presented = r.ssaa > 1 ? presented.as<uchar4>() + r.pixel_off : nullptr;
+    p.depth = depth.as<float>() + r.sample_off;
     p.width = r.width;
     p.height = r.height;
     p.ssaa = r.ssaa;
@@ -1127,52 +1118,59 @@ extern "C" int mopcuda_batch_autotune(MopCudaBatch *b, int reps, char *report,
       {"vertex_block", {{128, 0}, {256, 0}}},
       {"grid_mul", {{1, 0}, {2, 0}}},
   };
-  for (const Axis &ax : axes)
-    for (const auto &val : ax.values) {
-      MopCudaBatchConfig c = best;
-      const std::string nm = ax.name;
-      if (nm == "small") {
-        c.small_side = val.first;
-        c.small_area = val.second;
-      } else if (nm == "raster_block") {
-        c.raster_block = val.first;
-      } else if (nm == "setup_block") {
-        c.setup_block = val.first;
-      } else if (nm == "large_block") {
-        c.large_block = val.first;
-      } else if (nm == "shade_block") {
-        c.shade_block = val.first;
-      } else if (nm == "vertex_block") {
-        c.vertex_block = val.first;
-      } else {
-        c.grid_mul = val.first;
+  /* coordinate descent: passes over every axis until a pass improves nothing
+   * (at most three) */
+  int passes = 0;
+  for (bool improved = true; improved && passes < 3; passes++) {
+    improved = false;
+    for (const Axis &ax : axes)
+      for (const auto &val : ax.values) {
+        MopCudaBatchConfig c = best;
+        const std::string nm = ax.name;
+        if (nm == "small") {
+          c.small_side = val.first;
+          c.small_area = val.second;
+        } else if (nm == "raster_block") {
+          c.raster_block = val.first;
+        } else if (nm == "setup_block") {
+          c.setup_block = val.first;
+        } else if (nm == "large_block") {
+          c.large_block = val.first;
+        } else if (nm == "shade_block") {
+          c.shade_block = val.first;
+        } else if (nm == "vertex_block") {
+          c.vertex_block = val.first;
+        } else {
+          c.grid_mul = val.first;
+        }
+        if (memcmp(&c, &best, sizeof c) == 0)
+          continue;
+        b->core.cfg = c;
+        drop_graph(b);
+        float ms = 0.0f;
+        rc = time_config(b, reps, &ms);
+        if (rc)
+          return rc;
+        char buf[160];
+        snprintf(buf, sizeof buf, "%s{\"%s\": [%d, %d], \"ms\": %.4f}", first ? "" : ", ", ax.name,
+                 val.first, val.second, ms);
+        log += buf;
+        first = false;
+        if (ms < best_ms * 0.99f) {
+          best = c;
+          best_ms = ms;
+          improved = true;
+        }
       }
-      if (memcmp(&c, &best, sizeof c) == 0)
-        continue;
-      b->core.cfg = c;
-      drop_graph(b);
-      float ms = 0.0f;
-      rc = time_config(b, reps, &ms);
-      if (rc)
-        return rc;
-      char buf[160];
-      snprintf(buf, sizeof buf, "%s{\"%s\": [%d, %d], \"ms\": %.4f}", first ? "" : ", ", ax.name,
-               val.first, val.second, ms);
-      log += buf;
-      first = false;
-      if (ms < best_ms * 0.99f) {
-        best = c;
-        best_ms = ms;
-      }
-    }
+  }
   b->core.cfg = best;
   drop_graph(b);
   char tail[320];
   snprintf(tail, sizeof tail,
-           "], \"best_ms\": %.4f, \"best\": {\"small_side\": %d, \"small_area\": %d, "
+           "], \"passes\": %d, \"best_ms\": %.4f, \"best\": {\"small_side\": %d, \"small_area\": %d, "
            "\"vertex_block\": %d, \"setup_block\": %d, \"raster_block\": %d, "
            "\"large_block\": %d, \"shade_block\": %d, \"grid_mul\": %d}}",
-           best_ms, best.small_side, best.small_area, best.vertex_block, best.setup_block,
+           passes, best_ms, best.small_side, best.small_area, best.vertex_block, best.setup_block,
            best.raster_block, best.large_block, best.shade_block, best.grid_mul);
   log += tail;
   if (report && report_len) {

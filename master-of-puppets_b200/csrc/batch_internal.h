@@ -79,6 +79,7 @@ struct LaunchCore {
   float exposure = 1.0f;
   uint32_t post_effects = 0;
   float lut[256];
+  float fog[6] = {0, 0, 0, 0, 0, 0};
   uint64_t launches = 0;
 
   int init(MopCudaDevice *d);

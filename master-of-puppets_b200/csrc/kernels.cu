@@ -1426,6 +1426,7 @@ template <int SF> struct PostSmem {
   float l[TH][TW];
   float lut[256];
   uint8_t lut8[256];
+  float thr[256]; /* gamma byte thresholds (FOG bit only); thr[255] = +inf */
 };
 
 template <int SF>
@@ -1434,13 +1435,77 @@ __device__ __forceinline__ void post_load_luts(const PostArgs &a, PostSmem<SF> &
   for (int i = tid; i < 256; i += POST_BX * POST_BY) {
     sm.lut[i] = a.lut[i];
     sm.lut8[i] = a.lut8[i];
+    if (a.effects & 8u)
+      sm.thr[i] = i < 255 ? a.gamma_thr[i] : __int_as_float(0x7f800000);
   }
+}
+
+/* The byte of channel value t after the sRGB step, clamp and rounding
+ * (postprocess.c:73-78, 99-112): the number of thresholds at or below t,
+ * found by a binary search of the 255 sorted thresholds (thr[255] = +inf
+ * keeps every probe in range).  NaN compares below every threshold: 0, as
+ * the reference's `c > 0 ? c : 0` gives. */
+__device__ __forceinline__ uint8_t gamma_byte_of(const float *thr, float t) {
+  int n = 0;
+#pragma unroll
+  for (int step = 128; step >= 1; step >>= 1)
+    if (t >= thr[n + step - 1])
+      n += step;
+  return (uint8_t)n;
+}
+
+/* One sample of the post-process with the FOG bit (postprocess.c:43-112):
+ * the byte colour to [0, 1], fog from the sample's depth value, Reinhard,
+ * sRGB, vignette, clamp, rounding — the reference's float operations in its
+ * order.  Without vignette the sRGB step and rounding are the exact threshold
+ * search; with vignette the sRGB value itself is needed and powf is taken as
+ * the double-precision pow rounded to float (glibc's powf, 0.82 ulp, differs
+ * from it by one ulp for 0.06 % of inputs, which moves the byte only when the
+ * product lands within that ulp of a rounding boundary). */
+__device__ __forceinline__ uchar4 post_fog_sample(const PostArgs &a, const float *thr, uchar4 c,
+                                                  float depth, float vg) {
+  const uint32_t fx = a.effects;
+  float factor = 0.0f;
+  if (a.fog_range > 0.0f) {
+    factor = (depth - a.fog_near) / a.fog_range;
+    if (factor < 0.0f)
+      factor = 0.0f;
+    if (factor > 1.0f)
+      factor = 1.0f;
+  }
+  const uint8_t in[3] = {c.x, c.y, c.z};
+  uint8_t o[3];
+#pragma unroll
+  for (int k = 0; k < 3; k++) {
+    float v = (float)in[k] / 255.0f;
+    v = v + (a.fog_color[k] - v) * factor;
+    if (fx & 2u)
+      v = v / (v + 1.0f);
+    if ((fx & 1u) && !(fx & 4u)) {
+      o[k] = gamma_byte_of(thr, v);
+      continue;
+    }
+    if (fx & 1u) {
+      const float x = v > 0.0f ? v : 0.0f;
+      v = x <= 0.0031308f ? x * 12.92f
+                          : 1.055f * (float)pow((double)x, (double)(1.0f / 2.4f)) - 0.055f;
+    }
+    if (fx & 4u)
+      v *= vg;
+    if (v > 1.0f)
+      v = 1.0f;
+    if (v < 0.0f)
+      v = 0.0f;
+    o[k] = u8_of(v * 255.0f + 0.5f);
+  }
+  return make_uchar4(o[0], o[1], o[2], c.w);
 }
 
 template <int SF, int TW>
 __device__ __forceinline__ void post_pixel(const PostArgs &a, const uchar4 (*s_c)[TW],
                                            const float (*s_l)[TW], const float *s_lut,
-                                           const uint8_t *s_lut8, int px, int py);
+                                           const uint8_t *s_lut8, const float *s_thr, int px,
+                                           int py);
 
 /* One tile of POST_BX x POST_BY presented pixels (bx, by): FXAA, the
  * tonemap/gamma map and the SSAA box.  Block-uniform; ends with a barrier so
@@ -1467,14 +1532,15 @@ __device__ __forceinline__ void post_tile(const PostArgs &a, PostSmem<SF> &sm, i
   const int px = bx * POST_BX + (int)threadIdx.x;
   const int py = by * POST_BY + (int)threadIdx.y;
   if (px < pw && py < ph)
-    post_pixel<SF, TW>(a, s_c, s_l, s_lut, s_lut8, px, py);
+    post_pixel<SF, TW>(a, s_c, s_l, s_lut, s_lut8, sm.thr, px, py);
   __syncthreads();
 }
 
 template <int SF, int TW>
 __device__ __forceinline__ void post_pixel(const PostArgs &a, const uchar4 (*s_c)[TW],
                                            const float (*s_l)[TW], const float *s_lut,
-                                           const uint8_t *s_lut8, int px, int py) {
+                                           const uint8_t *s_lut8, const float *s_thr, int px,
+                                           int py) {
   const int w = a.width, h = a.height, pw = w / SF;
   const bool fx = (a.effects & 16u) && w >= 3 && h >= 3;
   uint32_t acc[4] = {0, 0, 0, 0};
@@ -1487,7 +1553,19 @@ __device__ __forceinline__ void post_pixel(const PostArgs &a, const uchar4 (*s_c
       uchar4 c = s_c[ti][tj];
       if (fx && x >= 1 && y >= 1 && x < w - 1 && y < h - 1)
         c = fxaa_tile<TW>(s_c, s_l, ti, tj);
-      if (a.effects != 0u && !(a.effects & 4u)) {
+      if (a.effects & 8u) {
+        float vg = 1.0f;
+        if (a.effects & 4u) {
+          const float cx = (float)w * 0.5f, cy = (float)h * 0.5f;
+          const float maxd = sqrtf(cx * cx + cy * cy);
+          const float ddx = (float)x - cx, ddy = (float)y - cy;
+          const float dist = sqrtf(ddx * ddx + ddy * ddy) / maxd;
+          vg = 1.0f - dist * dist * 0.5f;
+          if (vg < 0.0f)
+            vg = 0.0f;
+        }
+        c = post_fog_sample(a, s_thr, c, a.depth[(size_t)y * w + x], vg);
+      } else if (a.effects != 0u && !(a.effects & 4u)) {
         /* without vignette the post-process is a fixed byte map */
         c.x = s_lut8[c.x];
         c.y = s_lut8[c.y];
@@ -1867,7 +1945,7 @@ __global__ void __launch_bounds__(256) k_oraster(FrameArgs a) {
           zz = b0 * r.zc[0] + b1 * r.zc[1] + b2 * r.zc[2];
         }
         const uint32_t px = rowbase + (uint32_t)x;
-        if (zz < a.depth[px])
+        if (a.ordered_keep_all || zz < a.depth[px])
           push_fragment(a, px, r.order);
       }
       w0 = __fadd_rn(w0, r.dx[0]);
@@ -1930,17 +2008,32 @@ __global__ void __launch_bounds__(128) k_ofold(FrameArgs a) {
     }
     float depth = a.depth[px];
     uint32_t id = a.ids[px];
+    /* a depth-write-off draw's depth is undone when the draw ends: `saved`
+     * holds the depth from before it, `cur` the draw of the last fragment */
+    float saved = depth;
+    uint32_t cur = 0xffffffffu;
+    bool cur_nw = false;
     for (uint32_t k = 0; k < cnt; k++) {
       const uint32_t rid = record_of(a, ord[k]);
       if (rid >= a.rec_cap)
         continue;
       const RasterRec r = a.rrec[rid];
       const ShadeRec s = a.srec[rid];
-      const DrawRec &d = a.draws[s.draw < a.draw_count ? s.draw : 0];
+      const uint32_t di = s.draw < a.draw_count ? s.draw : 0;
+      const DrawRec &d = a.draws[di];
+      if (di != cur) {
+        if (cur_nw)
+          depth = saved; /* cpu_backend.c:575-580 */
+        cur = di;
+        cur_nw = (d.flags & DF_NO_DEPTH_WRITE) != 0;
+        if (cur_nw)
+          saved = depth; /* cpu_backend.c:536-544 */
+      }
+      const bool dtest = !(d.flags & DF_NO_DEPTH_TEST);
       const int jr = y - (int)r.y0, kc = x - (int)r.x0;
       if (r.y1 & REC_FLAT_BIT) { /* rasterize_filled_triangle, rasterizer.c:1000-1083 */
         const float z = fold_add(fold_add(r.zc[0], r.zc[2], jr), r.zc[1], kc);
-        if (z < depth) {
+        if (!dtest || z < depth) {
           const float ca = d.opacity < 0.0f ? 0.0f : (d.opacity > 1.0f ? 1.0f : d.opacity);
           if (d.blend_mode == 0 && ca >= 1.0f) {
             hdr[0] = s.col[0];
@@ -1967,7 +2060,7 @@ __global__ void __launch_bounds__(128) k_ofold(FrameArgs a) {
         w[e] = fold_add(fold_add(r.w0[e], r.dy[e], jr), r.dx[e], kc);
       const float b0 = w[0] * r.inv_area, b1 = w[1] * r.inv_area, b2 = w[2] * r.inv_area;
       const float z = b0 * r.zc[0] + b1 * r.zc[1] + b2 * r.zc[2];
-      if (!(z < depth))
+      if (dtest && !(z < depth))
         continue;
       if (s.v[0] >= a.vertex_cap || s.v[1] >= a.vertex_cap || s.v[2] >= a.vertex_cap)
         continue;
@@ -2024,6 +2117,8 @@ __global__ void __launch_bounds__(128) k_ofold(FrameArgs a) {
         }
       }
     }
+    if (cur_nw)
+      depth = saved;
     /* mop_sw_hdr_resolve (rasterizer.c:2776-2803) of the composited sample */
     if (id == 0u)
       a.pre[px] = make_uchar4(x86_f2u8(fminf(hdr[0], 1.0f) * 255.0f + 0.5f),

@@ -95,7 +95,8 @@ extern "C" MopCudaDevice *mopcuda_device_create(int ordinal) {
   d->cfg.num_sms = d->num_sms;
   if (cudaStreamCreateWithFlags(&d->stream, cudaStreamNonBlocking) != cudaSuccess ||
       cudaStreamCreateWithFlags(&d->copy_stream, cudaStreamNonBlocking) != cudaSuccess ||
-      cudaEventCreate(&d->ev0) != cudaSuccess || cudaEventCreate(&d->ev1) != cudaSuccess) {
+      cudaEventCreate(&d->ev0) != cudaSuccess || cudaEventCreate(&d->ev1) != cudaSuccess ||
+      cudaEventCreateWithFlags(&d->pick_ev, cudaEventDisableTiming) != cudaSuccess) {
     cudaGetLastError();
     fail(MOPCUDA_ECUDA, "stream/event creation failed");
     delete d;
@@ -180,6 +181,8 @@ extern "C" void mopcuda_device_destroy(MopCudaDevice *d) {
   d->h_deform.release();
   cudaEventDestroy(d->ev0);
   cudaEventDestroy(d->ev1);
+  if (d->pick_ev)
+    cudaEventDestroy(d->pick_ev);
   for (int i = 0; i <= MOPCUDA_STAGES; i++)
     if (d->stage_ev[i])
       cudaEventDestroy(d->stage_ev[i]);
@@ -440,6 +443,16 @@ extern "C" void mopcuda_set_post_effects(MopCudaDevice *d, uint32_t fx) {
   build_lut(d->lut, fx);
 }
 
+extern "C" int mopcuda_set_fog(MopCudaDevice *d, const float color[4], float near_dist,
+                               float far_dist) {
+  if (!d || !color)
+    return fail(MOPCUDA_EINVAL, "set_fog: %s", !d ? "no device" : "no colour");
+  memcpy(d->fog, color, 4 * sizeof(float));
+  d->fog[4] = near_dist;
+  d->fog[5] = far_dist;
+  return MOPCUDA_OK;
+}
+
 extern "C" int mopcuda_set_ibl(MopCudaDevice *d, const float *irr, int iw, int ih, const float *pf,
                                int pw, int ph, int levels, const float *brdf, int bs, float rot,
                                float intensity) {
@@ -596,11 +609,12 @@ extern "C" int mopcuda_frame_begin(MopCudaDevice *d, MopCudaFramebuffer *fb, con
 static float clamp01f(float x) { return x < 0.0f ? 0.0f : (x > 1.0f ? 1.0f : x); }
 
 /* Records one draw.  Opaque lit and opaque flat draws are order-independent;
- * blended draws (smooth or flat) and unlit smooth draws (the legacy path
- * with silhouette edge AA) depend on submission order and start the frame's
- * ordered suffix; zero-opacity draws are colour no-ops in the reference and
- * are dropped; wireframe, depth-test-off and depth-write-off draws are
- * reported as unsupported. */
+ * blended draws (smooth or flat), unlit smooth draws (the legacy path with
+ * silhouette edge AA) and draws with the depth test or the depth write off
+ * (the core's instanced pass and editor chrome) depend on submission order
+ * and start the frame's ordered suffix; zero-opacity draws are colour no-ops
+ * in the reference and are dropped; wireframe draws are reported as
+ * unsupported. */
 int mc_build_draw(const MopCudaDraw *c, const float *model, const float *mvp,
                   std::vector<LightRec> &lights, DrawRec &r, bool &skip) {
   skip = false;
@@ -612,10 +626,8 @@ int mc_build_draw(const MopCudaDraw *c, const float *model, const float *mvp,
     return MOPCUDA_OK;
   }
   bool lit = c->lights && c->light_count > 0;
-  if (c->wireframe || !c->depth_test || !c->depth_write) {
-    return fail(MOPCUDA_EUNSUPPORTED,
-                "draw: wireframe / depth-test-off / depth-write-off state is not implemented");
-  }
+  if (c->wireframe)
+    return fail(MOPCUDA_EUNSUPPORTED, "draw: wireframe (line) rendering is not implemented");
   uint32_t stride = 48;
   memset(&r, 0, sizeof r);
   if (c->layout) {
@@ -684,6 +696,10 @@ int mc_build_draw(const MopCudaDraw *c, const float *model, const float *mvp,
     r.flags |= DF_SMOOTH;
   if (c->backface_cull)
     r.flags |= DF_CULL;
+  if (!c->depth_test)
+    r.flags |= DF_NO_DEPTH_TEST;
+  else if (!c->depth_write)
+    r.flags |= DF_NO_DEPTH_WRITE;
   if (lit) {
     r.flags |= DF_LIT;
     /* the draw's active lights (inactive ones contribute nothing: the
@@ -745,9 +761,11 @@ static int record_draw(MopCudaDevice *d, const MopCudaDraw *c, const float *mode
     d->rec_skipped++;
     return MOPCUDA_OK;
   }
-  /* the first blended or unlit smooth draw starts the ordered suffix */
+  /* the first blended, unlit smooth, depth-write-off or depth-test-off draw
+   * starts the ordered suffix */
   const bool legacy = (r.flags & DF_SMOOTH) && !(r.flags & DF_LIT);
-  if ((r.blend_mode != 0 || clamp01f(r.opacity) < 1.0f || legacy) &&
+  if ((r.blend_mode != 0 || clamp01f(r.opacity) < 1.0f || legacy ||
+       (r.flags & (DF_NO_DEPTH_WRITE | DF_NO_DEPTH_TEST))) &&
       d->rec_ordered_from == UINT32_MAX)
     d->rec_ordered_from = (uint32_t)d->rec_draws.size();
   d->rec_draws.push_back(r);
@@ -839,13 +857,57 @@ void mc_ibl_consts(bool on, int pf_w, int pf_h, int pf_levels, int brdf_size, Dr
   }
 }
 
-void mc_post_args(const MopCudaDevice *d, PostArgs &p) {
+/* The byte the reference writes for a channel value t that reaches the
+ * gamma step (postprocess.c:73-78, then the clamp and rounding of :99-112),
+ * with this process's powf. */
+static int gamma_byte(float t) {
+  volatile float x = t > 0.0f ? t : 0.0f;
+  volatile float c = x <= 0.0031308f ? x * 12.92f : 1.055f * powf(x, 1.0f / 2.4f) - 0.055f;
+  float v = c;
+  if (v > 1.0f)
+    v = 1.0f;
+  if (v < 0.0f)
+    v = 0.0f;
+  volatile float q = v * 255.0f + 0.5f;
+  return (int)q;
+}
+
+/* Thresholds of gamma_byte: thr[k] is the smallest positive float whose byte
+ * is at least k + 1.  gamma_byte is non-decreasing in t (checked over every
+ * positive float up to 2.0 with glibc 2.39's powf: 255 steps, none down; all
+ * larger values and +inf give 255, NaN and t <= 0 give 0), so a value's byte
+ * is the number of thresholds at or below it, and a search of this table
+ * on the device returns powf's byte without evaluating powf there. */
+static void build_gamma_thresholds(float thr[255]) {
+  for (int k = 1; k <= 255; k++) {
+    uint32_t lo = 1u, hi = 0x7f800000u; /* smallest subnormal .. +inf */
+    while (lo < hi) {
+      const uint32_t mid = lo + (hi - lo) / 2u;
+      float t;
+      memcpy(&t, &mid, 4);
+      if (gamma_byte(t) >= k)
+        hi = mid;
+      else
+        lo = mid + 1u;
+    }
+    memcpy(&thr[k - 1], &lo, 4);
+  }
+}
+
+static const float *gamma_thresholds() {
+  static float thr[255];
+  static std::once_flag once;
+  std::call_once(once, [] { build_gamma_thresholds(thr); });
+  return thr;
+}
+
+void mc_post_template(uint32_t fx, const float lut[256], const float fog[6], PostArgs &p) {
   memset(&p, 0, sizeof p);
-  p.effects = d->post & (MOPCUDA_POST_GAMMA | MOPCUDA_POST_TONEMAP | MOPCUDA_POST_VIGNETTE |
-                         MOPCUDA_POST_FXAA);
-  memcpy(p.lut, d->lut, sizeof p.lut);
+  p.effects = fx & (MOPCUDA_POST_GAMMA | MOPCUDA_POST_TONEMAP | MOPCUDA_POST_VIGNETTE |
+                    MOPCUDA_POST_FOG | MOPCUDA_POST_FXAA);
+  memcpy(p.lut, lut, sizeof p.lut);
   for (int i = 0; i < 256; i++) {
-    float v = d->lut[i];
+    float v = lut[i];
     if (v > 1.0f)
       v = 1.0f;
     if (v < 0.0f)
@@ -853,7 +915,18 @@ void mc_post_args(const MopCudaDevice *d, PostArgs &p) {
     volatile float q = v * 255.0f + 0.5f; /* postprocess.c:110-112 */
     p.lut8[i] = (uint8_t)(int)q;
   }
+  if (fx & MOPCUDA_POST_FOG) {
+    p.fog_color[0] = fog[0];
+    p.fog_color[1] = fog[1];
+    p.fog_color[2] = fog[2];
+    p.fog_near = fog[4];
+    volatile float range = fog[5] - fog[4]; /* postprocess.c:53 */
+    p.fog_range = range;
+    memcpy(p.gamma_thr, gamma_thresholds(), sizeof p.gamma_thr);
+  }
 }
+
+void mc_post_args(const MopCudaDevice *d, PostArgs &p) { mc_post_template(d->post, d->lut, d->fog, p); }
 
 /* Runs between a launch's shading and its post pass: issues the previous
  * frame's deferred readback, then names the readback the post pass must wait
@@ -997,6 +1070,9 @@ static int launch_frame(MopCudaDevice *d) {
     a.olist = d->olist.as<uint32_t>();
     a.olist_items = d->olist_items.as<uint32_t>();
     a.olist_cap = ocap;
+    for (uint32_t i = d->ordered_from; i < nd; i++)
+      if (d->draws[i].flags & DF_NO_DEPTH_TEST)
+        a.ordered_keep_all = 1;
   }
 
   if (d->fr_sh >= 0) { /* the map bound at this frame's frame_end */
@@ -1014,6 +1090,7 @@ static int launch_frame(MopCudaDevice *d) {
                ? fb->ssaa
                : 1;
   p.presented = sf > 1 ? fb->presented.as<uchar4>() : nullptr;
+  p.depth = fb->depth.as<float>();
   p.width = fb->w;
   p.height = fb->h;
   p.ssaa = sf;
@@ -1059,7 +1136,10 @@ static int finish_frame(MopCudaDevice *d, int timeout_ms, bool defer_readback) {
   for (int attempt = 0; d->pending; attempt++) {
     int rc = mc_bounded_sync(d, d->ev1, timeout_ms);
     if (rc) {
-      d->pending = false;
+      /* a wait that ran out leaves the frame pending (a later wait resumes
+       * it); a device error loses it */
+      if (rc != MOPCUDA_ETIMEOUT)
+        d->pending = false;
       return rc;
     }
     d->pending = false;
@@ -1632,11 +1712,18 @@ extern "C" int mopcuda_measure_fp32_peak(MopCudaDevice *d, double *gops) {
  *
  * Set-up: the first call on a device (with that device current) resolves
  * the array's device address with cudaGetSymbolAddress — the host-side name
- * is only a stand-in, not a device address — and creates one event for the
- * bounded wait.  Make that first call before any stream capture.
+ * is only a stand-in, not a device address.  Make that first call before
+ * any stream capture.  The bounded wait uses an event the device made at
+ * mopcuda_device_create (one per MopCudaDevice, so two devices on one GPU
+ * never read each other's completion).
  * All calls share the array and it keeps the last call's contents (every
  * slot a call reads is written by that call first); calls whose work
  * overlaps on the GPU race on it, so callers must not overlap them.
+ * The results are copied straight into the caller's buffers: the wait is
+ * bounded only when they are page-locked (a copy into pageable memory holds
+ * the host until the pick kernel ends), and after MOPCUDA_ETIMEOUT the
+ * copies stay queued, so xy and the outputs remain in use until the device
+ * is synchronised or destroyed.
  * ------------------------------------------------------------------------ */
 #define NOALLOC_PICK_BYTES_PER_QUERY 20u /* int2 in, uint32 + float + int32 out */
 static __device__ __align__(256) unsigned char
@@ -1645,28 +1732,22 @@ static __device__ __align__(256) unsigned char
 #define NOALLOC_MAX_DEVICES 64
 static std::mutex g_noalloc_mu;
 static void *g_noalloc_ptr[NOALLOC_MAX_DEVICES];
-static cudaEvent_t g_noalloc_ev[NOALLOC_MAX_DEVICES];
 
-static int noalloc_setup(int ordinal, unsigned char **scratch, cudaEvent_t *ev) {
+static int noalloc_setup(int ordinal, unsigned char **scratch) {
   if (ordinal < 0 || ordinal >= NOALLOC_MAX_DEVICES)
     return fail(MOPCUDA_EINVAL, "pick_batch_noalloc: device ordinal %d unsupported", ordinal);
   std::lock_guard<std::mutex> lk(g_noalloc_mu);
   if (!g_noalloc_ptr[ordinal]) {
     void *p = nullptr;
     cudaError_t e = cudaGetSymbolAddress(&p, g_pick_scratch);
-    if (e != cudaSuccess || !p)
+    if (e != cudaSuccess || !p) {
+      cudaGetLastError(); /* leave no stale error for a later launch check */
       return fail(MOPCUDA_ECUDA, "pick_batch_noalloc: cudaGetSymbolAddress failed: %s",
                   cudaGetErrorString(e));
-    cudaEvent_t ev_new;
-    e = cudaEventCreateWithFlags(&ev_new, cudaEventDisableTiming);
-    if (e != cudaSuccess)
-      return fail(MOPCUDA_ECUDA, "pick_batch_noalloc: event creation failed: %s",
-                  cudaGetErrorString(e));
-    g_noalloc_ev[ordinal] = ev_new;
+    }
     g_noalloc_ptr[ordinal] = p;
   }
   *scratch = (unsigned char *)g_noalloc_ptr[ordinal];
-  *ev = g_noalloc_ev[ordinal];
   return MOPCUDA_OK;
 }
 
@@ -1686,10 +1767,10 @@ extern "C" int mopcuda_pick_batch_noalloc(MopCudaDevice *d, MopCudaFramebuffer *
                                 "mopcuda_frame_wait first (completion may reallocate)");
   CU_TRY(cudaSetDevice(d->ordinal));
   unsigned char *scratch = nullptr;
-  cudaEvent_t ev = nullptr;
-  int rc = noalloc_setup(d->ordinal, &scratch, &ev);
+  int rc = noalloc_setup(d->ordinal, &scratch);
   if (rc)
     return rc;
+  cudaEvent_t ev = d->pick_ev;
   int2 *dxy = (int2 *)scratch;
   uint32_t *oid = (uint32_t *)(scratch + 8ull * MOPCUDA_NOALLOC_PICK_MAX);
   float *odp = (float *)(oid + MOPCUDA_NOALLOC_PICK_MAX);

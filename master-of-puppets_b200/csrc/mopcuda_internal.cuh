@@ -27,6 +27,14 @@ enum DrawFlags : uint32_t {
   DF_LIT = 1u << 2,     /* light list present: _full entry (rasterizer.c:2458) */
   DF_TEXTURED = 1u << 3,
   DF_FLEX = 1u << 4,    /* flexible vertex layout                              */
+  /* depth_test && !depth_write: the CPU backend saves the depth buffer before
+   * the draw and restores it after (cpu_backend.c:536-544, 575-580), so the
+   * draw's fragments test against the depth before it and each other, and
+   * its colour and IDs stay while its depth does not */
+  DF_NO_DEPTH_WRITE = 1u << 5,
+  /* !depth_test: every covered fragment passes (rasterizer.c:1948) and
+   * writes depth */
+  DF_NO_DEPTH_TEST = 1u << 6,
 };
 
 /* One recorded draw, uploaded per frame (the MopRhiDrawCall fields the path
@@ -191,6 +199,10 @@ struct FrameArgs {
   uint32_t *olist;        /* live records of the suffix                          */
   uint32_t *olist_items;  /* their (row, chunk) item counts, then offsets        */
   uint32_t olist_cap;
+  /* the suffix holds a depth-test-off draw: its fragments pass whatever the
+   * depth, and later ones may pass where the opaque depth is nearer, so
+   * every covered fragment of the suffix is kept */
+  int ordered_keep_all;
   /* shadow map bound for directional lights (the rasteriser's shadow state,
    * rasterizer.c:141-157): shadow_w x shadow_h texel keys (shadow_texel),
    * null when none is bound; shadow_vp: the light's view-projection, 16
@@ -262,6 +274,14 @@ struct PostArgs {
   uint32_t effects;
   float lut[256];     /* per-byte value after tonemap/gamma */
   uint8_t lut8[256];  /* the whole per-channel map when vignette is off */
+  /* fog (FOG bit): each sample's depth value moves its colour towards
+   * fog_color by clamp((depth - fog_near) / fog_range, 0, 1) */
+  const float *depth;
+  float fog_color[3];
+  float fog_near, fog_range;
+  /* gamma_thr[k]: the smallest float whose sRGB value rounds to byte k + 1
+   * (host glibc powf); the byte of any value is the count of entries <= it */
+  float gamma_thr[255];
 };
 
 /* ------------------------------------------------------------------------

@@ -129,6 +129,7 @@ SIGNATURES = [
     ("mopcuda_framebuffer_set_ssaa", C.c_int, [_P, C.c_int]),
     ("mopcuda_set_exposure", None, [_P, C.c_float]),
     ("mopcuda_set_post_effects", None, [_P, C.c_uint32]),
+    ("mopcuda_set_fog", C.c_int, [_P, C.POINTER(C.c_float), C.c_float, C.c_float]),
     ("mopcuda_set_ibl", C.c_int, [_P, _P, C.c_int, C.c_int, _P, C.c_int, C.c_int, C.c_int, _P,
                                   C.c_int, C.c_float, C.c_float]),
     ("mopcuda_skin_apply", C.c_int, [_P, _P, _P, C.c_uint32, C.POINTER(MopCudaDeformLayout),
@@ -398,6 +399,18 @@ class _Resident:
                 vc, ic = v.shape[0], i.size
             self._buffers += [vb, ib]
             self.meshes.append((m, vb, ib, vc, ic))
+        # instanced meshes (mop_viewport_add_instanced_mesh): buffers + transforms
+        self.instanced = []
+        for im in getattr(scene, "instanced", []):
+            v = _f32(im.vertices)
+            i = np.ascontiguousarray(im.indices, np.uint32)
+            vb = L.mopcuda_buffer_create(d, v.ctypes.data, v.nbytes)
+            ib = L.mopcuda_buffer_create(d, i.ctypes.data, i.nbytes)
+            if not vb or not ib:
+                raise RuntimeError(f"buffer_create failed: {last_error()}")
+            self._buffers += [vb, ib]
+            tr = np.ascontiguousarray(np.asarray(im.transforms, np.float32).reshape(-1, 16))
+            self.instanced.append((im, vb, ib, v.shape[0], i.size, tr))
         self.textures = []
         for t in scene.textures:
             t = np.ascontiguousarray(t, np.uint8)
@@ -407,6 +420,11 @@ class _Resident:
             self.textures.append(th)
         L.mopcuda_set_exposure(d, scene.exposure)
         L.mopcuda_set_post_effects(d, scene.post_effects)
+        # mop_viewport_set_fog; a scene without fog keeps a new viewport's zeros
+        fog = getattr(scene, "fog", None)
+        fc, fnear, ffar = (fog[0], fog[1], fog[2]) if fog is not None else ((0, 0, 0, 0), 0, 0)
+        _check(L.mopcuda_set_fog(d, (C.c_float * 4)(*[float(x) for x in fc]), float(fnear),
+                                 float(ffar)), "set_fog")
         if ibl is not None:
             self.set_ibl(ibl)
         else:
@@ -450,6 +468,41 @@ class _Resident:
         dr.depth_test = dr.depth_write = dr.backface_cull = 1
         dr.blend_mode = getattr(m, "blend_mode", 0) or (1 if m.opacity < 1.0 else 0)
         dr.texture = self.textures[m.texture] if m.texture >= 0 else None
+        dr.lights = self.lights
+        dr.light_count = len(sc.lights)
+        dr.layout = None
+        if m.object_id >= 0xFFFD0000:  # chrome (EMIT_DRAW, reference viewport.c:2035-2076)
+            dr.depth_test = dr.backface_cull = 0
+            dr.lights, dr.light_count = None, 0
+            dr.ambient = 1.0
+        return dr
+
+    def instanced_struct(self, k) -> MopCudaDraw:
+        """pass_instanced's draw call for instanced mesh k (reference
+        viewport.c:2613-2641): identity model and mvp (replaced per instance),
+        the default material, no texture, culling only for a non-zero ID,
+        depth test with the depth write off, cam_eye left at zero."""
+        sc = self.scene
+        im, vb, ib, vc, ic, _ = self.instanced[k]
+        dr = MopCudaDraw()
+        dr.vertex_buffer, dr.index_buffer = vb, ib
+        dr.vertex_count, dr.index_count = vc, ic
+        dr.object_id = im.object_id
+        ident = [1.0, 0, 0, 0, 0, 1.0, 0, 0, 0, 0, 1.0, 0, 0, 0, 0, 1.0]
+        dr.model[:] = ident
+        dr.mvp[:] = ident
+        dr.cam_eye[:] = [0.0, 0.0, 0.0]
+        dr.light_dir[:] = DEFAULT_LIGHT_DIR
+        dr.ambient = min(max(sc.ambient, 0.0), 1.0)
+        dr.opacity = 1.0
+        dr.metallic, dr.roughness = 0.0, 0.5
+        dr.depth_bias = 0.0
+        dr.smooth = 1 if getattr(sc, "smooth", True) else 0
+        dr.wireframe = 0
+        dr.depth_test, dr.depth_write = 1, 0
+        dr.backface_cull = 1 if im.object_id != 0 else 0
+        dr.blend_mode = 0
+        dr.texture = None
         dr.lights = self.lights
         dr.light_count = len(sc.lights)
         dr.layout = None
@@ -502,6 +555,9 @@ class SceneRenderer(_Resident):
         self.draws = [self.draw_struct(k, self.view, self.proj, self.eye)
                       for k in scenes.draw_order(self.scene, self.eye)]
         self.draw_array = (MopCudaDraw * max(1, len(self.draws)))(*self.draws)
+        self.inst_draws = [self.instanced_struct(k) for k in range(len(self.instanced))]
+        self._view_arr = _f32(self.view)
+        self._proj_arr = _f32(self.proj)
 
     def shadow_pass(self) -> bool:
         """pass_shadow through the C ABI (reference viewport.c:2288-2442):
@@ -558,6 +614,11 @@ class SceneRenderer(_Resident):
         self.shadow_pass()
         _check(L.mopcuda_frame_begin(d, fb, self.clear), "frame_begin")
         _check(L.mopcuda_draw_list(d, fb, self.draw_array, len(self.draws)), "draw_list")
+        # pass_instanced after the transparent pass: one draw per instance
+        for dr, (_, _, _, _, _, tr) in zip(self.inst_draws, self.instanced):
+            _check(L.mopcuda_draw_instanced(d, fb, C.byref(dr), self._view_arr.ctypes.data,
+                                            self._proj_arr.ctypes.data, tr.ctypes.data,
+                                            tr.shape[0]), "draw_instanced")
         _check(L.mopcuda_frame_end(d, fb), "frame_end")
 
     def wait(self, timeout_ms: int = 20000):

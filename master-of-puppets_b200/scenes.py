@@ -52,6 +52,23 @@ class Mesh:
 
 
 @dataclasses.dataclass
+class InstancedMesh:
+    """mop_viewport_add_instanced_mesh (reference viewport.c:3774-3858): one
+    mesh drawn once per transform, all with one object ID, the default
+    material (metallic 0, roughness 0.5), no texture, opaque; the core draws
+    it in pass_instanced, after the transparent pass (viewport.c:3238-3240),
+    with mvp = P * (V * instance) (cpu_backend.c:638-657)."""
+    vertices: np.ndarray          # float32 [V, 12]
+    indices: np.ndarray           # uint32 [I]
+    object_id: int
+    transforms: np.ndarray        # float32 [N, 16], column-major
+
+    @property
+    def triangle_count(self) -> int:
+        return int(self.indices.size // 3) * int(self.transforms.shape[0])
+
+
+@dataclasses.dataclass
 class Light:
     type: int
     position: Tuple[float, float, float] = (0.0, 0.0, 0.0)
@@ -93,6 +110,7 @@ class Scene:
     smooth: bool = True           # MOP_SHADING_SMOOTH (viewport default)
     # MopFogParams ((r, g, b, a), near, far) for the MOP_POST_FOG bit; None: not set
     fog: Optional[Tuple[Tuple[float, float, float, float], float, float]] = None
+    instanced: List[InstancedMesh] = dataclasses.field(default_factory=list)
 
     @property
     def samples(self) -> int:
@@ -104,7 +122,8 @@ class Scene:
 
     @property
     def triangle_count(self) -> int:
-        return sum(m.triangle_count for m in self.meshes)
+        return (sum(m.triangle_count for m in self.meshes)
+                + sum(im.triangle_count for im in self.instanced))
 
 
 # --------------------------------------------------------------------------
@@ -611,9 +630,12 @@ def draw_order(scene: Scene, eye) -> List[int]:
     """Mesh indices in the core's draw order (viewport.c:2449-2553): opaque
     meshes in scene order, then blended meshes back to front by the float32
     squared distance of their translation to the eye (the core's insertion
-    sort: farthest first, ties keep scene order)."""
-    opaque = [k for k, m in enumerate(scene.meshes) if effective_blend(m) == BLEND_OPAQUE]
-    trans = [k for k, m in enumerate(scene.meshes) if effective_blend(m) != BLEND_OPAQUE]
+    sort: farthest first, ties keep scene order); IDs in the hidden range are
+    not drawn."""
+    shown = [k for k, m in enumerate(scene.meshes)
+             if m.object_id < HIDDEN_ID_FLOOR and m.object_id != GRID_ID]
+    opaque = [k for k in shown if effective_blend(scene.meshes[k]) == BLEND_OPAQUE]
+    trans = [k for k in shown if effective_blend(scene.meshes[k]) != BLEND_OPAQUE]
     e = np.asarray(eye, np.float32)
     dist = []
     for k in trans:
@@ -653,8 +675,80 @@ def transparent_scene(seed: int = 12, width: int = 160, height: int = 120, ssaa:
     return sc
 
 
+def instanced_scene(seed: int = 70, width: int = 192, height: int = 144, ssaa: int = 1,
+                    n_instances: int = 96, transparent: bool = False, env: int = 0,
+                    zero_id: bool = False) -> Scene:
+    """small_scene (or transparent_scene) plus an instanced icosphere: n_instances
+    copies with one object ID scattered through the opaque meshes, so instances
+    overlap each other and the scene.  The core draws them after the transparent
+    pass with the depth write off (each instance's depth is undone after it), so
+    a later instance behind an earlier one, but in front of the scene, replaces
+    its colour and ID.  zero_id adds 64 instanced tori with object ID 0 (back
+    faces not culled, resolved as background)."""
+    if transparent:
+        sc = transparent_scene(seed=seed, width=width, height=height, ssaa=ssaa, env=env)
+    else:
+        sc = small_scene(seed=seed, width=width, height=height, ssaa=ssaa, env=env)
+    sc.name = f"instanced{seed}"
+    rng = np.random.default_rng(seed + 300)
+
+    def scatter(n, smin, smax):
+        out = np.zeros((n, 16), np.float32)
+        for k in range(n):
+            t = rng.uniform(-2.8, 2.8, 3)
+            t[1] = float(rng.uniform(0.1, 1.8))
+            s = float(rng.uniform(smin, smax))
+            out[k] = mat_trs(t, random_rotation(rng), (s, s, s))
+        return out
+
+    v, i = icosphere(1, 0.3, _color(rng))
+    sc.instanced.append(InstancedMesh(v, i, 100, scatter(n_instances, 0.5, 1.3)))
+    if zero_id:
+        v, i = torus(16, 8, 0.35, 0.12, _color(rng))
+        sc.instanced.append(InstancedMesh(v, i, 0, scatter(64, 0.6, 1.4)))
+    return sc
+
+
 SHADOW_MAP_SIZE = 1024          # MOP_SHADOW_MAP_SIZE, reference viewport.c:2286
 CHROME_ID_FLOOR = 0xFFFD0000    # object IDs at or above it are editor chrome
+HIDDEN_ID_FLOOR = 0xFFFE0000    # object IDs at or above it are not drawn by the scene passes
+GRID_ID = 0xFFFD0001            # MOP_GRID_ID: drawn only by the chrome grid pass (viewport.c:122)
+
+
+def is_chrome(object_id: int) -> bool:
+    """EMIT_DRAW's chrome test (reference viewport.c:2035-2076): a chrome draw
+    has the depth test and back-face culling off, no light list (the legacy
+    single-light path) and ambient 1."""
+    return object_id >= CHROME_ID_FLOOR
+
+
+def chrome_scene(seed: int = 80, width: int = 192, height: int = 144, ssaa: int = 1) -> Scene:
+    """small_scene with three meshes in the editor-chrome ID range among its
+    opaque meshes: they draw over what came before them (depth test off) and
+    write depth that later meshes test against; one mesh in the hidden range
+    and one with the grid's ID are skipped by the scene passes."""
+    sc = small_scene(seed=seed, width=width, height=height, ssaa=ssaa, n_meshes=7)
+    sc.name = f"chrome{seed}"
+    rng = np.random.default_rng(seed + 500)
+    chrome = []
+    for k in range(3):
+        v, i = icosphere(2, float(rng.uniform(0.4, 0.7)), _color(rng)) if k != 1 else \
+            torus(24, 12, 0.8, 0.2, _color(rng))
+        t = rng.uniform(-1.5, 1.5, 3)
+        t[1] = float(rng.uniform(0.4, 1.4))
+        chrome.append(Mesh(v, i, CHROME_ID_FLOOR + 16 + k, mat_trs(t, random_rotation(rng),
+                                                                   (1.0, 1.0, 1.0))))
+    v, i = icosphere(1, 2.0, _color(rng))
+    hidden = Mesh(v, i, HIDDEN_ID_FLOOR + 5, mat_identity())
+    # chrome meshes among the opaque ones and last; the hidden one after the first, the
+    # grid-ID one after the first chrome mesh
+    sc.meshes.insert(1, hidden)
+    v, i = icosphere(1, 1.5, _color(rng))
+    sc.meshes.insert(3, Mesh(v, i, GRID_ID, mat_identity()))
+    sc.meshes.insert(2, chrome[0])
+    sc.meshes.insert(5, chrome[1])
+    sc.meshes.append(chrome[2])
+    return sc
 
 
 def shadow_light(scene: Scene):

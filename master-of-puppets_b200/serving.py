@@ -233,14 +233,18 @@ class PlainScene:
         self.mvp[:] = _mat_mul_rows(p, _mat_mul_rows(v, np.ascontiguousarray(self.model)))
         self.eye[:] = e
 
-    def frame(self, dev, fb, view):
+    def submit(self, dev, fb, view):
+        """Records and launches the frame (asynchronous)."""
         L, d = dev.L, dev.h
         clear = (C.c_float * 4)(*view.clear)
         mopcuda._check(L.mopcuda_frame_begin(d, fb, clear), "frame_begin")
         mopcuda._check(L.mopcuda_draw_list(d, fb, C.addressof(self.arr), len(self.arr)),
                        "draw_list")
         mopcuda._check(L.mopcuda_frame_end(d, fb), "frame_end")
-        mopcuda._check(L.mopcuda_frame_wait(d, 20000), "frame_wait")
+
+    def frame(self, dev, fb, view):
+        self.submit(dev, fb, view)
+        mopcuda._check(dev.L.mopcuda_frame_wait(dev.h, 20000), "frame_wait")
 
 
 def check_kept(dev, rss, trace: List[Request], kept: dict) -> dict:

@@ -38,7 +38,8 @@ class OrDraw(C.Structure):
                 ("smooth", C.c_int32), ("depth_test", C.c_int32),
                 ("backface_cull", C.c_int32), ("blend_mode", C.c_int32),
                 ("lights", C.POINTER(OrLight)), ("light_count", C.c_uint32),
-                ("texture", C.c_void_p), ("tex_w", C.c_int32), ("tex_h", C.c_int32)]
+                ("texture", C.c_void_p), ("tex_w", C.c_int32), ("tex_h", C.c_int32),
+                ("depth_write", C.c_int32)]
 
 
 class OrIBL(C.Structure):
@@ -207,9 +208,13 @@ def render(scene, ibl=None, want_hdr=False):
     for k, l in enumerate(scene.lights):
         lights[k] = _light(l)
     texs = [np.ascontiguousarray(t, np.uint8) for t in scene.textures]
-    draws = (OrDraw * max(1, len(scene.meshes)))()
+    inst = getattr(scene, "instanced", [])
+    n_inst = sum(int(im.transforms.shape[0]) for im in inst)
+    order = scenes.draw_order(scene, eye)
+    n_draws = len(order) + n_inst
+    draws = (OrDraw * max(1, n_draws))()
     amb = min(max(scene.ambient, 0.0), 1.0)
-    for k, mi in enumerate(scenes.draw_order(scene, eye)):
+    for k, mi in enumerate(order):
         m = scene.meshes[mi]
         v = _f32(m.vertices)
         i = np.ascontiguousarray(m.indices, np.uint32)
@@ -232,9 +237,42 @@ def render(scene, ibl=None, want_hdr=False):
         d.blend_mode = scenes.effective_blend(m)
         d.lights = lights
         d.light_count = len(scene.lights)
+        d.depth_write = 1
+        if scenes.is_chrome(m.object_id):  # EMIT_DRAW, viewport.c:2035-2076
+            d.depth_test, d.backface_cull = 0, 0
+            d.lights, d.light_count = None, 0
+            d.ambient = 1.0
         if m.texture >= 0:
             t = texs[m.texture]
             d.texture, d.tex_h, d.tex_w = t.ctypes.data, t.shape[0], t.shape[1]
+    # pass_instanced (reference viewport.c:2602-2646), after the transparent pass: one draw
+    # per instance (cpu_draw_instanced, cpu_backend.c:638-657) with model = the instance,
+    # mvp = P * (V * instance), the default material, no texture, culling only for
+    # non-zero IDs, depth test with the depth write off, and cam_eye left at zero
+    k = len(order)
+    for im in inst:
+        v = _f32(im.vertices)
+        i = np.ascontiguousarray(im.indices, np.uint32)
+        keep += [v, i]
+        for t in np.asarray(im.transforms, np.float32).reshape(-1, 16):
+            d = draws[k]
+            k += 1
+            d.vertices, d.vertex_count = v.ctypes.data, v.shape[0]
+            d.indices, d.index_count = i.ctypes.data, i.size
+            d.object_id = im.object_id
+            d.model[:] = [float(x) for x in t]
+            d.mvp[:] = [float(x) for x in mat4_multiply(proj, mat4_multiply(view, t))]
+            d.light_dir[:] = DEFAULT_LIGHT_DIR
+            d.ambient = amb
+            d.opacity = 1.0
+            d.metallic, d.roughness = 0.0, 0.5
+            d.cam_eye[:] = [0.0, 0.0, 0.0]
+            d.smooth = 1 if getattr(scene, "smooth", True) else 0
+            d.depth_test, d.depth_write = 1, 0
+            d.backface_cull = 1 if im.object_id != 0 else 0
+            d.blend_mode = 0
+            d.lights = lights
+            d.light_count = len(scene.lights)
     sw, sh = scene.width * scene.ssaa, scene.height * scene.ssaa
     out = {
         "color": np.zeros((scene.height, scene.width, 4), np.uint8),
@@ -278,7 +316,7 @@ def render(scene, ibl=None, want_hdr=False):
         keep += [shadow, so]
         f.shadow = C.pointer(so)
         out["shadow"] = shadow
-    rc = L.oracle_render(C.byref(f), draws, len(scene.meshes))
+    rc = L.oracle_render(C.byref(f), draws, n_draws)
     if rc != 0:
         raise RuntimeError(f"oracle_render failed: {rc}")
     return out

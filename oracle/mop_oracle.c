@@ -1445,6 +1445,14 @@ int oracle_render(OrFrame *f, const OrDraw *draws, uint32_t n) {
   }
   for (uint32_t di = 0; di < n; di++) {
     const OrDraw *d = &draws[di];
+    /* cpu_draw, cpu_backend.c:536-544 and 621-627: a read-only depth test
+     * keeps the depth buffer as it was before the draw */
+    float *saved = NULL;
+    if (d->depth_test && !d->depth_write) {
+      saved = malloc(px * 4);
+      if (saved)
+        memcpy(saved, fb.depth, px * 4);
+    }
     for (uint32_t i = 0; i + 2 < d->index_count; i += 3) {
       uint32_t ix[3] = {d->indices[i], d->indices[i + 1], d->indices[i + 2]};
       if (ix[0] >= d->vertex_count || ix[1] >= d->vertex_count || ix[2] >= d->vertex_count)
@@ -1453,6 +1461,10 @@ int oracle_render(OrFrame *f, const OrDraw *draws, uint32_t n) {
       for (int k = 0; k < 3; k++)
         prepare_vertex(d, d->vertices + (size_t)ix[k] * 12, &tri[k]);
       triangle(tri, d, f->ibl, &fb);
+    }
+    if (saved) {
+      memcpy(fb.depth, saved, px * 4);
+      free(saved);
     }
   }
   if (f->hdr)

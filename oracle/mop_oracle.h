@@ -63,6 +63,9 @@ typedef struct OrDraw {
   uint32_t light_count;
   const uint8_t *texture; /* RGBA8 or NULL */
   int32_t tex_w, tex_h;
+  /* 0 with depth_test: the depth buffer is saved before the draw and restored
+   * after it (cpu_backend.c:536-544, 621-627) */
+  int32_t depth_write;
 } OrDraw;
 
 typedef struct OrIBL {

@@ -89,6 +89,20 @@ static void cuda_shadow_hook(MopViewport *vp, void *ud) {
   free(models);
   free(casters);
 }
+
+/* The integration patch's post-process row for the CUDA backend: the core
+ * applies vp->post_effects and vp->fog_params itself for its CPU backend only
+ * (rg_cleanup, viewport.c:2950-2961); the patch hands both to the device,
+ * whose post pass runs them at frame end.  Run as a MOP_STAGE_PRE_SCENE hook,
+ * so the values of the frame being rendered apply. */
+static void cuda_post_hook(MopViewport *vp, void *ud) {
+  (void)ud;
+  MopCudaDevice *cu = mop_rhi_cuda_device(vp->device);
+  const float fog[4] = {vp->fog_params.color.r, vp->fog_params.color.g, vp->fog_params.color.b,
+                        vp->fog_params.color.a};
+  mopcuda_set_post_effects(cu, vp->post_effects);
+  mopcuda_set_fog(cu, fog, vp->fog_params.near_dist, vp->fog_params.far_dist);
+}
 #endif
 
 void *refh_create(const RefScene *sc) {
@@ -133,8 +147,10 @@ void *refh_create(const RefScene *sc) {
   }
 
 #ifdef REFH_CUDA_HOOKS
-  if (!cpu)
+  if (!cpu) {
     mop_viewport_add_hook(vp, MOP_STAGE_PRE_SCENE, cuda_shadow_hook, NULL);
+    mop_viewport_add_hook(vp, MOP_STAGE_PRE_SCENE, cuda_post_hook, NULL);
+  }
 #endif
   mop_viewport_set_chrome(vp, false);
   mop_viewport_set_overlay_enabled(vp, MOP_OVERLAY_OUTLINE, false);
@@ -211,6 +227,17 @@ void *refh_create(const RefScene *sc) {
       mop_mesh_set_blend_mode(mesh, (MopBlendMode)rm->blend_mode);
     if (rm->opacity != 1.0f)
       mop_mesh_set_opacity(mesh, rm->opacity);
+  }
+
+  for (uint32_t k = 0; k < sc->instanced_count; k++) {
+    const RefInstanced *ri = &sc->instanced[k];
+    MopMeshDesc md = {.vertices = (const MopVertex *)ri->vertices,
+                      .vertex_count = ri->vertex_count,
+                      .indices = ri->indices,
+                      .index_count = ri->index_count,
+                      .object_id = ri->object_id};
+    mop_viewport_add_instanced_mesh(vp, &md, (const MopMat4 *)ri->transforms,
+                                    ri->instance_count);
   }
 
   if (sc->env == 1) {

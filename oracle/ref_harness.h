@@ -34,6 +34,19 @@ typedef struct RefMesh {
   int32_t blend_mode;       /* > 0: mop_mesh_set_blend_mode before opacity  */
 } RefMesh;
 
+/* mop_viewport_add_instanced_mesh (reference viewport.c:3774-3858): one
+ * object ID, the default material, no texture; drawn by pass_instanced after
+ * the transparent pass with mvp = P * (V * instance) per instance. */
+typedef struct RefInstanced {
+  const float *vertices;    /* vertex_count * 12 floats, MopVertex layout   */
+  uint32_t vertex_count;
+  const uint32_t *indices;
+  uint32_t index_count;
+  uint32_t object_id;
+  const float *transforms;  /* instance_count column-major matrices         */
+  uint32_t instance_count;
+} RefInstanced;
+
 typedef struct RefLight {
   int32_t type;             /* 0 directional, 1 point, 2 spot              */
   float position[3];
@@ -76,6 +89,8 @@ typedef struct RefScene {
   int32_t fog_on;           /* 1: mop_viewport_set_fog with the values below */
   float fog_color[4];
   float fog_near, fog_far;
+  uint32_t instanced_count;
+  const RefInstanced *instanced;
 } RefScene;
 
 typedef struct RefFrame {

@@ -33,6 +33,13 @@ class RefLight(C.Structure):
                 ("active", C.c_int32), ("cast_shadows", C.c_int32)]
 
 
+class RefInstanced(C.Structure):
+    _fields_ = [("vertices", C.c_void_p), ("vertex_count", C.c_uint32),
+                ("indices", C.c_void_p), ("index_count", C.c_uint32),
+                ("object_id", C.c_uint32), ("transforms", C.c_void_p),
+                ("instance_count", C.c_uint32)]
+
+
 class RefScene(C.Structure):
     _fields_ = [("width", C.c_int32), ("height", C.c_int32), ("ssaa", C.c_int32),
                 ("clear_color", C.c_float * 4), ("eye", C.c_float * 3),
@@ -50,7 +57,8 @@ class RefScene(C.Structure):
                 ("flat", C.c_int32), ("workers", C.c_int32),
                 ("backend", C.c_int32), ("fog_on", C.c_int32),
                 ("fog_color", C.c_float * 4), ("fog_near", C.c_float),
-                ("fog_far", C.c_float)]
+                ("fog_far", C.c_float), ("instanced_count", C.c_uint32),
+                ("instanced", C.POINTER(RefInstanced))]
 
 
 class RefFrame(C.Structure):
@@ -180,7 +188,20 @@ class Reference:
             sc.fog_on = 1
             sc.fog_color[:] = fog[0]
             sc.fog_near, sc.fog_far = fog[1], fog[2]
-        self._keep += [meshes, lights, tw, th, td, sc]
+        inst = getattr(scene, "instanced", [])
+        ia = (RefInstanced * max(1, len(inst)))()
+        for k, im in enumerate(inst):
+            v = np.ascontiguousarray(im.vertices, np.float32)
+            i = np.ascontiguousarray(im.indices, np.uint32)
+            t = np.ascontiguousarray(im.transforms, np.float32).reshape(-1, 16)
+            self._keep += [v, i, t]
+            ia[k].vertices, ia[k].vertex_count = v.ctypes.data, v.shape[0]
+            ia[k].indices, ia[k].index_count = i.ctypes.data, i.size
+            ia[k].object_id = im.object_id
+            ia[k].transforms, ia[k].instance_count = t.ctypes.data, t.shape[0]
+        sc.instanced_count = len(inst)
+        sc.instanced = ia
+        self._keep += [meshes, lights, tw, th, td, sc, ia]
         self.h = L.refh_create(C.byref(sc))
         if not self.h:
             raise RuntimeError("refh_create failed")

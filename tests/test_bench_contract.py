@@ -32,6 +32,12 @@ def test_reference_arm_json_line():
     assert KEYS <= set(d) and d["impl"] == "reference"
     assert d["metric"] == d["unit"] == "Mpix/s" and d["higher_is_better"] is True
     assert d["value"] > 0 and d["config"]["workload"].startswith("config1")
+    # the driver's warm-up count is honoured, and the config object is the CUDA arm's
+    assert d["warmup"] == 1 and d["steps"] >= 1
+    sys.path.insert(0, str(ROOT))
+    import bench
+    sc, desc = bench.workload("config1")
+    assert d["config"] == bench.config_dict(desc, 1, sc)
     cb = d["cpu_baseline"]
     assert cb["kind"] == "reference" and cb["value"] == d["value"] and cb["cores"] >= 1
     assert "serial" in cb["modes"] and len(cb["modes"]) >= 1

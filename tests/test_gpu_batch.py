@@ -87,6 +87,19 @@ def test_batch_equals_single_viewport_frames(cuda_device, ibl):
         b.close()
 
 
+def test_batch_fog_equals_single_viewport_frames(cuda_device, ibl):
+    """A batch made while the device has the FOG bit and fog parameters set
+    applies them to every viewport as the plain frame does."""
+    sc = dataclasses.replace(_scene(), fog=((0.6, 0.65, 0.7, 1.0), 0.9, 0.999),
+                             post_effects=scenes.DEFAULT_POST | scenes.POST_FOG)
+    b = mopcuda.BatchRenderer(cuda_device, sc, _views(sc, 6, seed=9), ibl)
+    try:
+        b.render()
+        _check_batch(cuda_device, b, sc, ibl, "fog batch")
+    finally:
+        b.close()
+
+
 def test_batch_read_views_equals_single_reads(cuda_device, ibl):
     """mopcuda_batch_read_views (every view's buffer in one call) returns the
     bytes of one mopcuda_batch_read per view, for each buffer, and rejects a

@@ -48,6 +48,25 @@ CASES = {
     "shadow": lambda: scenes.shadow_scene(seed=27, width=192, height=144),
     "shadow_ssaa2_transparent": lambda: scenes.shadow_scene(seed=28, width=128, height=96,
                                                             ssaa=2, transparent=True),
+    # MOP_POST_FOG through mop_viewport_set_fog: the core applies post effects for its CPU
+    # backend only; the harness hands vp->post_effects and vp->fog_params to the device
+    # (the integration patch's post-process row) from a MOP_STAGE_PRE_SCENE hook
+    "fog": lambda: dataclasses.replace(
+        scenes.small_scene(seed=63, width=192, height=144),
+        post_effects=scenes.DEFAULT_POST | scenes.POST_FOG, fog=((0.6, 0.65, 0.7, 1.0), 0.85, 0.99)),
+    "fog_all_effects_ssaa2": lambda: dataclasses.replace(
+        scenes.small_scene(seed=64, width=160, height=120, ssaa=2),
+        post_effects=(scenes.POST_GAMMA | scenes.POST_TONEMAP | scenes.POST_VIGNETTE
+                      | scenes.POST_FOG | scenes.POST_FXAA),
+        fog=((0.2, 0.3, 0.5, 1.0), 0.9, 0.995)),
+    # mop_viewport_add_instanced_mesh: the core's pass_instanced calls the RHI's
+    # draw_instanced with the depth write off (cpu_backend.c:638-657, 536-580)
+    "instanced": lambda: scenes.instanced_scene(seed=65),
+    "instanced_zero_id_ssaa2": lambda: scenes.instanced_scene(seed=66, width=160, height=120,
+                                                              ssaa=2, zero_id=True),
+    "instanced_transparent": lambda: scenes.instanced_scene(seed=67, transparent=True),
+    # meshes with editor-chrome IDs: the core draws them with the depth test off
+    "chrome": lambda: scenes.chrome_scene(seed=68),
     "config2_reduced_no_ibl": lambda: dataclasses.replace(
         scenes.config2(width=480, height=270, ssaa=2, instances=48, tex_size=64), env=0),
 }

@@ -87,7 +87,50 @@ CASES = {
                                                           instances=24, tex_size=64)),
     "shadow_config3": lambda: _with_shadow(scenes.config3(seed=5, n_tris=80_000, width=480,
                                                           height=270)),
+    # MOP_POST_FOG with mop_viewport_set_fog: each sample's colour moved towards the fog colour
+    # by its depth value, ahead of tonemap / gamma / vignette
+    "fog": lambda: _fog(scenes.small_scene(seed=41), ((0.6, 0.65, 0.7, 1.0), 0.85, 0.99)),
+    "fog_ssaa2": lambda: _fog(scenes.small_scene(seed=44, ssaa=2),
+                              ((0.55, 0.6, 0.7, 1.0), 0.8, 0.99)),
+    "fog_all_effects_ssaa2": lambda: _fog(
+        scenes.small_scene(seed=42, ssaa=2), ((0.2, 0.3, 0.5, 1.0), 0.9, 0.995),
+        scenes.POST_GAMMA | scenes.POST_TONEMAP | scenes.POST_VIGNETTE | scenes.POST_FXAA),
+    "fog_tonemap_no_gamma": lambda: _fog(scenes.small_scene(seed=45),
+                                         ((0.9, 0.8, 0.7, 1.0), 0.7, 0.999),
+                                         scenes.POST_TONEMAP | scenes.POST_FXAA),
+    "fog_zero_range": lambda: _fog(scenes.small_scene(seed=43), ((1.0, 0.0, 0.0, 1.0), 0.95, 0.95)),
+    "fog_bright_colour_ssaa3": lambda: _fog(scenes.small_scene(seed=46, width=90, height=60, ssaa=3),
+                                            ((1.6, -0.2, 0.4, 1.0), 0.5, 0.98)),
+    "fog_transparent": lambda: _fog(scenes.transparent_scene(seed=47),
+                                    ((0.5, 0.5, 0.55, 1.0), 0.9, 0.999)),
+    "fog_config2_ibl": lambda: _fog(scenes.config2(width=320, height=180, ssaa=2, instances=24,
+                                                   tex_size=64), ((0.7, 0.75, 0.8, 1.0), 0.95, 1.0)),
+    # mop_viewport_add_instanced_mesh through mopcuda_draw_instanced: 96 instances with one
+    # ID after the transparent pass, depth write off (each instance's depth undone after it)
+    "instanced": lambda: scenes.instanced_scene(seed=71),
+    "instanced_zero_id_ssaa2": lambda: scenes.instanced_scene(seed=72, ssaa=2, zero_id=True),
+    "instanced_transparent": lambda: scenes.instanced_scene(seed=73, transparent=True),
+    "instanced_flat": lambda: dataclasses.replace(scenes.instanced_scene(seed=74), smooth=False),
+    "instanced_unlit": lambda: dataclasses.replace(scenes.instanced_scene(seed=75), lights=[]),
+    "instanced_shadow_ibl_ssaa2": lambda: _with_shadow(scenes.instanced_scene(seed=76, ssaa=2,
+                                                                              env=1)),
+    # editor-chrome IDs among the opaque meshes: depth test and culling off, unlit
+    "chrome": lambda: scenes.chrome_scene(seed=81),
+    "chrome_ssaa2_flat": lambda: dataclasses.replace(scenes.chrome_scene(seed=82, ssaa=2),
+                                                     smooth=False),
 }
+
+# fog cases whose colour is bit-exact: no IBL lookups (CUDA's atan2f/asinf) and no
+# vignette (the one place the sRGB value itself, not its byte, is needed)
+FOG_EXACT = ["fog", "fog_ssaa2", "fog_tonemap_no_gamma", "fog_zero_range",
+             "fog_bright_colour_ssaa3", "fog_transparent"]
+
+
+def _fog(sc, fog, post=None):
+    """The scene with the FOG bit added to its post effects (or to `post`) and
+    the given MopFogParams ((r, g, b, a), near, far)."""
+    fx = (sc.post_effects if post is None else post) | scenes.POST_FOG
+    return dataclasses.replace(sc, post_effects=fx, fog=fog)
 
 
 def _with_shadow(sc):
@@ -125,6 +168,43 @@ def test_frame_parity(cuda_device, name):
         assert (d1.view(np.uint32) == d2.view(np.uint32)).all()
     finally:
         got["renderer"].close()
+
+
+@pytest.mark.parametrize("name", FOG_EXACT)
+def test_fog_colour_bit_exact(cuda_device, name):
+    """The fog term, Reinhard and the sRGB step through the threshold table
+    give the reference's bytes exactly where no IBL lookup is involved."""
+    sc = CASES[name]()
+    ref = cpu_oracle.render(sc, None)
+    got = _render_cuda(cuda_device, sc, None)
+    try:
+        for key in ("color_full", "color"):
+            s = color_stats(got[key], ref[key])
+            assert s["exact"] == 1.0, (name, key, s)
+    finally:
+        got["renderer"].close()
+
+
+def test_fog_follows_set_fog(cuda_device):
+    """Fog parameters changed between frames take effect on the next frame;
+    the FOG bit with a new device's zero parameters leaves colours as they are."""
+    sc = CASES["fog"]()
+    plain = dataclasses.replace(sc, fog=None)
+    r = mopcuda.SceneRenderer(cuda_device, plain)
+    try:
+        r.render()
+        zero = r.color_full().copy()
+        ref0 = cpu_oracle.render(dataclasses.replace(sc, post_effects=scenes.DEFAULT_POST,
+                                                     fog=None), None)
+        assert (zero == ref0["color_full"]).all()
+        fc = (mopcuda.C.c_float * 4)(*sc.fog[0])
+        assert cuda_device.L.mopcuda_set_fog(cuda_device.h, fc, sc.fog[1], sc.fog[2]) == 0
+        r.render()
+        ref1 = cpu_oracle.render(sc, None)
+        assert (r.color_full() == ref1["color_full"]).all()
+        assert cuda_device.L.mopcuda_set_fog(cuda_device.h, None, 0.0, 1.0) != 0
+    finally:
+        r.close()
 
 
 def test_repeat_frames_identical(cuda_device):

@@ -92,6 +92,17 @@ LIVE = {
     "fog_zero_range": lambda: dataclasses.replace(
         scenes.small_scene(seed=43), post_effects=scenes.DEFAULT_POST | scenes.POST_FOG,
         fog=((1.0, 0.0, 0.0, 1.0), 0.95, 0.95)),
+    # mop_viewport_add_instanced_mesh: pass_instanced after the transparent pass, one draw
+    # per instance with the depth write off (depth saved and restored around each)
+    "instanced": lambda: scenes.instanced_scene(seed=71),
+    "instanced_zero_id_ssaa2": lambda: scenes.instanced_scene(seed=72, ssaa=2, zero_id=True),
+    "instanced_transparent": lambda: scenes.instanced_scene(seed=73, transparent=True),
+    "instanced_flat": lambda: dataclasses.replace(scenes.instanced_scene(seed=74), smooth=False),
+    "instanced_unlit": lambda: dataclasses.replace(scenes.instanced_scene(seed=75), lights=[]),
+    # meshes with editor-chrome IDs: depth test and culling off, legacy unlit path
+    "chrome": lambda: scenes.chrome_scene(seed=81),
+    "chrome_ssaa2_flat": lambda: dataclasses.replace(scenes.chrome_scene(seed=82, ssaa=2),
+                                                     smooth=False),
 }
 
 

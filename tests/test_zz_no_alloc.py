@@ -54,6 +54,36 @@ def test_noalloc_pick_matches_pick_batch():
                                             out.ctypes.data, out.ctypes.data, out.ctypes.data)
         assert rc == mopcuda.EINVAL
         assert "limit" in mopcuda.last_error()
+        # no queries: nothing to do, nothing touched
+        rc = r.L.mopcuda_pick_batch_noalloc(r.dev.h, r.fb, sc.ssaa, None, 0, None, None, None)
+        assert rc == mopcuda.OK
+    finally:
+        r.close()
+        dev.close()
+
+
+def test_noalloc_pick_refuses_pending_frame():
+    """With the framebuffer's frame still in flight the call returns EINVAL
+    (completing the frame could reallocate); after mopcuda_frame_wait it
+    answers as mopcuda_pick_batch does."""
+    dev = mopcuda.Device(0)
+    sc = scenes.small_scene(seed=32, width=160, height=120)
+    r = mopcuda.SceneRenderer(dev, sc)
+    try:
+        r.render()
+        xy = np.ascontiguousarray(scenes.pick_points(sc, 500, seed=4), np.int32)
+        n = xy.shape[0]
+        out = [np.zeros(n, np.uint32), np.zeros(n, np.float32), np.zeros(n, np.int32)]
+        r.submit()  # launched, not waited for
+        rc = r.L.mopcuda_pick_batch_noalloc(r.dev.h, r.fb, sc.ssaa, xy.ctypes.data, n,
+                                            *[o.ctypes.data for o in out])
+        # pending is host state (set by frame_end, cleared by frame_wait), so this holds
+        # however far the device has got
+        assert rc == mopcuda.EINVAL and "pending" in mopcuda.last_error()
+        r.wait()
+        got = _noalloc(r, xy)
+        for a, b in zip(r.pick(xy), got):
+            assert (a.view(np.uint32) == b.view(np.uint32)).all()
     finally:
         r.close()
         dev.close()
