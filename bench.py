@@ -53,7 +53,7 @@ def parse():
     ap.add_argument("--forms-only", action="store_true",
                     help="run only the batched and served forms (one JSON line)")
     ap.add_argument("--form", choices=["all", "batched", "served", "shadowed", "ibl",
-                                           "scene_load"], default="all",
+                                           "scene_load", "config3", "config1"], default="all",
                     help="with --forms-only: which form to run")
     return ap.parse_args()
 
@@ -342,8 +342,7 @@ def run_cuda(args):
     L = sum(1 for l in sc.lights if l.active)
     ops_per_sample = 80 + 120 * L + (150 if sc.env else 0)
     alu_achieved = covered * ops_per_sample / (tile_ms * 1e-3) / 1e9
-    frame_bytes = (sum(4 * m.indices.size + 48 * m.vertices.shape[0] for m in sc.meshes)
-                   + 64 * len(sc.meshes) + 12 * sc.samples + (4 * sc.pixels if sc.ssaa > 1 else 0))
+    frame_bytes = frame_bytes_of(sc)
 
     line = {"metric": "Mpix/s", "value": round(value, 3), "unit": "Mpix/s", "n_gpus": world,
             "steps": steps, "warmup": warm, "ms_per_step": round(total_ms / steps, 4),
@@ -515,13 +514,16 @@ def run_served(dev, rates=(2000.0, 4000.0, 6000.0), duration=2.0, n_scenes=32):
     import scenes
     import serving
     counts = scenes.served_triangle_counts(n_scenes)
-    scs = [scenes.served_scene(100 + i, c, tex_size=256) for i, c in enumerate(counts)]
+    scs = [scenes.served_scene(100 + i, c, tex_size=1024) for i, c in enumerate(counts)]
     ibl = scenes.procedural_ibl(scs[0].sun_dir)
     rss = [mopcuda.ResidentScene(dev, sc, ibl) for sc in scs]
     out = {"workload": f"{n_scenes} resident scenes ({sum(counts):,} tris, 50k-2M log-normal), "
                        "Poisson arrivals, 85% renders at 256^2/720p/1080p/1440p, 15% pick "
                        "batches of 1-64, 1% of a scene's instances moved per request",
            "server_config": {"max_views": 32, "max_inflight": 3, "hbm_budget_gib": 100},
+           "plain_arm": "one frame per request through the per-viewport C ABI, image read "
+                        "into page-locked memory",
+           "textures": "4 x 1024^2 RGBA8 per scene, as in config 2",
            "capped_config": {"max_launch_samples": CAP_SAMPLES},
            "rates": []}
     keys = ("p50_ms", "p99_ms", "mpix_s")
@@ -554,11 +556,73 @@ def run_served(dev, rates=(2000.0, 4000.0, 6000.0), duration=2.0, n_scenes=32):
             out["rates"].append({
                 "req_per_s": rate, "requests": len(trace), **runs,
                 "plain": {k: round(p[k], 3) for k in keys},
-                "exact_check": chk})
+                "speedup_vs_plain": {
+                    "mpix_s": round(runs["server"]["mpix_s"] / p["mpix_s"], 2),
+                    "p99": round(p["p99_ms"] / runs["server"]["p99_ms"], 2)},
+                "exact_check": dict(chk, against="each kept request's own plain frame (the "
+                                    "plain path is pinned to the CPU oracle by the GPU parity "
+                                    "tests; served requests are checked against the oracle "
+                                    "in tests/test_gpu_server.py)")})
     finally:
         for rs in rss:
             rs.close()
     return out
+
+
+def frame_bytes_of(sc):
+    """Algorithmic bytes of one frame: every mesh's indices and vertices read
+    once, 64 B of draw state per draw, colour + depth + ID per sample and the
+    presented image when SSAA is on."""
+    return (sum(4 * m.indices.size + 48 * m.vertices.shape[0] for m in sc.meshes)
+            + 64 * len(sc.meshes) + 12 * sc.samples + (4 * sc.pixels if sc.ssaa > 1 else 0))
+
+
+def run_frames_form(dev, name, steps=20, warm=3):
+    """Device-timed frames of another workload (an L2-sized buffer rewritten
+    between frames): frame ms, Mpix/s, Mtri/s, per-stage ms and the frame's
+    algorithmic bytes against the HBM peak."""
+    import numpy as np
+    import torch
+    import mopcuda
+    import scenes
+    if name == "config3":
+        sc = scenes.config3()
+        desc = ("config3: 1920x1080 ssaa1, 2,000,000 tris (0.1-8 px edges; 10% straddle the near "
+                "plane, 5% outside, 20% coplanar pairs in separate meshes, 5% skinned tubes), "
+                "1 dir + 1 point light")
+    else:
+        sc = scenes.config1()
+        desc = "config1: 800x600 ssaa1, UV sphere 64x32 + ground plane, 1 directional light"
+    r = mopcuda.SceneRenderer(dev, sc, None)
+    flush = torch.empty(64 << 20, dtype=torch.float32, device="cuda")
+    try:
+        dev.set_stage_timing(True)
+        for _ in range(warm):
+            r.render()
+        ms, stage = [], {k: 0.0 for k in mopcuda.Device.STAGES}
+        for _ in range(steps):
+            flush.add_(1.0)
+            torch.cuda.synchronize()
+            r.render()
+            ms.append(r.gpu_ms)
+            for k, v in dev.stage_times().items():
+                stage[k] += v
+        dev.set_stage_timing(False)
+        fm = float(np.median(ms))
+        peak, kind = read_peaks()
+        b = frame_bytes_of(sc)
+        return {"workload": desc, "steps": steps, "frame_ms": round(fm, 4),
+                "mpix_s": round(sc.pixels / (fm * 1e3), 1),
+                "mtri_s": round(sc.triangle_count / (fm * 1e3), 1),
+                "triangles": sc.triangle_count, "samples": sc.samples,
+                "stage_ms": {k: round(v / steps, 4) for k, v in stage.items()},
+                "roofline": {"bound": "hbm", "kernel": "whole frame",
+                             "algorithmic_bytes": b,
+                             "achieved": round(b / (fm * 1e-3) / 1e9, 1), "peak": peak,
+                             "unit": "GB/s", "frac": round(b / (fm * 1e-3) / 1e9 / peak, 4),
+                             "peak_source": kind}}
+    finally:
+        r.close()
 
 
 def run_shadowed(dev, steps=20, warm=3):
@@ -722,7 +786,9 @@ def run_forms(which="all"):
     out = {}
     for key, fn in (("batched", run_batched), ("served", run_served),
                     ("shadowed", run_shadowed), ("ibl", run_ibl),
-                    ("scene_load", run_scene_load)):
+                    ("scene_load", run_scene_load),
+                    ("config3", lambda d: run_frames_form(d, "config3")),
+                    ("config1", lambda d: run_frames_form(d, "config1"))):
         if which not in ("all", key):
             continue
         try:

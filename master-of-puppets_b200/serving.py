@@ -285,7 +285,9 @@ def run_plain(dev, rss, trace: List[Request], warmup: Optional[List[Request]] = 
         fb = L.mopcuda_framebuffer_create(d, w, h)
         L.mopcuda_framebuffer_set_ssaa(fb, 1)
         fbs[(w, h)] = fb
-    outs = {k: np.zeros((k[1], k[0], 4), np.uint8) for k in fbs}
+    # page-locked destinations: the image copies are direct DMA, as the server's are
+    pinned = {k: mopcuda.HostArray((k[1], k[0], 4), np.uint8) for k in fbs}
+    outs = {k: v.a for k, v in pinned.items()}
     lat = []
     try:
         for r in warmup or []:  # untimed: first-use allocations of every frame size
@@ -316,4 +318,6 @@ def run_plain(dev, rss, trace: List[Request], warmup: Optional[List[Request]] = 
     finally:
         for fb in fbs.values():
             L.mopcuda_framebuffer_destroy(d, fb)
+        for v in pinned.values():
+            v.close()
     return _summary(lat, sum(r.pixels for r in trace), wall)
