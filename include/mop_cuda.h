@@ -142,6 +142,16 @@ MopCudaTexture *mopcuda_texture_create_hdr(MopCudaDevice *dev, int width, int he
 void mopcuda_texture_destroy(MopCudaDevice *dev, MopCudaTexture *tex);
 int mopcuda_texture_read_rgba8(MopCudaDevice *dev, MopCudaTexture *tex, uint8_t *out,
                                size_t out_size);
+/* texture_create_ex (rhi.h:211-213), cpu_texture_create_ex
+ * (cpu_backend.c:1016-1056): format 0 is RGBA8 (mopcuda_texture_create);
+ * 1 BC1, 2 BC3, 3 BC5 (MopTexFormat, texture_pipeline.h:35-41) are copied to
+ * the device as stored and decoded there to RGBA8 exactly as
+ * bc_decompress_to_rgba8 does (cpu_backend.c:855-1014); BC7 (4) returns NULL
+ * with MOPCUDA_EUNSUPPORTED, as the CPU backend refuses it.  mip_levels is
+ * ignored (level 0 only, as the CPU backend).  A non-zero data_size smaller
+ * than the dimensions imply is refused (the reference would read past it). */
+MopCudaTexture *mopcuda_texture_create_ex(MopCudaDevice *dev, int width, int height, int format,
+                                          int mip_levels, const uint8_t *data, size_t data_size);
 
 /* ---- framebuffers: framebuffer_create/destroy/resize (rhi.h:146-151),
  *      cpu_backend.c:121-188 ------------------------------------------- */
@@ -154,6 +164,23 @@ int mopcuda_framebuffer_resize(MopCudaDevice *dev, MopCudaFramebuffer *fb, int w
  * set, frame_end fuses the box resolve of mop_viewport_read_color
  * (viewport.c:3385-3411) into its post pass. */
 int mopcuda_framebuffer_set_ssaa(MopCudaFramebuffer *fb, int ssaa);
+/* framebuffer_copy_to_texture (rhi.h:320-321), cpu_framebuffer_copy_to_texture
+ * (cpu_backend.c:741-790): the last frame's post-processed colour into an
+ * RGBA8 texture of the same size, or of a whole-number factor smaller on both
+ * axes (box of sf x sf samples, truncating mean); any other size is refused
+ * (MOPCUDA_EINVAL).  Waits for the frame; the texture's device copy (used by
+ * later draws) and host copy (mopcuda_texture_read_rgba8) are both updated. */
+int mopcuda_framebuffer_copy_to_texture(MopCudaDevice *dev, MopCudaFramebuffer *fb,
+                                        MopCudaTexture *target);
+/* framebuffer_create_from_texture (rhi.h:155-157),
+ * cpu_framebuffer_create_from_texture (cpu_backend.c:143-170): a framebuffer
+ * of the texture's size whose every completed frame lands in the texture
+ * (the CPU backend rasterises into the texture's pixels; here each frame's
+ * colour is copied in when it completes).  NULL for a size mismatch or an
+ * HDR texture.  The texture must outlive the framebuffer. */
+MopCudaFramebuffer *mopcuda_framebuffer_create_from_texture(MopCudaDevice *dev,
+                                                           MopCudaTexture *color, int width,
+                                                           int height);
 
 /* ---- vertex deformation: the core's mop_skin_apply / mop_morph_apply
  *      (reference src/core/viewport.c:1572-1680, 1763-1804) on the device.

@@ -127,6 +127,9 @@ struct MopCudaFramebuffer {
   void *rb_dst = nullptr;
   size_t rb_size = 0;
   int rb_ssaa = 1;
+  /* framebuffer_create_from_texture: every completed frame's colour is
+   * copied into this texture (device and host copies) */
+  MopCudaTexture *target = nullptr;
 };
 
 struct MopCudaDevice {
@@ -235,6 +238,9 @@ void mc_post_args(const MopCudaDevice *d, PostArgs &p);
  * (build_lut of fx) and fog parameters `fog` (colour RGBA, near, far); the
  * buffer pointers and sizes are left to the caller. */
 void mc_post_template(uint32_t fx, const float lut[256], const float fog[6], PostArgs &p);
+/* Copies a completed frame's colour into its framebuffer's render target,
+ * if it has one (device lock held). */
+int mc_target_update(MopCudaDevice *d, MopCudaFramebuffer *fb);
 /* mop_mat4_multiply order: running sum from 0.0f, no contraction. */
 void mc_mat4_mul(const float *a, const float *b, float *c);
 

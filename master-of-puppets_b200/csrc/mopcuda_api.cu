@@ -1149,6 +1149,8 @@ static int finish_frame(MopCudaDevice *d, int timeout_ms, bool defer_readback) {
         cudaEventElapsedTime(&d->stage_ms[i], d->stage_ev[i], d->stage_ev[i + 1]);
     const Counters *c = d->h_counters.as<Counters>();
     if (!c->overflow) {
+      if (d->fb && d->fb->target && (rc = mc_target_update(d, d->fb)))
+        return rc;
       if (d->fb && d->fb->rb_requested) {
         if (defer_readback) {
           d->rb_defer = d->fb; /* issued inside the caller's next launch */

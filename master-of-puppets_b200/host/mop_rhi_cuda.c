@@ -5,7 +5,10 @@
  * src/backend/cpu/cpu_backend.c:1296-1343): every mandatory entry of
  * MopRhiBackend (src/rhi/rhi.h:132-339) plus the recommended optional ones
  * (frame_submit, frame_gpu_time_ms, set_exposure, set_ibl_textures,
- * texture_read_rgba8, frame_wait_readback).  GPU-only effect hooks stay NULL
+ * texture_read_rgba8, frame_wait_readback, texture_create_ex with BC1/3/5
+ * decoded on the device, framebuffer_copy_to_texture and
+ * framebuffer_create_from_texture for render-to-texture).  GPU-only effect
+ * hooks stay NULL
  * exactly as the CPU table leaves them (every caller NULL-guards them,
  * rhi.h:112-130).
  *
@@ -253,6 +256,21 @@ static MopRhiTexture *cu_texture_create_hdr(MopRhiDevice *d, int w, int h, const
   return (MopRhiTexture *)mopcuda_texture_create_hdr(d->cu, w, h, rgba);
 }
 
+static MopRhiTexture *cu_texture_create_ex(MopRhiDevice *d, int w, int h, int format, int mips,
+                                          const uint8_t *data, size_t size) {
+  return (MopRhiTexture *)mopcuda_texture_create_ex(d->cu, w, h, format, mips, data, size);
+}
+
+static bool cu_framebuffer_copy_to_texture(MopRhiDevice *d, MopRhiFramebuffer *fb,
+                                           MopRhiTexture *t) {
+  return mopcuda_framebuffer_copy_to_texture(d->cu, FB(fb), TEX(t)) == MOPCUDA_OK;
+}
+
+static MopRhiFramebuffer *cu_framebuffer_create_from_texture(MopRhiDevice *d, MopRhiTexture *t,
+                                                             int w, int h) {
+  return (MopRhiFramebuffer *)mopcuda_framebuffer_create_from_texture(d->cu, TEX(t), w, h);
+}
+
 static void cu_texture_destroy(MopRhiDevice *d, MopRhiTexture *t) {
   mopcuda_texture_destroy(d->cu, TEX(t));
 }
@@ -285,7 +303,7 @@ static const MopRhiBackend CUDA_BACKEND = {
     .framebuffer_create = cu_framebuffer_create,
     .framebuffer_destroy = cu_framebuffer_destroy,
     .framebuffer_resize = cu_framebuffer_resize,
-    .framebuffer_create_from_texture = NULL,
+    .framebuffer_create_from_texture = cu_framebuffer_create_from_texture,
     .frame_begin = cu_frame_begin,
     .frame_end = cu_frame_end,
     .frame_submit = cu_frame_submit,
@@ -298,7 +316,7 @@ static const MopRhiBackend CUDA_BACKEND = {
     .framebuffer_read_depth = cu_read_depth,
     .texture_create = cu_texture_create,
     .texture_create_hdr = cu_texture_create_hdr,
-    .texture_create_ex = NULL,
+    .texture_create_ex = cu_texture_create_ex,
     .texture_destroy = cu_texture_destroy,
     .draw_instanced = cu_draw_instanced,
     .buffer_update = cu_buffer_update,
@@ -307,6 +325,7 @@ static const MopRhiBackend CUDA_BACKEND = {
     .set_exposure = cu_set_exposure,
     .set_ibl_textures = cu_set_ibl_textures,
     .texture_read_rgba8 = cu_texture_read_rgba8,
+    .framebuffer_copy_to_texture = cu_framebuffer_copy_to_texture,
 };
 
 const MopRhiBackend *mop_rhi_backend_cuda(void) { return &CUDA_BACKEND; }

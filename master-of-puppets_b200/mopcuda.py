@@ -123,10 +123,13 @@ SIGNATURES = [
     ("mopcuda_texture_create_hdr", _P, [_P, C.c_int, C.c_int, _P]),
     ("mopcuda_texture_destroy", None, [_P, _P]),
     ("mopcuda_texture_read_rgba8", C.c_int, [_P, _P, _P, C.c_size_t]),
+    ("mopcuda_texture_create_ex", _P, [_P, C.c_int, C.c_int, C.c_int, C.c_int, _P, C.c_size_t]),
     ("mopcuda_framebuffer_create", _P, [_P, C.c_int, C.c_int]),
     ("mopcuda_framebuffer_destroy", None, [_P, _P]),
     ("mopcuda_framebuffer_resize", C.c_int, [_P, _P, C.c_int, C.c_int]),
     ("mopcuda_framebuffer_set_ssaa", C.c_int, [_P, C.c_int]),
+    ("mopcuda_framebuffer_copy_to_texture", C.c_int, [_P, _P, _P]),
+    ("mopcuda_framebuffer_create_from_texture", _P, [_P, _P, C.c_int, C.c_int]),
     ("mopcuda_set_exposure", None, [_P, C.c_float]),
     ("mopcuda_set_post_effects", None, [_P, C.c_uint32]),
     ("mopcuda_set_fog", C.c_int, [_P, C.POINTER(C.c_float), C.c_float, C.c_float]),
@@ -413,6 +416,14 @@ class _Resident:
             self.instanced.append((im, vb, ib, v.shape[0], i.size, tr))
         self.textures = []
         for t in scene.textures:
+            if hasattr(t, "format"):  # block-compressed: texture_create_ex decodes on the device
+                b = np.ascontiguousarray(t.data, np.uint8)
+                th = L.mopcuda_texture_create_ex(d, t.width, t.height, t.format, 1, b.ctypes.data,
+                                                 b.size)
+                if not th:
+                    raise RuntimeError(f"texture_create_ex failed: {last_error()}")
+                self.textures.append(th)
+                continue
             t = np.ascontiguousarray(t, np.uint8)
             th = L.mopcuda_texture_create(d, t.shape[1], t.shape[0], t.ctypes.data)
             if not th:

@@ -51,6 +51,40 @@ class Mesh:
         return int(self.indices.size // 3)
 
 
+TEX_RGBA8, TEX_BC1, TEX_BC3, TEX_BC5, TEX_BC7 = 0, 1, 2, 3, 4  # MopTexFormat
+
+
+@dataclasses.dataclass
+class CompressedTexture:
+    """A block-compressed texture as mop_tex_create receives it (reference
+    include/mop/core/texture_pipeline.h:35-56): BC1 (8 bytes per 4x4 block),
+    BC3 or BC5 (16 bytes), blocks in row-major order."""
+    width: int
+    height: int
+    format: int
+    data: np.ndarray              # uint8 blocks
+
+    @property
+    def block_bytes(self) -> int:
+        return 8 if self.format == TEX_BC1 else 16
+
+
+def bc_texture(rng: np.random.Generator, fmt: int, width: int, height: int) -> CompressedTexture:
+    """Seeded random blocks: both endpoint orders of every block kind occur
+    (four-colour / three-colour BC1, eight-step / six-step BC4), and every
+    fourth block has equal endpoints."""
+    bw, bh = (width + 3) // 4, (height + 3) // 4
+    bs = 8 if fmt == TEX_BC1 else 16
+    data = rng.integers(0, 256, (bw * bh, bs), dtype=np.uint8)
+    for h in ([0] if fmt == TEX_BC1 else [0, 8]):
+        colour = fmt == TEX_BC1 or (fmt == TEX_BC3 and h == 8)
+        if colour:
+            data[::4, h + 2:h + 4] = data[::4, h:h + 2]  # c1 = c0 (16-bit endpoints)
+        else:
+            data[::4, h + 1] = data[::4, h]              # a1 = a0
+    return CompressedTexture(width, height, fmt, data.reshape(-1))
+
+
 @dataclasses.dataclass
 class InstancedMesh:
     """mop_viewport_add_instanced_mesh (reference viewport.c:3774-3858): one
@@ -706,6 +740,21 @@ def instanced_scene(seed: int = 70, width: int = 192, height: int = 144, ssaa: i
     if zero_id:
         v, i = torus(16, 8, 0.35, 0.12, _color(rng))
         sc.instanced.append(InstancedMesh(v, i, 0, scatter(64, 0.6, 1.4)))
+    return sc
+
+
+def bc_scene(seed: int = 90, width: int = 192, height: int = 144, ssaa: int = 1) -> Scene:
+    """small_scene whose meshes sample block-compressed textures (BC1, BC3
+    and BC5 of odd sizes, so the last row and column of blocks are clamped)
+    besides an RGBA8 one: textures modulate vertex colours at the vertices."""
+    sc = small_scene(seed=seed, width=width, height=height, ssaa=ssaa, n_meshes=8)
+    sc.name = f"bc{seed}"
+    rng = np.random.default_rng(seed + 700)
+    sc.textures.append(bc_texture(rng, TEX_BC1, 61, 47))
+    sc.textures.append(bc_texture(rng, TEX_BC3, 64, 64))
+    sc.textures.append(bc_texture(rng, TEX_BC5, 33, 70))
+    for k in range(1, len(sc.meshes)):
+        sc.meshes[k].texture = k % 4
     return sc
 
 

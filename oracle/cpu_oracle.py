@@ -121,6 +121,7 @@ def lib():
         _lib.oracle_morph_apply.argtypes = [C.POINTER(OrDeformLayout), C.c_void_p, C.c_uint32,
                                             C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p]
         _lib.oracle_mop_decode_mesh.argtypes = [C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p]
+        _lib.oracle_bc_decode.argtypes = [C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p]
         _lib.oracle_shadow_matrix.argtypes = [C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p]
         _lib.oracle_shadow_render.argtypes = [C.POINTER(OrShadowMesh), C.c_uint32, C.c_int,
                                               C.c_void_p, C.c_void_p]
@@ -207,7 +208,8 @@ def render(scene, ibl=None, want_hdr=False):
     lights = (OrLight * max(1, len(scene.lights)))()
     for k, l in enumerate(scene.lights):
         lights[k] = _light(l)
-    texs = [np.ascontiguousarray(t, np.uint8) for t in scene.textures]
+    texs = [bc_decode(t) if isinstance(t, scenes.CompressedTexture)
+            else np.ascontiguousarray(t, np.uint8) for t in scene.textures]
     inst = getattr(scene, "instanced", [])
     n_inst = sum(int(im.transforms.shape[0]) for im in inst)
     order = scenes.draw_order(scene, eye)
@@ -319,6 +321,16 @@ def render(scene, ibl=None, want_hdr=False):
     rc = L.oracle_render(C.byref(f), draws, n_draws)
     if rc != 0:
         raise RuntimeError(f"oracle_render failed: {rc}")
+    return out
+
+
+def bc_decode(t):
+    """The RGBA8 texels [h, w, 4] of a scenes.CompressedTexture
+    (bc_decompress_to_rgba8)."""
+    out = np.zeros((t.height, t.width, 4), np.uint8)
+    d = np.ascontiguousarray(t.data, np.uint8)
+    if lib().oracle_bc_decode(t.format, t.width, t.height, d.ctypes.data, out.ctypes.data):
+        raise ValueError(f"format {t.format} is not decoded")
     return out
 
 

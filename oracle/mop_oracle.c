@@ -1664,3 +1664,89 @@ int oracle_mop_decode_mesh(const uint8_t *sec, uint64_t size, float *out_v, uint
   }
   return 0;
 }
+
+/* ------------------------------------------------------------------------
+ * BC texture decode: bc_decode_rgb565, bc1/bc4/bc3/bc5_decode_block and
+ * bc_decompress_to_rgba8 (reference cpu_backend.c:859-1014), integer
+ * arithmetic with the same truncating divisions.
+ * ------------------------------------------------------------------------ */
+static void or_rgb565(unsigned c, unsigned o[3]) {
+  o[0] = ((c >> 11) & 0x1Fu) * 255u / 31u;
+  o[1] = ((c >> 5) & 0x3Fu) * 255u / 63u;
+  o[2] = (c & 0x1Fu) * 255u / 31u;
+}
+
+/* colour block (8 bytes) -> 16 texels of 4 bytes, texel t = y * 4 + x */
+static void or_bc1_block(const uint8_t *b, uint8_t tex[16][4]) {
+  unsigned c0 = (unsigned)b[0] | ((unsigned)b[1] << 8), c1 = (unsigned)b[2] | ((unsigned)b[3] << 8);
+  unsigned pal[4][4];
+  or_rgb565(c0, pal[0]);
+  or_rgb565(c1, pal[1]);
+  pal[0][3] = pal[1][3] = 255u;
+  for (int i = 0; i < 3; i++) {
+    if (c0 > c1) {
+      pal[2][i] = (2u * pal[0][i] + pal[1][i] + 1u) / 3u;
+      pal[3][i] = (pal[0][i] + 2u * pal[1][i] + 1u) / 3u;
+    } else {
+      pal[2][i] = (pal[0][i] + pal[1][i]) / 2u;
+      pal[3][i] = 0u;
+    }
+  }
+  pal[2][3] = 255u;
+  pal[3][3] = c0 > c1 ? 255u : 0u;
+  unsigned lut = (unsigned)b[4] | ((unsigned)b[5] << 8) | ((unsigned)b[6] << 16) |
+                 ((unsigned)b[7] << 24);
+  for (int t = 0; t < 16; t++)
+    for (int k = 0; k < 4; k++)
+      tex[t][k] = (uint8_t)pal[(lut >> (2 * t)) & 3u][k];
+}
+
+/* one-channel block (8 bytes) into channel ch of the 16 texels */
+static void or_bc4_block(const uint8_t *b, uint8_t tex[16][4], int ch) {
+  unsigned a0 = b[0], a1 = b[1], pal[8];
+  uint64_t bits = 0;
+  for (int i = 0; i < 6; i++)
+    bits |= (uint64_t)b[2 + i] << (8 * i);
+  pal[0] = a0;
+  pal[1] = a1;
+  if (a0 > a1) {
+    for (unsigned i = 1; i <= 6; i++)
+      pal[1 + i] = ((7u - i) * a0 + i * a1 + 3u) / 7u;
+  } else {
+    for (unsigned i = 1; i <= 4; i++)
+      pal[1 + i] = ((5u - i) * a0 + i * a1 + 2u) / 5u;
+    pal[6] = 0u;
+    pal[7] = 255u;
+  }
+  for (int t = 0; t < 16; t++)
+    tex[t][ch] = (uint8_t)pal[(bits >> (3 * t)) & 7u];
+}
+
+int oracle_bc_decode(int format, int w, int h, const uint8_t *blocks, uint8_t *out) {
+  if (format < 1 || format > 3 || w <= 0 || h <= 0)
+    return -1;
+  int bw = (w + 3) / 4, bh = (h + 3) / 4;
+  size_t bs = format == 1 ? 8 : 16;
+  for (int by = 0; by < bh; by++)
+    for (int bx = 0; bx < bw; bx++) {
+      const uint8_t *b = blocks + ((size_t)by * bw + bx) * bs;
+      uint8_t tex[16][4];
+      if (format == 1) {
+        or_bc1_block(b, tex);
+      } else if (format == 2) {
+        or_bc1_block(b + 8, tex);
+        or_bc4_block(b, tex, 3);
+      } else {
+        for (int t = 0; t < 16; t++) {
+          tex[t][0] = tex[t][1] = tex[t][2] = 0;
+          tex[t][3] = 255;
+        }
+        or_bc4_block(b, tex, 0);
+        or_bc4_block(b + 8, tex, 1);
+      }
+      for (int ty = 0; ty < 4 && by * 4 + ty < h; ty++)
+        for (int tx = 0; tx < 4 && bx * 4 + tx < w; tx++)
+          memcpy(out + (((size_t)(by * 4 + ty)) * w + bx * 4 + tx) * 4, tex[ty * 4 + tx], 4);
+    }
+  return 0;
+}

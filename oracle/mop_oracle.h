@@ -176,6 +176,12 @@ void oracle_morph_apply(const OrDeformLayout *l, const uint8_t *bind, uint32_t v
                         const float *targets, const float *weights, uint32_t target_count,
                         uint8_t *dst);
 
+/* bc_decompress_to_rgba8 (reference src/backend/cpu/cpu_backend.c:855-1014):
+ * a BC1 (format 1), BC3 (2) or BC5 (3) image of w x h texels, blocks in
+ * row-major order, decoded to RGBA8 (out: w * h * 4 bytes).  Returns 0, or -1
+ * for another format. */
+int oracle_bc_decode(int format, int w, int h, const uint8_t *blocks, uint8_t *out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -33,7 +33,20 @@ typedef struct RefH {
   uint32_t texture_count;
   int w, h, ssaa;
   int threads;
+  MopViewport *tex_vp;  /* owns the render target texture */
+  MopTexture *target;
+  bool cpu;             /* the viewport runs on the CPU backend */
 } RefH;
+
+/* The CPU backend's texture_create mallocs the texture record without
+ * clearing hdr_data (cpu_backend.c:811-827) and texture_destroy frees that
+ * field (:1064-1072), which faults once the heap hands back reused memory;
+ * the harness therefore leaves RGBA8 textures it made on the CPU backend
+ * alive (a test-sized leak) and destroys them on the CUDA backend. */
+static void harness_texture_release(RefH *h, MopViewport *vp, MopTexture *t) {
+  if (t && !h->cpu)
+    mop_viewport_destroy_texture(vp, t);
+}
 
 static int cmp_double(const void *a, const void *b);
 
@@ -112,13 +125,35 @@ void *refh_create(const RefScene *sc) {
   if (!h)
     return NULL;
   bool cpu = sc->backend == 0;
+  h->cpu = cpu;
   MopViewportDesc desc = {.width = sc->width,
                           .height = sc->height,
                           .backend = cpu ? MOP_BACKEND_CPU : (MopBackendType)sc->backend,
                           .reverse_z = false,
                           .ssaa_factor = sc->ssaa};
+  if (sc->render_target) {
+    /* the host-owned texture comes from another viewport of the backend */
+    MopViewportDesc td = desc;
+    td.width = td.height = 8;
+    td.ssaa_factor = 1;
+    h->tex_vp = mop_viewport_create(&td);
+    uint8_t *zero = calloc((size_t)sc->width * sc->height, 4);
+    if (h->tex_vp && zero)
+      h->target = mop_viewport_create_texture(h->tex_vp, sc->width, sc->height, zero);
+    free(zero);
+    if (!h->target) {
+      if (h->tex_vp)
+        mop_viewport_destroy(h->tex_vp);
+      free(h);
+      return NULL;
+    }
+    desc.render_target = h->target;
+  }
   h->vp = mop_viewport_create(&desc);
   if (!h->vp) {
+    harness_texture_release(h, h->tex_vp, h->target);
+    if (h->tex_vp)
+      mop_viewport_destroy(h->tex_vp);
     free(h);
     return NULL;
   }
@@ -197,9 +232,20 @@ void *refh_create(const RefScene *sc) {
   if (sc->texture_count) {
     h->textures = calloc(sc->texture_count, sizeof(MopTexture *));
     h->texture_count = sc->texture_count;
-    for (uint32_t t = 0; t < sc->texture_count; t++)
-      h->textures[t] = mop_viewport_create_texture(vp, sc->tex_w[t],
-                                                   sc->tex_h[t], sc->tex_data[t]);
+    for (uint32_t t = 0; t < sc->texture_count; t++) {
+      if (sc->tex_format && sc->tex_format[t] != 0) {
+        MopTextureDesc td = {.width = sc->tex_w[t],
+                             .height = sc->tex_h[t],
+                             .mip_levels = 1,
+                             .format = (MopTexFormat)sc->tex_format[t],
+                             .data = sc->tex_data[t],
+                             .data_size = sc->tex_bytes ? sc->tex_bytes[t] : 0};
+        h->textures[t] = mop_tex_create(vp, &td);
+      } else {
+        h->textures[t] = mop_viewport_create_texture(vp, sc->tex_w[t], sc->tex_h[t],
+                                                     sc->tex_data[t]);
+      }
+    }
   }
 
   for (uint32_t m = 0; m < sc->mesh_count; m++) {
@@ -453,7 +499,56 @@ void refh_destroy(void *hp) {
   /* Textures belong to the viewport and are released with it. */
   free(h->textures);
   mop_viewport_destroy(h->vp);
+  harness_texture_release(h, h->tex_vp, h->target);
+  if (h->tex_vp)
+    mop_viewport_destroy(h->tex_vp);
   free(h);
+}
+
+int refh_bc_decode(int backend, int format, int w, int h, const uint8_t *data, uint32_t size,
+                   uint8_t *out) {
+  const MopRhiBackend *rhi =
+      mop_rhi_get_backend(backend == 0 ? MOP_BACKEND_CPU : (MopBackendType)backend);
+  if (!rhi || !rhi->texture_create_ex || !rhi->texture_read_rgba8 || !data || !out)
+    return -1;
+  MopRhiDevice *dev = rhi->device_create();
+  if (!dev)
+    return -1;
+  int rc = -2;
+  MopRhiTexture *t = rhi->texture_create_ex(dev, w, h, format, 1, data, size);
+  if (t) {
+    rc = rhi->texture_read_rgba8(dev, t, out, (size_t)w * h * 4) ? 0 : -3;
+    /* not destroyed on the CPU backend (see harness_texture_release) */
+    if (backend != 0)
+      rhi->texture_destroy(dev, t);
+  }
+  rhi->device_destroy(dev);
+  return rc;
+}
+
+int refh_present_to_texture(void *hp, int tw, int th, uint8_t *out) {
+  RefH *h = hp;
+  if (!h || tw <= 0 || th <= 0 || !out)
+    return -1;
+  uint8_t *zero = calloc((size_t)tw * th, 4);
+  if (!zero)
+    return -1;
+  MopTexture *t = mop_viewport_create_texture(h->vp, tw, th, zero);
+  free(zero);
+  if (!t)
+    return -2;
+  int ok = mop_viewport_present_to_texture(h->vp, t) ? 1 : 0;
+  if (ok && !mop_tex_read_rgba8(h->vp, t, out, (size_t)tw * th * 4))
+    ok = -3;
+  harness_texture_release(h, h->vp, t);
+  return ok;
+}
+
+int refh_read_target(void *hp, uint8_t *out) {
+  RefH *h = hp;
+  if (!h || !h->target || !out)
+    return -1;
+  return mop_tex_read_rgba8(h->tex_vp, h->target, out, (size_t)h->w * h->h * 4) ? 0 : -2;
 }
 
 int refh_deform_probe(const uint8_t *vertices, uint32_t vertex_count, const float *bones,

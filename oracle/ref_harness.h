@@ -91,6 +91,15 @@ typedef struct RefScene {
   float fog_near, fog_far;
   uint32_t instanced_count;
   const RefInstanced *instanced;
+  /* per texture: MopTexFormat (0 RGBA8, 1 BC1, 2 BC3, 3 BC5) and the byte
+   * size of tex_data[t]; NULL: every texture is RGBA8.  Compressed textures
+   * are made with mop_tex_create (texture_create_ex). */
+  const int32_t *tex_format;
+  const uint32_t *tex_bytes;
+  /* 1: the viewport renders into a host texture (MopViewportDesc
+   * render_target, made through a helper viewport of the same backend);
+   * refh_read_target reads it back */
+  int32_t render_target;
 } RefScene;
 
 typedef struct RefFrame {
@@ -130,6 +139,17 @@ double refh_time_frames(void *h, int warm, int frames);
  * (sky generation + the three IBL precomputes, serial on the host). */
 double refh_time_environment(void *h, int reps);
 int refh_num_threads(void *h);
+/* The backend's texture_create_ex + texture_read_rgba8 of one image (backend
+ * 0: the CPU backend; 4 in the drop-in library: the CUDA backend): the
+ * decoded RGBA8 texels in out (w * h * 4).  0 on success. */
+int refh_bc_decode(int backend, int format, int w, int h, const uint8_t *data, uint32_t size,
+                   uint8_t *out);
+/* mop_viewport_present_to_texture into a new RGBA8 texture of tw x th, read
+ * back with mop_tex_read_rgba8.  Returns 1 when the present succeeded, 0 when
+ * the core refused it, negative on a harness error. */
+int refh_present_to_texture(void *h, int tw, int th, uint8_t *out);
+/* The render target's pixels after the last frame (render_target scenes). */
+int refh_read_target(void *h, uint8_t *out);
 void refh_destroy(void *h);
 
 /* Deformation probe: one mesh of vertex layout position float3 @0, normal

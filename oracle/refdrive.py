@@ -58,7 +58,8 @@ class RefScene(C.Structure):
                 ("backend", C.c_int32), ("fog_on", C.c_int32),
                 ("fog_color", C.c_float * 4), ("fog_near", C.c_float),
                 ("fog_far", C.c_float), ("instanced_count", C.c_uint32),
-                ("instanced", C.POINTER(RefInstanced))]
+                ("instanced", C.POINTER(RefInstanced)), ("tex_format", C.POINTER(C.c_int32)),
+                ("tex_bytes", C.POINTER(C.c_uint32)), ("render_target", C.c_int32)]
 
 
 class RefFrame(C.Structure):
@@ -117,6 +118,10 @@ def lib(kind: str = "cpu"):
         _lib.refh_time_environment.argtypes = [C.c_void_p, C.c_int]
         _lib.refh_num_threads.argtypes = [C.c_void_p]
         _lib.refh_destroy.argtypes = [C.c_void_p]
+        _lib.refh_bc_decode.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p,
+                                        C.c_uint32, C.c_void_p]
+        _lib.refh_present_to_texture.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_void_p]
+        _lib.refh_read_target.argtypes = [C.c_void_p, C.c_void_p]
         if hasattr(_lib, "refh_deform_probe"):
             _lib.refh_deform_probe.argtypes = [C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint32,
                                                C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p]
@@ -126,8 +131,12 @@ def lib(kind: str = "cpu"):
 class Reference:
     """A reference CPU-backend viewport holding one scene."""
 
-    def __init__(self, scene, serial: bool = True, workers: int = 0, backend: str = "cpu"):
+    def __init__(self, scene, serial: bool = True, workers: int = 0, backend: str = "cpu",
+                 render_target: bool = False):
+        """render_target: the viewport renders into a host texture
+        (MopViewportDesc.render_target), read back with read_target()."""
         L = self.L = lib(backend)
+        self.render_target = render_target
         self.scene = scene
         self._keep = []
         meshes = (RefMesh * max(1, len(scene.meshes)))()
@@ -155,7 +164,15 @@ class Reference:
         tw = (C.c_int32 * max(1, nt))()
         th = (C.c_int32 * max(1, nt))()
         td = (C.c_void_p * max(1, nt))()
+        tf = (C.c_int32 * max(1, nt))()
+        tb = (C.c_uint32 * max(1, nt))()
         for k, t in enumerate(scene.textures):
+            if hasattr(t, "format"):  # block-compressed (mop_tex_create)
+                d = np.ascontiguousarray(t.data, np.uint8)
+                self._keep.append(d)
+                th[k], tw[k], tf[k], tb[k] = t.height, t.width, t.format, d.size
+                td[k] = d.ctypes.data
+                continue
             t = np.ascontiguousarray(t, np.uint8)
             self._keep.append(t)
             th[k], tw[k] = t.shape[0], t.shape[1]
@@ -201,7 +218,9 @@ class Reference:
             ia[k].transforms, ia[k].instance_count = t.ctypes.data, t.shape[0]
         sc.instanced_count = len(inst)
         sc.instanced = ia
-        self._keep += [meshes, lights, tw, th, td, sc, ia]
+        sc.tex_format, sc.tex_bytes = tf, tb
+        sc.render_target = 1 if render_target else 0
+        self._keep += [meshes, lights, tw, th, td, tf, tb, sc, ia]
         self.h = L.refh_create(C.byref(sc))
         if not self.h:
             raise RuntimeError("refh_create failed")
@@ -228,6 +247,24 @@ class Reference:
         out["eye"] = np.array(f.eye[:], np.float32)
         out["triangle_count"] = f.triangle_count
         assert S == out["depth"].size
+        return out
+
+    def present_to_texture(self, tw: int, th: int):
+        """mop_viewport_present_to_texture into a new tw x th RGBA8 texture:
+        its pixels, or None when the core refused the present."""
+        out = np.zeros((th, tw, 4), np.uint8)
+        rc = self.L.refh_present_to_texture(self.h, tw, th, out.ctypes.data)
+        if rc < 0:
+            raise RuntimeError(f"refh_present_to_texture failed: {rc}")
+        return out if rc == 1 else None
+
+    def read_target(self):
+        """The render target texture's pixels (render_target viewports)."""
+        s = self.scene
+        out = np.zeros((s.height, s.width, 4), np.uint8)
+        rc = self.L.refh_read_target(self.h, out.ctypes.data)
+        if rc != 0:
+            raise RuntimeError(f"refh_read_target failed: {rc}")
         return out
 
     def pick(self, xy: np.ndarray):
@@ -339,3 +376,16 @@ def scene_file_mesh(path, idx: int, vcap: int = 1 << 22, icap: int = 1 << 24):
 def time_scene_file(path, reps: int = 3) -> float:
     """Median ms of the reference's mop_scene_load + every mop_scene_get_mesh."""
     return lib().refh_time_scene_file(str(path).encode(), reps)
+
+
+def bc_decode(t, backend: str = "cpu"):
+    """A scenes.CompressedTexture through the backend's texture_create_ex and
+    texture_read_rgba8 (the reference CPU backend, or the CUDA backend's RHI
+    table in the drop-in library): RGBA8 [h, w, 4], or None when the backend
+    refuses the format."""
+    L = lib(backend)
+    out = np.zeros((t.height, t.width, 4), np.uint8)
+    d = np.ascontiguousarray(t.data, np.uint8)
+    rc = L.refh_bc_decode(0 if backend == "cpu" else BACKEND_CUDA, t.format, t.width, t.height,
+                          d.ctypes.data, d.size, out.ctypes.data)
+    return out if rc == 0 else None

@@ -67,6 +67,8 @@ CASES = {
     "instanced_transparent": lambda: scenes.instanced_scene(seed=67, transparent=True),
     # meshes with editor-chrome IDs: the core draws them with the depth test off
     "chrome": lambda: scenes.chrome_scene(seed=68),
+    # BC1 / BC3 / BC5 textures through mop_tex_create -> texture_create_ex
+    "bc_textures": lambda: scenes.bc_scene(seed=69),
     "config2_reduced_no_ibl": lambda: dataclasses.replace(
         scenes.config2(width=480, height=270, ssaa=2, instances=48, tex_size=64), env=0),
 }
@@ -92,6 +94,55 @@ def test_viewport_api_cuda_matches_cpu(name):
         for x, y in zip(cpu.pick(xy), gpu.pick(xy)):
             assert (np.ascontiguousarray(x).view(np.uint8) ==
                     np.ascontiguousarray(y).view(np.uint8)).all()
+    finally:
+        gpu.close()
+        cpu.close()
+
+
+@pytest.mark.parametrize("ssaa", [1, 2])
+def test_present_to_texture_cuda_matches_cpu(ssaa):
+    """mop_viewport_present_to_texture (framebuffer_copy_to_texture): into a
+    texture of the framebuffer's size and, with SSAA, of the presented size
+    (the box filter); a texture of another size is refused by both
+    backends."""
+    if not refdrive.REF_CUDA_SO.exists():
+        pytest.skip("drop-in harness library not built")
+    sc = scenes.small_scene(seed=70 + ssaa, width=160, height=120, ssaa=ssaa)
+    cpu = refdrive.Reference(sc, serial=True)
+    gpu = refdrive.Reference(sc, backend="cuda")
+    try:
+        a, b = cpu.render(), gpu.render()
+        sizes = [(sc.width * ssaa, sc.height * ssaa)] + ([(sc.width, sc.height)] if ssaa > 1 else [])
+        for tw, th in sizes:
+            ta, tb = cpu.present_to_texture(tw, th), gpu.present_to_texture(tw, th)
+            assert ta is not None and tb is not None
+            s_ = color_stats(ta, tb)
+            assert s_["max"] <= COLOR_MAX_LSB and s_["within1"] >= COLOR_1LSB_FRACTION, (tw, s_)
+            key = "color_full" if tw == sc.width * ssaa else "color"
+            assert (tb == b[key]).all()
+        assert cpu.present_to_texture(sc.width + 3, sc.height) is None
+        assert gpu.present_to_texture(sc.width + 3, sc.height) is None
+    finally:
+        gpu.close()
+        cpu.close()
+
+
+def test_render_target_cuda_matches_cpu():
+    """MopViewportDesc.render_target (framebuffer_create_from_texture): the
+    viewport renders into a host texture; after each frame its pixels equal
+    the frame's colour, on both backends."""
+    if not refdrive.REF_CUDA_SO.exists():
+        pytest.skip("drop-in harness library not built")
+    sc = scenes.small_scene(seed=73, width=160, height=120, ssaa=1)
+    cpu = refdrive.Reference(sc, serial=True, render_target=True)
+    gpu = refdrive.Reference(sc, backend="cuda", render_target=True)
+    try:
+        a, b = cpu.render(), gpu.render()
+        ta, tb = cpu.read_target(), gpu.read_target()
+        assert (ta == a["color_full"]).all() and (tb == b["color_full"]).all()
+        s_ = color_stats(ta, tb)
+        assert s_["max"] <= COLOR_MAX_LSB and s_["within1"] >= COLOR_1LSB_FRACTION, s_
+        assert (a["object_id"] == b["object_id"]).all()
     finally:
         gpu.close()
         cpu.close()

@@ -103,6 +103,8 @@ LIVE = {
     "chrome": lambda: scenes.chrome_scene(seed=81),
     "chrome_ssaa2_flat": lambda: dataclasses.replace(scenes.chrome_scene(seed=82, ssaa=2),
                                                      smooth=False),
+    # BC1 / BC3 / BC5 textures made through mop_tex_create (texture_create_ex)
+    "bc_textures": lambda: scenes.bc_scene(seed=91),
 }
 
 
@@ -175,3 +177,23 @@ def test_reference_suite_on_its_cpu_backend(suite):
         pytest.skip("reference test programs not built (reference tree absent at build time)")
     p = subprocess.run([str(exe)], capture_output=True, text=True, timeout=300)
     assert p.returncode == 0 and "FAIL" not in p.stdout, p.stdout[-3000:]
+
+
+@pytest.mark.skipif(not refdrive.available(), reason="reference library not built")
+@pytest.mark.parametrize("fmt,w,h", [(scenes.TEX_BC1, 8, 8), (scenes.TEX_BC1, 13, 7),
+                                     (scenes.TEX_BC3, 64, 36), (scenes.TEX_BC3, 5, 5),
+                                     (scenes.TEX_BC5, 33, 70), (scenes.TEX_BC5, 1, 1)])
+def test_bc_decode_matches_reference(fmt, w, h):
+    """The oracle's block decode equals the CPU backend's texture_create_ex
+    (read back through texture_read_rgba8), texel for texel, including the
+    clamped last block row and column of odd sizes."""
+    t = scenes.bc_texture(np.random.default_rng(100 * fmt + w), fmt, w, h)
+    want = refdrive.bc_decode(t)
+    assert want is not None
+    assert (cpu_oracle.bc_decode(t) == want).all()
+
+
+@pytest.mark.skipif(not refdrive.available(), reason="reference library not built")
+def test_bc7_refused_by_reference():
+    t = scenes.bc_texture(np.random.default_rng(7), scenes.TEX_BC7, 8, 8)
+    assert refdrive.bc_decode(t) is None
