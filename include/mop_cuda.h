@@ -341,6 +341,27 @@ int mopcuda_draw(MopCudaDevice *dev, MopCudaFramebuffer *fb, const MopCudaDraw *
  * array; stops at the first draw that fails). */
 int mopcuda_draw_list(MopCudaDevice *dev, MopCudaFramebuffer *fb, const MopCudaDraw *draws,
                       uint32_t n);
+/* The environment background of the frame being recorded
+ * (pass_background_hdri_cpu, reference viewport.c:2128-2177, which the core
+ * runs on the CPU backend for an HDRI or procedural-sky environment with
+ * mop_viewport_set_environment_background on): every sample the draws leave
+ * uncovered shows the RGBA32F environment texture `env` (equirectangular)
+ * along the ray through the sample, times intensity, resolved as background
+ * (no ACES); blended draws composite over it.  eye/target/up/fov_deg are the
+ * camera as the viewport holds it for the frame (after its orbit update); the
+ * ray setup (forward, right, up, tan of half the fov) is the core's, computed
+ * with the same float operations.  Call between frame_begin and frame_end. */
+int mopcuda_draw_background(MopCudaDevice *dev, MopCudaFramebuffer *fb,
+                            const MopCudaTexture *env, const float eye[3], const float target[3],
+                            const float up[3], float fov_deg, float rotation, float intensity);
+/* draw_skybox (rhi.h:285-293): the same background from the inverse
+ * view-projection and camera position the core hands GPU backends
+ * (viewport.c:2209-2218); the ray setup is recovered from the far-plane
+ * points at ndc (0,0), (1,0), (0,1), so rays match the core's to float
+ * rounding rather than bit for bit. */
+int mopcuda_draw_skybox(MopCudaDevice *dev, MopCudaFramebuffer *fb, const MopCudaTexture *env,
+                        const float inv_vp[16], const float cam_pos[3], float rotation,
+                        float intensity);
 /* view/projection multiply per instance as cpu_draw_instanced does
  * (mvp = P * (V * instance), cpu_backend.c:638-657). */
 int mopcuda_draw_instanced(MopCudaDevice *dev, MopCudaFramebuffer *fb, const MopCudaDraw *draw,
@@ -612,6 +633,12 @@ void mopcuda_mat4_compose_trs(const float position[3], const float rotation[3],
 void mopcuda_camera_matrices(const float eye[3], const float target[3], const float up[3],
                              float fov_deg, float near_plane, float far_plane, int width,
                              int height, float view[16], float proj[16], float eye_out[3]);
+/* The eye and up vector a frame uses for a camera set with eye/target/up:
+ * the orbit parameters mop_viewport_set_camera stores (viewport.c:1079-1091)
+ * re-applied as mop_viewport_render does (what mopcuda_draw_background wants
+ * when the caller has no viewport core). */
+void mopcuda_camera_orbit(const float eye[3], const float target[3], const float up[3],
+                          float eye_out[3], float up_out[3]);
 /* The shadow pass's light view-projection (viewport.c:2303-2427): a scene
  * box from the casters' world transforms (translation +- 1.5 x the largest
  * column length), an orthographic light camera looking along `direction`

@@ -132,6 +132,15 @@ struct MopCudaFramebuffer {
   MopCudaTexture *target = nullptr;
 };
 
+/* A frame's environment background: the environment texture and the ray
+ * setup of pass_background_hdri_cpu (viewport.c:2128-2177). */
+struct SkyState {
+  bool on = false;
+  const MopCudaTexture *env = nullptr;
+  float fwd[3] = {0, 0, 0}, right[3] = {0, 0, 0}, up[3] = {0, 0, 0};
+  float half_w = 0, half_h = 0, rotation = 0, intensity = 1;
+};
+
 struct MopCudaDevice {
   int ordinal = 0;
   int num_sms = 148;
@@ -171,6 +180,7 @@ struct MopCudaDevice {
   uint32_t post = MOPCUDA_POST_GAMMA | MOPCUDA_POST_FXAA;
   float lut[256];
   float fog[6] = {0, 0, 0, 0, 0, 0}; /* MopFogParams: colour RGBA, near, far */
+  SkyState rec_sky, sky; /* background of the frame being recorded / launched */
   /* IBL */
   DevArena irr, pf, brdf;
   int irr_w = 0, irr_h = 0, pf_w = 0, pf_h = 0, pf_levels = 0, brdf_size = 0;

@@ -122,17 +122,16 @@ static void look_at(v3 e, v3 t, v3 u, float view[16]) {
   E(view, 2, 3) = dot(f, e);
 }
 
-void mopcuda_camera_matrices(const float eye[3], const float target[3], const float up[3],
-                             float fov_deg, float near_plane, float far_plane, int width,
-                             int height, float view[16], float proj[16], float eye_out[3]) {
-  if (!eye || !target || !up || !view || !proj || !eye_out)
-    return;
+/* The orbit parameters mop_viewport_set_camera recovers from eye and
+ * target (viewport.c:1079-1091), re-applied by mop_viewport_render: the eye
+ * and up vector the frame uses. */
+static void orbit(const float eye[3], const float target[3], const float up[3], v3 *e_out,
+                  v3 *u_out) {
   v3 e = {eye[0], eye[1], eye[2]}, t = {target[0], target[1], target[2]};
   v3 u = {up[0], up[1], up[2]};
   v3 off = {e.x - t.x, e.y - t.y, e.z - t.z};
   float dist = sqrtf(off.x * off.x + off.y * off.y + off.z * off.z);
   if (dist > 1e-6f) {
-    /* orbit parameters recovered by set_camera, re-applied by render */
     float yaw = atan2f(off.x, off.z);
     float pitch = asinf(off.y / dist);
     float sp = sinf(pitch), cp = cosf(pitch), sy = sinf(yaw), cy = cosf(yaw);
@@ -143,6 +142,32 @@ void mopcuda_camera_matrices(const float eye[3], const float target[3], const fl
              t.z + dist * cp2 * cosf(yaw)};
     e = oe;
   }
+  *e_out = e;
+  *u_out = u;
+}
+
+void mopcuda_camera_orbit(const float eye[3], const float target[3], const float up[3],
+                          float eye_out[3], float up_out[3]) {
+  if (!eye || !target || !up || !eye_out || !up_out)
+    return;
+  v3 e, u;
+  orbit(eye, target, up, &e, &u);
+  eye_out[0] = e.x;
+  eye_out[1] = e.y;
+  eye_out[2] = e.z;
+  up_out[0] = u.x;
+  up_out[1] = u.y;
+  up_out[2] = u.z;
+}
+
+void mopcuda_camera_matrices(const float eye[3], const float target[3], const float up[3],
+                             float fov_deg, float near_plane, float far_plane, int width,
+                             int height, float view[16], float proj[16], float eye_out[3]) {
+  if (!eye || !target || !up || !view || !proj || !eye_out)
+    return;
+  v3 t = {target[0], target[1], target[2]};
+  v3 e, u;
+  orbit(eye, target, up, &e, &u);
   look_at(e, t, u, view);
   float fov = fov_deg * (3.14159265358979323846f / 180.0f);
   float aspect = (float)width / (float)height;

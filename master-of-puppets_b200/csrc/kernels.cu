@@ -1131,6 +1131,56 @@ __device__ __forceinline__ float aces(float x) { /* rasterizer.c:2770-2774 */
   return m < 0.0f ? 0.0f : (m > 1.0f ? 1.0f : m);
 }
 
+/* The environment background's HDR colour at sample (x, y)
+ * (pass_background_hdri_cpu, viewport.c:2145-2175): the ray through the
+ * sample centre, normalised with divisions, to equirectangular (u, v) with
+ * atan2f / asinf (CUDA's; glibc's differ in the last ulp for some inputs, as
+ * in the IBL lookups), a bilinear sample (env_sample_bilinear, :2099-2124)
+ * times the intensity. */
+__device__ __noinline__ void sky_hdr(const FrameArgs &a, int x, int y, float out[3]) {
+  const float ndc_y = 1.0f - 2.0f * ((float)y + 0.5f) / (float)a.height;
+  const float ndc_x = 2.0f * ((float)x + 0.5f) / (float)a.width - 1.0f;
+  float d[3];
+  for (int c = 0; c < 3; c++)
+    d[c] = a.sky_fwd[c] + a.sky_right[c] * ndc_x * a.sky_half_w + a.sky_up[c] * ndc_y * a.sky_half_h;
+  const float len = sqrtf(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+  d[0] /= len;
+  d[1] /= len;
+  d[2] /= len;
+  const float pi = 3.14159265358979f;
+  const float phi = atan2f(d[2], d[0]) - a.sky_rotation;
+  const float cdy = d[1] < -1.0f ? -1.0f : (d[1] > 1.0f ? 1.0f : d[1]);
+  const float theta = asinf(cdy);
+  float u = phi / (2.0f * pi) + 0.5f, v = theta / pi + 0.5f;
+  u = u - floorf(u);
+  v = v - floorf(v);
+  const int w = a.sky_w, h = a.sky_h;
+  const float fx = u * (float)(w - 1), fy = v * (float)(h - 1);
+  int x0 = (int)fx, y0 = (int)fy;
+  x0 = x0 < 0 ? 0 : (x0 > w - 1 ? w - 1 : x0); /* u, v in [0, 1): already inside */
+  y0 = y0 < 0 ? 0 : (y0 > h - 1 ? h - 1 : y0);
+  const int x1 = (x0 + 1) % w, y1 = y0 + 1 < h ? y0 + 1 : h - 1;
+  const float sx = fx - (float)x0, sy = fy - (float)y0;
+  const float4 p00 = __ldg(a.sky + (size_t)y0 * w + x0), p10 = __ldg(a.sky + (size_t)y0 * w + x1);
+  const float4 p01 = __ldg(a.sky + (size_t)y1 * w + x0), p11 = __ldg(a.sky + (size_t)y1 * w + x1);
+  const float q00[3] = {p00.x, p00.y, p00.z}, q10[3] = {p10.x, p10.y, p10.z};
+  const float q01[3] = {p01.x, p01.y, p01.z}, q11[3] = {p11.x, p11.y, p11.z};
+  for (int c = 0; c < 3; c++) {
+    const float top = q00[c] * (1.0f - sx) + q10[c] * sx;
+    const float bot = q01[c] * (1.0f - sx) + q11[c] * sx;
+    out[c] = (top * (1.0f - sy) + bot * sy) * a.sky_intensity;
+  }
+}
+
+/* The background sample's resolved colour (id 0: no ACES, rasterizer.c:2785-2792). */
+__device__ __forceinline__ uchar4 sky_resolved(const FrameArgs &a, uint32_t i) {
+  float h[3];
+  sky_hdr(a, (int)(i % (uint32_t)a.width), (int)(i / (uint32_t)a.width), h);
+  return make_uchar4(x86_f2u8(fminf(h[0], 1.0f) * 255.0f + 0.5f),
+                     x86_f2u8(fminf(h[1], 1.0f) * 255.0f + 0.5f),
+                     x86_f2u8(fminf(h[2], 1.0f) * 255.0f + 0.5f), 255);
+}
+
 /* Writes the background (clear colour resolved with id 0 and depth 1,
  * rasterizer.c:2785-2792) to every sample with 16-byte stores — k_shade
  * overwrites the covered ones — and queues covered samples for shading in
@@ -1201,6 +1251,12 @@ __device__ __forceinline__ void resolve_chunk_keys(const FrameArgs &a, uint32_t 
         }
       }
     }
+    if (a.sky) /* the environment background replaces the clear colour */
+      for (int k = 0; k < RESOLVE_PER_THREAD; k++) {
+        const uint32_t i = i0 + (uint32_t)k;
+        if (i < S && !((mask >> k) & 1u))
+          a.pre[i] = sky_resolved(a, i);
+      }
     const uint32_t c = (uint32_t)__popc(mask);
     uint32_t incl = c;
     for (int o = 1; o < 32; o <<= 1) {
@@ -1256,6 +1312,48 @@ __global__ void __launch_bounds__(256) k_resolve(FrameArgs a) {
       resolve_load_keys(a, blk + stride, nk);
     resolve_chunk_keys(a, blk, ck, s_warp, &s_base);
   }
+}
+
+/* The three edge values after k sequential additions of their increments
+ * (fold_add for each edge).  Short folds (k <= FOLD_SERIAL_MAX) step the
+ * first two edges as one paired add (__fadd2_rn: two IEEE round-to-nearest
+ * single additions in one instruction) and the third alone, for as many
+ * steps as the longest short fold among the warp's converged lanes, each
+ * lane's steps past its own k predicated off; longer folds take the
+ * binade-skipping path per edge. */
+__device__ __forceinline__ void fold3(float w[3], const float d[3], int k) {
+  if (k <= FOLD_SERIAL_MAX) {
+    const int km = (int)__reduce_max_sync(__activemask(), (unsigned)k);
+    float2 p = make_float2(w[0], w[1]);
+    const float2 dp = make_float2(d[0], d[1]);
+    float q = w[2];
+#pragma unroll
+    for (int i = 0; i < FOLD_SERIAL_MAX; i++) {
+      if (i >= km)
+        break;
+      if (i < k) {
+        p = __fadd2_rn(p, dp);
+        q = __fadd_rn(q, d[2]);
+      }
+    }
+    w[0] = p.x;
+    w[1] = p.y;
+    w[2] = q;
+  } else {
+    for (int e = 0; e < 3; e++)
+      w[e] = fold_add_long(w[e], d[e], k);
+  }
+}
+
+/* Edge values of record r at row jr, column kc of its bbox: the row fold
+ * from the corner, then the column fold along the row, as the reference
+ * steps them. */
+__device__ __forceinline__ void fold_rec(const RasterRec &r, int jr, int kc, float w[3]) {
+  w[0] = r.w0[0];
+  w[1] = r.w0[1];
+  w[2] = r.w0[2];
+  fold3(w, r.dy, jr);
+  fold3(w, r.dx, kc);
 }
 
 /* Deferred shading of one covered sample: the winning record's exact edge
@@ -1319,8 +1417,7 @@ __device__ __forceinline__ void shade_item(const FrameArgs &a, uint32_t j, const
       hdr[2] = s.col[2];
     } else {
       float w[3];
-      for (int e = 0; e < 3; e++)
-        w[e] = fold_add(fold_add(r.w0[e], r.dy[e], jr), r.dx[e], kc);
+      fold_rec(r, jr, kc, w);
       float b0 = w[0] * r.inv_area, b1 = w[1] * r.inv_area, b2 = w[2] * r.inv_area;
       depth = b0 * r.zc[0] + b1 * r.zc[1] + b2 * r.zc[2];
       if (a.no_color || s.v[0] >= a.vertex_cap || s.v[1] >= a.vertex_cap ||
@@ -2001,6 +2098,8 @@ __global__ void __launch_bounds__(128) k_ofold(FrameArgs a) {
       hdr[0] = h.x;
       hdr[1] = h.y;
       hdr[2] = h.z;
+    } else if (a.sky) {
+      sky_hdr(a, x, y, hdr);
     } else {
       hdr[0] = a.clear[0];
       hdr[1] = a.clear[1];

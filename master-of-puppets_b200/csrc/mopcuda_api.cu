@@ -602,8 +602,111 @@ extern "C" int mopcuda_frame_begin(MopCudaDevice *d, MopCudaFramebuffer *fb, con
   d->rec_unsupported = 0;
   d->rec_skipped = 0;
   d->rec_ordered_from = UINT32_MAX;
+  d->rec_sky = SkyState();
   d->frame_open = true;
   return MOPCUDA_OK;
+}
+
+/* Host float helpers for the background's ray setup: the reference's
+ * mop_vec3_* operations (math.c:17-50), without contraction. */
+static void h_norm3(const float a[3], float o[3]) {
+  volatile float l = sqrtf(a[0] * a[0] + a[1] * a[1] + a[2] * a[2]);
+  if (l < 1e-8f) {
+    o[0] = o[1] = o[2] = 0.0f;
+    return;
+  }
+  volatile float inv = 1.0f / l;
+  o[0] = a[0] * inv;
+  o[1] = a[1] * inv;
+  o[2] = a[2] * inv;
+}
+static void h_cross3(const float a[3], const float b[3], float o[3]) {
+  o[0] = a[1] * b[2] - a[2] * b[1];
+  o[1] = a[2] * b[0] - a[0] * b[2];
+  o[2] = a[0] * b[1] - a[1] * b[0];
+}
+
+static int record_sky(MopCudaDevice *d, MopCudaFramebuffer *fb, const MopCudaTexture *env,
+                      const SkyState &s) {
+  if (!env || !env->hdr || !env->d)
+    return fail(MOPCUDA_EINVAL, "background: the environment must be an HDR (RGBA32F) texture");
+  if (!d->frame_open || d->rec_fb != fb)
+    return fail(MOPCUDA_EINVAL, "background outside frame_begin/frame_end");
+  d->rec_sky = s;
+  d->rec_sky.env = env;
+  d->rec_sky.on = true;
+  return MOPCUDA_OK;
+}
+
+extern "C" int mopcuda_draw_background(MopCudaDevice *d, MopCudaFramebuffer *fb,
+                                       const MopCudaTexture *env, const float eye[3],
+                                       const float target[3], const float up[3], float fov_deg,
+                                       float rotation, float intensity) {
+  if (!d || !fb || !eye || !target || !up)
+    return fail(MOPCUDA_EINVAL, "draw_background: bad arguments");
+  std::lock_guard<std::mutex> lk(d->mu);
+  /* pass_background_hdri_cpu's camera basis (viewport.c:2133-2143), the
+   * same float operations in the same order */
+  SkyState s;
+  volatile float fov = fov_deg * (3.14159265358979323846f / 180.0f);
+  volatile float aspect = (float)fb->w / (float)fb->h;
+  volatile float half_h = tanf(fov * 0.5f);
+  s.half_h = half_h;
+  s.half_w = half_h * aspect;
+  const float f_raw[3] = {target[0] - eye[0], target[1] - eye[1], target[2] - eye[2]};
+  h_norm3(f_raw, s.fwd);
+  float r_raw[3];
+  h_cross3(s.fwd, up, r_raw);
+  h_norm3(r_raw, s.right);
+  h_cross3(s.right, s.fwd, s.up);
+  s.rotation = rotation;
+  s.intensity = intensity;
+  return record_sky(d, fb, env, s);
+}
+
+extern "C" int mopcuda_draw_skybox(MopCudaDevice *d, MopCudaFramebuffer *fb,
+                                   const MopCudaTexture *env, const float inv_vp[16],
+                                   const float cam_pos[3], float rotation, float intensity) {
+  if (!d || !fb || !inv_vp || !cam_pos)
+    return fail(MOPCUDA_EINVAL, "draw_skybox: bad arguments");
+  std::lock_guard<std::mutex> lk(d->mu);
+  /* points of the far plane at ndc (0,0), (1,0), (0,1) through the inverse
+   * view-projection give the ray setup: the centre ray D * fwd, and
+   * D * right * half_w, D * up * half_h for the unit steps in ndc */
+  double p[3][3];
+  const double ndc[3][2] = {{0, 0}, {1, 0}, {0, 1}};
+  for (int k = 0; k < 3; k++) {
+    double v[4];
+    for (int r = 0; r < 4; r++)
+      v[r] = (double)inv_vp[r] * ndc[k][0] + (double)inv_vp[4 + r] * ndc[k][1] +
+             (double)inv_vp[8 + r] + (double)inv_vp[12 + r];
+    if (v[3] == 0.0)
+      return fail(MOPCUDA_EINVAL, "draw_skybox: inverse view-projection maps ndc to infinity");
+    for (int c = 0; c < 3; c++)
+      p[k][c] = v[c] / v[3];
+  }
+  double c0[3], dr[3], du[3];
+  for (int c = 0; c < 3; c++) {
+    c0[c] = p[0][c] - cam_pos[c];
+    dr[c] = p[1][c] - p[0][c];
+    du[c] = p[2][c] - p[0][c];
+  }
+  const double dist = sqrt(c0[0] * c0[0] + c0[1] * c0[1] + c0[2] * c0[2]);
+  const double lr = sqrt(dr[0] * dr[0] + dr[1] * dr[1] + dr[2] * dr[2]);
+  const double lu = sqrt(du[0] * du[0] + du[1] * du[1] + du[2] * du[2]);
+  if (!(dist > 0.0) || !(lr > 0.0) || !(lu > 0.0))
+    return fail(MOPCUDA_EINVAL, "draw_skybox: degenerate inverse view-projection");
+  SkyState s;
+  for (int c = 0; c < 3; c++) {
+    s.fwd[c] = (float)(c0[c] / dist);
+    s.right[c] = (float)(dr[c] / lr);
+    s.up[c] = (float)(du[c] / lu);
+  }
+  s.half_w = (float)(lr / dist);
+  s.half_h = (float)(lu / dist);
+  s.rotation = rotation;
+  s.intensity = intensity;
+  return record_sky(d, fb, env, s);
 }
 
 static float clamp01f(float x) { return x < 0.0f ? 0.0f : (x > 1.0f ? 1.0f : x); }
@@ -1058,6 +1161,19 @@ static int launch_frame(MopCudaDevice *d) {
   a.pre = fb->pre.as<uchar4>();
   a.depth = fb->depth.as<float>();
   a.ids = fb->ids.as<uint32_t>();
+  if (d->sky.on) {
+    const SkyState &k = d->sky;
+    a.sky = (const float4 *)k.env->d;
+    a.sky_w = k.env->w;
+    a.sky_h = k.env->h;
+    memcpy(a.sky_fwd, k.fwd, sizeof a.sky_fwd);
+    memcpy(a.sky_right, k.right, sizeof a.sky_right);
+    memcpy(a.sky_up, k.up, sizeof a.sky_up);
+    a.sky_half_w = k.half_w;
+    a.sky_half_h = k.half_h;
+    a.sky_rotation = k.rotation;
+    a.sky_intensity = k.intensity;
+  }
   a.small_side = d->cfg.small_side;
   a.small_area = d->cfg.small_area;
   if (ordered) {
@@ -1208,6 +1324,7 @@ extern "C" int mopcuda_frame_end(MopCudaDevice *d, MopCudaFramebuffer *fb) {
   d->unsupported_draws = d->rec_unsupported;
   d->skipped_draws = d->rec_skipped;
   d->ordered_from = d->rec_ordered_from;
+  d->sky = d->rec_sky;
   d->fr_sh = d->sh_bound ? d->sh_cur : -1;
   d->fr_sh_size = d->sh_size;
   rc = launch_frame(d);

@@ -199,6 +199,14 @@ struct FrameArgs {
   uint32_t *olist;        /* live records of the suffix                          */
   uint32_t *olist_items;  /* their (row, chunk) item counts, then offsets        */
   uint32_t olist_cap;
+  /* environment background (pass_background_hdri_cpu): every uncovered
+   * sample shows the RGBA32F environment (sky_w x sky_h) along the ray
+   * sky_fwd + sky_right * ndc_x * sky_half_w + sky_up * ndc_y * sky_half_h,
+   * times sky_intensity; null: the clear colour */
+  const float4 *sky;
+  int sky_w, sky_h;
+  float sky_fwd[3], sky_right[3], sky_up[3];
+  float sky_half_w, sky_half_h, sky_rotation, sky_intensity;
   /* the suffix holds a depth-test-off draw: its fragments pass whatever the
    * depth, and later ones may pass where the opaque depth is nearer, so
    * every covered fragment of the suffix is kept */

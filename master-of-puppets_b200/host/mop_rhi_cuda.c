@@ -7,8 +7,8 @@
  * (frame_submit, frame_gpu_time_ms, set_exposure, set_ibl_textures,
  * texture_read_rgba8, frame_wait_readback, texture_create_ex with BC1/3/5
  * decoded on the device, framebuffer_copy_to_texture and
- * framebuffer_create_from_texture for render-to-texture).  GPU-only effect
- * hooks stay NULL
+ * framebuffer_create_from_texture for render-to-texture, draw_skybox for the
+ * environment background).  GPU-only effect hooks stay NULL
  * exactly as the CPU table leaves them (every caller NULL-guards them,
  * rhi.h:112-130).
  *
@@ -218,6 +218,12 @@ static void cu_draw(MopRhiDevice *d, MopRhiFramebuffer *fb, const MopRhiDrawCall
     mopcuda_draw(d->cu, FB(fb), &dc);
 }
 
+static void cu_draw_skybox(MopRhiDevice *d, MopRhiFramebuffer *fb, MopRhiTexture *env,
+                           const float *inv_vp, const float *cam_pos, float rotation,
+                           float intensity) {
+  mopcuda_draw_skybox(d->cu, FB(fb), TEX(env), inv_vp, cam_pos, rotation, intensity);
+}
+
 static void cu_draw_instanced(MopRhiDevice *d, MopRhiFramebuffer *fb, const MopRhiDrawCall *c,
                               const MopMat4 *inst, uint32_t n) {
   if (!c || !inst || n == 0)
@@ -319,6 +325,7 @@ static const MopRhiBackend CUDA_BACKEND = {
     .texture_create_ex = cu_texture_create_ex,
     .texture_destroy = cu_texture_destroy,
     .draw_instanced = cu_draw_instanced,
+    .draw_skybox = cu_draw_skybox,
     .buffer_update = cu_buffer_update,
     .buffer_read = cu_buffer_read,
     .frame_gpu_time_ms = cu_frame_gpu_time_ms,

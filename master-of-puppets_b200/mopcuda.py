@@ -167,6 +167,9 @@ SIGNATURES = [
     ("mopcuda_draw", C.c_int, [_P, _P, C.POINTER(MopCudaDraw)]),
     ("mopcuda_draw_list", C.c_int, [_P, _P, _P, C.c_uint32]),
     ("mopcuda_draw_instanced", C.c_int, [_P, _P, C.POINTER(MopCudaDraw), _P, _P, _P, C.c_uint32]),
+    ("mopcuda_draw_background", C.c_int, [_P, _P, _P, _P, _P, _P, C.c_float, C.c_float,
+                                          C.c_float]),
+    ("mopcuda_draw_skybox", C.c_int, [_P, _P, _P, _P, _P, C.c_float, C.c_float]),
     ("mopcuda_frame_end", C.c_int, [_P, _P]),
     ("mopcuda_frame_wait", C.c_int, [_P, C.c_int]),
     ("mopcuda_frame_gpu_time_ms", C.c_float, [_P]),
@@ -220,6 +223,7 @@ SIGNATURES = [
     ("mopcuda_mat4_compose_trs", None, [_P, _P, _P, _P]),
     ("mopcuda_camera_matrices", None, [_P, _P, _P, C.c_float, C.c_float, C.c_float, C.c_int,
                                        C.c_int, _P, _P, _P]),
+    ("mopcuda_camera_orbit", None, [_P, _P, _P, _P, _P]),
     ("mopcuda_shadow_light_vp", C.c_int, [_P, C.c_uint32, _P, _P]),
 ]
 
@@ -429,6 +433,17 @@ class _Resident:
             if not th:
                 raise RuntimeError(f"texture_create failed: {last_error()}")
             self.textures.append(th)
+        # environment background (mop_viewport_set_environment_background): the
+        # environment map as an HDR texture, drawn behind every frame
+        self.env_tex = None
+        if getattr(scene, "env_background", False) and ibl is not None and "env" in ibl:
+            env = _f32(ibl["env"])
+            self._env = env
+            self.env_tex = L.mopcuda_texture_create_hdr(d, env.shape[1], env.shape[0],
+                                                        env.ctypes.data)
+            if not self.env_tex:
+                raise RuntimeError(f"texture_create_hdr failed: {last_error()}")
+            self.textures.append(self.env_tex)
         L.mopcuda_set_exposure(d, scene.exposure)
         L.mopcuda_set_post_effects(d, scene.post_effects)
         # mop_viewport_set_fog; a scene without fog keeps a new viewport's zeros
@@ -567,6 +582,13 @@ class SceneRenderer(_Resident):
                       for k in scenes.draw_order(self.scene, self.eye)]
         self.draw_array = (MopCudaDraw * max(1, len(self.draws)))(*self.draws)
         self.inst_draws = [self.instanced_struct(k) for k in range(len(self.instanced))]
+        sc = self.scene
+        self._orbit_eye = np.zeros(3, np.float32)
+        self._orbit_up = np.zeros(3, np.float32)
+        self.L.mopcuda_camera_orbit(_f32(sc.eye).ctypes.data, _f32(sc.target).ctypes.data,
+                                    _f32(sc.up).ctypes.data, self._orbit_eye.ctypes.data,
+                                    self._orbit_up.ctypes.data)
+        self._target = _f32(sc.target)
         self._view_arr = _f32(self.view)
         self._proj_arr = _f32(self.proj)
 
@@ -624,6 +646,12 @@ class SceneRenderer(_Resident):
         L, d, fb = self.L, self.dev.h, self.fb
         self.shadow_pass()
         _check(L.mopcuda_frame_begin(d, fb, self.clear), "frame_begin")
+        if self.env_tex:  # pass_background before the scene passes
+            sc = self.scene
+            _check(L.mopcuda_draw_background(d, fb, self.env_tex, self._orbit_eye.ctypes.data,
+                                             self._target.ctypes.data, self._orbit_up.ctypes.data,
+                                             sc.fov_deg, sc.env_rotation, sc.env_intensity),
+                   "draw_background")
         _check(L.mopcuda_draw_list(d, fb, self.draw_array, len(self.draws)), "draw_list")
         # pass_instanced after the transparent pass: one draw per instance
         for dr, (_, _, _, _, _, tr) in zip(self.inst_draws, self.instanced):

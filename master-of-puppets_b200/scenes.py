@@ -145,6 +145,8 @@ class Scene:
     # MopFogParams ((r, g, b, a), near, far) for the MOP_POST_FOG bit; None: not set
     fog: Optional[Tuple[Tuple[float, float, float, float], float, float]] = None
     instanced: List[InstancedMesh] = dataclasses.field(default_factory=list)
+    # mop_viewport_set_environment_background: the environment drawn behind the scene
+    env_background: bool = False
 
     @property
     def samples(self) -> int:

@@ -60,6 +60,12 @@ class OrShadowMesh(C.Structure):
                 ("model", C.c_float * 16)]
 
 
+class OrSky(C.Structure):
+    _fields_ = [("env", C.c_void_p), ("w", C.c_int32), ("h", C.c_int32),
+                ("rotation", C.c_float), ("intensity", C.c_float), ("eye", C.c_float * 3),
+                ("target", C.c_float * 3), ("up", C.c_float * 3), ("fov_deg", C.c_float)]
+
+
 class OrFrame(C.Structure):
     _fields_ = [("width", C.c_int32), ("height", C.c_int32), ("ssaa", C.c_int32),
                 ("clear", C.c_float * 4), ("exposure", C.c_float),
@@ -68,7 +74,7 @@ class OrFrame(C.Structure):
                 ("object_id", C.c_void_p), ("color_presented", C.c_void_p),
                 ("hdr", C.c_void_p), ("shadow", C.POINTER(OrShadow)),
                 ("fog_on", C.c_int32), ("fog_color", C.c_float * 4),
-                ("fog_near", C.c_float), ("fog_far", C.c_float)]
+                ("fog_near", C.c_float), ("fog_far", C.c_float), ("sky", C.POINTER(OrSky))]
 
 
 _lib = None
@@ -310,6 +316,15 @@ def render(scene, ibl=None, want_hdr=False):
     if want_hdr:
         out["hdr"] = np.zeros((sh, sw, 4), np.float32)
         f.hdr = out["hdr"].ctypes.data
+    if getattr(scene, "env_background", False) and ibl is not None and "env" in ibl:
+        env = _f32(ibl["env"])
+        sk = OrSky()
+        sk.env, sk.h, sk.w = env.ctypes.data, env.shape[0], env.shape[1]
+        sk.rotation, sk.intensity = scene.env_rotation, scene.env_intensity
+        sk.eye[:], sk.target[:], sk.up[:] = scene.eye, scene.target, scene.up
+        sk.fov_deg = scene.fov_deg
+        keep += [env, sk]
+        f.sky = C.pointer(sk)
     shadow = shadow_map(scene)
     if shadow is not None:
         so = OrShadow()

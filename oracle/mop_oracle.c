@@ -114,10 +114,10 @@ static void m4_perspective(float fov, float aspect, float n, float f, float *m) 
  * mop_viewport_render re-applies the orbit camera every frame
  * (viewport.c:3017 -> camera.c:35-63 -> set_camera_orbit viewport.c:1095-1128),
  * so the frame's eye/up come from sinf/cosf of the recovered yaw/pitch. */
-void oracle_camera(const float eye[3], const float target[3], const float up[3],
-                   float fov_deg, float near_plane, float far_plane, int width,
-                   int height, float view[16], float proj[16],
-                   float eye_out[3]) {
+/* The orbit re-derivation of the eye and up vector mop_viewport_render
+ * applies every frame (from the yaw/pitch mop_viewport_set_camera stored). */
+static void orbit_camera(const float eye[3], const float target[3], const float up[3],
+                         V3 *cam_eye_out, V3 *cam_up_out) {
   V3 e = v3(eye[0], eye[1], eye[2]);
   V3 t = v3(target[0], target[1], target[2]);
   V3 cam_eye = e, cam_up = v3(up[0], up[1], up[2]);
@@ -133,6 +133,17 @@ void oracle_camera(const float eye[3], const float target[3], const float up[3],
     cam_eye = v3(t.x + dist * cp2 * sinf(yaw), t.y + dist * sinf(pitch),
                  t.z + dist * cp2 * cosf(yaw));
   }
+  *cam_eye_out = cam_eye;
+  *cam_up_out = cam_up;
+}
+
+void oracle_camera(const float eye[3], const float target[3], const float up[3],
+                   float fov_deg, float near_plane, float far_plane, int width,
+                   int height, float view[16], float proj[16],
+                   float eye_out[3]) {
+  V3 t = v3(target[0], target[1], target[2]);
+  V3 cam_eye, cam_up;
+  orbit_camera(eye, target, up, &cam_eye, &cam_up);
   m4_look_at(cam_eye, t, cam_up, view);
   float fov = fov_deg * (3.14159265358979323846f / 180.0f);
   float aspect = (float)width / (float)height;
@@ -1421,6 +1432,67 @@ static void postprocess(FB *fb, uint32_t fx, const OrFrame *f) {
 /* ------------------------------------------------------------------------
  * frame driver
  * ------------------------------------------------------------------------ */
+/* env_sample_bilinear, viewport.c:2099-2124 */
+static void sky_bilinear(const float *d, int w, int h, float u, float v, float out[4]) {
+  u = u - floorf(u);
+  v = v - floorf(v);
+  float fx = u * (float)(w - 1), fy = v * (float)(h - 1);
+  int x0 = (int)fx, y0 = (int)fy;
+  int x1 = (x0 + 1) % w, y1 = y0 + 1;
+  if (y1 >= h)
+    y1 = h - 1;
+  float sx = fx - (float)x0, sy = fy - (float)y0;
+  const float *p00 = &d[((size_t)y0 * w + x0) * 4], *p10 = &d[((size_t)y0 * w + x1) * 4];
+  const float *p01 = &d[((size_t)y1 * w + x0) * 4], *p11 = &d[((size_t)y1 * w + x1) * 4];
+  for (int c = 0; c < 4; c++) {
+    float top = p00[c] * (1.0f - sx) + p10[c] * sx;
+    float bot = p01[c] * (1.0f - sx) + p11[c] * sx;
+    out[c] = top * (1.0f - sy) + bot * sy;
+  }
+}
+
+/* pass_background_hdri_cpu, viewport.c:2128-2177: the environment along the
+ * ray through every sample, into the HDR buffer (alpha 1). */
+static void sky_pass(FB *fb, const OrSky *s) {
+  V3 cam_eye, cam_up;
+  orbit_camera(s->eye, s->target, s->up, &cam_eye, &cam_up);
+  V3 t = v3(s->target[0], s->target[1], s->target[2]);
+  int sw = fb->w, sh = fb->h;
+  float fov = s->fov_deg * (3.14159265358979323846f / 180.0f);
+  float aspect = (float)sw / (float)sh;
+  float half_h = tanf(fov * 0.5f);
+  float half_w = half_h * aspect;
+  V3 fwd = v3_norm(v3_sub(t, cam_eye));
+  V3 right = v3_norm(v3_cross(fwd, cam_up));
+  V3 up = v3_cross(right, fwd);
+  const float pi = 3.14159265358979f;
+  for (int y = 0; y < sh; y++) {
+    float ndc_y = 1.0f - 2.0f * ((float)y + 0.5f) / (float)sh;
+    for (int x = 0; x < sw; x++) {
+      float ndc_x = 2.0f * ((float)x + 0.5f) / (float)sw - 1.0f;
+      float dx = fwd.x + right.x * ndc_x * half_w + up.x * ndc_y * half_h;
+      float dy = fwd.y + right.y * ndc_x * half_w + up.y * ndc_y * half_h;
+      float dz = fwd.z + right.z * ndc_x * half_w + up.z * ndc_y * half_h;
+      float len = sqrtf(dx * dx + dy * dy + dz * dz);
+      dx /= len;
+      dy /= len;
+      dz /= len;
+      float phi = atan2f(dz, dx) - s->rotation;
+      float cdy = dy < -1.0f ? -1.0f : (dy > 1.0f ? 1.0f : dy);
+      float theta = asinf(cdy);
+      float eu = phi / (2.0f * pi) + 0.5f;
+      float ev = theta / pi + 0.5f;
+      float smp[4];
+      sky_bilinear(s->env, s->w, s->h, eu, ev, smp);
+      float *o = &fb->hdr[((size_t)y * sw + x) * 4];
+      o[0] = smp[0] * s->intensity;
+      o[1] = smp[1] * s->intensity;
+      o[2] = smp[2] * s->intensity;
+      o[3] = 1.0f;
+    }
+  }
+}
+
 int oracle_render(OrFrame *f, const OrDraw *draws, uint32_t n) {
   if (!f || f->width <= 0 || f->height <= 0)
     return -1;
@@ -1443,6 +1515,8 @@ int oracle_render(OrFrame *f, const OrDraw *draws, uint32_t n) {
     fb.depth[i] = 1.0f;
     fb.id[i] = 0;
   }
+  if (f->sky && f->sky->env && f->sky->w > 0 && f->sky->h > 0)
+    sky_pass(&fb, f->sky);
   for (uint32_t di = 0; di < n; di++) {
     const OrDraw *d = &draws[di];
     /* cpu_draw, cpu_backend.c:536-544 and 621-627: a read-only depth test

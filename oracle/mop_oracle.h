@@ -87,6 +87,19 @@ typedef struct OrShadow {
   float vp[16];
 } OrShadow;
 
+/* The environment background (pass_background_hdri_cpu, reference
+ * viewport.c:2128-2177): every sample's HDR colour before the draws is the
+ * equirectangular environment (RGBA32F, w x h) seen along the ray through
+ * the sample, times intensity.  The camera is the one mop_viewport_set_camera
+ * took (the orbit re-derivation of the eye and up is applied here). */
+typedef struct OrSky {
+  const float *env;
+  int32_t w, h;
+  float rotation, intensity;
+  float eye[3], target[3], up[3];
+  float fov_deg;
+} OrSky;
+
 typedef struct OrFrame {
   int32_t width, height; /* sample resolution (presented * ssaa) */
   int32_t ssaa;
@@ -105,6 +118,7 @@ typedef struct OrFrame {
   int32_t fog_on;
   float fog_color[4];
   float fog_near, fog_far;
+  const OrSky *sky;         /* NULL = no environment background */
 } OrFrame;
 
 /* Render one frame of draws in submission order.  Returns 0 on success. */

@@ -103,11 +103,12 @@ static void cuda_shadow_hook(MopViewport *vp, void *ud) {
   free(casters);
 }
 
-/* The integration patch's post-process row for the CUDA backend: the core
- * applies vp->post_effects and vp->fog_params itself for its CPU backend only
- * (rg_cleanup, viewport.c:2950-2961); the patch hands both to the device,
- * whose post pass runs them at frame end.  Run as a MOP_STAGE_PRE_SCENE hook,
- * so the values of the frame being rendered apply. */
+/* The integration patch's post-process and IBL rows for the CUDA backend:
+ * the core applies vp->post_effects and vp->fog_params itself for its CPU
+ * backend only (rg_cleanup, viewport.c:2950-2961) and hands the IBL maps only
+ * to the CPU rasteriser; the patch gives all of them to the device.  Run as
+ * a MOP_STAGE_PRE_SCENE hook, so the values of the frame being rendered
+ * apply. */
 static void cuda_post_hook(MopViewport *vp, void *ud) {
   (void)ud;
   MopCudaDevice *cu = mop_rhi_cuda_device(vp->device);
@@ -115,6 +116,15 @@ static void cuda_post_hook(MopViewport *vp, void *ud) {
                         vp->fog_params.color.a};
   mopcuda_set_post_effects(cu, vp->post_effects);
   mopcuda_set_fog(cu, fog, vp->fog_params.near_dist, vp->fog_params.far_dist);
+  /* the IBL row: the maps, rotation and intensity rg_ibl_setup hands the
+   * CPU rasteriser (viewport.c:2698-2705); none bound when there are none */
+  if (vp->env_irradiance_data)
+    mopcuda_set_ibl(cu, vp->env_irradiance_data, vp->env_irradiance_w, vp->env_irradiance_h,
+                    vp->env_prefiltered_data, vp->env_prefiltered_w, vp->env_prefiltered_h,
+                    vp->env_prefiltered_levels, vp->env_brdf_lut_data, 256, vp->env_rotation,
+                    vp->env_intensity);
+  else
+    mopcuda_set_ibl(cu, NULL, 0, 0, NULL, 0, 0, 0, NULL, 0, 0.0f, 1.0f);
 }
 #endif
 
@@ -296,6 +306,8 @@ void *refh_create(const RefScene *sc) {
                               .rotation = sc->env_rotation,
                               .intensity = sc->env_intensity};
     mop_viewport_set_environment(vp, &env);
+    if (sc->env_background)
+      mop_viewport_set_environment_background(vp, true);
   }
   return h;
 }

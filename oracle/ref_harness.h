@@ -100,6 +100,7 @@ typedef struct RefScene {
    * render_target, made through a helper viewport of the same backend);
    * refh_read_target reads it back */
   int32_t render_target;
+  int32_t env_background;   /* 1: mop_viewport_set_environment_background */
 } RefScene;
 
 typedef struct RefFrame {

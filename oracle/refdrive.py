@@ -59,7 +59,8 @@ class RefScene(C.Structure):
                 ("fog_color", C.c_float * 4), ("fog_near", C.c_float),
                 ("fog_far", C.c_float), ("instanced_count", C.c_uint32),
                 ("instanced", C.POINTER(RefInstanced)), ("tex_format", C.POINTER(C.c_int32)),
-                ("tex_bytes", C.POINTER(C.c_uint32)), ("render_target", C.c_int32)]
+                ("tex_bytes", C.POINTER(C.c_uint32)), ("render_target", C.c_int32),
+                ("env_background", C.c_int32)]
 
 
 class RefFrame(C.Structure):
@@ -220,6 +221,7 @@ class Reference:
         sc.instanced = ia
         sc.tex_format, sc.tex_bytes = tf, tb
         sc.render_target = 1 if render_target else 0
+        sc.env_background = 1 if getattr(scene, "env_background", False) else 0
         self._keep += [meshes, lights, tw, th, td, tf, tb, sc, ia]
         self.h = L.refh_create(C.byref(sc))
         if not self.h:

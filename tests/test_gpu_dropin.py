@@ -8,9 +8,10 @@ mop_rhi_backend_cuda().  mop_viewport_read_color (SSAA box in the core),
 the object-ID / depth readbacks and mop_viewport_pick must agree: IDs and
 depth bit-exact, colour within the contract tolerance.
 
-Scenes avoid image-based lighting: the unmodified core hands IBL state only
-to its CPU path (reference viewport.c:2692-2706); the CUDA backend receives
-the full IBL state through mopcuda_set_ibl (covered by test_gpu_parity.py).
+The unmodified core hands IBL state only to its CPU path (reference
+viewport.c:2692-2706); on the CUDA side the harness's pre-scene hook passes
+the viewport's maps to mopcuda_set_ibl, as the integration patch's IBL row
+does (along with post effects and fog).
 Twelve of the reference's own test programs also run unmodified on the
 CUDA backend (a link-time wrapper of mop_viewport_create selects it).
 The shadow scenes run the core's own pass_shadow on the CPU side; on the
@@ -69,6 +70,10 @@ CASES = {
     "chrome": lambda: scenes.chrome_scene(seed=68),
     # BC1 / BC3 / BC5 textures through mop_tex_create -> texture_create_ex
     "bc_textures": lambda: scenes.bc_scene(seed=69),
+    # the environment behind the scene: the core's CPU sky pass against the RHI's
+    # draw_skybox (IBL maps handed over by the harness hook, as the patch's IBL row)
+    "env_background": lambda: dataclasses.replace(scenes.small_scene(seed=74, env=1),
+                                                  env_background=True),
     "config2_reduced_no_ibl": lambda: dataclasses.replace(
         scenes.config2(width=480, height=270, ssaa=2, instances=48, tex_size=64), env=0),
 }

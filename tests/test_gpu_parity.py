@@ -31,6 +31,8 @@ def _ibl_for(scene):
         return None
     r = refdrive.Reference(scene)
     maps = r.env_maps()
+    if scene.env_background:
+        maps["env"] = r.env_hdr()
     r.close()
     return maps
 
@@ -114,6 +116,12 @@ CASES = {
     "instanced_unlit": lambda: dataclasses.replace(scenes.instanced_scene(seed=75), lights=[]),
     "instanced_shadow_ibl_ssaa2": lambda: _with_shadow(scenes.instanced_scene(seed=76, ssaa=2,
                                                                               env=1)),
+    # mop_viewport_set_environment_background: the procedural sky behind the scene
+    "env_background": lambda: dataclasses.replace(scenes.small_scene(seed=97, env=1),
+                                                  env_background=True),
+    "env_background_ssaa2_transparent": lambda: dataclasses.replace(
+        scenes.transparent_scene(seed=98, ssaa=2, env=1), env_background=True,
+        env_rotation=0.7, env_intensity=1.3),
     # editor-chrome IDs among the opaque meshes: depth test and culling off, unlit
     "chrome": lambda: scenes.chrome_scene(seed=81),
     "chrome_ssaa2_flat": lambda: dataclasses.replace(scenes.chrome_scene(seed=82, ssaa=2),

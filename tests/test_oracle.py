@@ -105,6 +105,12 @@ LIVE = {
                                                      smooth=False),
     # BC1 / BC3 / BC5 textures made through mop_tex_create (texture_create_ex)
     "bc_textures": lambda: scenes.bc_scene(seed=91),
+    # mop_viewport_set_environment_background: the procedural sky behind the scene
+    "env_background": lambda: dataclasses.replace(scenes.small_scene(seed=92, env=1),
+                                                  env_background=True),
+    "env_background_ssaa2_transparent": lambda: dataclasses.replace(
+        scenes.transparent_scene(seed=93, ssaa=2, env=1), env_background=True,
+        env_rotation=0.7, env_intensity=1.3),
 }
 
 
@@ -116,6 +122,8 @@ def test_oracle_matches_reference_live(name):
     try:
         ref = r.render()
         ibl = r.env_maps() if sc.env else None
+        if sc.env_background:
+            ibl["env"] = r.env_hdr()
         out = cpu_oracle.render(sc, ibl)
         _assert_same(out, ref, name)
         for k in ("view", "proj", "eye"):
