@@ -53,7 +53,8 @@ def parse():
     ap.add_argument("--forms-only", action="store_true",
                     help="run only the batched and served forms (one JSON line)")
     ap.add_argument("--form", choices=["all", "batched", "served", "shadowed", "ibl",
-                                           "scene_load", "config3", "config1"], default="all",
+                                           "scene_load", "config3", "config1", "transparent"],
+                    default="all",
                     help="with --forms-only: which form to run")
     return ap.parse_args()
 
@@ -585,7 +586,16 @@ def run_frames_form(dev, name, steps=20, warm=3):
     import torch
     import mopcuda
     import scenes
-    if name == "config3":
+    if name == "transparent":
+        import dataclasses
+        sc = scenes.config2()
+        for k in range(0, len(sc.meshes), 3):  # every third instance blended, the core's order
+            sc.meshes[k] = dataclasses.replace(sc.meshes[k], opacity=0.35 + 0.1 * (k % 5),
+                                               blend_mode=(1, 2, 3, 1)[k % 4])
+        desc = ("config2 with every third of its 256 instances blended (alpha / additive / "
+                "multiply, opacity 0.35-0.75): the transparent pass composited per sample in "
+                "submission order")
+    elif name == "config3":
         sc = scenes.config3()
         desc = ("config3: 1920x1080 ssaa1, 2,000,000 tris (0.1-8 px edges; 10% straddle the near "
                 "plane, 5% outside, 20% coplanar pairs in separate meshes, 5% skinned tubes), "
@@ -593,7 +603,8 @@ def run_frames_form(dev, name, steps=20, warm=3):
     else:
         sc = scenes.config1()
         desc = "config1: 800x600 ssaa1, UV sphere 64x32 + ground plane, 1 directional light"
-    r = mopcuda.SceneRenderer(dev, sc, None)
+    ibl = scenes.procedural_ibl(sc.sun_dir) if sc.env else None
+    r = mopcuda.SceneRenderer(dev, sc, ibl)
     flush = torch.empty(64 << 20, dtype=torch.float32, device="cuda")
     try:
         dev.set_stage_timing(True)
@@ -788,6 +799,7 @@ def run_forms(which="all"):
                     ("shadowed", run_shadowed), ("ibl", run_ibl),
                     ("scene_load", run_scene_load),
                     ("config3", lambda d: run_frames_form(d, "config3")),
+                    ("transparent", lambda d: run_frames_form(d, "transparent")),
                     ("config1", lambda d: run_frames_form(d, "config1"))):
         if which not in ("all", key):
             continue

@@ -470,6 +470,16 @@ typedef struct MopCudaView {
 } MopCudaView;
 
 MopCudaScene *mopcuda_scene_create(MopCudaDevice *dev);
+/* The scene's shadow pass, as pass_shadow runs it for the frame
+ * (viewport.c:2288-2442): with size > 0, every launch that renders the scene
+ * first rasterises its casters (every draw below the editor-chrome IDs,
+ * with the model matrices the launch renders) into a size x size depth map
+ * from the light camera mopcuda_shadow_light_vp derives for `direction` (the
+ * first active directional light with cast_shadows), and its viewports'
+ * directional lights take the 3x3 PCF factor as in a plain frame.  size 0
+ * turns it off.  Each scene entry of a server launch (a scene as of the
+ * requests' submission) gets its own map. */
+int mopcuda_scene_set_shadow(MopCudaScene *scene, int size, const float direction[3]);
 void mopcuda_scene_destroy(MopCudaScene *scene);
 /* Appends a draw (its mvp and cam_eye are ignored: each viewport supplies
  * them).  Same state rules and errors as mopcuda_draw.  Returns the draw's

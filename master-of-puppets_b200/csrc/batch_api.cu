@@ -183,6 +183,16 @@ extern "C" int mopcuda_scene_set_model(MopCudaScene *s, uint32_t index, const fl
   return MOPCUDA_OK;
 }
 
+extern "C" int mopcuda_scene_set_shadow(MopCudaScene *s, int size, const float direction[3]) {
+  if (!s || size < 0 || size > 16384 || (size > 0 && !direction))
+    return fail(MOPCUDA_EINVAL, "scene_set_shadow: bad arguments");
+  std::lock_guard<std::mutex> lk(s->mu);
+  s->sh_size = size;
+  if (size > 0)
+    memcpy(s->sh_dir, direction, sizeof s->sh_dir);
+  return MOPCUDA_OK;
+}
+
 extern "C" uint32_t mopcuda_scene_draw_count(const MopCudaScene *s) {
   return s ? (uint32_t)s->draws.size() : 0u;
 }
@@ -298,6 +308,13 @@ void LaunchCore::release() {
                         &pre, &out, &depth, &ids, &presented};
   for (DevArena *a : arenas)
     a->release();
+  for (EntryShadow &e : shadows) {
+    DevArena *sa[] = {&e.map, &e.d_draws, &e.recs, &e.items, &e.ctr};
+    for (DevArena *a : sa)
+      a->release();
+    e.h_draws.release();
+  }
+  shadows.clear();
   h_views.release();
   h_draws.release();
   h_scenes.release();
@@ -330,6 +347,8 @@ uint64_t LaunchCore::device_bytes() const {
   uint64_t t = 0;
   for (const DevArena *a : arenas)
     t += a->cap;
+  for (const EntryShadow &e : shadows)
+    t += e.map.cap + e.d_draws.cap + e.recs.cap + e.items.cap + e.ctr.cap;
   return t;
 }
 
@@ -354,6 +373,8 @@ int LaunchCore::set_layout(const MopCudaView *views, const uint32_t *scene_of,
   else
     scene_models.assign(sc.size(), nullptr);
   scene_draw_off.assign(sc.size(), 0);
+  if (shadows.size() < sc.size()) /* entries keep their buffers; never shrunk */
+    shadows.resize(sc.size());
   total_draws = 0;
   for (size_t k = 0; k < sc.size(); k++) {
     scene_draw_off[k] = total_draws;
@@ -460,6 +481,79 @@ static int size_pools(LaunchCore *b, unsigned long long vneed, unsigned long lon
   return MOPCUDA_OK;
 }
 
+/* Entry k's shadow pass for this launch (pass_shadow, viewport.c:2288-2442):
+ * the light camera from its casters' model matrices as of the launch, every
+ * caster's light view-projection * model, the caster table staged in
+ * page-locked memory; the entry's SceneDesc names the map. */
+int LaunchCore::stage_shadow(size_t k, const DrawRec *dr, SceneDesc &d) {
+  EntryShadow &e = shadows[k];
+  const MopCudaScene *sc = scenes[k];
+  const int old_size = e.size;
+  const uint32_t old_casters = e.casters;
+  e.size = 0;
+  e.casters = 0;
+  e.tris = 0;
+  if (sc->sh_size > 0) {
+    std::vector<uint32_t> idx;
+    std::vector<float> models;
+    for (uint32_t i = 0; i < (uint32_t)sc->draws.size(); i++) {
+      const DrawRec &r = dr[i];
+      /* casters: every opaque draw below the editor-chrome IDs
+       * (viewport.c:2310-2315); empty slots hold dropped draws */
+      if (r.vertex_count == 0 || r.index_count < 3u || r.object_id >= 0xFFFD0000u)
+        continue;
+      idx.push_back(i);
+      models.insert(models.end(), r.model, r.model + 16);
+    }
+    float vp[16];
+    if (!idx.empty() && mopcuda_shadow_light_vp(models.data(), (uint32_t)idx.size(), sc->sh_dir, vp)) {
+      std::vector<ShadowDraw> cas(idx.size());
+      uint64_t T = 0;
+      for (size_t j = 0; j < idx.size(); j++) {
+        const DrawRec &r = dr[idx[j]];
+        ShadowDraw &c = cas[j];
+        const bool flex = (r.flags & DF_FLEX) != 0;
+        c.verts = r.vbuf + (flex ? r.off_pos : 0);
+        c.idx = r.ibuf;
+        c.vertex_count = r.vertex_count;
+        c.stride = flex ? r.stride : 48u;
+        c.tri_count = r.index_count / 3u;
+        c.tri_off = (uint32_t)T;
+        mc_mat4_mul(vp, r.model, c.mvp); /* mop_mat4_multiply(light_vp, model) */
+        T += c.tri_count;
+      }
+      if (T >= (1ull << 31))
+        return fail(MOPCUDA_EINVAL, "scene shadow pass too large: %llu triangles",
+                    (unsigned long long)T);
+      const size_t S = (size_t)sc->sh_size, n = cas.size();
+      void *before[6] = {e.map.p, e.d_draws.p, e.recs.p, e.items.p, e.ctr.p, e.h_draws.p};
+      int rc = 0;
+      rc |= e.map.ensure(4 * S * S + 64);
+      rc |= e.d_draws.ensure(sizeof(ShadowDraw) * n);
+      rc |= e.recs.ensure(sizeof(ShadowRec) * (size_t)T);
+      rc |= e.items.ensure(8 * (size_t)T);
+      rc |= e.ctr.ensure(sizeof(ShadowCounters));
+      rc |= e.h_draws.ensure(sizeof(ShadowDraw) * n + 64);
+      if (rc)
+        return MOPCUDA_ENOMEM;
+      void *after[6] = {e.map.p, e.d_draws.p, e.recs.p, e.items.p, e.ctr.p, e.h_draws.p};
+      if (memcmp(before, after, sizeof before) != 0)
+        shadow_moved = true;
+      memcpy(e.h_draws.p, cas.data(), sizeof(ShadowDraw) * n);
+      memcpy(e.h_draws.as<uint8_t>() + sizeof(ShadowDraw) * n, vp, 64);
+      e.size = (int)S;
+      e.casters = (uint32_t)n;
+      e.tris = T;
+      d.shadow_keys = e.map.as<uint32_t>();
+      d.shadow_vp = (const float *)(e.map.as<uint8_t>() + 4 * S * S);
+      d.shadow_size = (int)S;
+    }
+  }
+  if (e.size != old_size || e.casters != old_casters)
+    shadow_moved = true; /* the captured launch no longer matches */
+  return MOPCUDA_OK;
+}
+
 int LaunchCore::stage() {
   SceneDesc *sd = h_scenes.as<SceneDesc>();
   DrawRec *hd = h_draws.as<DrawRec>();
@@ -489,7 +583,12 @@ int LaunchCore::stage() {
       d.ibl_rotation = s->ibl_rot;
       d.ibl_intensity = s->ibl_int;
     }
+    if ((rc = stage_shadow(k, hd + scene_draw_off[k], d)))
+      return rc;
   }
+  any_shadow = false;
+  for (size_t k = 0; k < scenes.size(); k++)
+    any_shadow |= shadows[k].size > 0;
   memcpy(h_views.p, vrec.data(), sizeof(ViewRec) * nv);
   /* first pools: half the worst case (every draw visible in every view) */
   unsigned long long want[4] = {0, 0, 0, 0};
@@ -570,8 +669,35 @@ int LaunchCore::enqueue(int parts) {
     CU_TRY(cudaMemsetAsync(d_status.p, 0, sizeof(BatchStatus), s));
     CU_TRY(cudaMemsetAsync(keys.p, 0xff, 8ull * total_samples, s));
   }
-  launches = (uint64_t)mopcuda_launch_batch(a, d_posts.as<PostArgs>(), pv, post_count, post_tiles,
-                                            L, scenes.size() == 1, s, parts);
+  uint64_t sh_launches = 0;
+  if (parts & BATCH_PART_MAIN)
+    for (size_t k = 0; k < scenes.size(); k++) {
+      EntryShadow &e = shadows[k];
+      if (!e.size)
+        continue;
+      const size_t S = (size_t)e.size, db = sizeof(ShadowDraw) * e.casters;
+      CU_TRY(cudaMemcpyAsync(e.d_draws.p, e.h_draws.p, db, cudaMemcpyHostToDevice, s));
+      CU_TRY(cudaMemcpyAsync(e.map.as<uint8_t>() + 4 * S * S, e.h_draws.as<uint8_t>() + db, 64,
+                             cudaMemcpyHostToDevice, s));
+      /* cleared to 1.0 (viewport.c:2370-2373): the key 0xffffffff */
+      CU_TRY(cudaMemsetAsync(e.map.p, 0xff, 4 * S * S, s));
+      CU_TRY(cudaMemsetAsync(e.ctr.p, 0, sizeof(ShadowCounters), s));
+      ShadowArgs sa;
+      sa.draws = e.d_draws.as<ShadowDraw>();
+      sa.draw_count = e.casters;
+      sa.tri_total = (uint32_t)e.tris;
+      sa.map = e.map.as<uint32_t>();
+      sa.size = (int)S;
+      sa.small_area = SHADOW_SMALL_AREA;
+      sa.recs = e.recs.as<ShadowRec>();
+      sa.items = e.items.as<unsigned long long>();
+      sa.ctr = e.ctr.as<ShadowCounters>();
+      sa.num_sms = dev->num_sms;
+      sh_launches += (uint64_t)mopcuda_launch_shadow(sa, s);
+    }
+  launches = sh_launches +
+             (uint64_t)mopcuda_launch_batch(a, d_posts.as<PostArgs>(), pv, post_count, post_tiles,
+                                            L, scenes.size() == 1, any_shadow, s, parts);
   CU_TRY(cudaGetLastError());
   if (parts & BATCH_PART_POST) { /* status after the last kernel: read at completion */
     CU_TRY(cudaMemcpyAsync(h_status.p, d_status.p, sizeof(BatchStatus), cudaMemcpyDeviceToHost,
@@ -864,12 +990,13 @@ static int submit_locked(MopCudaBatch *b) {
   }
   const unsigned long long pools[4] = {b->core.vertex_pool, b->core.rec_pool, b->core.clip_pool,
                                        b->core.large_pool};
+  b->core.shadow_moved = false;
   rc = b->core.stage();
   if (rc)
     return rc;
   if (pools[0] != b->core.vertex_pool || pools[1] != b->core.rec_pool ||
-      pools[2] != b->core.clip_pool || pools[3] != b->core.large_pool)
-    drop_graph(b); /* the pools moved */
+      pools[2] != b->core.clip_pool || pools[3] != b->core.large_pool || b->core.shadow_moved)
+    drop_graph(b); /* the pools or the shadow passes moved */
   if (!b->exec) {
     rc = build_graph(b);
     if (rc)

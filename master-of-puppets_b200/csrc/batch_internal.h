@@ -28,7 +28,21 @@ struct MopCudaScene {
   bool ibl_on = false;
   int irr_w = 0, irr_h = 0, pf_w = 0, pf_h = 0, pf_levels = 0, brdf_size = 0;
   float ibl_rot = 0.0f, ibl_int = 1.0f;
+  /* shadow pass (mopcuda_scene_set_shadow): map size (0: none) and the
+   * directional light's direction */
+  int sh_size = 0;
+  float sh_dir[3] = {0.0f, 0.0f, 0.0f};
   std::mutex mu;
+};
+
+/* One scene entry's shadow pass in a launch: the map (texels, then the
+ * light's view-projection), the caster table and the raster's work space. */
+struct EntryShadow {
+  int size = 0;          /* 0: the entry renders without a map */
+  uint32_t casters = 0;
+  uint64_t tris = 0;
+  DevArena map, d_draws, recs, items, ctr;
+  HostArena h_draws;     /* caster table, then the view-projection */
 };
 
 /* Uploads bounds and lights when the draw list changed (synchronous). */
@@ -57,6 +71,9 @@ struct LaunchCore {
   std::vector<uint64_t> scene_draw_off;
   uint64_t total_draws = 0, view_draw_total = 0;
   std::vector<PostArgs> posts;
+  std::vector<EntryShadow> shadows; /* per scene entry */
+  bool any_shadow = false;
+  bool shadow_moved = false; /* stage() reallocated a shadow buffer */
   uint32_t post_count[4] = {0, 0, 0, 0}, post_tiles[4] = {0, 0, 0, 0};
   unsigned long long total_samples = 0, total_pixels = 0;
   /* inputs */
@@ -84,6 +101,7 @@ struct LaunchCore {
 
   int init(MopCudaDevice *d);
   void release();
+  int stage_shadow(size_t k, const DrawRec *dr, SceneDesc &d);
   /* views[i] renders scene scene_of[i] (index into sc); no_color[i] (may be
    * null) marks visibility-only viewports. */
   int set_layout(const MopCudaView *views, const uint32_t *scene_of, const uint8_t *no_color,

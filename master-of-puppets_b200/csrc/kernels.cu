@@ -238,6 +238,8 @@ __device__ __noinline__ float shadow_pcf_at(const uint32_t *__restrict__ keys,
 /* Kept out of line: frames without a shadow map never call it, and the
  * shading loops keep their registers. */
 __device__ __forceinline__ float shadow_pcf(const FrameArgs &a, V3 wp) {
+  if (!a.shadow_keys) /* a batch viewport whose scene has no map */
+    return 1.0f;
   return shadow_pcf_at(a.shadow_keys, a.shadow_vp, a.shadow_w, a.shadow_h, wp.x, wp.y, wp.z);
 }
 
@@ -995,11 +997,87 @@ __device__ __forceinline__ void raster_small_item(const FrameArgs &a, uint32_t r
   }
 }
 
+/* Small records, a warp at a time: the warp takes 32 consecutive records and
+ * deals their rows out to its lanes, a lane per (record, row), packing whole
+ * records into rounds of at most 32 rows (a record has at most 32 rows).  In
+ * each round a lane's row start is the record's corner value folded down its
+ * rows one addition at a time, as the reference steps them: the lanes of a
+ * record pass the running value along by shuffles, so after k steps every
+ * row <= k of every record holds its exact start.  Then each lane walks its
+ * row as raster_span does.  Lanes run rows of similar length instead of
+ * whole boxes of different sizes. */
+__device__ __forceinline__ void raster_small_warp(const FrameArgs &a, uint32_t base, uint32_t n,
+                                                  uint8_t *s_owner) {
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint32_t rid = base + lane;
+  int h = 0;
+  if (rid < n) {
+    const RasterRec r = a.rrec[rid];
+    if (rec_live(r, a.width, a.height) && !rec_large(a, r) && !rec_ordered(a, r))
+      h = (int)(r.y1 & 0x7fffu) - (int)r.y0 + 1;
+  }
+  /* greedy packing in lane order: (round, first lane) of every record */
+  int my_round = 0, my_start = 0, round = 0, pos = 0;
+  for (int j = 0; j < 32; j++) {
+    const int hj = __shfl_sync(0xffffffffu, h, j);
+    if (pos + hj > 32) {
+      round++;
+      pos = 0;
+    }
+    if ((int)lane == j) {
+      my_round = round;
+      my_start = pos;
+    }
+    pos += hj;
+  }
+  const int rounds = pos > 0 ? round + 1 : round;
+  for (int rd = 0; rd < rounds; rd++) {
+    const bool mine = h > 0 && my_round == rd;
+    const uint32_t starts = __reduce_or_sync(0xffffffffu, mine ? 1u << my_start : 0u);
+    const uint32_t used = __reduce_max_sync(0xffffffffu, mine ? (uint32_t)(my_start + h) : 0u);
+    if (mine)
+      s_owner[my_start] = (uint8_t)lane;
+    __syncwarp();
+    const uint32_t below = starts & (lane == 31u ? 0xffffffffu : ((2u << lane) - 1u));
+    const bool valid = lane < used && below != 0u;
+    const int seg = valid ? 31 - __clz((int)below) : 0;
+    const int jr = (int)lane - seg;
+    const uint32_t owner = valid ? (uint32_t)s_owner[seg] : lane;
+    __syncwarp();
+    RasterRec r;
+    if (valid)
+      r = a.rrec[base + owner];
+    const bool flat = valid && (r.y1 & REC_FLAT_BIT) != 0;
+    /* row starts: row jr of a record is row jr - 1 (the previous lane) plus
+     * one step of dy; after `step` rounds rows <= step are final */
+    float w0 = valid ? r.w0[0] : 0.0f, w1 = valid ? r.w0[1] : 0.0f, w2 = valid ? r.w0[2] : 0.0f;
+    float zr = valid ? r.zc[0] : 0.0f;
+    const int maxjr = (int)__reduce_max_sync(0xffffffffu, valid ? (uint32_t)jr : 0u);
+    for (int step = 1; step <= maxjr; step++) {
+      const float p0 = __shfl_up_sync(0xffffffffu, w0, 1);
+      const float p1 = __shfl_up_sync(0xffffffffu, w1, 1);
+      const float p2 = __shfl_up_sync(0xffffffffu, w2, 1);
+      const float pz = __shfl_up_sync(0xffffffffu, zr, 1);
+      if (valid && jr == step) {
+        w0 = __fadd_rn(p0, r.dy[0]);
+        w1 = __fadd_rn(p1, r.dy[1]);
+        w2 = __fadd_rn(p2, r.dy[2]);
+        if (flat)
+          zr = __fadd_rn(pz, r.zc[2]);
+      }
+    }
+    if (valid)
+      raster_span(a, r, flat, (int)r.y0 + jr, (int)r.x0, (int)r.x1, w0, w1, w2, zr);
+  }
+}
+
 __global__ void k_raster_small(FrameArgs a) {
+  __shared__ uint8_t s_owner[32 * 32]; /* per warp: first lane of a record -> its lane */
   const uint32_t n = raster_small_items(a);
-  for (uint32_t rid = blockIdx.x * blockDim.x + threadIdx.x; rid < n;
-       rid += gridDim.x * blockDim.x)
-    raster_small_item(a, rid);
+  const uint32_t warp = threadIdx.x >> 5, warps = blockDim.x >> 5;
+  for (uint32_t base = (blockIdx.x * warps + warp) * 32u; base < n;
+       base += gridDim.x * warps * 32u)
+    raster_small_warp(a, base, n, s_owner + 32u * warp);
 }
 
 /* Exclusive scan of the large records' item counts by one block of 1024:
@@ -1469,13 +1547,15 @@ __device__ __forceinline__ float luma(uchar4 p) {
   return 0.299f * (float)p.x + 0.587f * (float)p.y + 0.114f * (float)p.z;
 }
 
-/* FXAA of tile sample (i, j) from its 3x3 neighbourhood in the tile. */
+/* FXAA of tile sample (i, j) (rasterizer.c:2625-2761) from the lumas of its
+ * 3x3 neighbourhood (M the sample, N/S/W/E and the corners); the blend
+ * partner's colour comes from the tile, which holds the unfiltered values the
+ * reference reads from its copy of the buffer. */
 template <int TW>
-__device__ __forceinline__ uchar4 fxaa_tile(const uchar4 (*tc)[TW], const float (*tl)[TW], int i,
-                                            int j) {
+__device__ __forceinline__ uchar4 fxaa_core(const uchar4 (*tc)[TW], int i, int j, float lM,
+                                            float lN, float lS, float lW, float lE, float lNW,
+                                            float lNE, float lSW, float lSE) {
   const uchar4 c = tc[i][j];
-  const float lM = tl[i][j], lN = tl[i - 1][j], lS = tl[i + 1][j], lW = tl[i][j - 1],
-              lE = tl[i][j + 1];
   float mn = lM, mx = lM;
   if (lN < mn) mn = lN;
   if (lS < mn) mn = lS;
@@ -1488,8 +1568,6 @@ __device__ __forceinline__ uchar4 fxaa_tile(const uchar4 (*tc)[TW], const float 
   const float range = mx - mn;
   if (range < 0.0625f * mx + 0.004f)
     return c;
-  const float lNW = tl[i - 1][j - 1], lNE = tl[i - 1][j + 1], lSW = tl[i + 1][j - 1],
-              lSE = tl[i + 1][j + 1];
   const float avg =
       (lN + lS + lW + lE) * (2.0f / 12.0f) + (lNW + lNE + lSW + lSE) * (1.0f / 12.0f);
   float sub = fabsf(avg - lM);
@@ -1617,12 +1695,15 @@ __device__ __forceinline__ void post_tile(const PostArgs &a, PostSmem<SF> &sm, i
   const int tid = threadIdx.y * POST_BX + threadIdx.x;
   const int w = a.width, h = a.height;
   const int sx0 = bx * POST_BX * SF - 1, sy0 = by * POST_BY * SF - 1;
-  for (int i = tid; i < TW * TH; i += POST_BX * POST_BY) {
-    const int ty = i / TW, tx = i % TW;
-    const int sy = min(max(sy0 + ty, 0), h - 1), sx = min(max(sx0 + tx, 0), w - 1);
-    const uchar4 c = a.pre[(size_t)sy * w + sx];
-    s_c[ty][tx] = c;
-    s_l[ty][tx] = luma(c);
+  (void)tid;
+  /* a warp per tile row, a lane per column (clamped at the image edges) */
+  for (int ty = (int)threadIdx.y; ty < TH; ty += POST_BY) {
+    const uchar4 *row = a.pre + (size_t)min(max(sy0 + ty, 0), h - 1) * w;
+    for (int tx = (int)threadIdx.x; tx < TW; tx += POST_BX) {
+      const uchar4 c = row[min(max(sx0 + tx, 0), w - 1)];
+      s_c[ty][tx] = c;
+      s_l[ty][tx] = luma(c);
+    }
   }
   __syncthreads();
   const int pw = w / SF, ph = h / SF;
@@ -1641,15 +1722,29 @@ __device__ __forceinline__ void post_pixel(const PostArgs &a, const uchar4 (*s_c
   const int w = a.width, h = a.height, pw = w / SF;
   const bool fx = (a.effects & 16u) && w >= 3 && h >= 3;
   uint32_t acc[4] = {0, 0, 0, 0};
+  /* the lumas of this pixel's samples and their one-sample ring, read from
+   * the tile once */
+  float L[SF + 2][SF + 2];
+  const int ti0 = (int)threadIdx.y * SF, tj0 = (int)threadIdx.x * SF;
+  if (fx) {
 #pragma unroll
-  for (int dy = 0; dy < SF; dy++)
+    for (int i = 0; i < SF + 2; i++)
+#pragma unroll
+      for (int j = 0; j < SF + 2; j++)
+        L[i][j] = s_l[ti0 + i][tj0 + j];
+  }
+#pragma unroll
+  for (int dy = 0; dy < SF; dy++) {
+    uchar4 row_out[SF];
 #pragma unroll
     for (int dx = 0; dx < SF; dx++) {
       const int x = px * SF + dx, y = py * SF + dy;
-      const int ti = (int)threadIdx.y * SF + dy + 1, tj = (int)threadIdx.x * SF + dx + 1;
+      const int ti = ti0 + dy + 1, tj = tj0 + dx + 1;
       uchar4 c = s_c[ti][tj];
       if (fx && x >= 1 && y >= 1 && x < w - 1 && y < h - 1)
-        c = fxaa_tile<TW>(s_c, s_l, ti, tj);
+        c = fxaa_core<TW>(s_c, ti, tj, L[dy + 1][dx + 1], L[dy][dx + 1], L[dy + 2][dx + 1],
+                          L[dy + 1][dx], L[dy + 1][dx + 2], L[dy][dx], L[dy][dx + 2],
+                          L[dy + 2][dx], L[dy + 2][dx + 2]);
       if (a.effects & 8u) {
         float vg = 1.0f;
         if (a.effects & 4u) {
@@ -1690,12 +1785,29 @@ __device__ __forceinline__ void post_pixel(const PostArgs &a, const uchar4 (*s_c
         c.y = u8_of(v[1] * 255.0f + 0.5f);
         c.z = u8_of(v[2] * 255.0f + 0.5f);
       }
-      a.out[(size_t)y * w + x] = c;
+      row_out[dx] = c;
       acc[0] += c.x;
       acc[1] += c.y;
       acc[2] += c.z;
       acc[3] += c.w;
     }
+    /* the pixel's samples of this row with one store where they are
+     * aligned (w is a multiple of SF) */
+    uchar4 *dst = a.out + (size_t)(py * SF + dy) * w + (size_t)px * SF;
+    if constexpr (SF == 2) {
+      *reinterpret_cast<uint2 *>(dst) = make_uint2(*reinterpret_cast<const uint32_t *>(&row_out[0]),
+                                                   *reinterpret_cast<const uint32_t *>(&row_out[1]));
+    } else if constexpr (SF == 4) {
+      *reinterpret_cast<uint4 *>(dst) = make_uint4(*reinterpret_cast<const uint32_t *>(&row_out[0]),
+                                                   *reinterpret_cast<const uint32_t *>(&row_out[1]),
+                                                   *reinterpret_cast<const uint32_t *>(&row_out[2]),
+                                                   *reinterpret_cast<const uint32_t *>(&row_out[3]));
+    } else {
+#pragma unroll
+      for (int dx = 0; dx < SF; dx++)
+        dst[dx] = row_out[dx];
+    }
+  }
   if (a.presented) {
     const uint32_t n = (uint32_t)(SF * SF);
     a.presented[(size_t)py * pw + px] =
@@ -1833,7 +1945,9 @@ int mopcuda_launch_frame(const FrameArgs &a, const PostArgs &p, const LaunchCfg 
     cudaEventRecord(ev[2], s);
   cudaMemsetAsync(a.keys, 0xff, sizeof(unsigned long long) * (size_t)S, s);
   if (a.total_tris) {
-    const int rb = cfg.raster_block > 0 ? cfg.raster_block : 128;
+    /* a warp per 32 records; at most 32 warps per block (the owner table) */
+    const int rb = cfg.raster_block >= 32 && cfg.raster_block <= 1024 ? cfg.raster_block & ~31
+                                                                         : 128;
     const uint32_t rec_grid = blocks_for(a.rec_cap < (1u << 22) ? a.rec_cap : (1u << 22),
                                          (unsigned)rb);
     k_raster_small<<<rec_grid, rb, 0, s>>>(a);
@@ -2356,6 +2470,9 @@ __global__ void __launch_bounds__(256) k_batch_prepare(BatchArgs b) {
     FrameArgs a = b.tmpl;
     a.lights = sc.lights;
     a.light_total = sc.light_total;
+    a.shadow_keys = sc.shadow_keys;
+    a.shadow_vp = sc.shadow_vp;
+    a.shadow_w = a.shadow_h = sc.shadow_size;
     a.irr = sc.irr;
     a.irr_w = sc.irr_w;
     a.irr_h = sc.irr_h;
@@ -2525,7 +2642,7 @@ __device__ __forceinline__ uint32_t views_prefix(const FrameArgs *__restrict__ f
   return s_pre[nv];
 }
 
-template <int ST>
+template <int ST, bool SH>
 __global__ void __launch_bounds__(256) k_b_items(const FrameArgs *__restrict__ fr, uint32_t nv) {
   __shared__ uint32_t s_pre[MOPCUDA_MAX_VIEWS + 1];
   const uint32_t total = views_prefix<ST>(fr, nv, s_pre);
@@ -2539,9 +2656,9 @@ __global__ void __launch_bounds__(256) k_b_items(const FrameArgs *__restrict__ f
     if (ST == ST_VERTEX)
       vertex_item(a, i);
     else if (ST == ST_SETUP)
-      setup_item<false>(a, i);
+      setup_item<SH>(a, i);
     else if (ST == ST_CLIP)
-      clip_item<false>(a, i);
+      clip_item<SH>(a, i);
     else if (ST == ST_RSMALL)
       raster_small_item(a, i);
     else
@@ -2571,6 +2688,7 @@ __global__ void __launch_bounds__(256) k_b_resolve(const FrameArgs *__restrict__
 
 /* shared_lights: every viewport of the launch reads one light array (one
  * scene), staged in shared memory; otherwise each reads its own. */
+template <bool SH>
 __global__ void __launch_bounds__(256, 4) k_b_shade(const FrameArgs *__restrict__ fr,
                                                     uint32_t nv, int shared_lights) {
   __shared__ LightRec s_lights[SHADE_SMEM_LIGHTS];
@@ -2583,7 +2701,7 @@ __global__ void __launch_bounds__(256, 4) k_b_shade(const FrameArgs *__restrict_
     while (s_pre[v + 1] <= g)
       v++;
     const FrameArgs &a = fr[v];
-    shade_item<false>(a, g - s_pre[v], lights ? lights : a.lights);
+    shade_item<SH>(a, g - s_pre[v], lights ? lights : a.lights);
   }
 }
 
@@ -2646,17 +2764,18 @@ void mopcuda_batch_grids(BatchLaunch &cfg) {
   const int sms = cfg.num_sms > 0 ? cfg.num_sms : 148;
   const int gm = cfg.grid_mul > 0 ? cfg.grid_mul : 1;
   auto grid = [&](const void *fn, int block) { return sms * resident_blocks(fn, block) * gm; };
-  cfg.grid_vertex = grid((const void *)k_b_items<ST_VERTEX>, cfg.vertex_block);
-  cfg.grid_setup = grid((const void *)k_b_items<ST_SETUP>, cfg.setup_block);
-  cfg.grid_clip = grid((const void *)k_b_items<ST_CLIP>, 128);
-  cfg.grid_rsmall = grid((const void *)k_b_items<ST_RSMALL>, cfg.raster_block);
-  cfg.grid_rlarge = grid((const void *)k_b_items<ST_RLARGE>, cfg.large_block);
-  cfg.grid_shade = grid((const void *)k_b_shade, cfg.shade_block);
+  cfg.grid_vertex = grid((const void *)k_b_items<ST_VERTEX, false>, cfg.vertex_block);
+  cfg.grid_setup = grid((const void *)k_b_items<ST_SETUP, false>, cfg.setup_block);
+  cfg.grid_clip = grid((const void *)k_b_items<ST_CLIP, false>, 128);
+  cfg.grid_rsmall = grid((const void *)k_b_items<ST_RSMALL, false>, cfg.raster_block);
+  cfg.grid_rlarge = grid((const void *)k_b_items<ST_RLARGE, false>, cfg.large_block);
+  cfg.grid_shade = grid((const void *)k_b_shade<false>, cfg.shade_block);
 }
 
 int mopcuda_launch_batch(const BatchArgs &b, const PostArgs *posts, const uint32_t *post_views[4],
                          const uint32_t post_count[4], const uint32_t post_tiles[4],
-                         const BatchLaunch &cfg, bool shared_lights, cudaStream_t s, int parts) {
+                         const BatchLaunch &cfg, bool shared_lights, bool shadows,
+                         cudaStream_t s, int parts) {
   if (b.nv == 0)
     return 0;
   int launches = 0;
@@ -2666,14 +2785,24 @@ int mopcuda_launch_batch(const BatchArgs &b, const PostArgs *posts, const uint32
   if (parts & BATCH_PART_MAIN) {
     k_batch_prepare<<<nv, 256, 0, s>>>(b);
     k_batch_alloc<<<1, 256, 0, s>>>(b);
-    k_b_items<ST_VERTEX><<<cfg.grid_vertex, cfg.vertex_block, 0, s>>>(fr, nv);
-    k_b_items<ST_SETUP><<<cfg.grid_setup, cfg.setup_block, 0, s>>>(fr, nv);
-    k_b_items<ST_CLIP><<<cfg.grid_clip, 128, 0, s>>>(fr, nv);
-    k_b_items<ST_RSMALL><<<cfg.grid_rsmall, cfg.raster_block, 0, s>>>(fr, nv);
+    k_b_items<ST_VERTEX, false><<<cfg.grid_vertex, cfg.vertex_block, 0, s>>>(fr, nv);
+    /* setup (flat colours), clipping and shading read a scene's shadow map
+     * when any scene of the launch has one */
+    if (shadows) {
+      k_b_items<ST_SETUP, true><<<cfg.grid_setup, cfg.setup_block, 0, s>>>(fr, nv);
+      k_b_items<ST_CLIP, true><<<cfg.grid_clip, 128, 0, s>>>(fr, nv);
+    } else {
+      k_b_items<ST_SETUP, false><<<cfg.grid_setup, cfg.setup_block, 0, s>>>(fr, nv);
+      k_b_items<ST_CLIP, false><<<cfg.grid_clip, 128, 0, s>>>(fr, nv);
+    }
+    k_b_items<ST_RSMALL, false><<<cfg.grid_rsmall, cfg.raster_block, 0, s>>>(fr, nv);
     k_b_large_scan<<<nv, 1024, 0, s>>>(fr);
-    k_b_items<ST_RLARGE><<<cfg.grid_rlarge, cfg.large_block, 0, s>>>(fr, nv);
+    k_b_items<ST_RLARGE, false><<<cfg.grid_rlarge, cfg.large_block, 0, s>>>(fr, nv);
     k_b_resolve<<<sms * 8, 256, 0, s>>>(fr, nv);
-    k_b_shade<<<cfg.grid_shade, cfg.shade_block, 0, s>>>(fr, nv, shared_lights ? 1 : 0);
+    if (shadows)
+      k_b_shade<true><<<cfg.grid_shade, cfg.shade_block, 0, s>>>(fr, nv, shared_lights ? 1 : 0);
+    else
+      k_b_shade<false><<<cfg.grid_shade, cfg.shade_block, 0, s>>>(fr, nv, shared_lights ? 1 : 0);
     launches += 10;
   }
   if (!(parts & BATCH_PART_POST))

@@ -374,6 +374,11 @@ struct SceneDesc {
   const float *irr, *pf, *brdf;
   int irr_w, irr_h, pf_w, pf_h, pf_levels, brdf_size;
   float ibl_rotation, ibl_intensity;
+  /* the scene's shadow map for this launch (null: none): size x size keys,
+   * then the light's view-projection */
+  const uint32_t *shadow_keys;
+  const float *shadow_vp;
+  int shadow_size;
 };
 
 /* Mesh-local bounding sphere of a draw's vertices; r < 0 (or NaN) means the
@@ -444,8 +449,8 @@ void mopcuda_batch_grids(BatchLaunch &cfg);
 #define BATCH_PART_POST 2
 int mopcuda_launch_batch(const BatchArgs &b, const PostArgs *posts, const uint32_t *post_views[4],
                          const uint32_t post_count[4], const uint32_t post_tiles[4],
-                         const BatchLaunch &cfg, bool shared_lights, cudaStream_t s,
-                         int parts = BATCH_PART_MAIN | BATCH_PART_POST);
+                         const BatchLaunch &cfg, bool shared_lights, bool shadows,
+                         cudaStream_t s, int parts = BATCH_PART_MAIN | BATCH_PART_POST);
 
 /* ev (optional, 7 events): stage boundaries
  * vertex | setup+clip | raster | resolve | shade | post */

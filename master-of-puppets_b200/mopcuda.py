@@ -188,6 +188,7 @@ SIGNATURES = [
     ("mopcuda_measure_fp32_peak", C.c_int, [_P, C.POINTER(C.c_double)]),
     ("mopcuda_frame_io_bytes", C.c_int, [_P, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
     ("mopcuda_scene_create", _P, [_P]),
+    ("mopcuda_scene_set_shadow", C.c_int, [_P, C.c_int, _P]),
     ("mopcuda_scene_destroy", None, [_P]),
     ("mopcuda_scene_add_draw", C.c_int, [_P, C.POINTER(MopCudaDraw)]),
     ("mopcuda_scene_set_model", C.c_int, [_P, C.c_uint32, _P]),
@@ -758,6 +759,13 @@ class ResidentScene(_Resident):
             rc = L.mopcuda_scene_add_draw(self.sh_scene, C.byref(dr))
             if rc < 0:
                 raise MopCudaError(rc, "scene_add_draw")
+        # pass_shadow: the first active directional light with cast_shadows
+        import scenes as _sc
+        light = _sc.shadow_light(scene)
+        if light is not None:
+            dr_ = _f32(light.direction)
+            _check(L.mopcuda_scene_set_shadow(self.sh_scene, _sc.SHADOW_MAP_SIZE,
+                                              dr_.ctypes.data), "scene_set_shadow")
 
     def set_model(self, k: int, model):
         m = _f32(model)

@@ -100,6 +100,35 @@ def test_batch_fog_equals_single_viewport_frames(cuda_device, ibl):
         b.close()
 
 
+def _shadowed(sc):
+    """The scene with its first directional light casting shadows."""
+    for k, l in enumerate(sc.lights):
+        if l.type == scenes.LIGHT_DIRECTIONAL and l.active:
+            sc.lights[k] = dataclasses.replace(l, cast_shadows=True)
+            break
+    return sc
+
+
+def test_batch_shadow_equals_single_viewport_frames(cuda_device, ibl):
+    """A scene whose sun casts shadows: every viewport of the batch equals
+    the plain frame rendered after the plain path's shadow pass, and a TRS
+    update between launches moves the shadows as it moves them there."""
+    sc = _shadowed(_scene(instances=16))
+    b = mopcuda.BatchRenderer(cuda_device, sc, _views(sc, 6, seed=11), ibl)
+    try:
+        b.render()
+        _check_batch(cuda_device, b, sc, ibl, "shadow batch")
+        m = sc.meshes[3].transform.copy()
+        m[12:15] += np.float32(2.0)
+        b.set_model(3, m)
+        b.render()
+        moved = dataclasses.replace(sc, meshes=[dataclasses.replace(x, transform=m) if k == 3
+                                                else x for k, x in enumerate(sc.meshes)])
+        _check_batch(cuda_device, b, moved, ibl, "shadow batch after TRS")
+    finally:
+        b.close()
+
+
 def test_batch_read_views_equals_single_reads(cuda_device, ibl):
     """mopcuda_batch_read_views (every view's buffer in one call) returns the
     bytes of one mopcuda_batch_read per view, for each buffer, and rejects a

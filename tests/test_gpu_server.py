@@ -181,6 +181,43 @@ def test_served_requests_match_oracle(cuda_device):
         rs.close()
 
 
+def test_server_shadowed_scene_in_a_mix(cuda_device, world):
+    """A scene whose sun casts shadows served beside unshadowed ones: each
+    request equals its own plain frame (shadow pass included), and a request
+    submitted after a TRS update sees the moved caster's shadow while the
+    earlier one keeps the old."""
+    scs, rss, ibl = world
+    sc = scenes.config2(seed=14, width=160, height=90, ssaa=1, instances=12, tex_size=64)
+    for k, l in enumerate(sc.lights):
+        if l.type == scenes.LIGHT_DIRECTIONAL:
+            sc.lights[k] = dataclasses.replace(l, cast_shadows=True)
+            break
+    rs = mopcuda.ResidentScene(cuda_device, sc, ibl)
+    srv = mopcuda.Server(cuda_device, hbm_budget=8 << 30, max_views=16, max_inflight=2)
+    try:
+        sid = [srv.add_scene(r) for r in rss] + [srv.add_scene(rs)]
+        v = _views(sc, 1, seed=31)[0]
+        first = srv.submit_render(sid[3], v, want_ids=True, want_depth=True)
+        others = [srv.submit_render(sid[k % 3], _views(scs[k % 3], 1, seed=40 + k)[0])
+                  for k in range(5)]
+        m = sc.meshes[2].transform.copy()
+        m[12:15] += np.float32(1.5)
+        rs.set_model(2, m)
+        second = srv.submit_render(sid[3], v, want_ids=True, want_depth=True)
+        for t in [first, second] + others:
+            srv.wait(t)
+        _same_render(first, _plain(cuda_device, sc, v, ibl), "shadowed before TRS")
+        moved = dataclasses.replace(sc, meshes=[dataclasses.replace(x, transform=m) if k == 2
+                                                else x for k, x in enumerate(sc.meshes)])
+        _same_render(second, _plain(cuda_device, moved, v, ibl), "shadowed after TRS")
+        for t in others:
+            s_ = scs[sid.index(t.req.scene)]
+            assert (t.color == _plain(cuda_device, s_, t.view, ibl)["color"]).all()
+    finally:
+        srv.close()
+        rs.close()
+
+
 def test_server_trs_update_between_requests(cuda_device, world):
     scs, rss, ibl = world
     srv = mopcuda.Server(cuda_device, hbm_budget=8 << 30, max_views=8, max_inflight=2)
