@@ -472,8 +472,8 @@ typedef struct MopCudaView {
 MopCudaScene *mopcuda_scene_create(MopCudaDevice *dev);
 /* The scene's shadow pass, as pass_shadow runs it for the frame
  * (viewport.c:2288-2442): with size > 0, every launch that renders the scene
- * first rasterises its casters (every draw below the editor-chrome IDs,
- * with the model matrices the launch renders) into a size x size depth map
+ * first rasterises its casters (every opaque draw below the editor-chrome
+ * IDs, with the model matrices the launch renders) into a size x size depth map
  * from the light camera mopcuda_shadow_light_vp derives for `direction` (the
  * first active directional light with cast_shadows), and its viewports'
  * directional lights take the 3x3 PCF factor as in a plain frame.  size 0
@@ -482,8 +482,13 @@ MopCudaScene *mopcuda_scene_create(MopCudaDevice *dev);
 int mopcuda_scene_set_shadow(MopCudaScene *scene, int size, const float direction[3]);
 void mopcuda_scene_destroy(MopCudaScene *scene);
 /* Appends a draw (its mvp and cam_eye are ignored: each viewport supplies
- * them).  Same state rules and errors as mopcuda_draw.  Returns the draw's
- * index (>= 0) or an error code. */
+ * them).  Same state rules and errors as mopcuda_draw.  Draws go in mesh
+ * order; each viewport renders the non-blended ones in that order, then the
+ * blended ones (blend_mode != 0) back to front by the squared distance of
+ * their model translation to its eye (pass_scene_opaque /
+ * pass_scene_transparent, viewport.c:2449-2553).  Refused: draws with the
+ * depth test or the depth write off (MOPCUDA_EUNSUPPORTED) and a 1,025th
+ * blended draw.  Returns the draw's index (>= 0) or an error code. */
 int mopcuda_scene_add_draw(MopCudaScene *scene, const MopCudaDraw *draw);
 /* Replaces draw `index`'s model matrix (TRS update); effective from the next
  * batch submit. */

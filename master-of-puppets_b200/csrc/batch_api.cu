@@ -151,19 +151,32 @@ extern "C" int mopcuda_scene_add_draw(MopCudaScene *s, const MopCudaDraw *c) {
     s->lights.resize(nl);
     return rc;
   }
-  if (!skip && (r.blend_mode != 0 || r.opacity < 1.0f ||
-                ((r.flags & DF_SMOOTH) && !(r.flags & DF_LIT)) ||
-                (r.flags & (DF_NO_DEPTH_WRITE | DF_NO_DEPTH_TEST)))) {
+  if (!skip && (r.flags & (DF_NO_DEPTH_WRITE | DF_NO_DEPTH_TEST))) {
     s->lights.resize(nl);
     return fail(MOPCUDA_EUNSUPPORTED,
-                "scene_add_draw: batches render opaque lit or flat draws only");
+                "scene_add_draw: batches render depth-tested, depth-writing draws only");
   }
   if (skip) { /* zero opacity: a colour no-op, kept as an empty slot */
     memset(&r, 0, sizeof r);
     memcpy(r.model, c->model, sizeof r.model);
   }
+  /* blended, translucent and unlit smooth draws are order-dependent: each
+   * viewport composites them in its ordered suffix, the blended ones in
+   * the core's back-to-front order for that viewport's eye */
+  const float op = r.opacity < 0.0f ? 0.0f : (r.opacity > 1.0f ? 1.0f : r.opacity);
+  if (!skip && (r.blend_mode != 0 || op < 1.0f || ((r.flags & DF_SMOOTH) && !(r.flags & DF_LIT))))
+    r.flags |= DF_ORDERED;
+  if (r.blend_mode != 0 && s->blended >= BATCH_MAX_BLENDED) {
+    s->lights.resize(nl);
+    return fail(MOPCUDA_EUNSUPPORTED, "scene_add_draw: more than %d blended draws in a scene",
+                BATCH_MAX_BLENDED);
+  }
   if ((uint64_t)s->tris + r.index_count / 3u >= (1ull << (32 - ORDER_FAN_BITS)))
     return fail(MOPCUDA_EINVAL, "scene too large");
+  if (r.blend_mode != 0)
+    s->blended++;
+  if (r.flags & DF_ORDERED)
+    s->ordered_tris += r.index_count / 3u;
   s->draws.push_back(r);
   s->bounds.push_back(skip ? DrawBound{{0, 0, 0}, -1.0f} : mesh_bound(c));
   s->tris += r.index_count / 3u;
@@ -254,7 +267,12 @@ uint64_t mc_view_bytes(const MopCudaScene *s, uint64_t samples, uint64_t pixels)
   mc_pool_need(s->tris, s->verts, 1, 1, need);
   const uint64_t pools = 64ull * need[0] + (sizeof(RasterRec) + sizeof(ShadeRec)) * need[1] +
                          4ull * need[2] + 8ull * need[3];
-  return 28ull * samples + 4ull * pixels + pools / 2 + sizeof(DrawRec) * s->draws.size();
+  /* an ordered suffix: hdr, list heads and touched samples, a fragment per
+   * sample and the suffix-record list */
+  const uint64_t suffix =
+      s->ordered_tris ? 32ull * samples + 8ull * (s->ordered_tris + need[2]) + 4096ull * 8ull : 0ull;
+  return 28ull * samples + 4ull * pixels + pools / 2 + suffix +
+         sizeof(DrawRec) * s->draws.size();
 }
 
 /* ------------------------------------------------------------------------
@@ -305,9 +323,11 @@ void LaunchCore::release() {
   DevArena *arenas[] = {&d_views, &d_frames, &d_view_draws, &d_ctr, &d_status, &d_posts,
                         &d_post_views, &d_draws, &d_scenes, &clip, &world, &normal, &color,
                         &rrec, &srec, &clipq, &large_list, &large_items, &keys, &shade_list,
-                        &pre, &out, &depth, &ids, &presented};
+                        &pre, &out, &depth, &ids, &presented, &hdr, &frag_head, &touched,
+                        &frags, &olist, &olist_items};
   for (DevArena *a : arenas)
     a->release();
+  frag_pool = olist_pool = 0;
   for (EntryShadow &e : shadows) {
     DevArena *sa[] = {&e.map, &e.d_draws, &e.recs, &e.items, &e.ctr};
     for (DevArena *a : sa)
@@ -332,18 +352,22 @@ void LaunchCore::release() {
 void LaunchCore::trim() {
   if (stream)
     sync(10000);
-  DevArena *arenas[] = {&clip, &world, &normal, &color, &rrec, &srec, &clipq, &large_list,
-                        &large_items, &keys, &shade_list, &pre, &out, &depth, &ids, &presented};
+  DevArena *arenas[] = {&clip,       &world, &normal,  &color,      &rrec,      &srec,
+                        &clipq,      &large_list, &large_items, &keys, &shade_list, &pre,
+                        &out,        &depth, &ids,     &presented,  &hdr,       &frag_head,
+                        &touched,    &frags, &olist,   &olist_items};
   for (DevArena *a : arenas)
     a->release();
   vertex_pool = rec_pool = clip_pool = large_pool = 0;
+  frag_pool = olist_pool = 0;
 }
 
 uint64_t LaunchCore::device_bytes() const {
   const DevArena *arenas[] = {&d_views, &d_frames, &d_view_draws, &d_ctr, &d_status, &d_posts,
                               &d_post_views, &d_draws, &d_scenes, &clip, &world, &normal, &color,
                               &rrec, &srec, &clipq, &large_list, &large_items, &keys,
-                              &shade_list, &pre, &out, &depth, &ids, &presented};
+                              &shade_list, &pre, &out, &depth, &ids, &presented, &hdr,
+                              &frag_head, &touched, &frags, &olist, &olist_items};
   uint64_t t = 0;
   for (const DevArena *a : arenas)
     t += a->cap;
@@ -499,8 +523,9 @@ int LaunchCore::stage_shadow(size_t k, const DrawRec *dr, SceneDesc &d) {
     for (uint32_t i = 0; i < (uint32_t)sc->draws.size(); i++) {
       const DrawRec &r = dr[i];
       /* casters: every opaque draw below the editor-chrome IDs
-       * (viewport.c:2310-2315); empty slots hold dropped draws */
-      if (r.vertex_count == 0 || r.index_count < 3u || r.object_id >= 0xFFFD0000u)
+       * (viewport.c:2310-2317); empty slots hold dropped draws */
+      if (r.vertex_count == 0 || r.index_count < 3u || r.object_id >= 0xFFFD0000u ||
+          r.blend_mode != 0)
         continue;
       idx.push_back(i);
       models.insert(models.end(), r.model, r.model + 16);
@@ -601,10 +626,55 @@ int LaunchCore::stage() {
   }
   for (int k = 0; k < 4; k++)
     want[k] = std::max(want[k] / 2 + 4096, pool_floor[k]);
+  int rc = stage_suffix();
+  if (rc)
+    return rc;
   if (vertex_pool < want[0] || rec_pool < want[1] || clip_pool < want[2] ||
       large_pool < want[3])
     return size_pools(this, std::max(want[0], vertex_pool), std::max(want[1], rec_pool),
                       std::max(want[2], clip_pool), std::max(want[3], large_pool));
+  return MOPCUDA_OK;
+}
+
+/* The ordered suffix's buffers when a scene entry of the launch has
+ * order-dependent draws: composition colour, list heads and touched samples
+ * per sample; the suffix-record and fragment pools sized for every viewport
+ * of such a scene (the device reports larger needs, after() grows them). */
+int LaunchCore::stage_suffix() {
+  any_ordered = false;
+  for (const MopCudaScene *s : scenes)
+    any_ordered |= s->ordered_tris > 0;
+  if (!any_ordered)
+    return MOPCUDA_OK;
+  unsigned long long ol = 0, fr = 0;
+  for (uint32_t i = 0; i < nv; i++) {
+    const MopCudaScene *s = scenes[vrec[i].scene];
+    if (!s->ordered_tris)
+      continue;
+    unsigned long long need[4];
+    mc_pool_need(s->tris, s->verts, fan_num, large_num, need);
+    ol += s->ordered_tris + need[2];
+    fr += (unsigned long long)vrec[i].width * vrec[i].height * frag_num / 4ull + 4096ull;
+  }
+  const unsigned long long sa = std::max(total_samples, sample_floor);
+  void *before[6] = {hdr.p, frag_head.p, touched.p, frags.p, olist.p, olist_items.p};
+  int rc = 0;
+  rc |= hdr.ensure(16ull * sa);
+  rc |= frag_head.ensure(4ull * sa);
+  rc |= touched.ensure(4ull * sa);
+  if (olist_pool < ol) {
+    rc |= olist.ensure(4ull * ol);
+    rc |= olist_items.ensure(4ull * ol);
+  }
+  if (frag_pool < fr)
+    rc |= frags.ensure(8ull * fr);
+  if (rc)
+    return MOPCUDA_ENOMEM;
+  olist_pool = std::min(olist.cap / 4, olist_items.cap / 4);
+  frag_pool = frags.cap / 8;
+  void *after_[6] = {hdr.p, frag_head.p, touched.p, frags.p, olist.p, olist_items.p};
+  if (memcmp(before, after_, sizeof before) != 0)
+    suffix_moved = true;
   return MOPCUDA_OK;
 }
 
@@ -652,6 +722,18 @@ int LaunchCore::enqueue(int parts) {
   a.ids = ids.as<uint32_t>();
   a.fan_num = fan_num;
   a.large_num = large_num;
+  a.frag_num = frag_num;
+  a.samples = total_samples;
+  if (any_ordered) {
+    a.hdr = hdr.as<float4>();
+    a.frag_head = frag_head.as<uint32_t>();
+    a.touched = touched.as<uint32_t>();
+    a.frags = frags.as<uint2>();
+    a.frag_pool = frag_pool;
+    a.olist = olist.as<uint32_t>();
+    a.olist_items = olist_items.as<uint32_t>();
+    a.olist_pool = olist_pool;
+  }
 
   const uint32_t *pv[4];
   for (int k = 0; k < 4; k++)
@@ -697,7 +779,8 @@ int LaunchCore::enqueue(int parts) {
     }
   launches = sh_launches +
              (uint64_t)mopcuda_launch_batch(a, d_posts.as<PostArgs>(), pv, post_count, post_tiles,
-                                            L, scenes.size() == 1, any_shadow, s, parts);
+                                            L, scenes.size() == 1, any_shadow, any_ordered, s,
+                                            parts);
   CU_TRY(cudaGetLastError());
   if (parts & BATCH_PART_POST) { /* status after the last kernel: read at completion */
     CU_TRY(cudaMemcpyAsync(h_status.p, d_status.p, sizeof(BatchStatus), cudaMemcpyDeviceToHost,
@@ -730,7 +813,36 @@ int LaunchCore::after(bool *rerun, int attempt) {
       return fail(MOPCUDA_ENOMEM, "launch: large-record list exhausted");
     large_num *= 2u;
   }
-  if (st->overflow) {
+  if (view_over & 32u) { /* a viewport's suffix-record list: the fan reserve */
+    if (fan_num >= 256u)
+      return fail(MOPCUDA_ENOMEM, "launch: suffix-record list exhausted");
+    fan_num *= 2u;
+  }
+  if (view_over & 16u) { /* a viewport's fragments */
+    if (frag_num >= 4096u)
+      return fail(MOPCUDA_ENOMEM, "launch: blended-fragment reserve exhausted");
+    frag_num *= 2u;
+  }
+  if (st->overflow & 64u)
+    return fail(MOPCUDA_ENOMEM, "launch: a viewport has an ordered suffix but the launch has "
+                                "no suffix buffers");
+  if (st->overflow & 48u) { /* the suffix pools */
+    const unsigned long long ol = st->need_olist + st->need_olist / 4 + 4096ull;
+    const unsigned long long fr = st->need_frag + st->need_frag / 4 + 4096ull;
+    int rc = 0;
+    if ((st->overflow & 16u) && ol > olist_pool) {
+      rc |= olist.ensure(4ull * ol);
+      rc |= olist_items.ensure(4ull * ol);
+      olist_pool = std::min(olist.cap / 4, olist_items.cap / 4);
+    }
+    if ((st->overflow & 32u) && fr > frag_pool) {
+      rc |= frags.ensure(8ull * fr);
+      frag_pool = frags.cap / 8;
+    }
+    if (rc)
+      return MOPCUDA_ENOMEM;
+  }
+  if (st->overflow & 15u) {
     const unsigned long long need[4] = {st->need_vertex, st->need_rec, st->need_clip,
                                         st->need_large};
     unsigned long long cap[4] = {vertex_pool, rec_pool, clip_pool, large_pool};
@@ -990,13 +1102,14 @@ static int submit_locked(MopCudaBatch *b) {
   }
   const unsigned long long pools[4] = {b->core.vertex_pool, b->core.rec_pool, b->core.clip_pool,
                                        b->core.large_pool};
-  b->core.shadow_moved = false;
+  b->core.shadow_moved = b->core.suffix_moved = false;
   rc = b->core.stage();
   if (rc)
     return rc;
   if (pools[0] != b->core.vertex_pool || pools[1] != b->core.rec_pool ||
-      pools[2] != b->core.clip_pool || pools[3] != b->core.large_pool || b->core.shadow_moved)
-    drop_graph(b); /* the pools or the shadow passes moved */
+      pools[2] != b->core.clip_pool || pools[3] != b->core.large_pool ||
+      b->core.shadow_moved || b->core.suffix_moved)
+    drop_graph(b); /* the pools, the suffix buffers or the shadow passes moved */
   if (!b->exec) {
     rc = build_graph(b);
     if (rc)

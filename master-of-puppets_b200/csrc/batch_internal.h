@@ -32,6 +32,10 @@ struct MopCudaScene {
    * directional light's direction */
   int sh_size = 0;
   float sh_dir[3] = {0.0f, 0.0f, 0.0f};
+  /* order-dependent draws: blended ones (the core's transparent pass, sorted
+   * per viewport) and the triangles of every DF_ORDERED draw */
+  uint32_t blended = 0;
+  uint64_t ordered_tris = 0;
   std::mutex mu;
 };
 
@@ -74,6 +78,13 @@ struct LaunchCore {
   std::vector<EntryShadow> shadows; /* per scene entry */
   bool any_shadow = false;
   bool shadow_moved = false; /* stage() reallocated a shadow buffer */
+  /* ordered suffix: a scene entry with order-dependent draws gives the
+   * launch its per-sample buffers and pools; suffix_moved: stage()
+   * reallocated one of them */
+  bool any_ordered = false, suffix_moved = false;
+  DevArena hdr, frag_head, touched, frags, olist, olist_items;
+  unsigned long long frag_pool = 0, olist_pool = 0;
+  uint32_t frag_num = 4;
   uint32_t post_count[4] = {0, 0, 0, 0}, post_tiles[4] = {0, 0, 0, 0};
   unsigned long long total_samples = 0, total_pixels = 0;
   /* inputs */
@@ -102,6 +113,7 @@ struct LaunchCore {
   int init(MopCudaDevice *d);
   void release();
   int stage_shadow(size_t k, const DrawRec *dr, SceneDesc &d);
+  int stage_suffix();
   /* views[i] renders scene scene_of[i] (index into sc); no_color[i] (may be
    * null) marks visibility-only viewports. */
   int set_layout(const MopCudaView *views, const uint32_t *scene_of, const uint8_t *no_color,

@@ -997,87 +997,11 @@ __device__ __forceinline__ void raster_small_item(const FrameArgs &a, uint32_t r
   }
 }
 
-/* Small records, a warp at a time: the warp takes 32 consecutive records and
- * deals their rows out to its lanes, a lane per (record, row), packing whole
- * records into rounds of at most 32 rows (a record has at most 32 rows).  In
- * each round a lane's row start is the record's corner value folded down its
- * rows one addition at a time, as the reference steps them: the lanes of a
- * record pass the running value along by shuffles, so after k steps every
- * row <= k of every record holds its exact start.  Then each lane walks its
- * row as raster_span does.  Lanes run rows of similar length instead of
- * whole boxes of different sizes. */
-__device__ __forceinline__ void raster_small_warp(const FrameArgs &a, uint32_t base, uint32_t n,
-                                                  uint8_t *s_owner) {
-  const uint32_t lane = threadIdx.x & 31u;
-  const uint32_t rid = base + lane;
-  int h = 0;
-  if (rid < n) {
-    const RasterRec r = a.rrec[rid];
-    if (rec_live(r, a.width, a.height) && !rec_large(a, r) && !rec_ordered(a, r))
-      h = (int)(r.y1 & 0x7fffu) - (int)r.y0 + 1;
-  }
-  /* greedy packing in lane order: (round, first lane) of every record */
-  int my_round = 0, my_start = 0, round = 0, pos = 0;
-  for (int j = 0; j < 32; j++) {
-    const int hj = __shfl_sync(0xffffffffu, h, j);
-    if (pos + hj > 32) {
-      round++;
-      pos = 0;
-    }
-    if ((int)lane == j) {
-      my_round = round;
-      my_start = pos;
-    }
-    pos += hj;
-  }
-  const int rounds = pos > 0 ? round + 1 : round;
-  for (int rd = 0; rd < rounds; rd++) {
-    const bool mine = h > 0 && my_round == rd;
-    const uint32_t starts = __reduce_or_sync(0xffffffffu, mine ? 1u << my_start : 0u);
-    const uint32_t used = __reduce_max_sync(0xffffffffu, mine ? (uint32_t)(my_start + h) : 0u);
-    if (mine)
-      s_owner[my_start] = (uint8_t)lane;
-    __syncwarp();
-    const uint32_t below = starts & (lane == 31u ? 0xffffffffu : ((2u << lane) - 1u));
-    const bool valid = lane < used && below != 0u;
-    const int seg = valid ? 31 - __clz((int)below) : 0;
-    const int jr = (int)lane - seg;
-    const uint32_t owner = valid ? (uint32_t)s_owner[seg] : lane;
-    __syncwarp();
-    RasterRec r;
-    if (valid)
-      r = a.rrec[base + owner];
-    const bool flat = valid && (r.y1 & REC_FLAT_BIT) != 0;
-    /* row starts: row jr of a record is row jr - 1 (the previous lane) plus
-     * one step of dy; after `step` rounds rows <= step are final */
-    float w0 = valid ? r.w0[0] : 0.0f, w1 = valid ? r.w0[1] : 0.0f, w2 = valid ? r.w0[2] : 0.0f;
-    float zr = valid ? r.zc[0] : 0.0f;
-    const int maxjr = (int)__reduce_max_sync(0xffffffffu, valid ? (uint32_t)jr : 0u);
-    for (int step = 1; step <= maxjr; step++) {
-      const float p0 = __shfl_up_sync(0xffffffffu, w0, 1);
-      const float p1 = __shfl_up_sync(0xffffffffu, w1, 1);
-      const float p2 = __shfl_up_sync(0xffffffffu, w2, 1);
-      const float pz = __shfl_up_sync(0xffffffffu, zr, 1);
-      if (valid && jr == step) {
-        w0 = __fadd_rn(p0, r.dy[0]);
-        w1 = __fadd_rn(p1, r.dy[1]);
-        w2 = __fadd_rn(p2, r.dy[2]);
-        if (flat)
-          zr = __fadd_rn(pz, r.zc[2]);
-      }
-    }
-    if (valid)
-      raster_span(a, r, flat, (int)r.y0 + jr, (int)r.x0, (int)r.x1, w0, w1, w2, zr);
-  }
-}
-
 __global__ void k_raster_small(FrameArgs a) {
-  __shared__ uint8_t s_owner[32 * 32]; /* per warp: first lane of a record -> its lane */
   const uint32_t n = raster_small_items(a);
-  const uint32_t warp = threadIdx.x >> 5, warps = blockDim.x >> 5;
-  for (uint32_t base = (blockIdx.x * warps + warp) * 32u; base < n;
-       base += gridDim.x * warps * 32u)
-    raster_small_warp(a, base, n, s_owner + 32u * warp);
+  for (uint32_t rid = blockIdx.x * blockDim.x + threadIdx.x; rid < n;
+       rid += gridDim.x * blockDim.x)
+    raster_small_item(a, rid);
 }
 
 /* Exclusive scan of the large records' item counts by one block of 1024:
@@ -1215,7 +1139,7 @@ __device__ __forceinline__ float aces(float x) { /* rasterizer.c:2770-2774 */
  * atan2f / asinf (CUDA's; glibc's differ in the last ulp for some inputs, as
  * in the IBL lookups), a bilinear sample (env_sample_bilinear, :2099-2124)
  * times the intensity. */
-__device__ __noinline__ void sky_hdr(const FrameArgs &a, int x, int y, float out[3]) {
+__device__ __forceinline__ void sky_hdr(const FrameArgs &a, int x, int y, float out[3]) {
   const float ndc_y = 1.0f - 2.0f * ((float)y + 0.5f) / (float)a.height;
   const float ndc_x = 2.0f * ((float)x + 0.5f) / (float)a.width - 1.0f;
   float d[3];
@@ -1547,15 +1471,13 @@ __device__ __forceinline__ float luma(uchar4 p) {
   return 0.299f * (float)p.x + 0.587f * (float)p.y + 0.114f * (float)p.z;
 }
 
-/* FXAA of tile sample (i, j) (rasterizer.c:2625-2761) from the lumas of its
- * 3x3 neighbourhood (M the sample, N/S/W/E and the corners); the blend
- * partner's colour comes from the tile, which holds the unfiltered values the
- * reference reads from its copy of the buffer. */
+/* FXAA of tile sample (i, j) from its 3x3 neighbourhood in the tile. */
 template <int TW>
-__device__ __forceinline__ uchar4 fxaa_core(const uchar4 (*tc)[TW], int i, int j, float lM,
-                                            float lN, float lS, float lW, float lE, float lNW,
-                                            float lNE, float lSW, float lSE) {
+__device__ __forceinline__ uchar4 fxaa_tile(const uchar4 (*tc)[TW], const float (*tl)[TW], int i,
+                                            int j) {
   const uchar4 c = tc[i][j];
+  const float lM = tl[i][j], lN = tl[i - 1][j], lS = tl[i + 1][j], lW = tl[i][j - 1],
+              lE = tl[i][j + 1];
   float mn = lM, mx = lM;
   if (lN < mn) mn = lN;
   if (lS < mn) mn = lS;
@@ -1568,6 +1490,8 @@ __device__ __forceinline__ uchar4 fxaa_core(const uchar4 (*tc)[TW], int i, int j
   const float range = mx - mn;
   if (range < 0.0625f * mx + 0.004f)
     return c;
+  const float lNW = tl[i - 1][j - 1], lNE = tl[i - 1][j + 1], lSW = tl[i + 1][j - 1],
+              lSE = tl[i + 1][j + 1];
   const float avg =
       (lN + lS + lW + lE) * (2.0f / 12.0f) + (lNW + lNE + lSW + lSE) * (1.0f / 12.0f);
   float sub = fabsf(avg - lM);
@@ -1695,15 +1619,12 @@ __device__ __forceinline__ void post_tile(const PostArgs &a, PostSmem<SF> &sm, i
   const int tid = threadIdx.y * POST_BX + threadIdx.x;
   const int w = a.width, h = a.height;
   const int sx0 = bx * POST_BX * SF - 1, sy0 = by * POST_BY * SF - 1;
-  (void)tid;
-  /* a warp per tile row, a lane per column (clamped at the image edges) */
-  for (int ty = (int)threadIdx.y; ty < TH; ty += POST_BY) {
-    const uchar4 *row = a.pre + (size_t)min(max(sy0 + ty, 0), h - 1) * w;
-    for (int tx = (int)threadIdx.x; tx < TW; tx += POST_BX) {
-      const uchar4 c = row[min(max(sx0 + tx, 0), w - 1)];
-      s_c[ty][tx] = c;
-      s_l[ty][tx] = luma(c);
-    }
+  for (int i = tid; i < TW * TH; i += POST_BX * POST_BY) {
+    const int ty = i / TW, tx = i % TW;
+    const int sy = min(max(sy0 + ty, 0), h - 1), sx = min(max(sx0 + tx, 0), w - 1);
+    const uchar4 c = a.pre[(size_t)sy * w + sx];
+    s_c[ty][tx] = c;
+    s_l[ty][tx] = luma(c);
   }
   __syncthreads();
   const int pw = w / SF, ph = h / SF;
@@ -1722,29 +1643,15 @@ __device__ __forceinline__ void post_pixel(const PostArgs &a, const uchar4 (*s_c
   const int w = a.width, h = a.height, pw = w / SF;
   const bool fx = (a.effects & 16u) && w >= 3 && h >= 3;
   uint32_t acc[4] = {0, 0, 0, 0};
-  /* the lumas of this pixel's samples and their one-sample ring, read from
-   * the tile once */
-  float L[SF + 2][SF + 2];
-  const int ti0 = (int)threadIdx.y * SF, tj0 = (int)threadIdx.x * SF;
-  if (fx) {
 #pragma unroll
-    for (int i = 0; i < SF + 2; i++)
-#pragma unroll
-      for (int j = 0; j < SF + 2; j++)
-        L[i][j] = s_l[ti0 + i][tj0 + j];
-  }
-#pragma unroll
-  for (int dy = 0; dy < SF; dy++) {
-    uchar4 row_out[SF];
+  for (int dy = 0; dy < SF; dy++)
 #pragma unroll
     for (int dx = 0; dx < SF; dx++) {
       const int x = px * SF + dx, y = py * SF + dy;
-      const int ti = ti0 + dy + 1, tj = tj0 + dx + 1;
+      const int ti = (int)threadIdx.y * SF + dy + 1, tj = (int)threadIdx.x * SF + dx + 1;
       uchar4 c = s_c[ti][tj];
       if (fx && x >= 1 && y >= 1 && x < w - 1 && y < h - 1)
-        c = fxaa_core<TW>(s_c, ti, tj, L[dy + 1][dx + 1], L[dy][dx + 1], L[dy + 2][dx + 1],
-                          L[dy + 1][dx], L[dy + 1][dx + 2], L[dy][dx], L[dy][dx + 2],
-                          L[dy + 2][dx], L[dy + 2][dx + 2]);
+        c = fxaa_tile<TW>(s_c, s_l, ti, tj);
       if (a.effects & 8u) {
         float vg = 1.0f;
         if (a.effects & 4u) {
@@ -1785,29 +1692,12 @@ __device__ __forceinline__ void post_pixel(const PostArgs &a, const uchar4 (*s_c
         c.y = u8_of(v[1] * 255.0f + 0.5f);
         c.z = u8_of(v[2] * 255.0f + 0.5f);
       }
-      row_out[dx] = c;
+      a.out[(size_t)y * w + x] = c;
       acc[0] += c.x;
       acc[1] += c.y;
       acc[2] += c.z;
       acc[3] += c.w;
     }
-    /* the pixel's samples of this row with one store where they are
-     * aligned (w is a multiple of SF) */
-    uchar4 *dst = a.out + (size_t)(py * SF + dy) * w + (size_t)px * SF;
-    if constexpr (SF == 2) {
-      *reinterpret_cast<uint2 *>(dst) = make_uint2(*reinterpret_cast<const uint32_t *>(&row_out[0]),
-                                                   *reinterpret_cast<const uint32_t *>(&row_out[1]));
-    } else if constexpr (SF == 4) {
-      *reinterpret_cast<uint4 *>(dst) = make_uint4(*reinterpret_cast<const uint32_t *>(&row_out[0]),
-                                                   *reinterpret_cast<const uint32_t *>(&row_out[1]),
-                                                   *reinterpret_cast<const uint32_t *>(&row_out[2]),
-                                                   *reinterpret_cast<const uint32_t *>(&row_out[3]));
-    } else {
-#pragma unroll
-      for (int dx = 0; dx < SF; dx++)
-        dst[dx] = row_out[dx];
-    }
-  }
   if (a.presented) {
     const uint32_t n = (uint32_t)(SF * SF);
     a.presented[(size_t)py * pw + px] =
@@ -1945,9 +1835,7 @@ int mopcuda_launch_frame(const FrameArgs &a, const PostArgs &p, const LaunchCfg 
     cudaEventRecord(ev[2], s);
   cudaMemsetAsync(a.keys, 0xff, sizeof(unsigned long long) * (size_t)S, s);
   if (a.total_tris) {
-    /* a warp per 32 records; at most 32 warps per block (the owner table) */
-    const int rb = cfg.raster_block >= 32 && cfg.raster_block <= 1024 ? cfg.raster_block & ~31
-                                                                         : 128;
+    const int rb = cfg.raster_block > 0 ? cfg.raster_block : 128;
     const uint32_t rec_grid = blocks_for(a.rec_cap < (1u << 22) ? a.rec_cap : (1u << 22),
                                          (unsigned)rb);
     k_raster_small<<<rec_grid, rb, 0, s>>>(a);
@@ -2074,22 +1962,26 @@ __device__ __forceinline__ uint32_t ordered_record_items(const FrameArgs &a) {
   return raster_small_items(a);
 }
 
-/* Queue the live records of the suffix with their (row, chunk) counts. */
+/* Queues record rid if it is a live record of the suffix, with its
+ * (row, chunk) count. */
+__device__ __forceinline__ void ocount_item(const FrameArgs &a, uint32_t rid) {
+  const RasterRec r = a.rrec[rid];
+  if (!rec_live(r, a.width, a.height) || !rec_ordered(a, r))
+    return;
+  const uint32_t q = atomicAdd(&a.ctr->olist_count, 1u);
+  if (q < a.olist_cap) {
+    a.olist[q] = rid;
+    a.olist_items[q] = rec_items(r);
+  } else {
+    atomicOr(&a.ctr->overflow, 32u);
+  }
+}
+
 __global__ void __launch_bounds__(256) k_ocount(FrameArgs a) {
   const uint32_t n = ordered_record_items(a);
   for (uint32_t rid = blockIdx.x * blockDim.x + threadIdx.x; rid < n;
-       rid += gridDim.x * blockDim.x) {
-    const RasterRec r = a.rrec[rid];
-    if (!rec_live(r, a.width, a.height) || !rec_ordered(a, r))
-      continue;
-    const uint32_t q = atomicAdd(&a.ctr->olist_count, 1u);
-    if (q < a.olist_cap) {
-      a.olist[q] = rid;
-      a.olist_items[q] = rec_items(r);
-    } else {
-      atomicOr(&a.ctr->overflow, 32u);
-    }
-  }
+       rid += gridDim.x * blockDim.x)
+    ocount_item(a, rid);
 }
 
 __global__ void __launch_bounds__(1024) k_oscan(FrameArgs a) {
@@ -2112,60 +2004,66 @@ __device__ __forceinline__ void push_fragment(const FrameArgs &a, uint32_t px, u
     a.touched[atomicAdd(&a.ctr->touched_count, 1u)] = px;
 }
 
-/* One (row, 32-sample chunk) item of a suffix record: the reference's edge
- * walk from the folded chunk start; covered samples in front of the opaque
- * depth get a fragment. */
+/* One (row, 32-sample chunk) item of a suffix record (nl: records queued):
+ * the reference's edge walk from the folded chunk start; covered samples in
+ * front of the opaque depth get a fragment. */
+__device__ __forceinline__ void oraster_item(const FrameArgs &a, uint32_t it, uint32_t nl) {
+  uint32_t lo = 0, hi = nl;
+  while (hi - lo > 1) {
+    const uint32_t mid = (lo + hi) >> 1;
+    if (a.olist_items[mid] <= it)
+      lo = mid;
+    else
+      hi = mid;
+  }
+  const uint32_t rid = a.olist[lo];
+  if (rid >= a.rec_cap)
+    return;
+  const RasterRec r = a.rrec[rid];
+  const bool flat = (r.y1 & REC_FLAT_BIT) != 0;
+  const uint32_t wd = (uint32_t)r.x1 - (uint32_t)r.x0 + 1u;
+  const uint32_t chunks = (wd + RASTER_CHUNK - 1u) / RASTER_CHUNK;
+  const uint32_t local = it - a.olist_items[lo];
+  const int jr = (int)(local / chunks), kc = (int)((local % chunks) * RASTER_CHUNK);
+  const int y = (int)r.y0 + jr;
+  if (y > (int)(r.y1 & 0x7fffu))
+    return;
+  const int xs = (int)r.x0 + kc, xe = min((int)r.x1, xs + RASTER_CHUNK - 1);
+  float w0 = fold_add(fold_add(r.w0[0], r.dy[0], jr), r.dx[0], kc);
+  float w1 = fold_add(fold_add(r.w0[1], r.dy[1], jr), r.dx[1], kc);
+  float w2 = fold_add(fold_add(r.w0[2], r.dy[2], jr), r.dx[2], kc);
+  float z = flat ? fold_add(fold_add(r.zc[0], r.zc[2], jr), r.zc[1], kc) : 0.0f;
+  const uint32_t rowbase = (uint32_t)y * (uint32_t)a.width;
+  for (int x = xs; x <= xe; x++) {
+    if (w0 >= 0.0f && w1 >= 0.0f && w2 >= 0.0f) {
+      float zz = z;
+      if (!flat) {
+        const float b0 = w0 * r.inv_area, b1 = w1 * r.inv_area, b2 = w2 * r.inv_area;
+        zz = b0 * r.zc[0] + b1 * r.zc[1] + b2 * r.zc[2];
+      }
+      const uint32_t px = rowbase + (uint32_t)x;
+      if (a.ordered_keep_all || zz < a.depth[px])
+        push_fragment(a, px, r.order);
+    }
+    w0 = __fadd_rn(w0, r.dx[0]);
+    w1 = __fadd_rn(w1, r.dx[1]);
+    w2 = __fadd_rn(w2, r.dx[2]);
+    if (flat)
+      z = __fadd_rn(z, r.zc[1]);
+  }
+}
+
+__device__ __forceinline__ uint32_t olist_len(const FrameArgs &a) {
+  const uint32_t nl = a.ctr->olist_count;
+  return nl > a.olist_cap ? a.olist_cap : nl;
+}
+
 __global__ void __launch_bounds__(256) k_oraster(FrameArgs a) {
-  uint32_t nl = a.ctr->olist_count;
-  if (nl > a.olist_cap)
-    nl = a.olist_cap;
+  const uint32_t nl = olist_len(a);
   const uint32_t total = a.ctr->olist_items;
   for (uint32_t it = blockIdx.x * blockDim.x + threadIdx.x; it < total;
-       it += gridDim.x * blockDim.x) {
-    uint32_t lo = 0, hi = nl;
-    while (hi - lo > 1) {
-      const uint32_t mid = (lo + hi) >> 1;
-      if (a.olist_items[mid] <= it)
-        lo = mid;
-      else
-        hi = mid;
-    }
-    const uint32_t rid = a.olist[lo];
-    if (rid >= a.rec_cap)
-      continue;
-    const RasterRec r = a.rrec[rid];
-    const bool flat = (r.y1 & REC_FLAT_BIT) != 0;
-    const uint32_t wd = (uint32_t)r.x1 - (uint32_t)r.x0 + 1u;
-    const uint32_t chunks = (wd + RASTER_CHUNK - 1u) / RASTER_CHUNK;
-    const uint32_t local = it - a.olist_items[lo];
-    const int jr = (int)(local / chunks), kc = (int)((local % chunks) * RASTER_CHUNK);
-    const int y = (int)r.y0 + jr;
-    if (y > (int)(r.y1 & 0x7fffu))
-      continue;
-    const int xs = (int)r.x0 + kc, xe = min((int)r.x1, xs + RASTER_CHUNK - 1);
-    float w0 = fold_add(fold_add(r.w0[0], r.dy[0], jr), r.dx[0], kc);
-    float w1 = fold_add(fold_add(r.w0[1], r.dy[1], jr), r.dx[1], kc);
-    float w2 = fold_add(fold_add(r.w0[2], r.dy[2], jr), r.dx[2], kc);
-    float z = flat ? fold_add(fold_add(r.zc[0], r.zc[2], jr), r.zc[1], kc) : 0.0f;
-    const uint32_t rowbase = (uint32_t)y * (uint32_t)a.width;
-    for (int x = xs; x <= xe; x++) {
-      if (w0 >= 0.0f && w1 >= 0.0f && w2 >= 0.0f) {
-        float zz = z;
-        if (!flat) {
-          const float b0 = w0 * r.inv_area, b1 = w1 * r.inv_area, b2 = w2 * r.inv_area;
-          zz = b0 * r.zc[0] + b1 * r.zc[1] + b2 * r.zc[2];
-        }
-        const uint32_t px = rowbase + (uint32_t)x;
-        if (a.ordered_keep_all || zz < a.depth[px])
-          push_fragment(a, px, r.order);
-      }
-      w0 = __fadd_rn(w0, r.dx[0]);
-      w1 = __fadd_rn(w1, r.dx[1]);
-      w2 = __fadd_rn(w2, r.dx[2]);
-      if (flat)
-        z = __fadd_rn(z, r.zc[1]);
-    }
-  }
+       it += gridDim.x * blockDim.x)
+    oraster_item(a, it, nl);
 }
 
 /* The record behind an order (triangle << 5 | fan), as shade_item finds it. */
@@ -2179,22 +2077,162 @@ __device__ __forceinline__ uint32_t record_of(const FrameArgs &a, uint32_t order
   return fan == 0u ? t : 0xffffffffu;
 }
 
+/* The composition state of one sample while its fragments are applied. */
+struct OFold {
+  float hdr[3];
+  float depth;
+  uint32_t id;
+  /* a depth-write-off draw's depth is undone when the draw ends: `saved`
+   * holds the depth from before it, `cur` the draw of the last fragment */
+  float saved;
+  uint32_t cur;
+  bool cur_nw;
+};
+
+/* Applies the fragment of submission order `order` at sample (x, y). */
 template <bool SH>
-__global__ void __launch_bounds__(128) k_ofold(FrameArgs a) {
-  const uint32_t n = a.ctr->touched_count;
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    const uint32_t px = a.touched[i];
-    uint32_t ord[ORDERED_MAX_FRAGS];
-    uint32_t cnt = 0, total = 0;
-    for (uint32_t node = a.frag_head[px]; node != 0xffffffffu && node < a.frag_cap;
-         node = a.frags[node].x) {
-      if (cnt < ORDERED_MAX_FRAGS)
-        ord[cnt++] = a.frags[node].y;
-      if (++total > a.frag_cap)
-        break;
+__device__ __forceinline__ void ofold_fragment(const FrameArgs &a, OFold &st, int x, int y,
+                                               uint32_t order) {
+  const uint32_t rid = record_of(a, order);
+  if (rid >= a.rec_cap)
+    return;
+  const RasterRec r = a.rrec[rid];
+  const ShadeRec s = a.srec[rid];
+  const uint32_t di = s.draw < a.draw_count ? s.draw : 0;
+  const DrawRec &d = a.draws[di];
+  if (di != st.cur) {
+    if (st.cur_nw)
+      st.depth = st.saved; /* cpu_backend.c:575-580 */
+    st.cur = di;
+    st.cur_nw = (d.flags & DF_NO_DEPTH_WRITE) != 0;
+    if (st.cur_nw)
+      st.saved = st.depth; /* cpu_backend.c:536-544 */
+  }
+  const bool dtest = !(d.flags & DF_NO_DEPTH_TEST);
+  const int jr = y - (int)r.y0, kc = x - (int)r.x0;
+  if (r.y1 & REC_FLAT_BIT) { /* rasterize_filled_triangle, rasterizer.c:1000-1083 */
+    const float z = fold_add(fold_add(r.zc[0], r.zc[2], jr), r.zc[1], kc);
+    if (!dtest || z < st.depth) {
+      const float ca = d.opacity < 0.0f ? 0.0f : (d.opacity > 1.0f ? 1.0f : d.opacity);
+      if (d.blend_mode == 0 && ca >= 1.0f) {
+        st.hdr[0] = s.col[0];
+        st.hdr[1] = s.col[1];
+        st.hdr[2] = s.col[2];
+        st.depth = z;
+        st.id = d.object_id;
+      } else { /* blended: colour only, no depth or ID write */
+        const float inv_a = 1.0f - ca;
+        for (int c = 0; c < 3; c++) {
+          if (d.blend_mode == 2)
+            st.hdr[c] = st.hdr[c] + s.col[c] * ca;
+          else if (d.blend_mode == 3)
+            st.hdr[c] = st.hdr[c] * s.col[c];
+          else
+            st.hdr[c] = s.col[c] * ca + st.hdr[c] * inv_a;
+        }
+      }
     }
-    if (total > ORDERED_MAX_FRAGS)
-      atomicOr(&a.ctr->overflow, 64u); /* the frame is reported unsupported */
+    return;
+  }
+  float w[3];
+  for (int e = 0; e < 3; e++)
+    w[e] = fold_add(fold_add(r.w0[e], r.dy[e], jr), r.dx[e], kc);
+  const float b0 = w[0] * r.inv_area, b1 = w[1] * r.inv_area, b2 = w[2] * r.inv_area;
+  const float z = b0 * r.zc[0] + b1 * r.zc[1] + b2 * r.zc[2];
+  if (dtest && !(z < st.depth))
+    return;
+  if (s.v[0] >= a.vertex_cap || s.v[1] >= a.vertex_cap || s.v[2] >= a.vertex_cap)
+    return;
+  const float4 N[3] = {a.normal[s.v[0]], a.normal[s.v[1]], a.normal[s.v[2]]};
+  float pc[3] = {b0 * N[0].w, b1 * N[1].w, b2 * N[2].w};
+  const float ip = 1.0f / (pc[0] + pc[1] + pc[2]);
+  pc[0] *= ip;
+  pc[1] *= ip;
+  pc[2] *= ip;
+  /* edge-distance coverage (rasterizer.c:1899-1938, 1320-1361) */
+  float min_d = 0.0f;
+  for (int e = 0; e < 3; e++) {
+    const float len = sqrtf(r.dx[e] * r.dx[e] + r.dy[e] * r.dy[e]);
+    const float inv = len > 1e-6f ? 1.0f / len : 0.0f;
+    const float de = w[e] * inv;
+    if (e == 0 || de < min_d)
+      min_d = de;
+  }
+  const bool legacy = !(d.flags & DF_LIT);
+  if (legacy && !(min_d >= 0.0f))
+    return;
+  float p[3];
+  if (legacy)
+    shade_legacy(a, d, s.v, N, pc, p);
+  else
+    shade_smooth<SH>(a, d, a.lights + d.light_off, s.v, N, pc, p);
+  const float op = d.opacity < 0.0f ? 0.0f : (d.opacity > 1.0f ? 1.0f : d.opacity);
+  /* the legacy path blends at silhouettes only: where the sample's depth
+   * so far lies clearly behind the fragment (rasterizer.c:1425-1429);
+   * the multi-light path blends at every edge of a non-opaque draw
+   * (rasterizer.c:2097-2100) */
+  const float cov = legacy ? ((min_d < 1.0f && (st.depth - z) > 0.005f) ? min_d : 1.0f)
+                           : ((min_d < 1.0f && d.blend_mode != 0) ? min_d : 1.0f);
+  const float fa = op * cov;
+  if (d.blend_mode == 0 && fa >= 1.0f) {
+    st.hdr[0] = p[0];
+    st.hdr[1] = p[1];
+    st.hdr[2] = p[2];
+    st.depth = z;
+    st.id = d.object_id;
+  } else {
+    const float inv = 1.0f - fa;
+    for (int c = 0; c < 3; c++) {
+      if (d.blend_mode == 2)
+        st.hdr[c] = st.hdr[c] + p[c] * fa;
+      else if (d.blend_mode == 3)
+        st.hdr[c] = st.hdr[c] * p[c];
+      else
+        st.hdr[c] = p[c] * fa + st.hdr[c] * inv;
+    }
+    if (fa > 0.5f) {
+      st.depth = z;
+      st.id = d.object_id;
+    }
+  }
+}
+
+/* Each touched sample folds its fragments in submission order.  Up to
+ * ORDERED_MAX_FRAGS orders are gathered and insertion-sorted in registers;
+ * a longer list is applied by selection, each step walking the list for the
+ * smallest order above the last one applied (orders are distinct: one per
+ * record, and a record covers a sample once). */
+template <bool SH> __device__ __forceinline__ void ofold_item(const FrameArgs &a, uint32_t i) {
+  const uint32_t px = a.touched[i];
+  const uint32_t head = a.frag_head[px];
+  uint32_t ord[ORDERED_MAX_FRAGS];
+  uint32_t cnt = 0, total = 0;
+  for (uint32_t node = head; node != 0xffffffffu && node < a.frag_cap; node = a.frags[node].x) {
+    if (cnt < ORDERED_MAX_FRAGS)
+      ord[cnt++] = a.frags[node].y;
+    if (++total > a.frag_cap)
+      break;
+  }
+  const int x = (int)(px % (uint32_t)a.width), y = (int)(px / (uint32_t)a.width);
+  OFold st;
+  if (a.keys[px] != KEY_EMPTY) {
+    const float4 h = a.hdr[px];
+    st.hdr[0] = h.x;
+    st.hdr[1] = h.y;
+    st.hdr[2] = h.z;
+  } else if (a.sky) {
+    sky_hdr(a, x, y, st.hdr);
+  } else {
+    st.hdr[0] = a.clear[0];
+    st.hdr[1] = a.clear[1];
+    st.hdr[2] = a.clear[2];
+  }
+  st.depth = a.depth[px];
+  st.id = a.ids[px];
+  st.saved = st.depth;
+  st.cur = 0xffffffffu;
+  st.cur_nw = false;
+  if (total <= ORDERED_MAX_FRAGS) {
     for (uint32_t k = 1; k < cnt; k++) { /* submission order */
       const uint32_t v = ord[k];
       uint32_t j = k;
@@ -2204,146 +2242,49 @@ __global__ void __launch_bounds__(128) k_ofold(FrameArgs a) {
       }
       ord[j] = v;
     }
-    const int x = (int)(px % (uint32_t)a.width), y = (int)(px / (uint32_t)a.width);
-    const bool covered = a.keys[px] != KEY_EMPTY;
-    float hdr[3];
-    if (covered) {
-      const float4 h = a.hdr[px];
-      hdr[0] = h.x;
-      hdr[1] = h.y;
-      hdr[2] = h.z;
-    } else if (a.sky) {
-      sky_hdr(a, x, y, hdr);
-    } else {
-      hdr[0] = a.clear[0];
-      hdr[1] = a.clear[1];
-      hdr[2] = a.clear[2];
+    for (uint32_t k = 0; k < cnt; k++)
+      ofold_fragment<SH>(a, st, x, y, ord[k]);
+  } else {
+    uint32_t last = 0;
+    for (uint32_t k = 0; k < total; k++) {
+      bool found = false;
+      uint32_t best = 0, steps = 0;
+      for (uint32_t node = head; node != 0xffffffffu && node < a.frag_cap;
+           node = a.frags[node].x) {
+        const uint32_t o = a.frags[node].y;
+        if ((k == 0 || o > last) && (!found || o < best)) {
+          best = o;
+          found = true;
+        }
+        if (++steps >= total)
+          break;
+      }
+      if (!found)
+        break;
+      ofold_fragment<SH>(a, st, x, y, best);
+      last = best;
     }
-    float depth = a.depth[px];
-    uint32_t id = a.ids[px];
-    /* a depth-write-off draw's depth is undone when the draw ends: `saved`
-     * holds the depth from before it, `cur` the draw of the last fragment */
-    float saved = depth;
-    uint32_t cur = 0xffffffffu;
-    bool cur_nw = false;
-    for (uint32_t k = 0; k < cnt; k++) {
-      const uint32_t rid = record_of(a, ord[k]);
-      if (rid >= a.rec_cap)
-        continue;
-      const RasterRec r = a.rrec[rid];
-      const ShadeRec s = a.srec[rid];
-      const uint32_t di = s.draw < a.draw_count ? s.draw : 0;
-      const DrawRec &d = a.draws[di];
-      if (di != cur) {
-        if (cur_nw)
-          depth = saved; /* cpu_backend.c:575-580 */
-        cur = di;
-        cur_nw = (d.flags & DF_NO_DEPTH_WRITE) != 0;
-        if (cur_nw)
-          saved = depth; /* cpu_backend.c:536-544 */
-      }
-      const bool dtest = !(d.flags & DF_NO_DEPTH_TEST);
-      const int jr = y - (int)r.y0, kc = x - (int)r.x0;
-      if (r.y1 & REC_FLAT_BIT) { /* rasterize_filled_triangle, rasterizer.c:1000-1083 */
-        const float z = fold_add(fold_add(r.zc[0], r.zc[2], jr), r.zc[1], kc);
-        if (!dtest || z < depth) {
-          const float ca = d.opacity < 0.0f ? 0.0f : (d.opacity > 1.0f ? 1.0f : d.opacity);
-          if (d.blend_mode == 0 && ca >= 1.0f) {
-            hdr[0] = s.col[0];
-            hdr[1] = s.col[1];
-            hdr[2] = s.col[2];
-            depth = z;
-            id = d.object_id;
-          } else { /* blended: colour only, no depth or ID write */
-            const float inv_a = 1.0f - ca;
-            for (int c = 0; c < 3; c++) {
-              if (d.blend_mode == 2)
-                hdr[c] = hdr[c] + s.col[c] * ca;
-              else if (d.blend_mode == 3)
-                hdr[c] = hdr[c] * s.col[c];
-              else
-                hdr[c] = s.col[c] * ca + hdr[c] * inv_a;
-            }
-          }
-        }
-        continue;
-      }
-      float w[3];
-      for (int e = 0; e < 3; e++)
-        w[e] = fold_add(fold_add(r.w0[e], r.dy[e], jr), r.dx[e], kc);
-      const float b0 = w[0] * r.inv_area, b1 = w[1] * r.inv_area, b2 = w[2] * r.inv_area;
-      const float z = b0 * r.zc[0] + b1 * r.zc[1] + b2 * r.zc[2];
-      if (dtest && !(z < depth))
-        continue;
-      if (s.v[0] >= a.vertex_cap || s.v[1] >= a.vertex_cap || s.v[2] >= a.vertex_cap)
-        continue;
-      const float4 N[3] = {a.normal[s.v[0]], a.normal[s.v[1]], a.normal[s.v[2]]};
-      float pc[3] = {b0 * N[0].w, b1 * N[1].w, b2 * N[2].w};
-      const float ip = 1.0f / (pc[0] + pc[1] + pc[2]);
-      pc[0] *= ip;
-      pc[1] *= ip;
-      pc[2] *= ip;
-      /* edge-distance coverage (rasterizer.c:1899-1938, 1320-1361) */
-      float min_d = 0.0f;
-      for (int e = 0; e < 3; e++) {
-        const float len = sqrtf(r.dx[e] * r.dx[e] + r.dy[e] * r.dy[e]);
-        const float inv = len > 1e-6f ? 1.0f / len : 0.0f;
-        const float de = w[e] * inv;
-        if (e == 0 || de < min_d)
-          min_d = de;
-      }
-      const bool legacy = !(d.flags & DF_LIT);
-      if (legacy && !(min_d >= 0.0f))
-        continue;
-      float p[3];
-      if (legacy)
-        shade_legacy(a, d, s.v, N, pc, p);
-      else
-        shade_smooth<SH>(a, d, a.lights + d.light_off, s.v, N, pc, p);
-      const float op = d.opacity < 0.0f ? 0.0f : (d.opacity > 1.0f ? 1.0f : d.opacity);
-      /* the legacy path blends at silhouettes only: where the sample's depth
-       * so far lies clearly behind the fragment (rasterizer.c:1425-1429);
-       * the multi-light path blends at every edge of a non-opaque draw
-       * (rasterizer.c:2097-2100) */
-      const float cov = legacy ? ((min_d < 1.0f && (depth - z) > 0.005f) ? min_d : 1.0f)
-                               : ((min_d < 1.0f && d.blend_mode != 0) ? min_d : 1.0f);
-      const float fa = op * cov;
-      if (d.blend_mode == 0 && fa >= 1.0f) {
-        hdr[0] = p[0];
-        hdr[1] = p[1];
-        hdr[2] = p[2];
-        depth = z;
-        id = d.object_id;
-      } else {
-        const float inv = 1.0f - fa;
-        for (int c = 0; c < 3; c++) {
-          if (d.blend_mode == 2)
-            hdr[c] = hdr[c] + p[c] * fa;
-          else if (d.blend_mode == 3)
-            hdr[c] = hdr[c] * p[c];
-          else
-            hdr[c] = p[c] * fa + hdr[c] * inv;
-        }
-        if (fa > 0.5f) {
-          depth = z;
-          id = d.object_id;
-        }
-      }
-    }
-    if (cur_nw)
-      depth = saved;
-    /* mop_sw_hdr_resolve (rasterizer.c:2776-2803) of the composited sample */
-    if (id == 0u)
-      a.pre[px] = make_uchar4(x86_f2u8(fminf(hdr[0], 1.0f) * 255.0f + 0.5f),
-                              x86_f2u8(fminf(hdr[1], 1.0f) * 255.0f + 0.5f),
-                              x86_f2u8(fminf(hdr[2], 1.0f) * 255.0f + 0.5f), 255);
-    else
-      a.pre[px] = make_uchar4(u8_of(aces(hdr[0] * a.exposure) * 255.0f + 0.5f),
-                              u8_of(aces(hdr[1] * a.exposure) * 255.0f + 0.5f),
-                              u8_of(aces(hdr[2] * a.exposure) * 255.0f + 0.5f), 255);
-    a.depth[px] = depth;
-    a.ids[px] = id;
   }
+  if (st.cur_nw)
+    st.depth = st.saved;
+  /* mop_sw_hdr_resolve (rasterizer.c:2776-2803) of the composited sample */
+  if (st.id == 0u)
+    a.pre[px] = make_uchar4(x86_f2u8(fminf(st.hdr[0], 1.0f) * 255.0f + 0.5f),
+                            x86_f2u8(fminf(st.hdr[1], 1.0f) * 255.0f + 0.5f),
+                            x86_f2u8(fminf(st.hdr[2], 1.0f) * 255.0f + 0.5f), 255);
+  else
+    a.pre[px] = make_uchar4(u8_of(aces(st.hdr[0] * a.exposure) * 255.0f + 0.5f),
+                            u8_of(aces(st.hdr[1] * a.exposure) * 255.0f + 0.5f),
+                            u8_of(aces(st.hdr[2] * a.exposure) * 255.0f + 0.5f), 255);
+  a.depth[px] = st.depth;
+  a.ids[px] = st.id;
+}
+
+template <bool SH>
+__global__ void __launch_bounds__(128) k_ofold(FrameArgs a) {
+  const uint32_t n = a.ctr->touched_count;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    ofold_item<SH>(a, i);
 }
 
 /* ========================================================================
@@ -2398,73 +2339,172 @@ __device__ bool draw_culled(const float *m, const DrawBound &bd, bool zplanes) {
   return false;
 }
 
-/* Per viewport (one block of 256): mvp = P * (V * M) per scene draw, cull
- * by bounding sphere, and compact the visible draws in submission order
- * with their vertex/triangle bases; the triangle order of the survivors is
- * the scene's, so depth ties resolve as in the full frame. */
+/* Block-wide (256 threads) exclusive prefix of K counters in thread order,
+ * continuing the running totals s_tot (updated): off[k] is this thread's
+ * offset. */
+template <int K>
+__device__ __forceinline__ void block_prefix(const uint32_t x[K], uint32_t off[K],
+                                             uint32_t (*s_w)[K], uint32_t *s_tot) {
+  const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+  uint32_t incl[K];
+#pragma unroll
+  for (int k = 0; k < K; k++) {
+    incl[k] = x[k];
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xffffffffu, incl[k], o);
+      if (lane >= (uint32_t)o)
+        incl[k] += y;
+    }
+    if (lane == 31u)
+      s_w[warp][k] = incl[k];
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int k = 0; k < K; k++) {
+      uint32_t run = s_tot[k];
+      for (int w = 0; w < 8; w++) {
+        const uint32_t t = s_w[w][k];
+        s_w[w][k] = run;
+        run += t;
+      }
+      s_tot[k] = run;
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int k = 0; k < K; k++)
+    off[k] = s_w[warp][k] + incl[k] - x[k];
+  __syncthreads(); /* s_w is reused by the next call */
+}
+
+/* mvp = P * (V * M) of scene draw i in viewport vw; false when the draw has
+ * no triangles or its bounding sphere is outside the frustum. */
+__device__ __forceinline__ bool view_draw(const SceneDesc &sc, const ViewRec &vw, uint32_t i,
+                                          float mvp[16]) {
+  const DrawRec &sd = sc.draws[i];
+  float vm[16];
+  dev_mat4_mul(vw.view, sd.model, vm);
+  dev_mat4_mul(vw.proj, vm, mvp);
+  return sd.index_count / 3u > 0u && !draw_culled(mvp, sc.bounds[i], sd.depth_bias == 0.0f);
+}
+
+__device__ __forceinline__ void emit_view_draw(const SceneDesc &sc, const ViewRec &vw, uint32_t i,
+                                               const float mvp[16], DrawRec *out, uint32_t pos,
+                                               uint32_t vbase, uint32_t tbase) {
+  DrawRec r = sc.draws[i];
+  for (int k = 0; k < 16; k++)
+    r.mvp[k] = mvp[k];
+  r.cam_eye[0] = vw.eye[0];
+  r.cam_eye[1] = vw.eye[1];
+  r.cam_eye[2] = vw.eye[2];
+  r.vbase = vbase;
+  r.tbase = tbase;
+  out[pos] = r;
+}
+
+/* Per viewport (one block of 256): the viewport's draw list in the core's
+ * pass order (viewport.c:2449-2553) — the visible non-blended draws in scene
+ * order, then the visible blended draws back to front by the float squared
+ * distance of their translation to the eye (the core's insertion sort:
+ * farthest first, ties keep scene order) — with mvp = P * (V * M), culling
+ * by bounding sphere and the draws' vertex/triangle bases.  Depth ties
+ * resolve as in the full frame; the first draw flagged DF_ORDERED, or the
+ * first blended one, starts the viewport's ordered suffix (t_split). */
 __global__ void __launch_bounds__(256) k_batch_prepare(BatchArgs b) {
-  __shared__ uint32_t s_w[8][3];
-  __shared__ uint32_t s_tot[3];
+  __shared__ uint32_t s_w[8][4];
+  __shared__ uint32_t s_tot[4];
+  __shared__ uint32_t s_bl[BATCH_MAX_BLENDED]; /* blended draws, scene order */
+  __shared__ float s_bd[BATCH_MAX_BLENDED];    /* their squared eye distances */
+  __shared__ uint32_t s_by[BATCH_MAX_BLENDED]; /* back-to-front position -> s_bl slot */
+  __shared__ uint32_t s_split, s_nan;
   const uint32_t v = blockIdx.x;
   const ViewRec &vw = b.views[v];
   const SceneDesc &sc = b.scenes[vw.scene];
   DrawRec *out = b.view_draws + vw.draw_off;
-  const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
-  if (threadIdx.x == 0)
-    s_tot[0] = s_tot[1] = s_tot[2] = 0u;
+  if (threadIdx.x == 0) {
+    s_tot[0] = s_tot[1] = s_tot[2] = s_tot[3] = 0u;
+    s_split = 0xffffffffu;
+    s_nan = 0u;
+  }
   __syncthreads();
   for (uint32_t base = 0; base < sc.nd; base += 256u) {
     const uint32_t i = base + threadIdx.x;
     float mvp[16];
-    uint32_t x[3] = {0u, 0u, 0u};
-    if (i < sc.nd) {
+    uint32_t x[4] = {0u, 0u, 0u, 0u}, off[4];
+    if (i < sc.nd && view_draw(sc, vw, i, mvp)) {
       const DrawRec &sd = sc.draws[i];
-      float vm[16];
-      dev_mat4_mul(vw.view, sd.model, vm);
-      dev_mat4_mul(vw.proj, vm, mvp);
-      const uint32_t tc = sd.index_count / 3u;
-      if (tc > 0u && !draw_culled(mvp, sc.bounds[i], sd.depth_bias == 0.0f)) {
+      if (sd.blend_mode == 0) {
         x[0] = 1u;
         x[1] = sd.vertex_count;
-        x[2] = tc;
+        x[2] = sd.index_count / 3u;
+      } else {
+        x[3] = 1u;
       }
     }
-    uint32_t incl[3];
-    for (int k = 0; k < 3; k++) {
-      incl[k] = x[k];
-      for (int o = 1; o < 32; o <<= 1) {
-        const uint32_t y = __shfl_up_sync(0xffffffffu, incl[k], o);
-        if (lane >= (uint32_t)o)
-          incl[k] += y;
-      }
-      if (lane == 31u)
-        s_w[warp][k] = incl[k];
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      for (int k = 0; k < 3; k++) {
-        uint32_t run = s_tot[k];
-        for (int w = 0; w < 8; w++) {
-          const uint32_t t = s_w[w][k];
-          s_w[w][k] = run;
-          run += t;
-        }
-        s_tot[k] = run;
-      }
-    }
-    __syncthreads();
+    block_prefix<4>(x, off, s_w, s_tot);
     if (x[0]) {
-      DrawRec r = sc.draws[i];
-      for (int k = 0; k < 16; k++)
-        r.mvp[k] = mvp[k];
-      r.cam_eye[0] = vw.eye[0];
-      r.cam_eye[1] = vw.eye[1];
-      r.cam_eye[2] = vw.eye[2];
-      r.vbase = s_w[warp][1] + incl[1] - x[1];
-      r.tbase = s_w[warp][2] + incl[2] - x[2];
-      out[s_w[warp][0] + incl[0] - x[0]] = r;
+      emit_view_draw(sc, vw, i, mvp, out, off[0], off[1], off[2]);
+      if (sc.draws[i].flags & DF_ORDERED)
+        atomicMin(&s_split, off[2]);
     }
-    __syncthreads();
+    if (x[3] && off[3] < BATCH_MAX_BLENDED) {
+      const float *m = sc.draws[i].model;
+      const float dx = __fsub_rn(m[12], vw.eye[0]), dy = __fsub_rn(m[13], vw.eye[1]),
+                  dz = __fsub_rn(m[14], vw.eye[2]);
+      const float d2 = __fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), __fmul_rn(dz, dz));
+      s_bl[off[3]] = i;
+      s_bd[off[3]] = d2;
+      if (d2 != d2)
+        s_nan = 1u;
+    }
+  }
+  __syncthreads();
+  const uint32_t nb = s_tot[3] < BATCH_MAX_BLENDED ? s_tot[3] : BATCH_MAX_BLENDED;
+  if (!s_nan) {
+    /* the stable descending order as ranks: the draws farther away, then the
+     * equally far ones earlier in scene order */
+    for (uint32_t j = threadIdx.x; j < nb; j += 256u) {
+      const float dj = s_bd[j];
+      uint32_t r = 0;
+      for (uint32_t k = 0; k < nb; k++) {
+        const float dk = s_bd[k];
+        r += (dk > dj || (dk == dj && k < j)) ? 1u : 0u;
+      }
+      s_by[r] = j;
+    }
+  } else if (threadIdx.x == 0) {
+    /* a NaN distance: the reference's insertion sort itself */
+    for (uint32_t j = 0; j < nb; j++)
+      s_by[j] = j;
+    for (uint32_t j = 1; j < nb; j++) {
+      const uint32_t key = s_by[j];
+      const float kd = s_bd[key];
+      int k = (int)j - 1;
+      while (k >= 0 && s_bd[s_by[k]] < kd) {
+        s_by[k + 1] = s_by[k];
+        k--;
+      }
+      s_by[k + 1] = key;
+    }
+  }
+  if (threadIdx.x == 0 && nb)
+    atomicMin(&s_split, s_tot[2]); /* the first blended draw */
+  __syncthreads();
+  for (uint32_t base = 0; base < nb; base += 256u) {
+    const uint32_t j = base + threadIdx.x;
+    float mvp[16];
+    uint32_t x[4] = {0u, 0u, 0u, 0u}, off[4];
+    uint32_t i = 0;
+    if (j < nb) {
+      i = s_bl[s_by[j]];
+      view_draw(sc, vw, i, mvp);
+      x[0] = 1u;
+      x[1] = sc.draws[i].vertex_count;
+      x[2] = sc.draws[i].index_count / 3u;
+    }
+    block_prefix<4>(x, off, s_w, s_tot);
+    if (x[0])
+      emit_view_draw(sc, vw, i, mvp, out, off[0], off[1], off[2]);
   }
   if (threadIdx.x == 0) {
     FrameArgs a = b.tmpl;
@@ -2499,25 +2539,45 @@ __global__ void __launch_bounds__(256) k_batch_prepare(BatchArgs b) {
     for (int k = 0; k < 4; k++)
       a.clear[k] = vw.clear[k];
     a.ctr = b.ctr + v;
+    /* the suffix: its buffers here, its pools from k_batch_alloc */
+    a.t_split = s_split;
+    a.ordered_keep_all = 0;
+    a.frags = nullptr;
+    a.frag_cap = 0u;
+    a.olist = a.olist_items = nullptr;
+    a.olist_cap = 0u;
+    if (s_split != 0xffffffffu && b.hdr) {
+      a.hdr = b.hdr + vw.sample_off;
+      a.frag_head = b.frag_head + vw.sample_off;
+      a.touched = b.touched + vw.sample_off;
+    } else {
+      if (s_split != 0xffffffffu)
+        atomicOr(&b.status->overflow, 64u);
+      a.hdr = nullptr;
+      a.frag_head = a.touched = nullptr;
+    }
     b.frames[v] = a;
   }
 }
 
 /* One block of 256: carves every viewport's vertex streams, records, clip
- * queue and large list out of the batch pools (exclusive scans over the
- * viewports).  A viewport that does not fit renders nothing this time and
+ * queue, large list and — for a viewport with an ordered suffix — its
+ * suffix-record list and fragment pool out of the batch pools (exclusive
+ * scans over the viewports).  A viewport that does not fit renders nothing this time and
  * the status tells the host how large the pools must grow. */
 __global__ void __launch_bounds__(256) k_batch_alloc(BatchArgs b) {
-  __shared__ unsigned long long s_w[8][4];
-  __shared__ unsigned long long s_tot[4];
+  constexpr int NP = 6;
+  __shared__ unsigned long long s_w[8][NP];
+  __shared__ unsigned long long s_tot[NP];
   const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
-  const unsigned long long pool[4] = {b.vertex_pool, b.rec_pool, b.clip_pool, b.large_pool};
-  if (threadIdx.x < 4)
+  const unsigned long long pool[NP] = {b.vertex_pool, b.rec_pool,   b.clip_pool,
+                                       b.large_pool,  b.olist_pool, b.frag_pool};
+  if (threadIdx.x < NP)
     s_tot[threadIdx.x] = 0ull;
   __syncthreads();
   for (uint32_t base = 0; base < b.nv; base += 256u) {
     const uint32_t v = base + threadIdx.x;
-    unsigned long long need[4] = {0ull, 0ull, 0ull, 0ull};
+    unsigned long long need[NP] = {0ull, 0ull, 0ull, 0ull, 0ull, 0ull};
     if (v < b.nv) {
       const FrameArgs &a = b.frames[v];
       const unsigned long long T = a.total_tris, fan = T * b.fan_num / 8ull + 1024ull;
@@ -2525,9 +2585,14 @@ __global__ void __launch_bounds__(256) k_batch_alloc(BatchArgs b) {
       need[1] = T + fan;
       need[2] = fan;
       need[3] = T * b.large_num / 16ull + 1024ull;
+      if (a.hdr) {
+        need[4] = (T - (a.t_split < T ? a.t_split : T)) + fan;
+        need[5] = (unsigned long long)a.width * (unsigned long long)a.height * b.frag_num / 4ull +
+                  4096ull;
+      }
     }
-    unsigned long long incl[4];
-    for (int k = 0; k < 4; k++) {
+    unsigned long long incl[NP];
+    for (int k = 0; k < NP; k++) {
       incl[k] = need[k];
       for (int o = 1; o < 32; o <<= 1) {
         const unsigned long long y = __shfl_up_sync(0xffffffffu, incl[k], o);
@@ -2539,7 +2604,7 @@ __global__ void __launch_bounds__(256) k_batch_alloc(BatchArgs b) {
     }
     __syncthreads();
     if (threadIdx.x == 0) {
-      for (int k = 0; k < 4; k++) {
+      for (int k = 0; k < NP; k++) {
         unsigned long long run = s_tot[k];
         for (int w = 0; w < 8; w++) {
           const unsigned long long t = s_w[w][k];
@@ -2551,9 +2616,9 @@ __global__ void __launch_bounds__(256) k_batch_alloc(BatchArgs b) {
     }
     __syncthreads();
     if (v < b.nv) {
-      unsigned long long off[4];
+      unsigned long long off[NP];
       bool fits = true;
-      for (int k = 0; k < 4; k++) {
+      for (int k = 0; k < NP; k++) {
         off[k] = s_w[warp][k] + incl[k] - need[k];
         if (off[k] + need[k] > pool[k]) {
           fits = false;
@@ -2565,9 +2630,11 @@ __global__ void __launch_bounds__(256) k_batch_alloc(BatchArgs b) {
         a.draw_count = 0u;
         a.total_vertices = 0u;
         a.total_tris = 0u;
-        for (int k = 0; k < 4; k++)
+        a.hdr = nullptr;
+        for (int k = 0; k < NP; k++) {
           off[k] = 0ull;
-        need[0] = need[1] = need[2] = need[3] = 0ull;
+          need[k] = 0ull;
+        }
       }
       a.clip = b.clip + off[0];
       a.world = b.world + off[0];
@@ -2582,6 +2649,13 @@ __global__ void __launch_bounds__(256) k_batch_alloc(BatchArgs b) {
       a.large_list = b.large_list + off[3];
       a.large_items = b.large_items + off[3];
       a.large_cap = (uint32_t)need[3];
+      if (a.hdr) {
+        a.olist = b.olist + off[4];
+        a.olist_items = b.olist_items + off[4];
+        a.olist_cap = (uint32_t)need[4];
+        a.frags = b.frags + off[5];
+        a.frag_cap = (uint32_t)(need[5] < 0xfffffff0ull ? need[5] : 0xfffffff0ull);
+      }
     }
     __syncthreads();
   }
@@ -2590,10 +2664,13 @@ __global__ void __launch_bounds__(256) k_batch_alloc(BatchArgs b) {
     b.status->need_rec = s_tot[1];
     b.status->need_clip = s_tot[2];
     b.status->need_large = s_tot[3];
+    b.status->need_olist = s_tot[4];
+    b.status->need_frag = s_tot[5];
   }
 }
 
-enum { ST_VERTEX, ST_SETUP, ST_CLIP, ST_RSMALL, ST_RLARGE, ST_SHADE, ST_RESOLVE };
+enum { ST_VERTEX, ST_SETUP, ST_CLIP, ST_RSMALL, ST_RLARGE, ST_SHADE, ST_RESOLVE, ST_OCOUNT,
+       ST_ORASTER, ST_OFOLD };
 
 template <int ST> __device__ __forceinline__ uint32_t stage_count(const FrameArgs &a) {
   switch (ST) {
@@ -2609,6 +2686,12 @@ template <int ST> __device__ __forceinline__ uint32_t stage_count(const FrameArg
     return a.total_tris ? a.ctr->large_items : 0u;
   case ST_SHADE:
     return a.ctr->shade_count;
+  case ST_OCOUNT:
+    return a.hdr && a.total_tris ? ordered_record_items(a) : 0u;
+  case ST_ORASTER:
+    return a.hdr ? a.ctr->olist_items : 0u;
+  case ST_OFOLD:
+    return a.hdr ? a.ctr->touched_count : 0u;
   default: /* ST_RESOLVE: chunks of 256 x RESOLVE_PER_THREAD samples */
     return ((uint32_t)a.width * (uint32_t)a.height + 256u * RESOLVE_PER_THREAD - 1u) /
            (256u * RESOLVE_PER_THREAD);
@@ -2705,6 +2788,55 @@ __global__ void __launch_bounds__(256, 4) k_b_shade(const FrameArgs *__restrict_
   }
 }
 
+/* The ordered suffix of every viewport that has one, as the single-frame
+ * kernels run it: queue the suffix records, scan their item counts (a block
+ * per viewport), rasterise them into fragment lists, fold each touched
+ * sample's list in submission order. */
+__global__ void __launch_bounds__(256) k_b_ocount(const FrameArgs *__restrict__ fr, uint32_t nv) {
+  __shared__ uint32_t s_pre[MOPCUDA_MAX_VIEWS + 1];
+  const uint32_t total = views_prefix<ST_OCOUNT>(fr, nv, s_pre);
+  uint32_t v = 0;
+  for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < total;
+       g += gridDim.x * blockDim.x) {
+    while (s_pre[v + 1] <= g)
+      v++;
+    ocount_item(fr[v], g - s_pre[v]);
+  }
+}
+
+__global__ void __launch_bounds__(1024) k_b_oscan(const FrameArgs *__restrict__ fr) {
+  __shared__ uint32_t part[32];
+  const FrameArgs &a = fr[blockIdx.x];
+  if (a.hdr)
+    items_scan_block(a.olist_items, olist_len(a), &a.ctr->olist_items, part);
+}
+
+__global__ void __launch_bounds__(256) k_b_oraster(const FrameArgs *__restrict__ fr, uint32_t nv) {
+  __shared__ uint32_t s_pre[MOPCUDA_MAX_VIEWS + 1];
+  const uint32_t total = views_prefix<ST_ORASTER>(fr, nv, s_pre);
+  uint32_t v = 0;
+  for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < total;
+       g += gridDim.x * blockDim.x) {
+    while (s_pre[v + 1] <= g)
+      v++;
+    const FrameArgs &a = fr[v];
+    oraster_item(a, g - s_pre[v], olist_len(a));
+  }
+}
+
+template <bool SH>
+__global__ void __launch_bounds__(128) k_b_ofold(const FrameArgs *__restrict__ fr, uint32_t nv) {
+  __shared__ uint32_t s_pre[MOPCUDA_MAX_VIEWS + 1];
+  const uint32_t total = views_prefix<ST_OFOLD>(fr, nv, s_pre);
+  uint32_t v = 0;
+  for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < total;
+       g += gridDim.x * blockDim.x) {
+    while (s_pre[v + 1] <= g)
+      v++;
+    ofold_item<SH>(fr[v], g - s_pre[v]);
+  }
+}
+
 template <int SF>
 __device__ __forceinline__ uint32_t post_tiles_of(const PostArgs &p) {
   const uint32_t pw = (uint32_t)(p.width / SF), ph = (uint32_t)(p.height / SF);
@@ -2774,7 +2906,7 @@ void mopcuda_batch_grids(BatchLaunch &cfg) {
 
 int mopcuda_launch_batch(const BatchArgs &b, const PostArgs *posts, const uint32_t *post_views[4],
                          const uint32_t post_count[4], const uint32_t post_tiles[4],
-                         const BatchLaunch &cfg, bool shared_lights, bool shadows,
+                         const BatchLaunch &cfg, bool shared_lights, bool shadows, bool ordered,
                          cudaStream_t s, int parts) {
   if (b.nv == 0)
     return 0;
@@ -2804,6 +2936,17 @@ int mopcuda_launch_batch(const BatchArgs &b, const PostArgs *posts, const uint32
     else
       k_b_shade<false><<<cfg.grid_shade, cfg.shade_block, 0, s>>>(fr, nv, shared_lights ? 1 : 0);
     launches += 10;
+    if (ordered && b.hdr) {
+      cudaMemsetAsync(b.frag_head, 0xff, sizeof(uint32_t) * (size_t)b.samples, s);
+      k_b_ocount<<<sms * 8, 256, 0, s>>>(fr, nv);
+      k_b_oscan<<<nv, 1024, 0, s>>>(fr);
+      k_b_oraster<<<sms * 8, 256, 0, s>>>(fr, nv);
+      if (shadows)
+        k_b_ofold<true><<<sms * 8, 128, 0, s>>>(fr, nv);
+      else
+        k_b_ofold<false><<<sms * 8, 128, 0, s>>>(fr, nv);
+      launches += 4;
+    }
   }
   if (!(parts & BATCH_PART_POST))
     return launches;

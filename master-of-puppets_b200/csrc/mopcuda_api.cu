@@ -1282,9 +1282,6 @@ static int finish_frame(MopCudaDevice *d, int timeout_ms, bool defer_readback) {
     d->clip_hint = c->clip_count + c->clip_count / 4 + 1024;
     d->extra_hint = c->extra_vertices + c->extra_vertices / 4 + 1024;
     d->large_hint = c->large_count + c->large_count / 4 + 1024;
-    if (c->overflow & 64u)
-      return fail(MOPCUDA_EUNSUPPORTED, "frame: more than %d blended fragments on one sample",
-                  ORDERED_MAX_FRAGS);
     if (c->overflow & 16u)
       d->frag_hint = c->frag_count + c->frag_count / 4 + 65536;
     if (c->overflow & 32u)

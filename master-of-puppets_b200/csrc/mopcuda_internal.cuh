@@ -35,6 +35,9 @@ enum DrawFlags : uint32_t {
   /* !depth_test: every covered fragment passes (rasterizer.c:1948) and
    * writes depth */
   DF_NO_DEPTH_TEST = 1u << 6,
+  /* scene draws of a batch: blended, translucent or unlit smooth — the draw
+   * starts its viewport's ordered suffix (set by the host) */
+  DF_ORDERED = 1u << 7,
 };
 
 /* One recorded draw, uploaded per frame (the MopRhiDrawCall fields the path
@@ -124,13 +127,13 @@ struct Counters {
                                  queue, bit3 large list                          */
   uint32_t shade_count;       /* covered samples queued for shading              */
   /* ordered (blended) suffix of the frame; overflow bit4 fragment pool,
-   * bit5 ordered-record list, bit6 more than ORDERED_MAX_FRAGS fragments on
-   * one sample */
+   * bit5 ordered-record list */
   uint32_t frag_count, touched_count, olist_count, olist_items;
   uint32_t pad;
 };
 
-/* Blended fragments one sample may receive in a frame. */
+/* Blended fragments of one sample sorted in registers; a sample with more
+ * is composited by an in-order selection walk of its list. */
 #define ORDERED_MAX_FRAGS 48
 
 /* Records whose clamped bbox exceeds these bounds are rasterised as
@@ -391,10 +394,15 @@ struct DrawBound {
 /* Pool sizes that the allocation pass found too small; the host grows the
  * pools to at least these and re-runs the batch. */
 struct BatchStatus {
-  uint32_t overflow; /* bit0 vertex, bit1 records, bit2 clip queue, bit3 large list */
+  uint32_t overflow; /* bit0 vertex, bit1 records, bit2 clip queue, bit3 large list,
+                        bit4 ordered-record lists, bit5 fragment pool, bit6 a viewport
+                        with an ordered suffix in a launch without suffix buffers */
   uint32_t pad;
-  unsigned long long need_vertex, need_rec, need_clip, need_large;
+  unsigned long long need_vertex, need_rec, need_clip, need_large, need_olist, need_frag;
 };
+
+/* Blended draws of one scene a batch viewport sorts back to front. */
+#define BATCH_MAX_BLENDED 1024
 
 struct BatchArgs {
   const SceneDesc *scenes;
@@ -420,9 +428,20 @@ struct BatchArgs {
   uchar4 *pre;
   float *depth;
   uint32_t *ids;
+  /* ordered suffix (null when no scene of the launch has one): per-sample
+   * composition buffers at the viewports' sample offsets, and pools of
+   * fragments and suffix-record lists carved per viewport */
+  float4 *hdr;
+  uint32_t *frag_head, *touched;
+  uint2 *frags;
+  unsigned long long frag_pool;
+  uint32_t *olist, *olist_items;
+  unsigned long long olist_pool;
+  unsigned long long samples; /* samples of the launch (frag_head's length) */
   /* per-viewport reserves: clipped fans (records, extra vertices, clip
-   * queue) T * fan_num / 8 + 1024; large list T * large_num / 16 + 1024 */
-  uint32_t fan_num, large_num;
+   * queue) T * fan_num / 8 + 1024; large list T * large_num / 16 + 1024;
+   * fragments S * frag_num / 4 + 4096 */
+  uint32_t fan_num, large_num, frag_num;
 };
 
 /* Per-stage launch shape of a batch (the autotuner's search space). */
@@ -447,9 +466,11 @@ void mopcuda_batch_grids(BatchLaunch &cfg);
  * post passes, which write the colour images). */
 #define BATCH_PART_MAIN 1
 #define BATCH_PART_POST 2
+/* ordered: the launch has suffix buffers (b.hdr): the suffix kernels run
+ * after shading for the viewports that have a suffix. */
 int mopcuda_launch_batch(const BatchArgs &b, const PostArgs *posts, const uint32_t *post_views[4],
                          const uint32_t post_count[4], const uint32_t post_tiles[4],
-                         const BatchLaunch &cfg, bool shared_lights, bool shadows,
+                         const BatchLaunch &cfg, bool shared_lights, bool shadows, bool ordered,
                          cudaStream_t s, int parts = BATCH_PART_MAIN | BATCH_PART_POST);
 
 /* ev (optional, 7 events): stage boundaries

@@ -586,9 +586,10 @@ class SceneRenderer(_Resident):
         sc = self.scene
         self._orbit_eye = np.zeros(3, np.float32)
         self._orbit_up = np.zeros(3, np.float32)
-        self.L.mopcuda_camera_orbit(_f32(sc.eye).ctypes.data, _f32(sc.target).ctypes.data,
-                                    _f32(sc.up).ctypes.data, self._orbit_eye.ctypes.data,
-                                    self._orbit_up.ctypes.data)
+        # the inputs stay referenced until the call returns
+        eye_in, target_in, up_in = _f32(sc.eye), _f32(sc.target), _f32(sc.up)
+        self.L.mopcuda_camera_orbit(eye_in.ctypes.data, target_in.ctypes.data, up_in.ctypes.data,
+                                    self._orbit_eye.ctypes.data, self._orbit_up.ctypes.data)
         self._target = _f32(sc.target)
         self._view_arr = _f32(self.view)
         self._proj_arr = _f32(self.proj)

@@ -711,6 +711,28 @@ def transparent_scene(seed: int = 12, width: int = 160, height: int = 120, ssaa:
     return sc
 
 
+def deep_transparent_scene(seed: int = 64, width: int = 160, height: int = 120, ssaa: int = 1,
+                           layers: int = 64) -> Scene:
+    """small_scene with `layers` blended quads stacked along z in front of
+    the camera (alpha, additive, multiply and alpha-promoted opaque, opacity
+    0.05-0.7), so the middle samples receive more blended fragments than a
+    sample's sorted register list holds (48): the selection walk composites
+    them."""
+    sc = small_scene(seed=seed, width=width, height=height, ssaa=ssaa)
+    rng = np.random.default_rng(seed + 200)
+    oid = max(m.object_id for m in sc.meshes) + 1
+    modes = [BLEND_ALPHA, BLEND_ADDITIVE, BLEND_MULTIPLY, BLEND_OPAQUE]
+    for k in range(layers):
+        j = rng.uniform(-0.15, 0.15, 4)
+        v, i = _quad(-1.3 + j[0], -0.9 + j[1], 1.3 + j[2], 0.9 + j[3], 0.0, _color(rng))
+        z = -1.5 + 3.0 * k / max(1, layers - 1)
+        m = mat_trs((float(rng.uniform(-0.1, 0.1)), 1.0, z), np.eye(3), (1.0, 1.0, 1.0))
+        sc.meshes.append(Mesh(v, i, oid, m, 0.0, 0.5, opacity=float(rng.uniform(0.05, 0.7)),
+                              blend_mode=modes[k % 4]))
+        oid += 1
+    return sc
+
+
 def instanced_scene(seed: int = 70, width: int = 192, height: int = 144, ssaa: int = 1,
                     n_instances: int = 96, transparent: bool = False, env: int = 0,
                     zero_id: bool = False) -> Scene:

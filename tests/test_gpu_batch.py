@@ -129,6 +129,73 @@ def test_batch_shadow_equals_single_viewport_frames(cuda_device, ibl):
         b.close()
 
 
+def _blended(sc):
+    """Every third instance blended (alpha / additive / multiply, opacity
+    0.35-0.75): each viewport sorts them back to front for its own eye."""
+    for k in range(0, len(sc.meshes), 3):
+        sc.meshes[k] = dataclasses.replace(sc.meshes[k], opacity=0.35 + 0.1 * (k % 5),
+                                           blend_mode=(1, 2, 3, 1)[k % 4])
+    return sc
+
+
+def test_batch_blended_equals_single_viewport_frames(cuda_device, ibl):
+    """Blended instances: every viewport composites its ordered suffix in the
+    core's back-to-front order for its own camera, as the plain frame does;
+    a TRS update that changes a blended instance's distance reorders it."""
+    sc = _blended(_scene(instances=24))
+    b = mopcuda.BatchRenderer(cuda_device, sc, _views(sc, 8, seed=21), ibl)
+    try:
+        b.render()
+        _check_batch(cuda_device, b, sc, ibl, "blended batch")
+        m = sc.meshes[3].transform.copy()
+        m[12:15] *= np.float32(-1.5)
+        b.set_model(3, m)
+        b.render()
+        moved = dataclasses.replace(sc, meshes=[dataclasses.replace(x, transform=m) if k == 3
+                                                else x for k, x in enumerate(sc.meshes)])
+        _check_batch(cuda_device, b, moved, ibl, "blended batch after TRS")
+    finally:
+        b.close()
+
+
+def test_batch_blended_shadow_and_unlit(cuda_device, ibl):
+    """Blended instances with the sun casting shadows (blended meshes cast
+    none), and a scene without lights (the unlit smooth path, order-dependent
+    for every draw): each viewport equals its plain frame."""
+    sc = _shadowed(_blended(_scene(instances=12)))
+    b = mopcuda.BatchRenderer(cuda_device, sc, _views(sc, 4, seed=22), ibl)
+    try:
+        b.render()
+        _check_batch(cuda_device, b, sc, ibl, "blended shadow batch")
+    finally:
+        b.close()
+    unlit = dataclasses.replace(_scene(instances=8), lights=[])
+    b = mopcuda.BatchRenderer(cuda_device, unlit, _views(unlit, 4, seed=23), None)
+    try:
+        b.render()
+        _check_batch(cuda_device, b, unlit, None, "unlit batch")
+    finally:
+        b.close()
+
+
+def test_batch_blended_matches_oracle(cuda_device):
+    """Blended meshes in a batch against the oracle directly (two cameras,
+    different back-to-front orders)."""
+    sc = scenes.transparent_scene(seed=24, width=96, height=72)
+    views = [scenes.View(96, 72, 1, sc.eye, sc.target, fov_deg=sc.fov_deg, near=sc.near,
+                         far=sc.far, clear=sc.clear),
+             scenes.View(80, 48, 2, (-5.0, 2.0, -4.0), (0.0, 0.5, 0.0), fov_deg=45.0, near=0.1,
+                         far=50.0, clear=sc.clear)]
+    b = mopcuda.BatchRenderer(cuda_device, sc, views)
+    try:
+        b.render()
+        for i, v in enumerate(views):
+            ref = cpu_oracle.render(scenes.scene_for_view(sc, v), None)
+            assert_frame_parity(_batch_view(b, i), ref, f"blended oracle view {i}")
+    finally:
+        b.close()
+
+
 def test_batch_read_views_equals_single_reads(cuda_device, ibl):
     """mopcuda_batch_read_views (every view's buffer in one call) returns the
     bytes of one mopcuda_batch_read per view, for each buffer, and rejects a

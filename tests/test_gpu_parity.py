@@ -72,6 +72,10 @@ CASES = {
     "transparent": lambda: scenes.transparent_scene(seed=21),
     "transparent_ssaa2_ibl": lambda: scenes.transparent_scene(seed=22, ssaa=2, env=1),
     "transparent_config2": lambda: _transparent_config2(),
+    # 64 stacked blended quads: samples with more than 48 fragments (selection walk)
+    "transparent_deep": lambda: scenes.deep_transparent_scene(seed=65),
+    "transparent_deep_ssaa2": lambda: scenes.deep_transparent_scene(seed=66, ssaa=2,
+                                                                    layers=80),
     # blended flat draws (colour only, no depth or ID writes) in the transparent pass
     "transparent_flat": lambda: dataclasses.replace(scenes.transparent_scene(seed=60),
                                                     smooth=False),

@@ -218,6 +218,35 @@ def test_server_shadowed_scene_in_a_mix(cuda_device, world):
         rs.close()
 
 
+def test_server_blended_scene_in_a_mix(cuda_device, world):
+    """A scene with blended instances served beside opaque ones in the same
+    launches: each request (its own camera, so its own back-to-front order)
+    equals its plain frame, and the opaque requests are unchanged."""
+    scs, rss, ibl = world
+    sc = scenes.config2(seed=15, width=160, height=90, ssaa=1, instances=15, tex_size=64)
+    for k in range(0, len(sc.meshes), 3):
+        sc.meshes[k] = dataclasses.replace(sc.meshes[k], opacity=0.4 + 0.1 * (k % 4),
+                                           blend_mode=(1, 2, 3)[k % 3])
+    rs = mopcuda.ResidentScene(cuda_device, sc, ibl)
+    srv = mopcuda.Server(cuda_device, hbm_budget=8 << 30, max_views=16, max_inflight=2)
+    try:
+        sid = [srv.add_scene(r) for r in rss] + [srv.add_scene(rs)]
+        vs = _views(sc, 3, seed=51)
+        mine = [srv.submit_render(sid[3], v, want_ids=True, want_depth=True) for v in vs]
+        others = [srv.submit_render(sid[k % 3], _views(scs[k % 3], 1, seed=60 + k)[0])
+                  for k in range(4)]
+        for t in mine + others:
+            srv.wait(t)
+        for k, (t, v) in enumerate(zip(mine, vs)):
+            _same_render(t, _plain(cuda_device, sc, v, ibl), f"blended request {k}")
+        for t in others:
+            s_ = scs[sid.index(t.req.scene)]
+            assert (t.color == _plain(cuda_device, s_, t.view, ibl)["color"]).all()
+    finally:
+        srv.close()
+        rs.close()
+
+
 def test_server_trs_update_between_requests(cuda_device, world):
     scs, rss, ibl = world
     srv = mopcuda.Server(cuda_device, hbm_budget=8 << 30, max_views=8, max_inflight=2)

@@ -68,6 +68,8 @@ LIVE = {
     # blended meshes (alpha / additive / multiply) in the core's transparent pass order
     "transparent": lambda: scenes.transparent_scene(seed=17),
     "transparent_ssaa2_ibl": lambda: scenes.transparent_scene(seed=18, ssaa=2, env=1),
+    # 64 stacked blended quads: more fragments on a sample than the device sorts in registers
+    "transparent_deep": lambda: scenes.deep_transparent_scene(seed=19),
     "config3_small": lambda: scenes.config3(seed=19, n_tris=30_000, width=320, height=180),
     # pass_shadow + PCF: smooth, flat, SSAA 2 with IBL, with the transparent pass
     "shadow": lambda: scenes.shadow_scene(seed=31),
