@@ -1706,11 +1706,30 @@ __device__ __forceinline__ void post_pixel(const PostArgs &a, const uchar4 (*s_c
   }
 }
 
+/* Persistent: each block loads the tables once and takes tiles blockIdx.x,
+ * blockIdx.x + gridDim.x, ... in row-major tile order. */
 template <int SF>
 __global__ void __launch_bounds__(POST_BX *POST_BY) k_post(PostArgs a) {
   __shared__ PostSmem<SF> sm;
   post_load_luts<SF>(a, sm);
-  post_tile<SF>(a, sm, (int)blockIdx.x, (int)blockIdx.y);
+  const uint32_t tx = ((uint32_t)(a.width / SF) + POST_BX - 1u) / POST_BX;
+  const uint32_t ty = ((uint32_t)(a.height / SF) + POST_BY - 1u) / POST_BY;
+  for (uint32_t t = blockIdx.x; t < tx * ty; t += gridDim.x)
+    post_tile<SF>(a, sm, (int)(t % tx), (int)(t / tx));
+}
+
+/* Blocks of k_post<SF> resident on one SM (queried once per factor). */
+template <int SF> static int post_resident() {
+  static int nb = 0;
+  if (nb == 0) {
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_post<SF>, POST_BX * POST_BY, 0) !=
+            cudaSuccess ||
+        nb < 1) {
+      cudaGetLastError();
+      nb = 1;
+    }
+  }
+  return nb;
 }
 
 template __global__ void k_post<1>(PostArgs);
@@ -1875,20 +1894,24 @@ int mopcuda_launch_frame(const FrameArgs &a, const PostArgs &p, const LaunchCfg 
     cudaStreamWaitEvent(s, post_wait, 0);
   const int sf = p.ssaa;
   dim3 pb(POST_BX, POST_BY);
-  dim3 pg(blocks_for((uint32_t)(p.width / sf), POST_BX),
-          blocks_for((uint32_t)(p.height / sf), POST_BY));
+  const uint32_t tiles = blocks_for((uint32_t)(p.width / sf), POST_BX) *
+                         blocks_for((uint32_t)(p.height / sf), POST_BY);
+  auto pgrid = [&](int resident) {
+    const uint32_t g = (uint32_t)cfg.num_sms * (uint32_t)resident;
+    return tiles < g ? (tiles ? tiles : 1u) : g;
+  };
   switch (sf) {
   case 2:
-    k_post<2><<<pg, pb, 0, s>>>(p);
+    k_post<2><<<pgrid(post_resident<2>()), pb, 0, s>>>(p);
     break;
   case 3:
-    k_post<3><<<pg, pb, 0, s>>>(p);
+    k_post<3><<<pgrid(post_resident<3>()), pb, 0, s>>>(p);
     break;
   case 4:
-    k_post<4><<<pg, pb, 0, s>>>(p);
+    k_post<4><<<pgrid(post_resident<4>()), pb, 0, s>>>(p);
     break;
   default:
-    k_post<1><<<pg, pb, 0, s>>>(p);
+    k_post<1><<<pgrid(post_resident<1>()), pb, 0, s>>>(p);
     break;
   }
   launches++;
