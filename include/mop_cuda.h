@@ -99,7 +99,7 @@ typedef struct MopCudaDraw {
   float depth_bias;
   float cam_eye[3];
   int32_t smooth;        /* MOP_SHADING_SMOOTH                              */
-  int32_t wireframe;
+  int32_t wireframe;     /* the triangles' edges as anti-aliased lines       */
   int32_t depth_test;
   int32_t depth_write;
   int32_t backface_cull;

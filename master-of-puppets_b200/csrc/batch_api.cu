@@ -151,10 +151,10 @@ extern "C" int mopcuda_scene_add_draw(MopCudaScene *s, const MopCudaDraw *c) {
     s->lights.resize(nl);
     return rc;
   }
-  if (!skip && (r.flags & (DF_NO_DEPTH_WRITE | DF_NO_DEPTH_TEST))) {
+  if (!skip && (r.flags & (DF_NO_DEPTH_WRITE | DF_NO_DEPTH_TEST | DF_WIRE))) {
     s->lights.resize(nl);
-    return fail(MOPCUDA_EUNSUPPORTED,
-                "scene_add_draw: batches render depth-tested, depth-writing draws only");
+    return fail(MOPCUDA_EUNSUPPORTED, "scene_add_draw: batches render filled, depth-tested, "
+                                      "depth-writing draws only");
   }
   if (skip) { /* zero opacity: a colour no-op, kept as an empty slot */
     memset(&r, 0, sizeof r);

@@ -628,11 +628,21 @@ __device__ bool fan_setup(const FrameArgs &a, const DrawRec &d, const CV v[3], c
   float sarea = (sx[1] - sx[0]) * (sy[2] - sy[0]) - (sx[2] - sx[0]) * (sy[1] - sy[0]);
   if ((d.flags & DF_CULL) && sarea >= 0.0f)
     return false;
-  if (!edge_setup(sx, sy, a.width, a.height, rr))
+  const bool wire = (d.flags & DF_WIRE) != 0;
+  if (wire) { /* the edges are drawn whatever the area (rasterizer.c:1225-1235) */
+    for (int k = 0; k < 3; k++) {
+      rr.w0[k] = sx[k];
+      rr.dx[k] = sy[k];
+      rr.dy[k] = sz[k];
+    }
+    rr.x0 = rr.y0 = rr.y1 = 0;
+    rr.x1 = (uint16_t)REC_WIRE_X1;
+  } else if (!edge_setup(sx, sy, a.width, a.height, rr)) {
     return false;
+  }
   rr.order = order;
   sr.draw = (uint32_t)(&d - a.draws);
-  if (d.flags & DF_SMOOTH) {
+  if ((d.flags & DF_SMOOTH) && !wire) {
     rr.zc[0] = sz[0];
     rr.zc[1] = sz[1];
     rr.zc[2] = sz[2];
@@ -642,11 +652,13 @@ __device__ bool fan_setup(const FrameArgs &a, const DrawRec &d, const CV v[3], c
     return true;
   }
   /* flat: constant colour and incremental depth (rasterizer.c:2549-2609,
-   * 1164-1232, 971-974) */
-  rr.y1 |= REC_FLAT_BIT;
-  rr.zc[0] = (rr.w0[0] * sz[0] + rr.w0[1] * sz[1] + rr.w0[2] * sz[2]) * rr.inv_area;
-  rr.zc[1] = (rr.dx[0] * sz[0] + rr.dx[1] * sz[1] + rr.dx[2] * sz[2]) * rr.inv_area;
-  rr.zc[2] = (rr.dy[0] * sz[0] + rr.dy[1] * sz[1] + rr.dy[2] * sz[2]) * rr.inv_area;
+   * 1164-1232, 971-974); a wireframe triangle takes the same colour */
+  if (!wire) {
+    rr.y1 |= REC_FLAT_BIT;
+    rr.zc[0] = (rr.w0[0] * sz[0] + rr.w0[1] * sz[1] + rr.w0[2] * sz[2]) * rr.inv_area;
+    rr.zc[1] = (rr.dx[0] * sz[0] + rr.dx[1] * sz[1] + rr.dx[2] * sz[2]) * rr.inv_area;
+    rr.zc[2] = (rr.dy[0] * sz[0] + rr.dy[1] * sz[1] + rr.dy[2] * sz[2]) * rr.inv_area;
+  }
   V3 fn = norm3(mk3(v[0].n.x + v[1].n.x + v[2].n.x, v[0].n.y + v[1].n.y + v[2].n.y,
                     v[0].n.z + v[1].n.z + v[2].n.z));
   float avg[3];
@@ -686,16 +698,19 @@ __device__ __forceinline__ bool inside_all(float4 p) {
 }
 
 /* Warp-aggregated allocation of one slot from *counter: the converged lanes
- * share a single atomicAdd and take consecutive slots in lane order. */
+ * with the same counter (a batch warp can hold items of several viewports,
+ * each with its own counters) share a single atomicAdd and take
+ * consecutive slots in lane order. */
 __device__ __forceinline__ uint32_t warp_alloc1(uint32_t *counter) {
   const uint32_t mask = __activemask();
+  const uint32_t peers = __match_any_sync(mask, (unsigned long long)(uintptr_t)counter);
   const uint32_t lane = threadIdx.x & 31u;
-  const int leader = __ffs(mask) - 1;
+  const int leader = __ffs(peers) - 1;
   uint32_t base = 0;
   if ((int)lane == leader)
-    base = atomicAdd(counter, (uint32_t)__popc(mask));
-  base = __shfl_sync(mask, base, leader);
-  return base + (uint32_t)__popc(mask & ((1u << lane) - 1u));
+    base = atomicAdd(counter, (uint32_t)__popc(peers));
+  base = __shfl_sync(peers, base, leader);
+  return base + (uint32_t)__popc(peers & ((1u << lane) - 1u));
 }
 
 __device__ __forceinline__ bool rec_live(const RasterRec &r, int W, int H) {
@@ -774,7 +789,8 @@ __device__ __forceinline__ void setup_item(const FrameArgs &a, uint32_t t) {
         if (A.w > 0.0f && B.w > 0.0f && C.w > 0.0f && inside_all(A) && inside_all(B) &&
             inside_all(C)) {
           CV v[3];
-          if (d.flags & DF_SMOOTH) { /* smooth records reference the vertex streams */
+          if ((d.flags & (DF_SMOOTH | DF_WIRE)) == DF_SMOOTH) {
+            /* smooth records reference the vertex streams */
             v[0].p = A;
             v[1].p = B;
             v[2].p = C;
@@ -792,7 +808,7 @@ __device__ __forceinline__ void setup_item(const FrameArgs &a, uint32_t t) {
   if (status == 1) {
     a.rrec[t] = rr;
     a.srec[t] = sr;
-    if (rec_large(a, rr))
+    if (rec_live(rr, a.width, a.height) && rec_large(a, rr))
       push_large(a, t, rr);
   } else if (status == 2) {
     write_rec_tail(&a.rrec[t], 0u, REC_REDIRECT); /* k_clip fills in the target */
@@ -1791,7 +1807,10 @@ static inline unsigned blocks_for(uint32_t n, unsigned bs) { return (n + bs - 1u
 __global__ void k_ocount(FrameArgs a);
 __global__ void k_oscan(FrameArgs a);
 __global__ void k_oraster(FrameArgs a);
-template <bool SH> __global__ void k_ofold(FrameArgs a);
+template <bool SH, bool WIRE> __global__ void k_ofold(FrameArgs a);
+__global__ void k_wcount(FrameArgs a);
+__global__ void k_wscan(FrameArgs a);
+__global__ void k_wplot(FrameArgs a);
 
 /* The legacy smooth path's shading (mop_sw_rasterize_triangle_smooth,
  * rasterizer.c:1371-1420): interpolated normal and vertex colour, one
@@ -1880,11 +1899,22 @@ int mopcuda_launch_frame(const FrameArgs &a, const PostArgs &p, const LaunchCfg 
     k_ocount<<<blocks_for(nrec, 256), 256, 0, s>>>(a);
     k_oscan<<<1, 1024, 0, s>>>(a);
     k_oraster<<<cfg.num_sms * 8, 256, 0, s>>>(a);
-    if (a.shadow_keys)
-      k_ofold<true><<<cfg.num_sms * 8, 128, 0, s>>>(a);
-    else
-      k_ofold<false><<<cfg.num_sms * 8, 128, 0, s>>>(a);
-    launches += 4;
+    launches += 3;
+    if (a.wire) { /* wireframe draws: their line plots join the fragment lists */
+      k_wcount<<<blocks_for(nrec, 256), 256, 0, s>>>(a);
+      k_wscan<<<1, 1024, 0, s>>>(a);
+      k_wplot<<<cfg.num_sms * 8, 256, 0, s>>>(a);
+      launches += 3;
+      if (a.shadow_keys)
+        k_ofold<true, true><<<cfg.num_sms * 8, 128, 0, s>>>(a);
+      else
+        k_ofold<false, true><<<cfg.num_sms * 8, 128, 0, s>>>(a);
+    } else if (a.shadow_keys) {
+      k_ofold<true, false><<<cfg.num_sms * 8, 128, 0, s>>>(a);
+    } else {
+      k_ofold<false, false><<<cfg.num_sms * 8, 128, 0, s>>>(a);
+    }
+    launches += 1;
   }
   if (ev)
     cudaEventRecord(ev[5], s);
@@ -2015,8 +2045,12 @@ __global__ void __launch_bounds__(1024) k_oscan(FrameArgs a) {
   items_scan_block(a.olist_items, n, &a.ctr->olist_items, part);
 }
 
+/* Links a fragment into sample px's list.  Node and touched-list slots come
+ * from warp-aggregated allocations (one atomic per group of converged lanes,
+ * not one per fragment on two shared counters); the fold sorts each list,
+ * so the order of the slots does not matter. */
 __device__ __forceinline__ void push_fragment(const FrameArgs &a, uint32_t px, uint32_t order) {
-  const uint32_t node = atomicAdd(&a.ctr->frag_count, 1u);
+  const uint32_t node = warp_alloc1(&a.ctr->frag_count);
   if (node >= a.frag_cap) {
     atomicOr(&a.ctr->overflow, 16u);
     return;
@@ -2024,7 +2058,7 @@ __device__ __forceinline__ void push_fragment(const FrameArgs &a, uint32_t px, u
   const uint32_t prev = atomicExch(&a.frag_head[px], node);
   a.frags[node] = make_uint2(prev, order);
   if (prev == 0xffffffffu) /* first fragment of this sample */
-    a.touched[atomicAdd(&a.ctr->touched_count, 1u)] = px;
+    a.touched[warp_alloc1(&a.ctr->touched_count)] = px;
 }
 
 /* One (row, 32-sample chunk) item of a suffix record (nl: records queued):
@@ -2089,6 +2123,218 @@ __global__ void __launch_bounds__(256) k_oraster(FrameArgs a) {
     oraster_item(a, it, nl);
 }
 
+/* ------------------------------------------------------------------------
+ * Wireframe: mop_sw_draw_line_aa with thickness 1 (Xiaolin Wu,
+ * rasterizer.c:743-871) over the triangle's edges v0-v1, v1-v2, v2-v0.  A
+ * line's plots are numbered as the reference issues them: the first end
+ * pixel's two plots, the second end's two, then two per column between.
+ * Each plot is an item; its inputs are recomputed from the record wherever
+ * it is needed, the running row `intery` of column j by fold_add (the exact
+ * result of the reference's j sequential additions of the gradient).
+ * ------------------------------------------------------------------------ */
+struct WuLine {
+  float x0, y0, z0, x1, y1, z1; /* after the steep and left-to-right swaps */
+  float gradient, ye1, gap1, ye2, gap2, intery, steps;
+  int xp1, xp2;
+  bool steep;
+};
+
+__device__ __forceinline__ float wu_fpart(float x) { return x - floorf(x); }
+__device__ __forceinline__ float wu_rfpart(float x) { return 1.0f - wu_fpart(x); }
+
+__device__ __forceinline__ void wu_setup(float x0, float y0, float z0, float x1, float y1, float z1,
+                                         WuLine &L) {
+  L.steep = fabsf(y1 - y0) > fabsf(x1 - x0);
+  if (L.steep) {
+    float t = x0;
+    x0 = y0;
+    y0 = t;
+    t = x1;
+    x1 = y1;
+    y1 = t;
+  }
+  if (x0 > x1) {
+    float t = x0;
+    x0 = x1;
+    x1 = t;
+    t = y0;
+    y0 = y1;
+    y1 = t;
+    t = z0;
+    z0 = z1;
+    z1 = t;
+  }
+  L.x0 = x0;
+  L.y0 = y0;
+  L.z0 = z0;
+  L.x1 = x1;
+  L.y1 = y1;
+  L.z1 = z1;
+  const float dx = x1 - x0, dy = y1 - y0;
+  L.gradient = dx < 0.001f ? 1.0f : dy / dx;
+  float xe = roundf(x0);
+  L.ye1 = y0 + L.gradient * (xe - x0);
+  L.gap1 = wu_rfpart(x0 + 0.5f);
+  L.xp1 = x86_f2i(xe);
+  L.intery = L.ye1 + L.gradient;
+  xe = roundf(x1);
+  L.ye2 = y1 + L.gradient * (xe - x1);
+  L.gap2 = wu_fpart(x1 + 0.5f);
+  L.xp2 = x86_f2i(xe);
+  L.steps = (float)(L.xp2 - L.xp1);
+  if (L.steps < 1.0f)
+    L.steps = 1.0f;
+}
+
+__device__ __forceinline__ uint32_t wu_plots(const WuLine &L) {
+  const long long between = (long long)L.xp2 - (long long)L.xp1 - 1ll;
+  return 4u + (between > 0 ? 2u * (uint32_t)(between < 0x3fffffffll ? between : 0x3fffffffll) : 0u);
+}
+
+/* Plot k of line L: pixel, depth and coverage. */
+__device__ __forceinline__ void wu_plot(const WuLine &L, uint32_t k, int &px, int &py, float &z,
+                                        float &cov) {
+  int col, row;
+  if (k < 4u) {
+    const bool first = k < 2u;
+    const float ye = first ? L.ye1 : L.ye2, gap = first ? L.gap1 : L.gap2;
+    col = first ? L.xp1 : L.xp2;
+    z = first ? L.z0 : L.z1;
+    const int yp = x86_f2i(floorf(ye));
+    row = yp + (int)(k & 1u);
+    cov = (k & 1u) ? wu_fpart(ye) * gap : wu_rfpart(ye) * gap;
+  } else {
+    const int j = (int)((k - 4u) >> 1);
+    col = L.xp1 + 1 + j;
+    const float t = (float)(col - L.xp1) / L.steps;
+    z = L.z0 + t * (L.z1 - L.z0);
+    const float intery = fold_add(L.intery, L.gradient, j);
+    row = x86_f2i(floorf(intery)) + (int)(k & 1u);
+    cov = (k & 1u) ? wu_fpart(intery) : wu_rfpart(intery);
+  }
+  px = L.steep ? row : col;
+  py = L.steep ? col : row;
+}
+
+__device__ __forceinline__ void wu_edge(const RasterRec &r, int e, WuLine &L) {
+  const int f = e == 2 ? 0 : e + 1;
+  wu_setup(r.w0[e], r.dx[e], r.dy[e], r.w0[f], r.dx[f], r.dy[f], L);
+}
+
+/* The wireframe plot behind item `it` (the frame's wire-item numbering):
+ * its record, edge and plot. */
+__device__ __forceinline__ bool wire_item(const FrameArgs &a, uint32_t it, uint32_t &rid,
+                                          WuLine &L, uint32_t &k) {
+  uint32_t nl = a.ctr->wire_count;
+  if (nl > a.wlist_cap)
+    nl = a.wlist_cap;
+  if (nl == 0u)
+    return false;
+  uint32_t lo = 0, hi = nl;
+  while (hi - lo > 1) {
+    const uint32_t mid = (lo + hi) >> 1;
+    if (a.wlist_items[mid] <= it)
+      lo = mid;
+    else
+      hi = mid;
+  }
+  rid = a.wlist[lo];
+  if (rid >= a.rec_cap)
+    return false;
+  const RasterRec r = a.rrec[rid];
+  k = it - a.wlist_items[lo];
+  for (int e = 0; e < 3; e++) {
+    wu_edge(r, e, L);
+    const uint32_t n = wu_plots(L);
+    if (k < n)
+      return true;
+    k -= n;
+  }
+  return false;
+}
+
+/* Sort key of a fragment payload: (order, position among the record's
+ * plots) for a line plot, (order, 0) for a filled record. */
+__device__ __forceinline__ unsigned long long frag_key(const FrameArgs &a, uint32_t v) {
+  if (!(v & FRAG_WIRE_BIT))
+    return (unsigned long long)v << 32;
+  const uint32_t it = v & ~FRAG_WIRE_BIT;
+  uint32_t nl = a.ctr->wire_count;
+  if (nl > a.wlist_cap)
+    nl = a.wlist_cap;
+  if (nl == 0u)
+    return ~0ull;
+  uint32_t lo = 0, hi = nl;
+  while (hi - lo > 1) {
+    const uint32_t mid = (lo + hi) >> 1;
+    if (a.wlist_items[mid] <= it)
+      lo = mid;
+    else
+      hi = mid;
+  }
+  const uint32_t rid = a.wlist[lo];
+  if (rid >= a.rec_cap)
+    return ~0ull;
+  return ((unsigned long long)a.rrec[rid].order << 32) | (unsigned long long)(it - a.wlist_items[lo]);
+}
+
+/* Queues the live wireframe records of the suffix with their plot counts. */
+__device__ __forceinline__ void wcount_item(const FrameArgs &a, uint32_t rid) {
+  const RasterRec r = a.rrec[rid];
+  if (r.x1 != (uint16_t)REC_WIRE_X1 || r.y0 == REC_REDIRECT)
+    return;
+  uint32_t n = 0;
+  for (int e = 0; e < 3; e++) {
+    WuLine L;
+    wu_edge(r, e, L);
+    n += wu_plots(L);
+  }
+  const uint32_t q = atomicAdd(&a.ctr->wire_count, 1u);
+  if (q < a.wlist_cap) {
+    a.wlist[q] = rid;
+    a.wlist_items[q] = n;
+  } else {
+    atomicOr(&a.ctr->overflow, 128u);
+  }
+}
+
+__global__ void __launch_bounds__(256) k_wcount(FrameArgs a) {
+  const uint32_t n = ordered_record_items(a);
+  for (uint32_t rid = blockIdx.x * blockDim.x + threadIdx.x; rid < n;
+       rid += gridDim.x * blockDim.x)
+    wcount_item(a, rid);
+}
+
+__global__ void __launch_bounds__(1024) k_wscan(FrameArgs a) {
+  __shared__ uint32_t part[32];
+  uint32_t n = a.ctr->wire_count;
+  if (n > a.wlist_cap)
+    n = a.wlist_cap;
+  items_scan_block(a.wlist_items, n, &a.ctr->wire_items, part);
+}
+
+/* One line plot: in the framebuffer, coverage at least 0.004 and in front
+ * of the opaque depth (or any depth when the suffix keeps every fragment)
+ * gives a fragment. */
+__global__ void __launch_bounds__(256) k_wplot(FrameArgs a) {
+  const uint32_t total = a.ctr->wire_items;
+  for (uint32_t it = blockIdx.x * blockDim.x + threadIdx.x; it < total && it < FRAG_WIRE_BIT;
+       it += gridDim.x * blockDim.x) {
+    uint32_t rid, k;
+    WuLine L;
+    if (!wire_item(a, it, rid, L, k))
+      continue;
+    int x, y;
+    float z, cov;
+    wu_plot(L, k, x, y, z, cov);
+    if (x < 0 || x >= a.width || y < 0 || y >= a.height || cov < 0.004f)
+      continue;
+    const uint32_t px = (uint32_t)y * (uint32_t)a.width + (uint32_t)x;
+    if (a.ordered_keep_all || z < a.depth[px])
+      push_fragment(a, px, FRAG_WIRE_BIT | it);
+  }
+}
+
 /* The record behind an order (triangle << 5 | fan), as shade_item finds it. */
 __device__ __forceinline__ uint32_t record_of(const FrameArgs &a, uint32_t order) {
   const uint32_t t = order >> ORDER_FAN_BITS, fan = order & ((1u << ORDER_FAN_BITS) - 1u);
@@ -2112,6 +2358,49 @@ struct OFold {
   bool cur_nw;
 };
 
+/* A fragment of draw di follows: when the draw changes, a finished
+ * depth-write-off draw's depth is undone (cpu_backend.c:575-580) and a new
+ * one's saved (:536-544). */
+__device__ __forceinline__ void ofold_enter_draw(OFold &st, uint32_t di, const DrawRec &d) {
+  if (di != st.cur) {
+    if (st.cur_nw)
+      st.depth = st.saved;
+    st.cur = di;
+    st.cur_nw = (d.flags & DF_NO_DEPTH_WRITE) != 0;
+    if (st.cur_nw)
+      st.saved = st.depth;
+  }
+}
+
+/* Applies line plot `it` at its sample: aa_plot (rasterizer.c:687-729) on
+ * the sample's HDR colour, depth and ID. */
+__device__ __forceinline__ void ofold_wire(const FrameArgs &a, OFold &st, uint32_t it) {
+  uint32_t rid, k;
+  WuLine L;
+  if (!wire_item(a, it, rid, L, k))
+    return;
+  const ShadeRec s = a.srec[rid];
+  const uint32_t di = s.draw < a.draw_count ? s.draw : 0;
+  const DrawRec &d = a.draws[di];
+  ofold_enter_draw(st, di, d);
+  int px, py;
+  float z, cov;
+  wu_plot(L, k, px, py, z, cov);
+  if (!(d.flags & DF_NO_DEPTH_TEST) && z >= st.depth)
+    return;
+  const float inv = 1.0f - cov;
+  for (int c = 0; c < 3; c++) {
+    /* the line colour as the reference's byte (rasterizer.c:1226-1228) */
+    const float v = s.col[c] > 1.0f ? 1.0f : s.col[c];
+    const float src = (float)(uint8_t)x86_f2i(v * 255.0f) / 255.0f;
+    st.hdr[c] = src * cov + st.hdr[c] * inv;
+  }
+  if (cov > 0.5f) {
+    st.depth = z;
+    st.id = d.object_id;
+  }
+}
+
 /* Applies the fragment of submission order `order` at sample (x, y). */
 template <bool SH>
 __device__ __forceinline__ void ofold_fragment(const FrameArgs &a, OFold &st, int x, int y,
@@ -2123,14 +2412,7 @@ __device__ __forceinline__ void ofold_fragment(const FrameArgs &a, OFold &st, in
   const ShadeRec s = a.srec[rid];
   const uint32_t di = s.draw < a.draw_count ? s.draw : 0;
   const DrawRec &d = a.draws[di];
-  if (di != st.cur) {
-    if (st.cur_nw)
-      st.depth = st.saved; /* cpu_backend.c:575-580 */
-    st.cur = di;
-    st.cur_nw = (d.flags & DF_NO_DEPTH_WRITE) != 0;
-    if (st.cur_nw)
-      st.saved = st.depth; /* cpu_backend.c:536-544 */
-  }
+  ofold_enter_draw(st, di, d);
   const bool dtest = !(d.flags & DF_NO_DEPTH_TEST);
   const int jr = y - (int)r.y0, kc = x - (int)r.x0;
   if (r.y1 & REC_FLAT_BIT) { /* rasterize_filled_triangle, rasterizer.c:1000-1083 */
@@ -2221,11 +2503,28 @@ __device__ __forceinline__ void ofold_fragment(const FrameArgs &a, OFold &st, in
 }
 
 /* Each touched sample folds its fragments in submission order.  Up to
- * ORDERED_MAX_FRAGS orders are gathered and insertion-sorted in registers;
- * a longer list is applied by selection, each step walking the list for the
- * smallest order above the last one applied (orders are distinct: one per
- * record, and a record covers a sample once). */
-template <bool SH> __device__ __forceinline__ void ofold_item(const FrameArgs &a, uint32_t i) {
+ * ORDERED_MAX_FRAGS are gathered and insertion-sorted in registers; a
+ * longer list is applied by selection, each step walking the list for the
+ * smallest key above the last one applied (keys are distinct: a record
+ * covers a sample once, a line plot is one item).  WIRE: the frame has line
+ * plots, whose payloads sort by frag_key (a triangle's plots in the
+ * reference's drawing order after the triangles before it). */
+template <bool WIRE>
+__device__ __forceinline__ unsigned long long ofold_key(const FrameArgs &a, uint32_t v) {
+  return WIRE ? frag_key(a, v) : (unsigned long long)v;
+}
+
+template <bool SH, bool WIRE>
+__device__ __forceinline__ void ofold_apply(const FrameArgs &a, OFold &st, int x, int y,
+                                            uint32_t v) {
+  if (WIRE && (v & FRAG_WIRE_BIT))
+    ofold_wire(a, st, v & ~FRAG_WIRE_BIT);
+  else
+    ofold_fragment<SH>(a, st, x, y, v);
+}
+
+template <bool SH, bool WIRE>
+__device__ __forceinline__ void ofold_item(const FrameArgs &a, uint32_t i) {
   const uint32_t px = a.touched[i];
   const uint32_t head = a.frag_head[px];
   uint32_t ord[ORDERED_MAX_FRAGS];
@@ -2258,25 +2557,29 @@ template <bool SH> __device__ __forceinline__ void ofold_item(const FrameArgs &a
   if (total <= ORDERED_MAX_FRAGS) {
     for (uint32_t k = 1; k < cnt; k++) { /* submission order */
       const uint32_t v = ord[k];
+      const unsigned long long kv = ofold_key<WIRE>(a, v);
       uint32_t j = k;
-      while (j > 0 && ord[j - 1] > v) {
+      while (j > 0 && ofold_key<WIRE>(a, ord[j - 1]) > kv) {
         ord[j] = ord[j - 1];
         j--;
       }
       ord[j] = v;
     }
     for (uint32_t k = 0; k < cnt; k++)
-      ofold_fragment<SH>(a, st, x, y, ord[k]);
+      ofold_apply<SH, WIRE>(a, st, x, y, ord[k]);
   } else {
-    uint32_t last = 0;
+    unsigned long long last = 0;
     for (uint32_t k = 0; k < total; k++) {
       bool found = false;
       uint32_t best = 0, steps = 0;
+      unsigned long long best_key = 0;
       for (uint32_t node = head; node != 0xffffffffu && node < a.frag_cap;
            node = a.frags[node].x) {
         const uint32_t o = a.frags[node].y;
-        if ((k == 0 || o > last) && (!found || o < best)) {
+        const unsigned long long ko = ofold_key<WIRE>(a, o);
+        if ((k == 0 || ko > last) && (!found || ko < best_key)) {
           best = o;
+          best_key = ko;
           found = true;
         }
         if (++steps >= total)
@@ -2284,8 +2587,8 @@ template <bool SH> __device__ __forceinline__ void ofold_item(const FrameArgs &a
       }
       if (!found)
         break;
-      ofold_fragment<SH>(a, st, x, y, best);
-      last = best;
+      ofold_apply<SH, WIRE>(a, st, x, y, best);
+      last = best_key;
     }
   }
   if (st.cur_nw)
@@ -2303,11 +2606,11 @@ template <bool SH> __device__ __forceinline__ void ofold_item(const FrameArgs &a
   a.ids[px] = st.id;
 }
 
-template <bool SH>
+template <bool SH, bool WIRE>
 __global__ void __launch_bounds__(128) k_ofold(FrameArgs a) {
   const uint32_t n = a.ctr->touched_count;
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-    ofold_item<SH>(a, i);
+    ofold_item<SH, WIRE>(a, i);
 }
 
 /* ========================================================================
@@ -2856,7 +3159,7 @@ __global__ void __launch_bounds__(128) k_b_ofold(const FrameArgs *__restrict__ f
        g += gridDim.x * blockDim.x) {
     while (s_pre[v + 1] <= g)
       v++;
-    ofold_item<SH>(fr[v], g - s_pre[v]);
+    ofold_item<SH, false>(fr[v], g - s_pre[v]);
   }
 }
 

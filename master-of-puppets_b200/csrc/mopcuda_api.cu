@@ -155,7 +155,7 @@ extern "C" void mopcuda_device_destroy(MopCudaDevice *d) {
                         &d->clipq,    &d->keys,       &d->large_list,  &d->large_items,
                         &d->shade_list, &d->counters, &d->pick_xy,     &d->pick_out,
                         &d->deform_params, &d->hdr, &d->frag_head, &d->frags, &d->touched,
-                        &d->olist, &d->olist_items, &d->sh_map[0], &d->sh_map[1], &d->sh_d_draws,
+                        &d->olist, &d->olist_items, &d->wlist, &d->wlist_items, &d->sh_map[0], &d->sh_map[1], &d->sh_d_draws,
                         &d->sh_recs, &d->sh_items, &d->sh_ctr, &d->env, &d->ibl_tab};
   for (DevArena *a : arenas)
     a->release();
@@ -713,26 +713,26 @@ static float clamp01f(float x) { return x < 0.0f ? 0.0f : (x > 1.0f ? 1.0f : x);
 
 /* Records one draw.  Opaque lit and opaque flat draws are order-independent;
  * blended draws (smooth or flat), unlit smooth draws (the legacy path with
- * silhouette edge AA) and draws with the depth test or the depth write off
- * (the core's instanced pass and editor chrome) depend on submission order
- * and start the frame's ordered suffix; zero-opacity draws are colour no-ops
- * in the reference and are dropped; wireframe draws are reported as
- * unsupported. */
+ * silhouette edge AA), wireframe draws (anti-aliased lines blended over what
+ * is there) and draws with the depth test or the depth write off (the core's
+ * instanced pass and editor chrome) depend on submission order and start the
+ * frame's ordered suffix; zero-opacity filled draws are colour no-ops in the
+ * reference and are dropped (lines ignore the opacity). */
 int mc_build_draw(const MopCudaDraw *c, const float *model, const float *mvp,
                   std::vector<LightRec> &lights, DrawRec &r, bool &skip) {
   skip = false;
   if (!c->vertex_buffer || !c->index_buffer)
     return fail(MOPCUDA_EINVAL, "draw: missing buffers");
   float op = clamp01f(c->opacity);
-  if (op == 0.0f && c->blend_mode != 3) {
+  if (op == 0.0f && c->blend_mode != 3 && !c->wireframe) {
     skip = true;
     return MOPCUDA_OK;
   }
   bool lit = c->lights && c->light_count > 0;
-  if (c->wireframe)
-    return fail(MOPCUDA_EUNSUPPORTED, "draw: wireframe (line) rendering is not implemented");
   uint32_t stride = 48;
   memset(&r, 0, sizeof r);
+  if (c->wireframe)
+    r.flags |= DF_WIRE;
   if (c->layout) {
     const MopCudaVertexLayout *L = c->layout;
     stride = L->stride;
@@ -868,7 +868,7 @@ static int record_draw(MopCudaDevice *d, const MopCudaDraw *c, const float *mode
    * starts the ordered suffix */
   const bool legacy = (r.flags & DF_SMOOTH) && !(r.flags & DF_LIT);
   if ((r.blend_mode != 0 || clamp01f(r.opacity) < 1.0f || legacy ||
-       (r.flags & (DF_NO_DEPTH_WRITE | DF_NO_DEPTH_TEST))) &&
+       (r.flags & (DF_NO_DEPTH_WRITE | DF_NO_DEPTH_TEST | DF_WIRE))) &&
       d->rec_ordered_from == UINT32_MAX)
     d->rec_ordered_from = (uint32_t)d->rec_draws.size();
   d->rec_draws.push_back(r);
@@ -1104,6 +1104,17 @@ static int launch_frame(MopCudaDevice *d) {
     rc |= d->frags.ensure(8ull * fcap);
     rc |= d->olist.ensure(4ull * ocap);
     rc |= d->olist_items.ensure(4ull * ocap);
+    bool wire = false;
+    for (uint32_t i = d->ordered_from; i < nd && !wire; i++)
+      wire = (d->draws[i].flags & DF_WIRE) != 0;
+    if (wire) {
+      /* line plots mark fragment payloads with bit 31 (FRAG_WIRE_BIT) */
+      if (T >= (1ull << (31 - ORDER_FAN_BITS)))
+        return fail(MOPCUDA_EUNSUPPORTED, "frame: wireframe draws in a frame of %llu triangles",
+                    (unsigned long long)T);
+      rc |= d->wlist.ensure(4ull * ocap);
+      rc |= d->wlist_items.ensure(4ull * ocap);
+    }
   }
   if (rc)
     return MOPCUDA_ENOMEM;
@@ -1186,9 +1197,17 @@ static int launch_frame(MopCudaDevice *d) {
     a.olist = d->olist.as<uint32_t>();
     a.olist_items = d->olist_items.as<uint32_t>();
     a.olist_cap = ocap;
-    for (uint32_t i = d->ordered_from; i < nd; i++)
+    for (uint32_t i = d->ordered_from; i < nd; i++) {
       if (d->draws[i].flags & DF_NO_DEPTH_TEST)
         a.ordered_keep_all = 1;
+      if (d->draws[i].flags & DF_WIRE)
+        a.wire = 1;
+    }
+    if (a.wire) {
+      a.wlist = d->wlist.as<uint32_t>();
+      a.wlist_items = d->wlist_items.as<uint32_t>();
+      a.wlist_cap = ocap;
+    }
   }
 
   if (d->fr_sh >= 0) { /* the map bound at this frame's frame_end */
@@ -1286,6 +1305,8 @@ static int finish_frame(MopCudaDevice *d, int timeout_ms, bool defer_readback) {
       d->frag_hint = c->frag_count + c->frag_count / 4 + 65536;
     if (c->overflow & 32u)
       d->olist_hint = c->olist_count + c->olist_count / 4 + 1024;
+    if (c->overflow & 128u)
+      d->olist_hint = std::max(d->olist_hint, c->wire_count + c->wire_count / 4 + 1024);
     if (c->overflow & 1u)
       d->rec_hint *= 2;
     if (c->overflow & 2u)

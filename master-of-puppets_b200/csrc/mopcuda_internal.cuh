@@ -38,6 +38,9 @@ enum DrawFlags : uint32_t {
   /* scene draws of a batch: blended, translucent or unlit smooth — the draw
    * starts its viewport's ordered suffix (set by the host) */
   DF_ORDERED = 1u << 7,
+  /* wireframe: the triangle's three edges as anti-aliased lines in its flat
+   * colour (rasterizer.c:1225-1235, 743-871); part of the ordered suffix */
+  DF_WIRE = 1u << 8,
 };
 
 /* One recorded draw, uploaded per frame (the MopRhiDrawCall fields the path
@@ -106,6 +109,14 @@ struct __align__(16) RasterRec {
  * marker in y0 and, in `order`, the slot of its first fan record in the
  * overflow region that starts at slot total_tris. */
 #define REC_REDIRECT 0xffffu
+/* A wireframe triangle's record: x1 holds this marker (no filled raster
+ * kernel takes it: its box is empty), w0/dx/dy hold the screen x, y and z of
+ * its three vertices. */
+#define REC_WIRE_X1 0x8000u
+/* Fragment payloads of wireframe frames: bit 31 set marks a line plot, the
+ * rest its item index (the frame's triangle count stays below 2^26, so
+ * triangle orders keep bit 31 clear). */
+#define FRAG_WIRE_BIT 0x80000000u
 
 /* Per fan-triangle shading record, 16 bytes. */
 struct __align__(16) ShadeRec {
@@ -127,9 +138,10 @@ struct Counters {
                                  queue, bit3 large list                          */
   uint32_t shade_count;       /* covered samples queued for shading              */
   /* ordered (blended) suffix of the frame; overflow bit4 fragment pool,
-   * bit5 ordered-record list */
+   * bit5 ordered-record list, bit7 wireframe-record list */
   uint32_t frag_count, touched_count, olist_count, olist_items;
-  uint32_t pad;
+  uint32_t wire_count, wire_items; /* wireframe records queued, their plots */
+  uint32_t pad[2];
 };
 
 /* Blended fragments of one sample sorted in registers; a sample with more
@@ -214,6 +226,11 @@ struct FrameArgs {
    * depth, and later ones may pass where the opaque depth is nearer, so
    * every covered fragment of the suffix is kept */
   int ordered_keep_all;
+  /* wireframe records in the suffix: their queue and plot counts (then
+   * offsets); wire != 0 when the frame has wireframe draws */
+  uint32_t *wlist, *wlist_items;
+  uint32_t wlist_cap;
+  int wire;
   /* shadow map bound for directional lights (the rasteriser's shadow state,
    * rasterizer.c:141-157): shadow_w x shadow_h texel keys (shadow_texel),
    * null when none is bound; shadow_vp: the light's view-projection, 16

@@ -491,7 +491,8 @@ class _Resident:
         dr.roughness = m.roughness if m.has_material else 0.5
         dr.depth_bias = 0.0
         dr.smooth = 1 if getattr(sc, "smooth", True) else 0
-        dr.wireframe = 0
+        # MOP_RENDER_WIREFRAME: every mesh but ID 0 (EMIT_DRAW, viewport.c:2056-2057)
+        dr.wireframe = 1 if getattr(sc, "wireframe", False) and m.object_id != 0 else 0
         dr.depth_test = dr.depth_write = dr.backface_cull = 1
         dr.blend_mode = getattr(m, "blend_mode", 0) or (1 if m.opacity < 1.0 else 0)
         dr.texture = self.textures[m.texture] if m.texture >= 0 else None
@@ -525,7 +526,7 @@ class _Resident:
         dr.metallic, dr.roughness = 0.0, 0.5
         dr.depth_bias = 0.0
         dr.smooth = 1 if getattr(sc, "smooth", True) else 0
-        dr.wireframe = 0
+        dr.wireframe = 1 if getattr(sc, "wireframe", False) and im.object_id != 0 else 0
         dr.depth_test, dr.depth_write = 1, 0
         dr.backface_cull = 1 if im.object_id != 0 else 0
         dr.blend_mode = 0

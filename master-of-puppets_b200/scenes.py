@@ -147,6 +147,11 @@ class Scene:
     instanced: List[InstancedMesh] = dataclasses.field(default_factory=list)
     # mop_viewport_set_environment_background: the environment drawn behind the scene
     env_background: bool = False
+    # mop_viewport_set_render_mode(MOP_RENDER_WIREFRAME): meshes other than ID 0 as lines
+    wireframe: bool = False
+    # the reference core's own viewports only: keep its hidden grid mesh, which wireframe
+    # mode draws (as lines, depth test off) although its opacity is 0
+    wireframe_grid: bool = False
 
     @property
     def samples(self) -> int:
@@ -731,6 +736,24 @@ def deep_transparent_scene(seed: int = 64, width: int = 160, height: int = 120, 
                               blend_mode=modes[k % 4]))
         oid += 1
     return sc
+
+
+def wireframe_scene(seed: int = 110, width: int = 160, height: int = 120, ssaa: int = 1,
+                    lights: str = "mixed") -> Scene:
+    """small_scene in MOP_RENDER_WIREFRAME, plus an ID-0 quad (drawn filled:
+    the core keeps ID 0 solid) and a long thin triangle crossing the view
+    (steep and shallow edges, sub-pixel ends)."""
+    sc = small_scene(seed=seed, width=width, height=height, ssaa=ssaa, lights=lights)
+    v, i = _quad(-3.0, 0.2, -1.0, 1.4, 0.5, (0.9, 0.4, 0.2, 1.0))
+    sc.meshes.append(Mesh(v, i, 0, mat_identity()))
+    pos = np.array([[-4.0, 0.3, -1.0], [4.5, 2.6, 0.4], [-3.7, 0.45, -0.9]], np.float32)
+    nrm = np.tile(np.array([0.0, 1.0, 0.0], np.float32), (3, 1))
+    col = np.tile(np.array([0.3, 0.8, 1.0, 1.0], np.float32), (3, 1))
+    uv = np.zeros((3, 2), np.float32)
+    oid = max(m.object_id for m in sc.meshes) + 1
+    sc.meshes.append(Mesh(_pack(pos, nrm, col, uv), np.array([0, 1, 2, 0, 2, 1], np.uint32), oid,
+                          mat_identity()))
+    return dataclasses.replace(sc, wireframe=True)
 
 
 def instanced_scene(seed: int = 70, width: int = 192, height: int = 144, ssaa: int = 1,

@@ -39,7 +39,7 @@ class OrDraw(C.Structure):
                 ("backface_cull", C.c_int32), ("blend_mode", C.c_int32),
                 ("lights", C.POINTER(OrLight)), ("light_count", C.c_uint32),
                 ("texture", C.c_void_p), ("tex_w", C.c_int32), ("tex_h", C.c_int32),
-                ("depth_write", C.c_int32)]
+                ("depth_write", C.c_int32), ("wireframe", C.c_int32)]
 
 
 class OrIBL(C.Structure):
@@ -246,6 +246,8 @@ def render(scene, ibl=None, want_hdr=False):
         d.lights = lights
         d.light_count = len(scene.lights)
         d.depth_write = 1
+        # MOP_RENDER_WIREFRAME: every mesh but ID 0 as lines (viewport.c:2056-2057)
+        d.wireframe = 1 if getattr(scene, "wireframe", False) and m.object_id != 0 else 0
         if scenes.is_chrome(m.object_id):  # EMIT_DRAW, viewport.c:2035-2076
             d.depth_test, d.backface_cull = 0, 0
             d.lights, d.light_count = None, 0
@@ -281,6 +283,7 @@ def render(scene, ibl=None, want_hdr=False):
             d.blend_mode = 0
             d.lights = lights
             d.light_count = len(scene.lights)
+            d.wireframe = 1 if getattr(scene, "wireframe", False) and im.object_id != 0 else 0
     sw, sh = scene.width * scene.ssaa, scene.height * scene.ssaa
     out = {
         "color": np.zeros((scene.height, scene.width, 4), np.uint8),

@@ -1170,6 +1170,101 @@ static bool inside_all(V4 p) {
   return p.x >= -p.w && p.x <= p.w && p.y >= -p.w && p.y <= p.w && p.z >= -p.w && p.z <= p.w;
 }
 
+/* Xiaolin Wu anti-aliased lines (mop_sw_draw_line_aa with thickness 1,
+ * rasterizer.c:743-871) and their plot (aa_plot, :687-729): the colour
+ * blended over the HDR value by the coverage, depth and ID written above
+ * coverage 0.5.  The HDR buffer is what the frame's resolve reads, so the
+ * plot's byte write is left out. */
+static float wu_fpart(float x) { return x - floorf(x); }
+static float wu_rfpart(float x) { return 1.0f - wu_fpart(x); }
+
+static void wu_plot(FB *fb, int x, int y, float z, const uint8_t rgb[3], float cov,
+                    uint32_t id, bool dt) {
+  if (x < 0 || x >= fb->w || y < 0 || y >= fb->h || cov < 0.004f)
+    return;
+  size_t i = (size_t)y * (size_t)fb->w + (size_t)x;
+  if (dt && z >= fb->depth[i])
+    return;
+  float inv = 1.0f - cov;
+  for (int c = 0; c < 3; c++) {
+    float src = (float)rgb[c] / 255.0f;
+    fb->hdr[i * 4 + c] = src * cov + fb->hdr[i * 4 + c] * inv;
+  }
+  fb->hdr[i * 4 + 3] = 1.0f;
+  if (cov > 0.5f) {
+    fb->depth[i] = z;
+    fb->id[i] = id;
+  }
+}
+
+static void wu_line(FB *fb, float x0, float y0, float z0, float x1, float y1, float z1,
+                    const uint8_t rgb[3], uint32_t id, bool dt) {
+  bool steep = fabsf(y1 - y0) > fabsf(x1 - x0);
+  if (steep) { /* walk along y: swap the axes */
+    float t = x0;
+    x0 = y0;
+    y0 = t;
+    t = x1;
+    x1 = y1;
+    y1 = t;
+  }
+  if (x0 > x1) { /* left to right */
+    float t = x0;
+    x0 = x1;
+    x1 = t;
+    t = y0;
+    y0 = y1;
+    y1 = t;
+    t = z0;
+    z0 = z1;
+    z1 = t;
+  }
+  float gradient = (x1 - x0 < 0.001f) ? 1.0f : (y1 - y0) / (x1 - x0);
+  /* the two end pixels */
+  float xe = roundf(x0), ye = y0 + gradient * (xe - x0), gap = wu_rfpart(x0 + 0.5f);
+  int xp1 = (int)xe, yp = (int)floorf(ye);
+  float c_hi = wu_rfpart(ye) * gap, c_lo = wu_fpart(ye) * gap;
+  if (steep) {
+    wu_plot(fb, yp, xp1, z0, rgb, c_hi, id, dt);
+    wu_plot(fb, yp + 1, xp1, z0, rgb, c_lo, id, dt);
+  } else {
+    wu_plot(fb, xp1, yp, z0, rgb, c_hi, id, dt);
+    wu_plot(fb, xp1, yp + 1, z0, rgb, c_lo, id, dt);
+  }
+  float intery = ye + gradient;
+  xe = roundf(x1);
+  ye = y1 + gradient * (xe - x1);
+  gap = wu_fpart(x1 + 0.5f);
+  int xp2 = (int)xe;
+  yp = (int)floorf(ye);
+  c_hi = wu_rfpart(ye) * gap;
+  c_lo = wu_fpart(ye) * gap;
+  if (steep) {
+    wu_plot(fb, yp, xp2, z1, rgb, c_hi, id, dt);
+    wu_plot(fb, yp + 1, xp2, z1, rgb, c_lo, id, dt);
+  } else {
+    wu_plot(fb, xp2, yp, z1, rgb, c_hi, id, dt);
+    wu_plot(fb, xp2, yp + 1, z1, rgb, c_lo, id, dt);
+  }
+  /* the pixels between, depth interpolated by the step's fraction */
+  float steps = (float)(xp2 - xp1);
+  if (steps < 1.0f)
+    steps = 1.0f;
+  for (int x = xp1 + 1; x < xp2; x++) {
+    float t = (float)(x - xp1) / steps;
+    float z = z0 + t * (z1 - z0);
+    int iy = (int)floorf(intery);
+    if (steep) {
+      wu_plot(fb, iy, x, z, rgb, wu_rfpart(intery), id, dt);
+      wu_plot(fb, iy + 1, x, z, rgb, wu_fpart(intery), id, dt);
+    } else {
+      wu_plot(fb, x, iy, z, rgb, wu_rfpart(intery), id, dt);
+      wu_plot(fb, x, iy + 1, z, rgb, wu_fpart(intery), id, dt);
+    }
+    intery += gradient;
+  }
+}
+
 static void triangle(const CV tri[3], const OrDraw *d, const OrIBL *ibl, FB *fb) {
   V4 a = tri[0].p, b = tri[1].p, c = tri[2].p;
   bool lit = d->lights && d->light_count > 0;
@@ -1218,7 +1313,7 @@ static void triangle(const CV tri[3], const OrDraw *d, const OrIBL *ibl, FB *fb)
                   (sv[2].sx - sv[0].sx) * (sv[1].sy - sv[0].sy);
     if (d->backface_cull && sarea >= 0.0f)
       continue;
-    if (d->smooth) {
+    if (d->smooth && !d->wireframe) {
       if (lit)
         raster_smooth_ml(sv, d, ibl, fb);
       else
@@ -1256,6 +1351,17 @@ static void triangle(const CV tri[3], const OrDraw *d, const OrIBL *ibl, FB *fb)
         col[k] = 0.0f;
     float sx[3] = {sv[0].sx, sv[1].sx, sv[2].sx}, sy[3] = {sv[0].sy, sv[1].sy, sv[2].sy},
           sz[3] = {sv[0].sz, sv[1].sz, sv[2].sz};
+    if (d->wireframe) { /* rasterizer.c:1225-1235, 2595-2605 */
+      uint8_t rgb[3];
+      for (int k = 0; k < 3; k++)
+        rgb[k] = (uint8_t)((col[k] > 1.0f ? 1.0f : col[k]) * 255.0f);
+      for (int e = 0; e < 3; e++) {
+        int f = (e + 1) % 3;
+        wu_line(fb, sx[e], sy[e], sz[e], sx[f], sy[f], sz[f], rgb, d->object_id,
+                d->depth_test != 0);
+      }
+      continue;
+    }
     raster_flat(sx, sy, sz, col[0], col[1], col[2], caf, d->object_id, d->depth_test != 0,
                 d->blend_mode, fb);
   }

@@ -66,6 +66,9 @@ typedef struct OrDraw {
   /* 0 with depth_test: the depth buffer is saved before the draw and restored
    * after it (cpu_backend.c:536-544, 621-627) */
   int32_t depth_write;
+  /* MOP_RENDER_WIREFRAME on a non-zero ID: the triangle's three edges as
+   * anti-aliased lines in its flat colour (rasterizer.c:1225-1235) */
+  int32_t wireframe;
 } OrDraw;
 
 typedef struct OrIBL {

@@ -212,6 +212,13 @@ void *refh_create(const RefScene *sc) {
   }
   if (sc->flat)
     mop_viewport_set_shading(vp, MOP_SHADING_FLAT);
+  if (sc->wireframe) {
+    mop_viewport_set_render_mode(vp, MOP_RENDER_WIREFRAME);
+    if (sc->wireframe == 1 && vp->grid) {
+      mop_viewport_remove_mesh(vp, vp->grid);
+      vp->grid = NULL;
+    }
+  }
   mop_viewport_set_camera(
       vp, (MopVec3){sc->eye[0], sc->eye[1], sc->eye[2]},
       (MopVec3){sc->target[0], sc->target[1], sc->target[2]},

@@ -101,6 +101,11 @@ typedef struct RefScene {
    * refh_read_target reads it back */
   int32_t render_target;
   int32_t env_background;   /* 1: mop_viewport_set_environment_background */
+  int32_t wireframe;        /* 1: mop_viewport_set_render_mode(WIREFRAME)
+                               without the core's hidden grid mesh (with the
+                               chrome off it is a zero-opacity blended mesh,
+                               which wireframe mode draws as lines); 2: with
+                               it */
 } RefScene;
 
 typedef struct RefFrame {

@@ -60,7 +60,7 @@ class RefScene(C.Structure):
                 ("fog_far", C.c_float), ("instanced_count", C.c_uint32),
                 ("instanced", C.POINTER(RefInstanced)), ("tex_format", C.POINTER(C.c_int32)),
                 ("tex_bytes", C.POINTER(C.c_uint32)), ("render_target", C.c_int32),
-                ("env_background", C.c_int32)]
+                ("env_background", C.c_int32), ("wireframe", C.c_int32)]
 
 
 class RefFrame(C.Structure):
@@ -199,6 +199,8 @@ class Reference:
         sc.env_rotation, sc.env_intensity = scene.env_rotation, scene.env_intensity
         sc.serial = 1 if serial else 0
         sc.flat = 0 if getattr(scene, "smooth", True) else 1
+        sc.wireframe = (2 if getattr(scene, "wireframe_grid", False) else 1) \
+            if getattr(scene, "wireframe", False) else 0
         sc.workers = int(workers)
         sc.backend = 0 if backend == "cpu" else BACKEND_CUDA
         fog = getattr(scene, "fog", None)

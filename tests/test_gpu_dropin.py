@@ -74,6 +74,13 @@ CASES = {
     # draw_skybox (IBL maps handed over by the harness hook, as the patch's IBL row)
     "env_background": lambda: dataclasses.replace(scenes.small_scene(seed=74, env=1),
                                                   env_background=True),
+    # MOP_RENDER_WIREFRAME through mop_viewport_set_render_mode: the core marks every
+    # draw but ID 0 wireframe; with the chrome off its hidden grid (a zero-opacity blended
+    # chrome mesh) is drawn as lines too, on both backends
+    "wireframe_grid": lambda: dataclasses.replace(scenes.wireframe_scene(seed=75),
+                                                  wireframe_grid=True),
+    "wireframe_ssaa2_transparent": lambda: dataclasses.replace(
+        scenes.transparent_scene(seed=76, width=128, height=96, ssaa=2), wireframe=True),
     "config2_reduced_no_ibl": lambda: dataclasses.replace(
         scenes.config2(width=480, height=270, ssaa=2, instances=48, tex_size=64), env=0),
 }

@@ -126,6 +126,18 @@ CASES = {
     "env_background_ssaa2_transparent": lambda: dataclasses.replace(
         scenes.transparent_scene(seed=98, ssaa=2, env=1), env_background=True,
         env_rotation=0.7, env_intensity=1.3),
+    # MOP_RENDER_WIREFRAME: each triangle's edges as Xiaolin Wu lines in its flat colour,
+    # blended over what is there in submission order (ID 0 stays filled)
+    "wireframe": lambda: scenes.wireframe_scene(seed=121),
+    "wireframe_unlit_ssaa2": lambda: scenes.wireframe_scene(seed=122, ssaa=2, lights="none"),
+    "wireframe_flat_ssaa3": lambda: dataclasses.replace(
+        scenes.wireframe_scene(seed=123, width=96, height=64, ssaa=3), smooth=False),
+    "wireframe_transparent": lambda: dataclasses.replace(scenes.transparent_scene(seed=124),
+                                                         wireframe=True),
+    "wireframe_chrome": lambda: dataclasses.replace(scenes.chrome_scene(seed=125),
+                                                    wireframe=True),
+    "wireframe_instanced": lambda: dataclasses.replace(scenes.instanced_scene(seed=126),
+                                                       wireframe=True),
     # editor-chrome IDs among the opaque meshes: depth test and culling off, unlit
     "chrome": lambda: scenes.chrome_scene(seed=81),
     "chrome_ssaa2_flat": lambda: dataclasses.replace(scenes.chrome_scene(seed=82, ssaa=2),

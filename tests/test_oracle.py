@@ -70,6 +70,15 @@ LIVE = {
     "transparent_ssaa2_ibl": lambda: scenes.transparent_scene(seed=18, ssaa=2, env=1),
     # 64 stacked blended quads: more fragments on a sample than the device sorts in registers
     "transparent_deep": lambda: scenes.deep_transparent_scene(seed=19),
+    # MOP_RENDER_WIREFRAME: anti-aliased lines in the flat colour, lit and unlit, SSAA 2
+    "wireframe": lambda: scenes.wireframe_scene(seed=111),
+    "wireframe_unlit_ssaa2": lambda: scenes.wireframe_scene(seed=112, ssaa=2, lights="none"),
+    "wireframe_transparent": lambda: dataclasses.replace(scenes.transparent_scene(seed=113),
+                                                         wireframe=True),
+    "wireframe_instanced": lambda: dataclasses.replace(
+        scenes.instanced_scene(seed=114), wireframe=True),
+    "wireframe_chrome": lambda: dataclasses.replace(scenes.chrome_scene(seed=115),
+                                                    wireframe=True),
     "config3_small": lambda: scenes.config3(seed=19, n_tris=30_000, width=320, height=180),
     # pass_shadow + PCF: smooth, flat, SSAA 2 with IBL, with the transparent pass
     "shadow": lambda: scenes.shadow_scene(seed=31),
