@@ -756,6 +756,101 @@ def wireframe_scene(seed: int = 110, width: int = 160, height: int = 120, ssaa: 
     return dataclasses.replace(sc, wireframe=True)
 
 
+def fuzz_scene(seed: int) -> Scene:
+    """A seeded random frame for parity sweeps: 1-3 SSAA, random camera;
+    a ground plane plus 3-8 meshes drawn from spheres, tori and raw
+    triangle soups (degenerate, sliver, huge, behind the eye, straddling the
+    near plane, outside the frustum), random materials, opacities and blend
+    modes, some editor-chrome IDs; 0-5 lights of every type (some inactive,
+    some range-limited); smooth or flat shading, sometimes wireframe; random
+    post effects incl. fog and vignette."""
+    rng = np.random.default_rng(10_000 + seed)
+    w = int(rng.integers(40, 130))
+    h = int(rng.integers(30, 100))
+    ssaa = int(rng.integers(1, 4))
+    d = rng.normal(size=3)
+    d /= np.linalg.norm(d)
+    eye = tuple(float(x) for x in d * rng.uniform(3.0, 9.0))
+    target = tuple(float(x) for x in rng.uniform(-0.5, 0.5, 3))
+    sc = Scene(f"fuzz{seed}", w, h, ssaa, eye=eye, target=target,
+               fov_deg=float(rng.uniform(30.0, 90.0)), near=float(rng.uniform(0.05, 0.5)),
+               far=float(rng.uniform(20.0, 100.0)), sun_dir=(0.3, 0.8, 0.4))
+    n_lights = int(rng.integers(0, 6))
+    for k in range(n_lights):
+        t = int(rng.integers(0, 3))
+        p = tuple(float(x) for x in rng.uniform(-4, 4, 3))
+        dr = rng.normal(size=3)
+        dr /= np.linalg.norm(dr)
+        inner = float(rng.uniform(0.8, 0.99))
+        sc.lights.append(Light(t, position=p, direction=tuple(float(x) for x in dr),
+                               color=(*[float(x) for x in rng.uniform(0.3, 1.0, 3)], 1.0),
+                               intensity=float(rng.uniform(0.5, 30.0)),
+                               range=float(rng.uniform(2.0, 10.0)) if rng.random() < 0.3 else 0.0,
+                               spot_inner_cos=inner, spot_outer_cos=inner - float(rng.uniform(0.0, 0.2)),
+                               active=bool(rng.random() < 0.85)))
+    if rng.random() < 0.5:
+        sc.textures.append(value_noise_texture(rng, 32, 4))
+    v, i = ground_plane(float(rng.uniform(4.0, 20.0)), _color(rng))
+    sc.meshes.append(Mesh(v, i, 1, mat_identity(), *_mat_rand(rng)))
+    oid = 2
+    for n in range(int(rng.integers(3, 9))):
+        kind = int(rng.integers(0, 4))
+        c = _color(rng)
+        if kind == 0:
+            v, i = uv_sphere(int(rng.integers(6, 20)), int(rng.integers(4, 10)),
+                             float(rng.uniform(0.2, 1.2)), c)
+        elif kind == 1:
+            v, i = torus(int(rng.integers(8, 24)), int(rng.integers(4, 12)), 0.8, 0.25, c)
+        else:  # triangle soup with awkward cases
+            nt = int(rng.integers(4, 40))
+            pos = rng.uniform(-2.5, 2.5, (nt * 3, 3)).astype(np.float32)
+            for t in range(nt):
+                r = rng.random()
+                if r < 0.1:  # degenerate: repeated vertex
+                    pos[3 * t + 2] = pos[3 * t]
+                elif r < 0.2:  # sliver
+                    pos[3 * t + 2] = pos[3 * t] + (pos[3 * t + 1] - pos[3 * t]) * 0.5 + 1e-4
+                elif r < 0.3:  # huge
+                    pos[3 * t:3 * t + 3] *= 40.0
+                elif r < 0.4:  # through the eye / near plane
+                    pos[3 * t] = np.asarray(eye, np.float32) * float(rng.uniform(0.8, 1.2))
+            nrm = rng.normal(size=(nt * 3, 3)).astype(np.float32)
+            nrm /= np.linalg.norm(nrm, axis=1, keepdims=True)
+            col = np.concatenate([rng.uniform(0, 1, (nt * 3, 3)), np.ones((nt * 3, 1))], 1)
+            uv = rng.uniform(0, 1, (nt * 3, 2))
+            v = _pack(pos, nrm, col.astype(np.float32), uv.astype(np.float32))
+            i = np.arange(nt * 3, dtype=np.uint32)
+        t = rng.uniform(-2.0, 2.0, 3)
+        s_ = float(rng.uniform(0.5, 1.5))
+        m = mat_trs(t, random_rotation(rng), (s_, s_, s_))
+        mt, rough = _mat_rand(rng)
+        r = rng.random()
+        op, bm = 1.0, BLEND_OPAQUE
+        if r < 0.2:
+            op, bm = float(rng.uniform(0.1, 0.9)), BLEND_ALPHA
+        elif r < 0.3:
+            op, bm = float(rng.uniform(0.3, 1.0)), BLEND_ADDITIVE
+        elif r < 0.4:
+            op, bm = float(rng.uniform(0.3, 1.0)), BLEND_MULTIPLY
+        mid = CHROME_ID_FLOOR + 32 + n if rng.random() < 0.1 else oid
+        oid += 1
+        tex = 0 if (sc.textures and rng.random() < 0.5) else -1
+        sc.meshes.append(Mesh(v, i, mid, m, mt, rough, texture=tex, opacity=op, blend_mode=bm))
+    post = DEFAULT_POST
+    if rng.random() < 0.3:
+        post |= POST_TONEMAP
+    if rng.random() < 0.2:
+        post |= POST_VIGNETTE
+    fog = None
+    if rng.random() < 0.2:
+        post |= POST_FOG
+        fog = ((*[float(x) for x in rng.uniform(0, 1, 3)], 1.0), float(rng.uniform(0.8, 0.95)),
+               float(rng.uniform(0.95, 1.0)))
+    return dataclasses.replace(sc, smooth=bool(rng.random() < 0.75),
+                               wireframe=seed % 6 == 5 or bool(rng.random() < 0.1),
+                               post_effects=post, fog=fog)
+
+
 def instanced_scene(seed: int = 70, width: int = 192, height: int = 144, ssaa: int = 1,
                     n_instances: int = 96, transparent: bool = False, env: int = 0,
                     zero_id: bool = False) -> Scene:

@@ -128,7 +128,22 @@ LIVE = {
 @pytest.mark.skipif(not refdrive.available(), reason="reference library not built")
 @pytest.mark.parametrize("name", list(LIVE))
 def test_oracle_matches_reference_live(name):
-    sc = LIVE[name]()
+    _check_live(LIVE[name](), name)
+
+
+# seeded random frames (scenes.fuzz_scene): random geometry incl. degenerate, sliver, huge and
+# near-plane triangles, every light type, blend modes, flat / smooth / wireframe, chrome IDs,
+# post effects; the same seeds drive the device sweep in tests/test_gpu_fuzz.py
+FUZZ_SEEDS = list(range(96))
+
+
+@pytest.mark.skipif(not refdrive.available(), reason="reference library not built")
+@pytest.mark.parametrize("seed", FUZZ_SEEDS)
+def test_oracle_matches_reference_fuzz(seed):
+    _check_live(scenes.fuzz_scene(seed), f"fuzz{seed}")
+
+
+def _check_live(sc, name):
     r = refdrive.Reference(sc, serial=True)
     try:
         ref = r.render()
