@@ -486,9 +486,10 @@ void mopcuda_scene_destroy(MopCudaScene *scene);
  * order; each viewport renders the non-blended ones in that order, then the
  * blended ones (blend_mode != 0) back to front by the squared distance of
  * their model translation to its eye (pass_scene_opaque /
- * pass_scene_transparent, viewport.c:2449-2553).  Refused: draws with the
- * depth test or the depth write off (MOPCUDA_EUNSUPPORTED) and a 1,025th
- * blended draw.  Returns the draw's index (>= 0) or an error code. */
+ * pass_scene_transparent, viewport.c:2449-2553).  Refused
+ * (MOPCUDA_EUNSUPPORTED): draws with the depth test or the depth write off,
+ * a 1,025th blended draw, and wireframe draws in a scene of 2^26 or more
+ * triangles.  Returns the draw's index (>= 0) or an error code. */
 int mopcuda_scene_add_draw(MopCudaScene *scene, const MopCudaDraw *draw);
 /* Replaces draw `index`'s model matrix (TRS update); effective from the next
  * batch submit. */

@@ -204,6 +204,7 @@ struct MopCudaDevice {
   DevArena deform_params; /* bone matrices / morph weights of a deform call */
   DevArena hdr, frag_head, frags, touched, olist, olist_items; /* blended suffix */
   DevArena wlist, wlist_items; /* wireframe records of the suffix */
+  DevArena oscratch;           /* the fold's sort scratch for long fragment lists */
   uint32_t frag_hint = 0, olist_hint = 0;
   HostArena h_deform;
   /* shadow pass: casters recorded between shadow_begin and shadow_end; the

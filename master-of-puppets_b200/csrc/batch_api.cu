@@ -151,10 +151,10 @@ extern "C" int mopcuda_scene_add_draw(MopCudaScene *s, const MopCudaDraw *c) {
     s->lights.resize(nl);
     return rc;
   }
-  if (!skip && (r.flags & (DF_NO_DEPTH_WRITE | DF_NO_DEPTH_TEST | DF_WIRE))) {
+  if (!skip && (r.flags & (DF_NO_DEPTH_WRITE | DF_NO_DEPTH_TEST))) {
     s->lights.resize(nl);
-    return fail(MOPCUDA_EUNSUPPORTED, "scene_add_draw: batches render filled, depth-tested, "
-                                      "depth-writing draws only");
+    return fail(MOPCUDA_EUNSUPPORTED,
+                "scene_add_draw: batches render depth-tested, depth-writing draws only");
   }
   if (skip) { /* zero opacity: a colour no-op, kept as an empty slot */
     memset(&r, 0, sizeof r);
@@ -164,8 +164,18 @@ extern "C" int mopcuda_scene_add_draw(MopCudaScene *s, const MopCudaDraw *c) {
    * viewport composites them in its ordered suffix, the blended ones in
    * the core's back-to-front order for that viewport's eye */
   const float op = r.opacity < 0.0f ? 0.0f : (r.opacity > 1.0f ? 1.0f : r.opacity);
-  if (!skip && (r.blend_mode != 0 || op < 1.0f || ((r.flags & DF_SMOOTH) && !(r.flags & DF_LIT))))
+  if (!skip && (r.blend_mode != 0 || op < 1.0f || ((r.flags & DF_SMOOTH) && !(r.flags & DF_LIT)) ||
+                (r.flags & DF_WIRE)))
     r.flags |= DF_ORDERED;
+  /* line plots mark fragment payloads with bit 31: a viewport's triangles
+   * stay below 2^26 when the scene has wireframe draws */
+  if ((r.flags & DF_WIRE) || s->wire) {
+    if ((uint64_t)s->tris + r.index_count / 3u >= (1ull << (31 - ORDER_FAN_BITS))) {
+      s->lights.resize(nl);
+      return fail(MOPCUDA_EUNSUPPORTED, "scene_add_draw: wireframe draws in a scene of 2^26 "
+                                        "or more triangles");
+    }
+  }
   if (r.blend_mode != 0 && s->blended >= BATCH_MAX_BLENDED) {
     s->lights.resize(nl);
     return fail(MOPCUDA_EUNSUPPORTED, "scene_add_draw: more than %d blended draws in a scene",
@@ -175,6 +185,8 @@ extern "C" int mopcuda_scene_add_draw(MopCudaScene *s, const MopCudaDraw *c) {
     return fail(MOPCUDA_EINVAL, "scene too large");
   if (r.blend_mode != 0)
     s->blended++;
+  if (r.flags & DF_WIRE)
+    s->wire = true;
   if (r.flags & DF_ORDERED)
     s->ordered_tris += r.index_count / 3u;
   s->draws.push_back(r);
@@ -270,7 +282,9 @@ uint64_t mc_view_bytes(const MopCudaScene *s, uint64_t samples, uint64_t pixels)
   /* an ordered suffix: hdr, list heads and touched samples, a fragment per
    * sample and the suffix-record list */
   const uint64_t suffix =
-      s->ordered_tris ? 32ull * samples + 8ull * (s->ordered_tris + need[2]) + 4096ull * 8ull : 0ull;
+      s->ordered_tris ? 32ull * samples + (s->wire ? 16ull : 8ull) * (s->ordered_tris + need[2]) +
+                            4096ull * 8ull
+                      : 0ull;
   return 28ull * samples + 4ull * pixels + pools / 2 + suffix +
          sizeof(DrawRec) * s->draws.size();
 }
@@ -324,10 +338,10 @@ void LaunchCore::release() {
                         &d_post_views, &d_draws, &d_scenes, &clip, &world, &normal, &color,
                         &rrec, &srec, &clipq, &large_list, &large_items, &keys, &shade_list,
                         &pre, &out, &depth, &ids, &presented, &hdr, &frag_head, &touched,
-                        &frags, &olist, &olist_items};
+                        &frags, &olist, &olist_items, &wlist, &wlist_items, &oscratch};
   for (DevArena *a : arenas)
     a->release();
-  frag_pool = olist_pool = 0;
+  frag_pool = olist_pool = wlist_pool = 0;
   for (EntryShadow &e : shadows) {
     DevArena *sa[] = {&e.map, &e.d_draws, &e.recs, &e.items, &e.ctr};
     for (DevArena *a : sa)
@@ -355,11 +369,12 @@ void LaunchCore::trim() {
   DevArena *arenas[] = {&clip,       &world, &normal,  &color,      &rrec,      &srec,
                         &clipq,      &large_list, &large_items, &keys, &shade_list, &pre,
                         &out,        &depth, &ids,     &presented,  &hdr,       &frag_head,
-                        &touched,    &frags, &olist,   &olist_items};
+                        &touched,    &frags, &olist,   &olist_items, &wlist, &wlist_items,
+                        &oscratch};
   for (DevArena *a : arenas)
     a->release();
   vertex_pool = rec_pool = clip_pool = large_pool = 0;
-  frag_pool = olist_pool = 0;
+  frag_pool = olist_pool = wlist_pool = 0;
 }
 
 uint64_t LaunchCore::device_bytes() const {
@@ -367,7 +382,8 @@ uint64_t LaunchCore::device_bytes() const {
                               &d_post_views, &d_draws, &d_scenes, &clip, &world, &normal, &color,
                               &rrec, &srec, &clipq, &large_list, &large_items, &keys,
                               &shade_list, &pre, &out, &depth, &ids, &presented, &hdr,
-                              &frag_head, &touched, &frags, &olist, &olist_items};
+                              &frag_head, &touched, &frags, &olist, &olist_items, &wlist,
+                              &wlist_items, &oscratch};
   uint64_t t = 0;
   for (const DevArena *a : arenas)
     t += a->cap;
@@ -646,7 +662,8 @@ int LaunchCore::stage_suffix() {
     any_ordered |= s->ordered_tris > 0;
   if (!any_ordered)
     return MOPCUDA_OK;
-  unsigned long long ol = 0, fr = 0;
+  unsigned long long ol = 0, fr = 0, wl = 0;
+  any_wire = false;
   for (uint32_t i = 0; i < nv; i++) {
     const MopCudaScene *s = scenes[vrec[i].scene];
     if (!s->ordered_tris)
@@ -655,9 +672,14 @@ int LaunchCore::stage_suffix() {
     mc_pool_need(s->tris, s->verts, fan_num, large_num, need);
     ol += s->ordered_tris + need[2];
     fr += (unsigned long long)vrec[i].width * vrec[i].height * frag_num / 4ull + 4096ull;
+    if (s->wire) {
+      any_wire = true;
+      wl += s->ordered_tris + need[2];
+    }
   }
   const unsigned long long sa = std::max(total_samples, sample_floor);
-  void *before[6] = {hdr.p, frag_head.p, touched.p, frags.p, olist.p, olist_items.p};
+  void *before[9] = {hdr.p, frag_head.p, touched.p, frags.p, olist.p, olist_items.p,
+                     wlist.p, wlist_items.p, oscratch.p};
   int rc = 0;
   rc |= hdr.ensure(16ull * sa);
   rc |= frag_head.ensure(4ull * sa);
@@ -666,13 +688,21 @@ int LaunchCore::stage_suffix() {
     rc |= olist.ensure(4ull * ol);
     rc |= olist_items.ensure(4ull * ol);
   }
-  if (frag_pool < fr)
+  if (frag_pool < fr) {
     rc |= frags.ensure(8ull * fr);
+    rc |= oscratch.ensure(16ull * fr);
+  }
+  if (any_wire && wlist_pool < wl) {
+    rc |= wlist.ensure(4ull * wl);
+    rc |= wlist_items.ensure(4ull * wl);
+  }
   if (rc)
     return MOPCUDA_ENOMEM;
   olist_pool = std::min(olist.cap / 4, olist_items.cap / 4);
-  frag_pool = frags.cap / 8;
-  void *after_[6] = {hdr.p, frag_head.p, touched.p, frags.p, olist.p, olist_items.p};
+  frag_pool = std::min(frags.cap / 8, oscratch.cap / 16);
+  wlist_pool = std::min(wlist.cap / 4, wlist_items.cap / 4);
+  void *after_[9] = {hdr.p, frag_head.p, touched.p, frags.p, olist.p, olist_items.p,
+                     wlist.p, wlist_items.p, oscratch.p};
   if (memcmp(before, after_, sizeof before) != 0)
     suffix_moved = true;
   return MOPCUDA_OK;
@@ -733,6 +763,13 @@ int LaunchCore::enqueue(int parts) {
     a.olist = olist.as<uint32_t>();
     a.olist_items = olist_items.as<uint32_t>();
     a.olist_pool = olist_pool;
+    a.oscratch = oscratch.as<ulonglong2>();
+    a.oscratch_count = &d_status.as<BatchStatus>()->scratch_count;
+    if (any_wire) {
+      a.wlist = wlist.as<uint32_t>();
+      a.wlist_items = wlist_items.as<uint32_t>();
+      a.wlist_pool = wlist_pool;
+    }
   }
 
   const uint32_t *pv[4];
@@ -818,18 +855,43 @@ int LaunchCore::after(bool *rerun, int attempt) {
       return fail(MOPCUDA_ENOMEM, "launch: suffix-record list exhausted");
     fan_num *= 2u;
   }
-  if (view_over & 16u) { /* a viewport's fragments */
-    if (frag_num >= 4096u)
-      return fail(MOPCUDA_ENOMEM, "launch: blended-fragment reserve exhausted");
-    frag_num *= 2u;
+  if (view_over & 128u) { /* a viewport's wireframe-record list: the fan reserve */
+    if (fan_num >= 256u)
+      return fail(MOPCUDA_ENOMEM, "launch: wireframe-record list exhausted");
+    fan_num *= 2u;
   }
-  if (st->overflow & 64u)
+  if (view_over & 16u) { /* a viewport's fragments: its counter holds the demand */
+    if (frag_num >= (1u << 20))
+      return fail(MOPCUDA_ENOMEM, "launch: blended-fragment reserve exhausted");
+    unsigned long long want = 2ull * frag_num;
+    for (uint32_t i = 0; i < nv; i++) {
+      if (!(ctr[i].overflow & 16u))
+        continue;
+      const unsigned long long S = (unsigned long long)vrec[i].width * vrec[i].height;
+      const unsigned long long need = 4ull * ctr[i].frag_count / (S ? S : 1ull) + 1ull;
+      want = std::max(want, need + need / 4);
+    }
+    while (frag_num < want && frag_num < (1u << 20))
+      frag_num *= 2u;
+  }
+  if (st->overflow & 256u)
     return fail(MOPCUDA_ENOMEM, "launch: a viewport has an ordered suffix but the launch has "
                                 "no suffix buffers");
-  if (st->overflow & 48u) { /* the suffix pools */
+  if (view_over & (16u | 32u | 128u)) { /* the reserves grew: pools to match */
+    int rc = stage_suffix();
+    if (rc)
+      return rc;
+  }
+  if (st->overflow & 112u) { /* the suffix pools */
     const unsigned long long ol = st->need_olist + st->need_olist / 4 + 4096ull;
     const unsigned long long fr = st->need_frag + st->need_frag / 4 + 4096ull;
+    const unsigned long long wl = st->need_wlist + st->need_wlist / 4 + 4096ull;
     int rc = 0;
+    if ((st->overflow & 64u) && wl > wlist_pool) {
+      rc |= wlist.ensure(4ull * wl);
+      rc |= wlist_items.ensure(4ull * wl);
+      wlist_pool = std::min(wlist.cap / 4, wlist_items.cap / 4);
+    }
     if ((st->overflow & 16u) && ol > olist_pool) {
       rc |= olist.ensure(4ull * ol);
       rc |= olist_items.ensure(4ull * ol);
@@ -837,7 +899,8 @@ int LaunchCore::after(bool *rerun, int attempt) {
     }
     if ((st->overflow & 32u) && fr > frag_pool) {
       rc |= frags.ensure(8ull * fr);
-      frag_pool = frags.cap / 8;
+      rc |= oscratch.ensure(16ull * fr);
+      frag_pool = std::min(frags.cap / 8, oscratch.cap / 16);
     }
     if (rc)
       return MOPCUDA_ENOMEM;

@@ -36,6 +36,7 @@ struct MopCudaScene {
    * per viewport) and the triangles of every DF_ORDERED draw */
   uint32_t blended = 0;
   uint64_t ordered_tris = 0;
+  bool wire = false; /* has wireframe draws */
   std::mutex mu;
 };
 
@@ -81,9 +82,9 @@ struct LaunchCore {
   /* ordered suffix: a scene entry with order-dependent draws gives the
    * launch its per-sample buffers and pools; suffix_moved: stage()
    * reallocated one of them */
-  bool any_ordered = false, suffix_moved = false;
-  DevArena hdr, frag_head, touched, frags, olist, olist_items;
-  unsigned long long frag_pool = 0, olist_pool = 0;
+  bool any_ordered = false, any_wire = false, suffix_moved = false;
+  DevArena hdr, frag_head, touched, frags, olist, olist_items, wlist, wlist_items, oscratch;
+  unsigned long long frag_pool = 0, olist_pool = 0, wlist_pool = 0;
   uint32_t frag_num = 4;
   uint32_t post_count[4] = {0, 0, 0, 0}, post_tiles[4] = {0, 0, 0, 0};
   unsigned long long total_samples = 0, total_pixels = 0;

@@ -2316,23 +2316,28 @@ __global__ void __launch_bounds__(1024) k_wscan(FrameArgs a) {
 /* One line plot: in the framebuffer, coverage at least 0.004 and in front
  * of the opaque depth (or any depth when the suffix keeps every fragment)
  * gives a fragment. */
+__device__ __forceinline__ void wplot_item(const FrameArgs &a, uint32_t it) {
+  if (it >= FRAG_WIRE_BIT)
+    return;
+  uint32_t rid, k;
+  WuLine L;
+  if (!wire_item(a, it, rid, L, k))
+    return;
+  int x, y;
+  float z, cov;
+  wu_plot(L, k, x, y, z, cov);
+  if (x < 0 || x >= a.width || y < 0 || y >= a.height || cov < 0.004f)
+    return;
+  const uint32_t px = (uint32_t)y * (uint32_t)a.width + (uint32_t)x;
+  if (a.ordered_keep_all || z < a.depth[px])
+    push_fragment(a, px, FRAG_WIRE_BIT | it);
+}
+
 __global__ void __launch_bounds__(256) k_wplot(FrameArgs a) {
   const uint32_t total = a.ctr->wire_items;
-  for (uint32_t it = blockIdx.x * blockDim.x + threadIdx.x; it < total && it < FRAG_WIRE_BIT;
-       it += gridDim.x * blockDim.x) {
-    uint32_t rid, k;
-    WuLine L;
-    if (!wire_item(a, it, rid, L, k))
-      continue;
-    int x, y;
-    float z, cov;
-    wu_plot(L, k, x, y, z, cov);
-    if (x < 0 || x >= a.width || y < 0 || y >= a.height || cov < 0.004f)
-      continue;
-    const uint32_t px = (uint32_t)y * (uint32_t)a.width + (uint32_t)x;
-    if (a.ordered_keep_all || z < a.depth[px])
-      push_fragment(a, px, FRAG_WIRE_BIT | it);
-  }
+  for (uint32_t it = blockIdx.x * blockDim.x + threadIdx.x; it < total;
+       it += gridDim.x * blockDim.x)
+    wplot_item(a, it);
 }
 
 /* The record behind an order (triangle << 5 | fan), as shade_item finds it. */
@@ -2418,7 +2423,9 @@ __device__ __forceinline__ void ofold_fragment(const FrameArgs &a, OFold &st, in
   if (r.y1 & REC_FLAT_BIT) { /* rasterize_filled_triangle, rasterizer.c:1000-1083 */
     const float z = fold_add(fold_add(r.zc[0], r.zc[2], jr), r.zc[1], kc);
     if (!dtest || z < st.depth) {
-      const float ca = d.opacity < 0.0f ? 0.0f : (d.opacity > 1.0f ? 1.0f : d.opacity);
+      float ca = d.opacity < 0.0f ? 0.0f : (d.opacity > 1.0f ? 1.0f : d.opacity);
+      if (!(d.flags & DF_LIT)) /* the unlit path quantises it (rasterizer.c:1159, 1237) */
+        ca = (float)(uint8_t)x86_f2i(ca * 255.0f) / 255.0f;
       if (d.blend_mode == 0 && ca >= 1.0f) {
         st.hdr[0] = s.col[0];
         st.hdr[1] = s.col[1];
@@ -2502,22 +2509,52 @@ __device__ __forceinline__ void ofold_fragment(const FrameArgs &a, OFold &st, in
   }
 }
 
+/* Ascending heapsort of n (key, payload) pairs by key (distinct keys). */
+__device__ __forceinline__ void heap_sift(ulonglong2 *h, uint32_t i, uint32_t n) {
+  const ulonglong2 v = h[i];
+  for (;;) {
+    uint32_t c = 2u * i + 1u;
+    if (c >= n)
+      break;
+    if (c + 1u < n && h[c + 1u].x > h[c].x)
+      c++;
+    if (h[c].x <= v.x)
+      break;
+    h[i] = h[c];
+    i = c;
+  }
+  h[i] = v;
+}
+
+__device__ __noinline__ void heapsort_keys(ulonglong2 *h, uint32_t n) {
+  if (n < 2u)
+    return;
+  for (uint32_t i = n / 2u; i-- > 0u;)
+    heap_sift(h, i, n);
+  for (uint32_t e = n - 1u; e > 0u; e--) {
+    const ulonglong2 t = h[0];
+    h[0] = h[e];
+    h[e] = t;
+    heap_sift(h, 0u, e);
+  }
+}
+
 /* Each touched sample folds its fragments in submission order.  Up to
  * ORDERED_MAX_FRAGS are gathered and insertion-sorted in registers; a
- * longer list is applied by selection, each step walking the list for the
- * smallest key above the last one applied (keys are distinct: a record
- * covers a sample once, a line plot is one item).  WIRE: the frame has line
+ * longer list is copied with its keys into the fold's scratch and heapsorted
+ * there (keys are distinct: a record covers a sample once, a line plot is
+ * one item).  WIRE: the frame has line
  * plots, whose payloads sort by frag_key (a triangle's plots in the
  * reference's drawing order after the triangles before it). */
 template <bool WIRE>
 __device__ __forceinline__ unsigned long long ofold_key(const FrameArgs &a, uint32_t v) {
-  return WIRE ? frag_key(a, v) : (unsigned long long)v;
+  return (WIRE && a.wire) ? frag_key(a, v) : (unsigned long long)v;
 }
 
 template <bool SH, bool WIRE>
 __device__ __forceinline__ void ofold_apply(const FrameArgs &a, OFold &st, int x, int y,
                                             uint32_t v) {
-  if (WIRE && (v & FRAG_WIRE_BIT))
+  if (WIRE && a.wire && (v & FRAG_WIRE_BIT))
     ofold_wire(a, st, v & ~FRAG_WIRE_BIT);
   else
     ofold_fragment<SH>(a, st, x, y, v);
@@ -2555,41 +2592,52 @@ __device__ __forceinline__ void ofold_item(const FrameArgs &a, uint32_t i) {
   st.cur = 0xffffffffu;
   st.cur_nw = false;
   if (total <= ORDERED_MAX_FRAGS) {
-    for (uint32_t k = 1; k < cnt; k++) { /* submission order */
-      const uint32_t v = ord[k];
-      const unsigned long long kv = ofold_key<WIRE>(a, v);
-      uint32_t j = k;
-      while (j > 0 && ofold_key<WIRE>(a, ord[j - 1]) > kv) {
-        ord[j] = ord[j - 1];
-        j--;
+    if (WIRE && a.wire) { /* keys computed once: a plot's key takes a search */
+      unsigned long long key[WIRE ? ORDERED_MAX_FRAGS : 1];
+      for (uint32_t k = 0; k < cnt; k++)
+        key[k] = frag_key(a, ord[k]);
+      for (uint32_t k = 1; k < cnt; k++) {
+        const uint32_t v = ord[k];
+        const unsigned long long kv = key[k];
+        uint32_t j = k;
+        while (j > 0 && key[j - 1] > kv) {
+          ord[j] = ord[j - 1];
+          key[j] = key[j - 1];
+          j--;
+        }
+        ord[j] = v;
+        key[j] = kv;
       }
-      ord[j] = v;
+    } else {
+      for (uint32_t k = 1; k < cnt; k++) { /* submission order */
+        const uint32_t v = ord[k];
+        uint32_t j = k;
+        while (j > 0 && ord[j - 1] > v) {
+          ord[j] = ord[j - 1];
+          j--;
+        }
+        ord[j] = v;
+      }
     }
     for (uint32_t k = 0; k < cnt; k++)
       ofold_apply<SH, WIRE>(a, st, x, y, ord[k]);
   } else {
-    unsigned long long last = 0;
-    for (uint32_t k = 0; k < total; k++) {
-      bool found = false;
-      uint32_t best = 0, steps = 0;
-      unsigned long long best_key = 0;
-      for (uint32_t node = head; node != 0xffffffffu && node < a.frag_cap;
-           node = a.frags[node].x) {
-        const uint32_t o = a.frags[node].y;
-        const unsigned long long ko = ofold_key<WIRE>(a, o);
-        if ((k == 0 || ko > last) && (!found || ko < best_key)) {
-          best = o;
-          best_key = ko;
-          found = true;
-        }
-        if (++steps >= total)
-          break;
-      }
-      if (!found)
-        break;
-      ofold_apply<SH, WIRE>(a, st, x, y, best);
-      last = best_key;
+    /* a long list: its (key, payload) pairs heapsorted in the scratch */
+    const uint32_t base = atomicAdd(a.oscratch_count, total);
+    if (!a.oscratch || (unsigned long long)base + total > a.oscratch_cap) {
+      atomicOr(&a.ctr->overflow, 16u); /* unreachable: the scratch holds the fragment pool */
+      return;
     }
+    ulonglong2 *sc = a.oscratch + base;
+    uint32_t m = 0;
+    for (uint32_t node = head; node != 0xffffffffu && node < a.frag_cap && m < total;
+         node = a.frags[node].x) {
+      const uint32_t v = a.frags[node].y;
+      sc[m++] = make_ulonglong2(ofold_key<WIRE>(a, v), (unsigned long long)v);
+    }
+    heapsort_keys(sc, m);
+    for (uint32_t k = 0; k < m; k++)
+      ofold_apply<SH, WIRE>(a, st, x, y, (uint32_t)sc[k].y);
   }
   if (st.cur_nw)
     st.depth = st.saved;
@@ -2742,7 +2790,7 @@ __global__ void __launch_bounds__(256) k_batch_prepare(BatchArgs b) {
   __shared__ uint32_t s_bl[BATCH_MAX_BLENDED]; /* blended draws, scene order */
   __shared__ float s_bd[BATCH_MAX_BLENDED];    /* their squared eye distances */
   __shared__ uint32_t s_by[BATCH_MAX_BLENDED]; /* back-to-front position -> s_bl slot */
-  __shared__ uint32_t s_split, s_nan;
+  __shared__ uint32_t s_split, s_nan, s_wire;
   const uint32_t v = blockIdx.x;
   const ViewRec &vw = b.views[v];
   const SceneDesc &sc = b.scenes[vw.scene];
@@ -2751,6 +2799,7 @@ __global__ void __launch_bounds__(256) k_batch_prepare(BatchArgs b) {
     s_tot[0] = s_tot[1] = s_tot[2] = s_tot[3] = 0u;
     s_split = 0xffffffffu;
     s_nan = 0u;
+    s_wire = 0u;
   }
   __syncthreads();
   for (uint32_t base = 0; base < sc.nd; base += 256u) {
@@ -2772,6 +2821,8 @@ __global__ void __launch_bounds__(256) k_batch_prepare(BatchArgs b) {
       emit_view_draw(sc, vw, i, mvp, out, off[0], off[1], off[2]);
       if (sc.draws[i].flags & DF_ORDERED)
         atomicMin(&s_split, off[2]);
+      if (sc.draws[i].flags & DF_WIRE)
+        atomicOr(&s_wire, 1u);
     }
     if (x[3] && off[3] < BATCH_MAX_BLENDED) {
       const float *m = sc.draws[i].model;
@@ -2829,8 +2880,11 @@ __global__ void __launch_bounds__(256) k_batch_prepare(BatchArgs b) {
       x[2] = sc.draws[i].index_count / 3u;
     }
     block_prefix<4>(x, off, s_w, s_tot);
-    if (x[0])
+    if (x[0]) {
       emit_view_draw(sc, vw, i, mvp, out, off[0], off[1], off[2]);
+      if (sc.draws[i].flags & DF_WIRE)
+        atomicOr(&s_wire, 1u);
+    }
   }
   if (threadIdx.x == 0) {
     FrameArgs a = b.tmpl;
@@ -2872,13 +2926,21 @@ __global__ void __launch_bounds__(256) k_batch_prepare(BatchArgs b) {
     a.frag_cap = 0u;
     a.olist = a.olist_items = nullptr;
     a.olist_cap = 0u;
+    a.wire = (int)s_wire;
+    a.wlist = a.wlist_items = nullptr;
+    a.wlist_cap = 0u;
+    a.oscratch = b.oscratch;
+    a.oscratch_count = b.oscratch_count;
+    a.oscratch_cap = (uint32_t)(b.frag_pool < 0xffffffffull ? b.frag_pool : 0xffffffffull);
+    if (s_wire && !b.wlist)
+      atomicOr(&b.status->overflow, 256u);
     if (s_split != 0xffffffffu && b.hdr) {
       a.hdr = b.hdr + vw.sample_off;
       a.frag_head = b.frag_head + vw.sample_off;
       a.touched = b.touched + vw.sample_off;
     } else {
       if (s_split != 0xffffffffu)
-        atomicOr(&b.status->overflow, 64u);
+        atomicOr(&b.status->overflow, 256u);
       a.hdr = nullptr;
       a.frag_head = a.touched = nullptr;
     }
@@ -2892,18 +2954,18 @@ __global__ void __launch_bounds__(256) k_batch_prepare(BatchArgs b) {
  * scans over the viewports).  A viewport that does not fit renders nothing this time and
  * the status tells the host how large the pools must grow. */
 __global__ void __launch_bounds__(256) k_batch_alloc(BatchArgs b) {
-  constexpr int NP = 6;
+  constexpr int NP = 7;
   __shared__ unsigned long long s_w[8][NP];
   __shared__ unsigned long long s_tot[NP];
   const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
-  const unsigned long long pool[NP] = {b.vertex_pool, b.rec_pool,   b.clip_pool,
-                                       b.large_pool,  b.olist_pool, b.frag_pool};
+  const unsigned long long pool[NP] = {b.vertex_pool, b.rec_pool,   b.clip_pool, b.large_pool,
+                                       b.olist_pool,  b.frag_pool, b.wlist_pool};
   if (threadIdx.x < NP)
     s_tot[threadIdx.x] = 0ull;
   __syncthreads();
   for (uint32_t base = 0; base < b.nv; base += 256u) {
     const uint32_t v = base + threadIdx.x;
-    unsigned long long need[NP] = {0ull, 0ull, 0ull, 0ull, 0ull, 0ull};
+    unsigned long long need[NP] = {0ull, 0ull, 0ull, 0ull, 0ull, 0ull, 0ull};
     if (v < b.nv) {
       const FrameArgs &a = b.frames[v];
       const unsigned long long T = a.total_tris, fan = T * b.fan_num / 8ull + 1024ull;
@@ -2915,6 +2977,8 @@ __global__ void __launch_bounds__(256) k_batch_alloc(BatchArgs b) {
         need[4] = (T - (a.t_split < T ? a.t_split : T)) + fan;
         need[5] = (unsigned long long)a.width * (unsigned long long)a.height * b.frag_num / 4ull +
                   4096ull;
+        if (a.wire)
+          need[6] = need[4];
       }
     }
     unsigned long long incl[NP];
@@ -2981,6 +3045,11 @@ __global__ void __launch_bounds__(256) k_batch_alloc(BatchArgs b) {
         a.olist_cap = (uint32_t)need[4];
         a.frags = b.frags + off[5];
         a.frag_cap = (uint32_t)(need[5] < 0xfffffff0ull ? need[5] : 0xfffffff0ull);
+        if (a.wire) {
+          a.wlist = b.wlist + off[6];
+          a.wlist_items = b.wlist_items + off[6];
+          a.wlist_cap = (uint32_t)need[6];
+        }
       }
     }
     __syncthreads();
@@ -2992,11 +3061,12 @@ __global__ void __launch_bounds__(256) k_batch_alloc(BatchArgs b) {
     b.status->need_large = s_tot[3];
     b.status->need_olist = s_tot[4];
     b.status->need_frag = s_tot[5];
+    b.status->need_wlist = s_tot[6];
   }
 }
 
 enum { ST_VERTEX, ST_SETUP, ST_CLIP, ST_RSMALL, ST_RLARGE, ST_SHADE, ST_RESOLVE, ST_OCOUNT,
-       ST_ORASTER, ST_OFOLD };
+       ST_ORASTER, ST_OFOLD, ST_WCOUNT, ST_WPLOT };
 
 template <int ST> __device__ __forceinline__ uint32_t stage_count(const FrameArgs &a) {
   switch (ST) {
@@ -3018,6 +3088,10 @@ template <int ST> __device__ __forceinline__ uint32_t stage_count(const FrameArg
     return a.hdr ? a.ctr->olist_items : 0u;
   case ST_OFOLD:
     return a.hdr ? a.ctr->touched_count : 0u;
+  case ST_WCOUNT:
+    return a.hdr && a.wire && a.total_tris ? ordered_record_items(a) : 0u;
+  case ST_WPLOT:
+    return a.hdr && a.wire ? a.ctr->wire_items : 0u;
   default: /* ST_RESOLVE: chunks of 256 x RESOLVE_PER_THREAD samples */
     return ((uint32_t)a.width * (uint32_t)a.height + 256u * RESOLVE_PER_THREAD - 1u) /
            (256u * RESOLVE_PER_THREAD);
@@ -3150,7 +3224,44 @@ __global__ void __launch_bounds__(256) k_b_oraster(const FrameArgs *__restrict__
   }
 }
 
-template <bool SH>
+/* Wireframe records of the viewports that have them (k_wcount, k_wscan,
+ * k_wplot per viewport). */
+__global__ void __launch_bounds__(256) k_b_wcount(const FrameArgs *__restrict__ fr, uint32_t nv) {
+  __shared__ uint32_t s_pre[MOPCUDA_MAX_VIEWS + 1];
+  const uint32_t total = views_prefix<ST_WCOUNT>(fr, nv, s_pre);
+  uint32_t v = 0;
+  for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < total;
+       g += gridDim.x * blockDim.x) {
+    while (s_pre[v + 1] <= g)
+      v++;
+    wcount_item(fr[v], g - s_pre[v]);
+  }
+}
+
+__global__ void __launch_bounds__(1024) k_b_wscan(const FrameArgs *__restrict__ fr) {
+  __shared__ uint32_t part[32];
+  const FrameArgs &a = fr[blockIdx.x];
+  if (a.hdr && a.wire) {
+    uint32_t n = a.ctr->wire_count;
+    if (n > a.wlist_cap)
+      n = a.wlist_cap;
+    items_scan_block(a.wlist_items, n, &a.ctr->wire_items, part);
+  }
+}
+
+__global__ void __launch_bounds__(256) k_b_wplot(const FrameArgs *__restrict__ fr, uint32_t nv) {
+  __shared__ uint32_t s_pre[MOPCUDA_MAX_VIEWS + 1];
+  const uint32_t total = views_prefix<ST_WPLOT>(fr, nv, s_pre);
+  uint32_t v = 0;
+  for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < total;
+       g += gridDim.x * blockDim.x) {
+    while (s_pre[v + 1] <= g)
+      v++;
+    wplot_item(fr[v], g - s_pre[v]);
+  }
+}
+
+template <bool SH, bool WIRE>
 __global__ void __launch_bounds__(128) k_b_ofold(const FrameArgs *__restrict__ fr, uint32_t nv) {
   __shared__ uint32_t s_pre[MOPCUDA_MAX_VIEWS + 1];
   const uint32_t total = views_prefix<ST_OFOLD>(fr, nv, s_pre);
@@ -3159,7 +3270,7 @@ __global__ void __launch_bounds__(128) k_b_ofold(const FrameArgs *__restrict__ f
        g += gridDim.x * blockDim.x) {
     while (s_pre[v + 1] <= g)
       v++;
-    ofold_item<SH, false>(fr[v], g - s_pre[v]);
+    ofold_item<SH, WIRE>(fr[v], g - s_pre[v]);
   }
 }
 
@@ -3267,11 +3378,21 @@ int mopcuda_launch_batch(const BatchArgs &b, const PostArgs *posts, const uint32
       k_b_ocount<<<sms * 8, 256, 0, s>>>(fr, nv);
       k_b_oscan<<<nv, 1024, 0, s>>>(fr);
       k_b_oraster<<<sms * 8, 256, 0, s>>>(fr, nv);
-      if (shadows)
-        k_b_ofold<true><<<sms * 8, 128, 0, s>>>(fr, nv);
-      else
-        k_b_ofold<false><<<sms * 8, 128, 0, s>>>(fr, nv);
       launches += 4;
+      if (b.wlist) { /* some viewport has wireframe draws */
+        k_b_wcount<<<sms * 8, 256, 0, s>>>(fr, nv);
+        k_b_wscan<<<nv, 1024, 0, s>>>(fr);
+        k_b_wplot<<<sms * 8, 256, 0, s>>>(fr, nv);
+        launches += 3;
+        if (shadows)
+          k_b_ofold<true, true><<<sms * 8, 128, 0, s>>>(fr, nv);
+        else
+          k_b_ofold<false, true><<<sms * 8, 128, 0, s>>>(fr, nv);
+      } else if (shadows) {
+        k_b_ofold<true, false><<<sms * 8, 128, 0, s>>>(fr, nv);
+      } else {
+        k_b_ofold<false, false><<<sms * 8, 128, 0, s>>>(fr, nv);
+      }
     }
   }
   if (!(parts & BATCH_PART_POST))

@@ -155,7 +155,7 @@ extern "C" void mopcuda_device_destroy(MopCudaDevice *d) {
                         &d->clipq,    &d->keys,       &d->large_list,  &d->large_items,
                         &d->shade_list, &d->counters, &d->pick_xy,     &d->pick_out,
                         &d->deform_params, &d->hdr, &d->frag_head, &d->frags, &d->touched,
-                        &d->olist, &d->olist_items, &d->wlist, &d->wlist_items, &d->sh_map[0], &d->sh_map[1], &d->sh_d_draws,
+                        &d->olist, &d->olist_items, &d->wlist, &d->wlist_items, &d->oscratch, &d->sh_map[0], &d->sh_map[1], &d->sh_d_draws,
                         &d->sh_recs, &d->sh_items, &d->sh_ctr, &d->env, &d->ibl_tab};
   for (DevArena *a : arenas)
     a->release();
@@ -1104,6 +1104,7 @@ static int launch_frame(MopCudaDevice *d) {
     rc |= d->frags.ensure(8ull * fcap);
     rc |= d->olist.ensure(4ull * ocap);
     rc |= d->olist_items.ensure(4ull * ocap);
+    rc |= d->oscratch.ensure(16ull * fcap);
     bool wire = false;
     for (uint32_t i = d->ordered_from; i < nd && !wire; i++)
       wire = (d->draws[i].flags & DF_WIRE) != 0;
@@ -1197,6 +1198,9 @@ static int launch_frame(MopCudaDevice *d) {
     a.olist = d->olist.as<uint32_t>();
     a.olist_items = d->olist_items.as<uint32_t>();
     a.olist_cap = ocap;
+    a.oscratch = d->oscratch.as<ulonglong2>();
+    a.oscratch_count = &d->counters.as<Counters>()->scratch_count;
+    a.oscratch_cap = fcap;
     for (uint32_t i = d->ordered_from; i < nd; i++) {
       if (d->draws[i].flags & DF_NO_DEPTH_TEST)
         a.ordered_keep_all = 1;

@@ -141,11 +141,12 @@ struct Counters {
    * bit5 ordered-record list, bit7 wireframe-record list */
   uint32_t frag_count, touched_count, olist_count, olist_items;
   uint32_t wire_count, wire_items; /* wireframe records queued, their plots */
-  uint32_t pad[2];
+  uint32_t scratch_count;          /* sort-scratch entries taken by long lists */
+  uint32_t pad;
 };
 
 /* Blended fragments of one sample sorted in registers; a sample with more
- * is composited by an in-order selection walk of its list. */
+ * sorts its list in the fold's global scratch (heapsort). */
 #define ORDERED_MAX_FRAGS 48
 
 /* Records whose clamped bbox exceeds these bounds are rasterised as
@@ -231,6 +232,12 @@ struct FrameArgs {
   uint32_t *wlist, *wlist_items;
   uint32_t wlist_cap;
   int wire;
+  /* sort scratch of the fold for lists longer than ORDERED_MAX_FRAGS:
+   * (key, payload) pairs, oscratch_cap entries (at least the fragment pool,
+   * so it cannot run out), taken from *oscratch_count */
+  ulonglong2 *oscratch;
+  uint32_t *oscratch_count;
+  uint32_t oscratch_cap;
   /* shadow map bound for directional lights (the rasteriser's shadow state,
    * rasterizer.c:141-157): shadow_w x shadow_h texel keys (shadow_texel),
    * null when none is bound; shadow_vp: the light's view-projection, 16
@@ -411,11 +418,13 @@ struct DrawBound {
 /* Pool sizes that the allocation pass found too small; the host grows the
  * pools to at least these and re-runs the batch. */
 struct BatchStatus {
-  uint32_t overflow; /* bit0 vertex, bit1 records, bit2 clip queue, bit3 large list,
-                        bit4 ordered-record lists, bit5 fragment pool, bit6 a viewport
-                        with an ordered suffix in a launch without suffix buffers */
-  uint32_t pad;
-  unsigned long long need_vertex, need_rec, need_clip, need_large, need_olist, need_frag;
+  uint32_t overflow; /* pools: bit0 vertex, bit1 records, bit2 clip queue, bit3 large
+                        list, bit4 ordered-record lists, bit5 fragments, bit6 wireframe-
+                        record lists; bit8 a viewport with an ordered suffix or wireframe
+                        draws in a launch without the buffers for them */
+  uint32_t scratch_count; /* the fold's sort scratch, shared by the viewports */
+  unsigned long long need_vertex, need_rec, need_clip, need_large, need_olist, need_frag,
+      need_wlist;
 };
 
 /* Blended draws of one scene a batch viewport sorts back to front. */
@@ -454,6 +463,10 @@ struct BatchArgs {
   unsigned long long frag_pool;
   uint32_t *olist, *olist_items;
   unsigned long long olist_pool;
+  uint32_t *wlist, *wlist_items; /* wireframe-record lists (null: no wireframe draws) */
+  unsigned long long wlist_pool;
+  ulonglong2 *oscratch;          /* the fold's sort scratch, frag_pool entries, shared */
+  uint32_t *oscratch_count;      /* by the launch's viewports through one counter */
   unsigned long long samples; /* samples of the launch (frag_head's length) */
   /* per-viewport reserves: clipped fans (records, extra vertices, clip
    * queue) T * fan_num / 8 + 1024; large list T * large_num / 16 + 1024;

@@ -721,7 +721,7 @@ def deep_transparent_scene(seed: int = 64, width: int = 160, height: int = 120, 
     """small_scene with `layers` blended quads stacked along z in front of
     the camera (alpha, additive, multiply and alpha-promoted opaque, opacity
     0.05-0.7), so the middle samples receive more blended fragments than a
-    sample's sorted register list holds (48): the selection walk composites
+    sample's sorted register list holds (48): the scratch heapsort orders
     them."""
     sc = small_scene(seed=seed, width=width, height=height, ssaa=ssaa)
     rng = np.random.default_rng(seed + 200)

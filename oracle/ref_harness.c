@@ -150,6 +150,22 @@ void *refh_create(const RefScene *sc) {
     uint8_t *zero = calloc((size_t)sc->width * sc->height, 4);
     if (h->tex_vp && zero)
       h->target = mop_viewport_create_texture(h->tex_vp, sc->width, sc->height, zero);
+    /* The CPU backend's cpu_texture_create (cpu_backend.c:811) mallocs its
+     * texture record without setting is_hdr / hdr_data, and
+     * framebuffer_create_from_texture refuses a target whose is_hdr reads
+     * true (:156), so whether a render target works depends on what the
+     * allocator hands back.  The harness sets the two fields the reference
+     * leaves unset, through the record's layout (cpu_backend.c:43-49). */
+    if (cpu && h->target && h->target->rhi_texture) {
+      struct CpuTexRecord {
+        int width, height;
+        uint8_t *data;
+        float *hdr_data;
+        bool is_hdr;
+      } *rec = (struct CpuTexRecord *)(void *)h->target->rhi_texture;
+      rec->hdr_data = NULL;
+      rec->is_hdr = false;
+    }
     free(zero);
     if (!h->target) {
       if (h->tex_vp)

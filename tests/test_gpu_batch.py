@@ -178,6 +178,33 @@ def test_batch_blended_shadow_and_unlit(cuda_device, ibl):
         b.close()
 
 
+def test_batch_wireframe_equals_single_viewport_frames(cuda_device, ibl):
+    """MOP_RENDER_WIREFRAME in a batch (with blended instances, and with the
+    sun casting shadows): every viewport's line plots composite in its own
+    suffix as in its plain frame; and against the oracle directly."""
+    sc = dataclasses.replace(_blended(_scene(instances=10)), wireframe=True)
+    b = mopcuda.BatchRenderer(cuda_device, sc, _views(sc, 5, seed=25), ibl)
+    try:
+        b.render()
+        _check_batch(cuda_device, b, sc, ibl, "wireframe batch")
+    finally:
+        b.close()
+    small = dataclasses.replace(scenes.wireframe_scene(seed=26, width=96, height=72),
+                                lights=[])
+    views = [scenes.View(96, 72, 1, small.eye, small.target, fov_deg=small.fov_deg,
+                         near=small.near, far=small.far, clear=small.clear),
+             scenes.View(64, 48, 2, (-4.0, 3.0, 5.0), (0.0, 0.4, 0.0), fov_deg=55.0, near=0.1,
+                         far=50.0, clear=small.clear)]
+    b = mopcuda.BatchRenderer(cuda_device, small, views)
+    try:
+        b.render()
+        for i, v in enumerate(views):
+            ref = cpu_oracle.render(scenes.scene_for_view(small, v), None)
+            assert_frame_parity(_batch_view(b, i), ref, f"wireframe oracle view {i}")
+    finally:
+        b.close()
+
+
 def test_batch_blended_matches_oracle(cuda_device):
     """Blended meshes in a batch against the oracle directly (two cameras,
     different back-to-front orders)."""

@@ -72,7 +72,7 @@ CASES = {
     "transparent": lambda: scenes.transparent_scene(seed=21),
     "transparent_ssaa2_ibl": lambda: scenes.transparent_scene(seed=22, ssaa=2, env=1),
     "transparent_config2": lambda: _transparent_config2(),
-    # 64 stacked blended quads: samples with more than 48 fragments (selection walk)
+    # 64 stacked blended quads: samples with more than 48 fragments (scratch heapsort)
     "transparent_deep": lambda: scenes.deep_transparent_scene(seed=65),
     "transparent_deep_ssaa2": lambda: scenes.deep_transparent_scene(seed=66, ssaa=2,
                                                                     layers=80),
