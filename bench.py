@@ -277,8 +277,8 @@ def run_cuda(args):
     warm = max(3, args.warmup)
     steps = max(1, args.steps)
 
-    # ---- device-timed frames ----
-    dev.set_stage_timing(True)
+    # ---- device-timed frames (no stage events inside the timed frames) ----
+    dev.set_stage_timing(False)
     for _ in range(warm):
         r.render()
     ids = r.object_id()
@@ -286,18 +286,25 @@ def run_cuda(args):
     barrier()
     sampler = ClockSampler(local)
     sampler.start()
-    frame_ms, stage = [], {k: 0.0 for k in mopcuda.Device.STAGES}
+    frame_ms = []
     l0 = dev.launches
     for _ in range(steps):
         flush.add_(1.0)  # rewrite > L2 (126 MB) between frames
         torch.cuda.synchronize()
         r.render()
         frame_ms.append(r.gpu_ms)
-        for k, v in dev.stage_times().items():
-            stage[k] += v
     launches = dev.launches - l0
     barrier()
     clocks = sampler.stop()
+    # ---- per-stage times: the same frames again with events between the stages ----
+    dev.set_stage_timing(True)
+    stage = {k: 0.0 for k in mopcuda.Device.STAGES}
+    for _ in range(steps):
+        flush.add_(1.0)
+        torch.cuda.synchronize()
+        r.render()
+        for k, v in dev.stage_times().items():
+            stage[k] += v
     total_ms, value, mtri = aggregate(sum(frame_ms), steps, world, sc.pixels,
                                       sc.triangle_count, dist, "cuda")
 

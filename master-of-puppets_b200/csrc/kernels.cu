@@ -24,6 +24,31 @@
  */
 #include "mopcuda_internal.cuh"
 
+/* Programmatic dependent launch.  The frame's kernels from the vertex pass
+ * to the post pass are launched with programmatic stream serialisation: a
+ * kernel may be scheduled while its predecessor drains, and its first
+ * statement, pdl_wait(), holds every thread until the predecessor has
+ * completed and its writes are visible (griddepcontrol.wait).  A kernel
+ * launched without the attribute passes pdl_wait() at once, so the kernels
+ * stay correct wherever they are launched from.  No kernel triggers early:
+ * a successor starts once all of its predecessor's blocks have exited. */
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
+template <typename Arg>
+static void pdl(void (*k)(Arg), dim3 grid, dim3 block, cudaStream_t s, Arg arg) {
+  cudaLaunchConfig_t c = {};
+  c.gridDim = grid;
+  c.blockDim = block;
+  c.dynamicSmemBytes = 0;
+  c.stream = s;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  c.attrs = at;
+  c.numAttrs = 1;
+  cudaLaunchKernelEx(&c, k, arg);
+}
+
 #define PI_F 3.14159274f /* (float)M_PI */
 
 /* (uint8_t) of a value already clamped to [0, 255.5] (or NaN): plain
@@ -155,6 +180,7 @@ __device__ __forceinline__ void vertex_item(const FrameArgs &a, uint32_t g) {
 }
 
 __global__ void k_vertex(FrameArgs a) {
+  pdl_wait();
   const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
   if (g < a.total_vertices)
     vertex_item(a, g);
@@ -826,6 +852,7 @@ __device__ __forceinline__ void setup_item(const FrameArgs &a, uint32_t t) {
  * and more resident warps hide them. */
 template <bool SH>
 __global__ void __launch_bounds__(256, 5) k_setup(FrameArgs a) {
+  pdl_wait();
   const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t < a.total_tris)
     setup_item<SH>(a, t);
@@ -948,6 +975,7 @@ __device__ __forceinline__ void clip_item(const FrameArgs &a, uint32_t qi) {
 
 template <bool SH>
 __global__ void k_clip(FrameArgs a) {
+  pdl_wait();
   const uint32_t n_q = clip_items(a);
   for (uint32_t qi = blockIdx.x * blockDim.x + threadIdx.x; qi < n_q;
        qi += gridDim.x * blockDim.x)
@@ -1014,6 +1042,7 @@ __device__ __forceinline__ void raster_small_item(const FrameArgs &a, uint32_t r
 }
 
 __global__ void k_raster_small(FrameArgs a) {
+  pdl_wait();
   const uint32_t n = raster_small_items(a);
   for (uint32_t rid = blockIdx.x * blockDim.x + threadIdx.x; rid < n;
        rid += gridDim.x * blockDim.x)
@@ -1091,6 +1120,7 @@ __device__ __forceinline__ void large_scan_block(const FrameArgs &a, uint32_t *p
 }
 
 __global__ void __launch_bounds__(1024) k_large_scan(FrameArgs a) {
+  pdl_wait();
   __shared__ uint32_t part[1024];
   large_scan_block(a, part);
 }
@@ -1134,6 +1164,7 @@ __device__ __forceinline__ void raster_large_item(const FrameArgs &a, uint32_t i
 }
 
 __global__ void k_raster_large(FrameArgs a) {
+  pdl_wait();
   const uint32_t total = a.ctr->large_items;
   for (uint32_t it = blockIdx.x * blockDim.x + threadIdx.x; it < total;
        it += gridDim.x * blockDim.x)
@@ -1313,6 +1344,7 @@ __device__ __forceinline__ void resolve_chunk(const FrameArgs &a, uint32_t blk, 
 /* The next chunk's keys are loaded before this chunk's barriers and
  * compaction atomic, so they are in flight while the block waits. */
 __global__ void __launch_bounds__(256) k_resolve(FrameArgs a) {
+  pdl_wait();
   __shared__ uint32_t s_warp[8];
   __shared__ uint32_t s_base;
   const uint32_t S = (uint32_t)a.width * (uint32_t)a.height;
@@ -1466,6 +1498,7 @@ __device__ __forceinline__ void shade_item(const FrameArgs &a, uint32_t j, const
  * extra warps hide the dependent-latency stalls of the lighting chains. */
 template <bool SH>
 __global__ void __launch_bounds__(256, 4) k_shade(FrameArgs a) {
+  pdl_wait();
   __shared__ LightRec s_lights[SHADE_SMEM_LIGHTS];
   const LightRec *lights = stage_lights(a, s_lights);
   const uint32_t n = a.ctr->shade_count;
@@ -1726,6 +1759,7 @@ __device__ __forceinline__ void post_pixel(const PostArgs &a, const uchar4 (*s_c
  * blockIdx.x + gridDim.x, ... in row-major tile order. */
 template <int SF>
 __global__ void __launch_bounds__(POST_BX *POST_BY) k_post(PostArgs a) {
+  pdl_wait();
   __shared__ PostSmem<SF> sm;
   post_load_luts<SF>(a, sm);
   const uint32_t tx = ((uint32_t)(a.width / SF) + POST_BX - 1u) / POST_BX;
@@ -1852,8 +1886,11 @@ int mopcuda_launch_frame(const FrameArgs &a, const PostArgs &p, const LaunchCfg 
   const uint32_t S = (uint32_t)a.width * (uint32_t)a.height;
   if (ev)
     cudaEventRecord(ev[0], s);
+  /* the key clear first, so the kernels from here to the post pass follow
+   * one another with programmatic dependent launches (pdl) */
+  cudaMemsetAsync(a.keys, 0xff, sizeof(unsigned long long) * (size_t)S, s);
   if (a.total_vertices) {
-    k_vertex<<<blocks_for(a.total_vertices, 256), 256, 0, s>>>(a);
+    pdl(k_vertex, blocks_for(a.total_vertices, 256), 256, s, a);
     launches++;
   }
   if (ev)
@@ -1861,58 +1898,57 @@ int mopcuda_launch_frame(const FrameArgs &a, const PostArgs &p, const LaunchCfg 
   if (a.total_tris) {
     const unsigned cg = blocks_for(a.clip_cap < 65536u ? a.clip_cap : 65536u, 128);
     if (a.shadow_keys) {
-      k_setup<true><<<blocks_for(a.total_tris, 256), 256, 0, s>>>(a);
-      k_clip<true><<<cg, 128, 0, s>>>(a);
+      pdl(k_setup<true>, blocks_for(a.total_tris, 256), 256, s, a);
+      pdl(k_clip<true>, cg, 128, s, a);
     } else {
-      k_setup<false><<<blocks_for(a.total_tris, 256), 256, 0, s>>>(a);
-      k_clip<false><<<cg, 128, 0, s>>>(a);
+      pdl(k_setup<false>, blocks_for(a.total_tris, 256), 256, s, a);
+      pdl(k_clip<false>, cg, 128, s, a);
     }
     launches += 2;
   }
   if (ev)
     cudaEventRecord(ev[2], s);
-  cudaMemsetAsync(a.keys, 0xff, sizeof(unsigned long long) * (size_t)S, s);
   if (a.total_tris) {
     const int rb = cfg.raster_block > 0 ? cfg.raster_block : 128;
     const uint32_t rec_grid = blocks_for(a.rec_cap < (1u << 22) ? a.rec_cap : (1u << 22),
                                          (unsigned)rb);
-    k_raster_small<<<rec_grid, rb, 0, s>>>(a);
-    k_large_scan<<<1, 1024, 0, s>>>(a);
-    k_raster_large<<<cfg.num_sms * 8, 256, 0, s>>>(a);
+    pdl(k_raster_small, rec_grid, rb, s, a);
+    pdl(k_large_scan, 1, 1024, s, a);
+    pdl(k_raster_large, cfg.num_sms * 8, 256, s, a);
     launches += 3;
   }
   if (ev)
     cudaEventRecord(ev[3], s);
-  k_resolve<<<cfg.num_sms * 8, 256, 0, s>>>(a);
+  pdl(k_resolve, cfg.num_sms * 8, 256, s, a);
   if (ev)
     cudaEventRecord(ev[4], s);
   const int sb = cfg.shade_block > 0 ? cfg.shade_block : 256;
   const int waves = cfg.shade_waves > 0 ? cfg.shade_waves : 4;
   if (a.shadow_keys)
-    k_shade<true><<<cfg.num_sms * waves, sb, 0, s>>>(a);
+    pdl(k_shade<true>, cfg.num_sms * waves, sb, s, a);
   else
-    k_shade<false><<<cfg.num_sms * waves, sb, 0, s>>>(a);
+    pdl(k_shade<false>, cfg.num_sms * waves, sb, s, a);
   launches += 2;
   if (a.hdr) { /* blended suffix, composited in submission order */
     cudaMemsetAsync(a.frag_head, 0xff, sizeof(uint32_t) * (size_t)S, s);
     const uint32_t nrec = a.rec_cap < (1u << 22) ? a.rec_cap : (1u << 22);
-    k_ocount<<<blocks_for(nrec, 256), 256, 0, s>>>(a);
-    k_oscan<<<1, 1024, 0, s>>>(a);
-    k_oraster<<<cfg.num_sms * 8, 256, 0, s>>>(a);
+    pdl(k_ocount, blocks_for(nrec, 256), 256, s, a);
+    pdl(k_oscan, 1, 1024, s, a);
+    pdl(k_oraster, cfg.num_sms * 8, 256, s, a);
     launches += 3;
     if (a.wire) { /* wireframe draws: their line plots join the fragment lists */
-      k_wcount<<<blocks_for(nrec, 256), 256, 0, s>>>(a);
-      k_wscan<<<1, 1024, 0, s>>>(a);
-      k_wplot<<<cfg.num_sms * 8, 256, 0, s>>>(a);
+      pdl(k_wcount, blocks_for(nrec, 256), 256, s, a);
+      pdl(k_wscan, 1, 1024, s, a);
+      pdl(k_wplot, cfg.num_sms * 8, 256, s, a);
       launches += 3;
       if (a.shadow_keys)
-        k_ofold<true, true><<<cfg.num_sms * 8, 128, 0, s>>>(a);
+        pdl(k_ofold<true, true>, cfg.num_sms * 8, 128, s, a);
       else
-        k_ofold<false, true><<<cfg.num_sms * 8, 128, 0, s>>>(a);
+        pdl(k_ofold<false, true>, cfg.num_sms * 8, 128, s, a);
     } else if (a.shadow_keys) {
-      k_ofold<true, false><<<cfg.num_sms * 8, 128, 0, s>>>(a);
+      pdl(k_ofold<true, false>, cfg.num_sms * 8, 128, s, a);
     } else {
-      k_ofold<false, false><<<cfg.num_sms * 8, 128, 0, s>>>(a);
+      pdl(k_ofold<false, false>, cfg.num_sms * 8, 128, s, a);
     }
     launches += 1;
   }
@@ -1932,16 +1968,16 @@ int mopcuda_launch_frame(const FrameArgs &a, const PostArgs &p, const LaunchCfg 
   };
   switch (sf) {
   case 2:
-    k_post<2><<<pgrid(post_resident<2>()), pb, 0, s>>>(p);
+    pdl(k_post<2>, pgrid(post_resident<2>()), pb, s, p);
     break;
   case 3:
-    k_post<3><<<pgrid(post_resident<3>()), pb, 0, s>>>(p);
+    pdl(k_post<3>, pgrid(post_resident<3>()), pb, s, p);
     break;
   case 4:
-    k_post<4><<<pgrid(post_resident<4>()), pb, 0, s>>>(p);
+    pdl(k_post<4>, pgrid(post_resident<4>()), pb, s, p);
     break;
   default:
-    k_post<1><<<pgrid(post_resident<1>()), pb, 0, s>>>(p);
+    pdl(k_post<1>, pgrid(post_resident<1>()), pb, s, p);
     break;
   }
   launches++;
@@ -2031,6 +2067,7 @@ __device__ __forceinline__ void ocount_item(const FrameArgs &a, uint32_t rid) {
 }
 
 __global__ void __launch_bounds__(256) k_ocount(FrameArgs a) {
+  pdl_wait();
   const uint32_t n = ordered_record_items(a);
   for (uint32_t rid = blockIdx.x * blockDim.x + threadIdx.x; rid < n;
        rid += gridDim.x * blockDim.x)
@@ -2038,6 +2075,7 @@ __global__ void __launch_bounds__(256) k_ocount(FrameArgs a) {
 }
 
 __global__ void __launch_bounds__(1024) k_oscan(FrameArgs a) {
+  pdl_wait();
   __shared__ uint32_t part[32];
   uint32_t n = a.ctr->olist_count;
   if (n > a.olist_cap)
@@ -2116,6 +2154,7 @@ __device__ __forceinline__ uint32_t olist_len(const FrameArgs &a) {
 }
 
 __global__ void __launch_bounds__(256) k_oraster(FrameArgs a) {
+  pdl_wait();
   const uint32_t nl = olist_len(a);
   const uint32_t total = a.ctr->olist_items;
   for (uint32_t it = blockIdx.x * blockDim.x + threadIdx.x; it < total;
@@ -2299,6 +2338,7 @@ __device__ __forceinline__ void wcount_item(const FrameArgs &a, uint32_t rid) {
 }
 
 __global__ void __launch_bounds__(256) k_wcount(FrameArgs a) {
+  pdl_wait();
   const uint32_t n = ordered_record_items(a);
   for (uint32_t rid = blockIdx.x * blockDim.x + threadIdx.x; rid < n;
        rid += gridDim.x * blockDim.x)
@@ -2306,6 +2346,7 @@ __global__ void __launch_bounds__(256) k_wcount(FrameArgs a) {
 }
 
 __global__ void __launch_bounds__(1024) k_wscan(FrameArgs a) {
+  pdl_wait();
   __shared__ uint32_t part[32];
   uint32_t n = a.ctr->wire_count;
   if (n > a.wlist_cap)
@@ -2334,6 +2375,7 @@ __device__ __forceinline__ void wplot_item(const FrameArgs &a, uint32_t it) {
 }
 
 __global__ void __launch_bounds__(256) k_wplot(FrameArgs a) {
+  pdl_wait();
   const uint32_t total = a.ctr->wire_items;
   for (uint32_t it = blockIdx.x * blockDim.x + threadIdx.x; it < total;
        it += gridDim.x * blockDim.x)
@@ -2656,6 +2698,7 @@ __device__ __forceinline__ void ofold_item(const FrameArgs &a, uint32_t i) {
 
 template <bool SH, bool WIRE>
 __global__ void __launch_bounds__(128) k_ofold(FrameArgs a) {
+  pdl_wait();
   const uint32_t n = a.ctr->touched_count;
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
     ofold_item<SH, WIRE>(a, i);
