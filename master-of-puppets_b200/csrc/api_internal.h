@@ -198,8 +198,13 @@ struct MopCudaDevice {
   float ibl_rot = 0.0f, ibl_int = 1.0f;
   bool ibl_on = false;
   /* frame arenas */
-  DevArena d_draws, d_lights, clip, world, normal, color, rrec, srec, clipq, keys,
+  DevArena d_draws, d_lights, clip, world, normal, color, rrec, srec, clipq,
       large_list, large_items, shade_list, counters, pick_xy, pick_out;
+  /* visibility keys: two buffers in turn, a frame's shading pass clearing the
+   * one the next frame uses; keys_clean[i] = samples of buffer i known clear */
+  DevArena keys[2];
+  int keys_cur = 0;
+  size_t keys_clean[2] = {0, 0};
   HostArena h_draws, h_lights, h_counters, h_pick;
   DevArena deform_params; /* bone matrices / morph weights of a deform call */
   DevArena hdr, frag_head, frags, touched, olist, olist_items; /* blended suffix */

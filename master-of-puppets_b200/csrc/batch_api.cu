@@ -837,6 +837,9 @@ int LaunchCore::after(bool *rerun, int attempt) {
     view_over |= ctr[i].overflow;
   if (!st->overflow && !view_over)
     return MOPCUDA_OK;
+  if (view_over & 512u)
+    return fail(MOPCUDA_EUNSUPPORTED,
+                "launch: a viewport's large-triangle raster items exceed 2^32");
   if (attempt >= 8)
     return fail(MOPCUDA_ENOMEM, "launch pools overflowed repeatedly (flags %u/%u)", st->overflow,
                 view_over);

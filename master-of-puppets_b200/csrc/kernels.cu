@@ -766,11 +766,20 @@ __device__ __forceinline__ uint32_t rec_items(const RasterRec &r) {
 }
 
 /* Queue a large record for item-parallel rasterisation. */
+/* Queues a large record: one 64-bit atomic takes its list slot (high word)
+ * and the offset of its first item (low word) together, so the offsets come
+ * out ascending with the slot and no scan pass is needed.  An item total
+ * past 2^32 carries into the slot count: flagged (bit 9), the frame fails. */
 __device__ __forceinline__ void push_large(const FrameArgs &a, uint32_t rid, const RasterRec &r) {
-  uint32_t q = atomicAdd(&a.ctr->large_count, 1u);
+  const uint32_t n = rec_items(r);
+  const unsigned long long old = atomicAdd(
+      reinterpret_cast<unsigned long long *>(&a.ctr->large_items), (1ull << 32) | n);
+  const uint32_t q = (uint32_t)(old >> 32), off = (uint32_t)old;
+  if (off + n < off)
+    atomicOr(&a.ctr->overflow, 512u);
   if (q < a.large_cap) {
     a.large_list[q] = rid;
-    a.large_items[q] = rec_items(r);
+    a.large_items[q] = off;
   } else {
     atomicOr(&a.ctr->overflow, 8u);
   }
@@ -1049,7 +1058,8 @@ __global__ void k_raster_small(FrameArgs a) {
     raster_small_item(a, rid);
 }
 
-/* Exclusive scan of the large records' item counts by one block of 1024:
+/* Exclusive scan of a record list's item counts (the ordered, wireframe and
+ * shadow lists) by one block of 1024:
  * tiles of 4096 counts (4 consecutive per thread), warp-shuffle scans, the
  * next tile's counts loaded before the current one is scanned; part holds
  * >= 32 words. */
@@ -1110,19 +1120,6 @@ __device__ __forceinline__ void items_scan_block(T *items, uint32_t n, T *total_
   }
   if (tid == 0)
     *total_out = carry;
-}
-
-__device__ __forceinline__ void large_scan_block(const FrameArgs &a, uint32_t *part) {
-  uint32_t n = a.ctr->large_count;
-  if (n > a.large_cap)
-    n = a.large_cap;
-  items_scan_block(a.large_items, n, &a.ctr->large_items, part);
-}
-
-__global__ void __launch_bounds__(1024) k_large_scan(FrameArgs a) {
-  pdl_wait();
-  __shared__ uint32_t part[1024];
-  large_scan_block(a, part);
 }
 
 /* Large records: one thread per (row, RASTER_CHUNK-sample chunk); the edge
@@ -1496,14 +1493,36 @@ __device__ __forceinline__ void shade_item(const FrameArgs &a, uint32_t j, const
 
 /* 4 blocks of 256 per SM (64 registers): the kernel is issue-bound and the
  * extra warps hide the dependent-latency stalls of the lighting chains. */
+/* With keys_next set, the kernel also clears the next frame's key buffer
+ * (keys alternate between two buffers): 16-byte stores g + m * step (g the
+ * thread's index, step the grid's threads), two per shaded sample and the
+ * rest after the last one, so the writes spread over a kernel whose time is
+ * arithmetic, and no frame waits for a clear of its own. */
 template <bool SH>
 __global__ void __launch_bounds__(256, 4) k_shade(FrameArgs a) {
   pdl_wait();
   __shared__ LightRec s_lights[SHADE_SMEM_LIGHTS];
   const LightRec *lights = stage_lights(a, s_lights);
   const uint32_t n = a.ctr->shade_count;
-  for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x)
+  const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x, step = gridDim.x * blockDim.x;
+  const size_t S = (size_t)a.width * (size_t)a.height;
+  const uint32_t nk = a.keys_next ? (uint32_t)(S >> 1) : 0u;
+  uint4 *kn = reinterpret_cast<uint4 *>(a.keys_next);
+  const uint4 ones = make_uint4(~0u, ~0u, ~0u, ~0u);
+  uint32_t j = g;
+  for (; j < n; j += step) {
+    const uint32_t c = 2u * j - g; /* = g + 2 * iteration * step */
+    if (c < nk) {
+      kn[c] = ones;
+      if (c + step < nk)
+        kn[c + step] = ones;
+    }
     shade_item<SH>(a, j, lights);
+  }
+  for (uint32_t c = 2u * j - g; c < nk; c += step)
+    kn[c] = ones;
+  if (nk && (S & 1u) && g == 0u)
+    a.keys_next[S - 1u] = ~0ull;
 }
 
 /* ------------------------------------------------------------------------
@@ -1568,14 +1587,107 @@ __device__ __forceinline__ uchar4 fxaa_tile(const uchar4 (*tc)[TW], const float 
   return o;
 }
 
+/* The sample tile of one block: rows -1 .. POST_BY*SF of the block's pixels'
+ * samples and columns -OX .. POST_BX*SF+OX-1, so that each row is whole
+ * 16-byte chunks of the image; NBUF colour tiles, the next one filling by
+ * asynchronous copies while the current one is filtered. */
 template <int SF> struct PostSmem {
-  static constexpr int TW = POST_BX * SF + 2, TH = POST_BY * SF + 2;
-  uchar4 c[TH][TW];
+  static constexpr int OX = 4; /* tile column of the block's first own sample */
+  static constexpr int TW = POST_BX * SF + 2 * OX, TH = POST_BY * SF + 2;
+  static constexpr int NBUF = SF <= 3 ? 2 : 1; /* within 48 KB of static shared memory */
+  alignas(16) uchar4 c[NBUF][TH][TW];
   float l[TH][TW];
   float lut[256];
   uint8_t lut8[256];
   float thr[256]; /* gamma byte thresholds (FOG bit only); thr[255] = +inf */
 };
+
+__device__ __forceinline__ void cp_async4(void *smem, const void *gmem) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(
+                   (uint32_t)__cvta_generic_to_shared(smem)),
+               "l"(gmem)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(
+                   (uint32_t)__cvta_generic_to_shared(smem)),
+               "l"(gmem)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+  asm volatile("cp.async.commit_group;" ::: "memory");
+}
+template <int N> __device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+/* Samples of the tile that lie off the image are neither copied nor read:
+ * FXAA reads the neighbours of samples at least one away from every edge,
+ * and every presented pixel's samples are on the image. */
+__device__ __forceinline__ bool post_vec(const PostArgs &a) {
+  return (a.width & 3) == 0 && ((uintptr_t)a.pre & 15u) == 0u;
+}
+
+/* Issues this thread's copies of tile (bx, by) into colour buffer c (one
+ * commit group).  With 16-byte rows (post_vec) a copy moves 4 samples. */
+template <int SF>
+__device__ __forceinline__ void post_fetch(const PostArgs &a, bool vec,
+                                           uchar4 (*c)[PostSmem<SF>::TW], int bx, int by) {
+  constexpr int TW = PostSmem<SF>::TW, TH = PostSmem<SF>::TH, OX = PostSmem<SF>::OX;
+  const int tid = threadIdx.y * POST_BX + threadIdx.x;
+  const int w = a.width, h = a.height;
+  const int sx0 = bx * POST_BX * SF - OX, sy0 = by * POST_BY * SF - 1;
+  if (vec) {
+    for (int i = tid; i < (TW / 4) * TH; i += POST_BX * POST_BY) {
+      const int ty = i / (TW / 4), tx = 4 * (i % (TW / 4));
+      const int sy = sy0 + ty, sx = sx0 + tx;
+      if (sy >= 0 && sy < h && sx >= 0 && sx < w)
+        cp_async16(&c[ty][tx], a.pre + (size_t)sy * w + sx);
+    }
+  } else {
+    for (int i = tid; i < TW * TH; i += POST_BX * POST_BY) {
+      const int ty = i / TW, tx = i % TW;
+      const int sy = sy0 + ty, sx = sx0 + tx;
+      if (sy >= 0 && sy < h && sx >= 0 && sx < w)
+        cp_async4(&c[ty][tx], a.pre + (size_t)sy * w + sx);
+    }
+  }
+  cp_async_commit();
+}
+
+/* The luma of the samples this thread copied (its own copies are visible
+ * to it once waited for). */
+template <int SF>
+__device__ __forceinline__ void post_luma(const PostArgs &a, bool vec,
+                                          const uchar4 (*c)[PostSmem<SF>::TW],
+                                          float (*l)[PostSmem<SF>::TW], int bx, int by) {
+  constexpr int TW = PostSmem<SF>::TW, TH = PostSmem<SF>::TH, OX = PostSmem<SF>::OX;
+  const int tid = threadIdx.y * POST_BX + threadIdx.x;
+  const int w = a.width, h = a.height;
+  const int sx0 = bx * POST_BX * SF - OX, sy0 = by * POST_BY * SF - 1;
+  if (vec) {
+    for (int i = tid; i < (TW / 4) * TH; i += POST_BX * POST_BY) {
+      const int ty = i / (TW / 4), tx = 4 * (i % (TW / 4));
+      const int sy = sy0 + ty, sx = sx0 + tx;
+      if (sy >= 0 && sy < h && sx >= 0 && sx < w) {
+        const uint4 q = *reinterpret_cast<const uint4 *>(&c[ty][tx]);
+        float4 o;
+        o.x = luma(*reinterpret_cast<const uchar4 *>(&q.x));
+        o.y = luma(*reinterpret_cast<const uchar4 *>(&q.y));
+        o.z = luma(*reinterpret_cast<const uchar4 *>(&q.z));
+        o.w = luma(*reinterpret_cast<const uchar4 *>(&q.w));
+        *reinterpret_cast<float4 *>(&l[ty][tx]) = o;
+      }
+    }
+  } else {
+    for (int i = tid; i < TW * TH; i += POST_BX * POST_BY) {
+      const int ty = i / TW, tx = i % TW;
+      const int sy = sy0 + ty, sx = sx0 + tx;
+      if (sy >= 0 && sy < h && sx >= 0 && sx < w)
+        l[ty][tx] = luma(c[ty][tx]);
+    }
+  }
+}
 
 template <int SF>
 __device__ __forceinline__ void post_load_luts(const PostArgs &a, PostSmem<SF> &sm) {
@@ -1655,33 +1767,32 @@ __device__ __forceinline__ void post_pixel(const PostArgs &a, const uchar4 (*s_c
                                            const uint8_t *s_lut8, const float *s_thr, int px,
                                            int py);
 
-/* One tile of POST_BX x POST_BY presented pixels (bx, by): FXAA, the
- * tonemap/gamma map and the SSAA box.  Block-uniform; ends with a barrier so
- * the caller may reuse the shared tile. */
+/* Filters tile (bx, by) from colour buffer `buf` once its copies have
+ * landed: this thread's lumas, a barrier, then each thread's pixel (FXAA,
+ * the tonemap/gamma map and the SSAA box).  Block-uniform; ends with a
+ * barrier so the caller may refill the buffers. */
 template <int SF>
-__device__ __forceinline__ void post_tile(const PostArgs &a, PostSmem<SF> &sm, int bx, int by) {
-  constexpr int TW = PostSmem<SF>::TW, TH = PostSmem<SF>::TH;
-  auto &s_c = sm.c;
-  auto &s_l = sm.l;
-  const float *s_lut = sm.lut;
-  const uint8_t *s_lut8 = sm.lut8;
-  const int tid = threadIdx.y * POST_BX + threadIdx.x;
-  const int w = a.width, h = a.height;
-  const int sx0 = bx * POST_BX * SF - 1, sy0 = by * POST_BY * SF - 1;
-  for (int i = tid; i < TW * TH; i += POST_BX * POST_BY) {
-    const int ty = i / TW, tx = i % TW;
-    const int sy = min(max(sy0 + ty, 0), h - 1), sx = min(max(sx0 + tx, 0), w - 1);
-    const uchar4 c = a.pre[(size_t)sy * w + sx];
-    s_c[ty][tx] = c;
-    s_l[ty][tx] = luma(c);
-  }
+__device__ __forceinline__ void post_filter(const PostArgs &a, bool vec, PostSmem<SF> &sm, int buf,
+                                            int bx, int by) {
+  constexpr int TW = PostSmem<SF>::TW;
+  post_luma<SF>(a, vec, sm.c[buf], sm.l, bx, by);
   __syncthreads();
-  const int pw = w / SF, ph = h / SF;
+  const int pw = a.width / SF, ph = a.height / SF;
   const int px = bx * POST_BX + (int)threadIdx.x;
   const int py = by * POST_BY + (int)threadIdx.y;
   if (px < pw && py < ph)
-    post_pixel<SF, TW>(a, s_c, s_l, s_lut, s_lut8, sm.thr, px, py);
+    post_pixel<SF, TW>(a, sm.c[buf], sm.l, sm.lut, sm.lut8, sm.thr, px, py);
   __syncthreads();
+}
+
+/* One tile of POST_BX x POST_BY presented pixels (bx, by), copied and
+ * filtered with nothing in flight around it. */
+template <int SF>
+__device__ __forceinline__ void post_tile(const PostArgs &a, PostSmem<SF> &sm, int bx, int by) {
+  const bool vec = post_vec(a);
+  post_fetch<SF>(a, vec, sm.c[0], bx, by);
+  cp_async_wait<0>();
+  post_filter<SF>(a, vec, sm, 0, bx, by);
 }
 
 template <int SF, int TW>
@@ -1697,7 +1808,8 @@ __device__ __forceinline__ void post_pixel(const PostArgs &a, const uchar4 (*s_c
 #pragma unroll
     for (int dx = 0; dx < SF; dx++) {
       const int x = px * SF + dx, y = py * SF + dy;
-      const int ti = (int)threadIdx.y * SF + dy + 1, tj = (int)threadIdx.x * SF + dx + 1;
+      const int ti = (int)threadIdx.y * SF + dy + 1,
+                tj = (int)threadIdx.x * SF + dx + PostSmem<SF>::OX;
       uchar4 c = s_c[ti][tj];
       if (fx && x >= 1 && y >= 1 && x < w - 1 && y < h - 1)
         c = fxaa_tile<TW>(s_c, s_l, ti, tj);
@@ -1756,16 +1868,37 @@ __device__ __forceinline__ void post_pixel(const PostArgs &a, const uchar4 (*s_c
 }
 
 /* Persistent: each block loads the tables once and takes tiles blockIdx.x,
- * blockIdx.x + gridDim.x, ... in row-major tile order. */
+ * blockIdx.x + gridDim.x, ... in row-major tile order; with two colour
+ * buffers the copies of the next tile are in flight while the current one
+ * is filtered. */
 template <int SF>
 __global__ void __launch_bounds__(POST_BX *POST_BY) k_post(PostArgs a) {
   pdl_wait();
   __shared__ PostSmem<SF> sm;
   post_load_luts<SF>(a, sm);
+  const bool vec = post_vec(a);
   const uint32_t tx = ((uint32_t)(a.width / SF) + POST_BX - 1u) / POST_BX;
   const uint32_t ty = ((uint32_t)(a.height / SF) + POST_BY - 1u) / POST_BY;
-  for (uint32_t t = blockIdx.x; t < tx * ty; t += gridDim.x)
-    post_tile<SF>(a, sm, (int)(t % tx), (int)(t / tx));
+  const uint32_t nt = tx * ty;
+  if (PostSmem<SF>::NBUF == 1) {
+    for (uint32_t t = blockIdx.x; t < nt; t += gridDim.x)
+      post_tile<SF>(a, sm, (int)(t % tx), (int)(t / tx));
+    return;
+  }
+  uint32_t t = blockIdx.x;
+  if (t < nt)
+    post_fetch<SF>(a, vec, sm.c[0], (int)(t % tx), (int)(t / tx));
+  for (int buf = 0; t < nt; t += gridDim.x, buf ^= 1) {
+    const uint32_t tn = t + gridDim.x;
+    if (tn < nt) { /* the other buffer was released by the last filter's barrier */
+      post_fetch<SF>(a, vec, sm.c[buf ^ (PostSmem<SF>::NBUF - 1)], (int)(tn % tx),
+                     (int)(tn / tx));
+      cp_async_wait<1>();
+    } else {
+      cp_async_wait<0>();
+    }
+    post_filter<SF>(a, vec, sm, buf & (PostSmem<SF>::NBUF - 1), (int)(t % tx), (int)(t / tx));
+  }
 }
 
 /* Blocks of k_post<SF> resident on one SM (queried once per factor). */
@@ -1886,9 +2019,8 @@ int mopcuda_launch_frame(const FrameArgs &a, const PostArgs &p, const LaunchCfg 
   const uint32_t S = (uint32_t)a.width * (uint32_t)a.height;
   if (ev)
     cudaEventRecord(ev[0], s);
-  /* the key clear first, so the kernels from here to the post pass follow
-   * one another with programmatic dependent launches (pdl) */
-  cudaMemsetAsync(a.keys, 0xff, sizeof(unsigned long long) * (size_t)S, s);
+  /* the kernels from here to the post pass follow one another with
+   * programmatic dependent launches (pdl) */
   if (a.total_vertices) {
     pdl(k_vertex, blocks_for(a.total_vertices, 256), 256, s, a);
     launches++;
@@ -1913,9 +2045,8 @@ int mopcuda_launch_frame(const FrameArgs &a, const PostArgs &p, const LaunchCfg 
     const uint32_t rec_grid = blocks_for(a.rec_cap < (1u << 22) ? a.rec_cap : (1u << 22),
                                          (unsigned)rb);
     pdl(k_raster_small, rec_grid, rb, s, a);
-    pdl(k_large_scan, 1, 1024, s, a);
     pdl(k_raster_large, cfg.num_sms * 8, 256, s, a);
-    launches += 3;
+    launches += 2;
   }
   if (ev)
     cudaEventRecord(ev[3], s);
@@ -3192,12 +3323,6 @@ __global__ void __launch_bounds__(256) k_b_items(const FrameArgs *__restrict__ f
   }
 }
 
-__global__ void __launch_bounds__(1024) k_b_large_scan(const FrameArgs *__restrict__ fr) {
-  __shared__ uint32_t part[1024];
-  if (fr[blockIdx.x].total_tris)
-    large_scan_block(fr[blockIdx.x], part);
-}
-
 __global__ void __launch_bounds__(256) k_b_resolve(const FrameArgs *__restrict__ fr,
                                                    uint32_t nv) {
   __shared__ uint32_t s_pre[MOPCUDA_MAX_VIEWS + 1];
@@ -3325,7 +3450,7 @@ __device__ __forceinline__ uint32_t post_tiles_of(const PostArgs &p) {
 
 /* Post tiles of the viewports listed in views (all with ssaa SF). */
 template <int SF>
-__global__ void __launch_bounds__(POST_BX *POST_BY) k_b_post(const PostArgs *__restrict__ posts,
+__global__ void __launch_bounds__(POST_BX *POST_BY, 4) k_b_post(const PostArgs *__restrict__ posts,
                                                              const uint32_t *__restrict__ views,
                                                              uint32_t n) {
   __shared__ PostSmem<SF> sm;
@@ -3408,14 +3533,13 @@ int mopcuda_launch_batch(const BatchArgs &b, const PostArgs *posts, const uint32
       k_b_items<ST_CLIP, false><<<cfg.grid_clip, 128, 0, s>>>(fr, nv);
     }
     k_b_items<ST_RSMALL, false><<<cfg.grid_rsmall, cfg.raster_block, 0, s>>>(fr, nv);
-    k_b_large_scan<<<nv, 1024, 0, s>>>(fr);
     k_b_items<ST_RLARGE, false><<<cfg.grid_rlarge, cfg.large_block, 0, s>>>(fr, nv);
     k_b_resolve<<<sms * 8, 256, 0, s>>>(fr, nv);
     if (shadows)
       k_b_shade<true><<<cfg.grid_shade, cfg.shade_block, 0, s>>>(fr, nv, shared_lights ? 1 : 0);
     else
       k_b_shade<false><<<cfg.grid_shade, cfg.shade_block, 0, s>>>(fr, nv, shared_lights ? 1 : 0);
-    launches += 10;
+    launches += 9;
     if (ordered && b.hdr) {
       cudaMemsetAsync(b.frag_head, 0xff, sizeof(uint32_t) * (size_t)b.samples, s);
       k_b_ocount<<<sms * 8, 256, 0, s>>>(fr, nv);

@@ -152,7 +152,8 @@ extern "C" void mopcuda_device_destroy(MopCudaDevice *d) {
   DevArena *arenas[] = {&d->irr,      &d->pf,         &d->brdf,        &d->d_draws,
                         &d->d_lights, &d->clip,       &d->world,       &d->normal,
                         &d->color,    &d->rrec,       &d->srec,
-                        &d->clipq,    &d->keys,       &d->large_list,  &d->large_items,
+                        &d->clipq,    &d->keys[0],    &d->keys[1],     &d->large_list,
+                        &d->large_items,
                         &d->shade_list, &d->counters, &d->pick_xy,     &d->pick_out,
                         &d->deform_params, &d->hdr, &d->frag_head, &d->frags, &d->touched,
                         &d->olist, &d->olist_items, &d->wlist, &d->wlist_items, &d->oscratch, &d->sh_map[0], &d->sh_map[1], &d->sh_d_draws,
@@ -1083,7 +1084,12 @@ static int launch_frame(MopCudaDevice *d) {
   rc |= d->rrec.ensure(sizeof(RasterRec) * (size_t)rcap);
   rc |= d->srec.ensure(sizeof(ShadeRec) * (size_t)rcap);
   rc |= d->clipq.ensure(4ull * ccap);
-  rc |= d->keys.ensure(8ull * S);
+  for (int i = 0; i < 2; i++) {
+    const void *was = d->keys[i].p;
+    rc |= d->keys[i].ensure(8ull * S);
+    if (d->keys[i].p != was)
+      d->keys_clean[i] = 0;
+  }
   rc |= d->large_list.ensure(4ull * lcap);
   rc |= d->large_items.ensure(4ull * lcap);
   rc |= d->shade_list.ensure(4ull * S);
@@ -1149,7 +1155,9 @@ static int launch_frame(MopCudaDevice *d) {
   a.clip_cap = ccap;
   a.width = fb->w;
   a.height = fb->h;
-  a.keys = d->keys.as<unsigned long long>();
+  const int kb = d->keys_cur;
+  a.keys = d->keys[kb].as<unsigned long long>();
+  a.keys_next = d->keys[kb ^ 1].as<unsigned long long>();
   a.large_list = d->large_list.as<uint32_t>();
   a.large_items = d->large_items.as<uint32_t>();
   a.large_cap = lcap;
@@ -1243,11 +1251,18 @@ static int launch_frame(MopCudaDevice *d) {
     CU_TRY(cudaMemcpyAsync(d->d_lights.p, d->h_lights.p, sizeof(LightRec) * d->lights.size(),
                            cudaMemcpyHostToDevice, s));
   CU_TRY(cudaMemsetAsync(d->counters.p, 0, sizeof(Counters), s));
+  /* this frame dirties its key buffer and its shading pass clears the other */
+  const bool keys_clear = d->keys_clean[kb] >= S;
+  d->keys_clean[0] = d->keys_clean[1] = 0;
+  if (!keys_clear)
+    CU_TRY(cudaMemsetAsync(a.keys, 0xff, 8ull * S, s));
   d->rb_defer_rc = MOPCUDA_OK;
   d->launches += (uint64_t)mopcuda_launch_frame(a, p, d->cfg, s,
                                                 d->stage_timing ? d->stage_ev : nullptr,
                                                 frame_pre_post, d);
   CU_TRY(cudaGetLastError());
+  d->keys_clean[kb ^ 1] = S;
+  d->keys_cur = kb ^ 1;
   CU_TRY(cudaMemcpyAsync(d->h_counters.p, d->counters.p, sizeof(Counters), cudaMemcpyDeviceToHost,
                          s));
   CU_TRY(cudaEventRecord(d->ev1, s));
@@ -1299,6 +1314,9 @@ static int finish_frame(MopCudaDevice *d, int timeout_ms, bool defer_readback) {
       }
       break;
     }
+    if (c->overflow & 512u)
+      return fail(MOPCUDA_EUNSUPPORTED,
+                  "frame: the large triangles' raster items exceed 2^32 in one frame");
     if (attempt >= 4)
       return fail(MOPCUDA_ENOMEM, "frame arenas overflowed repeatedly (flags %u)", c->overflow);
     d->rec_hint = c->rec_count + c->rec_count / 4 + 1024;

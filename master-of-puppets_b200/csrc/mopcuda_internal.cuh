@@ -13,6 +13,7 @@
 #define MOPCUDA_INTERNAL_CUH
 
 #include <cuda_runtime.h>
+#include <stddef.h>
 #include <stdint.h>
 
 #include "fold.h"
@@ -128,22 +129,29 @@ struct __align__(16) ShadeRec {
 };
 
 /* Frame counters and error flags, zeroed at frame start. */
-struct Counters {
+struct alignas(8) Counters {
   uint32_t rec_count;         /* fan records of clipped triangles (overflow region) */
   uint32_t extra_vertices;
+  /* one 64-bit counter: low word the items of the large records pushed so far
+   * (their list offsets, ascending with the list index), high word the number
+   * of large records (rasterised as (row, chunk) items); 8-byte aligned */
+  uint32_t large_items;
+  uint32_t large_count;
   uint32_t clip_count;
-  uint32_t large_count;       /* records rasterised as (row, chunk) items       */
-  uint32_t large_items;       /* total items of the large records                */
   uint32_t overflow;          /* bit0 records, bit1 extra vertices, bit2 clip
-                                 queue, bit3 large list                          */
+                                 queue, bit3 large list, bit9 large-record
+                                 items past 2^32                               */
   uint32_t shade_count;       /* covered samples queued for shading              */
   /* ordered (blended) suffix of the frame; overflow bit4 fragment pool,
    * bit5 ordered-record list, bit7 wireframe-record list */
   uint32_t frag_count, touched_count, olist_count, olist_items;
   uint32_t wire_count, wire_items; /* wireframe records queued, their plots */
   uint32_t scratch_count;          /* sort-scratch entries taken by long lists */
-  uint32_t pad;
+  uint32_t pad[2];
 };
+/* arrays of counters (one per viewport) keep the 64-bit pair aligned */
+static_assert(sizeof(Counters) % 8 == 0 && offsetof(Counters, large_items) % 8 == 0,
+              "large-record counter pair must be 8-byte aligned");
 
 /* Blended fragments of one sample sorted in registers; a sample with more
  * sorts its list in the fold's global scratch (heapsort). */
@@ -178,8 +186,10 @@ struct FrameArgs {
   /* visibility */
   int width, height;                /* sample resolution */
   unsigned long long *keys;         /* per sample: depth_key << 32 | order */
+  unsigned long long *keys_next;    /* the next frame's key buffer, cleared by k_shade
+                                       (null: none) */
   uint32_t *large_list;             /* record ids of large records */
-  uint32_t *large_items;            /* their item counts, then exclusive offsets */
+  uint32_t *large_items;            /* offset of each one's first item (ascending) */
   uint32_t large_cap;
   uint32_t *shade_list;             /* covered sample indices */
   Counters *ctr;
